@@ -1,0 +1,232 @@
+"""g3sa_b200 -- B200-native BWA-MEM seed extension (ksw_extend2 + band retry).
+
+The product is the native library ``libg3x.so`` (sm_100a kernels behind the C ABI in
+``include/g3x.h``).  This module is the Python host mirror used by the tests and the
+benchmark: numpy record types matching the C structs, a ctypes binding of the C ABI, and
+helpers that move torch tensors (device memory and streams) through it.  There is no
+Python or CPU fallback for the extension itself: if ``libg3x.so`` cannot be loaded, every
+call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libg3x.so")
+SYNTH_PATH = os.path.join(HERE, "libg3x_synth.so")
+
+# ---- status codes (include/g3x.h) ------------------------------------------------------
+G3X_OK = 0
+G3X_ERR_INVALID = -1
+G3X_ERR_SCORE = -2
+G3X_ERR_TOO_LONG = -3
+G3X_ERR_CUDA = -4
+G3X_ERR_TIMEOUT = -5
+G3X_ERR_INTERNAL = -6
+G3X_ERR_NOMEM = -7
+G3X_ERR_NOT_TRAINED = -8
+
+SCHED_PLAIN, SCHED_SORTED, SCHED_LEARNED = 0, 1, 2
+JOB_QREV, JOB_TREV = 1, 2
+
+# ---- record types (byte-identical to the C structs) -------------------------------------
+SCORE_DT = np.dtype([("mat", "i1", 25), ("pad_", "i1", 3), ("m", "<i4"), ("o_del", "<i4"),
+                     ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4"), ("zdrop", "<i4"),
+                     ("end_bonus", "<i4")])
+JOB_DT = np.dtype([("q_off", "<u4"), ("t_off", "<u4"), ("qlen", "<u2"), ("tlen", "<u2"),
+                   ("h0", "<i4"), ("w", "<i4"), ("flags", "<u4")])
+EXT_DT = np.dtype([("score", "<i4"), ("qle", "<i4"), ("tle", "<i4"), ("gtle", "<i4"),
+                   ("gscore", "<i4"), ("max_off", "<i4")])
+SEED_DT = np.dtype([("read_off", "<i8"), ("win_off", "<i8"), ("rmax0", "<i8"), ("rmax1", "<i8"),
+                    ("rbeg", "<i8"), ("l_query", "<i4"), ("qbeg", "<i4"), ("len", "<i4"),
+                    ("pad_", "<i4")])
+BATCH_OPTS_DT = np.dtype([("schedule", "<i4"), ("max_qlen", "<i4"), ("max_tlen", "<i4"),
+                          ("lanes", "<i4"), ("d_cells", "<u8")])
+SYNTH_PARAMS_DT = np.dtype([("kind", "<i4"), ("n", "<i4"), ("w", "<i4"), ("a", "<i4"),
+                            ("o_del", "<i4"), ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4"),
+                            ("threads", "<i4"), ("pad_", "<i4"), ("unrelated", "<f8"),
+                            ("seed", "<u8")])
+assert SCORE_DT.itemsize == 56 and JOB_DT.itemsize == 24 and EXT_DT.itemsize == 24
+assert SEED_DT.itemsize == 56
+
+
+def bwa_matrix(a=1, b=4):
+    """bwa_fill_scmat (bwa/src/fastmap.cpp:115-124): match a, mismatch -b, N row/column -1."""
+    m = np.full((5, 5), -1, np.int8)
+    for i in range(4):
+        for j in range(4):
+            m[i, j] = a if i == j else -b
+    return m.ravel()
+
+
+def default_score(a=1, b=4, o_del=6, e_del=1, o_ins=6, e_ins=1, zdrop=100, end_bonus=5):
+    """mem_opt_init defaults (bwa/src/fastmap.cpp:77-113); end_bonus = pen_clip5/3."""
+    s = np.zeros(1, SCORE_DT)
+    s["mat"][0] = bwa_matrix(a, b)
+    s["m"] = 5
+    s["o_del"], s["e_del"], s["o_ins"], s["e_ins"] = o_del, e_del, o_ins, e_ins
+    s["zdrop"], s["end_bonus"] = zdrop, end_bonus
+    return s
+
+
+# ---- native libraries ------------------------------------------------------------------
+_lib = None
+_synth = None
+
+
+def lib():
+    """The product library.  Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libg3x.so is not built (python -m g3sa_b200.build)")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I32 = ctypes.c_void_p, ctypes.c_int32
+        L.g3x_ctx_create.argtypes = [ctypes.POINTER(P), ctypes.c_int]
+        L.g3x_ctx_create.restype = ctypes.c_int
+        L.g3x_ctx_destroy.argtypes = [P]
+        L.g3x_ctx_destroy.restype = ctypes.c_int
+        L.g3x_strerror.argtypes = [ctypes.c_int]
+        L.g3x_strerror.restype = ctypes.c_char_p
+        L.g3x_ksw_extend2_batch.argtypes = [P, P, P, I32, P, P, P, P, P, P]
+        L.g3x_ksw_extend2_batch.restype = ctypes.c_int
+        L.g3x_pack_codes.argtypes = [P, ctypes.c_int64, P, P, ctypes.c_int64]
+        L.g3x_pack_codes.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def synth_lib():
+    global _synth
+    if _synth is None:
+        if not os.path.exists(SYNTH_PATH):
+            raise RuntimeError("libg3x_synth.so is not built (python -m g3sa_b200.build)")
+        L = ctypes.CDLL(SYNTH_PATH)
+        P = ctypes.c_void_p
+        L.g3x_synth_create.argtypes = [P]
+        L.g3x_synth_create.restype = P
+        L.g3x_synth_count.argtypes = [P, ctypes.c_int]
+        L.g3x_synth_count.restype = ctypes.c_int64
+        L.g3x_synth_copy.argtypes = [P, P, P, P]
+        L.g3x_synth_copy.restype = ctypes.c_int
+        L.g3x_synth_free.argtypes = [P]
+        L.g3x_synth_free.restype = None
+        L.g3x_synth_pack.argtypes = [P, ctypes.c_int64, P, P, ctypes.c_int]
+        L.g3x_synth_pack.restype = ctypes.c_int
+        _synth = L
+    return _synth
+
+
+def strerror(code):
+    return lib().g3x_strerror(int(code)).decode()
+
+
+class G3xError(RuntimeError):
+    def __init__(self, code, what=""):
+        super().__init__(f"{what}: {strerror(code)} ({code})" if what else f"{strerror(code)} ({code})")
+        self.code = code
+
+
+def _check(rc, what):
+    if rc != G3X_OK:
+        raise G3xError(rc, what)
+
+
+# ---- synthetic workloads ---------------------------------------------------------------
+class Workload:
+    """A generated job set: u8 codes (one byte per base), jobs (JOB_DT) indexing it, seeds."""
+
+    def __init__(self, u8, jobs, seeds):
+        self.u8, self.jobs, self.seeds = u8, jobs, seeds
+        self._planes = None
+
+    @property
+    def n(self):
+        return len(self.jobs)
+
+    def planes(self, threads=0):
+        """2-bit codes and N-mask planes (uint32) of the whole u8 buffer, base index = byte."""
+        if self._planes is None:
+            self._planes = pack_planes(self.u8, threads)
+        return self._planes
+
+    def cells_upper(self):
+        return int((self.jobs["qlen"].astype(np.int64) * self.jobs["tlen"]).sum())
+
+
+def synth(kind, n, seed, w=100, unrelated=0.2, threads=0, a=1, o_del=6, e_del=1, o_ins=6, e_ins=1):
+    """Seeded synthetic jobs; kinds 1 (right extensions), 2 (seeds -> left/right), 4 (long)."""
+    L = synth_lib()
+    p = np.zeros(1, SYNTH_PARAMS_DT)
+    p["kind"], p["n"], p["w"], p["a"] = kind, n, w, a
+    p["o_del"], p["e_del"], p["o_ins"], p["e_ins"] = o_del, e_del, o_ins, e_ins
+    p["threads"], p["unrelated"], p["seed"] = threads, unrelated, seed
+    h = L.g3x_synth_create(p.ctypes.data)
+    if not h:
+        raise ValueError("bad synth parameters")
+    try:
+        nj, nb, ns = (L.g3x_synth_count(h, k) for k in range(3))
+        jobs = np.zeros(nj, JOB_DT)
+        u8 = np.zeros(max(nb, 1), np.uint8)
+        seeds = np.zeros(ns, SEED_DT)
+        L.g3x_synth_copy(h, jobs.ctypes.data, u8.ctypes.data, seeds.ctypes.data)
+    finally:
+        L.g3x_synth_free(h)
+    return Workload(u8[:nb] if nb else u8[:0], jobs, seeds)
+
+
+def pack_planes(u8, threads=0):
+    n = len(u8)
+    codes = np.zeros((n + 31) // 32 * 2 + 2, np.uint32)
+    nmask = np.zeros((n + 31) // 32 + 1, np.uint32)
+    u8 = np.ascontiguousarray(u8, np.uint8)
+    synth_lib().g3x_synth_pack(u8.ctypes.data, n, codes.ctypes.data, nmask.ctypes.data, threads)
+    return codes, nmask
+
+
+# ---- device-side API -------------------------------------------------------------------
+class Context:
+    """A g3x_ctx bound to one CUDA device."""
+
+    def __init__(self, device=0):
+        self._h = ctypes.c_void_p()
+        _check(lib().g3x_ctx_create(ctypes.byref(self._h), int(device)), "g3x_ctx_create")
+        self.device = device
+
+    def close(self):
+        if self._h:
+            lib().g3x_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def extend_batch(self, score, d_jobs, n, d_codes, d_nmask, d_out, d_status, max_qlen,
+                     max_tlen, schedule=SCHED_PLAIN, lanes=0, d_cells=None, stream=None):
+        """g3x_ksw_extend2_batch on torch device tensors (or raw device pointers)."""
+        opts = np.zeros(1, BATCH_OPTS_DT)
+        opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
+            schedule, max_qlen, max_tlen, lanes)
+        opts["d_cells"] = _ptr(d_cells) if d_cells is not None else 0
+        rc = lib().g3x_ksw_extend2_batch(self._h, score.ctypes.data, _ptr(d_jobs), int(n),
+                                         _ptr(d_codes), _ptr(d_nmask), _ptr(d_out),
+                                         _ptr(d_status), opts.ctypes.data, _stream(stream))
+        _check(rc, "g3x_ksw_extend2_batch")
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def _stream(s):
+    if s is None:
+        return None
+    return s.cuda_stream if hasattr(s, "cuda_stream") else int(s)

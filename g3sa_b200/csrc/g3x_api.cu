@@ -1,0 +1,130 @@
+// g3x_api.cu -- host side of the C ABI declared in include/g3x.h.
+#include <cuda_runtime.h>
+#include <stdlib.h>
+#include <string.h>
+#include <new>
+#include "g3x_internal.h"
+
+struct g3x_ctx {
+    int device;
+    int sms;
+    int32_t* d_queue;      // persistent-kernel job counter
+};
+
+namespace {
+
+int score_params(const g3x_score_t* s, g3x::ScoreParams* sp) {
+    if (!s) return G3X_ERR_INVALID;
+    if (s->m != 5 || s->e_del <= 0 || s->e_ins <= 0 || s->o_del < 0 || s->o_ins < 0)
+        return G3X_ERR_SCORE;
+    memset(sp, 0, sizeof(*sp));
+    int max_sc = 0;
+    for (int k = 0; k < 25; ++k) {
+        sp->mat[k] = s->mat[k];
+        if (s->mat[k] > max_sc) max_sc = s->mat[k];
+    }
+    sp->o_del = s->o_del; sp->e_del = s->e_del; sp->o_ins = s->o_ins; sp->e_ins = s->e_ins;
+    sp->zdrop = s->zdrop; sp->end_bonus = s->end_bonus; sp->max_sc = max_sc;
+    return G3X_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* g3x_strerror(int code) {
+    switch (code) {
+        case G3X_OK: return "ok";
+        case G3X_ERR_INVALID: return "invalid argument";
+        case G3X_ERR_SCORE: return "unsupported scoring (m must be 5, gap extensions > 0)";
+        case G3X_ERR_TOO_LONG: return "job exceeds the length limits";
+        case G3X_ERR_CUDA: return "CUDA runtime error";
+        case G3X_ERR_TIMEOUT: return "bounded device wait gave up";
+        case G3X_ERR_INTERNAL: return "device consistency check failed";
+        case G3X_ERR_NOMEM: return "out of device memory for library scratch";
+        case G3X_ERR_NOT_TRAINED: return "learned schedule requested before a model was set";
+        default: return "unknown error";
+    }
+}
+
+int g3x_ctx_create(g3x_ctx** out, int device) {
+    if (!out) return G3X_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return G3X_ERR_CUDA;
+    if (cudaSetDevice(device) != cudaSuccess) return G3X_ERR_CUDA;
+    g3x_ctx* c = new (std::nothrow) g3x_ctx();
+    if (!c) return G3X_ERR_NOMEM;
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaMalloc(&c->d_queue, 64 * sizeof(int32_t)) != cudaSuccess) {
+        delete c;
+        return G3X_ERR_NOMEM;
+    }
+    *out = c;
+    return G3X_OK;
+}
+
+int g3x_ctx_destroy(g3x_ctx* c) {
+    if (!c) return G3X_ERR_INVALID;
+    cudaSetDevice(c->device);
+    cudaFree(c->d_queue);
+    delete c;
+    return G3X_OK;
+}
+
+int g3x_ksw_extend2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs,
+                          int32_t n, const uint32_t* d_codes, const uint32_t* d_nmask,
+                          g3x_ext_t* d_out, int32_t* d_status, const g3x_batch_opts_t* opts,
+                          void* stream) {
+    if (!ctx || !opts || n < 0) return G3X_ERR_INVALID;
+    if (n == 0) return G3X_OK;
+    if (!d_jobs || !d_codes || !d_nmask || !d_out || !d_status) return G3X_ERR_INVALID;
+    if (opts->max_qlen < 0 || opts->max_tlen < 0 || opts->max_qlen > 65534) return G3X_ERR_INVALID;
+    g3x::ScoreParams sp;
+    int rc = score_params(score, &sp);
+    if (rc) return rc;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    g3x::LaunchDesc d;
+    memset(&d, 0, sizeof(d));
+    d.jobs = d_jobs; d.codes = d_codes; d.nmask = d_nmask; d.out = d_out; d.status = d_status;
+    d.cells = opts->d_cells; d.n = n; d.qmax = opts->max_qlen; d.tmax = opts->max_tlen;
+    switch (opts->schedule) {
+        case G3X_SCHED_PLAIN:
+            d.lanes = 32; d.persistent = 0; d.warps_per_block = 1;
+            break;
+        case G3X_SCHED_SORTED:
+        case G3X_SCHED_LEARNED: {
+            int lanes = opts->lanes ? opts->lanes : 16;
+            if (lanes != 8 && lanes != 16 && lanes != 32) return G3X_ERR_INVALID;
+            // Shared memory per job grows with the query; a warp of narrow groups must fit.
+            if (!opts->lanes)
+                while (lanes < 32 && (32 / lanes) * g3x::group_smem_bytes(d.qmax, d.tmax) > 227 * 1024)
+                    lanes *= 2;
+            d.lanes = lanes; d.persistent = 1; d.warps_per_block = 4;
+            d.queue = ctx->d_queue;
+            if (cudaMemsetAsync(ctx->d_queue, 0, sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
+            break;
+        }
+        default:
+            return G3X_ERR_INVALID;
+    }
+    return g3x::launch_extend(d, sp, st);
+}
+
+int g3x_pack_codes(const uint8_t* h_seq, int64_t len, uint32_t* h_codes, uint32_t* h_nmask,
+                   int64_t base) {
+    if (len < 0 || base < 0 || (len && (!h_seq || !h_codes || !h_nmask))) return G3X_ERR_INVALID;
+    for (int64_t k = 0; k < len; ++k) {
+        int64_t b = base + k;
+        uint32_t c = h_seq[k];
+        uint32_t sh = (uint32_t)(b & 15) << 1;
+        h_codes[b >> 4] = (h_codes[b >> 4] & ~(3u << sh)) | ((c & 3u) << sh);
+        uint32_t nb = 1u << (b & 31);
+        if (c > 3) h_nmask[b >> 5] |= nb; else h_nmask[b >> 5] &= ~nb;
+    }
+    return G3X_OK;
+}
+
+}  // extern "C"

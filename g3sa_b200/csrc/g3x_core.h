@@ -1,0 +1,240 @@
+// g3x_core.h -- per-lane step logic of the banded-extension wavefront.
+//
+// One job (one ksw_extend2 call, bwa/src/ksw.cu:303-401) is processed by a group of G
+// lanes.  Lane r of the group owns target rows r, r+G, r+2G, ... ("rolling rows"); a lane
+// walks its row left to right one cell per step and trails the lane that owns the
+// previous row, so the group sweeps anti-diagonals.  The reference's single row buffer
+// eh[] (ksw.cu:310) is kept verbatim in shared memory: every row reads and overwrites it
+// at the same positions, in the same row order, as the scalar loop does, so the stale
+// entries the reference reads when its band grows by two columns (ksw.cu:388-391) hold
+// the same values here.
+//
+// The scalar loop decides the band of row i+1 only after row i has finished
+// (ksw.cu:388-391).  Here the lane that owns row i+1 instead watches, every step, how far
+// row i has got (`col`: columns < col are final) and the last non-zero entry row i has
+// written (`lnz1` = that column + 1).  Column j of row i+1 is inside the reference's band
+// exactly when j <= L_i + 1 (L_i = row i's last non-zero), so the lane computes cell j as
+// soon as row i has written a non-zero entry at column >= j-1, and ends the row once row i
+// is finished and has none.  The left edge uses the first non-zero entry of row i
+// (`fnz`), and the fixed band limits i-w and i+w+1 are applied as in ksw.cu:338-340.
+// Rows therefore end in row order, one per step at most, and the per-row bookkeeping of
+// ksw.cu:371-386 (to-end score, max tracking, z-drop) is applied in row order by a
+// uniform "commit" over the group.  Rows started after the row that ends the extension
+// are speculative and are discarded.
+//
+// Everything in this header is plain C++ usable on the host as well, so a CPU model of
+// the warp protocol (g3x_emu.cpp, test-only) runs this same code.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define G3X_HD __host__ __device__ __forceinline__
+#else
+#define G3X_HD inline
+#endif
+
+namespace g3x {
+
+constexpr uint32_t kNone = 0xFFFFu;   // "no column yet" / "row finished" marker
+
+enum LaneState : int32_t { kIdle = 0, kWait = 1, kRun = 2, kDone = 3 };
+
+// Per-job constants, derived once at job start (ksw.cu:305-333).
+struct JobConst {
+    int32_t qlen, tlen, w, h0;
+    int32_t o_del, e_del, o_ins, e_ins, oe_del, oe_ins, zdrop;
+};
+
+// One H/E entry of the reference's row buffer (eh_t, ksw.cu:299-301).
+struct EhCell {
+    int32_t h, e;
+};
+
+// What one lane carries for the row it owns.
+struct Lane {
+    int32_t st;     // LaneState
+    int32_t i;      // row (target position)
+    int32_t j;      // next column to compute
+    int32_t beg;    // first column of the row
+    int32_t cap;    // min(i + w + 1, qlen): fixed right limit of the band
+    int32_t h1;     // H(i, j-1)
+    int32_t f;      // F(i, j)
+    int32_t m, mj;  // row maximum and the last column reaching it
+    int32_t fnz;    // first column whose new eh entry is non-zero (kNone: none yet)
+    int32_t lnz1;   // 1 + last column whose new eh entry is non-zero (0: none)
+    int32_t qrow;   // offset of this row's query-profile row
+};
+
+// What a lane hands to the group when its row ends.
+struct RowDone {
+    int32_t m, mj;
+    int32_t gval;   // H at the last column when the row reached qlen, else -1
+    int32_t ncells; // cells computed in the row (trip count of ksw.cu:346)
+};
+
+// Group-uniform result state (ksw.cu:331-333 and the outputs of ksw.cu:395-400).
+struct Commit {
+    int32_t next;       // next row to commit
+    int32_t stop;       // extension finished (break or last row)
+    int32_t best, best_i, best_j;
+    int32_t gscore, max_ie, max_off;
+    int64_t cells;
+};
+
+// Band clamp, ksw.cu:321-329, in integer form: (int)((double)num/e + 1.) clamped to >= 1
+// equals num/e + 1 for num >= 0 and 1 for num < 0 (e > 0).
+G3X_HD int32_t gap_limit(int32_t qlen, int32_t max_sc, int32_t end_bonus, int32_t o, int32_t e) {
+    int32_t num = qlen * max_sc + end_bonus - o;
+    int32_t v = num >= 0 ? num / e + 1 : 1;
+    return v > 1 ? v : 1;
+}
+
+G3X_HD int32_t clamp_w(int32_t w, int32_t qlen, int32_t max_sc, int32_t end_bonus,
+                       int32_t o_del, int32_t e_del, int32_t o_ins, int32_t e_ins) {
+    int32_t a = gap_limit(qlen, max_sc, end_bonus, o_ins, e_ins);
+    int32_t b = gap_limit(qlen, max_sc, end_bonus, o_del, e_del);
+    w = w < a ? w : a;
+    return w < b ? w : b;
+}
+
+// Row "-1" of the buffer (ksw.cu:317-319) in closed form: h0 at 0, then the insertion
+// scores h0 - oe_ins - (j-1)*e_ins while positive, zero beyond; e is zero everywhere.
+G3X_HD int32_t init_h(int32_t j, const JobConst& c) {
+    if (j == 0) return c.h0;
+    int32_t v1 = c.h0 > c.oe_ins ? c.h0 - c.oe_ins : 0;
+    if (j > c.qlen) return j == 1 ? v1 : 0;   // only eh[1] of an empty query is written
+    int32_t v = v1 - (j - 1) * c.e_ins;
+    return v > 0 ? v : 0;
+}
+
+G3X_HD void commit_init(Commit& k, const JobConst& c) {
+    k.next = 0;
+    k.stop = c.tlen <= 0;
+    k.best = c.h0; k.best_i = -1; k.best_j = -1;
+    k.gscore = -1; k.max_ie = -1; k.max_off = 0;
+    k.cells = 0;
+}
+
+// Row bookkeeping of ksw.cu:372-386 for the next row in order.
+G3X_HD void commit_row(Commit& k, const JobConst& c, const RowDone& d) {
+    const int32_t i = k.next;
+    if (d.gval >= 0) {                                   // row reached qlen (ksw.cu:372-375)
+        if (!(k.gscore > d.gval)) k.max_ie = i;
+        if (d.gval > k.gscore) k.gscore = d.gval;
+    }
+    k.cells += d.ncells;
+    k.next = i + 1;
+    if (d.m == 0) { k.stop = 1; return; }                // ksw.cu:376
+    if (d.m > k.best) {                                  // ksw.cu:377-379
+        k.best = d.m; k.best_i = i; k.best_j = d.mj;
+        int32_t off = d.mj > i ? d.mj - i : i - d.mj;
+        if (off > k.max_off) k.max_off = off;
+    } else if (c.zdrop > 0) {                            // ksw.cu:380-386
+        int32_t di = i - k.best_i, dj = d.mj - k.best_j;
+        if (di > dj) {
+            if (k.best - d.m - (di - dj) * c.e_del > c.zdrop) { k.stop = 1; return; }
+        } else {
+            if (k.best - d.m - (dj - di) * c.e_ins > c.zdrop) { k.stop = 1; return; }
+        }
+    }
+    if (k.next >= c.tlen) k.stop = 1;
+}
+
+// The words a lane publishes to its successor each step.
+G3X_HD uint32_t lane_prog(const Lane& L) {
+    uint32_t col = L.st == kDone ? kNone : (L.st == kRun ? (uint32_t)L.j : 0u);
+    uint32_t lnz = (L.st == kDone || L.st == kRun) ? (uint32_t)L.lnz1 : 0u;
+    return (col << 16) | lnz;
+}
+G3X_HD uint32_t lane_fnz(const Lane& L) {
+    return (L.st == kDone || L.st == kRun) ? (uint32_t)L.fnz : kNone;
+}
+
+G3X_HD void lane_begin_row(Lane& L, int32_t beg, const JobConst& c, int32_t tcode,
+                           int32_t qstride) {
+    L.st = kRun;
+    L.beg = beg;
+    L.j = beg;
+    int32_t cap = L.i + c.w + 1;
+    L.cap = cap < c.qlen ? cap : c.qlen;
+    if (beg == 0) {                                      // ksw.cu:342-345
+        int32_t h = c.h0 - (c.o_del + c.e_del * (L.i + 1));
+        L.h1 = h > 0 ? h : 0;
+    } else {
+        L.h1 = 0;
+    }
+    L.f = 0; L.m = 0; L.mj = -1;
+    L.fnz = (int32_t)kNone; L.lnz1 = 0;
+    L.qrow = tcode * qstride;
+}
+
+// One step of one lane.  `pprog`/`pfnz` are the predecessor's published words at the start
+// of the step; `committed` is the group's Commit::next.  Returns true when the lane's row
+// ended in this step (then *done is filled).  `eh`, `qp` and `tgt` are the job's buffers.
+template <class EhT>
+G3X_HD bool lane_step(Lane& L, const JobConst& c, uint32_t pprog, uint32_t pfnz,
+                      int32_t committed, int32_t G, EhT* eh, const int8_t* qp,
+                      const uint8_t* tgt, int32_t qstride, RowDone* done) {
+    if (L.st == kWait) {
+        if (L.i == 0) {
+            int32_t b = -c.w;
+            lane_begin_row(L, b > 0 ? b : 0, c, tgt[0], qstride);
+        } else if (pfnz != kNone) {
+            int32_t b = L.i - c.w;
+            lane_begin_row(L, (int32_t)pfnz > b ? (int32_t)pfnz : b, c, tgt[L.i], qstride);
+        }
+        return false;
+    }
+    if (L.st == kDone) {
+        if (committed >= L.i + 2 || L.i + 1 >= c.tlen) {
+            L.i += G;
+            L.st = L.i < c.tlen ? kWait : kIdle;
+        }
+        return false;
+    }
+    if (L.st != kRun) return false;
+    uint32_t colp = pprog >> 16, lnzp = pprog & 0xFFFFu;
+    if (L.i == 0) { colp = kNone; lnzp = kNone; }        // row 0 reads the initial buffer
+    const bool pdone = colp == kNone;
+    const int32_t j = L.j;
+    if (j < L.cap && (uint32_t)j < colp && (uint32_t)j <= lnzp) {
+        // One cell of ksw.cu:346-370.
+        EhCell v = eh[j].load();
+        int32_t s = qp[L.qrow + j];
+        int32_t M = v.h ? v.h + s : 0;
+        int32_t h = M > v.e ? M : v.e;
+        h = h > L.f ? h : L.f;
+        int32_t t = M - c.oe_del; t = t > 0 ? t : 0;
+        int32_t e = v.e - c.e_del; e = e > t ? e : t;
+        eh[j].store(L.h1, e);
+        if ((L.h1 | e) != 0) {
+            L.lnz1 = j + 1;
+            if (L.fnz == (int32_t)kNone) L.fnz = j;
+        }
+        L.h1 = h;
+        if (h >= L.m) { L.m = h; L.mj = j; }
+        t = M - c.oe_ins; t = t > 0 ? t : 0;
+        int32_t f = L.f - c.e_ins; L.f = f > t ? f : t;
+        L.j = j + 1;
+    }
+    const int32_t jn = L.j;
+    if (jn >= L.cap || (pdone && (uint32_t)jn > lnzp)) {
+        // Row end, ksw.cu:371-375.  For an empty row (jn == beg) the reference's loop
+        // variable is beg, its eh[end] write is never read again (the row breaks), and the
+        // to-end test uses the row's initial h1.
+        if (jn > L.beg) {
+            eh[jn].store(L.h1, 0);
+            if (L.h1 != 0) L.lnz1 = jn + 1;
+        }
+        if (L.fnz == (int32_t)kNone) L.fnz = jn;
+        done->m = L.m;
+        done->mj = L.mj;
+        done->gval = jn == c.qlen ? L.h1 : -1;
+        done->ncells = jn - L.beg;
+        L.st = kDone;
+        return true;
+    }
+    return false;
+}
+
+}  // namespace g3x

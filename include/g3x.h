@@ -1,0 +1,122 @@
+/*
+ * g3x.h -- C ABI of the B200 BWA-MEM seed-extension library (libg3x.so).
+ *
+ * The library replaces the seed-extension stage of the sunwookim028/G3SA bwa/ pipeline:
+ * the per-job device function
+ *     int ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+ *                     int m, const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins,
+ *                     int w, int end_bonus, int zdrop, int h0, int *_qle, int *_tle,
+ *                     int *_gtle, int *_gscore, int *_max_off, void *d_buffer_ptr)
+ *     (bwa/src/ksw.h:33, bwa/src/ksw.cu:303-401)
+ * and its callers: the left/right band-retry loop of mem_chain2aln
+ * (bwa/src/aux.cu:250-301, MAX_BAND_TRY at bwa/src/aux.cuh:401) and the batch stage kernel
+ * localExtending (bwa/src/aux.cuh:208-214, launched at bwa/src/bwamem.cu:276).
+ *
+ * Every output (score, qle, tle, gtle, gscore, max_off) is bit-identical to the
+ * reference's CPU ksw_extend2 on the same inputs.
+ *
+ * Conventions
+ *   - Return value: 0 (G3X_OK) or a negative G3X_ERR_* code; g3x_strerror() names it.
+ *     Nothing traps and nothing calls exit().
+ *   - d_* pointers are device memory owned by the caller; h_* pointers are host memory.
+ *   - A g3x_ctx is bound to one GPU and one host thread at a time (not thread-safe).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Sequences travel as two bit planes over one base index space:
+ *   codes[b >> 4] bits 2*(b & 15) .. +1   : 2-bit base code (A=0 C=1 G=2 T=3)
+ *   nmask[b >> 5] bit  (b & 31)           : 1 = ambiguous base N (code 4)
+ * A job names its query and target by their first base index and length.
+ */
+#ifndef G3X_H
+#define G3X_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------------------- */
+#define G3X_OK                 0
+#define G3X_ERR_INVALID       -1   /* bad argument (null pointer, n < 0, bad option) */
+#define G3X_ERR_SCORE         -2   /* scoring the kernels do not support (m != 5, e <= 0) */
+#define G3X_ERR_TOO_LONG      -3   /* a job exceeds the length limits (per-job status) */
+#define G3X_ERR_CUDA          -4   /* a CUDA runtime call failed */
+#define G3X_ERR_TIMEOUT       -5   /* a bounded device wait gave up (per-job status) */
+#define G3X_ERR_INTERNAL      -6   /* a device-side consistency check failed (per-job) */
+#define G3X_ERR_NOMEM         -7   /* allocation of library-owned scratch failed */
+#define G3X_ERR_NOT_TRAINED   -8   /* learned schedule requested before a model was set */
+
+/* ---- data records -------------------------------------------------------------------- */
+
+/* Scoring, as mem_opt_t carries it (bwa/src/bwa.h:157-189; defaults bwa/src/fastmap.cpp:77-124:
+   a=1 b=4 o=6 e=1 zdrop=100 pen_clip=5, mat from bwa_fill_scmat). mat[t*5 + q] scores target
+   code t against query code q, as the query profile at bwa/src/ksw.cu:312-315 indexes it. */
+typedef struct {
+    int8_t  mat[25];
+    int8_t  pad_[3];
+    int32_t m;            /* alphabet size; must be 5 */
+    int32_t o_del, e_del, o_ins, e_ins;
+    int32_t zdrop;
+    int32_t end_bonus;    /* only clamps the band, as in bwa/src/ksw.cu:325-329 */
+} g3x_score_t;            /* 56 bytes */
+
+/* One extension job = one ksw_extend2 call. */
+#define G3X_JOB_QREV 1u   /* read the query backwards: query[k] = base q_off + qlen-1-k */
+#define G3X_JOB_TREV 2u   /* read the target backwards */
+typedef struct {
+    uint32_t q_off;       /* base index of the query's first base in the planes */
+    uint32_t t_off;       /* base index of the target's first base */
+    uint16_t qlen, tlen;  /* qlen <= 65534 */
+    int32_t  h0;          /* score of the seed (ksw_extend2's h0) */
+    int32_t  w;           /* band width before clamping */
+    uint32_t flags;       /* G3X_JOB_* */
+} g3x_job_t;              /* 24 bytes */
+
+/* ksw_extend2's return value and out-parameters, in that order. */
+typedef struct {
+    int32_t score, qle, tle, gtle, gscore, max_off;
+} g3x_ext_t;              /* 24 bytes */
+
+/* ---- context ------------------------------------------------------------------------- */
+typedef struct g3x_ctx g3x_ctx;
+
+/* Binds a context to CUDA device `device` (one GPU only). */
+int g3x_ctx_create(g3x_ctx **ctx, int device);
+int g3x_ctx_destroy(g3x_ctx *ctx);
+const char *g3x_strerror(int code);
+
+/* ---- batched ksw_extend2 ------------------------------------------------------------- */
+
+#define G3X_SCHED_PLAIN   0   /* one 32-lane block per job, jobs in the given order */
+#define G3X_SCHED_SORTED  1   /* persistent kernel, jobs ordered by length (fallback) */
+#define G3X_SCHED_LEARNED 2   /* persistent kernel, jobs ordered by the learned cost model */
+
+typedef struct {
+    int32_t schedule;     /* G3X_SCHED_* */
+    int32_t max_qlen;     /* upper bound of qlen over the batch (required) */
+    int32_t max_tlen;     /* upper bound of tlen over the batch (required) */
+    int32_t lanes;        /* lanes per job for persistent schedules: 8, 16, 32, or 0 = tuned */
+    int32_t *d_cells;     /* optional per-job DP cell count (trip count of ksw.cu:346) */
+} g3x_batch_opts_t;
+
+/* n jobs; outputs to d_out[k] and d_status[k] (G3X_OK or a G3X_ERR_* per job).
+   Replaces n calls of ksw_extend2 (bwa/src/ksw.h:33) issued by localExtending
+   (bwa/src/aux.cu:2289-2382). Asynchronous on `stream`. */
+int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs,
+                          int32_t n, const uint32_t *d_codes, const uint32_t *d_nmask,
+                          g3x_ext_t *d_out, int32_t *d_status, const g3x_batch_opts_t *opts,
+                          void *stream);
+
+/* ---- host-side packing ----------------------------------------------------------------- */
+
+/* Packs len u8 codes (0-3 bases, anything else = N) into the planes starting at base index
+   `base` (codes/nmask must be large enough and zero-initialised where not yet written).
+   Replaces the u8 query/target buffers the reference hands ksw_extend2. */
+int g3x_pack_codes(const uint8_t *h_seq, int64_t len, uint32_t *h_codes, uint32_t *h_nmask,
+                   int64_t base);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* G3X_H */

@@ -1,0 +1,48 @@
+#!/bin/sh
+# Builds oracle/_ref/libksw_ref.so: the reference's own ksw_extend2, compiled from its
+# source file where it lies (bwa/src/ksw.cu, lines 299-401 = eh_t + ksw_extend2) as host
+# C++, the reference's own band-retry lines of mem_chain2aln (bwa/src/aux.cu:253-255,
+# 258-301, 309), plus the ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
+# reference tree into the compiler; no reference source is copied into this repository.
+# Usage: sh oracle/build_ref.sh [reference_root]   (default /root/reference)
+set -eu
+HERE=$(cd "$(dirname "$0")" && pwd)
+REF=${1:-${G3X_REFERENCE:-/root/reference}}
+SRC="$REF/bwa/src/ksw.cu"
+OUT="$HERE/_ref"
+if [ ! -f "$SRC" ]; then
+    echo "build_ref.sh: $SRC not found; oracle/_ref not built" >&2
+    exit 2
+fi
+# Guard: the extracted range must be exactly the eh_t typedef and the ksw_extend2 body.
+L299=$(sed -n '299p' "$SRC" | tr -d '\r')
+L303=$(sed -n '303p' "$SRC" | tr -d '\r' | cut -c1-30)
+L401=$(sed -n '401p' "$SRC" | tr -d '\r')
+if [ "$L299" != "typedef struct {" ] || [ "$L303" != "__device__ int ksw_extend2(int" ] || [ "$L401" != "}" ]; then
+    echo "build_ref.sh: unexpected content at ksw.cu:299/303/401; refusing to build" >&2
+    exit 3
+fi
+mkdir -p "$OUT"
+CXX=${CXX:-g++}
+sed -n '299,401p' "$SRC" | tr -d '\r' | \
+    $CXX -O3 -fPIC -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/ksw_ref_fn.o"
+# The band-retry driver: mem_chain2aln's left/right extension lines, unmodified, inside a
+# host function whose locals ref_seed_head.inc declares.
+AUX="$REF/bwa/src/aux.cu"
+AUXH="$REF/bwa/src/aux.cuh"
+A258=$(sed -n '258p' "$AUX" | tr -d '\r' | sed 's/^ *//')
+A301=$(sed -n '301p' "$AUX" | tr -d '\r' | sed 's/^ *//')
+A309=$(sed -n '309p' "$AUX" | tr -d '\r' | sed 's/^ *//')
+if [ "$A258" != "if (s->qbeg) { // left extension" ] || \
+   [ "$A301" != "} else a->qe = l_query, a->re = s->rbeg + s->len;" ] || \
+   [ "$A309" != "a->w = aw[0] > aw[1]? aw[0] : aw[1];" ]; then
+    echo "build_ref.sh: unexpected content at aux.cu:258/301/309; refusing to build" >&2
+    exit 3
+fi
+{ grep -m1 '^#define MAX_BAND_TRY' "$AUXH"; cat "$HERE/ref_seed_head.inc"; \
+  sed -n '253,255p;258,301p;309p' "$AUX"; echo '}'; } | tr -d '\r' | \
+    $CXX -O3 -fPIC -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/seed_ref_fn.o"
+$CXX -O3 -fPIC -shared -std=c++17 "$HERE/ref_wrap.cpp" "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" \
+    -o "$OUT/libksw_ref.so" -lpthread
+rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o"
+echo "built $OUT/libksw_ref.so"

@@ -1,0 +1,405 @@
+/*
+ * ksw_oracle.c -- CPU restatement of BWA-MEM seed extension, used ONLY as test
+ * infrastructure (parity checker and CPU baseline).  Nothing in the product path
+ * (g3sa_b200/) links, loads or calls this file.
+ *
+ * What it restates (paths are relative to the sunwookim028/G3SA tree):
+ *   - ksw_extend2:            bwa/src/ksw.cu:299-401   (eh_t + the banded extension)
+ *   - band-retry driver:      bwa/src/aux.cu:250-301   (left/right extension of one seed,
+ *                                                       MAX_BAND_TRY = 2, aux.cuh:401)
+ *   - cal_max_gap:            bwa/src/aux.cu:168-175
+ *
+ * Parity pin: tests/test_oracle.py checks this restatement against the reference's own
+ * ksw_extend2 compiled from its source (oracle/build_ref.sh -> oracle/_ref/libksw_ref.so)
+ * on seeded jobs, and against the committed golden vectors in tests/golden/ that were
+ * generated from that compiled reference.
+ *
+ * Extra output not present in the reference: the number of DP cells evaluated
+ * (the trip count of the inner loop at ksw.cu:346, summed over the executed rows,
+ * including the row that breaks), and the number of target rows entered.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+
+typedef struct { int32_t h, e; } g3o_eh;          /* ksw.cu:299-301 */
+
+typedef struct {
+    int32_t score, qle, tle, gtle, gscore, max_off;  /* ksw_extend2 return + out params */
+} g3o_ext;
+
+/* Band clamp of ksw.cu:321-329: (int)((double)(qlen*max + end_bonus - o)/e + 1.), >= 1. */
+static int g3o_gap_limit(int qlen, int max_sc, int end_bonus, int o, int e)
+{
+    int v = (int)((double)(qlen * max_sc + end_bonus - o) / e + 1.);
+    return v > 1 ? v : 1;
+}
+
+/*
+ * One banded extension.  Same argument meaning as ksw_extend2 (ksw.h:33); scratch is
+ * malloc'd here instead of coming from the device arena.  *cells / *rows receive the
+ * work counters (may be NULL).
+ */
+static int g3o_extend_impl(int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                           int m, const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins,
+                           int w, int end_bonus, int zdrop, int h0,
+                           int *qle_out, int *tle_out, int *gtle_out, int *gscore_out,
+                           int *max_off_out, int64_t *cells_out, int32_t *rows_out,
+                           int clean_stale, int32_t *stale_reads)
+{
+    const int oe_del = o_del + e_del, oe_ins = o_ins + e_ins;
+    int8_t *prof = (int8_t *)malloc((size_t)(qlen > 0 ? qlen : 1) * m);
+    /* qlen + 2 entries: the reference writes eh[1] even when qlen == 0 (an arena slot
+       past its qlen + 1 entries that is never read back); keep that write in bounds. */
+    g3o_eh *row = (g3o_eh *)calloc((size_t)qlen + 2, sizeof(g3o_eh));
+    int64_t cells = 0;
+    int32_t rows = 0;
+
+    /* query profile, ksw.cu:312-315: prof[k*qlen + j] = mat[k*m + query[j]] */
+    for (int k = 0; k < m; ++k)
+        for (int j = 0; j < qlen; ++j)
+            prof[k * qlen + j] = mat[k * m + query[j]];
+
+    /* row "-1", ksw.cu:317-319 */
+    row[0].h = h0;
+    row[1].h = h0 > oe_ins ? h0 - oe_ins : 0;
+    for (int j = 2; j <= qlen && row[j - 1].h > e_ins; ++j)
+        row[j].h = row[j - 1].h - e_ins;
+
+    /* band clamp, ksw.cu:321-329 */
+    int max_sc = 0;
+    for (int k = 0; k < m * m; ++k)
+        if (mat[k] > max_sc) max_sc = mat[k];
+    {
+        int lim = g3o_gap_limit(qlen, max_sc, end_bonus, o_ins, e_ins);
+        if (w > lim) w = lim;
+        lim = g3o_gap_limit(qlen, max_sc, end_bonus, o_del, e_del);
+        if (w > lim) w = lim;
+    }
+
+    int best = h0, best_i = -1, best_j = -1;   /* ksw.cu:331 */
+    int prev_end = -1;                          /* end of the previous row (-1: row 0) */
+    int32_t stale = 0;
+    int g_best = -1, g_row = -1;                /* gscore, max_ie */
+    int off_max = 0;
+    int beg = 0, end = qlen;
+
+    for (int i = 0; i < tlen; ++i) {           /* ksw.cu:334 */
+        const int8_t *sc = &prof[target[i] * qlen];
+        int f = 0, hleft, rmax = 0, rmax_j = -1, j;
+        ++rows;
+        if (beg < i - w) beg = i - w;           /* ksw.cu:338-340 */
+        if (end > i + w + 1) end = i + w + 1;
+        if (end > qlen) end = qlen;
+        if (beg == 0) {                         /* ksw.cu:342-345: first column */
+            hleft = h0 - (o_del + e_del * (i + 1));
+            if (hleft < 0) hleft = 0;
+        } else {
+            hleft = 0;
+        }
+        for (j = beg; j < end; ++j) {           /* ksw.cu:346-370 */
+            int diag = row[j].h, e = row[j].e, mm, h, t;
+            if (prev_end >= 0 && j > prev_end) {
+                /* entry not written by the previous row: left over from an older row
+                   (the band grew by two columns, ksw.cu:390) */
+                if (diag | e) ++stale;
+                if (clean_stale) { diag = 0; e = 0; }
+            }
+            row[j].h = hleft;
+            mm = diag ? diag + sc[j] : 0;
+            h = mm > e ? mm : e;
+            if (f > h) h = f;
+            hleft = h;
+            if (!(rmax > h)) rmax_j = j;        /* ties move to the later column */
+            if (h > rmax) rmax = h;
+            t = mm - oe_del; if (t < 0) t = 0;
+            e -= e_del;     if (e < t) e = t;
+            row[j].e = e;
+            t = mm - oe_ins; if (t < 0) t = 0;
+            f -= e_ins;     if (f < t) f = t;
+        }
+        cells += (end > beg) ? (end - beg) : 0;
+        row[end].h = hleft;                     /* ksw.cu:371 */
+        row[end].e = 0;
+        prev_end = end;
+        if (j == qlen) {                        /* ksw.cu:372-375: to-end score */
+            if (!(g_best > hleft)) g_row = i;
+            if (hleft > g_best) g_best = hleft;
+        }
+        if (rmax == 0) break;                   /* ksw.cu:376 */
+        if (rmax > best) {                      /* ksw.cu:377-379 */
+            best = rmax; best_i = i; best_j = rmax_j;
+            {
+                int d = rmax_j - i; if (d < 0) d = -d;
+                if (d > off_max) off_max = d;
+            }
+        } else if (zdrop > 0) {                 /* ksw.cu:380-386 */
+            int di = i - best_i, dj = rmax_j - best_j;
+            if (di > dj) {
+                if (best - rmax - (di - dj) * e_del > zdrop) break;
+            } else {
+                if (best - rmax - (dj - di) * e_ins > zdrop) break;
+            }
+        }
+        /* ksw.cu:388-391: shrink the band to the non-zero span of this row */
+        for (j = beg; j < end && row[j].h == 0 && row[j].e == 0; ++j) ;
+        beg = j;
+        for (j = end; j >= beg && row[j].h == 0 && row[j].e == 0; --j) ;
+        end = j + 2 < qlen ? j + 2 : qlen;
+    }
+    free(row);
+    free(prof);
+    if (qle_out) *qle_out = best_j + 1;        /* ksw.cu:395-400 */
+    if (tle_out) *tle_out = best_i + 1;
+    if (gtle_out) *gtle_out = g_row + 1;
+    if (gscore_out) *gscore_out = g_best;
+    if (max_off_out) *max_off_out = off_max;
+    if (cells_out) *cells_out = cells;
+    if (rows_out) *rows_out = rows;
+    if (stale_reads) *stale_reads = stale;
+    return best;
+}
+
+int g3o_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                    int m, const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins,
+                    int w, int end_bonus, int zdrop, int h0,
+                    int *qle_out, int *tle_out, int *gtle_out, int *gscore_out,
+                    int *max_off_out, int64_t *cells_out, int32_t *rows_out)
+{
+    return g3o_extend_impl(qlen, query, tlen, target, m, mat, o_del, e_del, o_ins, e_ins, w,
+                           end_bonus, zdrop, h0, qle_out, tle_out, gtle_out, gscore_out,
+                           max_off_out, cells_out, rows_out, 0, NULL);
+}
+
+/* Test-only probe: the same extension with stale buffer entries read as zero when
+   clean_stale != 0, and the count of non-zero stale reads.  Used to find jobs whose
+   result depends on the reference's stale-entry reads (they become known-answer tests). */
+int g3o_ksw_extend2_probe(int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                          const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins, int w,
+                          int end_bonus, int zdrop, int h0, int clean_stale, int32_t *out6,
+                          int32_t *stale_reads)
+{
+    out6[0] = g3o_extend_impl(qlen, query, tlen, target, 5, mat, o_del, e_del, o_ins, e_ins, w,
+                              end_bonus, zdrop, h0, &out6[1], &out6[2], &out6[3], &out6[4],
+                              &out6[5], NULL, NULL, clean_stale, stale_reads);
+    return out6[0];
+}
+
+/* ---------------------------------------------------------------------------------- */
+/* Batched form: jobs index into one u8 code buffer.                                    */
+/* ---------------------------------------------------------------------------------- */
+
+#define G3O_QREV 1           /* query read backwards from q_off + qlen - 1 */
+#define G3O_TREV 2           /* target read backwards */
+typedef struct {
+    int64_t q_off, t_off;        /* byte offsets into codes[] */
+    int32_t qlen, tlen, h0, w;
+    int32_t flags, pad_;         /* G3O_QREV / G3O_TREV: the reversed copies mem_chain2aln
+                                    makes for the left extension (aux.cu:261-265) */
+} g3o_job;
+
+typedef struct {
+    int8_t mat[25];
+    int32_t o_del, e_del, o_ins, e_ins, zdrop, end_bonus;
+} g3o_score;
+
+typedef struct {
+    const g3o_job *jobs;
+    const uint8_t *codes;
+    const g3o_score *sc;
+    g3o_ext *out;
+    int64_t *cells;
+    int32_t *rows;
+    int64_t n;
+    int64_t next;                /* shared work counter */
+    pthread_mutex_t lock;
+} g3o_batch_ctx;
+
+static const uint8_t *g3o_view(const uint8_t *src, int32_t len, int rev, uint8_t **buf)
+{
+    if (!rev) return src;
+    *buf = (uint8_t *)malloc((size_t)len + 1);
+    for (int32_t k = 0; k < len; ++k) (*buf)[k] = src[len - 1 - k];
+    return *buf;
+}
+
+static void g3o_run_one(const g3o_batch_ctx *c, int64_t k)
+{
+    const g3o_job *jb = &c->jobs[k];
+    g3o_ext *o = &c->out[k];
+    uint8_t *qb = NULL, *tb = NULL;
+    const uint8_t *q = g3o_view(c->codes + jb->q_off, jb->qlen, jb->flags & G3O_QREV, &qb);
+    const uint8_t *t = g3o_view(c->codes + jb->t_off, jb->tlen, jb->flags & G3O_TREV, &tb);
+    o->score = g3o_ksw_extend2(jb->qlen, q, jb->tlen, t,
+                               5, c->sc->mat, c->sc->o_del, c->sc->e_del, c->sc->o_ins,
+                               c->sc->e_ins, jb->w, c->sc->end_bonus, c->sc->zdrop, jb->h0,
+                               &o->qle, &o->tle, &o->gtle, &o->gscore, &o->max_off,
+                               c->cells ? &c->cells[k] : NULL, c->rows ? &c->rows[k] : NULL);
+    free(qb);
+    free(tb);
+}
+
+static void *g3o_worker(void *arg)
+{
+    g3o_batch_ctx *c = (g3o_batch_ctx *)arg;
+    for (;;) {
+        int64_t b, e;
+        pthread_mutex_lock(&c->lock);
+        b = c->next;
+        c->next += 256;
+        pthread_mutex_unlock(&c->lock);
+        if (b >= c->n) break;
+        e = b + 256 < c->n ? b + 256 : c->n;
+        for (int64_t k = b; k < e; ++k) g3o_run_one(c, k);
+    }
+    return NULL;
+}
+
+/* Runs n jobs on `threads` host threads (1 = the calling thread only). */
+int g3o_extend_batch(const g3o_job *jobs, int64_t n, const uint8_t *codes, const g3o_score *sc,
+                     g3o_ext *out, int64_t *cells, int32_t *rows, int threads)
+{
+    g3o_batch_ctx c;
+    c.jobs = jobs; c.codes = codes; c.sc = sc; c.out = out; c.cells = cells; c.rows = rows;
+    c.n = n; c.next = 0;
+    pthread_mutex_init(&c.lock, NULL);
+    if (threads <= 1) {
+        g3o_worker(&c);
+    } else {
+        pthread_t *tid = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)threads);
+        for (int t = 0; t < threads; ++t) pthread_create(&tid[t], NULL, g3o_worker, &c);
+        for (int t = 0; t < threads; ++t) pthread_join(tid[t], NULL);
+        free(tid);
+    }
+    pthread_mutex_destroy(&c.lock);
+    return 0;
+}
+
+/* ---------------------------------------------------------------------------------- */
+/* Seed-level driver: left + right extension with band retry, aux.cu:250-301.           */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct {
+    int32_t a, o_del, e_del, o_ins, e_ins, w, zdrop, pen_clip5, pen_clip3;
+    int8_t mat[25];
+} g3o_opt;
+
+typedef struct {
+    int64_t read_off;            /* byte offset of the read in codes[] */
+    int64_t win_off;             /* byte offset of the reference window rseq[] in codes[] */
+    int64_t rmax0, rmax1;        /* window [rmax0, rmax1) in reference coordinates */
+    int64_t rbeg;                /* seed start on the reference */
+    int32_t l_query, qbeg, len;  /* read length, seed start on the read, seed length */
+} g3o_seed;
+
+typedef struct {
+    int64_t rb, re;
+    int32_t qb, qe, score, truesc, w;
+    int32_t tries_left, tries_right;    /* ksw_extend2 calls made on each side */
+    int64_t cells;                       /* DP cells over all calls of this seed */
+} g3o_reg;
+
+/* aux.cu:168-175 */
+int g3o_cal_max_gap(const g3o_opt *opt, int qlen)
+{
+    int l_del = (int)((double)(qlen * opt->a - opt->o_del) / opt->e_del + 1.);
+    int l_ins = (int)((double)(qlen * opt->a - opt->o_ins) / opt->e_ins + 1.);
+    int l = l_del > l_ins ? l_del : l_ins;
+    l = l > 1 ? l : 1;
+    return l < opt->w << 1 ? l : opt->w << 1;
+}
+
+void g3o_extend_seed(const g3o_opt *opt, const uint8_t *codes, const g3o_seed *s, g3o_reg *a)
+{
+    const uint8_t *query = codes + s->read_off;
+    const uint8_t *rseq = codes + s->win_off;
+    int aw0 = opt->w, aw1 = opt->w;
+    int64_t cells = 0, c1;
+    memset(a, 0, sizeof(*a));
+    a->score = a->truesc = -1;
+    if (s->qbeg) {                                          /* aux.cu:258-281 */
+        int qle, tle, gtle, gscore, max_off;
+        int ql = s->qbeg;
+        int64_t tl = s->rbeg - s->rmax0;
+        uint8_t *qs = (uint8_t *)malloc((size_t)ql + 1), *rs = (uint8_t *)malloc((size_t)tl + 1);
+        for (int i = 0; i < ql; ++i) qs[i] = query[ql - 1 - i];
+        for (int64_t i = 0; i < tl; ++i) rs[i] = rseq[tl - 1 - i];
+        for (int i = 0; i < 2; ++i) {                       /* MAX_BAND_TRY = 2 */
+            int prev = a->score;
+            aw0 = opt->w << i;
+            a->score = g3o_ksw_extend2(ql, qs, (int)tl, rs, 5, opt->mat, opt->o_del, opt->e_del,
+                                       opt->o_ins, opt->e_ins, aw0, opt->pen_clip5, opt->zdrop,
+                                       s->len * opt->a, &qle, &tle, &gtle, &gscore, &max_off,
+                                       &c1, NULL);
+            cells += c1;
+            a->tries_left = i + 1;
+            if (a->score == prev || max_off < (aw0 >> 1) + (aw0 >> 2)) break;
+        }
+        if (gscore <= 0 || gscore <= a->score - opt->pen_clip5) {
+            a->qb = s->qbeg - qle; a->rb = s->rbeg - tle; a->truesc = a->score;
+        } else {
+            a->qb = 0; a->rb = s->rbeg - gtle; a->truesc = gscore;
+        }
+        free(qs); free(rs);
+    } else {
+        a->score = a->truesc = s->len * opt->a; a->qb = 0; a->rb = s->rbeg;
+    }
+    if (s->qbeg + s->len != s->l_query) {                   /* aux.cu:283-301 */
+        int qle, tle, gtle, gscore, max_off, sc0 = a->score;
+        int qe = s->qbeg + s->len;
+        int64_t re = s->rbeg + s->len - s->rmax0;
+        for (int i = 0; i < 2; ++i) {
+            int prev = a->score;
+            aw1 = opt->w << i;
+            a->score = g3o_ksw_extend2(s->l_query - qe, query + qe,
+                                       (int)(s->rmax1 - s->rmax0 - re), rseq + re, 5, opt->mat,
+                                       opt->o_del, opt->e_del, opt->o_ins, opt->e_ins, aw1,
+                                       opt->pen_clip3, opt->zdrop, sc0, &qle, &tle, &gtle,
+                                       &gscore, &max_off, &c1, NULL);
+            cells += c1;
+            a->tries_right = i + 1;
+            if (a->score == prev || max_off < (aw1 >> 1) + (aw1 >> 2)) break;
+        }
+        if (gscore <= 0 || gscore <= a->score - opt->pen_clip3) {
+            a->qe = qe + qle; a->re = s->rmax0 + re + tle; a->truesc += a->score - sc0;
+        } else {
+            a->qe = s->l_query; a->re = s->rmax0 + re + gtle; a->truesc += gscore - sc0;
+        }
+    } else {
+        a->qe = s->l_query; a->re = s->rbeg + s->len;
+    }
+    a->w = aw0 > aw1 ? aw0 : aw1;
+    a->cells = cells;
+}
+
+void g3o_extend_seeds(const g3o_opt *opt, const uint8_t *codes, const g3o_seed *seeds,
+                      int64_t n, g3o_reg *out)
+{
+    for (int64_t k = 0; k < n; ++k) g3o_extend_seed(opt, codes, &seeds[k], &out[k]);
+}
+
+/* Test-only: flags[k] = 1 when job k's outputs change if stale buffer entries are read as
+   zero, 0 otherwise (stale[k] = number of non-zero stale reads). */
+void g3o_stale_scan(const g3o_job *jobs, int64_t n, const uint8_t *codes, const g3o_score *sc,
+                    int32_t *flags, int32_t *stale)
+{
+    for (int64_t k = 0; k < n; ++k) {
+        const g3o_job *jb = &jobs[k];
+        uint8_t *qb = NULL, *tb = NULL;
+        const uint8_t *q = g3o_view(codes + jb->q_off, jb->qlen, jb->flags & G3O_QREV, &qb);
+        const uint8_t *t = g3o_view(codes + jb->t_off, jb->tlen, jb->flags & G3O_TREV, &tb);
+        int32_t a[6], b[6], st = 0, st2 = 0;
+        g3o_ksw_extend2_probe(jb->qlen, q, jb->tlen, t, sc->mat, sc->o_del, sc->e_del, sc->o_ins,
+                              sc->e_ins, jb->w, sc->end_bonus, sc->zdrop, jb->h0, 0, a, &st);
+        flags[k] = 0;
+        stale[k] = st;
+        if (st) {
+            g3o_ksw_extend2_probe(jb->qlen, q, jb->tlen, t, sc->mat, sc->o_del, sc->e_del, sc->o_ins,
+                                  sc->e_ins, jb->w, sc->end_bonus, sc->zdrop, jb->h0, 1, b, &st2);
+            flags[k] = memcmp(a, b, sizeof(a)) != 0;
+        }
+        free(qb);
+        free(tb);
+    }
+}

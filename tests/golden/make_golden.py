@@ -1,0 +1,170 @@
+"""Generates the golden vectors in tests/golden/ from the reference's own code.
+
+Run in a checkout where the reference tree exists (oracle/build_ref.sh has built
+oracle/_ref/libksw_ref.so from bwa/src/ksw.cu and bwa/src/aux.cu):
+
+    python tests/golden/make_golden.py
+
+Every expected output is computed by the reference's compiled ksw_extend2 (job sets) or by
+its compiled mem_chain2aln band-retry lines (seed sets); the oracle restatement is checked
+against these files by tests/test_oracle.py and the GPU kernels by tests/test_gpu_parity.py.
+Inputs are seeded synthetic jobs (g3sa_b200.synth) plus hand-built edge cases.
+
+Files:
+    jobs_<name>.npz   u8 (one byte per base), jobs (JOB_DT), score (SCORE_DT), ext (n x 6)
+    seeds_<name>.npz  u8, seeds (SEED_DT), opt (CPU_OPT_DT), reg (CPU_REG_DT)
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import g3sa_b200 as g  # noqa: E402
+from tests import native as nat  # noqa: E402
+
+
+class JobBuilder:
+    """Collects explicit (query, target, h0, w, flags) jobs into one u8 buffer."""
+
+    def __init__(self):
+        self.parts, self.jobs, self.off = [], [], 0
+
+    def add(self, q, t, h0, w, flags=0):
+        q = np.asarray(q, np.uint8)
+        t = np.asarray(t, np.uint8)
+        qo = self.off
+        self.parts.append(q)
+        self.off += len(q)
+        to = self.off
+        self.parts.append(t)
+        self.off += len(t)
+        self.jobs.append((qo, to, len(q), len(t), h0, w, flags))
+
+    def build(self):
+        jobs = np.array(self.jobs, dtype=g.JOB_DT)
+        u8 = np.concatenate(self.parts) if self.parts else np.zeros(0, np.uint8)
+        return u8, jobs
+
+
+def edge_jobs(rng):
+    b = JobBuilder()
+    rnd = lambda n: rng.integers(0, 4, n).astype(np.uint8)  # noqa: E731
+    # qlen = 1, several h0 and targets
+    for h0 in (1, 5, 7, 8, 19, 60):
+        for t in ([0], [1], [4], [0, 0, 0], list(rnd(30))):
+            b.add([0], t, h0, 100)
+    # tlen < qlen, tlen = 0, qlen = 0
+    for ql, tl in ((50, 10), (30, 1), (20, 0), (0, 20), (0, 0), (1, 0)):
+        q = rnd(ql)
+        t = q[:tl].copy() if tl <= ql else np.concatenate([q, rnd(tl - ql)])
+        b.add(q, t, 30, 100)
+    # h0 <= oe_ins and h0 = 0
+    for h0 in (0, 1, 6, 7):
+        q = rnd(40)
+        b.add(q, np.concatenate([q, rnd(20)]), h0, 100)
+    # all-N query, N-rich target
+    b.add(np.full(40, 4, np.uint8), rnd(60), 50, 100)
+    q = rnd(40)
+    t = q.copy()
+    t[::3] = 4
+    b.add(q, t, 50, 100)
+    # unrelated target: immediate z-drop / m == 0
+    for h0 in (19, 100, 150):
+        b.add(rnd(120), rnd(220), h0, 100)
+    # band widths: w > qlen, w = 0, 1, 2, negative
+    for w in (1000, 0, 1, 2, -1, -5):
+        q = rnd(60)
+        b.add(q, np.concatenate([q, rnd(30)]), 40, w)
+    # ties: two-letter alphabet, short
+    for _ in range(60):
+        ql, tl = rng.integers(1, 9), rng.integers(1, 9)
+        b.add(rng.integers(0, 2, ql), rng.integers(0, 2, tl), int(rng.integers(1, 20)), int(rng.integers(1, 6)))
+    # large h0, long query
+    q = rnd(600)
+    b.add(q, np.concatenate([q, rnd(200)]), 1000, 100)
+    # maximum query length of the long-segment configuration
+    q = rnd(5000)
+    t = q.copy()
+    t[rng.random(5000) < 0.005] = rnd(1)[0]
+    b.add(q, np.concatenate([t, rnd(200)]), 150, 500)
+    # reversed reads through the flags
+    q = rnd(80)
+    t = np.concatenate([rnd(20), q[::-1]])
+    b.add(q, t, 40, 100, g.JOB_QREV | g.JOB_TREV)
+    b.add(q, t[::-1].copy(), 40, 100, g.JOB_QREV)
+    return b
+
+
+def find_stale_sensitive(score, want=16, seed0=4242):
+    """Jobs whose outputs change when the stale row-buffer entries (left over from older rows
+    when the band grows by two columns, bwa/src/ksw.cu:388-391) are read as zero instead."""
+    orc = nat.oracle()
+    orc.g3o_stale_scan.argtypes = [ctypes.c_void_p, ctypes.c_int64] + [ctypes.c_void_p] * 4
+    found = JobBuilder()
+    k = 0
+    for it in range(20):
+        wl = g.synth(1, 200000, seed=seed0 + it, w=100, unrelated=0.2)
+        cj, cs = nat.cpu_jobs(wl.jobs), nat.cpu_score(score)
+        flags = np.zeros(wl.n, np.int32)
+        stale = np.zeros(wl.n, np.int32)
+        orc.g3o_stale_scan(cj.ctypes.data, wl.n, wl.u8.ctypes.data, cs.ctypes.data,
+                           flags.ctypes.data, stale.ctypes.data)
+        for idx in np.nonzero(flags)[0]:
+            jb = wl.jobs[idx]
+            q = wl.u8[jb["q_off"]:jb["q_off"] + jb["qlen"]]
+            t = wl.u8[jb["t_off"]:jb["t_off"] + jb["tlen"]]
+            found.add(q, t, int(jb["h0"]), int(jb["w"]))
+            k += 1
+        print(f"stale search: batch {it}, found {k}", flush=True)
+        if k >= want:
+            break
+    return found
+
+
+def save_jobs(name, u8, jobs, score):
+    ext = nat.ref_extend(jobs, u8, score)
+    np.savez_compressed(os.path.join(HERE, f"jobs_{name}.npz"), u8=u8, jobs=jobs, score=score, ext=ext)
+    print(f"jobs_{name}: {len(jobs)} jobs, {len(u8)} bases")
+
+
+def save_seeds(name, wl, opt):
+    reg = nat.ref_seeds(wl.seeds, wl.u8, opt)
+    np.savez_compressed(os.path.join(HERE, f"seeds_{name}.npz"), u8=wl.u8, seeds=wl.seeds, opt=opt, reg=reg)
+    print(f"seeds_{name}: {len(wl.seeds)} seeds")
+
+
+def main():
+    if not nat.have_ref():
+        sys.exit("oracle/_ref/libksw_ref.so missing: run sh oracle/build_ref.sh first")
+    rng = np.random.default_rng(2025)
+    sc = g.default_score()
+    wl = g.synth(1, 1500, seed=0x6A5 + 1, w=100)
+    save_jobs("cfg1", wl.u8, wl.jobs, sc)
+    wl = g.synth(2, 800, seed=0x6A5 + 2, w=100, unrelated=0.2)
+    save_jobs("cfg2", wl.u8, wl.jobs, sc)
+    for w in (100, 500):
+        wl = g.synth(4, 12, seed=0x6A5 + 4 + w, w=w)
+        save_jobs(f"cfg4_w{w}", wl.u8, wl.jobs, sc)
+    u8, jobs = edge_jobs(rng).build()
+    save_jobs("edge", u8, jobs, sc)
+    # a different scoring: a=2 b=3, gaps 5/2 (del) and 4/3 (ins), zdrop 40, end bonus 12
+    sc2 = g.default_score(a=2, b=3, o_del=5, e_del=2, o_ins=4, e_ins=3, zdrop=40, end_bonus=12)
+    wl = g.synth(1, 600, seed=0x6A5 + 7, w=50, a=2, o_del=5, e_del=2, o_ins=4, e_ins=3)
+    save_jobs("score2", wl.u8, wl.jobs, sc2)
+    sc3 = g.default_score(zdrop=0)  # z-drop disabled
+    wl = g.synth(2, 300, seed=0x6A5 + 8, w=100)
+    save_jobs("nozdrop", wl.u8, wl.jobs, sc3)
+    u8, jobs = find_stale_sensitive(sc).build()
+    save_jobs("stale", u8, jobs, sc)
+    for w in (100, 5):
+        wl = g.synth(2, 1500, seed=0x6A5 + 5 + w, w=w, unrelated=0.2)
+        save_seeds(f"cfg5_w{w}", wl, nat.opt_from_score(sc, w=w))
+
+
+if __name__ == "__main__":
+    main()

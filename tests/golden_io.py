@@ -1,0 +1,25 @@
+"""Loads the committed golden vectors (tests/golden/*.npz)."""
+import glob
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def job_sets():
+    return sorted(os.path.basename(p)[5:-4] for p in glob.glob(os.path.join(GOLDEN, "jobs_*.npz")))
+
+
+def seed_sets():
+    return sorted(os.path.basename(p)[6:-4] for p in glob.glob(os.path.join(GOLDEN, "seeds_*.npz")))
+
+
+def load_jobs(name):
+    z = np.load(os.path.join(GOLDEN, f"jobs_{name}.npz"))
+    return z["u8"], z["jobs"], z["score"], z["ext"]
+
+
+def load_seeds(name):
+    z = np.load(os.path.join(GOLDEN, f"seeds_{name}.npz"))
+    return z["u8"], z["seeds"], z["opt"], z["reg"]

@@ -1,0 +1,36 @@
+"""Helpers for the GPU tests: run batches through the C ABI with torch-owned device buffers."""
+import numpy as np
+
+import g3sa_b200 as g
+
+_ctx = None
+
+
+def ctx():
+    global _ctx
+    if _ctx is None:
+        _ctx = g.Context(0)
+    return _ctx
+
+
+def to_dev(a):
+    import torch
+    a = np.ascontiguousarray(a)
+    return torch.from_numpy(a.view(np.uint8).copy()).cuda()
+
+
+def run_batch(u8, jobs, score, schedule=g.SCHED_PLAIN, lanes=0, max_qlen=None, max_tlen=None):
+    """Returns (ext[n,6], status[n], cells[n]) from the GPU."""
+    import torch
+    n = len(jobs)
+    codes, nmask = g.pack_planes(u8)
+    d_jobs, d_codes, d_nmask = to_dev(jobs), to_dev(codes), to_dev(nmask)
+    out = torch.full((n, 6), -777, dtype=torch.int32, device="cuda")
+    status = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+    cells = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    mq = int(jobs["qlen"].max()) if max_qlen is None else max_qlen
+    mt = int(jobs["tlen"].max()) if max_tlen is None else max_tlen
+    ctx().extend_batch(score, d_jobs, n, d_codes, d_nmask, out, status, mq, mt,
+                       schedule=schedule, lanes=lanes, d_cells=cells)
+    torch.cuda.synchronize()
+    return out.cpu().numpy(), status.cpu().numpy(), cells.cpu().numpy()

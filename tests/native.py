@@ -1,0 +1,151 @@
+"""Test-only bindings: the CPU oracle (oracle/), the reference's own ksw_extend2 compiled
+from its source (oracle/_ref/), and the CPU model of the kernels' warp protocol
+(libg3x_emu.so).  Only tests, __graft_entry__.smoke() and bench.py's CPU arm import this."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "libg3x_oracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libksw_ref.so")
+EMU_SO = os.path.join(ROOT, "g3sa_b200", "libg3x_emu.so")
+
+# g3o_job / RefJob (oracle/ksw_oracle.c, oracle/ref_wrap.cpp)
+CPU_JOB_DT = np.dtype([("q_off", "<i8"), ("t_off", "<i8"), ("qlen", "<i4"), ("tlen", "<i4"),
+                       ("h0", "<i4"), ("w", "<i4"), ("flags", "<i4"), ("pad_", "<i4")])
+# g3o_score / RefScore
+CPU_SCORE_DT = np.dtype([("mat", "i1", 25), ("pad_", "i1", 3), ("o_del", "<i4"), ("e_del", "<i4"),
+                         ("o_ins", "<i4"), ("e_ins", "<i4"), ("zdrop", "<i4"), ("end_bonus", "<i4")])
+CPU_OPT_DT = np.dtype([("a", "<i4"), ("o_del", "<i4"), ("e_del", "<i4"), ("o_ins", "<i4"),
+                       ("e_ins", "<i4"), ("w", "<i4"), ("zdrop", "<i4"), ("pen_clip5", "<i4"),
+                       ("pen_clip3", "<i4"), ("mat", "i1", 25), ("pad_", "i1", 3)])
+CPU_REG_DT = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), ("score", "<i4"),
+                       ("truesc", "<i4"), ("w", "<i4"), ("tries_left", "<i4"),
+                       ("tries_right", "<i4"), ("pad_", "<i4"), ("cells", "<i8")])
+
+_oracle = _ref = _emu = None
+
+
+def build_oracle():
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build_oracle()
+        _oracle = ctypes.CDLL(ORACLE_SO)
+        _oracle.g3o_extend_batch.argtypes = [ctypes.c_void_p, ctypes.c_int64] + [ctypes.c_void_p] * 5 + [ctypes.c_int]
+        _oracle.g3o_extend_seeds.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_void_p]
+        _oracle.g3o_ksw_extend2.restype = ctypes.c_int
+    return _oracle
+
+
+def have_ref():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(REF_SO)
+        _ref.g3r_ksw_extend2_batch.argtypes = [ctypes.c_void_p, ctypes.c_int64] + [ctypes.c_void_p] * 3 + [ctypes.c_int]
+        _ref.g3r_extend_seeds.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_void_p]
+    return _ref
+
+
+def emu():
+    global _emu
+    if _emu is None:
+        _emu = ctypes.CDLL(EMU_SO)
+        _emu.g3x_emu_extend_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 4
+    return _emu
+
+
+def cpu_jobs(jobs):
+    j = np.zeros(len(jobs), CPU_JOB_DT)
+    for f in ("q_off", "t_off", "qlen", "tlen", "h0", "w", "flags"):
+        j[f] = jobs[f]
+    return j
+
+
+def cpu_score(score):
+    s = np.zeros(1, CPU_SCORE_DT)
+    for f in ("mat", "o_del", "e_del", "o_ins", "e_ins", "zdrop", "end_bonus"):
+        s[f] = score[f]
+    return s
+
+
+def oracle_extend(jobs, u8, score, threads=8):
+    """(ext[n,6] int32, cells[n] int64, rows[n] int32) from the C restatement."""
+    n = len(jobs)
+    cj = cpu_jobs(jobs)
+    cs = cpu_score(score)
+    out = np.zeros((n, 6), np.int32)
+    cells = np.zeros(n, np.int64)
+    rows = np.zeros(n, np.int32)
+    u8 = np.ascontiguousarray(u8)
+    oracle().g3o_extend_batch(cj.ctypes.data, n, u8.ctypes.data, cs.ctypes.data, out.ctypes.data,
+                              cells.ctypes.data, rows.ctypes.data, threads)
+    return out, cells, rows
+
+
+def ref_extend(jobs, u8, score, threads=8):
+    """ext[n,6] from the reference's own ksw_extend2 (oracle/_ref)."""
+    n = len(jobs)
+    cj = cpu_jobs(jobs)
+    cs = cpu_score(score)
+    out = np.zeros((n, 6), np.int32)
+    u8 = np.ascontiguousarray(u8)
+    ref().g3r_ksw_extend2_batch(cj.ctypes.data, n, u8.ctypes.data, cs.ctypes.data, out.ctypes.data, threads)
+    return out
+
+
+def emu_extend(jobs, codes, nmask, score, G):
+    n = len(jobs)
+    out = np.zeros((n, 6), np.int32)
+    status = np.zeros(n, np.int32)
+    cells = np.zeros(n, np.int32)
+    stats = np.zeros((n, 4), np.int64)
+    jobs = np.ascontiguousarray(jobs)
+    emu().g3x_emu_extend_batch(score.ctypes.data, jobs.ctypes.data, n, codes.ctypes.data,
+                               nmask.ctypes.data, G, out.ctypes.data, status.ctypes.data,
+                               cells.ctypes.data, stats.ctypes.data)
+    return out, status, cells, stats
+
+
+def opt_from_score(score, a=1, w=100, pen_clip5=5, pen_clip3=5):
+    o = np.zeros(1, CPU_OPT_DT)
+    o["a"], o["w"], o["pen_clip5"], o["pen_clip3"] = a, w, pen_clip5, pen_clip3
+    for f in ("o_del", "e_del", "o_ins", "e_ins", "zdrop", "mat"):
+        o[f] = score[f]
+    return o
+
+
+def oracle_seeds(seeds, u8, opt):
+    out = np.zeros(len(seeds), CPU_REG_DT)
+    oracle().g3o_extend_seeds(opt.ctypes.data, np.ascontiguousarray(u8).ctypes.data,
+                              np.ascontiguousarray(seeds).ctypes.data, len(seeds), out.ctypes.data)
+    return out
+
+
+# RefOpt layout (oracle/ref_seed_head.inc mem_opt_t)
+REF_OPT_DT = np.dtype([("a", "<i4"), ("b", "<i4"), ("o_del", "<i4"), ("e_del", "<i4"), ("o_ins", "<i4"),
+                       ("e_ins", "<i4"), ("pen_clip5", "<i4"), ("pen_clip3", "<i4"), ("w", "<i4"),
+                       ("zdrop", "<i4"), ("mat", "i1", 25), ("pad_", "i1", 3)])
+
+
+def ref_seeds(seeds, u8, opt):
+    """Seed-level outputs (CPU_REG_DT, first 7 fields) from the reference's own mem_chain2aln
+    band-retry lines."""
+    ro = np.zeros(1, REF_OPT_DT)
+    for f in ("a", "o_del", "e_del", "o_ins", "e_ins", "pen_clip5", "pen_clip3", "w", "zdrop", "mat"):
+        ro[f] = opt[f]
+    out = np.zeros(len(seeds), CPU_REG_DT)
+    ref().g3r_extend_seeds(ro.ctypes.data, np.ascontiguousarray(u8).ctypes.data,
+                           np.ascontiguousarray(seeds).ctypes.data, len(seeds), out.ctypes.data)
+    return out
