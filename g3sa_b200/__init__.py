@@ -91,6 +91,8 @@ def lib():
         L.g3x_strerror.restype = ctypes.c_char_p
         L.g3x_ksw_extend2_batch.argtypes = [P, P, P, I32, P, P, P, P, P, P]
         L.g3x_ksw_extend2_batch.restype = ctypes.c_int
+        L.g3x_int_peak.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+        L.g3x_int_peak.restype = ctypes.c_int
         L.g3x_pack_codes.argtypes = [P, ctypes.c_int64, P, P, ctypes.c_int64]
         L.g3x_pack_codes.restype = ctypes.c_int
         _lib = L
@@ -204,6 +206,12 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def int_peak(self):
+        """Measured 32-bit integer ALU ops/s of this GPU (g3x_int_peak)."""
+        v = ctypes.c_double()
+        _check(lib().g3x_int_peak(self._h, ctypes.byref(v)), "g3x_int_peak")
+        return v.value
 
     def extend_batch(self, score, d_jobs, n, d_codes, d_nmask, d_out, d_status, max_qlen,
                      max_tlen, schedule=SCHED_PLAIN, lanes=0, d_cells=None, stream=None):

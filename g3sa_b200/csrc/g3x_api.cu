@@ -98,10 +98,10 @@ int g3x_ksw_extend2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_
         case G3X_SCHED_LEARNED: {
             int lanes = opts->lanes ? opts->lanes : 16;
             if (lanes != 8 && lanes != 16 && lanes != 32) return G3X_ERR_INVALID;
-            // Shared memory per job grows with the query; a warp of narrow groups must fit.
-            if (!opts->lanes)
-                while (lanes < 32 && (32 / lanes) * g3x::group_smem_bytes(d.qmax, d.tmax) > 227 * 1024)
-                    lanes *= 2;
+            // Shared memory per job grows with the query; a warp of narrow groups must fit,
+            // so the lane count is raised until it does.
+            while (lanes < 32 && (32 / lanes) * g3x::group_smem_bytes(d.qmax, d.tmax) > 227 * 1024)
+                lanes *= 2;
             d.lanes = lanes; d.persistent = 1; d.warps_per_block = 4;
             d.queue = ctx->d_queue;
             if (cudaMemsetAsync(ctx->d_queue, 0, sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
@@ -111,6 +111,12 @@ int g3x_ksw_extend2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_
             return G3X_ERR_INVALID;
     }
     return g3x::launch_extend(d, sp, st);
+}
+
+int g3x_int_peak(g3x_ctx* ctx, double* ops_per_s) {
+    if (!ctx || !ops_per_s) return G3X_ERR_INVALID;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    return g3x::measure_int_peak(ctx->device, ops_per_s);
 }
 
 int g3x_pack_codes(const uint8_t* h_seq, int64_t len, uint32_t* h_codes, uint32_t* h_nmask,

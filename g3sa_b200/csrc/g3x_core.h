@@ -2,12 +2,12 @@
 //
 // One job (one ksw_extend2 call, bwa/src/ksw.cu:303-401) is processed by a group of G
 // lanes.  Lane r of the group owns target rows r, r+G, r+2G, ... ("rolling rows"); a lane
-// walks its row left to right one cell per step and trails the lane that owns the
-// previous row, so the group sweeps anti-diagonals.  The reference's single row buffer
-// eh[] (ksw.cu:310) is kept verbatim in shared memory: every row reads and overwrites it
-// at the same positions, in the same row order, as the scalar loop does, so the stale
-// entries the reference reads when its band grows by two columns (ksw.cu:388-391) hold
-// the same values here.
+// walks its row left to right, up to one aligned block of four cells per step, and trails
+// the lane that owns the previous row, so the group sweeps anti-diagonals.  The
+// reference's single row buffer eh[] (ksw.cu:310) is kept verbatim in shared memory: every
+// row reads and overwrites it at the same positions, in the same row order, as the scalar
+// loop does, so the stale entries the reference reads when its band grows by two columns
+// (ksw.cu:388-391) hold the same values here.
 //
 // The scalar loop decides the band of row i+1 only after row i has finished
 // (ksw.cu:388-391).  Here the lane that owns row i+1 instead watches, every step, how far
@@ -21,6 +21,9 @@
 // ksw.cu:371-386 (to-end score, max tracking, z-drop) is applied in row order by a
 // uniform "commit" over the group.  Rows started after the row that ends the extension
 // are speculative and are discarded.
+//
+// A finished row publishes its final words for exactly one step; its successor latches
+// them, so the lane can take its next row immediately.
 //
 // Everything in this header is plain C++ usable on the host as well, so a CPU model of
 // the warp protocol (g3x_emu.cpp, test-only) runs this same code.
@@ -36,6 +39,7 @@
 namespace g3x {
 
 constexpr uint32_t kNone = 0xFFFFu;   // "no column yet" / "row finished" marker
+constexpr int kBlock = 4;             // cells per lane-step (one aligned block)
 
 enum LaneState : int32_t { kIdle = 0, kWait = 1, kRun = 2, kDone = 3 };
 
@@ -45,7 +49,6 @@ struct JobConst {
     int32_t o_del, e_del, o_ins, e_ins, oe_del, oe_ins, zdrop;
 };
 
-// One H/E entry of the reference's row buffer (eh_t, ksw.cu:299-301).
 struct EhCell {
     int32_t h, e;
 };
@@ -59,10 +62,13 @@ struct Lane {
     int32_t cap;    // min(i + w + 1, qlen): fixed right limit of the band
     int32_t h1;     // H(i, j-1)
     int32_t f;      // F(i, j)
-    int32_t m, mj;  // row maximum and the last column reaching it
+    int32_t key;    // narrow rows: (row max << 16) | last column reaching it; -1 = none
+    int32_t m, mj;  // wide rows: row maximum and the last column reaching it
     int32_t fnz;    // first column whose new eh entry is non-zero (kNone: none yet)
     int32_t lnz1;   // 1 + last column whose new eh entry is non-zero (0: none)
     int32_t qrow;   // offset of this row's query-profile row
+    uint32_t lat_prog, lat_fnz;  // predecessor's final words, latched when it finished
+    int32_t lat;    // 1 when the latch holds the predecessor row of this lane's row
 };
 
 // What a lane hands to the group when its row ends.
@@ -107,6 +113,14 @@ G3X_HD int32_t init_h(int32_t j, const JobConst& c) {
     return v > 0 ? v : 0;
 }
 
+// A job is "narrow" when every H it can produce is below 2^15: then a row's maximum and
+// its column pack into one int32 key.  H <= h0 + max_sc * min(qlen, tlen).
+G3X_HD bool job_is_narrow(const JobConst& c, int32_t max_sc) {
+    int64_t mn = c.qlen < c.tlen ? c.qlen : c.tlen;
+    int64_t hmax = (int64_t)(c.h0 > 0 ? c.h0 : 0) + (int64_t)max_sc * mn;
+    return hmax < 32768 && c.qlen < 65535;
+}
+
 G3X_HD void commit_init(Commit& k, const JobConst& c) {
     k.next = 0;
     k.stop = c.tlen <= 0;
@@ -140,6 +154,15 @@ G3X_HD void commit_row(Commit& k, const JobConst& c, const RowDone& d) {
     if (k.next >= c.tlen) k.stop = 1;
 }
 
+G3X_HD void lane_init(Lane& L, int32_t r, int32_t tlen) {
+    L.st = r < tlen ? kWait : kIdle;
+    L.i = r;
+    L.j = L.beg = L.cap = L.h1 = L.f = L.m = L.qrow = 0;
+    L.mj = -1; L.key = -1;
+    L.fnz = (int32_t)kNone; L.lnz1 = 0;
+    L.lat_prog = 0; L.lat_fnz = kNone; L.lat = 0;
+}
+
 // The words a lane publishes to its successor each step.
 G3X_HD uint32_t lane_prog(const Lane& L) {
     uint32_t col = L.st == kDone ? kNone : (L.st == kRun ? (uint32_t)L.j : 0u);
@@ -163,18 +186,84 @@ G3X_HD void lane_begin_row(Lane& L, int32_t beg, const JobConst& c, int32_t tcod
     } else {
         L.h1 = 0;
     }
-    L.f = 0; L.m = 0; L.mj = -1;
+    L.f = 0; L.m = 0; L.mj = -1; L.key = -1;
     L.fnz = (int32_t)kNone; L.lnz1 = 0;
     L.qrow = tcode * qstride;
 }
 
+#if defined(__CUDACC__)
+G3X_HD int32_t max3_i32(int32_t a, int32_t b, int32_t c) {
+#if defined(__CUDA_ARCH__)
+    return __vimax3_s32(a, b, c);
+#else
+    int32_t m = a > b ? a : b; return m > c ? m : c;
+#endif
+}
+// max(a + b, c)
+G3X_HD int32_t addmax_i32(int32_t a, int32_t b, int32_t c) {
+#if defined(__CUDA_ARCH__)
+    return __viaddmax_s32(a, b, c);
+#else
+    int32_t s = a + b; return s > c ? s : c;
+#endif
+}
+// min(a + b, c)
+G3X_HD int32_t addmin_i32(int32_t a, int32_t b, int32_t c) {
+#if defined(__CUDA_ARCH__)
+    return __viaddmin_s32(a, b, c);
+#else
+    int32_t s = a + b; return s < c ? s : c;
+#endif
+}
+#else
+inline int32_t max3_i32(int32_t a, int32_t b, int32_t c) { int32_t m = a > b ? a : b; return m > c ? m : c; }
+inline int32_t addmax_i32(int32_t a, int32_t b, int32_t c) { int32_t s = a + b; return s > c ? s : c; }
+inline int32_t addmin_i32(int32_t a, int32_t b, int32_t c) { int32_t s = a + b; return s < c ? s : c; }
+#endif
+
+// Row end, ksw.cu:371-375.  For an empty row (j == beg) the reference's loop variable is
+// beg, its eh[end] write is never read again (the row breaks), and the to-end test uses
+// the row's initial h1.
+template <bool kNarrow, class Buf>
+G3X_HD void lane_end_row(Lane& L, const JobConst& c, Buf& buf, RowDone* done) {
+    const int32_t jn = L.j;
+    if (jn > L.beg) {
+        buf.store(jn, L.h1, 0);
+        if (L.h1 != 0) L.lnz1 = jn + 1;
+    }
+    if (L.fnz == (int32_t)kNone) L.fnz = jn;
+    if (kNarrow) {
+        done->m = L.key < 0 ? 0 : (L.key >> 16);
+        done->mj = L.key < 0 ? -1 : (L.key & 0xFFFF);
+    } else {
+        done->m = L.m;
+        done->mj = L.mj;
+    }
+    done->gval = jn == c.qlen ? L.h1 : -1;
+    done->ncells = jn - L.beg;
+    L.st = kDone;
+    L.lat = 0;
+}
+
 // One step of one lane.  `pprog`/`pfnz` are the predecessor's published words at the start
-// of the step; `committed` is the group's Commit::next.  Returns true when the lane's row
-// ended in this step (then *done is filled).  `eh`, `qp` and `tgt` are the job's buffers.
-template <class EhT>
-G3X_HD bool lane_step(Lane& L, const JobConst& c, uint32_t pprog, uint32_t pfnz,
-                      int32_t committed, int32_t G, EhT* eh, const int8_t* qp,
-                      const uint8_t* tgt, int32_t qstride, RowDone* done) {
+// of the step.  Returns true when the lane's row ended in this step (then *done is
+// filled).  `buf` gives the job's row buffer (load4 / store / note_read), `qp` the query
+// profile, `tgt` the target codes.
+//
+// Buf interface:  load4(jb, EhCell v[4])  -- the four slots of the aligned block at jb
+//                 store(c, h, e)          -- write slot c
+//                 note_read(c)            -- the lane consumed slot c (test hook)
+template <int G, bool kNarrow, class Buf>
+G3X_HD bool lane_step(Lane& L, const JobConst& c, uint32_t pprog, uint32_t pfnz, Buf& buf,
+                      const int8_t* qp, const uint8_t* tgt, int32_t qstride, RowDone* done) {
+    // Latch the predecessor's final words the step they appear (it moves on next step).
+    if ((pprog >> 16) == kNone) { L.lat_prog = pprog; L.lat_fnz = pfnz; L.lat = 1; }
+    if (L.lat) { pprog = L.lat_prog; pfnz = L.lat_fnz; }
+
+    if (L.st == kDone) {                                  // published once; take next row
+        L.i += G;
+        L.st = L.i < c.tlen ? kWait : kIdle;
+    }
     if (L.st == kWait) {
         if (L.i == 0) {
             int32_t b = -c.w;
@@ -183,55 +272,60 @@ G3X_HD bool lane_step(Lane& L, const JobConst& c, uint32_t pprog, uint32_t pfnz,
             int32_t b = L.i - c.w;
             lane_begin_row(L, (int32_t)pfnz > b ? (int32_t)pfnz : b, c, tgt[L.i], qstride);
         }
-        return false;
-    }
-    if (L.st == kDone) {
-        if (committed >= L.i + 2 || L.i + 1 >= c.tlen) {
-            L.i += G;
-            L.st = L.i < c.tlen ? kWait : kIdle;
-        }
-        return false;
     }
     if (L.st != kRun) return false;
+
     uint32_t colp = pprog >> 16, lnzp = pprog & 0xFFFFu;
     if (L.i == 0) { colp = kNone; lnzp = kNone; }        // row 0 reads the initial buffer
     const bool pdone = colp == kNone;
-    const int32_t j = L.j;
-    if (j < L.cap && (uint32_t)j < colp && (uint32_t)j <= lnzp) {
-        // One cell of ksw.cu:346-370.
-        EhCell v = eh[j].load();
-        int32_t s = qp[L.qrow + j];
-        int32_t M = v.h ? v.h + s : 0;
-        int32_t h = M > v.e ? M : v.e;
-        h = h > L.f ? h : L.f;
-        int32_t t = M - c.oe_del; t = t > 0 ? t : 0;
-        int32_t e = v.e - c.e_del; e = e > t ? e : t;
-        eh[j].store(L.h1, e);
-        if ((L.h1 | e) != 0) {
-            L.lnz1 = j + 1;
-            if (L.fnz == (int32_t)kNone) L.fnz = j;
+    int32_t lim = L.cap;                                  // cells j < lim may be computed
+    if ((int32_t)colp < lim) lim = (int32_t)colp;
+    if ((int32_t)lnzp + 1 < lim) lim = (int32_t)lnzp + 1;
+    const int32_t j0 = L.j;
+    if (j0 < lim) {
+        const int32_t jb = j0 & ~(kBlock - 1);
+        EhCell v[kBlock];
+        buf.load4(jb, v);
+        const uint32_t sc4 = *reinterpret_cast<const uint32_t*>(qp + L.qrow + jb);
+        int32_t h1 = L.h1, f = L.f, key = L.key, m = L.m, mj = L.mj, lnz1 = L.lnz1;
+        bool fnz_open = L.fnz == (int32_t)kNone;
+#pragma unroll
+        for (int t = 0; t < kBlock; ++t) {
+            const int32_t col = jb + t;
+            if (col >= j0 && col < lim) {
+                // One cell of ksw.cu:346-370.  M = H(i-1,j-1) ? H(i-1,j-1) + S : 0 is written
+                // as min(H + S, 256 H): equal when H > 0, and <= 0 when H == 0, which every
+                // use below clips to 0 exactly like the reference's 0.
+                buf.note_read(col);
+                const int32_t s = (int32_t)(int8_t)(sc4 >> (8 * t));
+                const int32_t hd = v[t].h, ed = v[t].e;
+                const int32_t M = addmin_i32(hd, s, hd << 8);
+                const int32_t h = max3_i32(M, ed, f);
+                const int32_t te = addmax_i32(M, -c.oe_del, 0);
+                const int32_t e2 = addmax_i32(ed, -c.e_del, te);
+                buf.store(col, h1, e2);
+                if ((h1 | e2) != 0) {
+                    lnz1 = col + 1;
+                    if (fnz_open) { L.fnz = col; fnz_open = false; }
+                }
+                if (kNarrow) {
+                    const int32_t k2 = (h << 16) | col;
+                    key = key > k2 ? key : k2;
+                } else {
+                    if (h >= m) { m = h; mj = col; }
+                }
+                const int32_t tf = addmax_i32(M, -c.oe_ins, 0);
+                f = addmax_i32(f, -c.e_ins, tf);
+                h1 = h;
+            }
         }
-        L.h1 = h;
-        if (h >= L.m) { L.m = h; L.mj = j; }
-        t = M - c.oe_ins; t = t > 0 ? t : 0;
-        int32_t f = L.f - c.e_ins; L.f = f > t ? f : t;
-        L.j = j + 1;
+        L.h1 = h1; L.f = f; L.key = key; L.m = m; L.mj = mj; L.lnz1 = lnz1;
+        const int32_t jend = jb + kBlock < lim ? jb + kBlock : lim;
+        L.j = jend;
     }
     const int32_t jn = L.j;
     if (jn >= L.cap || (pdone && (uint32_t)jn > lnzp)) {
-        // Row end, ksw.cu:371-375.  For an empty row (jn == beg) the reference's loop
-        // variable is beg, its eh[end] write is never read again (the row breaks), and the
-        // to-end test uses the row's initial h1.
-        if (jn > L.beg) {
-            eh[jn].store(L.h1, 0);
-            if (L.h1 != 0) L.lnz1 = jn + 1;
-        }
-        if (L.fnz == (int32_t)kNone) L.fnz = jn;
-        done->m = L.m;
-        done->mj = L.mj;
-        done->gval = jn == c.qlen ? L.h1 : -1;
-        done->ncells = jn - L.beg;
-        L.st = kDone;
+        lane_end_row<kNarrow>(L, c, buf, done);
         return true;
     }
     return false;

@@ -34,5 +34,6 @@ struct LaunchDesc {
 
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 size_t group_smem_bytes(int qmax, int tmax);
+int measure_int_peak(int device, double* ops_per_s);
 
 }  // namespace g3x

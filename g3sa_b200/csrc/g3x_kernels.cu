@@ -17,21 +17,33 @@ namespace g3x {
 // int32 H/E slot of the shared row buffer.
 struct EhSlot32 {
     int32_t h, e;
-    __device__ __forceinline__ EhCell load() const {
-        int2 v = *reinterpret_cast<const int2*>(this);
-        return EhCell{v.x, v.y};
+};
+
+// The row buffer as lane_step sees it: one aligned block of four slots is read with two
+// 16-byte shared loads; each computed cell is written back with one 8-byte store.
+struct SmemEh {
+    EhSlot32* p;
+    __device__ __forceinline__ void load4(int jb, EhCell v[4]) const {
+        const int4 a = *reinterpret_cast<const int4*>(p + jb);
+        const int4 b = *reinterpret_cast<const int4*>(p + jb + 2);
+        v[0] = EhCell{a.x, a.y}; v[1] = EhCell{a.z, a.w};
+        v[2] = EhCell{b.x, b.y}; v[3] = EhCell{b.z, b.w};
     }
-    __device__ __forceinline__ void store(int32_t hh, int32_t ee) {
-        *reinterpret_cast<int2*>(this) = make_int2(hh, ee);
+    __device__ __forceinline__ void store(int c, int32_t h, int32_t e) {
+        *reinterpret_cast<int2*>(p + c) = make_int2(h, e);
     }
+    __device__ __forceinline__ void note_read(int) const {}
 };
 
 __host__ __device__ constexpr int align16(int x) { return (x + 15) & ~15; }
 
+// Slots: every block read (jb <= qmax-1, 4 slots) and the end write at qlen stay inside.
+__host__ __device__ inline int eh_slots(int qmax) { return (qmax + 8) & ~3; }
+// Query-profile row stride: a 4-byte read at any block start jb <= qmax-1 stays in the row.
 __host__ __device__ inline int qstride_of(int qmax) { return (qmax + 4) & ~3; }
 
 __host__ __device__ inline size_t group_bytes(int qmax, int tmax) {
-    return (size_t)align16((qmax + 2) * (int)sizeof(EhSlot32)) +
+    return (size_t)align16(eh_slots(qmax) * (int)sizeof(EhSlot32)) +
            (size_t)align16(5 * qstride_of(qmax)) + (size_t)align16(tmax + 1);
 }
 
@@ -46,14 +58,54 @@ __device__ __forceinline__ int decode_base(const uint32_t* __restrict__ codes,
     return nb ? 4 : (int)c;
 }
 
+template <int G, bool kNarrow>
+__device__ void run_dp(int job, const JobConst& c, const LaunchDesc& d, SmemEh buf,
+                       const int8_t* qp, const uint8_t* tgt, int qs, int r, unsigned gmask) {
+    Lane L;
+    lane_init(L, r, c.tlen);
+    Commit K;
+    commit_init(K, c);
+    const int pred = (r + G - 1) & (G - 1);
+    // Every step either advances a row or moves a lane between states; the oldest
+    // unfinished row always advances, so this bound is never reached by a correct run.  It
+    // turns a logic error into a per-job status instead of a hang.
+    const long long limit = 8LL * ((long long)c.tlen + 2) * ((long long)c.qlen + 8) + 4096;
+    long long steps = 0;
+    int32_t err = G3X_OK;
+    while (!K.stop) {
+        const uint32_t pp = __shfl_sync(gmask, lane_prog(L), pred, G);
+        const uint32_t pf = __shfl_sync(gmask, lane_fnz(L), pred, G);
+        RowDone rd;
+        const bool fin = lane_step<G, kNarrow>(L, c, pp, pf, buf, qp, tgt, qs, &rd);
+        const unsigned b = __ballot_sync(gmask, fin);
+        if (b) {
+            if (__popc(b) != 1) { err = G3X_ERR_INTERNAL; break; }
+            const int src = (__ffs(b) - 1) & (G - 1);
+            RowDone cd;
+            cd.m = __shfl_sync(gmask, rd.m, src, G);
+            cd.mj = __shfl_sync(gmask, rd.mj, src, G);
+            cd.gval = __shfl_sync(gmask, rd.gval, src, G);
+            cd.ncells = __shfl_sync(gmask, rd.ncells, src, G);
+            commit_row(K, c, cd);
+        }
+        __syncwarp(gmask);
+        if (++steps > limit) { err = G3X_ERR_TIMEOUT; break; }
+    }
+    if (r == 0) {
+        d.out[job] = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};
+        d.status[job] = err;
+        if (d.cells) d.cells[job] = (int32_t)K.cells;
+    }
+}
+
 template <int G>
 __device__ void run_job(int job, const LaunchDesc& d, const ScoreParams& sp, char* gsm,
                         int r, unsigned gmask) {
     const int qmax = d.qmax, tmax = d.tmax;
     const int qs = qstride_of(qmax);
     EhSlot32* eh = reinterpret_cast<EhSlot32*>(gsm);
-    int8_t* qp = reinterpret_cast<int8_t*>(gsm + align16((qmax + 2) * (int)sizeof(EhSlot32)));
-    uint8_t* tgt = reinterpret_cast<uint8_t*>(gsm + align16((qmax + 2) * (int)sizeof(EhSlot32)) +
+    int8_t* qp = reinterpret_cast<int8_t*>(gsm + align16(eh_slots(qmax) * (int)sizeof(EhSlot32)));
+    uint8_t* tgt = reinterpret_cast<uint8_t*>(gsm + align16(eh_slots(qmax) * (int)sizeof(EhSlot32)) +
                                               align16(5 * qs));
 
     const g3x_job_t jb = d.jobs[job];
@@ -80,47 +132,19 @@ __device__ void run_job(int job, const LaunchDesc& d, const ScoreParams& sp, cha
         for (int a = 0; a < 5; ++a) qp[a * qs + k] = sp.mat[a * 5 + code];
     }
     for (int k = r; k < tlen; k += G) tgt[k] = (uint8_t)decode_base(d.codes, d.nmask, jb.t_off, k, tlen, trev);
-    for (int k = r; k <= qlen + 1; k += G) eh[k].store(init_h(k, c), 0);
+    const int nslots = eh_slots(qlen);
+    for (int k = r; k < nslots; k += G) {
+        EhSlot32 v;
+        v.h = k <= qlen + 1 ? init_h(k, c) : 0;
+        v.e = 0;
+        eh[k] = v;
+    }
     __syncwarp(gmask);
-
-    Lane L;
-    L.st = r < tlen ? kWait : kIdle;
-    L.i = r;
-    L.j = L.beg = L.cap = L.h1 = L.f = L.m = L.mj = L.qrow = 0;
-    L.fnz = (int32_t)kNone; L.lnz1 = 0;
-    Commit K;
-    commit_init(K, c);
-    const int pred = (r + G - 1) & (G - 1);
-    // Every step either advances a row by one cell or moves a lane between states; the
-    // oldest unfinished row always advances, so this bound is never reached by a correct
-    // run.  It turns a logic error into a per-job status instead of a hang.
-    const long long limit = 8LL * ((long long)tlen + 2) * ((long long)qlen + 8) + 4096;
-    long long steps = 0;
-    int32_t err = G3X_OK;
-    while (!K.stop) {
-        uint32_t pp = __shfl_sync(gmask, lane_prog(L), pred, G);
-        uint32_t pf = __shfl_sync(gmask, lane_fnz(L), pred, G);
-        RowDone rd;
-        bool fin = lane_step(L, c, pp, pf, K.next, G, eh, qp, tgt, qs, &rd);
-        unsigned b = __ballot_sync(gmask, fin);
-        if (b) {
-            if (__popc(b) != 1) { err = G3X_ERR_INTERNAL; break; }
-            int src = (__ffs(b) - 1) & (G - 1);
-            RowDone cd;
-            cd.m = __shfl_sync(gmask, rd.m, src, G);
-            cd.mj = __shfl_sync(gmask, rd.mj, src, G);
-            cd.gval = __shfl_sync(gmask, rd.gval, src, G);
-            cd.ncells = __shfl_sync(gmask, rd.ncells, src, G);
-            commit_row(K, c, cd);
-        }
-        __syncwarp(gmask);
-        if (++steps > limit) { err = G3X_ERR_TIMEOUT; break; }
-    }
-    if (r == 0) {
-        d.out[job] = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};
-        d.status[job] = err;
-        if (d.cells) d.cells[job] = (int32_t)K.cells;
-    }
+    SmemEh buf{eh};
+    if (job_is_narrow(c, sp.max_sc))
+        run_dp<G, true>(job, c, d, buf, qp, tgt, qs, r, gmask);
+    else
+        run_dp<G, false>(job, c, d, buf, qp, tgt, qs, r, gmask);
     __syncwarp(gmask);
 }
 

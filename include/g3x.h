@@ -96,7 +96,8 @@ typedef struct {
     int32_t schedule;     /* G3X_SCHED_* */
     int32_t max_qlen;     /* upper bound of qlen over the batch (required) */
     int32_t max_tlen;     /* upper bound of tlen over the batch (required) */
-    int32_t lanes;        /* lanes per job for persistent schedules: 8, 16, 32, or 0 = tuned */
+    int32_t lanes;        /* lanes per job for persistent schedules: 8, 16, 32, or 0 = tuned;
+                             raised when a warp of such groups would not fit in shared memory */
     int32_t *d_cells;     /* optional per-job DP cell count (trip count of ksw.cu:346) */
 } g3x_batch_opts_t;
 
@@ -107,6 +108,13 @@ int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
                           int32_t n, const uint32_t *d_codes, const uint32_t *d_nmask,
                           g3x_ext_t *d_out, int32_t *d_status, const g3x_batch_opts_t *opts,
                           void *stream);
+
+/* ---- diagnostics ------------------------------------------------------------------------ */
+
+/* Measured 32-bit integer ALU throughput of the context's GPU (ops/s): independent chains of
+   the 3-input DPX maximum on every SM.  The cells/s roofline is this figure / 8 (ops per DP
+   cell).  No counterpart in the reference. */
+int g3x_int_peak(g3x_ctx *ctx, double *ops_per_s);
 
 /* ---- host-side packing ----------------------------------------------------------------- */
 
