@@ -41,6 +41,14 @@ EXT_DT = np.dtype([("score", "<i4"), ("qle", "<i4"), ("tle", "<i4"), ("gtle", "<
 SEED_DT = np.dtype([("read_off", "<i8"), ("win_off", "<i8"), ("rmax0", "<i8"), ("rmax1", "<i8"),
                     ("rbeg", "<i8"), ("l_query", "<i4"), ("qbeg", "<i4"), ("len", "<i4"),
                     ("pad_", "<i4")])
+OPT_DT = np.dtype([("score", SCORE_DT), ("a", "<i4"), ("w", "<i4"), ("pen_clip5", "<i4"),
+                   ("pen_clip3", "<i4")])
+DSEED_DT = np.dtype([("read_off", "<u4"), ("win_off", "<u4"), ("l_query", "<i4"), ("qbeg", "<i4"),
+                     ("len", "<i4"), ("pad_", "<i4"), ("rbeg", "<i8"), ("rmax0", "<i8"),
+                     ("rmax1", "<i8")])
+REG_DT = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), ("score", "<i4"),
+                   ("truesc", "<i4"), ("w", "<i4"), ("tries_left", "u1"), ("tries_right", "u1"),
+                   ("pad_", "u1", 2)])
 BATCH_OPTS_DT = np.dtype([("schedule", "<i4"), ("max_qlen", "<i4"), ("max_tlen", "<i4"),
                           ("lanes", "<i4"), ("d_cells", "<u8")])
 SYNTH_PARAMS_DT = np.dtype([("kind", "<i4"), ("n", "<i4"), ("w", "<i4"), ("a", "<i4"),
@@ -48,7 +56,24 @@ SYNTH_PARAMS_DT = np.dtype([("kind", "<i4"), ("n", "<i4"), ("w", "<i4"), ("a", "
                             ("threads", "<i4"), ("pad_", "<i4"), ("unrelated", "<f8"),
                             ("seed", "<u8")])
 assert SCORE_DT.itemsize == 56 and JOB_DT.itemsize == 24 and EXT_DT.itemsize == 24
-assert SEED_DT.itemsize == 56
+assert SEED_DT.itemsize == 56 and OPT_DT.itemsize == 72 and DSEED_DT.itemsize == 48
+assert REG_DT.itemsize == 40
+
+
+def default_opt(w=100, a=1, pen_clip5=5, pen_clip3=5, **score_kw):
+    """g3x_opt_t with mem_opt_init defaults (bwa/src/fastmap.cpp:77-113)."""
+    o = np.zeros(1, OPT_DT)
+    o["score"] = default_score(a=a, **score_kw)
+    o["a"], o["w"], o["pen_clip5"], o["pen_clip3"] = a, w, pen_clip5, pen_clip3
+    return o
+
+
+def device_seeds(seeds):
+    """SEED_DT records (the generator's / oracle's layout) as g3x_seed_t records."""
+    d = np.zeros(len(seeds), DSEED_DT)
+    for f in ("read_off", "win_off", "l_query", "qbeg", "len", "rbeg", "rmax0", "rmax1"):
+        d[f] = seeds[f]
+    return d
 
 
 def bwa_matrix(a=1, b=4):
@@ -91,6 +116,11 @@ def lib():
         L.g3x_strerror.restype = ctypes.c_char_p
         L.g3x_ksw_extend2_batch.argtypes = [P, P, P, I32, P, P, P, P, P, P]
         L.g3x_ksw_extend2_batch.restype = ctypes.c_int
+        L.g3x_extend_seeds.argtypes = [P, P, P, I32, P, P, P, P, P, P]
+        L.g3x_extend_seeds.restype = ctypes.c_int
+        L.g3x_extend_seeds_stream.argtypes = [P, P, P, ctypes.c_int64, P, P, ctypes.c_int64, P, P,
+                                              I32, P]
+        L.g3x_extend_seeds_stream.restype = ctypes.c_int
         L.g3x_int_peak.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
         L.g3x_int_peak.restype = ctypes.c_int
         L.g3x_pack_codes.argtypes = [P, ctypes.c_int64, P, P, ctypes.c_int64]
@@ -224,6 +254,30 @@ class Context:
                                          _ptr(d_codes), _ptr(d_nmask), _ptr(d_out),
                                          _ptr(d_status), opts.ctypes.data, _stream(stream))
         _check(rc, "g3x_ksw_extend2_batch")
+
+
+    def extend_seeds(self, opt, d_seeds, n, d_codes, d_nmask, d_regs, d_status, max_qlen,
+                     max_tlen, schedule=SCHED_SORTED, lanes=0, stream=None):
+        """g3x_extend_seeds: left + right extension with band retry on device buffers."""
+        opts = np.zeros(1, BATCH_OPTS_DT)
+        opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
+            schedule, max_qlen, max_tlen, lanes)
+        rc = lib().g3x_extend_seeds(self._h, opt.ctypes.data, _ptr(d_seeds), int(n), _ptr(d_codes),
+                                    _ptr(d_nmask), _ptr(d_regs), _ptr(d_status), opts.ctypes.data,
+                                    _stream(stream))
+        _check(rc, "g3x_extend_seeds")
+
+    def extend_seeds_stream(self, opt, seeds, codes, nmask, n_bases, regs, status, max_qlen,
+                            max_tlen, chunk=65536, schedule=SCHED_SORTED, lanes=0):
+        """g3x_extend_seeds_stream on host arrays (numpy or pinned torch tensors)."""
+        opts = np.zeros(1, BATCH_OPTS_DT)
+        opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
+            schedule, max_qlen, max_tlen, lanes)
+        hp = lambda a: a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr()  # noqa: E731
+        rc = lib().g3x_extend_seeds_stream(self._h, opt.ctypes.data, hp(seeds), len(seeds), hp(codes),
+                                           hp(nmask), int(n_bases), hp(regs), hp(status), int(chunk),
+                                           opts.ctypes.data)
+        _check(rc, "g3x_extend_seeds_stream")
 
 
 def _ptr(t):

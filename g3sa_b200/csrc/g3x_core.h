@@ -245,35 +245,70 @@ G3X_HD void lane_end_row(Lane& L, const JobConst& c, Buf& buf, RowDone* done) {
     L.lat = 0;
 }
 
-// One step of one lane.  `pprog`/`pfnz` are the predecessor's published words at the start
-// of the step.  Returns true when the lane's row ended in this step (then *done is
-// filled).  `buf` gives the job's row buffer (load4 / store / note_read), `qp` the query
-// profile, `tgt` the target codes.
-//
-// Buf interface:  load4(jb, EhCell v[4])  -- the four slots of the aligned block at jb
-//                 store(c, h, e)          -- write slot c
-//                 note_read(c)            -- the lane consumed slot c (test hook)
-template <int G, bool kNarrow, class Buf>
-G3X_HD bool lane_step(Lane& L, const JobConst& c, uint32_t pprog, uint32_t pfnz, Buf& buf,
-                      const int8_t* qp, const uint8_t* tgt, int32_t qstride, RowDone* done) {
-    // Latch the predecessor's final words the step they appear (it moves on next step).
-    if ((pprog >> 16) == kNone) { L.lat_prog = pprog; L.lat_fnz = pfnz; L.lat = 1; }
-    if (L.lat) { pprog = L.lat_prog; pfnz = L.lat_fnz; }
+// One cell of ksw.cu:346-370 on the lane's running state.  M = H(i-1,j-1) ? H(i-1,j-1) + S : 0
+// is written as min(H + S, 256 H): equal when H > 0, and <= 0 when H == 0, which every use
+// below clips to 0 exactly like the reference's 0.  Writes eh[col] = {H(i,col-1), E(i+1,col)}
+// and returns that entry's "non-zero" word.
+template <bool kNarrow, class Buf>
+G3X_HD int32_t dp_cell(const JobConst& c, Buf& buf, int32_t col, EhCell v, int32_t s,
+                       int32_t& h1, int32_t& f, int32_t& key, int32_t& m, int32_t& mj) {
+    const int32_t M = addmin_i32(v.h, s, v.h << 8);
+    const int32_t h = max3_i32(M, v.e, f);
+    const int32_t te = addmax_i32(M, -c.oe_del, 0);
+    const int32_t e2 = addmax_i32(v.e, -c.e_del, te);
+    buf.store(col, h1, e2);
+    const int32_t nz = h1 | e2;
+    if (kNarrow) {
+        const int32_t k2 = (h << 16) | col;
+        key = key > k2 ? key : k2;
+    } else {
+        if (h >= m) { m = h; mj = col; }
+    }
+    const int32_t tf = addmax_i32(M, -c.oe_ins, 0);
+    f = addmax_i32(f, -c.e_ins, tf);
+    h1 = h;
+    return nz;
+}
 
-    if (L.st == kDone) {                                  // published once; take next row
+// Lane transitions outside a running row: a finished row is published for one step, then
+// the lane takes row i+G; a waiting lane starts once its predecessor row has a first
+// non-zero column (or is finished).
+template <int G, class Tgt>
+G3X_HD void lane_advance(Lane& L, const JobConst& c, uint32_t pfnz, const Tgt& tgt,
+                         int32_t qstride) {
+    if (L.st == kDone) {
         L.i += G;
         L.st = L.i < c.tlen ? kWait : kIdle;
     }
     if (L.st == kWait) {
         if (L.i == 0) {
             int32_t b = -c.w;
-            lane_begin_row(L, b > 0 ? b : 0, c, tgt[0], qstride);
+            lane_begin_row(L, b > 0 ? b : 0, c, tgt.code(0), qstride);
         } else if (pfnz != kNone) {
             int32_t b = L.i - c.w;
-            lane_begin_row(L, (int32_t)pfnz > b ? (int32_t)pfnz : b, c, tgt[L.i], qstride);
+            lane_begin_row(L, (int32_t)pfnz > b ? (int32_t)pfnz : b, c, tgt.code(L.i), qstride);
         }
     }
-    if (L.st != kRun) return false;
+}
+
+// One step of one lane.  `pprog`/`pfnz` are the predecessor's published words at the start
+// of the step.  Returns true when the lane's row ended in this step (then *done is
+// filled).  `buf` gives the job's row buffer, `qp` the query profile, `tgt` the target.
+//
+// Buf interface:  load4(jb, EhCell v[4])  -- the four slots of the aligned block at jb
+//                 store(c, h, e)          -- write slot c
+//                 note_read(c)            -- the lane consumed slot c (test hook)
+// Tgt interface:  code(i)                 -- target code (0-4) of row i
+template <int G, bool kNarrow, class Buf, class Tgt>
+G3X_HD bool lane_step(Lane& L, const JobConst& c, uint32_t pprog, uint32_t pfnz, Buf& buf,
+                      const int8_t* qp, const Tgt& tgt, int32_t qstride, RowDone* done) {
+    // Latch the predecessor's final words the step they appear (it moves on next step).
+    if ((pprog >> 16) == kNone) { L.lat_prog = pprog; L.lat_fnz = pfnz; L.lat = 1; }
+    if (L.lat) { pprog = L.lat_prog; pfnz = L.lat_fnz; }
+    if (L.st != kRun) {
+        lane_advance<G>(L, c, pfnz, tgt, qstride);
+        if (L.st != kRun) return false;
+    }
 
     uint32_t colp = pprog >> 16, lnzp = pprog & 0xFFFFu;
     if (L.i == 0) { colp = kNone; lnzp = kNone; }        // row 0 reads the initial buffer
@@ -288,40 +323,37 @@ G3X_HD bool lane_step(Lane& L, const JobConst& c, uint32_t pprog, uint32_t pfnz,
         buf.load4(jb, v);
         const uint32_t sc4 = *reinterpret_cast<const uint32_t*>(qp + L.qrow + jb);
         int32_t h1 = L.h1, f = L.f, key = L.key, m = L.m, mj = L.mj, lnz1 = L.lnz1;
-        bool fnz_open = L.fnz == (int32_t)kNone;
+        int32_t nzw[kBlock];
+        if (j0 == jb && jb + kBlock <= lim) {
+            // whole block inside the band: no per-cell predicates
 #pragma unroll
-        for (int t = 0; t < kBlock; ++t) {
-            const int32_t col = jb + t;
-            if (col >= j0 && col < lim) {
-                // One cell of ksw.cu:346-370.  M = H(i-1,j-1) ? H(i-1,j-1) + S : 0 is written
-                // as min(H + S, 256 H): equal when H > 0, and <= 0 when H == 0, which every
-                // use below clips to 0 exactly like the reference's 0.
-                buf.note_read(col);
-                const int32_t s = (int32_t)(int8_t)(sc4 >> (8 * t));
-                const int32_t hd = v[t].h, ed = v[t].e;
-                const int32_t M = addmin_i32(hd, s, hd << 8);
-                const int32_t h = max3_i32(M, ed, f);
-                const int32_t te = addmax_i32(M, -c.oe_del, 0);
-                const int32_t e2 = addmax_i32(ed, -c.e_del, te);
-                buf.store(col, h1, e2);
-                if ((h1 | e2) != 0) {
-                    lnz1 = col + 1;
-                    if (fnz_open) { L.fnz = col; fnz_open = false; }
-                }
-                if (kNarrow) {
-                    const int32_t k2 = (h << 16) | col;
-                    key = key > k2 ? key : k2;
-                } else {
-                    if (h >= m) { m = h; mj = col; }
-                }
-                const int32_t tf = addmax_i32(M, -c.oe_ins, 0);
-                f = addmax_i32(f, -c.e_ins, tf);
-                h1 = h;
+            for (int t = 0; t < kBlock; ++t) {
+                buf.note_read(jb + t);
+                nzw[t] = dp_cell<kNarrow>(c, buf, jb + t, v[t], (int32_t)(int8_t)(sc4 >> (8 * t)),
+                                          h1, f, key, m, mj);
+                if (nzw[t]) lnz1 = jb + t + 1;
             }
+            L.j = jb + kBlock;
+        } else {
+#pragma unroll
+            for (int t = 0; t < kBlock; ++t) {
+                const int32_t col = jb + t;
+                nzw[t] = 0;
+                if (col >= j0 && col < lim) {
+                    buf.note_read(col);
+                    nzw[t] = dp_cell<kNarrow>(c, buf, col, v[t], (int32_t)(int8_t)(sc4 >> (8 * t)),
+                                              h1, f, key, m, mj);
+                    if (nzw[t]) lnz1 = col + 1;
+                }
+            }
+            L.j = jb + kBlock < lim ? jb + kBlock : lim;
+        }
+        if (L.fnz == (int32_t)kNone) {            // first non-zero entry of the row (rare path)
+#pragma unroll
+            for (int t = kBlock - 1; t >= 0; --t)
+                if (nzw[t]) L.fnz = jb + t;
         }
         L.h1 = h1; L.f = f; L.key = key; L.m = m; L.mj = mj; L.lnz1 = lnz1;
-        const int32_t jend = jb + kBlock < lim ? jb + kBlock : lim;
-        L.j = jend;
     }
     const int32_t jn = L.j;
     if (jn >= L.cap || (pdone && (uint32_t)jn > lnzp)) {

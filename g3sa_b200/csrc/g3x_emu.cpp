@@ -36,11 +36,17 @@ struct EmuBuf {
     void note_read(int c) const { touch(c); }
 };
 
+struct EmuTgt {
+    const uint8_t* p;
+    int32_t code(int32_t i) const { return p[i]; }
+};
+
 template <int G>
 bool step_g(bool narrow, g3x::Lane& L, const g3x::JobConst& c, uint32_t pp, uint32_t pf, EmuBuf& eh,
             const int8_t* qp, const uint8_t* tgt, int qs, g3x::RowDone* rd) {
-    return narrow ? g3x::lane_step<G, true>(L, c, pp, pf, eh, qp, tgt, qs, rd)
-                  : g3x::lane_step<G, false>(L, c, pp, pf, eh, qp, tgt, qs, rd);
+    const EmuTgt tg{tgt};
+    return narrow ? g3x::lane_step<G, true>(L, c, pp, pf, eh, qp, tg, qs, rd)
+                  : g3x::lane_step<G, false>(L, c, pp, pf, eh, qp, tg, qs, rd);
 }
 
 // The lane count is a template parameter of lane_step (it sets the row stride).

@@ -33,6 +33,27 @@ struct LaunchDesc {
 };
 
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+
+// Device scratch of one seed-level call (capacity >= n seeds).
+struct SeedScratch {
+    g3x_job_t *ljobs, *rjobs;
+    g3x_ext_t *lext, *rext;
+    int32_t *lstatus, *rstatus;
+    int32_t* order[4];     // left wave 1/2, right wave 1/2
+    int32_t* counters;     // 16 ints
+    int64_t cap;
+};
+
+int extend_seeds(const SeedScratch& ws, const g3x_opt_t& opt, const ScoreParams& sp,
+                 const g3x_seed_t* seeds, int n, const uint32_t* codes, const uint32_t* nmask,
+                 g3x_reg_t* regs, int32_t* status, const LaunchDesc& proto, cudaStream_t st);
+int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), const g3x_opt_t& opt,
+                        const ScoreParams& sp, const g3x_seed_t* h_seeds, int64_t n,
+                        const uint32_t* h_codes, const uint32_t* h_nmask, int64_t n_bases,
+                        g3x_reg_t* h_regs, int32_t* h_status, int32_t chunk,
+                        const LaunchDesc& proto);
+int score_params(const g3x_score_t* s, ScoreParams* sp);
+int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d);
 size_t group_smem_bytes(int qmax, int tmax);
 int measure_int_peak(int device, double* ops_per_s);
 

@@ -109,6 +109,59 @@ int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
                           g3x_ext_t *d_out, int32_t *d_status, const g3x_batch_opts_t *opts,
                           void *stream);
 
+/* ---- seed-level extension with band retry ---------------------------------------------- */
+
+/* Options of the seed-level call: scoring, match score a (the seed scores len * a), the first
+   band width w (a retry uses 2w; MAX_BAND_TRY = 2, bwa/src/aux.cuh:401) and the clipping
+   penalties that choose local vs to-end extension (mem_opt_t pen_clip5/pen_clip3,
+   bwa/src/bwa.h:157-189). */
+typedef struct {
+    g3x_score_t score;
+    int32_t a, w, pen_clip5, pen_clip3;
+} g3x_opt_t;              /* 72 bytes */
+
+/* One seed of a chain with its reference window, as mem_chain2aln sees it
+   (mem_seed_t, bwa/src/bwa.h:202-210; window [rmax0, rmax1) of bwa/src/aux.cu:187-205). */
+typedef struct {
+    uint32_t read_off;    /* base index of read[0] in the planes */
+    uint32_t win_off;     /* base index of reference position rmax0 in the planes */
+    int32_t  l_query;     /* read length */
+    int32_t  qbeg, len;   /* seed on the read */
+    int32_t  pad_;
+    int64_t  rbeg;        /* seed start on the reference */
+    int64_t  rmax0, rmax1;
+} g3x_seed_t;             /* 48 bytes */
+
+/* The mem_alnreg_t fields the extension block of mem_chain2aln sets
+   (bwa/src/bwa.h:229-247, bwa/src/aux.cu:253-309). */
+typedef struct {
+    int64_t rb, re;       /* [rb, re) on the reference */
+    int32_t qb, qe;       /* [qb, qe) on the read */
+    int32_t score, truesc;
+    int32_t w;            /* band width used: max over the two sides */
+    uint8_t tries_left, tries_right;   /* ksw_extend2 calls made on each side (0-2) */
+    uint8_t pad_[2];
+} g3x_reg_t;              /* 40 bytes */
+
+/* Left then right extension of n seeds with BWA's band retry, replacing the extension block
+   of mem_chain2aln (bwa/src/aux.cu:253-310) for one seed per call.  Device buffers;
+   asynchronous on `stream`.  opts->max_qlen / max_tlen bound read and window lengths;
+   opts->schedule and lanes pick the extension kernel.  The first call with a larger n
+   allocates context scratch (synchronously). */
+int g3x_extend_seeds(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t *d_seeds, int32_t n,
+                     const uint32_t *d_codes, const uint32_t *d_nmask, g3x_reg_t *d_regs,
+                     int32_t *d_status, const g3x_batch_opts_t *opts, void *stream);
+
+/* The same over n host seeds in chunks of `chunk` seeds: each chunk's seeds and the plane
+   words they reference are copied to the GPU while the previous chunk is extended (two
+   device buffer sets, a copy stream and a compute stream), and the regions come back to
+   h_regs/h_status.  Host buffers should be pinned for the copies to overlap.  Blocks until
+   all chunks are done. */
+int g3x_extend_seeds_stream(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t *h_seeds,
+                            int64_t n, const uint32_t *h_codes, const uint32_t *h_nmask,
+                            int64_t n_bases, g3x_reg_t *h_regs, int32_t *h_status,
+                            int32_t chunk, const g3x_batch_opts_t *opts);
+
 /* ---- diagnostics ------------------------------------------------------------------------ */
 
 /* Measured 32-bit integer ALU throughput of the context's GPU (ops/s): independent chains of

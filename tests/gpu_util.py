@@ -34,3 +34,19 @@ def run_batch(u8, jobs, score, schedule=g.SCHED_PLAIN, lanes=0, max_qlen=None, m
                        schedule=schedule, lanes=lanes, d_cells=cells)
     torch.cuda.synchronize()
     return out.cpu().numpy(), status.cpu().numpy(), cells.cpu().numpy()
+
+
+def run_seeds(u8, seeds, opt, schedule=g.SCHED_SORTED, lanes=0):
+    """Seed-level extension on the GPU: returns (regs REG_DT, status)."""
+    import torch
+    codes, nmask = g.pack_planes(u8)
+    ds = g.device_seeds(seeds)
+    n = len(ds)
+    d_seeds, d_codes, d_nmask = to_dev(ds), to_dev(codes), to_dev(nmask)
+    d_regs = torch.zeros(n * g.REG_DT.itemsize, dtype=torch.uint8, device="cuda")
+    d_status = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+    mq = int(seeds["l_query"].max())
+    mt = int((seeds["rmax1"] - seeds["rmax0"]).max())
+    ctx().extend_seeds(opt, d_seeds, n, d_codes, d_nmask, d_regs, d_status, mq, mt, schedule, lanes)
+    torch.cuda.synchronize()
+    return d_regs.cpu().numpy().view(g.REG_DT), d_status.cpu().numpy()
