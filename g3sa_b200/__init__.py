@@ -50,7 +50,10 @@ REG_DT = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), (
                    ("truesc", "<i4"), ("w", "<i4"), ("tries_left", "u1"), ("tries_right", "u1"),
                    ("pad_", "u1", 2)])
 BATCH_OPTS_DT = np.dtype([("schedule", "<i4"), ("max_qlen", "<i4"), ("max_tlen", "<i4"),
-                          ("lanes", "<i4"), ("d_cells", "<u8")])
+                          ("lanes", "<i4"), ("tile", "<i4"), ("kernel", "<i4"), ("d_cells", "<u8")])
+KERNEL_AUTO, KERNEL_ROLLING, KERNEL_ROWPAR = 0, 1, 2
+TILE_DT = np.dtype([("width", "<i4"), ("lanes", "<i4"), ("tile", "<i4"), ("warp_batch", "<i4")])
+MLP_PARAMS, MLP_FEATURES = 4609, 5
 SYNTH_PARAMS_DT = np.dtype([("kind", "<i4"), ("n", "<i4"), ("w", "<i4"), ("a", "<i4"),
                             ("o_del", "<i4"), ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4"),
                             ("threads", "<i4"), ("pad_", "<i4"), ("unrelated", "<f8"),
@@ -121,6 +124,17 @@ def lib():
         L.g3x_extend_seeds_stream.argtypes = [P, P, P, ctypes.c_int64, P, P, ctypes.c_int64, P, P,
                                               I32, P]
         L.g3x_extend_seeds_stream.restype = ctypes.c_int
+        L.g3x_features.argtypes = [P, P, I32, P, P, P, P]
+        L.g3x_mlp_init.argtypes = [P, ctypes.c_uint64]
+        L.g3x_mlp_train.argtypes = [P, P, P, I32, I32, I32, ctypes.c_float, ctypes.c_uint64, P]
+        L.g3x_mlp_gradient.argtypes = [P, P, P, I32, P, P]
+        L.g3x_mlp_predict.argtypes = [P, P, I32, P, P]
+        L.g3x_mlp_get_params.argtypes = [P, P]
+        L.g3x_mlp_set_params.argtypes = [P, P]
+        L.g3x_get_tiles.argtypes = [P, P, P]
+        L.g3x_set_tiles.argtypes = [P, P, I32]
+        L.g3x_autotune.argtypes = [P, P, P, I32, P, P, I32, I32, P, P]
+        L.g3x_last_stats.argtypes = [P, P]
         L.g3x_int_peak.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
         L.g3x_int_peak.restype = ctypes.c_int
         L.g3x_pack_codes.argtypes = [P, ctypes.c_int64, P, P, ctypes.c_int64]
@@ -237,6 +251,65 @@ class Context:
         except Exception:
             pass
 
+    # ---- learned cost model ----
+    def features(self, d_jobs, n, d_codes, d_nmask, d_feat, stream=None):
+        _check(lib().g3x_features(self._h, _ptr(d_jobs), int(n), _ptr(d_codes), _ptr(d_nmask),
+                                  _ptr(d_feat), _stream(stream)), "g3x_features")
+
+    def mlp_init(self, seed):
+        _check(lib().g3x_mlp_init(self._h, int(seed)), "g3x_mlp_init")
+
+    def mlp_train(self, d_feat, d_target, n, epochs, batch, lr, seed=0):
+        losses = np.zeros(max(epochs, 1), np.float32)
+        _check(lib().g3x_mlp_train(self._h, _ptr(d_feat), _ptr(d_target), int(n), int(epochs),
+                                   int(batch), float(lr), int(seed), losses.ctypes.data),
+               "g3x_mlp_train")
+        return losses[:epochs]
+
+    def mlp_gradient(self, d_feat, d_target, n):
+        grad = np.zeros(MLP_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        _check(lib().g3x_mlp_gradient(self._h, _ptr(d_feat), _ptr(d_target), int(n),
+                                      grad.ctypes.data, ctypes.addressof(loss)), "g3x_mlp_gradient")
+        return grad, loss.value
+
+    def mlp_predict(self, d_feat, n, d_pred, stream=None):
+        _check(lib().g3x_mlp_predict(self._h, _ptr(d_feat), int(n), _ptr(d_pred), _stream(stream)),
+               "g3x_mlp_predict")
+
+    def mlp_params(self):
+        p = np.zeros(MLP_PARAMS, np.float32)
+        _check(lib().g3x_mlp_get_params(self._h, p.ctypes.data), "g3x_mlp_get_params")
+        return p
+
+    def mlp_set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        _check(lib().g3x_mlp_set_params(self._h, p.ctypes.data), "g3x_mlp_set_params")
+
+    # ---- width classes / autotuning ----
+    def get_tiles(self):
+        t = np.zeros(8, TILE_DT)
+        n = ctypes.c_int32()
+        _check(lib().g3x_get_tiles(self._h, t.ctypes.data, ctypes.addressof(n)), "g3x_get_tiles")
+        return [tuple(int(v) for v in row) for row in t[:n.value]]
+
+    def set_tiles(self, tiles):
+        t = np.array([tuple(x) for x in tiles], TILE_DT)
+        _check(lib().g3x_set_tiles(self._h, t.ctypes.data, len(t)), "g3x_set_tiles")
+
+    def autotune(self, score, d_jobs, n, d_codes, d_nmask, max_qlen, max_tlen):
+        t = np.zeros(8, TILE_DT)
+        k = ctypes.c_int32()
+        _check(lib().g3x_autotune(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
+                                  _ptr(d_nmask), int(max_qlen), int(max_tlen), t.ctypes.data,
+                                  ctypes.addressof(k)), "g3x_autotune")
+        return [tuple(int(v) for v in row) for row in t[:k.value]]
+
+    def last_stats(self):
+        s = np.zeros(3, np.uint64)
+        _check(lib().g3x_last_stats(self._h, s.ctypes.data), "g3x_last_stats")
+        return [int(v) for v in s]
+
     def int_peak(self):
         """Measured 32-bit integer ALU ops/s of this GPU (g3x_int_peak)."""
         v = ctypes.c_double()
@@ -244,11 +317,13 @@ class Context:
         return v.value
 
     def extend_batch(self, score, d_jobs, n, d_codes, d_nmask, d_out, d_status, max_qlen,
-                     max_tlen, schedule=SCHED_PLAIN, lanes=0, d_cells=None, stream=None):
+                     max_tlen, schedule=SCHED_PLAIN, lanes=0, d_cells=None, stream=None,
+                     tile=0, kernel=KERNEL_AUTO):
         """g3x_ksw_extend2_batch on torch device tensors (or raw device pointers)."""
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
             schedule, max_qlen, max_tlen, lanes)
+        opts["tile"], opts["kernel"] = tile, kernel
         opts["d_cells"] = _ptr(d_cells) if d_cells is not None else 0
         rc = lib().g3x_ksw_extend2_batch(self._h, score.ctypes.data, _ptr(d_jobs), int(n),
                                          _ptr(d_codes), _ptr(d_nmask), _ptr(d_out),
@@ -257,22 +332,26 @@ class Context:
 
 
     def extend_seeds(self, opt, d_seeds, n, d_codes, d_nmask, d_regs, d_status, max_qlen,
-                     max_tlen, schedule=SCHED_SORTED, lanes=0, stream=None):
+                     max_tlen, schedule=SCHED_SORTED, lanes=0, stream=None, tile=0,
+                     kernel=KERNEL_AUTO):
         """g3x_extend_seeds: left + right extension with band retry on device buffers."""
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
             schedule, max_qlen, max_tlen, lanes)
+        opts["tile"], opts["kernel"] = tile, kernel
         rc = lib().g3x_extend_seeds(self._h, opt.ctypes.data, _ptr(d_seeds), int(n), _ptr(d_codes),
                                     _ptr(d_nmask), _ptr(d_regs), _ptr(d_status), opts.ctypes.data,
                                     _stream(stream))
         _check(rc, "g3x_extend_seeds")
 
     def extend_seeds_stream(self, opt, seeds, codes, nmask, n_bases, regs, status, max_qlen,
-                            max_tlen, chunk=65536, schedule=SCHED_SORTED, lanes=0):
+                            max_tlen, chunk=65536, schedule=SCHED_SORTED, lanes=0, tile=0,
+                            kernel=KERNEL_AUTO):
         """g3x_extend_seeds_stream on host arrays (numpy or pinned torch tensors)."""
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
             schedule, max_qlen, max_tlen, lanes)
+        opts["tile"], opts["kernel"] = tile, kernel
         hp = lambda a: a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr()  # noqa: E731
         rc = lib().g3x_extend_seeds_stream(self._h, opt.ctypes.data, hp(seeds), len(seeds), hp(codes),
                                            hp(nmask), int(n_bases), hp(regs), hp(status), int(chunk),

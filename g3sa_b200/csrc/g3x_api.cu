@@ -11,6 +11,12 @@ struct g3x_ctx {
     int sms;
     int32_t* d_queue;            // persistent-kernel job counters
     g3x::SeedScratch seeds;      // seed-level scratch, grown on demand
+    g3x::ModelState model;       // learned cost model
+    g3x::SchedScratch sched;     // job order and width classes of a persistent batch
+    g3x::TileTable tiles;        // width classes and their kernel configurations
+    unsigned long long* d_stats; // occupancy counters of the last persistent batch
+    cudaStream_t side[g3x::kMaxBuckets];   // one stream per width class
+    cudaEvent_t fork, join[g3x::kMaxBuckets];
 };
 
 namespace g3x {
@@ -27,6 +33,7 @@ int score_params(const g3x_score_t* s, ScoreParams* sp) {
     }
     sp->o_del = s->o_del; sp->e_del = s->e_del; sp->o_ins = s->o_ins; sp->e_ins = s->e_ins;
     sp->zdrop = s->zdrop; sp->end_bonus = s->end_bonus; sp->max_sc = max_sc;
+    sp->oe_del = s->o_del + s->e_del; sp->oe_ins = s->o_ins + s->e_ins;
     return G3X_OK;
 }
 
@@ -39,25 +46,37 @@ int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d) {
     d->qmax = opts->max_qlen;
     d->tmax = opts->max_tlen;
     d->cells = opts->d_cells;
-    switch (opts->schedule) {
-        case G3X_SCHED_PLAIN:
-            d->lanes = 32; d->persistent = 0; d->warps_per_block = 1;
-            break;
-        case G3X_SCHED_SORTED:
-        case G3X_SCHED_LEARNED: {
-            int lanes = opts->lanes ? opts->lanes : 8;
-            if (lanes != 8 && lanes != 16 && lanes != 32) return G3X_ERR_INVALID;
-            // Shared memory per job grows with the query; a warp of narrow groups must fit,
-            // so the lane count is raised until it does.
-            while (lanes < 32 && (32 / lanes) * group_smem_bytes(d->qmax, d->tmax) > 227 * 1024)
-                lanes *= 2;
-            d->lanes = lanes; d->persistent = 1; d->warps_per_block = 4;
-            d->queue = queue;
-            break;
+    if (opts->schedule != G3X_SCHED_PLAIN && opts->schedule != G3X_SCHED_SORTED &&
+        opts->schedule != G3X_SCHED_LEARNED)
+        return G3X_ERR_INVALID;
+    if (opts->kernel < G3X_KERNEL_AUTO || opts->kernel > G3X_KERNEL_ROWPAR) return G3X_ERR_INVALID;
+    const bool plain = opts->schedule == G3X_SCHED_PLAIN;
+    d->kernel = opts->kernel == G3X_KERNEL_AUTO ? (plain ? kKernelRolling : kKernelRowpar)
+                                                : (opts->kernel == G3X_KERNEL_ROLLING ? kKernelRolling : kKernelRowpar);
+    if (plain) {
+        // one 32-lane block per job, jobs in the given order
+        d->lanes = 32; d->tile = opts->tile ? opts->tile : 9; d->persistent = 0; d->warps_per_block = 1;
+    } else {
+        int lanes = opts->lanes, tile = opts->tile ? opts->tile : 9;
+        if (!lanes) {
+            // row-parallel: the narrowest group whose tile covers the widest query;
+            // rolling: 8-lane groups
+            lanes = 8;
+            if (d->kernel == kKernelRowpar) {
+                lanes = 4;
+                while (lanes < 32 && lanes * tile < d->qmax) lanes *= 2;
+            }
         }
-        default:
-            return G3X_ERR_INVALID;
+        if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) return G3X_ERR_INVALID;
+        if (lanes == 4 && d->kernel != kKernelRowpar) return G3X_ERR_INVALID;
+        // Shared memory per job grows with the query; a warp of narrow groups must fit,
+        // so the lane count is raised until it does.
+        while (lanes < 32 && (32 / lanes) * group_smem_bytes(d->qmax, d->tmax) > 227 * 1024)
+            lanes *= 2;
+        d->lanes = lanes; d->tile = tile; d->persistent = 1; d->warps_per_block = 4;
+        d->queue = queue;
     }
+    if (d->tile != 5 && d->tile != 9 && d->tile != 13) return G3X_ERR_INVALID;
     return G3X_OK;
 }
 
@@ -84,6 +103,96 @@ int alloc_seed_scratch(SeedScratch& w, int64_t n) {
     if (!ok) { free_seed_scratch(w); return G3X_ERR_NOMEM; }
     w.cap = cap;
     return G3X_OK;
+}
+
+static void free_sched(SchedScratch& s) {
+    cudaFree(s.bin); cudaFree(s.order); cudaFree(s.hist); cudaFree(s.cursor); cudaFree(s.bucket_oc);
+    cudaFree(s.feat); cudaFree(s.pred);
+    s = SchedScratch();
+}
+
+static int alloc_sched(SchedScratch& s, int64_t n) {
+    if (n <= s.cap && s.order) return G3X_OK;
+    free_sched(s);
+    const int64_t cap = std::max<int64_t>(n, 1024);
+    const int bins = kMaxBuckets * 1024;
+    if (cudaMalloc(&s.bin, cap * sizeof(int32_t)) || cudaMalloc(&s.order, cap * sizeof(int32_t)) ||
+        cudaMalloc(&s.hist, bins * sizeof(int32_t)) || cudaMalloc(&s.cursor, bins * sizeof(int32_t)) ||
+        cudaMalloc(&s.bucket_oc, 2 * kMaxBuckets * sizeof(int32_t)) ||
+        cudaMalloc(&s.feat, cap * G3X_MLP_FEATURES * sizeof(float)) || cudaMalloc(&s.pred, cap * sizeof(float))) {
+        free_sched(s);
+        return G3X_ERR_NOMEM;
+    }
+    s.cap = cap;
+    return G3X_OK;
+}
+
+// Default width classes: each uses the narrowest group whose tile (lanes x odd cells per lane)
+// covers the class width; the last class tiles wider rows.
+static void default_tiles(TileTable& t) {
+    const int w[] = {20, 36, 72, 144, 288, 0x7FFFFFFF};
+    const int l[] = {4, 4, 8, 16, 32, 32};
+    const int c[] = {5, 9, 9, 9, 9, 9};
+    t.n = 6;
+    for (int k = 0; k < t.n; ++k) {
+        t.width[k] = w[k]; t.lanes[k] = l[k]; t.tile[k] = c[k]; t.warp_batch[k] = 0;
+    }
+}
+
+// Largest query a class stages: its width, except for the unbounded last class.
+static int class_qcap(const TileTable& t, int k, int qmax) {
+    return k == t.n - 1 ? qmax : std::min(qmax, t.width[k]);
+}
+
+// Runs the persistent row-parallel kernel over every width class of an ordered batch: one
+// launch per class on its own stream, forked from and joined back into `st`.
+static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParams& sp, cudaStream_t st,
+                          int only = -1, const TileTable* tt_override = nullptr) {
+    const TileTable& tt = tt_override ? *tt_override : ctx->tiles;
+    if (cudaEventRecord(ctx->fork, st) != cudaSuccess) return G3X_ERR_CUDA;
+    int rc = G3X_OK;
+    for (int k = 0; k < tt.n && rc == G3X_OK; ++k) {
+        if (only >= 0 && k != only) continue;
+        if (cudaStreamWaitEvent(ctx->side[k], ctx->fork, 0) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
+        LaunchDesc d = base;
+        d.kernel = kKernelRowpar;
+        d.lanes = tt.lanes[k];
+        d.tile = tt.tile[k];
+        d.warp_batch = tt.warp_batch[k];
+        d.persistent = 1;
+        d.warps_per_block = 4;
+        d.qmax = class_qcap(tt, k, base.qmax);
+        d.order = ctx->sched.order;
+        d.order_off = ctx->sched.bucket_oc + 2 * k;
+        d.count = ctx->sched.bucket_oc + 2 * k + 1;
+        d.queue = ctx->d_queue + k;
+        d.stats = ctx->d_stats;
+        while (d.lanes < 32 && (32 / d.lanes) * group_smem_bytes(d.qmax, d.tmax) > 227 * 1024) d.lanes *= 2;
+        rc = launch_rowpar(d, sp, ctx->side[k]);
+        if (rc == G3X_OK && cudaEventRecord(ctx->join[k], ctx->side[k]) != cudaSuccess) rc = G3X_ERR_CUDA;
+        if (rc == G3X_OK && cudaStreamWaitEvent(st, ctx->join[k], 0) != cudaSuccess) rc = G3X_ERR_CUDA;
+    }
+    return rc;
+}
+
+// Schedules and runs a persistent batch: cost per job (length, or the model's prediction),
+// counting sort into width classes, one launch per class.
+static int run_scheduled(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParams& sp, bool learned,
+                         cudaStream_t st) {
+    int rc = alloc_sched(ctx->sched, base.n);
+    if (rc) return rc;
+    const float* pred = nullptr;
+    if (learned) {
+        if (!ctx->model.params || !ctx->model.trained) return G3X_ERR_NOT_TRAINED;
+        if ((rc = model_features(base.jobs, base.n, base.codes, base.nmask, ctx->sched.feat, st))) return rc;
+        if ((rc = model_predict(ctx->model.params, ctx->sched.feat, base.n, ctx->sched.pred, st))) return rc;
+        pred = ctx->sched.pred;
+    }
+    if ((rc = schedule_jobs(ctx->sched, base.jobs, base.n, sp, pred, ctx->tiles, st))) return rc;
+    if (cudaMemsetAsync(ctx->d_queue, 0, kMaxBuckets * sizeof(int32_t), st) != cudaSuccess ||
+        cudaMemsetAsync(ctx->d_stats, 0, 4 * sizeof(unsigned long long), st) != cudaSuccess)
+        return G3X_ERR_CUDA;
+    return launch_classes(ctx, base, sp, st);
 }
 
 }  // namespace g3x
@@ -116,10 +225,18 @@ int g3x_ctx_create(g3x_ctx** out, int device) {
     memset(&c->seeds, 0, sizeof(c->seeds));
     c->device = device;
     cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
-    if (cudaMalloc(&c->d_queue, 64 * sizeof(int32_t)) != cudaSuccess) {
+    g3x::default_tiles(c->tiles);
+    bool ok = cudaMalloc(&c->d_queue, 64 * sizeof(int32_t)) == cudaSuccess &&
+              cudaMalloc(&c->d_stats, 4 * sizeof(unsigned long long)) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < g3x::kMaxBuckets && ok; ++k)
+        ok = cudaStreamCreateWithFlags(&c->side[k], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
         delete c;
         return G3X_ERR_NOMEM;
     }
+    cudaMemset(c->d_stats, 0, 4 * sizeof(unsigned long long));
     *out = c;
     return G3X_OK;
 }
@@ -127,7 +244,16 @@ int g3x_ctx_create(g3x_ctx** out, int device) {
 int g3x_ctx_destroy(g3x_ctx* c) {
     if (!c) return G3X_ERR_INVALID;
     cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
     g3x::free_seed_scratch(c->seeds);
+    g3x::model_free(c->model);
+    g3x::free_sched(c->sched);
+    for (int k = 0; k < g3x::kMaxBuckets; ++k) {
+        cudaStreamDestroy(c->side[k]);
+        cudaEventDestroy(c->join[k]);
+    }
+    cudaEventDestroy(c->fork);
+    cudaFree(c->d_stats);
     cudaFree(c->d_queue);
     delete c;
     return G3X_OK;
@@ -149,9 +275,124 @@ int g3x_ksw_extend2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_
     cudaStream_t st = (cudaStream_t)stream;
     d.jobs = d_jobs; d.codes = d_codes; d.nmask = d_nmask; d.out = d_out; d.status = d_status;
     d.n = n;
-    if (d.persistent && cudaMemsetAsync(ctx->d_queue, 0, sizeof(int32_t), st) != cudaSuccess)
-        return G3X_ERR_CUDA;
+    // Persistent row-parallel batches without a fixed group size go through the scheduler.
+    if (d.persistent && d.kernel == g3x::kKernelRowpar && opts->lanes == 0 && opts->tile == 0)
+        return g3x::run_scheduled(ctx, d, sp, opts->schedule == G3X_SCHED_LEARNED, st);
+    if (opts->schedule == G3X_SCHED_LEARNED) return G3X_ERR_INVALID;   // needs the scheduler
+    if (d.persistent) {
+        d.stats = ctx->d_stats;
+        if (cudaMemsetAsync(ctx->d_queue, 0, sizeof(int32_t), st) != cudaSuccess ||
+            cudaMemsetAsync(ctx->d_stats, 0, 4 * sizeof(unsigned long long), st) != cudaSuccess)
+            return G3X_ERR_CUDA;
+    }
     return g3x::launch_extend(d, sp, st);
+}
+
+int g3x_get_tiles(g3x_ctx* ctx, g3x_tile_t* h, int32_t* n) {
+    if (!ctx || !h || !n) return G3X_ERR_INVALID;
+    for (int k = 0; k < ctx->tiles.n; ++k)
+        h[k] = g3x_tile_t{ctx->tiles.width[k], ctx->tiles.lanes[k], ctx->tiles.tile[k], ctx->tiles.warp_batch[k]};
+    *n = ctx->tiles.n;
+    return G3X_OK;
+}
+
+int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
+    if (!ctx || !h || n < 1 || n > G3X_MAX_CLASSES) return G3X_ERR_INVALID;
+    for (int k = 0; k < n; ++k) {
+        const g3x_tile_t& t = h[k];
+        if ((t.lanes != 4 && t.lanes != 8 && t.lanes != 16 && t.lanes != 32) ||
+            (t.tile != 5 && t.tile != 9 && t.tile != 13) || t.width < 1 ||
+            (k && t.width <= h[k - 1].width) || (t.warp_batch != 0 && t.warp_batch != 1))
+            return G3X_ERR_INVALID;
+    }
+    ctx->tiles.n = n;
+    for (int k = 0; k < n; ++k) {
+        ctx->tiles.width[k] = k == n - 1 ? 0x7FFFFFFF : h[k].width;
+        ctx->tiles.lanes[k] = h[k].lanes;
+        ctx->tiles.tile[k] = h[k].tile;
+        ctx->tiles.warp_batch[k] = h[k].warp_batch;
+    }
+    return G3X_OK;
+}
+
+int g3x_last_stats(g3x_ctx* ctx, uint64_t* h) {
+    if (!ctx || !h) return G3X_ERR_INVALID;
+    if (cudaSetDevice(ctx->device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return G3X_ERR_CUDA;
+    unsigned long long v[4];
+    if (cudaMemcpy(v, ctx->d_stats, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return G3X_ERR_CUDA;
+    for (int k = 0; k < 3; ++k) h[k] = v[k];
+    return G3X_OK;
+}
+
+int g3x_autotune(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs, int32_t n,
+                 const uint32_t* d_codes, const uint32_t* d_nmask, int32_t max_qlen,
+                 int32_t max_tlen, g3x_tile_t* h_tiles, int32_t* n_tiles) {
+    if (!ctx || !d_jobs || !d_codes || !d_nmask || n <= 0) return G3X_ERR_INVALID;
+    g3x::ScoreParams sp;
+    int rc = g3x::score_params(score, &sp);
+    if (rc) return rc;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    if ((rc = g3x::alloc_sched(ctx->sched, n))) return rc;
+    g3x_ext_t* out = nullptr;
+    int32_t* status = nullptr;
+    if (cudaMalloc(&out, (size_t)n * sizeof(g3x_ext_t)) || cudaMalloc(&status, (size_t)n * sizeof(int32_t))) {
+        cudaFree(out);
+        return G3X_ERR_NOMEM;
+    }
+    g3x::LaunchDesc base;
+    memset(&base, 0, sizeof(base));
+    base.jobs = d_jobs; base.codes = d_codes; base.nmask = d_nmask; base.out = out; base.status = status;
+    base.n = n; base.qmax = max_qlen; base.tmax = max_tlen;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    rc = g3x::schedule_jobs(ctx->sched, d_jobs, n, sp, nullptr, ctx->tiles, st);
+    int32_t oc[2 * g3x::kMaxBuckets];
+    if (rc == G3X_OK && cudaMemcpy(oc, ctx->sched.bucket_oc, sizeof(oc), cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = G3X_ERR_CUDA;
+    const int cand_l[] = {4, 4, 4, 8, 8, 8, 16, 16, 16, 32, 32, 32};
+    const int cand_c[] = {5, 9, 13, 5, 9, 13, 5, 9, 13, 5, 9, 13};
+    g3x::TileTable best = ctx->tiles;
+    for (int k = 0; k < ctx->tiles.n && rc == G3X_OK; ++k) {
+        if (oc[2 * k + 1] == 0) continue;
+        float best_ms = 1e30f;
+        for (int cnd = 0; cnd < 12 && rc == G3X_OK; ++cnd) {
+            const int S = cand_l[cnd] * cand_c[cnd];
+            const int lo = k ? ctx->tiles.width[k - 1] : 0;
+            // candidates: single-tile ones no wider than 2x the class, plus the current one
+            if (!(S >= std::min(ctx->tiles.width[k], 4096) && S <= 2 * std::max(ctx->tiles.width[k], lo + 1)) &&
+                !(cand_l[cnd] == ctx->tiles.lanes[k] && cand_c[cnd] == ctx->tiles.tile[k]) &&
+                !(k == ctx->tiles.n - 1 && cand_l[cnd] == 32))
+                continue;
+            for (int wb = 0; wb < 2 && rc == G3X_OK; ++wb) {
+                g3x::TileTable tt = ctx->tiles;
+                tt.lanes[k] = cand_l[cnd]; tt.tile[k] = cand_c[cnd]; tt.warp_batch[k] = wb;
+                float ms = 0;
+                for (int rep = 0; rep < 2 && rc == G3X_OK; ++rep) {
+                    cudaMemsetAsync(ctx->d_queue, 0, g3x::kMaxBuckets * sizeof(int32_t), st);
+                    cudaEventRecord(e0, st);
+                    rc = g3x::launch_classes(ctx, base, sp, st, k, &tt);
+                    cudaEventRecord(e1, st);
+                    if (cudaEventSynchronize(e1) != cudaSuccess) rc = G3X_ERR_CUDA;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                }
+                if (rc == G3X_OK && ms < best_ms) {
+                    best_ms = ms;
+                    best.lanes[k] = cand_l[cnd]; best.tile[k] = cand_c[cnd]; best.warp_batch[k] = wb;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    cudaFree(status);
+    if (rc == G3X_OK) {
+        ctx->tiles = best;
+        if (h_tiles && n_tiles) rc = g3x_get_tiles(ctx, h_tiles, n_tiles);
+    }
+    return rc;
 }
 
 int g3x_extend_seeds(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_seed_t* d_seeds, int32_t n,
@@ -189,6 +430,71 @@ int g3x_extend_seeds_stream(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_seed_t
     if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
     return g3x::extend_seeds_stream(ctx->seeds, g3x::alloc_seed_scratch, *opt, sp, h_seeds, n,
                                     h_codes, h_nmask, n_bases, h_regs, h_status, chunk, proto);
+}
+
+int g3x_features(g3x_ctx* ctx, const g3x_job_t* d_jobs, int32_t n, const uint32_t* d_codes,
+                 const uint32_t* d_nmask, float* d_feat, void* stream) {
+    if (!ctx || n < 0 || (n && (!d_jobs || !d_codes || !d_nmask || !d_feat))) return G3X_ERR_INVALID;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    return g3x::model_features(d_jobs, n, d_codes, d_nmask, d_feat, (cudaStream_t)stream);
+}
+
+int g3x_mlp_init(g3x_ctx* ctx, uint64_t seed) {
+    if (!ctx) return G3X_ERR_INVALID;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    return g3x::model_init(ctx->model, seed);
+}
+
+int g3x_mlp_train(g3x_ctx* ctx, const float* d_feat, const float* d_target, int32_t n,
+                  int32_t epochs, int32_t batch, float lr, uint64_t seed, float* h_epoch_loss) {
+    if (!ctx || !d_feat || !d_target || n <= 0 || epochs < 0 || batch <= 0 || batch > n) return G3X_ERR_INVALID;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    if (!ctx->model.params) {
+        int rc = g3x::model_init(ctx->model, seed);
+        if (rc) return rc;
+    }
+    int rc = g3x::model_train(ctx->model, d_feat, d_target, n, epochs, batch, lr, seed, h_epoch_loss, 0);
+    if (rc == G3X_OK && cudaDeviceSynchronize() != cudaSuccess) rc = G3X_ERR_CUDA;
+    if (rc == G3X_OK) ctx->model.trained = 1;
+    return rc;
+}
+
+int g3x_mlp_gradient(g3x_ctx* ctx, const float* d_feat, const float* d_target, int32_t n,
+                     float* h_grad, float* h_loss) {
+    if (!ctx || !d_feat || !d_target || n <= 0 || !h_grad) return G3X_ERR_INVALID;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    if (!ctx->model.params) return G3X_ERR_NOT_TRAINED;
+    return g3x::model_gradient(ctx->model, d_feat, d_target, n, h_grad, h_loss, 0);
+}
+
+int g3x_mlp_predict(g3x_ctx* ctx, const float* d_feat, int32_t n, float* d_pred, void* stream) {
+    if (!ctx || n < 0 || (n && (!d_feat || !d_pred))) return G3X_ERR_INVALID;
+    if (!ctx->model.params) return G3X_ERR_NOT_TRAINED;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    return g3x::model_predict(ctx->model.params, d_feat, n, d_pred, (cudaStream_t)stream);
+}
+
+int g3x_mlp_get_params(g3x_ctx* ctx, float* h_params) {
+    if (!ctx || !h_params) return G3X_ERR_INVALID;
+    if (!ctx->model.params) return G3X_ERR_NOT_TRAINED;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    return cudaMemcpy(h_params, ctx->model.params, G3X_MLP_PARAMS * sizeof(float),
+                      cudaMemcpyDeviceToHost) == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
+
+int g3x_mlp_set_params(g3x_ctx* ctx, const float* h_params) {
+    if (!ctx || !h_params) return G3X_ERR_INVALID;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    int rc = g3x::model_alloc(ctx->model, 256);
+    if (rc) return rc;
+    if (cudaMemcpy(ctx->model.params, h_params, G3X_MLP_PARAMS * sizeof(float),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+        return G3X_ERR_CUDA;
+    cudaMemset(ctx->model.m, 0, G3X_MLP_PARAMS * sizeof(float));
+    cudaMemset(ctx->model.v, 0, G3X_MLP_PARAMS * sizeof(float));
+    ctx->model.t = 0;
+    ctx->model.trained = 1;
+    return G3X_OK;
 }
 
 int g3x_int_peak(g3x_ctx* ctx, double* ops_per_s) {

@@ -11,6 +11,7 @@ struct ScoreParams {
     int8_t mat[25];
     int8_t pad_[3];
     int32_t o_del, e_del, o_ins, e_ins, zdrop, end_bonus, max_sc;
+    int32_t oe_del, oe_ins;   // o + e
 };
 
 // One launch of the extension kernel family.
@@ -24,15 +25,47 @@ struct LaunchDesc {
     const int32_t* order;  // optional permutation: queue slot -> job index
     const int32_t* count;  // optional device-side job count (overrides n when set)
     int32_t* queue;        // persistent kernels: device counter (zeroed by the caller)
+    const int32_t* order_off;  // optional device offset added to `order` (bucket start)
+    unsigned long long* stats; // optional: [0] group-rows computed, [1] group-rows idle
+                               // (warp-batched pulling), [2] warp batches
     int32_t n;
     int32_t qmax, tmax;    // smem sizing bounds
-    int32_t lanes;         // 8, 16 or 32
+    int32_t kernel;        // kKernelRolling or kKernelRowpar
+    int32_t lanes;         // lanes per job
+    int32_t tile;          // row-parallel kernel: cells per lane per tile
     int32_t persistent;    // 0: one group per job slot; 1: groups pull from `queue`
     int32_t warps_per_block;
     int32_t blocks;        // persistent grid size (0 = derive from occupancy)
+    int32_t warp_batch;    // persistent row-parallel: 1 = a warp pulls one job per group at
+                           // once and waits for all of them; 0 = each group refills alone
 };
 
+// Tile configurations by job width class (ascending width; the last class is unbounded).
+constexpr int kMaxBuckets = 8;
+struct TileTable {
+    int32_t n;
+    int32_t width[kMaxBuckets];   // widest row this class holds
+    int32_t lanes[kMaxBuckets];
+    int32_t tile[kMaxBuckets];
+    int32_t warp_batch[kMaxBuckets];
+};
+
+// Device scratch of the scheduler and of the learned schedule (capacity >= n jobs).
+struct SchedScratch {
+    int32_t *bin = nullptr, *order = nullptr, *hist = nullptr, *cursor = nullptr;
+    int32_t* bucket_oc = nullptr;  // [offset, count] per bucket
+    float *feat = nullptr, *pred = nullptr;
+    int64_t cap = 0;
+};
+int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScoreParams& sp,
+                  const float* pred, const TileTable& tt, cudaStream_t st);
+
+constexpr int32_t kKernelRolling = 1;   // anti-diagonal wavefront, rows on lanes
+constexpr int32_t kKernelRowpar = 2;    // one row per step, columns on lanes
+
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+int launch_rolling(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+int launch_rowpar(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 
 // Device scratch of one seed-level call (capacity >= n seeds).
 struct SeedScratch {
@@ -53,6 +86,27 @@ int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), con
                         g3x_reg_t* h_regs, int32_t* h_status, int32_t chunk,
                         const LaunchDesc& proto);
 int score_params(const g3x_score_t* s, ScoreParams* sp);
+
+// Learned cost model state (device buffers; g3x_model.cu).
+struct ModelState {
+    float *params = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
+    float *h1 = nullptr, *h2 = nullptr, *dh1 = nullptr, *dh2 = nullptr, *dy = nullptr;
+    float* loss_part = nullptr;
+    int* perm = nullptr;
+    int batch_cap = 0, perm_cap = 0;
+    long long t = 0;       // Adam step
+    int trained = 0;       // parameters set by training or by the caller
+};
+int model_alloc(ModelState& M, int batch);
+void model_free(ModelState& M);
+int model_init(ModelState& M, uint64_t seed);
+int model_features(const g3x_job_t* jobs, int n, const uint32_t* codes, const uint32_t* nmask,
+                   float* feat, cudaStream_t st);
+int model_predict(const float* params, const float* feat, int n, float* out, cudaStream_t st);
+int model_gradient(ModelState& M, const float* X, const float* T, int B, float* h_grad,
+                   float* h_loss, cudaStream_t st);
+int model_train(ModelState& M, const float* X, const float* T, int n, int epochs, int batch,
+                float lr, uint64_t seed, float* h_epoch_loss, cudaStream_t st);
 int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d);
 size_t group_smem_bytes(int qmax, int tmax);
 int measure_int_peak(int device, double* ops_per_s);

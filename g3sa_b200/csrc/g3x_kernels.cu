@@ -1,117 +1,24 @@
 // g3x_kernels.cu -- sm_100a kernels for batched ksw_extend2 (bwa/src/ksw.cu:303-401).
 //
-// A job is run by a group of G lanes (G = 8, 16 or 32) that sweeps anti-diagonals of the
+// Rolling anti-diagonal family.  A job is run by a group of G lanes (G = 8, 16 or 32) that
+// sweeps anti-diagonals of the
 // banded DP with the rolling-row protocol of g3x_core.h.  A warp holds 32/G groups and runs
 // ONE step loop for all of them: every iteration each group with a job advances one step,
 // and a group whose job finished stages its next job in the same iteration.  All warp
 // collectives (progress shuffles, the row-end ballot, the commit broadcast) use the full
 // warp with per-lane source lanes, so groups never split the warp's instruction stream
 // except while one of them stages a job.
-//
-// Per group, shared memory holds the job's working set:
-//   eh   : the reference's H/E row buffer (ksw.cu:310), int32 pairs
-//   qp   : the query profile, 5 rows of qstride int8 scores (ksw.cu:309, 312-315)
-//   tgt  : the target codes, one nibble per base (0-3, >= 4 means N)
+// The per-job shared-memory working set and its staging are in g3x_stage.cuh.
 #include <cuda_runtime.h>
 #include "g3x_core.h"
 #include "g3x_internal.h"
+#include "g3x_stage.cuh"
 
 namespace g3x {
 
-struct EhSlot32 {
-    int32_t h, e;
-};
-
-// The row buffer as lane_step sees it: one aligned block of four slots is read with two
-// 16-byte shared loads; each computed cell is written back with one 8-byte store.
-struct SmemEh {
-    EhSlot32* p;
-    __device__ __forceinline__ void load4(int jb, EhCell v[4]) const {
-        const int4 a = *reinterpret_cast<const int4*>(p + jb);
-        const int4 b = *reinterpret_cast<const int4*>(p + jb + 2);
-        v[0] = EhCell{a.x, a.y}; v[1] = EhCell{a.z, a.w};
-        v[2] = EhCell{b.x, b.y}; v[3] = EhCell{b.z, b.w};
-    }
-    __device__ __forceinline__ void store(int c, int32_t h, int32_t e) {
-        *reinterpret_cast<int2*>(p + c) = make_int2(h, e);
-    }
-    __device__ __forceinline__ void note_read(int) const {}
-};
-
-// Target codes, 16 nibbles per 64-bit word.
-struct SmemTgt {
-    const uint64_t* p;
-    __device__ __forceinline__ int32_t code(int32_t i) const {
-        const uint32_t nib = (uint32_t)(p[i >> 4] >> ((i & 15) << 2)) & 15u;
-        return nib < 4u ? (int32_t)nib : 4;
-    }
-};
-
-__host__ __device__ constexpr int align16(int x) { return (x + 15) & ~15; }
-
-// Slots: every block read (jb <= qmax-1, 4 slots), every 2-slot init store and the end write
-// at qlen stay inside.
-__host__ __device__ inline int eh_slots(int qmax) { return (qmax + 8) & ~3; }
-// Query-profile row stride: 16-byte aligned rows; a 4-byte read at any block start
-// jb <= qmax-1 and a 16-byte staging store at any 16-base chunk stay in the row.
-__host__ __device__ inline int qstride_of(int qmax) { return (qmax + 16) & ~15; }
-__host__ __device__ inline int tgt_bytes(int tmax) { return ((tmax + 15) >> 4) * 8 + 8; }
-
-__host__ __device__ inline size_t group_bytes(int qmax, int tmax) {
-    return (size_t)align16(eh_slots(qmax) * (int)sizeof(EhSlot32)) +
-           (size_t)align16(5 * qstride_of(qmax)) + (size_t)align16(tgt_bytes(tmax));
-}
-
 size_t group_smem_bytes(int qmax, int tmax) { return group_bytes(qmax, tmax); }
 
-// 16 bases of a sequence (bases 16*ch .. 16*ch+15, in the job's reading direction) as 16
-// 2-bit fields (x) and 16 N bits (nb).  Only plane words that hold valid bases are read.
-__device__ __forceinline__ void load16(const uint32_t* __restrict__ codes,
-                                       const uint32_t* __restrict__ nmask, uint32_t off,
-                                       int len, int ch, bool rev, uint32_t& x, uint32_t& nb) {
-    const int k0 = ch << 4;
-    const int nv = len - k0 < 16 ? len - k0 : 16;
-    if (!rev) {
-        const uint32_t p0 = off + (uint32_t)k0;
-        const uint32_t w = p0 >> 4, sh = p0 & 15u;
-        uint64_t v = __ldg(codes + w);
-        if (sh + (uint32_t)nv > 16u) v |= (uint64_t)__ldg(codes + w + 1) << 32;
-        x = (uint32_t)(v >> (sh << 1));
-        const uint32_t nw = p0 >> 5, nsh = p0 & 31u;
-        uint64_t m = __ldg(nmask + nw);
-        if (nsh + (uint32_t)nv > 32u) m |= (uint64_t)__ldg(nmask + nw + 1) << 32;
-        nb = (uint32_t)(m >> nsh) & 0xFFFFu;
-    } else {
-        const uint32_t ph = off + (uint32_t)(len - 1 - k0);   // plane position of base k0
-        const uint32_t w = ph >> 4, sh = ph & 15u;
-        uint64_t v = (uint64_t)__ldg(codes + w) << 32;
-        if ((uint32_t)nv > sh + 1u) v |= __ldg(codes + w - 1);
-        uint32_t y = (uint32_t)(v >> ((sh << 1) + 2));        // field 15 = position ph
-        y = __brev(y);                                          // field order reversed...
-        x = ((y >> 1) & 0x55555555u) | ((y & 0x55555555u) << 1);  // ...and each field's bits
-        const uint32_t nw = ph >> 5, nsh = ph & 31u;
-        uint64_t m = (uint64_t)__ldg(nmask + nw) << 32;
-        if ((uint32_t)nv > nsh + 1u) m |= __ldg(nmask + nw - 1);
-        nb = __brev((uint32_t)(m >> (nsh + 17)) & 0xFFFFu) >> 16;
-    }
-}
-
-// 16 codes as 16 nibbles: the 2-bit code in bits 0-1, the N flag in bit 2.
-__device__ __forceinline__ uint64_t nibbles16(uint32_t x, uint32_t nb) {
-    uint64_t t = x;
-    t = (t | (t << 16)) & 0x0000FFFF0000FFFFull;
-    t = (t | (t << 8)) & 0x00FF00FF00FF00FFull;
-    t = (t | (t << 4)) & 0x0F0F0F0F0F0F0F0Full;
-    t = (t | (t << 2)) & 0x3333333333333333ull;
-    uint64_t n = nb;
-    n = (n | (n << 24)) & 0x000000FF000000FFull;
-    n = (n | (n << 12)) & 0x000F000F000F000Full;
-    n = (n | (n << 6)) & 0x0303030303030303ull;
-    n = (n | (n << 3)) & 0x1111111111111111ull;
-    return t | (n << 2);
-}
-
-// Per-group job state, identical in every lane of the group.
+// Per-group job state of the rolling kernel, identical in every lane of the group.
 struct GroupJob {
     int job;          // job index, -1 = none
     int narrow;
@@ -119,71 +26,6 @@ struct GroupJob {
     Commit K;
     long long steps, limit;
 };
-
-// Stages job `job` into the group's shared memory.  Returns false (after writing the job's
-// status) when the job is rejected.
-template <int G>
-__device__ bool stage_job(int job, const LaunchDesc& d, const ScoreParams& sp,
-                          const uint32_t (&prof_lo)[5], const uint32_t (&prof_hi)[5],
-                          EhSlot32* eh, int8_t* qp, uint64_t* tgt, int qs, int r,
-                          GroupJob& gj) {
-    const g3x_job_t jb = d.jobs[job];
-    const int qlen = jb.qlen, tlen = jb.tlen;
-    if (qlen > d.qmax || tlen > d.tmax || qlen > 65534) {
-        if (r == 0) {
-            d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
-            d.status[job] = G3X_ERR_TOO_LONG;
-            if (d.cells) d.cells[job] = 0;
-        }
-        return false;
-    }
-    JobConst& c = gj.c;
-    c.qlen = qlen; c.tlen = tlen; c.h0 = jb.h0;
-    c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
-    c.oe_del = sp.o_del + sp.e_del; c.oe_ins = sp.o_ins + sp.e_ins; c.zdrop = sp.zdrop;
-    c.w = clamp_w(jb.w, qlen, sp.max_sc, sp.end_bonus, sp.o_del, sp.e_del, sp.o_ins, sp.e_ins);
-    const bool qrev = (jb.flags & G3X_JOB_QREV) != 0, trev = (jb.flags & G3X_JOB_TREV) != 0;
-    // query profile, 16 bases per lane-iteration: one byte permute per 4 scores
-    for (int ch = r; (ch << 4) < qlen; ch += G) {
-        uint32_t x, nb;
-        load16(d.codes, d.nmask, jb.q_off, qlen, ch, qrev, x, nb);
-        const uint64_t sel = nibbles16(x, nb);
-        const uint32_t s0 = (uint32_t)sel, s1 = (uint32_t)(sel >> 16), s2 = (uint32_t)(sel >> 32),
-                       s3 = (uint32_t)(sel >> 48);
-#pragma unroll
-        for (int a = 0; a < 5; ++a) {
-            uint4 v;
-            v.x = __byte_perm(prof_lo[a], prof_hi[a], s0);
-            v.y = __byte_perm(prof_lo[a], prof_hi[a], s1);
-            v.z = __byte_perm(prof_lo[a], prof_hi[a], s2);
-            v.w = __byte_perm(prof_lo[a], prof_hi[a], s3);
-            *reinterpret_cast<uint4*>(qp + a * qs + (ch << 4)) = v;
-        }
-    }
-    for (int ch = r; (ch << 4) < tlen; ch += G) {
-        uint32_t x, nb;
-        load16(d.codes, d.nmask, jb.t_off, tlen, ch, trev, x, nb);
-        tgt[ch] = nibbles16(x, nb);
-    }
-    const int nslots = eh_slots(qlen);
-    for (int k = r << 1; k < nslots; k += G << 1) {
-        int4 v;
-        v.x = k <= qlen + 1 ? init_h(k, c) : 0;
-        v.y = 0;
-        v.z = k + 1 <= qlen + 1 ? init_h(k + 1, c) : 0;
-        v.w = 0;
-        *reinterpret_cast<int4*>(eh + k) = v;
-    }
-    gj.narrow = job_is_narrow(c, sp.max_sc);
-    commit_init(gj.K, c);
-    gj.steps = 0;
-    // Every step either advances a row or moves a lane between states; the oldest
-    // unfinished row always advances, so this bound is never reached by a correct run.  It
-    // turns a logic error into a per-job status instead of a hang.
-    gj.limit = 8LL * ((long long)tlen + 2) * ((long long)qlen + 8) + 4096;
-    gj.job = job;
-    return true;
-}
 
 template <int G>
 __global__ void __launch_bounds__(256) extend_kernel(LaunchDesc d, ScoreParams sp) {
@@ -202,14 +44,8 @@ __global__ void __launch_bounds__(256) extend_kernel(LaunchDesc d, ScoreParams s
     const int n = d.count ? *d.count : d.n;
     const int pred = gbase + ((r + G - 1) & (G - 1));
 
-    // score rows as byte-permute pools: bytes 0-3 = codes 0-3, bytes 4-7 = N
     uint32_t prof_lo[5], prof_hi[5];
-#pragma unroll
-    for (int a = 0; a < 5; ++a) {
-        prof_lo[a] = (uint32_t)(uint8_t)sp.mat[a * 5 + 0] | ((uint32_t)(uint8_t)sp.mat[a * 5 + 1] << 8) |
-                     ((uint32_t)(uint8_t)sp.mat[a * 5 + 2] << 16) | ((uint32_t)(uint8_t)sp.mat[a * 5 + 3] << 24);
-        prof_hi[a] = (uint32_t)(uint8_t)sp.mat[a * 5 + 4] * 0x01010101u;
-    }
+    score_pools(sp, prof_lo, prof_hi);
 
     GroupJob gj;
     gj.job = -1;
@@ -236,7 +72,15 @@ __global__ void __launch_bounds__(256) extend_kernel(LaunchDesc d, ScoreParams s
                 }
                 if (slot >= n) { exhausted = true; break; }
                 const int job = d.order ? d.order[slot] : slot;
-                if (stage_job<G>(job, d, sp, prof_lo, prof_hi, eh, qp, tgt, qs, r, gj)) {
+                StagedJob sj;
+                if (stage_job<G>(job, d, sp, prof_lo, prof_hi, eh, qp, tgt, qs, r, sj)) {
+                    gj.job = job; gj.narrow = sj.narrow; gj.c = sj.c;
+                    commit_init(gj.K, gj.c);
+                    gj.steps = 0;
+                    // Every step either advances a row or moves a lane between states; the
+                    // oldest unfinished row always advances, so this bound is never reached
+                    // by a correct run.  It turns a logic error into a per-job status.
+                    gj.limit = 8LL * ((long long)gj.c.tlen + 2) * ((long long)gj.c.qlen + 8) + 4096;
                     lane_init(L, r, gj.c.tlen);
                     err = G3X_OK;
                     break;
@@ -317,13 +161,17 @@ static int launch_g(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t str
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }
 
-int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
+int launch_rolling(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
     switch (d.lanes) {
         case 8: return launch_g<8>(d, sp, stream);
         case 16: return launch_g<16>(d, sp, stream);
         case 32: return launch_g<32>(d, sp, stream);
         default: return G3X_ERR_INVALID;
     }
+}
+
+int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
+    return d.kernel == kKernelRowpar ? launch_rowpar(d, sp, stream) : launch_rolling(d, sp, stream);
 }
 
 }  // namespace g3x

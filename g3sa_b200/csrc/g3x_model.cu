@@ -1,0 +1,387 @@
+// g3x_model.cu -- learned per-job cost model: features, an MLP 5 -> 64 -> 64 -> 1 (ReLU,
+// fp32, 4,609 parameters), and its forward, backward and Adam kernels.
+//
+// The model predicts a job's work (the caller trains it on log2(1 + DP cells) measured by
+// the extension kernel's own cell counters) from five features of the job header and its
+// sequences.  The scheduler orders and buckets jobs by the prediction; scores never depend
+// on it.
+//
+// Parameter layout (floats): W1[64][5] | b1[64] | W2[64][64] | b2[64] | W3[64] | b3.
+// Training works on one mini-batch at a time as a sequence of small kernels; every gradient
+// is a fixed-order sum over the batch (no atomics), so training is deterministic.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "g3x_internal.h"
+#include "g3x_stage.cuh"
+
+namespace g3x {
+
+constexpr int kF = 5, kH = 64;
+constexpr int oW1 = 0, ob1 = oW1 + kH * kF, oW2 = ob1 + kH, ob2 = oW2 + kH * kH, oW3 = ob2 + kH,
+              ob3 = oW3 + kH, kParams = ob3 + 1;
+static_assert(kParams == G3X_MLP_PARAMS, "parameter count");
+
+// ---- features ---------------------------------------------------------------------------
+
+// Per job: qlen/128, tlen/256, h0/64, GC fraction of the query, and the mismatch fraction of
+// the first min(32, qlen, tlen) bases of query and target next to the seed (N counts as a
+// mismatch).  One thread per job.
+__global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
+                                const uint32_t* __restrict__ codes,
+                                const uint32_t* __restrict__ nmask, float* __restrict__ feat) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const g3x_job_t jb = jobs[k];
+    const bool qrev = (jb.flags & G3X_JOB_QREV) != 0, trev = (jb.flags & G3X_JOB_TREV) != 0;
+    int gc = 0, nq = 0;
+    for (int ch = 0; (ch << 4) < jb.qlen; ++ch) {
+        uint32_t x, nb;
+        load16(codes, nmask, jb.q_off, jb.qlen, ch, qrev, x, nb);
+        const int nv = jb.qlen - (ch << 4) < 16 ? jb.qlen - (ch << 4) : 16;
+        const uint32_t valid = nv == 16 ? 0xFFFFu : ((1u << nv) - 1u);
+        // code 1 (C) or 2 (G): the two bits of the field differ
+        const uint32_t diff = (x ^ (x >> 1)) & 0x55555555u;
+        uint32_t gcm = 0;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) gcm |= ((diff >> (2 * t)) & 1u) << t;
+        gc += __popc(gcm & ~nb & valid);
+        nq += __popc(~nb & valid);
+    }
+    const int k0 = jb.qlen < jb.tlen ? jb.qlen : jb.tlen;
+    const int kk = k0 < 32 ? k0 : 32;
+    int mism = 0;
+    for (int ch = 0; (ch << 4) < kk; ++ch) {
+        uint32_t xq, nq2, xt, nt;
+        load16(codes, nmask, jb.q_off, jb.qlen, ch, qrev, xq, nq2);
+        load16(codes, nmask, jb.t_off, jb.tlen, ch, trev, xt, nt);
+        const int nv = kk - (ch << 4) < 16 ? kk - (ch << 4) : 16;
+        const uint32_t valid = nv == 16 ? 0xFFFFu : ((1u << nv) - 1u);
+        const uint32_t d2 = xq ^ xt;
+        const uint32_t dd = (d2 | (d2 >> 1)) & 0x55555555u;
+        uint32_t mm = 0;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) mm |= ((dd >> (2 * t)) & 1u) << t;
+        mism += __popc((mm | nq2 | nt) & valid);
+    }
+    float* f = feat + (size_t)k * kF;
+    f[0] = jb.qlen * (1.0f / 128.0f);
+    f[1] = jb.tlen * (1.0f / 256.0f);
+    f[2] = jb.h0 * (1.0f / 64.0f);
+    f[3] = nq ? (float)gc / (float)nq : 0.0f;
+    f[4] = kk ? (float)mism / (float)kk : 0.0f;
+}
+
+// ---- inference ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) predict_kernel(const float* __restrict__ params,
+                                                      const float* __restrict__ feat, int n,
+                                                      float* __restrict__ out) {
+    __shared__ float w[kParams];
+    for (int t = threadIdx.x; t < kParams; t += blockDim.x) w[t] = params[t];
+    __syncthreads();
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    float x[kF];
+#pragma unroll
+    for (int f = 0; f < kF; ++f) x[f] = feat[(size_t)k * kF + f];
+    float h1[kH];
+#pragma unroll
+    for (int u = 0; u < kH; ++u) {
+        float a = w[ob1 + u];
+#pragma unroll
+        for (int f = 0; f < kF; ++f) a = fmaf(w[oW1 + u * kF + f], x[f], a);
+        h1[u] = fmaxf(a, 0.0f);
+    }
+    float y = w[ob3];
+    for (int u = 0; u < kH; ++u) {
+        float a = w[ob2 + u];
+#pragma unroll
+        for (int q = 0; q < kH; ++q) a = fmaf(w[oW2 + u * kH + q], h1[q], a);
+        y = fmaf(w[oW3 + u], fmaxf(a, 0.0f), y);
+    }
+    out[k] = y;
+}
+
+// ---- training: forward with saved activations, backward, Adam ----------------------------
+
+// H1[b][u], H2[b][u] for a mini-batch, and dY[b] = 2 (Y - T) / B; loss partials per block.
+__global__ void train_fwd_kernel(const float* __restrict__ p, const float* __restrict__ X,
+                                 const float* __restrict__ T, const int* __restrict__ idx, int B,
+                                 float* __restrict__ H1, float* __restrict__ H2,
+                                 float* __restrict__ dY, float* __restrict__ loss_part) {
+    __shared__ float w[kParams];
+    __shared__ float red[256];
+    for (int t = threadIdx.x; t < kParams; t += blockDim.x) w[t] = p[t];
+    __syncthreads();
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    float sq = 0.0f;
+    if (b < B) {
+        const int s = idx ? idx[b] : b;
+        float x[kF];
+#pragma unroll
+        for (int f = 0; f < kF; ++f) x[f] = X[(size_t)s * kF + f];
+        float h1[kH];
+#pragma unroll
+        for (int u = 0; u < kH; ++u) {
+            float a = w[ob1 + u];
+#pragma unroll
+            for (int f = 0; f < kF; ++f) a = fmaf(w[oW1 + u * kF + f], x[f], a);
+            h1[u] = fmaxf(a, 0.0f);
+            H1[(size_t)b * kH + u] = h1[u];
+        }
+        float y = w[ob3];
+        for (int u = 0; u < kH; ++u) {
+            float a = w[ob2 + u];
+#pragma unroll
+            for (int q = 0; q < kH; ++q) a = fmaf(w[oW2 + u * kH + q], h1[q], a);
+            a = fmaxf(a, 0.0f);
+            H2[(size_t)b * kH + u] = a;
+            y = fmaf(w[oW3 + u], a, y);
+        }
+        const float e = y - T[s];
+        dY[b] = 2.0f * e / (float)B;
+        sq = e * e;
+    }
+    red[threadIdx.x] = sq;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) loss_part[blockIdx.x] = red[0];
+}
+
+// dH2[b][u] = dY[b] * W3[u] * (H2 > 0);  dW3[u] = sum_b dY[b] H2[b][u]; db3 = sum_b dY[b]
+__global__ void train_bwd3_kernel(const float* __restrict__ p, const float* __restrict__ H2,
+                                  const float* __restrict__ dY, int B, float* __restrict__ dH2,
+                                  float* __restrict__ g) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < B * kH) {
+        const int b = t / kH, u = t % kH;
+        dH2[t] = H2[t] > 0.0f ? dY[b] * p[oW3 + u] : 0.0f;
+    }
+    if (blockIdx.x == 0 && threadIdx.x <= kH) {
+        float a = 0.0f;
+        if (threadIdx.x < kH) {
+            for (int b = 0; b < B; ++b) a = fmaf(dY[b], H2[(size_t)b * kH + threadIdx.x], a);
+            g[oW3 + threadIdx.x] = a;
+        } else {
+            for (int b = 0; b < B; ++b) a += dY[b];
+            g[ob3] = a;
+        }
+    }
+}
+
+// dW2[u][q] = sum_b dH2[b][u] H1[b][q];  db2[u] = sum_b dH2[b][u]
+__global__ void train_gw2_kernel(const float* __restrict__ H1, const float* __restrict__ dH2,
+                                 int B, float* __restrict__ g) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < kH * kH) {
+        const int u = t / kH, q = t % kH;
+        float a = 0.0f;
+        for (int b = 0; b < B; ++b) a = fmaf(dH2[(size_t)b * kH + u], H1[(size_t)b * kH + q], a);
+        g[oW2 + t] = a;
+    } else if (t < kH * kH + kH) {
+        const int u = t - kH * kH;
+        float a = 0.0f;
+        for (int b = 0; b < B; ++b) a += dH2[(size_t)b * kH + u];
+        g[ob2 + u] = a;
+    }
+}
+
+// dH1[b][q] = (sum_u dH2[b][u] W2[u][q]) * (H1 > 0)
+__global__ void train_dh1_kernel(const float* __restrict__ p, const float* __restrict__ H1,
+                                 const float* __restrict__ dH2, int B, float* __restrict__ dH1) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= B * kH) return;
+    const int b = t / kH, q = t % kH;
+    float a = 0.0f;
+    for (int u = 0; u < kH; ++u) a = fmaf(dH2[(size_t)b * kH + u], p[oW2 + u * kH + q], a);
+    dH1[t] = H1[t] > 0.0f ? a : 0.0f;
+}
+
+// dW1[u][f] = sum_b dH1[b][u] X[b][f];  db1[u] = sum_b dH1[b][u]
+__global__ void train_gw1_kernel(const float* __restrict__ X, const int* __restrict__ idx,
+                                 const float* __restrict__ dH1, int B, float* __restrict__ g) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < kH * kF) {
+        const int u = t / kF, f = t % kF;
+        float a = 0.0f;
+        for (int b = 0; b < B; ++b) {
+            const int s = idx ? idx[b] : b;
+            a = fmaf(dH1[(size_t)b * kH + u], X[(size_t)s * kF + f], a);
+        }
+        g[oW1 + t] = a;
+    } else if (t < kH * kF + kH) {
+        const int u = t - kH * kF;
+        float a = 0.0f;
+        for (int b = 0; b < B; ++b) a += dH1[(size_t)b * kH + u];
+        g[ob1 + u] = a;
+    }
+}
+
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g,
+                            float* __restrict__ m, float* __restrict__ v, float lr, float b1,
+                            float b2, float eps, float c1, float c2) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= kParams) return;
+    const float gg = g[t];
+    const float mm = b1 * m[t] + (1.0f - b1) * gg;
+    const float vv = b2 * v[t] + (1.0f - b2) * gg * gg;
+    m[t] = mm;
+    v[t] = vv;
+    p[t] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+}
+
+// Fisher-Yates shuffle of 0..n-1 with a splitmix64 stream, on one thread (n <= a few M).
+__global__ void perm_kernel(int* __restrict__ idx, int n, unsigned long long seed) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int k = 0; k < n; ++k) idx[k] = k;
+    unsigned long long s = seed;
+    for (int k = n - 1; k > 0; --k) {
+        unsigned long long z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        const int j = (int)(z % (unsigned long long)(k + 1));
+        const int tmp = idx[k]; idx[k] = idx[j]; idx[j] = tmp;
+    }
+}
+
+// ---- host side ---------------------------------------------------------------------------
+
+int model_features(const g3x_job_t* jobs, int n, const uint32_t* codes, const uint32_t* nmask,
+                   float* feat, cudaStream_t st) {
+    if (n <= 0) return G3X_OK;
+    features_kernel<<<(n + 255) / 256, 256, 0, st>>>(jobs, n, codes, nmask, feat);
+    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
+
+int model_predict(const float* params, const float* feat, int n, float* out, cudaStream_t st) {
+    if (n <= 0) return G3X_OK;
+    predict_kernel<<<(n + 255) / 256, 256, 0, st>>>(params, feat, n, out);
+    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
+
+// One mini-batch gradient into g (and the batch's squared-error sum in *loss_sum_dev).
+static int batch_grad(ModelState& M, const float* X, const float* T, const int* idx, int B,
+                      cudaStream_t st) {
+    const int nb = (B + 255) / 256;
+    train_fwd_kernel<<<nb, 256, 0, st>>>(M.params, X, T, idx, B, M.h1, M.h2, M.dy, M.loss_part);
+    train_bwd3_kernel<<<(B * kH + 255) / 256, 256, 0, st>>>(M.params, M.h2, M.dy, B, M.dh2, M.grad);
+    train_gw2_kernel<<<(kH * kH + kH + 255) / 256, 256, 0, st>>>(M.h1, M.dh2, B, M.grad);
+    train_dh1_kernel<<<(B * kH + 255) / 256, 256, 0, st>>>(M.params, M.h1, M.dh2, B, M.dh1);
+    train_gw1_kernel<<<(kH * kF + kH + 255) / 256, 256, 0, st>>>(X, idx, M.dh1, B, M.grad);
+    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
+
+int model_alloc(ModelState& M, int batch) {
+    if (M.params && batch <= M.batch_cap) return G3X_OK;
+    if (!M.params) {
+        if (cudaMalloc(&M.params, kParams * sizeof(float)) || cudaMalloc(&M.grad, kParams * sizeof(float)) ||
+            cudaMalloc(&M.m, kParams * sizeof(float)) || cudaMalloc(&M.v, kParams * sizeof(float)))
+            return G3X_ERR_NOMEM;
+        cudaMemset(M.params, 0, kParams * sizeof(float));
+    }
+    cudaFree(M.h1); cudaFree(M.h2); cudaFree(M.dh1); cudaFree(M.dh2); cudaFree(M.dy);
+    cudaFree(M.loss_part);
+    const size_t b = (size_t)batch;
+    if (cudaMalloc(&M.h1, b * kH * sizeof(float)) || cudaMalloc(&M.h2, b * kH * sizeof(float)) ||
+        cudaMalloc(&M.dh1, b * kH * sizeof(float)) || cudaMalloc(&M.dh2, b * kH * sizeof(float)) ||
+        cudaMalloc(&M.dy, b * sizeof(float)) ||
+        cudaMalloc(&M.loss_part, ((b + 255) / 256) * sizeof(float)))
+        return G3X_ERR_NOMEM;
+    M.batch_cap = batch;
+    return G3X_OK;
+}
+
+void model_free(ModelState& M) {
+    cudaFree(M.params); cudaFree(M.grad); cudaFree(M.m); cudaFree(M.v);
+    cudaFree(M.h1); cudaFree(M.h2); cudaFree(M.dh1); cudaFree(M.dh2); cudaFree(M.dy);
+    cudaFree(M.loss_part); cudaFree(M.perm);
+    M = ModelState();
+}
+
+int model_gradient(ModelState& M, const float* X, const float* T, int B, float* h_grad,
+                   float* h_loss, cudaStream_t st) {
+    int rc = model_alloc(M, B);
+    if (rc) return rc;
+    if ((rc = batch_grad(M, X, T, nullptr, B, st))) return rc;
+    const int nb = (B + 255) / 256;
+    float* lp = new float[nb];
+    if (cudaMemcpyAsync(h_grad, M.grad, kParams * sizeof(float), cudaMemcpyDeviceToHost, st) ||
+        cudaMemcpyAsync(lp, M.loss_part, nb * sizeof(float), cudaMemcpyDeviceToHost, st) ||
+        cudaStreamSynchronize(st)) {
+        delete[] lp;
+        return G3X_ERR_CUDA;
+    }
+    double s = 0;
+    for (int k = 0; k < nb; ++k) s += lp[k];
+    delete[] lp;
+    if (h_loss) *h_loss = (float)(s / B);
+    return G3X_OK;
+}
+
+int model_train(ModelState& M, const float* X, const float* T, int n, int epochs, int batch,
+                float lr, uint64_t seed, float* h_epoch_loss, cudaStream_t st) {
+    if (batch <= 0 || n < batch) return G3X_ERR_INVALID;
+    int rc = model_alloc(M, batch);
+    if (rc) return rc;
+    if (n > M.perm_cap) {
+        cudaFree(M.perm);
+        if (cudaMalloc(&M.perm, (size_t)n * sizeof(int))) return G3X_ERR_NOMEM;
+        M.perm_cap = n;
+    }
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const int steps = n / batch;
+    const int nb = (batch + 255) / 256;
+    float* lp = new float[nb];
+    for (int ep = 0; ep < epochs; ++ep) {
+        perm_kernel<<<1, 1, 0, st>>>(M.perm, n, seed * 1000003ull + (unsigned long long)ep);
+        double loss = 0;
+        for (int s = 0; s < steps; ++s) {
+            if ((rc = batch_grad(M, X, T, M.perm + (size_t)s * batch, batch, st))) break;
+            ++M.t;
+            const float c1 = 1.0f - powf(b1, (float)M.t), c2 = 1.0f - powf(b2, (float)M.t);
+            adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(M.params, M.grad, M.m, M.v, lr, b1, b2, eps, c1, c2);
+            if (h_epoch_loss && s == steps - 1) {
+                if (cudaMemcpyAsync(lp, M.loss_part, nb * sizeof(float), cudaMemcpyDeviceToHost, st) ||
+                    cudaStreamSynchronize(st)) { rc = G3X_ERR_CUDA; break; }
+                for (int k = 0; k < nb; ++k) loss += lp[k];
+            }
+        }
+        if (rc) break;
+        if (h_epoch_loss) h_epoch_loss[ep] = (float)(loss / batch);
+    }
+    delete[] lp;
+    if (rc == G3X_OK && cudaPeekAtLastError() != cudaSuccess) rc = G3X_ERR_CUDA;
+    return rc;
+}
+
+// He-style initialisation from a splitmix64 stream (host), Adam state zeroed.
+int model_init(ModelState& M, uint64_t seed) {
+    int rc = model_alloc(M, 256);
+    if (rc) return rc;
+    float* h = new float[kParams];
+    uint64_t s = seed;
+    auto uni = [&]() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (float)((double)(z >> 11) * (1.0 / 9007199254740992.0)) * 2.0f - 1.0f;
+    };
+    for (int k = 0; k < kParams; ++k) h[k] = 0.0f;
+    for (int k = 0; k < kH * kF; ++k) h[oW1 + k] = uni() * sqrtf(6.0f / kF);
+    for (int k = 0; k < kH * kH; ++k) h[oW2 + k] = uni() * sqrtf(6.0f / kH);
+    for (int k = 0; k < kH; ++k) h[oW3 + k] = uni() * sqrtf(3.0f / kH);
+    rc = cudaMemcpy(M.params, h, kParams * sizeof(float), cudaMemcpyHostToDevice) ? G3X_ERR_CUDA : G3X_OK;
+    delete[] h;
+    cudaMemset(M.m, 0, kParams * sizeof(float));
+    cudaMemset(M.v, 0, kParams * sizeof(float));
+    M.t = 0;
+    M.trained = rc == G3X_OK ? 0 : M.trained;
+    return rc;
+}
+
+}  // namespace g3x

@@ -1,0 +1,97 @@
+// g3x_sched.cu -- job scheduling for the persistent row-parallel kernels.
+//
+// Every job gets
+//   a bucket : the first width class that holds its query (the class's tile, G lanes x C
+//              cells, covers the class width, so it covers the job's widest possible row
+//              min(qlen, 2w' + 1), w' the clamped band of ksw.cu:321-329); one persistent
+//              launch per class;
+//   a cost   : length-sorted fallback: log2(1 + widest row * tlen), an upper bound of the
+//              job's DP cells; learned: the cost model's prediction of log2(1 + cells).
+// A device counting sort over (bucket, quantised cost) bins -- histogram, exclusive scan,
+// scatter -- writes the job order with each bucket's jobs contiguous and in decreasing
+// cost, plus each bucket's (offset, count).  Nothing returns to the host, so the whole
+// batch (features, prediction, sort, launches) can be captured in one CUDA graph.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "g3x_core.h"
+#include "g3x_internal.h"
+
+namespace g3x {
+
+namespace {
+
+constexpr int kLevels = 1024;          // cost quantisation levels per bucket
+
+__global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScoreParams sp,
+                            const float* __restrict__ pred, TileTable tt,
+                            int32_t* __restrict__ bin, int32_t* __restrict__ hist) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const g3x_job_t jb = jobs[k];
+    const int w = clamp_w(jb.w, jb.qlen, sp.max_sc, sp.end_bonus, sp.o_del, sp.e_del, sp.o_ins, sp.e_ins);
+    const int wide = jb.qlen < 2 * w + 1 ? jb.qlen : 2 * w + 1;
+    // A class stages queries up to its width (the last class any query), and its tile covers
+    // its width, so the class follows qlen, which bounds the widest row.
+    int b = tt.n - 1;
+    for (int t = 0; t < tt.n; ++t)
+        if (tt.width[t] >= jb.qlen) { b = t; break; }
+    float cost = pred ? pred[k] : log2f(1.0f + (float)wide * (float)jb.tlen);
+    int q = (int)((26.0f - cost) * (kLevels / 26.0f));   // larger cost -> earlier bin
+    q = q < 0 ? 0 : (q >= kLevels ? kLevels - 1 : q);
+    const int bn = b * kLevels + q;
+    bin[k] = bn;
+    atomicAdd(hist + bn, 1);
+}
+
+// Exclusive scan of nb <= 16384 bins in one block; also each bucket's (offset, count).
+__global__ void scan_kernel(const int32_t* __restrict__ hist, int nb, int32_t* __restrict__ cursor,
+                            int32_t* __restrict__ bucket_oc, int nbuckets) {
+    __shared__ int32_t part[1024];
+    const int per = (nb + 1023) / 1024;
+    const int t = threadIdx.x;
+    int s = 0;
+    for (int k = t * per; k < (t + 1) * per && k < nb; ++k) s += hist[k];
+    part[t] = s;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+        const int v = t >= d ? part[t - d] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int run = t ? part[t - 1] : 0;
+    for (int k = t * per; k < (t + 1) * per && k < nb; ++k) {
+        cursor[k] = run;
+        run += hist[k];
+    }
+    __syncthreads();
+    if (t < nbuckets) {
+        const int lo = cursor[t * kLevels];
+        const int hi = t + 1 < nbuckets ? cursor[(t + 1) * kLevels] : part[1023];
+        bucket_oc[2 * t] = lo;
+        bucket_oc[2 * t + 1] = hi - lo;
+    }
+}
+
+__global__ void scatter_kernel(const int32_t* __restrict__ bin, int n, int32_t* __restrict__ cursor,
+                               int32_t* __restrict__ order) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int at = atomicAdd(cursor + bin[k], 1);
+    order[at] = k;
+}
+
+}  // namespace
+
+int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScoreParams& sp,
+                  const float* pred, const TileTable& tt, cudaStream_t st) {
+    const int nbins = tt.n * kLevels;
+    if (cudaMemsetAsync(s.hist, 0, nbins * sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
+    const int tb = 256, nb = (n + tb - 1) / tb;
+    cost_kernel<<<nb, tb, 0, st>>>(jobs, n, sp, pred, tt, s.bin, s.hist);
+    scan_kernel<<<1, 1024, 0, st>>>(s.hist, nbins, s.cursor, s.bucket_oc, tt.n);
+    scatter_kernel<<<nb, tb, 0, st>>>(s.bin, n, s.cursor, s.order);
+    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
+
+}  // namespace g3x

@@ -92,14 +92,20 @@ const char *g3x_strerror(int code);
 #define G3X_SCHED_SORTED  1   /* persistent kernel, jobs ordered by length (fallback) */
 #define G3X_SCHED_LEARNED 2   /* persistent kernel, jobs ordered by the learned cost model */
 
+#define G3X_KERNEL_AUTO    0  /* rolling for G3X_SCHED_PLAIN, row-parallel otherwise */
+#define G3X_KERNEL_ROLLING 1  /* anti-diagonal wavefront: rows on lanes, 4-cell lane steps */
+#define G3X_KERNEL_ROWPAR  2  /* one row per step: columns on lanes, F by shuffle scan */
+
 typedef struct {
     int32_t schedule;     /* G3X_SCHED_* */
     int32_t max_qlen;     /* upper bound of qlen over the batch (required) */
     int32_t max_tlen;     /* upper bound of tlen over the batch (required) */
-    int32_t lanes;        /* lanes per job for persistent schedules: 8, 16, 32, or 0 = tuned;
+    int32_t lanes;        /* lanes per job: 4 (row-parallel only), 8, 16, 32, or 0 = tuned;
                              raised when a warp of such groups would not fit in shared memory */
+    int32_t tile;         /* row-parallel: cells per lane per tile (5, 9 or 13), 0 = tuned */
+    int32_t kernel;       /* G3X_KERNEL_* */
     int32_t *d_cells;     /* optional per-job DP cell count (trip count of ksw.cu:346) */
-} g3x_batch_opts_t;
+} g3x_batch_opts_t;       /* 32 bytes */
 
 /* n jobs; outputs to d_out[k] and d_status[k] (G3X_OK or a G3X_ERR_* per job).
    Replaces n calls of ksw_extend2 (bwa/src/ksw.h:33) issued by localExtending
@@ -108,6 +114,32 @@ int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
                           int32_t n, const uint32_t *d_codes, const uint32_t *d_nmask,
                           g3x_ext_t *d_out, int32_t *d_status, const g3x_batch_opts_t *opts,
                           void *stream);
+
+/* ---- schedule tuning ----------------------------------------------------------------------- */
+/* The persistent schedules split a batch into width classes: a job belongs to the first class
+   whose `width` holds its query (qlen bounds the widest row, min(qlen, 2w+1), w after the
+   clamp of bwa/src/ksw.cu:321-329); the last class takes every longer job (several tiles per
+   row when its rows are wider than one tile).  Each
+   class runs the row-parallel kernel with `lanes` lanes per job and `tile` cells per lane;
+   `warp_batch` = 1 makes a warp pull one job per group at once and wait for all of them
+   (jobs then balance by the schedule's cost order), 0 lets each group refill on its own. */
+#define G3X_MAX_CLASSES 8
+typedef struct {
+    int32_t width, lanes, tile, warp_batch;
+} g3x_tile_t;
+
+int g3x_get_tiles(g3x_ctx *ctx, g3x_tile_t *h_tiles, int32_t *n);
+int g3x_set_tiles(g3x_ctx *ctx, const g3x_tile_t *h_tiles, int32_t n);
+/* Times the candidate configurations of every width class on the given jobs (device
+   buffers, each job run as it would be in its class) and keeps the fastest per class in the
+   context; h_tiles/n receive the table.  Blocks.  Outputs of the trial runs are discarded. */
+int g3x_autotune(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
+                 const uint32_t *d_codes, const uint32_t *d_nmask, int32_t max_qlen,
+                 int32_t max_tlen, g3x_tile_t *h_tiles, int32_t *n_tiles);
+/* Occupancy counters of the last persistent batch on this context: h_stats[0] = group-rows
+   computed, [1] = group-rows a group waited for the other groups of its warp (warp_batch),
+   [2] = warp batches.  Synchronises the context's device. */
+int g3x_last_stats(g3x_ctx *ctx, uint64_t *h_stats);
 
 /* ---- seed-level extension with band retry ---------------------------------------------- */
 
@@ -161,6 +193,32 @@ int g3x_extend_seeds_stream(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t
                             int64_t n, const uint32_t *h_codes, const uint32_t *h_nmask,
                             int64_t n_bases, g3x_reg_t *h_regs, int32_t *h_status,
                             int32_t chunk, const g3x_batch_opts_t *opts);
+
+/* ---- learned cost model ------------------------------------------------------------------ */
+/* A 5 -> 64 -> 64 -> 1 ReLU MLP (fp32) per context that predicts a job's work from five
+   features: qlen/128, tlen/256, h0/64, query GC fraction, and the mismatch fraction of the
+   first min(32, qlen, tlen) bases next to the seed.  Trained on the GPU by the library's own
+   forward/backward/Adam kernels; G3X_SCHED_LEARNED orders jobs by its prediction.  No
+   counterpart in the reference (its extension stage has no scheduler). */
+#define G3X_MLP_FEATURES 5
+#define G3X_MLP_PARAMS 4609   /* W1[64][5] b1[64] W2[64][64] b2[64] W3[64] b3 */
+
+/* d_feat[k*5 .. k*5+4] = features of job k. */
+int g3x_features(g3x_ctx *ctx, const g3x_job_t *d_jobs, int32_t n, const uint32_t *d_codes,
+                 const uint32_t *d_nmask, float *d_feat, void *stream);
+/* Fresh He-style parameters from `seed`; clears the optimiser state. */
+int g3x_mlp_init(g3x_ctx *ctx, uint64_t seed);
+/* Mini-batch Adam on mean squared error over n samples (d_feat n x 5, d_target n); the
+   last mini-batch's loss of each epoch goes to h_epoch_loss[epoch] when not NULL. Blocks. */
+int g3x_mlp_train(g3x_ctx *ctx, const float *d_feat, const float *d_target, int32_t n,
+                  int32_t epochs, int32_t batch, float lr, uint64_t seed, float *h_epoch_loss);
+/* Gradient of the mean squared error over the first n samples (host copy) and the loss. */
+int g3x_mlp_gradient(g3x_ctx *ctx, const float *d_feat, const float *d_target, int32_t n,
+                     float *h_grad, float *h_loss);
+/* d_pred[k] = model output for job k. Asynchronous on `stream`. */
+int g3x_mlp_predict(g3x_ctx *ctx, const float *d_feat, int32_t n, float *d_pred, void *stream);
+int g3x_mlp_get_params(g3x_ctx *ctx, float *h_params);
+int g3x_mlp_set_params(g3x_ctx *ctx, const float *h_params);
 
 /* ---- diagnostics ------------------------------------------------------------------------ */
 

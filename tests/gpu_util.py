@@ -19,7 +19,8 @@ def to_dev(a):
     return torch.from_numpy(a.view(np.uint8).copy()).cuda()
 
 
-def run_batch(u8, jobs, score, schedule=g.SCHED_PLAIN, lanes=0, max_qlen=None, max_tlen=None):
+def run_batch(u8, jobs, score, schedule=g.SCHED_PLAIN, lanes=0, max_qlen=None, max_tlen=None,
+              tile=0, kernel=g.KERNEL_AUTO):
     """Returns (ext[n,6], status[n], cells[n]) from the GPU."""
     import torch
     n = len(jobs)
@@ -31,7 +32,7 @@ def run_batch(u8, jobs, score, schedule=g.SCHED_PLAIN, lanes=0, max_qlen=None, m
     mq = int(jobs["qlen"].max()) if max_qlen is None else max_qlen
     mt = int(jobs["tlen"].max()) if max_tlen is None else max_tlen
     ctx().extend_batch(score, d_jobs, n, d_codes, d_nmask, out, status, mq, mt,
-                       schedule=schedule, lanes=lanes, d_cells=cells)
+                       schedule=schedule, lanes=lanes, d_cells=cells, tile=tile, kernel=kernel)
     torch.cuda.synchronize()
     return out.cpu().numpy(), status.cpu().numpy(), cells.cpu().numpy()
 

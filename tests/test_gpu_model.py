@@ -1,0 +1,109 @@
+"""Learned cost model on the GPU: feature kernel vs the oracle's features, CUDA gradients vs
+the numpy oracle (oracle/mlp_oracle.py), training that lowers the loss, inference vs the
+oracle's forward pass, and learned / length-sorted schedules that stay bit-exact."""
+import numpy as np
+import pytest
+
+import g3sa_b200 as g
+from oracle import mlp_oracle as mo
+from tests import native as nat
+from tests.gpu_util import ctx, to_dev, run_batch
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_features(wl):
+    import torch
+    codes, nmask = wl.planes()
+    d_feat = torch.zeros((wl.n, 5), dtype=torch.float32, device="cuda")
+    ctx().features(to_dev(wl.jobs), wl.n, to_dev(codes), to_dev(nmask), d_feat)
+    torch.cuda.synchronize()
+    return d_feat
+
+
+def test_features_match_oracle():
+    wl = g.synth(2, 1500, seed=8, w=100, unrelated=0.2)
+    f = gpu_features(wl).cpu().numpy()
+    ref = mo.features(wl.jobs, wl.u8)
+    assert np.allclose(f, ref, rtol=1e-6, atol=1e-6)
+
+
+def test_gradient_matches_oracle():
+    import torch
+    wl = g.synth(1, 600, seed=9)
+    feat = gpu_features(wl)
+    rng = np.random.default_rng(1)
+    t = torch.from_numpy(rng.normal(10, 2, wl.n).astype(np.float32)).cuda()
+    c = ctx()
+    c.mlp_init(1234)
+    p = c.mlp_params()
+    grad, loss = c.mlp_gradient(feat, t, wl.n)
+    rl, rg = mo.loss_and_grad(p, feat.cpu().numpy(), t.cpu().numpy())
+    assert abs(loss - rl) <= 1e-4 * abs(rl) + 1e-5
+    scale = np.abs(rg).max()
+    assert np.allclose(grad, rg, rtol=2e-3, atol=2e-5 * scale), np.abs(grad - rg).max()
+
+
+def test_predict_matches_oracle_forward():
+    import torch
+    wl = g.synth(2, 800, seed=10)
+    feat = gpu_features(wl)
+    c = ctx()
+    c.mlp_init(99)
+    p = c.mlp_params()
+    c.mlp_set_params(p)
+    pred = torch.zeros(wl.n, dtype=torch.float32, device="cuda")
+    c.mlp_predict(feat, wl.n, pred)
+    torch.cuda.synchronize()
+    y, _ = mo.forward(p, feat.cpu().numpy())
+    assert np.allclose(pred.cpu().numpy(), y, rtol=1e-4, atol=1e-4)
+
+
+def test_training_lowers_loss_and_predicts_cells():
+    import torch
+    wl = g.synth(1, 60000, seed=11, w=100, unrelated=0.2)
+    sc = g.default_score()
+    out, status, cells = run_batch(wl.u8, wl.jobs, sc, g.SCHED_PLAIN)
+    assert (status == 0).all()
+    feat = gpu_features(wl)
+    target = torch.from_numpy(np.log2(1.0 + cells.astype(np.float32))).cuda()
+    c = ctx()
+    c.mlp_init(7)
+    losses = c.mlp_train(feat, target, wl.n, epochs=6, batch=1024, lr=3e-3, seed=7)
+    assert losses[-1] < 0.5 * losses[0], losses
+    pred = torch.zeros(wl.n, dtype=torch.float32, device="cuda")
+    c.mlp_predict(feat, wl.n, pred)
+    torch.cuda.synchronize()
+    r = np.corrcoef(pred.cpu().numpy(), target.cpu().numpy())[0, 1]
+    assert r > 0.9, r
+
+
+@pytest.mark.parametrize("schedule", [g.SCHED_SORTED, g.SCHED_LEARNED])
+def test_scheduled_batches_are_exact(schedule):
+    wl = g.synth(2, 20000, seed=12, w=100, unrelated=0.2)
+    sc = g.default_score()
+    if schedule == g.SCHED_LEARNED:
+        c = ctx()
+        c.mlp_init(5)
+        c.mlp_set_params(c.mlp_params())
+    ref, rcells, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
+    out, status, cells = run_batch(wl.u8, wl.jobs, sc, schedule)
+    assert (status == 0).all()
+    assert (out == ref).all()
+    assert (cells == rcells).all()
+
+
+def test_warp_batched_classes_are_exact():
+    wl = g.synth(1, 20000, seed=13, w=100, unrelated=0.2)
+    sc = g.default_score()
+    c = ctx()
+    tiles = c.get_tiles()
+    try:
+        c.set_tiles([(w, l, t, 1) for (w, l, t, _) in tiles])
+        ref, _, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
+        out, status, _ = run_batch(wl.u8, wl.jobs, sc, g.SCHED_SORTED)
+        assert (status == 0).all() and (out == ref).all()
+        stats = c.last_stats()
+        assert stats[0] > 0 and stats[2] > 0
+    finally:
+        c.set_tiles(tiles)
