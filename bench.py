@@ -165,6 +165,25 @@ def run_reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def timed_steps(fn, k, w, stream, flush):
+    """W untimed calls, then K calls each bracketed by CUDA events on `stream`, with a
+    256 MiB write between them so no step starts with the previous step's data in L2."""
+    import torch
+    for _ in range(w):
+        fn()
+    ms = []
+    for _ in range(k):
+        flush.fill_(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return ms
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup()
@@ -173,15 +192,20 @@ def main():
         return
     import torch
     import g3sa_b200 as g
-    from g3sa_b200 import build
+    from g3sa_b200 import build, learn
     build.build_lib()
     torch.cuda.set_device(local)
-    pg = None
+    dist = None
     if ws > 1:
         import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
 
     kind_, units, w, unrel, desc = WORKLOADS[args.workload]
     wl = g.synth(kind_, units, seed=args.seed + 1000 * rank, w=w, unrelated=unrel)
@@ -194,9 +218,7 @@ def main():
     h_jobs = torch.from_numpy(wl.jobs.view(np.uint8).copy()).pin_memory()
     h_codes = torch.from_numpy(codes.view(np.uint8).copy()).pin_memory()
     h_nmask = torch.from_numpy(nmask.view(np.uint8).copy()).pin_memory()
-    d_jobs = h_jobs.to(dev)
-    d_codes = h_codes.to(dev)
-    d_nmask = h_nmask.to(dev)
+    d_jobs, d_codes, d_nmask = h_jobs.to(dev), h_codes.to(dev), h_nmask.to(dev)
     d_out = torch.zeros((n, 6), dtype=torch.int32, device=dev)
     d_status = torch.zeros(n, dtype=torch.int32, device=dev)
     d_cells = torch.zeros(n, dtype=torch.int32, device=dev)
@@ -204,53 +226,62 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
     stream = torch.cuda.current_stream(dev)
 
-    sched = {"plain": g.SCHED_PLAIN, "sorted": g.SCHED_SORTED, "learned": g.SCHED_LEARNED,
-             "auto": g.SCHED_SORTED}[args.schedule]
-    lanes = 8
-
-    def step(schedule, lanes_):
+    def batch(schedule, **kw):
         ctx.extend_batch(sc, d_jobs, n, d_codes, d_nmask, d_out, d_status, mq, mt,
-                         schedule=schedule, lanes=lanes_, d_cells=d_cells, stream=stream)
+                         schedule=schedule, stream=stream, **kw)
 
-    # correctness gate and useful-cell count (device counter == oracle trip count)
-    step(sched, lanes)
+    # Useful cells of this batch: the kernels' own trip-count counters (plain kernel).
+    batch(g.SCHED_PLAIN, d_cells=d_cells)
     torch.cuda.synchronize()
-    st = d_status.cpu().numpy()
-    if (st != 0).any():
-        raise SystemExit(f"per-job status errors: {np.unique(st)}")
-    cells = int(d_cells.to(torch.int64).sum().item())
+    if (d_status != 0).any():
+        raise SystemExit("per-job status errors in the plain run")
+    cells_np = d_cells.cpu().numpy()
+    cells = int(cells_np.astype(np.int64).sum())
+    plain_out = d_out.cpu().numpy().copy()
 
-    def timed(schedule, lanes_, k, w_):
-        for _ in range(w_):
-            step(schedule, lanes_)
-        ms = []
-        for _ in range(k):
-            flush.fill_(1)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            step(schedule, lanes_)
-            e1.record(stream)
-            e1.synchronize()
-            ms.append(e0.elapsed_time(e1))
-        return ms
+    # Learned cost model: trained on the GPU on config-1 traces from the plain kernel.
+    train_metrics = learn.train(ctx, n_train=2_000_000, seed_train=0xA11CE + rank)
+    pred_err = learn.prediction_error(ctx, d_jobs, n, d_codes, d_nmask, cells_np)
 
-    def barrier():
-        torch.cuda.synchronize()
-        if pg is not None:
-            pg.barrier()
+    # Autotune the width classes on this batch (length-sorted order), then capture graphs.
+    t_tune = time.perf_counter()
+    tiles = ctx.autotune(sc, d_jobs, n, d_codes, d_nmask, mq, mt)
+    t_tune = time.perf_counter() - t_tune
+    sched = {"plain": g.SCHED_PLAIN, "sorted": g.SCHED_SORTED, "learned": g.SCHED_LEARNED,
+             "auto": g.SCHED_LEARNED}[args.schedule]
+    graphs = {}
+    for sname, sval in (("learned", g.SCHED_LEARNED), ("sorted", g.SCHED_SORTED)):
+        graphs[sname] = ctx.capture_batch(sc, d_jobs, n, d_codes, d_nmask, d_out, d_status, mq, mt,
+                                          schedule=sval)
+    main_graph = graphs["learned" if sched == g.SCHED_LEARNED else "sorted"]
+    if sched == g.SCHED_PLAIN:
+        main_fn = lambda: batch(g.SCHED_PLAIN)  # noqa: E731
+    else:
+        main_fn = lambda: main_graph.launch(stream)  # noqa: E731
+
+    # exactness of the timed configuration against the plain kernel (itself pinned to the oracle)
+    main_fn()
+    torch.cuda.synchronize()
+    if (d_status != 0).any() or not np.array_equal(d_out.cpu().numpy(), plain_out):
+        raise SystemExit("scheduled batch differs from the plain kernel")
 
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
-    ms = timed(sched, lanes, args.steps, args.warmup)
+    ms = timed_steps(main_fn, args.steps, args.warmup, stream, flush)
     barrier()
     clk = clocks.stop()
     t_step = sum(ms) / len(ms)
+    stats_main = ctx.last_stats()
 
-    # plain one-block-per-job kernel on the same batch, for the learned/plain comparison
-    ms_plain = timed(g.SCHED_PLAIN, 0, max(2, args.steps // 2), 1)
-    t_plain = sum(ms_plain) / len(ms_plain)
+    # comparison arms on the same batch
+    k2 = max(3, args.steps // 2)
+    ms_sorted = timed_steps(lambda: graphs["sorted"].launch(stream), k2, 1, stream, flush)
+    stats_sorted = ctx.last_stats()
+    ms_learned = timed_steps(lambda: graphs["learned"].launch(stream), k2, 1, stream, flush)
+    stats_learned = ctx.last_stats()
+    ms_plain = timed_steps(lambda: batch(g.SCHED_PLAIN), k2, 1, stream, flush)
+    t_sorted, t_learned, t_plain = (sum(x) / len(x) for x in (ms_sorted, ms_learned, ms_plain))
 
     # end to end through the C ABI with host buffers: H2D job stream, extension, D2H results
     bi = h_jobs.numel() + h_codes.numel() + h_nmask.numel()
@@ -260,54 +291,51 @@ def main():
         d_jobs.copy_(h_jobs, non_blocking=True)
         d_codes.copy_(h_codes, non_blocking=True)
         d_nmask.copy_(h_nmask, non_blocking=True)
-        step(sched, lanes)
+        main_fn()
         h_out.copy_(d_out, non_blocking=True)
 
-    for _ in range(args.warmup):
-        e2e_step()
     barrier()
-    e2e_ms = []
-    for _ in range(args.steps):
-        flush.fill_(1)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        e2e_step()
-        e1.record(stream)
-        e1.synchronize()
-        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_ms = timed_steps(e2e_step, args.steps, args.warmup, stream, flush)
     barrier()
     t_e2e = sum(e2e_ms) / len(e2e_ms)
 
-    # max over ranks, sums of work
     tot_cells, tot_jobs = cells, n
-    if pg is not None:
-        import torch.distributed as dist
-        v = torch.tensor([t_step, t_e2e, t_plain], dtype=torch.float64, device=dev)
+    if dist is not None:
+        v = torch.tensor([t_step, t_e2e, t_plain, t_sorted, t_learned], dtype=torch.float64, device=dev)
         dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        t_step, t_e2e, t_plain = v.tolist()
-        c = torch.tensor([tot_cells, tot_jobs], dtype=torch.int64, device=dev)
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        tot_cells, tot_jobs = c.tolist()
+        t_step, t_e2e, t_plain, t_sorted, t_learned = v.tolist()
+        cnt = torch.tensor([tot_cells, tot_jobs], dtype=torch.int64, device=dev)
+        dist.all_reduce(cnt, op=dist.ReduceOp.SUM)
+        tot_cells, tot_jobs = cnt.tolist()
 
     peak_ops = ctx.int_peak()
     if rank == 0:
         gcups = tot_cells / (t_step * 1e-3) / 1e9
         peak_gcups = peak_ops / 8 / 1e9
-        kind, cpu_t, _ = cpu_reference(wl, os.cpu_count() or 1)
+        kind, cpu_t, cpu_out = cpu_reference(wl, os.cpu_count() or 1)
         cpu_gcups = cells / cpu_t / 1e9
+        idle = lambda s: round(s[1] / max(1, s[0] + s[1]), 4)  # noqa: E731
         line = {
             "metric": METRIC, "value": round(gcups, 3), "unit": "GCUPS", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator, shapes of the benchmark configuration)",
             "config": {"workload": desc, "jobs_per_gpu": n, "cells_per_gpu": cells,
-                       "schedule": args.schedule, "lanes": lanes, "max_qlen": mq, "max_tlen": mt,
+                       "schedule": args.schedule if args.schedule != "auto" else "learned",
+                       "launch": "one CUDA graph per step (features, MLP, counting sort, one persistent launch per width class)",
+                       "width_classes": tiles, "max_qlen": mq, "max_tlen": mt,
                        "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas x{ws}"},
             "extensions_per_s": round(tot_jobs / (t_step * 1e-3), 1),
-            "plain": {"gcups": round(tot_cells / (t_plain * 1e-3) / 1e9, 3), "ms_per_step": round(t_plain, 4),
-                      "schedule": "one 32-lane block per job, input order"},
-            "speedup_vs_plain": round(t_plain / t_step, 3),
+            "arms": {"learned": {"gcups": round(tot_cells / (t_learned * 1e-3) / 1e9, 3), "ms": round(t_learned, 4),
+                                 "warp_idle_frac": idle(stats_learned)},
+                     "sorted": {"gcups": round(tot_cells / (t_sorted * 1e-3) / 1e9, 3), "ms": round(t_sorted, 4),
+                                "warp_idle_frac": idle(stats_sorted)},
+                     "plain": {"gcups": round(tot_cells / (t_plain * 1e-3) / 1e9, 3), "ms": round(t_plain, 4),
+                               "kernel": "one 32-lane block per job, anti-diagonal wavefront, input order"}},
+            "speedup_learned_vs_plain": round(t_plain / t_learned, 3),
+            "speedup_learned_vs_sorted": round(t_sorted / t_learned, 3),
+            "cost_model": {**train_metrics, "prediction_on_this_batch": pred_err},
+            "autotune_s": round(t_tune, 2),
             "e2e": {"value": round(tot_cells / (t_e2e * 1e-3) / 1e9, 3), "unit": "GCUPS",
                     "ms_per_step": round(t_e2e, 4), "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
             "roofline": {"bound": "int_alu", "achieved": round(gcups / max(ws, 1), 3),
@@ -316,13 +344,15 @@ def main():
                          "peak_source": "measured live: g3x_int_peak (DPX VIMNMX3 chains) / 8 ops per cell",
                          "int_ops_per_s": peak_ops},
             "cpu_baseline": {"value": round(cpu_gcups, 4), "unit": "GCUPS", "cores": os.cpu_count(),
-                             "kind": kind, "sample": f"whole rank-0 workload ({n} jobs), one pass"},
+                             "kind": kind, "sample": f"whole rank-0 workload ({n} jobs), one pass",
+                             "gpu_outputs_identical": bool(np.array_equal(cpu_out, plain_out))},
             "clocks": clk,
-            "gpu_launches": args.steps * 1,
+            "gpu_launches": args.steps * (5 + sum(1 for _ in tiles)),
         }
         print(json.dumps(line), flush=True)
-    if pg is not None:
-        import torch.distributed as dist
+    for gr in graphs.values():
+        gr.close()
+    if dist is not None:
         dist.destroy_process_group()
 
 

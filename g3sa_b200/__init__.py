@@ -51,8 +51,9 @@ REG_DT = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), (
                    ("pad_", "u1", 2)])
 BATCH_OPTS_DT = np.dtype([("schedule", "<i4"), ("max_qlen", "<i4"), ("max_tlen", "<i4"),
                           ("lanes", "<i4"), ("tile", "<i4"), ("kernel", "<i4"), ("d_cells", "<u8")])
-KERNEL_AUTO, KERNEL_ROLLING, KERNEL_ROWPAR = 0, 1, 2
-TILE_DT = np.dtype([("width", "<i4"), ("lanes", "<i4"), ("tile", "<i4"), ("warp_batch", "<i4")])
+KERNEL_AUTO, KERNEL_ROLLING, KERNEL_ROWPAR, KERNEL_LANE = 0, 1, 2, 3
+TILE_DT = np.dtype([("width", "<i4"), ("lanes", "<i4"), ("tile", "<i4"), ("warp_batch", "<i4"),
+                    ("refill", "<i4")])
 MLP_PARAMS, MLP_FEATURES = 4609, 5
 SYNTH_PARAMS_DT = np.dtype([("kind", "<i4"), ("n", "<i4"), ("w", "<i4"), ("a", "<i4"),
                             ("o_del", "<i4"), ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4"),
@@ -135,6 +136,9 @@ def lib():
         L.g3x_set_tiles.argtypes = [P, P, I32]
         L.g3x_autotune.argtypes = [P, P, P, I32, P, P, I32, I32, P, P]
         L.g3x_last_stats.argtypes = [P, P]
+        L.g3x_graph_capture.argtypes = [P, P, P, I32, P, P, P, P, P, ctypes.POINTER(P)]
+        L.g3x_graph_launch.argtypes = [P, P]
+        L.g3x_graph_destroy.argtypes = [P]
         L.g3x_int_peak.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
         L.g3x_int_peak.restype = ctypes.c_int
         L.g3x_pack_codes.argtypes = [P, ctypes.c_int64, P, P, ctypes.c_int64]
@@ -251,6 +255,21 @@ class Context:
         except Exception:
             pass
 
+    def capture_batch(self, score, d_jobs, n, d_codes, d_nmask, d_out, d_status, max_qlen,
+                      max_tlen, schedule=SCHED_SORTED, lanes=0, d_cells=None, tile=0,
+                      kernel=KERNEL_AUTO):
+        """g3x_graph_capture of one batch; returns a Graph whose launch() replays it."""
+        opts = np.zeros(1, BATCH_OPTS_DT)
+        opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
+            schedule, max_qlen, max_tlen, lanes)
+        opts["tile"], opts["kernel"] = tile, kernel
+        opts["d_cells"] = _ptr(d_cells) if d_cells is not None else 0
+        h = ctypes.c_void_p()
+        _check(lib().g3x_graph_capture(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
+                                       _ptr(d_nmask), _ptr(d_out), _ptr(d_status), opts.ctypes.data,
+                                       ctypes.byref(h)), "g3x_graph_capture")
+        return Graph(h)
+
     # ---- learned cost model ----
     def features(self, d_jobs, n, d_codes, d_nmask, d_feat, stream=None):
         _check(lib().g3x_features(self._h, _ptr(d_jobs), int(n), _ptr(d_codes), _ptr(d_nmask),
@@ -357,6 +376,27 @@ class Context:
                                            hp(nmask), int(n_bases), hp(regs), hp(status), int(chunk),
                                            opts.ctypes.data)
         _check(rc, "g3x_extend_seeds_stream")
+
+
+class Graph:
+    """An executable CUDA graph of one captured batch (g3x_graph)."""
+
+    def __init__(self, h):
+        self._h = h
+
+    def launch(self, stream=None):
+        _check(lib().g3x_graph_launch(self._h, _stream(stream)), "g3x_graph_launch")
+
+    def close(self):
+        if self._h:
+            lib().g3x_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _ptr(t):

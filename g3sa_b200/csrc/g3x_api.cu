@@ -49,10 +49,17 @@ int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d) {
     if (opts->schedule != G3X_SCHED_PLAIN && opts->schedule != G3X_SCHED_SORTED &&
         opts->schedule != G3X_SCHED_LEARNED)
         return G3X_ERR_INVALID;
-    if (opts->kernel < G3X_KERNEL_AUTO || opts->kernel > G3X_KERNEL_ROWPAR) return G3X_ERR_INVALID;
+    if (opts->kernel < G3X_KERNEL_AUTO || opts->kernel > G3X_KERNEL_LANE) return G3X_ERR_INVALID;
     const bool plain = opts->schedule == G3X_SCHED_PLAIN;
     d->kernel = opts->kernel == G3X_KERNEL_AUTO ? (plain ? kKernelRolling : kKernelRowpar)
-                                                : (opts->kernel == G3X_KERNEL_ROLLING ? kKernelRolling : kKernelRowpar);
+                : opts->kernel == G3X_KERNEL_ROLLING ? kKernelRolling
+                : opts->kernel == G3X_KERNEL_ROWPAR ? kKernelRowpar : kKernelLane;
+    if (d->kernel == kKernelLane) {
+        if (plain) return G3X_ERR_INVALID;            // the lane kernel is persistent only
+        d->lanes = 1; d->tile = 0; d->persistent = 1; d->warps_per_block = 4; d->queue = queue;
+        d->refill = opts->tile > 0 ? opts->tile : 1;  // tile carries the refill threshold
+        return G3X_OK;
+    }
     if (plain) {
         // one 32-lane block per job, jobs in the given order
         d->lanes = 32; d->tile = opts->tile ? opts->tile : 9; d->persistent = 0; d->warps_per_block = 1;
@@ -135,12 +142,12 @@ static void default_tiles(TileTable& t) {
     const int c[] = {5, 9, 9, 9, 9, 9};
     t.n = 6;
     for (int k = 0; k < t.n; ++k) {
-        t.width[k] = w[k]; t.lanes[k] = l[k]; t.tile[k] = c[k]; t.warp_batch[k] = 0;
+        t.width[k] = w[k]; t.lanes[k] = l[k]; t.tile[k] = c[k]; t.warp_batch[k] = 0; t.refill[k] = 1;
     }
 }
 
 // Largest query a class stages: its width, except for the unbounded last class.
-static int class_qcap(const TileTable& t, int k, int qmax) {
+int class_qcap(const TileTable& t, int k, int qmax) {
     return k == t.n - 1 ? qmax : std::min(qmax, t.width[k]);
 }
 
@@ -155,10 +162,11 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
         if (only >= 0 && k != only) continue;
         if (cudaStreamWaitEvent(ctx->side[k], ctx->fork, 0) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
         LaunchDesc d = base;
-        d.kernel = kKernelRowpar;
+        d.kernel = tt.lanes[k] == 1 ? kKernelLane : kKernelRowpar;
         d.lanes = tt.lanes[k];
         d.tile = tt.tile[k];
         d.warp_batch = tt.warp_batch[k];
+        d.refill = tt.refill[k];
         d.persistent = 1;
         d.warps_per_block = 4;
         d.qmax = class_qcap(tt, k, base.qmax);
@@ -167,8 +175,12 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
         d.count = ctx->sched.bucket_oc + 2 * k + 1;
         d.queue = ctx->d_queue + k;
         d.stats = ctx->d_stats;
-        while (d.lanes < 32 && (32 / d.lanes) * group_smem_bytes(d.qmax, d.tmax) > 227 * 1024) d.lanes *= 2;
-        rc = launch_rowpar(d, sp, ctx->side[k]);
+        if (d.kernel == kKernelLane) {
+            rc = launch_lane(d, sp, ctx->side[k]);
+        } else {
+            while (d.lanes < 32 && (32 / d.lanes) * group_smem_bytes(d.qmax, d.tmax) > 227 * 1024) d.lanes *= 2;
+            rc = launch_rowpar(d, sp, ctx->side[k]);
+        }
         if (rc == G3X_OK && cudaEventRecord(ctx->join[k], ctx->side[k]) != cudaSuccess) rc = G3X_ERR_CUDA;
         if (rc == G3X_OK && cudaStreamWaitEvent(st, ctx->join[k], 0) != cudaSuccess) rc = G3X_ERR_CUDA;
     }
@@ -275,8 +287,9 @@ int g3x_ksw_extend2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_
     cudaStream_t st = (cudaStream_t)stream;
     d.jobs = d_jobs; d.codes = d_codes; d.nmask = d_nmask; d.out = d_out; d.status = d_status;
     d.n = n;
-    // Persistent row-parallel batches without a fixed group size go through the scheduler.
-    if (d.persistent && d.kernel == g3x::kKernelRowpar && opts->lanes == 0 && opts->tile == 0)
+    // Persistent batches without a fixed kernel shape go through the scheduler.
+    if (d.persistent && d.kernel == g3x::kKernelRowpar && opts->kernel == G3X_KERNEL_AUTO &&
+        opts->lanes == 0 && opts->tile == 0)
         return g3x::run_scheduled(ctx, d, sp, opts->schedule == G3X_SCHED_LEARNED, st);
     if (opts->schedule == G3X_SCHED_LEARNED) return G3X_ERR_INVALID;   // needs the scheduler
     if (d.persistent) {
@@ -288,10 +301,65 @@ int g3x_ksw_extend2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_
     return g3x::launch_extend(d, sp, st);
 }
 
+struct g3x_graph {
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+};
+
+int g3x_graph_capture(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs, int32_t n,
+                      const uint32_t* d_codes, const uint32_t* d_nmask, g3x_ext_t* d_out,
+                      int32_t* d_status, const g3x_batch_opts_t* opts, g3x_graph** out) {
+    if (!ctx || !out) return G3X_ERR_INVALID;
+    *out = nullptr;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    // Scratch must exist before capture (allocation is not a graph operation).
+    if (opts && opts->schedule != G3X_SCHED_PLAIN) {
+        int rc = g3x::alloc_sched(ctx->sched, n);
+        if (rc) return rc;
+    }
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return G3X_ERR_CUDA;
+    g3x_graph* g = new (std::nothrow) g3x_graph();
+    if (!g) { cudaStreamDestroy(cs); return G3X_ERR_NOMEM; }
+    int rc = G3X_OK;
+    if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = G3X_ERR_CUDA;
+    if (rc == G3X_OK) {
+        rc = g3x_ksw_extend2_batch(ctx, score, d_jobs, n, d_codes, d_nmask, d_out, d_status, opts, cs);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(cs, &graph);
+        if (rc == G3X_OK && e != cudaSuccess) rc = G3X_ERR_CUDA;
+        g->graph = graph;
+        if (rc == G3X_OK && cudaGraphInstantiate(&g->exec, graph, 0) != cudaSuccess) rc = G3X_ERR_CUDA;
+    }
+    cudaStreamDestroy(cs);
+    if (rc != G3X_OK) {
+        if (g->graph) cudaGraphDestroy(g->graph);
+        delete g;
+        cudaGetLastError();
+        return rc;
+    }
+    *out = g;
+    return G3X_OK;
+}
+
+int g3x_graph_launch(g3x_graph* g, void* stream) {
+    if (!g) return G3X_ERR_INVALID;
+    return cudaGraphLaunch(g->exec, (cudaStream_t)stream) == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
+
+int g3x_graph_destroy(g3x_graph* g) {
+    if (!g) return G3X_ERR_INVALID;
+    cudaGraphExecDestroy(g->exec);
+    cudaGraphDestroy(g->graph);
+    delete g;
+    return G3X_OK;
+}
+
 int g3x_get_tiles(g3x_ctx* ctx, g3x_tile_t* h, int32_t* n) {
     if (!ctx || !h || !n) return G3X_ERR_INVALID;
     for (int k = 0; k < ctx->tiles.n; ++k)
-        h[k] = g3x_tile_t{ctx->tiles.width[k], ctx->tiles.lanes[k], ctx->tiles.tile[k], ctx->tiles.warp_batch[k]};
+        h[k] = g3x_tile_t{ctx->tiles.width[k], ctx->tiles.lanes[k], ctx->tiles.tile[k],
+                          ctx->tiles.warp_batch[k], ctx->tiles.refill[k]};
     *n = ctx->tiles.n;
     return G3X_OK;
 }
@@ -300,9 +368,11 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
     if (!ctx || !h || n < 1 || n > G3X_MAX_CLASSES) return G3X_ERR_INVALID;
     for (int k = 0; k < n; ++k) {
         const g3x_tile_t& t = h[k];
-        if ((t.lanes != 4 && t.lanes != 8 && t.lanes != 16 && t.lanes != 32) ||
-            (t.tile != 5 && t.tile != 9 && t.tile != 13) || t.width < 1 ||
-            (k && t.width <= h[k - 1].width) || (t.warp_batch != 0 && t.warp_batch != 1))
+        const bool lane = t.lanes == 1;
+        if ((!lane && t.lanes != 4 && t.lanes != 8 && t.lanes != 16 && t.lanes != 32) ||
+            (!lane && t.tile != 5 && t.tile != 9 && t.tile != 13) || t.width < 1 ||
+            (k && t.width <= h[k - 1].width) || (t.warp_batch != 0 && t.warp_batch != 1) ||
+            (lane && (t.refill < 1 || t.refill > 32)))
             return G3X_ERR_INVALID;
     }
     ctx->tiles.n = n;
@@ -311,6 +381,7 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
         ctx->tiles.lanes[k] = h[k].lanes;
         ctx->tiles.tile[k] = h[k].tile;
         ctx->tiles.warp_batch[k] = h[k].warp_batch;
+        ctx->tiles.refill[k] = h[k].refill < 1 ? 1 : h[k].refill;
     }
     return G3X_OK;
 }
@@ -351,36 +422,43 @@ int g3x_autotune(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs
     int32_t oc[2 * g3x::kMaxBuckets];
     if (rc == G3X_OK && cudaMemcpy(oc, ctx->sched.bucket_oc, sizeof(oc), cudaMemcpyDeviceToHost) != cudaSuccess)
         rc = G3X_ERR_CUDA;
-    const int cand_l[] = {4, 4, 4, 8, 8, 8, 16, 16, 16, 32, 32, 32};
-    const int cand_c[] = {5, 9, 13, 5, 9, 13, 5, 9, 13, 5, 9, 13};
+    // Candidates per class: the lane-per-job kernel with refill waves of 1, 8 or 32 lanes
+    // (where a warp's working set fits), and row-parallel groups whose tile covers the class
+    // width (the unbounded class: 32-lane groups), each refilling per group or per warp.
+    struct Cand { int lanes, tile, wb, refill; };
+    Cand cands[64];
     g3x::TileTable best = ctx->tiles;
     for (int k = 0; k < ctx->tiles.n && rc == G3X_OK; ++k) {
         if (oc[2 * k + 1] == 0) continue;
+        const int width = std::min(ctx->tiles.width[k], max_qlen);
+        const bool last = k == ctx->tiles.n - 1;
+        int nc = 0;
+        if (!last && g3x::lane_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen), max_tlen) <= 200 * 1024)
+            for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 0, 0, rf};
+        for (int l : {4, 8, 16, 32})
+            for (int c : {5, 9, 13}) {
+                const int S = l * c;
+                if (last ? l != 32 : (S < width || S > 2 * width + 40)) continue;
+                for (int wb = 0; wb < 2; ++wb) cands[nc++] = Cand{l, c, wb, 1};
+            }
         float best_ms = 1e30f;
-        for (int cnd = 0; cnd < 12 && rc == G3X_OK; ++cnd) {
-            const int S = cand_l[cnd] * cand_c[cnd];
-            const int lo = k ? ctx->tiles.width[k - 1] : 0;
-            // candidates: single-tile ones no wider than 2x the class, plus the current one
-            if (!(S >= std::min(ctx->tiles.width[k], 4096) && S <= 2 * std::max(ctx->tiles.width[k], lo + 1)) &&
-                !(cand_l[cnd] == ctx->tiles.lanes[k] && cand_c[cnd] == ctx->tiles.tile[k]) &&
-                !(k == ctx->tiles.n - 1 && cand_l[cnd] == 32))
-                continue;
-            for (int wb = 0; wb < 2 && rc == G3X_OK; ++wb) {
-                g3x::TileTable tt = ctx->tiles;
-                tt.lanes[k] = cand_l[cnd]; tt.tile[k] = cand_c[cnd]; tt.warp_batch[k] = wb;
-                float ms = 0;
-                for (int rep = 0; rep < 2 && rc == G3X_OK; ++rep) {
-                    cudaMemsetAsync(ctx->d_queue, 0, g3x::kMaxBuckets * sizeof(int32_t), st);
-                    cudaEventRecord(e0, st);
-                    rc = g3x::launch_classes(ctx, base, sp, st, k, &tt);
-                    cudaEventRecord(e1, st);
-                    if (cudaEventSynchronize(e1) != cudaSuccess) rc = G3X_ERR_CUDA;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                }
-                if (rc == G3X_OK && ms < best_ms) {
-                    best_ms = ms;
-                    best.lanes[k] = cand_l[cnd]; best.tile[k] = cand_c[cnd]; best.warp_batch[k] = wb;
-                }
+        for (int ci = 0; ci < nc && rc == G3X_OK; ++ci) {
+            g3x::TileTable tt = ctx->tiles;
+            tt.lanes[k] = cands[ci].lanes; tt.tile[k] = cands[ci].tile;
+            tt.warp_batch[k] = cands[ci].wb; tt.refill[k] = cands[ci].refill;
+            float ms = 0;
+            for (int rep = 0; rep < 2 && rc == G3X_OK; ++rep) {
+                cudaMemsetAsync(ctx->d_queue, 0, g3x::kMaxBuckets * sizeof(int32_t), st);
+                cudaEventRecord(e0, st);
+                rc = g3x::launch_classes(ctx, base, sp, st, k, &tt);
+                cudaEventRecord(e1, st);
+                if (cudaEventSynchronize(e1) != cudaSuccess) rc = G3X_ERR_CUDA;
+                cudaEventElapsedTime(&ms, e0, e1);
+            }
+            if (rc == G3X_OK && ms < best_ms) {
+                best_ms = ms;
+                best.lanes[k] = tt.lanes[k]; best.tile[k] = tt.tile[k];
+                best.warp_batch[k] = tt.warp_batch[k]; best.refill[k] = tt.refill[k];
             }
         }
     }

@@ -38,6 +38,7 @@ struct LaunchDesc {
     int32_t blocks;        // persistent grid size (0 = derive from occupancy)
     int32_t warp_batch;    // persistent row-parallel: 1 = a warp pulls one job per group at
                            // once and waits for all of them; 0 = each group refills alone
+    int32_t refill;        // lane-per-job kernel: idle lanes that trigger a refill wave
 };
 
 // Tile configurations by job width class (ascending width; the last class is unbounded).
@@ -48,6 +49,7 @@ struct TileTable {
     int32_t lanes[kMaxBuckets];
     int32_t tile[kMaxBuckets];
     int32_t warp_batch[kMaxBuckets];
+    int32_t refill[kMaxBuckets];
 };
 
 // Device scratch of the scheduler and of the learned schedule (capacity >= n jobs).
@@ -62,10 +64,13 @@ int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScorePara
 
 constexpr int32_t kKernelRolling = 1;   // anti-diagonal wavefront, rows on lanes
 constexpr int32_t kKernelRowpar = 2;    // one row per step, columns on lanes
+constexpr int32_t kKernelLane = 3;      // one job per lane
 
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_rolling(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_rowpar(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+size_t lane_smem_per_warp(int qcap, int tcap);
 
 // Device scratch of one seed-level call (capacity >= n seeds).
 struct SeedScratch {

@@ -95,13 +95,15 @@ const char *g3x_strerror(int code);
 #define G3X_KERNEL_AUTO    0  /* rolling for G3X_SCHED_PLAIN, row-parallel otherwise */
 #define G3X_KERNEL_ROLLING 1  /* anti-diagonal wavefront: rows on lanes, 4-cell lane steps */
 #define G3X_KERNEL_ROWPAR  2  /* one row per step: columns on lanes, F by shuffle scan */
+#define G3X_KERNEL_LANE    3  /* one job per lane: the scalar row loop, 8-column blocks */
 
 typedef struct {
     int32_t schedule;     /* G3X_SCHED_* */
     int32_t max_qlen;     /* upper bound of qlen over the batch (required) */
     int32_t max_tlen;     /* upper bound of tlen over the batch (required) */
-    int32_t lanes;        /* lanes per job: 4 (row-parallel only), 8, 16, 32, or 0 = tuned;
-                             raised when a warp of such groups would not fit in shared memory */
+    int32_t lanes;        /* lanes per job: 1 (lane kernel), 4 (row-parallel only), 8, 16, 32,
+                             or 0 = tuned; raised when a warp of such groups would not fit in
+                             shared memory */
     int32_t tile;         /* row-parallel: cells per lane per tile (5, 9 or 13), 0 = tuned */
     int32_t kernel;       /* G3X_KERNEL_* */
     int32_t *d_cells;     /* optional per-job DP cell count (trip count of ksw.cu:346) */
@@ -122,10 +124,15 @@ int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
    row when its rows are wider than one tile).  Each
    class runs the row-parallel kernel with `lanes` lanes per job and `tile` cells per lane;
    `warp_batch` = 1 makes a warp pull one job per group at once and wait for all of them
-   (jobs then balance by the schedule's cost order), 0 lets each group refill on its own. */
+   (jobs then balance by the schedule's cost order), 0 lets each group refill on its own;
+   the lane-per-job kernel (lanes = 1) refills its idle lanes in waves of at least `refill`. */
 #define G3X_MAX_CLASSES 8
 typedef struct {
-    int32_t width, lanes, tile, warp_batch;
+    int32_t width;        /* widest query of the class (the last class: unbounded) */
+    int32_t lanes;        /* 1 = lane-per-job kernel; 4, 8, 16, 32 = row-parallel groups */
+    int32_t tile;         /* row-parallel: cells per lane per tile (5, 9, 13); lane kernel: 0 */
+    int32_t warp_batch;   /* 1: a warp takes its jobs together and waits for all of them */
+    int32_t refill;       /* lane kernel: idle lanes that trigger a refill wave (1-32) */
 } g3x_tile_t;
 
 int g3x_get_tiles(g3x_ctx *ctx, g3x_tile_t *h_tiles, int32_t *n);
@@ -193,6 +200,19 @@ int g3x_extend_seeds_stream(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t
                             int64_t n, const uint32_t *h_codes, const uint32_t *h_nmask,
                             int64_t n_bases, g3x_reg_t *h_regs, int32_t *h_status,
                             int32_t chunk, const g3x_batch_opts_t *opts);
+
+/* ---- CUDA graphs ------------------------------------------------------------------------- */
+/* Captures one g3x_ksw_extend2_batch call (all of its kernels and memsets, on the
+   context's streams) into an executable CUDA graph bound to these buffers and options;
+   g3x_graph_launch replays it on `stream`.  The captured batch reads its inputs when it runs,
+   so new jobs written into the same buffers are processed by the next replay. */
+typedef struct g3x_graph g3x_graph;
+int g3x_graph_capture(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs,
+                      int32_t n, const uint32_t *d_codes, const uint32_t *d_nmask,
+                      g3x_ext_t *d_out, int32_t *d_status, const g3x_batch_opts_t *opts,
+                      g3x_graph **graph);
+int g3x_graph_launch(g3x_graph *graph, void *stream);
+int g3x_graph_destroy(g3x_graph *graph);
 
 /* ---- learned cost model ------------------------------------------------------------------ */
 /* A 5 -> 64 -> 64 -> 1 ReLU MLP (fp32) per context that predicts a job's work from five

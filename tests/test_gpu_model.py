@@ -99,7 +99,7 @@ def test_warp_batched_classes_are_exact():
     c = ctx()
     tiles = c.get_tiles()
     try:
-        c.set_tiles([(w, l, t, 1) for (w, l, t, _) in tiles])
+        c.set_tiles([(w, l, t, 1, r) for (w, l, t, _, r) in tiles])
         ref, _, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
         out, status, _ = run_batch(wl.u8, wl.jobs, sc, g.SCHED_SORTED)
         assert (status == 0).all() and (out == ref).all()
@@ -107,3 +107,25 @@ def test_warp_batched_classes_are_exact():
         assert stats[0] > 0 and stats[2] > 0
     finally:
         c.set_tiles(tiles)
+
+
+def test_graph_capture_replays_exactly():
+    import torch
+    wl = g.synth(2, 8000, seed=21, w=100, unrelated=0.2)
+    sc = g.default_score()
+    codes, nmask = wl.planes()
+    d_jobs, d_codes, d_nmask = to_dev(wl.jobs), to_dev(codes), to_dev(nmask)
+    out = torch.zeros((wl.n, 6), dtype=torch.int32, device="cuda")
+    status = torch.full((wl.n,), 9, dtype=torch.int32, device="cuda")
+    mq, mt = int(wl.jobs["qlen"].max()), int(wl.jobs["tlen"].max())
+    ref, _, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
+    graph = ctx().capture_batch(sc, d_jobs, wl.n, d_codes, d_nmask, out, status, mq, mt,
+                                schedule=g.SCHED_SORTED)
+    for _ in range(2):
+        out.zero_()
+        status.fill_(9)
+        graph.launch()
+        torch.cuda.synchronize()
+        assert (status.cpu().numpy() == 0).all()
+        assert (out.cpu().numpy() == ref).all()
+    graph.close()

@@ -14,14 +14,17 @@ R, P = g.KERNEL_ROLLING, g.KERNEL_ROWPAR
 # (schedule, kernel, lanes, tile)
 SCHEDULES = [(g.SCHED_PLAIN, R, 0, 0), (g.SCHED_SORTED, R, 8, 0), (g.SCHED_SORTED, R, 16, 0),
              (g.SCHED_SORTED, R, 32, 0), (g.SCHED_PLAIN, P, 0, 9)] + \
-            [(g.SCHED_SORTED, P, l, t) for l in (4, 8, 16, 32) for t in (5, 9, 13)]
-IDS = [f"{'plain' if s == 0 else 'pers'}-{'roll' if k == R else 'row'}-g{l}-c{t}" for s, k, l, t in SCHEDULES]
+            [(g.SCHED_SORTED, P, l, t) for l in (4, 8, 16, 32) for t in (5, 9, 13)] + \
+            [(g.SCHED_SORTED, g.KERNEL_LANE, 1, rf) for rf in (1, 8, 32)]
+IDS = [f"{'plain' if s == 0 else 'pers'}-{ {R: 'roll', P: 'row', 3: 'lane'}[k]}-g{l}-c{t}" for s, k, l, t in SCHEDULES]
 
 
 @pytest.mark.parametrize("sched,kernel,lanes,tile", SCHEDULES, ids=IDS)
 @pytest.mark.parametrize("name", golden_io.job_sets())
 def test_gpu_matches_golden(name, sched, kernel, lanes, tile):
     u8, jobs, score, ext = golden_io.load_jobs(name)
+    if kernel == g.KERNEL_LANE and jobs["qlen"].max() > 1000:
+        pytest.skip("the lane-per-job kernel holds each lane's query in shared memory (short queries)")
     out, status, cells = run_batch(u8, jobs, score, sched, lanes, tile=tile, kernel=kernel)
     assert (status == 0).all(), np.unique(status)
     bad = np.nonzero((out != ext).any(1))[0]
@@ -31,6 +34,8 @@ def test_gpu_matches_golden(name, sched, kernel, lanes, tile):
 @pytest.mark.parametrize("sched,kernel,lanes,tile", SCHEDULES, ids=IDS)
 @pytest.mark.parametrize("kind,n,w", [(1, 30000, 100), (2, 15000, 100), (4, 150, 100), (4, 150, 500)])
 def test_gpu_matches_oracle_fresh(kind, n, w, sched, kernel, lanes, tile):
+    if kernel == g.KERNEL_LANE and kind == 4:
+        pytest.skip("the lane-per-job kernel holds each lane's query in shared memory (short queries)")
     wl = g.synth(kind, n, seed=0x6A5 + 100 * kind + w, w=w, unrelated=0.2 if kind == 2 else 0.0)
     sc = g.default_score()
     ref, rcells, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
