@@ -165,13 +165,16 @@ def run_reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def timed_steps(fn, k, w, stream, flush):
+def timed_steps(fn, k, w, stream, flush, nvtx=None):
     """W untimed calls, then K calls each bracketed by CUDA events on `stream`, with a
-    256 MiB write between them so no step starts with the previous step's data in L2."""
+    256 MiB write between them so no step starts with the previous step's data in L2.  With
+    `nvtx`, the K timed calls sit inside an NVTX range of that name (for profiler filters)."""
     import torch
     for _ in range(w):
         fn()
     ms = []
+    if nvtx:
+        torch.cuda.nvtx.range_push(nvtx)
     for _ in range(k):
         flush.fill_(1)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -181,6 +184,8 @@ def timed_steps(fn, k, w, stream, flush):
         e1.record(stream)
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
+    if nvtx:
+        torch.cuda.nvtx.range_pop()
     return ms
 
 
@@ -239,8 +244,10 @@ def main():
     cells = int(cells_np.astype(np.int64).sum())
     plain_out = d_out.cpu().numpy().copy()
 
-    # Learned cost model: trained on the GPU on config-1 traces from the plain kernel.
-    train_metrics = learn.train(ctx, n_train=2_000_000, seed_train=0xA11CE + rank)
+    # Learned cost model: trained on the GPU on plain-kernel traces of a held-out batch of the
+    # same generator (another seed), about 2M jobs.
+    train_metrics = learn.train(ctx, n_train=max(1, 2_000_000 * units // max(n, 1)),
+                                seed_train=0xA11CE + rank, kind=kind_, w=w, unrelated=unrel)
     pred_err = learn.prediction_error(ctx, d_jobs, n, d_codes, d_nmask, cells_np)
 
     # Autotune the width classes on this batch (length-sorted order), then capture graphs.
@@ -268,7 +275,7 @@ def main():
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
-    ms = timed_steps(main_fn, args.steps, args.warmup, stream, flush)
+    ms = timed_steps(main_fn, args.steps, args.warmup, stream, flush, nvtx="bench_timed")
     barrier()
     clk = clocks.stop()
     t_step = sum(ms) / len(ms)

@@ -1,7 +1,7 @@
 """Training workflow of the learned cost model (host orchestration over the C ABI).
 
-Traces come from the method itself: synthetic right-extension jobs (the config-1 generator)
-are extended by the plain kernel, whose per-job cell counters are the targets
+Traces come from the method itself: a held-out synthetic batch of the workload to be scheduled
+(same generator kind, another seed) is extended by the plain kernel, whose per-job cell counters are the targets
 (log2(1 + cells)); the features come from the library's feature kernel; the 5 -> 64 -> 64 -> 1
 MLP is trained on the GPU by the library's own forward/backward/Adam kernels
 (g3x_mlp_train).  Everything runs on the device; only the loss curve comes back.
@@ -18,11 +18,12 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).cuda()
 
 
-def traces(ctx, n, seed, w=100, unrelated=0.2, score=None):
-    """(features [n,5] device, targets [n] device, cells numpy) from n config-1 jobs."""
+def traces(ctx, n, seed, kind=1, w=100, unrelated=0.2, score=None):
+    """(features [m,5] device, targets [m] device, cells numpy) from the m jobs the generator
+    `kind` makes for n units (jobs for kind 1, seeds for kind 2, segments for kind 4)."""
     import torch
     score = g.default_score() if score is None else score
-    wl = g.synth(1, n, seed=seed, w=w, unrelated=unrelated)
+    wl = g.synth(kind, n, seed=seed, w=w, unrelated=unrelated)
     codes, nmask = wl.planes()
     d_jobs, d_codes, d_nmask = _dev(wl.jobs), _dev(codes), _dev(nmask)
     out = torch.zeros((wl.n, 6), dtype=torch.int32, device="cuda")
@@ -40,15 +41,18 @@ def traces(ctx, n, seed, w=100, unrelated=0.2, score=None):
     return feat, target, cells.cpu().numpy()
 
 
-def train(ctx, n_train=2_000_000, seed_train=0xA11CE, epochs=4, batch=4096, lr=2e-3, init_seed=17):
-    """Trains the context's model on n_train config-1 traces; returns a metrics dict."""
+def train(ctx, n_train=2_000_000, seed_train=0xA11CE, epochs=4, batch=4096, lr=2e-3, init_seed=17,
+          kind=1, w=100, unrelated=0.2):
+    """Trains the context's model on the traces of n_train generator units; returns a metrics
+    dict."""
     t0 = time.perf_counter()
-    feat, target, _ = traces(ctx, n_train, seed_train)
+    feat, target, _ = traces(ctx, n_train, seed_train, kind=kind, w=w, unrelated=unrelated)
+    m = int(target.shape[0])
     t1 = time.perf_counter()
     ctx.mlp_init(init_seed)
-    losses = ctx.mlp_train(feat, target, n_train, epochs, batch, lr, seed=init_seed)
+    losses = ctx.mlp_train(feat, target, m, epochs, batch, lr, seed=init_seed)
     t2 = time.perf_counter()
-    return {"traces": n_train, "trace_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3),
+    return {"traces": m, "trace_kind": kind, "trace_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3),
             "epochs": epochs, "batch": batch, "lr": lr, "loss_curve": [round(float(x), 5) for x in losses],
             "params": g.MLP_PARAMS}
 
