@@ -222,6 +222,7 @@ const char* g3x_strerror(int code) {
         case G3X_ERR_INTERNAL: return "device consistency check failed";
         case G3X_ERR_NOMEM: return "out of device memory for library scratch";
         case G3X_ERR_NOT_TRAINED: return "learned schedule requested before a model was set";
+        case G3X_ERR_SCRATCH: return "batch exceeds the static scratch of g3x_ksw_extend2_batch_noalloc (at most G3X_NOALLOC_MAX_JOBS = 1048576 jobs)";
         default: return "unknown error";
     }
 }

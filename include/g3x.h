@@ -46,6 +46,7 @@ extern "C" {
 #define G3X_ERR_INTERNAL      -6   /* a device-side consistency check failed (per-job) */
 #define G3X_ERR_NOMEM         -7   /* allocation of library-owned scratch failed */
 #define G3X_ERR_NOT_TRAINED   -8   /* learned schedule requested before a model was set */
+#define G3X_ERR_SCRATCH       -9   /* batch larger than the fixed scratch of a no-alloc call */
 
 /* ---- data records -------------------------------------------------------------------- */
 
@@ -116,6 +117,23 @@ int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
                           int32_t n, const uint32_t *d_codes, const uint32_t *d_nmask,
                           g3x_ext_t *d_out, int32_t *d_status, const g3x_batch_opts_t *opts,
                           void *stream);
+
+/* No counterpart in the reference: a variant of g3x_ksw_extend2_batch with G3X_SCHED_SORTED
+   (same width classes and kernels, same outputs) that allocates nothing.  For callers that
+   must not allocate device memory while they run: a pipeline stage between other stages'
+   kernels, where cudaMalloc/cudaFree would synchronise the device; a process that reserved
+   the GPU's memory up front (as the reference's device_alloc does); a framework whose
+   allocator owns all device memory.  It needs no context: its scratch (sort keys, job order,
+   histogram, per-class job counters) is one static device array of the library, 8.06 MiB,
+   looked up once per device.  At most G3X_NOALLOC_MAX_JOBS jobs per call, else
+   G3X_ERR_SCRATCH.  All calls on a device share that array: calls that overlap on the GPU
+   (two streams, two host threads) race and corrupt each other's results, so serialise them.
+   Makes `device` current.  Asynchronous on `stream`. */
+#define G3X_NOALLOC_MAX_JOBS 1048576
+int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t *score, const g3x_job_t *d_jobs,
+                                  int32_t n, const uint32_t *d_codes, const uint32_t *d_nmask,
+                                  g3x_ext_t *d_out, int32_t *d_status, int32_t max_qlen,
+                                  int32_t max_tlen, void *stream);
 
 /* ---- schedule tuning ----------------------------------------------------------------------- */
 /* The persistent schedules split a batch into width classes: a job belongs to the first class
