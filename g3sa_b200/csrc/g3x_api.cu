@@ -3,6 +3,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <algorithm>
+#include <cmath>
 #include <new>
 #include "g3x_internal.h"
 
@@ -49,14 +50,16 @@ int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d) {
     if (opts->schedule != G3X_SCHED_PLAIN && opts->schedule != G3X_SCHED_SORTED &&
         opts->schedule != G3X_SCHED_LEARNED)
         return G3X_ERR_INVALID;
-    if (opts->kernel < G3X_KERNEL_AUTO || opts->kernel > G3X_KERNEL_LANE) return G3X_ERR_INVALID;
+    if (opts->kernel < G3X_KERNEL_AUTO || opts->kernel > G3X_KERNEL_LANE16) return G3X_ERR_INVALID;
     const bool plain = opts->schedule == G3X_SCHED_PLAIN;
     d->kernel = opts->kernel == G3X_KERNEL_AUTO ? (plain ? kKernelRolling : kKernelRowpar)
                 : opts->kernel == G3X_KERNEL_ROLLING ? kKernelRolling
-                : opts->kernel == G3X_KERNEL_ROWPAR ? kKernelRowpar : kKernelLane;
-    if (d->kernel == kKernelLane) {
-        if (plain) return G3X_ERR_INVALID;            // the lane kernel is persistent only
-        d->lanes = 1; d->tile = 0; d->persistent = 1; d->warps_per_block = 4; d->queue = queue;
+                : opts->kernel == G3X_KERNEL_ROWPAR ? kKernelRowpar
+                : opts->kernel == G3X_KERNEL_LANE ? kKernelLane : kKernelLane16;
+    if (d->kernel == kKernelLane || d->kernel == kKernelLane16) {
+        if (plain) return G3X_ERR_INVALID;            // the lane kernels are persistent only
+        d->lanes = 1; d->tile = d->kernel == kKernelLane16 ? 2 : 0;
+        d->persistent = 1; d->warps_per_block = 4; d->queue = queue;
         d->refill = opts->tile > 0 ? opts->tile : 1;  // tile carries the refill threshold
         return G3X_OK;
     }
@@ -122,7 +125,7 @@ static int alloc_sched(SchedScratch& s, int64_t n) {
     if (n <= s.cap && s.order) return G3X_OK;
     free_sched(s);
     const int64_t cap = std::max<int64_t>(n, 1024);
-    const int bins = kMaxBuckets * 1024;
+    const int bins = kMaxBuckets * kSchedLevels;
     if (cudaMalloc(&s.bin, cap * sizeof(int32_t)) || cudaMalloc(&s.order, cap * sizeof(int32_t)) ||
         cudaMalloc(&s.hist, bins * sizeof(int32_t)) || cudaMalloc(&s.cursor, bins * sizeof(int32_t)) ||
         cudaMalloc(&s.bucket_oc, 2 * kMaxBuckets * sizeof(int32_t)) ||
@@ -162,7 +165,7 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
         if (only >= 0 && k != only) continue;
         if (cudaStreamWaitEvent(ctx->side[k], ctx->fork, 0) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
         LaunchDesc d = base;
-        d.kernel = tt.lanes[k] == 1 ? kKernelLane : kKernelRowpar;
+        d.kernel = tt.lanes[k] != 1 ? kKernelRowpar : tt.tile[k] == 2 ? kKernelLane16 : kKernelLane;
         d.lanes = tt.lanes[k];
         d.tile = tt.tile[k];
         d.warp_batch = tt.warp_batch[k];
@@ -177,6 +180,8 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
         d.stats = ctx->d_stats;
         if (d.kernel == kKernelLane) {
             rc = launch_lane(d, sp, ctx->side[k]);
+        } else if (d.kernel == kKernelLane16) {
+            rc = launch_lane16(d, sp, ctx->side[k]);
         } else {
             while (d.lanes < 32 && (32 / d.lanes) * group_smem_bytes(d.qmax, d.tmax) > 227 * 1024) d.lanes *= 2;
             rc = launch_rowpar(d, sp, ctx->side[k]);
@@ -371,7 +376,8 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
         const g3x_tile_t& t = h[k];
         const bool lane = t.lanes == 1;
         if ((!lane && t.lanes != 4 && t.lanes != 8 && t.lanes != 16 && t.lanes != 32) ||
-            (!lane && t.tile != 5 && t.tile != 9 && t.tile != 13) || t.width < 1 ||
+            (!lane && t.tile != 5 && t.tile != 9 && t.tile != 13) || (lane && t.tile != 0 && t.tile != 2) ||
+            t.width < 1 ||
             (k && t.width <= h[k - 1].width) || (t.warp_batch != 0 && t.warp_batch != 1) ||
             (lane && (t.refill < 1 || t.refill > 32)))
             return G3X_ERR_INVALID;
@@ -416,6 +422,27 @@ int g3x_autotune(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs
     base.jobs = d_jobs; base.codes = d_codes; base.nmask = d_nmask; base.out = out; base.status = status;
     base.n = n; base.qmax = max_qlen; base.tmax = max_tlen;
     cudaStream_t st = nullptr;
+    // Class widths follow the batch: up to seven classes at max_qlen * (k/7)^1.5, rounded up to
+    // eight columns, then the unbounded class.  A class's shared memory per job is sized by its
+    // width, so narrow steps near the bulk of the queries waste little of it.
+    {
+        g3x::TileTable t;
+        t.n = 0;
+        for (int k = 1; k <= 7; ++k) {
+            const double f = (double)k / 7.0;
+            int wk = (int)(max_qlen * f * std::sqrt(f) + 0.999);
+            wk = std::max(8, (wk + 7) & ~7);
+            if (t.n && wk <= t.width[t.n - 1]) continue;
+            t.width[t.n] = wk;
+            t.lanes[t.n] = 4;
+            while (t.lanes[t.n] < 32 && t.lanes[t.n] * 9 < wk) t.lanes[t.n] *= 2;
+            t.tile[t.n] = 9; t.warp_batch[t.n] = 0; t.refill[t.n] = 1;
+            ++t.n;
+        }
+        t.width[t.n] = 0x7FFFFFFF; t.lanes[t.n] = 32; t.tile[t.n] = 9; t.warp_batch[t.n] = 0; t.refill[t.n] = 1;
+        ++t.n;
+        ctx->tiles = t;
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -436,6 +463,8 @@ int g3x_autotune(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs
         int nc = 0;
         if (!last && g3x::lane_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen), max_tlen) <= 200 * 1024)
             for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 0, 0, rf};
+        if (!last && g3x::lane16_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen)) <= 200 * 1024)
+            for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 2, 0, rf};
         for (int l : {4, 8, 16, 32})
             for (int c : {5, 9, 13}) {
                 const int S = l * c;

@@ -121,6 +121,30 @@ G3X_HD bool job_is_narrow(const JobConst& c, int32_t max_sc) {
     return hmax < 32768 && c.qlen < 65535;
 }
 
+// The lane-per-job kernel keeps H and E of a job in 16-bit fields: it takes narrow jobs with
+// h0 >= 0 (its M = min(H + S, 256 H) form needs H >= 0).
+G3X_HD bool job_fits_lane(const JobConst& c, int32_t max_sc) {
+    return c.h0 >= 0 && job_is_narrow(c, max_sc);
+}
+
+// Shift k of the int16x2 kernel's M = min(H + S, H << k): the smallest k with 2^k >= 1 + max_sc,
+// so that H << k >= H + S for every H > 0.
+G3X_HD int32_t int16_shift(int32_t max_sc) {
+    int32_t k = 0;
+    while ((1 << k) < 1 + max_sc && k < 15) ++k;
+    return k;
+}
+
+// A job fits the int16x2 kernel when every value of its DP, H << k included, stays below 2^15:
+// 0 <= H <= h0 + max_sc * min(qlen, tlen) (E and F are bounded by H), and the penalties keep
+// M - o - e above -2^15.
+G3X_HD bool job_fits_int16(const JobConst& c, int32_t max_sc) {
+    if (c.h0 < 0 || c.qlen >= 65535 || c.oe_del >= 16384 || c.oe_ins >= 16384) return false;
+    const int64_t mn = c.qlen < c.tlen ? c.qlen : c.tlen;
+    const int64_t hmax = (int64_t)c.h0 + (int64_t)(max_sc > 0 ? max_sc : 0) * mn;
+    return (hmax << int16_shift(max_sc)) < 32768;
+}
+
 G3X_HD void commit_init(Commit& k, const JobConst& c) {
     k.next = 0;
     k.stop = c.tlen <= 0;

@@ -52,6 +52,9 @@ struct TileTable {
     int32_t refill[kMaxBuckets];
 };
 
+// Sort bins per width class of schedule_jobs (its histogram holds kMaxBuckets * kSchedLevels).
+constexpr int kSchedLevels = 2048;
+
 // Device scratch of the scheduler and of the learned schedule (capacity >= n jobs).
 struct SchedScratch {
     int32_t *bin = nullptr, *order = nullptr, *hist = nullptr, *cursor = nullptr;
@@ -65,11 +68,14 @@ int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScorePara
 constexpr int32_t kKernelRolling = 1;   // anti-diagonal wavefront, rows on lanes
 constexpr int32_t kKernelRowpar = 2;    // one row per step, columns on lanes
 constexpr int32_t kKernelLane = 3;      // one job per lane
+constexpr int32_t kKernelLane16 = 4;    // two jobs per lane, int16x2
 
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_rolling(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_rowpar(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+int launch_lane16(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+size_t lane16_smem_per_warp(int qcap);
 size_t lane_smem_per_warp(int qcap, int tcap);
 
 // Device scratch of one seed-level call (capacity >= n seeds).

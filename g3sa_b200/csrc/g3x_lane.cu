@@ -1,23 +1,28 @@
 // g3x_lane.cu -- lane-per-job sm_100a kernel for batched ksw_extend2 (bwa/src/ksw.cu:303-401).
 //
 // Each lane of a warp runs one job through the reference's own row loop: rows in order, the
-// reference's band [beg, end) per row (ksw.cu:338-340, 388-391), and the per-row bookkeeping
-// of ksw.cu:371-386 -- so the semantics are the scalar loop's by construction.  A lane walks
-// its current row in aligned blocks of eight columns; when it reaches the row's end it does
-// the row bookkeeping and starts the next row (that step diverges from the lanes still inside
-// their rows, and is short).  The 32 jobs of a warp are chosen by the scheduler to need
-// similar work, so the lanes stay busy together.
+// reference's band [beg, end) per row (ksw.cu:338-340, 388-391) and the per-row bookkeeping of
+// ksw.cu:371-386, so the semantics are the scalar loop's by construction.  The warp is
+// row-synchronous: every lane starts its job's next row at the same time, walks it in aligned
+// blocks of eight columns (the first and last block of a row masked to [beg, end), the blocks
+// between them unmasked), and all lanes do the row-end bookkeeping together.  The 32 jobs of a
+// warp are chosen by the scheduler to have rows of similar width, so few lanes wait.
 //
-// Shared memory holds each lane's job in a lane-interleaved layout, so that every access of
-// the warp is free of bank conflicts whatever column each lane is at:
-//   eh   : the row buffer (ksw.cu:310) as 16-bit H | 16-bit E words ("narrow" jobs only,
-//          H <= h0 + max_score * min(qlen, tlen) < 2^15); slot k of lane L is word
-//          ((k/4)*32 + L)*4 + k%4, so a lane's aligned 8-column block is two 16-byte loads
-//   qnib : query codes, eight 4-bit codes per word; a byte permute of the row's score pool
-//          turns four codes into four scores
-//   tnib : target codes, eight 4-bit codes per word
-// Idle lanes are refilled in waves: when at least `refill` lanes of the warp are idle, the
-// whole warp stages one new job per idle lane together (all lanes decode each job).
+// Per cell the lane keeps no bookkeeping besides its running H and F: the row maximum is taken
+// per block (three-input maxima), and the column that reaches it (the last one, ksw.cu:364) is
+// found at row end among the eight H values of the winning block, which the row buffer holds
+// (eh[c+1].h = H(i, c), ksw.cu:350 and 371).  The next row's band is found as the reference
+// finds it, by scanning the row buffer from both ends (ksw.cu:388-391); beg only grows and end
+// regrows by at most two columns per row, so the scans take O(1) steps per row on average.
+//
+// Shared memory holds, per lane, the row buffer (ksw.cu:310) as 16-bit H | 16-bit E words
+// (jobs with 0 <= h0 and H <= h0 + max_score * min(qlen, tlen) < 2^15) and the query as 4-bit
+// codes, both lane-interleaved so that every access of the warp is free of bank conflicts
+// whatever column each lane is at: row-buffer slot k of lane L is word ((k/4)*32 + L)*4 + k%4,
+// so an aligned 8-column block is two 16-byte loads.  The target is read from the packed
+// planes in global memory, sixteen codes at a time, one chunk ahead.  Idle lanes are refilled
+// in waves at row boundaries: when at least `refill` lanes of the warp are idle, the whole warp
+// stages one new job per idle lane together.
 #include <cuda_runtime.h>
 #include "g3x_core.h"
 #include "g3x_internal.h"
@@ -35,50 +40,118 @@ __host__ __device__ inline int lane_eh_words(int qcap) { return (qcap + 8 + kLB 
 __device__ __forceinline__ int ehw(int k, int L) { return (((k >> 2) * 32 + L) << 2) + (k & 3); }
 __host__ __device__ inline int lane_nib_words(int len) { return (len + 7) / 8 + 2; }
 
+// Byte t of x, sign-extended (prmt with the sign-replicating selector for bytes 1-3).
+template <int t>
+__device__ __forceinline__ int32_t sbyte(uint32_t x) {
+    constexpr uint32_t sel = (uint32_t)t | ((8u | t) << 4) | ((8u | t) << 8) | ((8u | t) << 12);
+    uint32_t r;
+    asm("prmt.b32 %0, %1, 0, %2;" : "=r"(r) : "r"(x), "n"(sel));
+    return (int32_t)r;
+}
+
 struct LaneJob {
     int job;                 // job index, -1 = none
     int32_t qlen, tlen, w, h0;
-    Commit K;
-    int32_t i, beg, end, j;  // row, band, next column
-    int32_t h1, f, key, fnz, lnz;
-    uint32_t pool_lo, pool_hi;   // this row's scores by query code (byte permute pools)
+    uint32_t t_off;
+    int32_t trev;
+    Commit K;                // K.next is the row to run next
+    int32_t beg, end;        // that row's band before the clamps of ksw.cu:338-340
+    uint32_t tx, tn, px, pn; // target codes / N bits of chunk K.next >> 4 and of the next chunk
 };
 
+// State of the row a lane is running.
+struct RowState {
+    int32_t beg, end, h1, f, m, mjb;
+    uint32_t plo, phi;       // this row's scores by query code (byte permute pools)
+};
 
-__device__ __forceinline__ int32_t tcode_at(const uint32_t* tn, int lane, int i) {
-    const uint32_t nib = (tn[(i >> 3) * 32 + lane] >> ((i & 7) << 2)) & 15u;
-    return nib < 4u ? (int32_t)nib : 4;
+// One aligned block of eight columns at jb (ksw.cu:346-370).  M = H(i-1,j-1) ? H(i-1,j-1) + S : 0
+// is min(H + S, 256 H): equal when H > 0, and <= 0 when H == 0, which every use clips to 0
+// exactly like the reference's 0.  Writes eh[col] = {H(i, col-1), E(i+1, col)}.  kMasked blocks
+// leave columns outside [beg, end) untouched.
+// The row-buffer words and query codes of the block at jb.
+struct BlockIn {
+    uint4 wa, wb;
+    uint32_t qw;
+};
+
+__device__ __forceinline__ BlockIn load_block(const uint32_t* __restrict__ eh, const uint32_t* __restrict__ qn,
+                                              int lane, int32_t jb) {
+    const uint32_t* ep = eh + ehw(jb, lane);
+    BlockIn b;
+    b.wa = *reinterpret_cast<const uint4*>(ep);
+    b.wb = *reinterpret_cast<const uint4*>(ep + 128);
+    b.qw = qn[(jb >> 3) * 32 + lane];
+    return b;
 }
 
-// Begins row J.i: band clamps, first-column value, row score pool (ksw.cu:335-345).  `pools`
-// holds, per target code t, the byte-permute pool of its scores (bytes 0-3: vs query codes
-// 0-3, bytes 4-7: vs N), in shared memory so that t can index it.
-__device__ __forceinline__ void begin_row(LaneJob& J, const ScoreParams& sp, const uint32_t* tn, int lane,
-                                          const uint2* pools) {
-    const int32_t i = J.i;
-    if (J.beg < i - J.w) J.beg = i - J.w;
-    if (J.end > i + J.w + 1) J.end = i + J.w + 1;
-    if (J.end > J.qlen) J.end = J.qlen;
-    if (J.beg == 0) {
-        const int32_t h = J.h0 - (sp.o_del + sp.e_del * (i + 1));
-        J.h1 = h > 0 ? h : 0;
-    } else {
-        J.h1 = 0;
+template <bool kMasked>
+__device__ __forceinline__ void lane_block(uint32_t* __restrict__ eh, const BlockIn& in,
+                                           int lane, int32_t jb, RowState& r, const ScoreParams& sp) {
+    uint32_t* ep = eh + ehw(jb, lane);
+    const uint4 wa = in.wa, wb = in.wb;
+    const uint32_t wv[kLB] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+    const uint32_t qw = in.qw;
+    const uint32_t sc_lo = __byte_perm(r.plo, r.phi, qw);
+    const uint32_t sc_hi = __byte_perm(r.plo, r.phi, qw >> 16);
+    uint32_t ov[kLB];
+    int32_t hv[kLB];
+    int32_t h1 = r.h1, f = r.f;
+#pragma unroll
+    for (int t = 0; t < kLB; ++t) {
+        const uint32_t w = wv[t];
+        const int32_t hd = (int32_t)(w >> 16), ed = (int32_t)(w & 0xFFFFu);
+        int32_t s;
+        switch (t & 3) {
+            case 0: s = sbyte<0>(t < 4 ? sc_lo : sc_hi); break;
+            case 1: s = sbyte<1>(t < 4 ? sc_lo : sc_hi); break;
+            case 2: s = sbyte<2>(t < 4 ? sc_lo : sc_hi); break;
+            default: s = sbyte<3>(t < 4 ? sc_lo : sc_hi); break;
+        }
+        const int32_t M = addmin_i32(hd, s, hd * 256);
+        const int32_t h = max3_i32(M, ed, f);
+        const int32_t te = addmax_i32(M, -sp.oe_del, 0);
+        const int32_t e2 = addmax_i32(ed, -sp.e_del, te);
+        const uint32_t nw = __byte_perm((uint32_t)e2, (uint32_t)h1, 0x5410);
+        const int32_t tf = addmax_i32(M, -sp.oe_ins, 0);
+        const int32_t fn = addmax_i32(f, -sp.e_ins, tf);
+        if (kMasked) {
+            const int32_t col = jb + t;
+            const bool valid = col >= r.beg && col < r.end;
+            ov[t] = valid ? nw : w;
+            hv[t] = valid ? h : -1;
+            if (valid) { f = fn; h1 = h; }
+        } else {
+            ov[t] = nw;
+            hv[t] = h;
+            f = fn;
+            h1 = h;
+        }
     }
-    J.j = J.beg;
-    J.f = 0; J.key = -1; J.fnz = 0x7FFFFFFF; J.lnz = -1;
-    const uint2 p = pools[tcode_at(tn, lane, i)];
-    J.pool_lo = p.x;
-    J.pool_hi = p.y;
+    *reinterpret_cast<uint4*>(ep) = make_uint4(ov[0], ov[1], ov[2], ov[3]);
+    *reinterpret_cast<uint4*>(ep + 128) = make_uint4(ov[4], ov[5], ov[6], ov[7]);
+    const int32_t bm = max3_i32(max3_i32(hv[0], hv[1], hv[2]), max3_i32(hv[3], hv[4], hv[5]),
+                                hv[6] > hv[7] ? hv[6] : hv[7]);
+    if (bm >= r.m) { r.m = bm; r.mjb = jb; }   // ties: the later block holds the later column
+    r.h1 = h1;
+    r.f = f;
+}
+
+__device__ __forceinline__ JobConst job_const(const LaneJob& J, const ScoreParams& sp) {
+    JobConst c;
+    c.qlen = J.qlen; c.tlen = J.tlen; c.w = J.w; c.h0 = J.h0;
+    c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
+    c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
+    return c;
 }
 
 }  // namespace
 
-__host__ __device__ inline size_t lane_warp_bytes(int qcap, int tcap) {
-    return (size_t)128 * (lane_eh_words(qcap) + lane_nib_words(qcap) + lane_nib_words(tcap));
+__host__ __device__ inline size_t lane_warp_bytes(int qcap) {
+    return (size_t)128 * (lane_eh_words(qcap) + lane_nib_words(qcap));
 }
 
-size_t lane_smem_per_warp(int qcap, int tcap) { return lane_warp_bytes(qcap, tcap); }
+size_t lane_smem_per_warp(int qcap, int tcap) { (void)tcap; return lane_warp_bytes(qcap); }
 
 __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp) {
     extern __shared__ __align__(16) char smem[];
@@ -94,10 +167,9 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int qcap = d.qmax, tcap = d.tmax;
-    uint32_t* base = reinterpret_cast<uint32_t*>(smem + (size_t)warp * lane_warp_bytes(qcap, tcap));
+    uint32_t* base = reinterpret_cast<uint32_t*>(smem + (size_t)warp * lane_warp_bytes(qcap));
     uint32_t* eh = base;                                         // [slot*32 + lane]
     uint32_t* qn = eh + 32 * lane_eh_words(qcap);                // [word*32 + lane]
-    uint32_t* tn = qn + 32 * lane_nib_words(qcap);
     const int n = d.count ? *d.count : d.n;
     const int* order = d.order ? d.order + (d.order_off ? *d.order_off : 0) : nullptr;
     const int refill = d.warp_batch ? 32 : (d.refill > 0 ? d.refill : 1);
@@ -129,7 +201,7 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                     c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
                     c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
                     c.w = clamp_w(jb.w, c.qlen, sp.max_sc, sp.end_bonus, sp.o_del, sp.e_del, sp.o_ins, sp.e_ins);
-                    if (c.qlen > qcap || c.tlen > tcap || !job_is_narrow(c, sp.max_sc)) {
+                    if (c.qlen > qcap || c.tlen > tcap || !job_fits_lane(c, sp.max_sc)) {
                         d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
                         d.status[job] = G3X_ERR_TOO_LONG;
                         if (d.cells) d.cells[job] = 0;
@@ -137,9 +209,13 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                         my_job = job;
                         J.job = job;
                         J.qlen = c.qlen; J.tlen = c.tlen; J.w = c.w; J.h0 = c.h0;
+                        J.t_off = jb.t_off;
+                        J.trev = (jb.flags & G3X_JOB_TREV) != 0;
                         commit_init(J.K, c);
-                        J.i = 0; J.beg = 0; J.end = c.qlen;
-                        J.j = -1;                          // row 0 not begun
+                        J.beg = 0; J.end = c.qlen;
+                        J.tx = J.tn = J.px = J.pn = 0;
+                        if (c.tlen > 0) load16(d.codes, d.nmask, J.t_off, c.tlen, 0, J.trev, J.tx, J.tn);
+                        if (c.tlen > 16) load16(d.codes, d.nmask, J.t_off, c.tlen, 1, J.trev, J.px, J.pn);
                     }
                 }
             }
@@ -149,21 +225,14 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                 m &= m - 1;
                 const int job = __shfl_sync(0xFFFFFFFFu, my_job, L);
                 const g3x_job_t jb = d.jobs[job];
-                const int qlen = jb.qlen, tlen = jb.tlen;
-                const bool qrev = (jb.flags & G3X_JOB_QREV) != 0, trev = (jb.flags & G3X_JOB_TREV) != 0;
+                const int qlen = jb.qlen;
+                const bool qrev = (jb.flags & G3X_JOB_QREV) != 0;
                 for (int ch = lane; (ch << 4) < qlen; ch += 32) {
                     uint32_t x, nb;
                     load16(d.codes, d.nmask, jb.q_off, qlen, ch, qrev, x, nb);
                     const uint64_t v = nibbles16(x, nb);
                     qn[(2 * ch) * 32 + L] = (uint32_t)v;
                     qn[(2 * ch + 1) * 32 + L] = (uint32_t)(v >> 32);
-                }
-                for (int ch = lane; (ch << 4) < tlen; ch += 32) {
-                    uint32_t x, nb;
-                    load16(d.codes, d.nmask, jb.t_off, tlen, ch, trev, x, nb);
-                    const uint64_t v = nibbles16(x, nb);
-                    tn[(2 * ch) * 32 + L] = (uint32_t)v;
-                    tn[(2 * ch + 1) * 32 + L] = (uint32_t)(v >> 32);
                 }
                 JobConst c;
                 c.qlen = qlen; c.h0 = jb.h0; c.oe_ins = sp.oe_ins; c.e_ins = sp.e_ins;
@@ -176,72 +245,91 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
             if (exhausted) break;
             continue;
         }
-        if (active) ++busy; else ++idle;
-        // A freshly staged job begins its first row (a job with tlen == 0 has none).
-        if (active && !J.K.stop && J.j < 0) begin_row(J, sp, tn, lane, pools);
-        if (active && !J.K.stop) {
-            // ---- one block of up to eight columns of the current row ----
-            if (J.j < J.end) {
-                const int32_t jb = J.j & ~(kLB - 1);
-                const uint32_t qw = qn[(jb >> 3) * 32 + lane];
-                // the block's eight slots, loaded up front (slots past the row are never used)
-                uint32_t* ep = eh + ehw(jb, lane);
-                const uint4 wa = *reinterpret_cast<const uint4*>(ep);
-                const uint4 wb = *reinterpret_cast<const uint4*>(ep + 128);
-                const uint32_t wv[kLB] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
-                const uint32_t sc_lo = __byte_perm(J.pool_lo, J.pool_hi, qw & 0xFFFFu);
-                const uint32_t sc_hi = __byte_perm(J.pool_lo, J.pool_hi, qw >> 16);
-                int32_t h1 = J.h1, f = J.f, key = J.key, fnz = J.fnz, lnz = J.lnz;
-                const int32_t lo = J.j, hi = J.end;
+        // A job staged with tlen == 0 has no row: it finishes at once.
+        const bool run = active && !J.K.stop;
+
+        // ---- row begin (ksw.cu:335-345) ----
+        RowState r;
+        r.beg = 0; r.end = 0; r.h1 = 0; r.f = 0; r.m = 0; r.mjb = -1; r.plo = 0; r.phi = 0;
+        if (run) {
+            const int32_t i = J.K.next;
+            r.beg = J.beg > i - J.w ? J.beg : i - J.w;
+            r.end = J.end < i + J.w + 1 ? J.end : i + J.w + 1;
+            if (r.end > J.qlen) r.end = J.qlen;
+            if (r.beg == 0) {
+                const int32_t h = J.h0 - (sp.o_del + sp.e_del * (i + 1));
+                r.h1 = h > 0 ? h : 0;
+            }
+            if ((i & 15) == 0 && i > 0) {
+                J.tx = J.px; J.tn = J.pn;
+                const int ch = (i >> 4) + 1;
+                if ((ch << 4) < J.tlen) load16(d.codes, d.nmask, J.t_off, J.tlen, ch, J.trev, J.px, J.pn);
+            }
+            uint32_t code = (J.tx >> ((i & 15) << 1)) & 3u;
+            if ((J.tn >> (i & 15)) & 1u) code = 4;
+            const uint2 p = pools[code];
+            r.plo = p.x;
+            r.phi = p.y;
+        }
+        const bool nonempty = run && r.beg < r.end;
+        const int32_t jb0 = r.beg & ~(kLB - 1);
+        const int nblk = nonempty ? ((r.end - 1) >> 3) - (r.beg >> 3) + 1 : 0;
+        const int kmax = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nblk);
+        busy += nblk;
+        idle += kmax - nblk;
+
+        // ---- the row's blocks: masked first block, unmasked middle, masked last block ----
+        // Each middle block's words are loaded one block ahead (blocks never overlap, so the
+        // load may precede the previous block's store).
+        BlockIn next;
+        if (nblk > 2) next = load_block(eh, qn, lane, jb0 + kLB);
+        if (nblk > 0) lane_block<true>(eh, load_block(eh, qn, lane, jb0), lane, jb0, r, sp);
+        for (int k = 1; k < kmax - 1; ++k) {
+            if (k < nblk - 1) {
+                const BlockIn cur = next;
+                if (k + 1 < nblk - 1) next = load_block(eh, qn, lane, jb0 + (k + 1) * kLB);
+                lane_block<false>(eh, cur, lane, jb0 + k * kLB, r, sp);
+            }
+        }
+        if (nblk > 1) {
+            const int32_t jl = jb0 + (nblk - 1) * kLB;
+            lane_block<true>(eh, load_block(eh, qn, lane, jl), lane, jl, r, sp);
+        }
+
+        // ---- row end (ksw.cu:371-391) ----
+        if (run) {
+            const int32_t beg = r.beg, end = r.end;
+            if (end >= 0) eh[ehw(end, lane)] = (uint32_t)r.h1 << 16;
+            RowDone rd;
+            rd.m = r.m;
+            rd.mj = -1;
+            if (r.m > 0) {
+                // the last column of the winning block that reaches the maximum; H(i, c) is
+                // eh[c+1].h, so the block's eight H values are slots mjb+1 .. mjb+8
+                const int32_t mjb = r.mjb;
+                const int32_t lo = mjb > beg ? mjb : beg;
+                const int32_t hi = mjb + kLB < end ? mjb + kLB : end;
+                const uint4 a = *reinterpret_cast<const uint4*>(eh + ehw(mjb, lane));
+                const uint4 b = *reinterpret_cast<const uint4*>(eh + ehw(mjb + 4, lane));
+                const uint32_t hs[kLB] = {a.y, a.z, a.w, b.x, b.y, b.z, b.w, eh[ehw(mjb + 8, lane)]};
 #pragma unroll
                 for (int t = 0; t < kLB; ++t) {
-                    const int32_t col = jb + t;
-                    if (col >= lo && col < hi) {
-                        const uint32_t w = wv[t];
-                        const int32_t hd = (int32_t)(w >> 16), ed = (int32_t)(w & 0xFFFFu);
-                        const uint32_t sw = t < 4 ? sc_lo : sc_hi;
-                        const int32_t s = (int32_t)(int8_t)(sw >> (8 * (t & 3)));
-                        const int32_t M = addmin_i32(hd, s, hd << 8);
-                        const int32_t h = max3_i32(M, ed, f);
-                        const int32_t te = addmax_i32(M, -sp.oe_del, 0);
-                        const int32_t e2 = addmax_i32(ed, -sp.e_del, te);
-                        const uint32_t nw = ((uint32_t)h1 << 16) | (uint32_t)e2;
-                        ep[(t >> 2) * 128 + (t & 3)] = nw;
-                        if (nw) { lnz = col; fnz = fnz < col ? fnz : col; }
-                        const int32_t k2 = (h << 16) | col;
-                        key = key > k2 ? key : k2;
-                        const int32_t tf = addmax_i32(M, -sp.oe_ins, 0);
-                        f = addmax_i32(f, -sp.e_ins, tf);
-                        h1 = h;
-                    }
+                    const int32_t c = mjb + t;
+                    if (c >= lo && c < hi && (int32_t)(hs[t] >> 16) == r.m) rd.mj = c;
                 }
-                J.h1 = h1; J.f = f; J.key = key; J.fnz = fnz; J.lnz = lnz;
-                J.j = jb + kLB < hi ? jb + kLB : hi;
             }
-            // ---- row end (ksw.cu:371-391) and the next row ----
-            if (J.j >= J.end) {
-                const int32_t beg = J.beg, end = J.end;
-                const bool nonempty = beg < end;
-                if (end >= 0) eh[ehw(end, lane)] = (uint32_t)J.h1 << 16;
-                if (nonempty && J.h1 != 0) J.lnz = end;
-                RowDone rd;
-                rd.m = J.key < 0 ? 0 : (J.key >> 16);
-                rd.mj = J.key < 0 ? -1 : (J.key & 0xFFFF);
-                rd.gval = (nonempty ? end : beg) == J.qlen ? J.h1 : -1;
-                rd.ncells = nonempty ? end - beg : 0;
-                JobConst c;
-                c.qlen = J.qlen; c.tlen = J.tlen; c.w = J.w; c.h0 = J.h0;
-                c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
-                c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
-                commit_row(J.K, c, rd);
-                if (!J.K.stop) {
-                    const int32_t nb = J.fnz < end ? J.fnz : end;
-                    const int32_t L = J.lnz >= nb ? J.lnz : nb - 1;
-                    J.beg = nb;
-                    J.end = L + 2 < J.qlen ? L + 2 : J.qlen;
-                    ++J.i;
-                    begin_row(J, sp, tn, lane, pools);
-                }
+            rd.gval = (nonempty ? end : beg) == J.qlen ? r.h1 : -1;
+            rd.ncells = nonempty ? end - beg : 0;
+            const JobConst c = job_const(J, sp);
+            commit_row(J.K, c, rd);
+            if (!J.K.stop) {
+                int32_t j = beg;
+                while (j < end && eh[ehw(j, lane)] == 0u) ++j;
+                const int32_t nb = j;
+                j = end;
+                while (j >= nb && eh[ehw(j, lane)] == 0u) --j;
+                J.beg = nb;
+                J.end = j + 2 < J.qlen ? j + 2 : J.qlen;
             }
         }
         if (active && J.K.stop) {
@@ -261,23 +349,30 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
 }
 
 int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
-    const size_t wb = lane_warp_bytes(d.qmax, d.tmax);
+    const size_t wb = lane_warp_bytes(d.qmax);
     const size_t kMaxSmem = 227 * 1024;
-    int wpb = d.warps_per_block > 0 ? d.warps_per_block : 4;
-    while (wpb > 1 && (size_t)wpb * wb > kMaxSmem) --wpb;
     if (wb > kMaxSmem) return G3X_ERR_TOO_LONG;
-    const size_t smem = (size_t)wpb * wb;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return G3X_ERR_CUDA;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // Warps per block: the choice among 1, 2 and 4 that keeps the most warps resident (shared
+    // memory is allotted per block, so small blocks waste less of it).
+    int best_wpb = 1, best_warps = 0, best_blocks = 0;
+    const int max_wpb = d.warps_per_block > 0 ? d.warps_per_block : 4;
+    for (int wpb = 1; wpb <= max_wpb; wpb *= 2) {
+        const size_t smem = (size_t)wpb * wb;
+        if (smem > kMaxSmem) break;
+        if (cudaFuncSetAttribute(lane_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return G3X_ERR_CUDA;
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane_kernel, 32 * wpb, smem);
+        if (per_sm * wpb >= best_warps) { best_warps = per_sm * wpb; best_wpb = wpb; best_blocks = per_sm; }
+    }
+    const size_t smem = (size_t)best_wpb * wb;
     if (cudaFuncSetAttribute(lane_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return G3X_ERR_CUDA;
-    int blocks = d.blocks;
-    if (blocks <= 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane_kernel, 32 * wpb, smem);
-        blocks = sms * (per_sm > 0 ? per_sm : 1);
-    }
-    lane_kernel<<<blocks, 32 * wpb, smem, stream>>>(d, sp);
+    int blocks = d.blocks > 0 ? d.blocks : sms * (best_blocks > 0 ? best_blocks : 1);
+    lane_kernel<<<blocks, 32 * best_wpb, smem, stream>>>(d, sp);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }
 

@@ -27,7 +27,7 @@ namespace g3x {
 
 namespace {
 
-constexpr int kBins = kMaxBuckets * 1024;                 // schedule_jobs' histogram bins
+constexpr int kBins = kMaxBuckets * kSchedLevels;         // schedule_jobs' histogram bins
 // Word layout of the scratch array (int32 words).
 constexpr int64_t kQueueAt = 0;                           // kMaxBuckets job-queue counters
 constexpr int64_t kBucketAt = 64;                         // 2 * kMaxBuckets (offset, count)
@@ -35,7 +35,7 @@ constexpr int64_t kHistAt = 128;                          // kBins
 constexpr int64_t kCursorAt = kHistAt + kBins;            // kBins
 constexpr int64_t kBinAt = kCursorAt + kBins;             // G3X_NOALLOC_MAX_JOBS
 constexpr int64_t kOrderAt = kBinAt + G3X_NOALLOC_MAX_JOBS;  // G3X_NOALLOC_MAX_JOBS
-constexpr int64_t kWords = kOrderAt + G3X_NOALLOC_MAX_JOBS;  // 8.06 MiB in all
+constexpr int64_t kWords = kOrderAt + G3X_NOALLOC_MAX_JOBS;  // 8.13 MiB in all
 
 static_assert(kBinAt % 64 == 0 && kOrderAt % 64 == 0, "256-byte aligned sub-arrays");
 

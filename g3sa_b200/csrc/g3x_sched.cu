@@ -5,11 +5,14 @@
 //              cells, covers the class width, so it covers the job's widest possible row
 //              min(qlen, 2w' + 1), w' the clamped band of ksw.cu:321-329); one persistent
 //              launch per class;
-//   a cost   : length-sorted fallback: log2(1 + widest row * tlen), an upper bound of the
-//              job's DP cells; learned: the cost model's prediction of log2(1 + cells).
-// A device counting sort over (bucket, quantised cost) bins -- histogram, exclusive scan,
-// scatter -- writes the job order with each bucket's jobs contiguous and in decreasing
-// cost, plus each bucket's (offset, count).  Nothing returns to the host, so the whole
+//   a key    : the job's row count, then its widest row.  The row count is the length-sorted
+//              fallback's bound tlen, or, learned, the cost model's prediction of
+//              log2(1 + cells) less log2(widest row); the widest row is min(qlen, 2w' + 1).
+//              A warp of a row-synchronous kernel takes consecutive jobs, so jobs of similar
+//              row count and similar row width run together, longest first.
+// A device counting sort over (bucket, key) bins -- histogram, exclusive scan, scatter --
+// writes the job order with each bucket's jobs contiguous and in decreasing row count, plus
+// each bucket's (offset, count).  Nothing returns to the host, so the whole
 // batch (features, prediction, sort, launches) can be captured in one CUDA graph.
 #include <cuda_runtime.h>
 #include <math.h>
@@ -20,7 +23,9 @@ namespace g3x {
 
 namespace {
 
-constexpr int kLevels = 1024;          // cost quantisation levels per bucket
+constexpr int kLevels = kSchedLevels;  // key levels per bucket: 64 row-count x 32 width bins
+constexpr int kRowBins = 64, kWidthBins = 32;
+static_assert(kRowBins * kWidthBins == kLevels, "key layout");
 
 __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScoreParams sp,
                             const float* __restrict__ pred, TileTable tt,
@@ -35,15 +40,29 @@ __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScorePara
     int b = tt.n - 1;
     for (int t = 0; t < tt.n; ++t)
         if (tt.width[t] >= jb.qlen) { b = t; break; }
-    float cost = pred ? pred[k] : log2f(1.0f + (float)wide * (float)jb.tlen);
-    int q = (int)((26.0f - cost) * (kLevels / 26.0f));   // larger cost -> earlier bin
-    q = q < 0 ? 0 : (q >= kLevels ? kLevels - 1 : q);
-    const int bn = b * kLevels + q;
+    // A lane class holds H and E in 16-bit fields (int16x2 arithmetic when tile == 2): a job
+    // whose scores do not provably fit goes to the last class.
+    if (tt.lanes[b] == 1 && b != tt.n - 1) {
+        JobConst c;
+        c.qlen = jb.qlen; c.tlen = jb.tlen; c.h0 = jb.h0; c.w = w;
+        c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
+        c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
+        const bool fits = tt.tile[b] == 2 ? job_fits_int16(c, sp.max_sc) : job_fits_lane(c, sp.max_sc);
+        if (!fits) b = tt.n - 1;
+    }
+    // log2 of the row count, 0..16; four bins per doubling, more rows -> earlier bin
+    float lr = pred ? pred[k] - log2f((float)(wide > 1 ? wide : 1)) : log2f(1.0f + (float)jb.tlen);
+    int rb = (int)((16.0f - lr) * (kRowBins / 16.0f));
+    rb = rb < 0 ? 0 : (rb >= kRowBins ? kRowBins - 1 : rb);
+    // eight-column blocks of the widest row, wider -> earlier bin
+    int wb = (wide + 7) >> 3;
+    wb = kWidthBins - 1 - (wb < kWidthBins - 1 ? wb : kWidthBins - 1);
+    const int bn = b * kLevels + rb * kWidthBins + wb;
     bin[k] = bn;
     atomicAdd(hist + bn, 1);
 }
 
-// Exclusive scan of nb <= 16384 bins in one block; also each bucket's (offset, count).
+// Exclusive scan of the nb bins in one block; also each bucket's (offset, count).
 __global__ void scan_kernel(const int32_t* __restrict__ hist, int nb, int32_t* __restrict__ cursor,
                             int32_t* __restrict__ bucket_oc, int nbuckets) {
     __shared__ int32_t part[1024];

@@ -97,6 +97,7 @@ const char *g3x_strerror(int code);
 #define G3X_KERNEL_ROLLING 1  /* anti-diagonal wavefront: rows on lanes, 4-cell lane steps */
 #define G3X_KERNEL_ROWPAR  2  /* one row per step: columns on lanes, F by shuffle scan */
 #define G3X_KERNEL_LANE    3  /* one job per lane: the scalar row loop, 8-column blocks */
+#define G3X_KERNEL_LANE16  4  /* two jobs per lane in int16x2 (jobs whose scores fit 16 bits) */
 
 typedef struct {
     int32_t schedule;     /* G3X_SCHED_* */
@@ -110,7 +111,9 @@ typedef struct {
     int32_t *d_cells;     /* optional per-job DP cell count (trip count of ksw.cu:346) */
 } g3x_batch_opts_t;       /* 32 bytes */
 
-/* n jobs; outputs to d_out[k] and d_status[k] (G3X_OK or a G3X_ERR_* per job).
+/* n jobs; outputs to d_out[k] and d_status[k] (G3X_OK or a G3X_ERR_* per job: TOO_LONG for a
+   job beyond max_qlen/max_tlen or beyond what a fixed lane kernel holds, INVALID for a seed
+   score -max_score < h0 < 0, which callers of ksw_extend2 never pass).
    Replaces n calls of ksw_extend2 (bwa/src/ksw.h:33) issued by localExtending
    (bwa/src/aux.cu:2289-2382). Asynchronous on `stream`. */
 int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs,
@@ -124,7 +127,7 @@ int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
    kernels, where cudaMalloc/cudaFree would synchronise the device; a process that reserved
    the GPU's memory up front (as the reference's device_alloc does); a framework whose
    allocator owns all device memory.  It needs no context: its scratch (sort keys, job order,
-   histogram, per-class job counters) is one static device array of the library, 8.06 MiB,
+   histogram, per-class job counters) is one static device array of the library, 8.13 MiB,
    looked up once per device.  At most G3X_NOALLOC_MAX_JOBS jobs per call, else
    G3X_ERR_SCRATCH.  All calls on a device share that array: calls that overlap on the GPU
    (two streams, two host threads) race and corrupt each other's results, so serialise them.
@@ -143,21 +146,27 @@ int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t *score, const g3
    class runs the row-parallel kernel with `lanes` lanes per job and `tile` cells per lane;
    `warp_batch` = 1 makes a warp pull one job per group at once and wait for all of them
    (jobs then balance by the schedule's cost order), 0 lets each group refill on its own;
-   the lane-per-job kernel (lanes = 1) refills its idle lanes in waves of at least `refill`. */
+   the lane-per-job kernels (lanes = 1) refill their idle lanes in waves of at least `refill`.
+   A lane class with tile = 2 runs two jobs per lane in int16x2; the scheduler sends a job whose
+   scores do not provably fit a lane class's arithmetic (16-bit fields, h0 >= 0) to the last
+   class instead. */
 #define G3X_MAX_CLASSES 8
 typedef struct {
     int32_t width;        /* widest query of the class (the last class: unbounded) */
     int32_t lanes;        /* 1 = lane-per-job kernel; 4, 8, 16, 32 = row-parallel groups */
-    int32_t tile;         /* row-parallel: cells per lane per tile (5, 9, 13); lane kernel: 0 */
+    int32_t tile;         /* row-parallel: cells per lane per tile (5, 9, 13); lane kernel: 0
+                             (int32, one job per lane) or 2 (int16x2, two jobs per lane) */
     int32_t warp_batch;   /* 1: a warp takes its jobs together and waits for all of them */
     int32_t refill;       /* lane kernel: idle lanes that trigger a refill wave (1-32) */
 } g3x_tile_t;
 
 int g3x_get_tiles(g3x_ctx *ctx, g3x_tile_t *h_tiles, int32_t *n);
 int g3x_set_tiles(g3x_ctx *ctx, const g3x_tile_t *h_tiles, int32_t n);
-/* Times the candidate configurations of every width class on the given jobs (device
-   buffers, each job run as it would be in its class) and keeps the fastest per class in the
-   context; h_tiles/n receive the table.  Blocks.  Outputs of the trial runs are discarded. */
+/* Fits the width classes to the given jobs (device buffers) and tunes them: the class widths
+   become max_qlen * (k/7)^1.5 for k = 1..7 (rounded up to 8 columns, duplicates dropped) plus
+   the unbounded class; then every candidate configuration of each class is timed on the class's
+   jobs and the fastest kept in the context; h_tiles/n receive the table.  Blocks.  Outputs of
+   the trial runs are discarded. */
 int g3x_autotune(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
                  const uint32_t *d_codes, const uint32_t *d_nmask, int32_t max_qlen,
                  int32_t max_tlen, g3x_tile_t *h_tiles, int32_t *n_tiles);

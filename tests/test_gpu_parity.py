@@ -10,40 +10,96 @@ from tests.gpu_util import run_batch
 
 pytestmark = pytest.mark.gpu
 
-R, P = g.KERNEL_ROLLING, g.KERNEL_ROWPAR
+R, P, LN, L16 = g.KERNEL_ROLLING, g.KERNEL_ROWPAR, g.KERNEL_LANE, g.KERNEL_LANE16
 # (schedule, kernel, lanes, tile)
 SCHEDULES = [(g.SCHED_PLAIN, R, 0, 0), (g.SCHED_SORTED, R, 8, 0), (g.SCHED_SORTED, R, 16, 0),
              (g.SCHED_SORTED, R, 32, 0), (g.SCHED_PLAIN, P, 0, 9)] + \
             [(g.SCHED_SORTED, P, l, t) for l in (4, 8, 16, 32) for t in (5, 9, 13)] + \
-            [(g.SCHED_SORTED, g.KERNEL_LANE, 1, rf) for rf in (1, 8, 32)]
-IDS = [f"{'plain' if s == 0 else 'pers'}-{ {R: 'roll', P: 'row', 3: 'lane'}[k]}-g{l}-c{t}" for s, k, l, t in SCHEDULES]
+            [(g.SCHED_SORTED, LN, 1, rf) for rf in (1, 8, 32)] + \
+            [(g.SCHED_SORTED, L16, 1, rf) for rf in (1, 8, 32)]
+NAMES = {R: "roll", P: "row", LN: "lane", L16: "lane16"}
+IDS = [f"{'plain' if s == 0 else 'pers'}-{NAMES[k]}-g{l}-c{t}" for s, k, l, t in SCHEDULES]
+
+
+def lane_fits(jobs, score, kernel):
+    """Jobs a lane-per-job kernel takes (the others get G3X_ERR_TOO_LONG): h0 >= 0 and every H
+    below 2^15 (int32 lane kernel), or below 2^15 >> k with 2^k >= 1 + max_score (int16x2)."""
+    max_sc = int(score["mat"][0].max())
+    mn = np.minimum(jobs["qlen"], jobs["tlen"]).astype(np.int64)
+    hmax = jobs["h0"].astype(np.int64) + max(max_sc, 0) * mn
+    ok = (jobs["h0"] >= 0) & (jobs["qlen"] < 65535)
+    if kernel == LN:
+        return ok & (hmax < 32768)
+    k = 0
+    while (1 << k) < 1 + max_sc and k < 15:
+        k += 1
+    oe_del, oe_ins = int(score["o_del"][0] + score["e_del"][0]), int(score["o_ins"][0] + score["e_ins"][0])
+    return ok & ((hmax << k) < 32768) & (oe_del < 16384) & (oe_ins < 16384)
+
+
+def check_status(jobs, score, kernel, status):
+    """Mask of the jobs whose outputs are compared: all of them, except the jobs a lane-per-job
+    kernel must reject (which must carry G3X_ERR_TOO_LONG)."""
+    if kernel in (LN, L16):
+        fits = lane_fits(jobs, score, kernel)
+        assert (status[~fits] == g.G3X_ERR_TOO_LONG).all()
+        assert (status[fits] == 0).all(), np.unique(status[fits])
+        assert fits.mean() > 0.5
+        return fits
+    assert (status == 0).all(), np.unique(status)
+    return np.ones(len(jobs), bool)
 
 
 @pytest.mark.parametrize("sched,kernel,lanes,tile", SCHEDULES, ids=IDS)
 @pytest.mark.parametrize("name", golden_io.job_sets())
 def test_gpu_matches_golden(name, sched, kernel, lanes, tile):
     u8, jobs, score, ext = golden_io.load_jobs(name)
-    if kernel == g.KERNEL_LANE and jobs["qlen"].max() > 1000:
-        pytest.skip("the lane-per-job kernel holds each lane's query in shared memory (short queries)")
+    if kernel in (LN, L16) and jobs["qlen"].max() > 1000:
+        pytest.skip("the lane-per-job kernels hold each lane's query in shared memory (short queries)")
     out, status, cells = run_batch(u8, jobs, score, sched, lanes, tile=tile, kernel=kernel)
-    assert (status == 0).all(), np.unique(status)
-    bad = np.nonzero((out != ext).any(1))[0]
+    keep = check_status(jobs, score, kernel, status)
+    bad = np.nonzero(((out != ext).any(1)) & keep)[0]
     assert bad.size == 0, f"{name}: jobs {bad[:5]} got {out[bad[:3]]} want {ext[bad[:3]]}"
 
 
 @pytest.mark.parametrize("sched,kernel,lanes,tile", SCHEDULES, ids=IDS)
 @pytest.mark.parametrize("kind,n,w", [(1, 30000, 100), (2, 15000, 100), (4, 150, 100), (4, 150, 500)])
 def test_gpu_matches_oracle_fresh(kind, n, w, sched, kernel, lanes, tile):
-    if kernel == g.KERNEL_LANE and kind == 4:
-        pytest.skip("the lane-per-job kernel holds each lane's query in shared memory (short queries)")
+    if kernel in (LN, L16) and kind == 4:
+        pytest.skip("the lane-per-job kernels hold each lane's query in shared memory (short queries)")
     wl = g.synth(kind, n, seed=0x6A5 + 100 * kind + w, w=w, unrelated=0.2 if kind == 2 else 0.0)
     sc = g.default_score()
     ref, rcells, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
     out, status, cells = run_batch(wl.u8, wl.jobs, sc, sched, lanes, tile=tile, kernel=kernel)
-    assert (status == 0).all()
-    bad = np.nonzero((out != ref).any(1))[0]
+    keep = check_status(wl.jobs, sc, kernel, status)
+    bad = np.nonzero(((out != ref).any(1)) & keep)[0]
     assert bad.size == 0, f"jobs {bad[:5]}"
-    assert (cells == rcells).all()
+    assert (cells[keep] == rcells[keep]).all()
+
+
+# Width classes on the lane-per-job kernels (int16x2 and int32) with the row-parallel kernel
+# as the last class: the scheduler routes every job a lane class cannot hold to the last class.
+LANE_TILES = [(20, 1, 2, 0, 1), (36, 1, 2, 0, 32), (72, 1, 0, 0, 8), (144, 1, 2, 0, 32),
+              (288, 1, 2, 0, 8), (1 << 30, 32, 9, 0, 1)]
+
+
+@pytest.mark.parametrize("name", golden_io.job_sets())
+def test_gpu_lane_classes_route_every_job(name):
+    import torch
+    from tests.gpu_util import to_dev
+    u8, jobs, score, ext = golden_io.load_jobs(name)
+    ctx = g.Context(0)
+    ctx.set_tiles(LANE_TILES)
+    codes, nmask = g.pack_planes(u8)
+    d_jobs, d_codes, d_nmask = to_dev(jobs), to_dev(codes), to_dev(nmask)
+    n = len(jobs)
+    out = torch.full((n, 6), -777, dtype=torch.int32, device="cuda")
+    status = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+    ctx.extend_batch(score, d_jobs, n, d_codes, d_nmask, out, status, int(jobs["qlen"].max()),
+                     int(jobs["tlen"].max()), schedule=g.SCHED_SORTED)
+    torch.cuda.synchronize()
+    assert (status.cpu().numpy() == 0).all()
+    np.testing.assert_array_equal(out.cpu().numpy(), ext)
 
 
 def test_gpu_too_long_jobs_get_status():
@@ -64,3 +120,28 @@ def test_gpu_rejects_bad_scoring():
         with pytest.raises(g.G3xError) as ei:
             run_batch(u8, jobs, bad)
         assert ei.value.code == g.G3X_ERR_SCORE
+
+
+def test_gpu_lane_classes_route_jobs_beyond_16_bits():
+    """Seed scores that leave the int16x2 range (17000), the 16-bit fields (40000) or are
+    negative: the scheduler sends those jobs to the last class, and every output is exact."""
+    import torch
+    from tests.gpu_util import to_dev
+    u8, jobs, score, _ = golden_io.load_jobs("cfg1")
+    jobs = jobs.copy()
+    jobs["h0"][0::7] = 17000
+    jobs["h0"][3::11] = 40000
+    jobs["h0"][5::13] = -5
+    ref, _, _ = nat.oracle_extend(jobs, u8, score)
+    ctx = g.Context(0)
+    ctx.set_tiles(LANE_TILES)
+    codes, nmask = g.pack_planes(u8)
+    d_jobs, d_codes, d_nmask = to_dev(jobs), to_dev(codes), to_dev(nmask)
+    n = len(jobs)
+    out = torch.full((n, 6), -777, dtype=torch.int32, device="cuda")
+    status = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+    ctx.extend_batch(score, d_jobs, n, d_codes, d_nmask, out, status, int(jobs["qlen"].max()),
+                     int(jobs["tlen"].max()), schedule=g.SCHED_SORTED)
+    torch.cuda.synchronize()
+    assert (status.cpu().numpy() == 0).all()
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)
