@@ -31,6 +31,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "ksw_extend2 GCUPS & extensions/s on 1 B200, learned vs plain schedule, bit-exact"
+# DRAM bytes (read + write) per launch of each kernel at this workload's size, from the ncu
+# captures summarised under profiles/ (a 100k-seed case scaled by 5, the DRAM traffic of a
+# launch growing with the jobs it stages).  None until a capture of that kernel exists.
+TRAFFIC_PER_LAUNCH = {("lane", 232): 27.9e6}
 WORKLOADS = {
     # name: (synth kind, units, w, unrelated, description)
     "cfg2": (2, 500000, 100, 0.2,
@@ -165,6 +169,20 @@ def run_reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def combine_ranks(dist, times, counts, device):
+    """Every rank calls this with its own step times and counts: returns the max over ranks
+    of each time (the slowest replica sets the pace) and the sum over ranks of each count.
+    Without a process group it returns the inputs."""
+    import torch
+    if dist is None:
+        return list(times), list(counts)
+    v = torch.tensor(list(times), dtype=torch.float64, device=device)
+    dist.all_reduce(v, op=dist.ReduceOp.MAX)
+    c = torch.tensor(list(counts), dtype=torch.int64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return v.tolist(), c.tolist()
+
+
 def timed_steps(fn, k, w, stream, flush, nvtx=None):
     """W untimed calls, then K calls each bracketed by CUDA events on `stream`, with a
     256 MiB write between them so no step starts with the previous step's data in L2.  With
@@ -250,16 +268,20 @@ def main():
                                 seed_train=0xA11CE + rank, kind=kind_, w=w, unrelated=unrel)
     pred_err = learn.prediction_error(ctx, d_jobs, n, d_codes, d_nmask, cells_np)
 
-    # Autotune the width classes on this batch (length-sorted order), then capture graphs.
+    # Autotune the width classes on this batch for each schedule's own job order, and capture
+    # each schedule's graph with its own tiles (a graph keeps the launch configuration it was
+    # captured with).
     t_tune = time.perf_counter()
-    tiles = ctx.autotune(sc, d_jobs, n, d_codes, d_nmask, mq, mt)
-    t_tune = time.perf_counter() - t_tune
     sched = {"plain": g.SCHED_PLAIN, "sorted": g.SCHED_SORTED, "learned": g.SCHED_LEARNED,
              "auto": g.SCHED_LEARNED}[args.schedule]
-    graphs = {}
-    for sname, sval in (("learned", g.SCHED_LEARNED), ("sorted", g.SCHED_SORTED)):
+    graphs, tiles_of = {}, {}
+    for sname, sval in (("sorted", g.SCHED_SORTED), ("learned", g.SCHED_LEARNED)):
+        tiles_of[sname] = ctx.autotune(sc, d_jobs, n, d_codes, d_nmask, mq, mt, schedule=sval)
         graphs[sname] = ctx.capture_batch(sc, d_jobs, n, d_codes, d_nmask, d_out, d_status, mq, mt,
                                           schedule=sval)
+    t_tune = time.perf_counter() - t_tune
+    tiles = tiles_of["learned" if sched != g.SCHED_SORTED else "sorted"]
+    ctx.set_tiles(tiles)
     main_graph = graphs["learned" if sched == g.SCHED_LEARNED else "sorted"]
     if sched == g.SCHED_PLAIN:
         main_fn = lambda: batch(g.SCHED_PLAIN)  # noqa: E731
@@ -290,6 +312,42 @@ def main():
     ms_plain = timed_steps(lambda: batch(g.SCHED_PLAIN), k2, 1, stream, flush)
     t_sorted, t_learned, t_plain = (sum(x) / len(x) for x in (ms_sorted, ms_learned, ms_plain))
 
+    # Per-class launch durations of the learned batch (the same kernels the graph replays),
+    # each from CUDA events on the class's own stream, while the other classes run beside it.
+    widths = np.array([t[0] for t in tiles], np.int64)
+    member = np.searchsorted(widths, wl.jobs["qlen"].astype(np.int64), side="left")
+    cls_jobs = np.bincount(member, minlength=len(tiles))
+    cls_cells = np.bincount(member, weights=cells_np.astype(np.float64), minlength=len(tiles))
+
+    def class_table(schedule, mode):
+        ctx.set_timing(mode)
+        cls_ms = []
+        for _ in range(3):
+            flush.fill_(1)
+            batch(schedule)
+            cls_ms.append(ctx.class_times())
+        ctx.set_timing(0)
+        rows = []
+        for k, t in enumerate(tiles):
+            ms_k = [c[k][0] for c in cls_ms if c[k][0] >= 0]
+            if cls_ms[-1][k][1] != int(cls_jobs[k]):
+                raise SystemExit(f"class {k}: the library scheduled {cls_ms[-1][k][1]} jobs, qlen says {cls_jobs[k]}")
+            if not ms_k:
+                continue
+            mk = sum(ms_k) / len(ms_k)
+            rows.append({"width": int(t[0]), "kernel": ("lane16" if t[2] == 2 else "lane") if t[1] == 1
+                         else f"rowpar g{t[1]} c{t[2]}", "jobs": int(cls_jobs[k]),
+                         "cells": int(cls_cells[k]), "ms": round(mk, 4),
+                         "gcups": round(cls_cells[k] / (mk * 1e-3) / 1e9, 3)})
+        return rows
+
+    # each class alone (its own kernel roofline), and side by side as the step runs them
+    classes = class_table(g.SCHED_LEARNED, 2)
+    classes_conc = class_table(g.SCHED_LEARNED, 1)
+    ctx.set_tiles(tiles_of["sorted"])
+    classes_sorted = class_table(g.SCHED_SORTED, 2)
+    ctx.set_tiles(tiles)
+
     # end to end through the C ABI with host buffers: H2D job stream, extension, D2H results
     bi = h_jobs.numel() + h_codes.numel() + h_nmask.numel()
     bo = h_out.numel() * 4
@@ -306,19 +364,19 @@ def main():
     barrier()
     t_e2e = sum(e2e_ms) / len(e2e_ms)
 
-    tot_cells, tot_jobs = cells, n
-    if dist is not None:
-        v = torch.tensor([t_step, t_e2e, t_plain, t_sorted, t_learned], dtype=torch.float64, device=dev)
-        dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        t_step, t_e2e, t_plain, t_sorted, t_learned = v.tolist()
-        cnt = torch.tensor([tot_cells, tot_jobs], dtype=torch.int64, device=dev)
-        dist.all_reduce(cnt, op=dist.ReduceOp.SUM)
-        tot_cells, tot_jobs = cnt.tolist()
+    (t_step, t_e2e, t_plain, t_sorted, t_learned), (tot_cells, tot_jobs) = combine_ranks(
+        dist, [t_step, t_e2e, t_plain, t_sorted, t_learned], [cells, n], dev)
 
     peak_ops = ctx.int_peak()
     if rank == 0:
         gcups = tot_cells / (t_step * 1e-3) / 1e9
         peak_gcups = peak_ops / 8 / 1e9
+        dom = max(classes, key=lambda c: c["ms"])
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+                hbm_peak, hbm_src = float(json.load(fh)["hbm_gbs"]), "measured"
+        except (OSError, ValueError, KeyError):
+            hbm_peak, hbm_src = 6650.0, "fallback"
         kind, cpu_t, cpu_out = cpu_reference(wl, os.cpu_count() or 1)
         cpu_gcups = cells / cpu_t / 1e9
         idle = lambda s: round(s[1] / max(1, s[0] + s[1]), 4)  # noqa: E731
@@ -330,13 +388,15 @@ def main():
             "config": {"workload": desc, "jobs_per_gpu": n, "cells_per_gpu": cells,
                        "schedule": args.schedule if args.schedule != "auto" else "learned",
                        "launch": "one CUDA graph per step (features, MLP, counting sort, one persistent launch per width class)",
-                       "width_classes": tiles, "max_qlen": mq, "max_tlen": mt,
+                       "width_classes": tiles, "width_classes_sorted": tiles_of["sorted"],
+                       "max_qlen": mq, "max_tlen": mt,
                        "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas x{ws}"},
             "extensions_per_s": round(tot_jobs / (t_step * 1e-3), 1),
             "arms": {"learned": {"gcups": round(tot_cells / (t_learned * 1e-3) / 1e9, 3), "ms": round(t_learned, 4),
                                  "warp_idle_frac": idle(stats_learned)},
                      "sorted": {"gcups": round(tot_cells / (t_sorted * 1e-3) / 1e9, 3), "ms": round(t_sorted, 4),
-                                "warp_idle_frac": idle(stats_sorted)},
+                                "warp_idle_frac": idle(stats_sorted),
+                                "class_ms": [c["ms"] for c in classes_sorted]},
                      "plain": {"gcups": round(tot_cells / (t_plain * 1e-3) / 1e9, 3), "ms": round(t_plain, 4),
                                "kernel": "one 32-lane block per job, anti-diagonal wavefront, input order"}},
             "speedup_learned_vs_plain": round(t_plain / t_learned, 3),
@@ -345,11 +405,20 @@ def main():
             "autotune_s": round(t_tune, 2),
             "e2e": {"value": round(tot_cells / (t_e2e * 1e-3) / 1e9, 3), "unit": "GCUPS",
                     "ms_per_step": round(t_e2e, 4), "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
-            "roofline": {"bound": "int_alu", "achieved": round(gcups / max(ws, 1), 3),
-                         "peak": round(peak_gcups, 3), "unit": "GCUPS",
-                         "frac": round(gcups / max(ws, 1) / peak_gcups, 4), "traffic": None,
-                         "peak_source": "measured live: g3x_int_peak (DPX VIMNMX3 chains) / 8 ops per cell",
-                         "int_ops_per_s": peak_ops},
+            "roofline": {"bound": "int_alu", "kernel": f"{dom['kernel']} (width class {dom['width']})",
+                         "achieved": dom["gcups"], "peak": round(peak_gcups, 3), "unit": "GCUPS",
+                         "frac": round(dom["gcups"] / peak_gcups, 4),
+                         "traffic": TRAFFIC_PER_LAUNCH.get((dom["kernel"], dom["width"])),
+                         "traffic_unit": "DRAM bytes per launch",
+                         "algorithmic": "cells of the class launch (trip count of ksw.cu:346) / its "
+                                        "CUDA-event duration, the class launched alone on the bench stream",
+                         "class_ms_side_by_side": [c["ms"] for c in classes_conc],
+                         "peak_source": "measured live: g3x_int_peak (DPX VIMNMX3 chains, 32-bit int ops/s) / 8 ops per cell",
+                         "int_ops_per_s": peak_ops, "step_frac": round(gcups / max(ws, 1) / peak_gcups, 4),
+                         "classes": classes},
+            "hbm_job_stream": {"achieved_gbs": round(bi / (t_step * 1e-3) / 1e9, 2), "peak_gbs": hbm_peak,
+                               "frac": round(bi / (t_step * 1e-3) / 1e9 / hbm_peak, 5),
+                               "peak_source": hbm_src, "bytes_per_step": bi},
             "cpu_baseline": {"value": round(cpu_gcups, 4), "unit": "GCUPS", "cores": os.cpu_count(),
                              "kind": kind, "sample": f"whole rank-0 workload ({n} jobs), one pass",
                              "gpu_outputs_identical": bool(np.array_equal(cpu_out, plain_out))},

@@ -135,7 +135,10 @@ def lib():
         L.g3x_get_tiles.argtypes = [P, P, P]
         L.g3x_set_tiles.argtypes = [P, P, I32]
         L.g3x_autotune.argtypes = [P, P, P, I32, P, P, I32, I32, P, P]
+        L.g3x_autotune_schedule.argtypes = [P, I32, P, P, I32, P, P, I32, I32, P, P]
         L.g3x_last_stats.argtypes = [P, P]
+        L.g3x_set_timing.argtypes = [P, I32]
+        L.g3x_class_times.argtypes = [P, P, P, P]
         L.g3x_graph_capture.argtypes = [P, P, P, I32, P, P, P, P, P, ctypes.POINTER(P)]
         L.g3x_graph_launch.argtypes = [P, P]
         L.g3x_graph_destroy.argtypes = [P]
@@ -316,18 +319,32 @@ class Context:
         t = np.array([tuple(x) for x in tiles], TILE_DT)
         _check(lib().g3x_set_tiles(self._h, t.ctypes.data, len(t)), "g3x_set_tiles")
 
-    def autotune(self, score, d_jobs, n, d_codes, d_nmask, max_qlen, max_tlen):
+    def autotune(self, score, d_jobs, n, d_codes, d_nmask, max_qlen, max_tlen, schedule=SCHED_SORTED):
         t = np.zeros(8, TILE_DT)
         k = ctypes.c_int32()
-        _check(lib().g3x_autotune(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
-                                  _ptr(d_nmask), int(max_qlen), int(max_tlen), t.ctypes.data,
-                                  ctypes.addressof(k)), "g3x_autotune")
+        _check(lib().g3x_autotune_schedule(self._h, int(schedule), score.ctypes.data, _ptr(d_jobs), int(n),
+                                           _ptr(d_codes), _ptr(d_nmask), int(max_qlen), int(max_tlen),
+                                           t.ctypes.data, ctypes.addressof(k)), "g3x_autotune_schedule")
         return [tuple(int(v) for v in row) for row in t[:k.value]]
 
     def last_stats(self):
         s = np.zeros(3, np.uint64)
         _check(lib().g3x_last_stats(self._h, s.ctypes.data), "g3x_last_stats")
         return [int(v) for v in s]
+
+    def set_timing(self, mode):
+        """0 off; 1: CUDA events around every class launch of later scheduled batches (classes
+        side by side); 2: classes one after another on the caller's stream, each timed alone."""
+        _check(lib().g3x_set_timing(self._h, int(mode)), "g3x_set_timing")
+
+    def class_times(self):
+        """[(ms, jobs)] per width class of the last timed scheduled batch (ms -1: not run)."""
+        ms = np.zeros(8, np.float32)
+        jobs = np.zeros(8, np.int32)
+        n = ctypes.c_int32()
+        _check(lib().g3x_class_times(self._h, ms.ctypes.data, jobs.ctypes.data, ctypes.addressof(n)),
+               "g3x_class_times")
+        return [(float(ms[k]), int(jobs[k])) for k in range(n.value)]
 
     def int_peak(self):
         """Measured 32-bit integer ALU ops/s of this GPU (g3x_int_peak)."""

@@ -18,6 +18,9 @@ struct g3x_ctx {
     unsigned long long* d_stats; // occupancy counters of the last persistent batch
     cudaStream_t side[g3x::kMaxBuckets];   // one stream per width class
     cudaEvent_t fork, join[g3x::kMaxBuckets];
+    int timing;                             // bracket class launches with timing events
+    cudaEvent_t cls0[g3x::kMaxBuckets], cls1[g3x::kMaxBuckets];
+    int cls_timed[g3x::kMaxBuckets];        // 1 when the last batch recorded class k
 };
 
 namespace g3x {
@@ -160,10 +163,18 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
                           int only = -1, const TileTable* tt_override = nullptr) {
     const TileTable& tt = tt_override ? *tt_override : ctx->tiles;
     if (cudaEventRecord(ctx->fork, st) != cudaSuccess) return G3X_ERR_CUDA;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cap);
+    const bool timed = ctx->timing && cap == cudaStreamCaptureStatusNone && !tt_override;
+    // timing mode 2 runs the classes one after another on `st`, each timed alone
+    const bool serial = timed && ctx->timing == 2;
+    if (timed)
+        for (int k = 0; k < kMaxBuckets; ++k) ctx->cls_timed[k] = 0;
     int rc = G3X_OK;
     for (int k = 0; k < tt.n && rc == G3X_OK; ++k) {
         if (only >= 0 && k != only) continue;
-        if (cudaStreamWaitEvent(ctx->side[k], ctx->fork, 0) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
+        cudaStream_t cs = serial ? st : ctx->side[k];
+        if (!serial && cudaStreamWaitEvent(cs, ctx->fork, 0) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
         LaunchDesc d = base;
         d.kernel = tt.lanes[k] != 1 ? kKernelRowpar : tt.tile[k] == 2 ? kKernelLane16 : kKernelLane;
         d.lanes = tt.lanes[k];
@@ -178,15 +189,21 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
         d.count = ctx->sched.bucket_oc + 2 * k + 1;
         d.queue = ctx->d_queue + k;
         d.stats = ctx->d_stats;
+        if (timed && cudaEventRecord(ctx->cls0[k], cs) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
         if (d.kernel == kKernelLane) {
-            rc = launch_lane(d, sp, ctx->side[k]);
+            rc = launch_lane(d, sp, cs);
         } else if (d.kernel == kKernelLane16) {
-            rc = launch_lane16(d, sp, ctx->side[k]);
+            rc = launch_lane16(d, sp, cs);
         } else {
             while (d.lanes < 32 && (32 / d.lanes) * group_smem_bytes(d.qmax, d.tmax) > 227 * 1024) d.lanes *= 2;
-            rc = launch_rowpar(d, sp, ctx->side[k]);
+            rc = launch_rowpar(d, sp, cs);
         }
-        if (rc == G3X_OK && cudaEventRecord(ctx->join[k], ctx->side[k]) != cudaSuccess) rc = G3X_ERR_CUDA;
+        if (rc == G3X_OK && timed) {
+            if (cudaEventRecord(ctx->cls1[k], cs) != cudaSuccess) rc = G3X_ERR_CUDA;
+            else ctx->cls_timed[k] = 1;
+        }
+        if (serial) continue;
+        if (rc == G3X_OK && cudaEventRecord(ctx->join[k], cs) != cudaSuccess) rc = G3X_ERR_CUDA;
         if (rc == G3X_OK && cudaStreamWaitEvent(st, ctx->join[k], 0) != cudaSuccess) rc = G3X_ERR_CUDA;
     }
     return rc;
@@ -249,7 +266,8 @@ int g3x_ctx_create(g3x_ctx** out, int device) {
               cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
     for (int k = 0; k < g3x::kMaxBuckets && ok; ++k)
         ok = cudaStreamCreateWithFlags(&c->side[k], cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming) == cudaSuccess;
+             cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreate(&c->cls0[k]) == cudaSuccess && cudaEventCreate(&c->cls1[k]) == cudaSuccess;
     if (!ok) {
         delete c;
         return G3X_ERR_NOMEM;
@@ -269,6 +287,8 @@ int g3x_ctx_destroy(g3x_ctx* c) {
     for (int k = 0; k < g3x::kMaxBuckets; ++k) {
         cudaStreamDestroy(c->side[k]);
         cudaEventDestroy(c->join[k]);
+        cudaEventDestroy(c->cls0[k]);
+        cudaEventDestroy(c->cls1[k]);
     }
     cudaEventDestroy(c->fork);
     cudaFree(c->d_stats);
@@ -393,6 +413,29 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
     return G3X_OK;
 }
 
+int g3x_set_timing(g3x_ctx* ctx, int32_t on) {
+    if (!ctx || on < 0 || on > 2) return G3X_ERR_INVALID;
+    ctx->timing = on;
+    return G3X_OK;
+}
+
+int g3x_class_times(g3x_ctx* ctx, float* h_ms, int32_t* h_jobs, int32_t* n) {
+    if (!ctx || !h_ms || !h_jobs || !n) return G3X_ERR_INVALID;
+    if (cudaSetDevice(ctx->device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return G3X_ERR_CUDA;
+    int32_t oc[2 * g3x::kMaxBuckets] = {0};
+    if (ctx->sched.bucket_oc &&
+        cudaMemcpy(oc, ctx->sched.bucket_oc, sizeof(oc), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return G3X_ERR_CUDA;
+    for (int k = 0; k < ctx->tiles.n; ++k) {
+        h_ms[k] = -1.0f;
+        if (ctx->cls_timed[k] && cudaEventElapsedTime(&h_ms[k], ctx->cls0[k], ctx->cls1[k]) != cudaSuccess)
+            return G3X_ERR_CUDA;
+        h_jobs[k] = oc[2 * k + 1];
+    }
+    *n = ctx->tiles.n;
+    return G3X_OK;
+}
+
 int g3x_last_stats(g3x_ctx* ctx, uint64_t* h) {
     if (!ctx || !h) return G3X_ERR_INVALID;
     if (cudaSetDevice(ctx->device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return G3X_ERR_CUDA;
@@ -402,10 +445,12 @@ int g3x_last_stats(g3x_ctx* ctx, uint64_t* h) {
     return G3X_OK;
 }
 
-int g3x_autotune(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs, int32_t n,
-                 const uint32_t* d_codes, const uint32_t* d_nmask, int32_t max_qlen,
-                 int32_t max_tlen, g3x_tile_t* h_tiles, int32_t* n_tiles) {
+int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* score, const g3x_job_t* d_jobs,
+                          int32_t n, const uint32_t* d_codes, const uint32_t* d_nmask, int32_t max_qlen,
+                          int32_t max_tlen, g3x_tile_t* h_tiles, int32_t* n_tiles) {
     if (!ctx || !d_jobs || !d_codes || !d_nmask || n <= 0) return G3X_ERR_INVALID;
+    if (schedule != G3X_SCHED_SORTED && schedule != G3X_SCHED_LEARNED) return G3X_ERR_INVALID;
+    if (schedule == G3X_SCHED_LEARNED && (!ctx->model.params || !ctx->model.trained)) return G3X_ERR_NOT_TRAINED;
     g3x::ScoreParams sp;
     int rc = g3x::score_params(score, &sp);
     if (rc) return rc;
@@ -446,7 +491,13 @@ int g3x_autotune(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    rc = g3x::schedule_jobs(ctx->sched, d_jobs, n, sp, nullptr, ctx->tiles, st);
+    const float* pred = nullptr;
+    if (schedule == G3X_SCHED_LEARNED) {
+        rc = g3x::model_features(d_jobs, n, d_codes, d_nmask, ctx->sched.feat, st);
+        if (rc == G3X_OK) rc = g3x::model_predict(ctx->model.params, ctx->sched.feat, n, ctx->sched.pred, st);
+        pred = ctx->sched.pred;
+    }
+    if (rc == G3X_OK) rc = g3x::schedule_jobs(ctx->sched, d_jobs, n, sp, pred, ctx->tiles, st);
     int32_t oc[2 * g3x::kMaxBuckets];
     if (rc == G3X_OK && cudaMemcpy(oc, ctx->sched.bucket_oc, sizeof(oc), cudaMemcpyDeviceToHost) != cudaSuccess)
         rc = G3X_ERR_CUDA;
@@ -501,6 +552,13 @@ int g3x_autotune(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs
         if (h_tiles && n_tiles) rc = g3x_get_tiles(ctx, h_tiles, n_tiles);
     }
     return rc;
+}
+
+int g3x_autotune(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs, int32_t n,
+                 const uint32_t* d_codes, const uint32_t* d_nmask, int32_t max_qlen,
+                 int32_t max_tlen, g3x_tile_t* h_tiles, int32_t* n_tiles) {
+    return g3x_autotune_schedule(ctx, G3X_SCHED_SORTED, score, d_jobs, n, d_codes, d_nmask, max_qlen,
+                                 max_tlen, h_tiles, n_tiles);
 }
 
 int g3x_extend_seeds(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_seed_t* d_seeds, int32_t n,

@@ -71,6 +71,23 @@ constexpr int32_t kKernelLane = 3;      // one job per lane
 constexpr int32_t kKernelLane16 = 4;    // two jobs per lane, int16x2
 
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+
+// Lets kernel `fn` launch with all the dynamic shared memory a block can have on this device
+// (the opt-in maximum less the kernel's static shared memory), which *limit receives.  Always
+// the same value: a kernel launched by several width classes (possibly captured in one CUDA
+// graph) must never see another launch lower its limit below its own size.
+template <class F>
+inline cudaError_t allow_max_smem(F* fn, size_t* limit = nullptr) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes a;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, fn);
+    if (e != cudaSuccess) return e;
+    const int dyn = optin - (int)a.sharedSizeBytes;
+    if (limit) *limit = (size_t)dyn;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+}
 int launch_rolling(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_rowpar(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);

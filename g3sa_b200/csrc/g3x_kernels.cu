@@ -134,15 +134,13 @@ template <int G>
 static int launch_g(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
     int wpb = d.warps_per_block > 0 ? d.warps_per_block : 1;
     const size_t gb = group_bytes(d.qmax, d.tmax);
-    const size_t kMaxSmem = 227 * 1024;
-    while (wpb > 1 && (size_t)(32 * wpb / G) * gb > kMaxSmem) --wpb;   // fewer warps for long jobs
+    size_t max_smem = 0;
+    if (allow_max_smem(extend_kernel<G>, &max_smem) != cudaSuccess) return G3X_ERR_CUDA;
+    while (wpb > 1 && (size_t)(32 * wpb / G) * gb > max_smem) --wpb;   // fewer warps for long jobs
     const int threads = 32 * wpb;
     const int groups = threads / G;
     const size_t smem = groups * gb;
-    if (smem > kMaxSmem) return G3X_ERR_TOO_LONG;
-    if (cudaFuncSetAttribute(extend_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-        return G3X_ERR_CUDA;
+    if (smem > max_smem) return G3X_ERR_TOO_LONG;
     int blocks;
     if (d.persistent) {
         blocks = d.blocks;

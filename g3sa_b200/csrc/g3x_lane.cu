@@ -137,6 +137,64 @@ __device__ __forceinline__ void lane_block(uint32_t* __restrict__ eh, const Bloc
     r.f = f;
 }
 
+// -t * e_ins for t = 0..8 (the F of cell t of a block, relative to the F entering it).
+struct InsSteps {
+    int32_t n[kLB + 1];
+};
+
+// An unmasked block, with F written out: F(t) = max(F_in - t e_ins, V(t)), V(0) = 0,
+// V(t+1) = max(V(t) - e_ins, T(t)), T(t) = max(M(t) - oe_ins, 0) -- the recurrence
+// F(t+1) = max(F(t) - e_ins, T(t)) of ksw.cu:368-370 unrolled.  V does not depend on F_in, so
+// the only value a block hands to the next through a dependency chain is F_in itself (one
+// operation per block instead of eight).
+__device__ __forceinline__ void lane_block_mid(uint32_t* __restrict__ eh, const BlockIn& in, int lane,
+                                               int32_t jb, RowState& r, const ScoreParams& sp,
+                                               const InsSteps& ins) {
+    uint32_t* ep = eh + ehw(jb, lane);
+    const uint32_t wv[kLB] = {in.wa.x, in.wa.y, in.wa.z, in.wa.w, in.wb.x, in.wb.y, in.wb.z, in.wb.w};
+    const uint32_t sc_lo = __byte_perm(r.plo, r.phi, in.qw);
+    const uint32_t sc_hi = __byte_perm(r.plo, r.phi, in.qw >> 16);
+    int32_t M[kLB], ed[kLB], V[kLB + 1];
+    uint32_t ov[kLB];
+    int32_t hv[kLB];
+    V[0] = 0;
+#pragma unroll
+    for (int t = 0; t < kLB; ++t) {
+        const uint32_t w = wv[t];
+        const int32_t hd = (int32_t)(w >> 16);
+        ed[t] = (int32_t)(w & 0xFFFFu);
+        int32_t s;
+        switch (t & 3) {
+            case 0: s = sbyte<0>(t < 4 ? sc_lo : sc_hi); break;
+            case 1: s = sbyte<1>(t < 4 ? sc_lo : sc_hi); break;
+            case 2: s = sbyte<2>(t < 4 ? sc_lo : sc_hi); break;
+            default: s = sbyte<3>(t < 4 ? sc_lo : sc_hi); break;
+        }
+        M[t] = addmin_i32(hd, s, hd * 256);
+        const int32_t tf = addmax_i32(M[t], -sp.oe_ins, 0);
+        V[t + 1] = addmax_i32(V[t], -sp.e_ins, tf);
+    }
+    const int32_t fin = r.f;
+    int32_t h1 = r.h1;
+#pragma unroll
+    for (int t = 0; t < kLB; ++t) {
+        const int32_t f = t == 0 ? fin : addmax_i32(fin, ins.n[t], V[t]);
+        const int32_t h = max3_i32(M[t], ed[t], f);
+        const int32_t te = addmax_i32(M[t], -sp.oe_del, 0);
+        const int32_t e2 = addmax_i32(ed[t], -sp.e_del, te);
+        ov[t] = __byte_perm((uint32_t)e2, (uint32_t)h1, 0x5410);
+        hv[t] = h;
+        h1 = h;
+    }
+    *reinterpret_cast<uint4*>(ep) = make_uint4(ov[0], ov[1], ov[2], ov[3]);
+    *reinterpret_cast<uint4*>(ep + 128) = make_uint4(ov[4], ov[5], ov[6], ov[7]);
+    const int32_t bm = max3_i32(max3_i32(hv[0], hv[1], hv[2]), max3_i32(hv[3], hv[4], hv[5]),
+                                hv[6] > hv[7] ? hv[6] : hv[7]);
+    if (bm >= r.m) { r.m = bm; r.mjb = jb; }
+    r.h1 = h1;
+    r.f = addmax_i32(fin, ins.n[kLB], V[kLB]);
+}
+
 __device__ __forceinline__ JobConst job_const(const LaneJob& J, const ScoreParams& sp) {
     JobConst c;
     c.qlen = J.qlen; c.tlen = J.tlen; c.w = J.w; c.h0 = J.h0;
@@ -173,6 +231,9 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
     const int n = d.count ? *d.count : d.n;
     const int* order = d.order ? d.order + (d.order_off ? *d.order_off : 0) : nullptr;
     const int refill = d.warp_batch ? 32 : (d.refill > 0 ? d.refill : 1);
+    InsSteps ins;
+#pragma unroll
+    for (int t = 0; t <= kLB; ++t) ins.n[t] = -t * sp.e_ins;
 
     LaneJob J;
     J.job = -1;
@@ -288,7 +349,7 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
             if (k < nblk - 1) {
                 const BlockIn cur = next;
                 if (k + 1 < nblk - 1) next = load_block(eh, qn, lane, jb0 + (k + 1) * kLB);
-                lane_block<false>(eh, cur, lane, jb0 + k * kLB, r, sp);
+                lane_block_mid(eh, cur, lane, jb0 + k * kLB, r, sp, ins);
             }
         }
         if (nblk > 1) {
@@ -350,8 +411,9 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
 
 int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
     const size_t wb = lane_warp_bytes(d.qmax);
-    const size_t kMaxSmem = 227 * 1024;
-    if (wb > kMaxSmem) return G3X_ERR_TOO_LONG;
+    size_t max_smem = 0;
+    if (allow_max_smem(lane_kernel, &max_smem) != cudaSuccess) return G3X_ERR_CUDA;
+    if (wb > max_smem) return G3X_ERR_TOO_LONG;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return G3X_ERR_CUDA;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -361,16 +423,12 @@ int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream)
     const int max_wpb = d.warps_per_block > 0 ? d.warps_per_block : 4;
     for (int wpb = 1; wpb <= max_wpb; wpb *= 2) {
         const size_t smem = (size_t)wpb * wb;
-        if (smem > kMaxSmem) break;
-        if (cudaFuncSetAttribute(lane_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return G3X_ERR_CUDA;
+        if (smem > max_smem) break;
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane_kernel, 32 * wpb, smem);
         if (per_sm * wpb >= best_warps) { best_warps = per_sm * wpb; best_wpb = wpb; best_blocks = per_sm; }
     }
     const size_t smem = (size_t)best_wpb * wb;
-    if (cudaFuncSetAttribute(lane_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return G3X_ERR_CUDA;
     int blocks = d.blocks > 0 ? d.blocks : sms * (best_blocks > 0 ? best_blocks : 1);
     lane_kernel<<<blocks, 32 * best_wpb, smem, stream>>>(d, sp);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;

@@ -410,8 +410,9 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
 
 int launch_lane16(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
     const size_t wb = pair_warp_bytes(d.qmax);
-    const size_t kMaxSmem = 227 * 1024;
-    if (wb > kMaxSmem) return G3X_ERR_TOO_LONG;
+    size_t max_smem = 0;
+    if (allow_max_smem(lane16_kernel, &max_smem) != cudaSuccess) return G3X_ERR_CUDA;
+    if (wb > max_smem) return G3X_ERR_TOO_LONG;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return G3X_ERR_CUDA;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -419,16 +420,12 @@ int launch_lane16(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t strea
     const int max_wpb = d.warps_per_block > 0 ? d.warps_per_block : 4;
     for (int wpb = 1; wpb <= max_wpb; wpb *= 2) {
         const size_t smem = (size_t)wpb * wb;
-        if (smem > kMaxSmem) break;
-        if (cudaFuncSetAttribute(lane16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return G3X_ERR_CUDA;
+        if (smem > max_smem) break;
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane16_kernel, 32 * wpb, smem);
         if (per_sm * wpb >= best_warps) { best_warps = per_sm * wpb; best_wpb = wpb; best_blocks = per_sm; }
     }
     const size_t smem = (size_t)best_wpb * wb;
-    if (cudaFuncSetAttribute(lane16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return G3X_ERR_CUDA;
     const int blocks = d.blocks > 0 ? d.blocks : sms * (best_blocks > 0 ? best_blocks : 1);
     lane16_kernel<<<blocks, 32 * best_wpb, smem, stream>>>(d, sp);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;

@@ -170,10 +170,27 @@ int g3x_set_tiles(g3x_ctx *ctx, const g3x_tile_t *h_tiles, int32_t n);
 int g3x_autotune(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
                  const uint32_t *d_codes, const uint32_t *d_nmask, int32_t max_qlen,
                  int32_t max_tlen, g3x_tile_t *h_tiles, int32_t *n_tiles);
+/* The same, with the jobs ordered as `schedule` (G3X_SCHED_SORTED or G3X_SCHED_LEARNED, which
+   needs a trained model) orders them, so the choices fit that schedule; g3x_autotune is the
+   G3X_SCHED_SORTED form. */
+int g3x_autotune_schedule(g3x_ctx *ctx, int32_t schedule, const g3x_score_t *score,
+                          const g3x_job_t *d_jobs, int32_t n, const uint32_t *d_codes,
+                          const uint32_t *d_nmask, int32_t max_qlen, int32_t max_tlen,
+                          g3x_tile_t *h_tiles, int32_t *n_tiles);
 /* Occupancy counters of the last persistent batch on this context: h_stats[0] = group-rows
    computed, [1] = group-rows a group waited for the other groups of its warp (warp_batch),
    [2] = warp batches.  Synchronises the context's device. */
 int g3x_last_stats(g3x_ctx *ctx, uint64_t *h_stats);
+
+/* Per-class kernel timing of the scheduled batches (no counterpart in the reference): with
+   timing on (1), every persistent class launch made outside CUDA-graph capture is bracketed by
+   CUDA events on the stream it runs on, the classes running side by side as usual; with 2,
+   the classes run one after another on the caller's stream, each timed alone; 0 = off.
+   g3x_class_times then returns, for the last such batch, each class's launch duration in ms
+   (-1: not launched) and job count; n receives the number of classes.  Synchronises the
+   context's device. */
+int g3x_set_timing(g3x_ctx *ctx, int32_t on);
+int g3x_class_times(g3x_ctx *ctx, float *h_ms, int32_t *h_jobs, int32_t *n);
 
 /* ---- seed-level extension with band retry ---------------------------------------------- */
 
