@@ -38,6 +38,7 @@ int score_params(const g3x_score_t* s, ScoreParams* sp) {
     sp->o_del = s->o_del; sp->e_del = s->e_del; sp->o_ins = s->o_ins; sp->e_ins = s->e_ins;
     sp->zdrop = s->zdrop; sp->end_bonus = s->end_bonus; sp->max_sc = max_sc;
     sp->oe_del = s->o_del + s->e_del; sp->oe_ins = s->o_ins + s->e_ins;
+    sp->k16 = 1u << 16; sp->k8 = 1u << 8;
     return G3X_OK;
 }
 
@@ -53,15 +54,16 @@ int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d) {
     if (opts->schedule != G3X_SCHED_PLAIN && opts->schedule != G3X_SCHED_SORTED &&
         opts->schedule != G3X_SCHED_LEARNED)
         return G3X_ERR_INVALID;
-    if (opts->kernel < G3X_KERNEL_AUTO || opts->kernel > G3X_KERNEL_LANE16) return G3X_ERR_INVALID;
+    if (opts->kernel < G3X_KERNEL_AUTO || opts->kernel > G3X_KERNEL_LANE2) return G3X_ERR_INVALID;
     const bool plain = opts->schedule == G3X_SCHED_PLAIN;
     d->kernel = opts->kernel == G3X_KERNEL_AUTO ? (plain ? kKernelRolling : kKernelRowpar)
                 : opts->kernel == G3X_KERNEL_ROLLING ? kKernelRolling
                 : opts->kernel == G3X_KERNEL_ROWPAR ? kKernelRowpar
-                : opts->kernel == G3X_KERNEL_LANE ? kKernelLane : kKernelLane16;
-    if (d->kernel == kKernelLane || d->kernel == kKernelLane16) {
+                : opts->kernel == G3X_KERNEL_LANE ? kKernelLane
+                : opts->kernel == G3X_KERNEL_LANE16 ? kKernelLane16 : kKernelLane2;
+    if (d->kernel == kKernelLane || d->kernel == kKernelLane16 || d->kernel == kKernelLane2) {
         if (plain) return G3X_ERR_INVALID;            // the lane kernels are persistent only
-        d->lanes = 1; d->tile = d->kernel == kKernelLane16 ? 2 : 0;
+        d->lanes = 1; d->tile = d->kernel == kKernelLane16 ? 2 : d->kernel == kKernelLane2 ? 4 : 0;
         d->persistent = 1; d->warps_per_block = 4; d->queue = queue;
         d->refill = opts->tile > 0 ? opts->tile : 1;  // tile carries the refill threshold
         return G3X_OK;
@@ -171,12 +173,16 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
     if (timed)
         for (int k = 0; k < kMaxBuckets; ++k) ctx->cls_timed[k] = 0;
     int rc = G3X_OK;
-    for (int k = 0; k < tt.n && rc == G3X_OK; ++k) {
+    // Widest class first: its long rows make the longest-running blocks, and the narrow
+    // classes' short jobs then fill the SMs its tail leaves idle.
+    for (int kk = tt.n - 1; kk >= 0 && rc == G3X_OK; --kk) {
+        const int k = kk;
         if (only >= 0 && k != only) continue;
         cudaStream_t cs = serial ? st : ctx->side[k];
         if (!serial && cudaStreamWaitEvent(cs, ctx->fork, 0) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
         LaunchDesc d = base;
-        d.kernel = tt.lanes[k] != 1 ? kKernelRowpar : tt.tile[k] == 2 ? kKernelLane16 : kKernelLane;
+        d.kernel = tt.lanes[k] != 1 ? kKernelRowpar : tt.tile[k] == 2 ? kKernelLane16
+                 : tt.tile[k] == 4 ? kKernelLane2 : kKernelLane;
         d.lanes = tt.lanes[k];
         d.tile = tt.tile[k];
         d.warp_batch = tt.warp_batch[k];
@@ -194,6 +200,8 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
             rc = launch_lane(d, sp, cs);
         } else if (d.kernel == kKernelLane16) {
             rc = launch_lane16(d, sp, cs);
+        } else if (d.kernel == kKernelLane2) {
+            rc = launch_lane2(d, sp, cs);
         } else {
             while (d.lanes < 32 && (32 / d.lanes) * group_smem_bytes(d.qmax, d.tmax) > 227 * 1024) d.lanes *= 2;
             rc = launch_rowpar(d, sp, cs);
@@ -396,7 +404,7 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
         const g3x_tile_t& t = h[k];
         const bool lane = t.lanes == 1;
         if ((!lane && t.lanes != 4 && t.lanes != 8 && t.lanes != 16 && t.lanes != 32) ||
-            (!lane && t.tile != 5 && t.tile != 9 && t.tile != 13) || (lane && t.tile != 0 && t.tile != 2) ||
+            (!lane && t.tile != 5 && t.tile != 9 && t.tile != 13) || (lane && t.tile != 0 && t.tile != 2 && t.tile != 4) ||
             t.width < 1 ||
             (k && t.width <= h[k - 1].width) || (t.warp_batch != 0 && t.warp_batch != 1) ||
             (lane && (t.refill < 1 || t.refill > 32)))
@@ -516,6 +524,8 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
             for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 0, 0, rf};
         if (!last && g3x::lane16_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen)) <= 200 * 1024)
             for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 2, 0, rf};
+        if (!last && g3x::lane2_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen)) <= 200 * 1024)
+            for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 4, 0, rf};
         for (int l : {4, 8, 16, 32})
             for (int c : {5, 9, 13}) {
                 const int S = l * c;

@@ -12,6 +12,10 @@ struct ScoreParams {
     int8_t pad_[3];
     int32_t o_del, e_del, o_ins, e_ins, zdrop, end_bonus, max_sc;
     int32_t oe_del, oe_ins;   // o + e
+    // 2^16 and 2^8 as run-time values: multiplying by them keeps 16-bit field packing and
+    // unpacking on the FMA pipe (IMAD), which the compiler would turn into ALU shifts and
+    // logic operations for literal constants, and the ALU pipe is the one the DP saturates
+    uint32_t k16, k8;
 };
 
 // One launch of the extension kernel family.
@@ -69,6 +73,7 @@ constexpr int32_t kKernelRolling = 1;   // anti-diagonal wavefront, rows on lane
 constexpr int32_t kKernelRowpar = 2;    // one row per step, columns on lanes
 constexpr int32_t kKernelLane = 3;      // one job per lane
 constexpr int32_t kKernelLane16 = 4;    // two jobs per lane, int16x2
+constexpr int32_t kKernelLane2 = 5;     // one job per lane, two rows in flight
 
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 
@@ -92,6 +97,8 @@ int launch_rolling(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stre
 int launch_rowpar(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_lane16(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+int launch_lane2(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+size_t lane2_smem_per_warp(int qcap);
 size_t lane16_smem_per_warp(int qcap);
 size_t lane_smem_per_warp(int qcap, int tcap);
 

@@ -171,6 +171,7 @@ int launch_rolling(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stre
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
     if (d.kernel == kKernelLane) return launch_lane(d, sp, stream);
     if (d.kernel == kKernelLane16) return launch_lane16(d, sp, stream);
+    if (d.kernel == kKernelLane2) return launch_lane2(d, sp, stream);
     return d.kernel == kKernelRowpar ? launch_rowpar(d, sp, stream) : launch_rolling(d, sp, stream);
 }
 

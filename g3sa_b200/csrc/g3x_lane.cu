@@ -161,8 +161,8 @@ __device__ __forceinline__ void lane_block_mid(uint32_t* __restrict__ eh, const 
 #pragma unroll
     for (int t = 0; t < kLB; ++t) {
         const uint32_t w = wv[t];
-        const int32_t hd = (int32_t)(w >> 16);
-        ed[t] = (int32_t)(w & 0xFFFFu);
+        const int32_t hd = (int32_t)__umulhi(w, sp.k16);           // w >> 16 on the FMA pipe
+        ed[t] = (int32_t)(w - (uint32_t)hd * sp.k16);               // w & 0xFFFF likewise
         int32_t s;
         switch (t & 3) {
             case 0: s = sbyte<0>(t < 4 ? sc_lo : sc_hi); break;
@@ -170,7 +170,7 @@ __device__ __forceinline__ void lane_block_mid(uint32_t* __restrict__ eh, const 
             case 2: s = sbyte<2>(t < 4 ? sc_lo : sc_hi); break;
             default: s = sbyte<3>(t < 4 ? sc_lo : sc_hi); break;
         }
-        M[t] = addmin_i32(hd, s, hd * 256);
+        M[t] = addmin_i32(hd, s, hd * (int32_t)sp.k8);
         const int32_t tf = addmax_i32(M[t], -sp.oe_ins, 0);
         V[t + 1] = addmax_i32(V[t], -sp.e_ins, tf);
     }
@@ -182,7 +182,7 @@ __device__ __forceinline__ void lane_block_mid(uint32_t* __restrict__ eh, const 
         const int32_t h = max3_i32(M[t], ed[t], f);
         const int32_t te = addmax_i32(M[t], -sp.oe_del, 0);
         const int32_t e2 = addmax_i32(ed[t], -sp.e_del, te);
-        ov[t] = __byte_perm((uint32_t)e2, (uint32_t)h1, 0x5410);
+        ov[t] = (uint32_t)h1 * sp.k16 + (uint32_t)e2;              // {h1, e2}, both < 2^15
         hv[t] = h;
         h1 = h;
     }

@@ -30,6 +30,8 @@ def main():
                     help="width classes of the sorted schedule, e.g. 20:4:5:1:1,288:1:0:0:8 "
                          "(lanes 1 = the lane-per-job kernel); default: the context's")
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--class-times", action="store_true",
+                    help="run the width classes one after another and print each one's time")
     ap.add_argument("--seed", type=int, default=0x6A5 + 2)
     a = ap.parse_args()
     import torch
@@ -47,6 +49,8 @@ def main():
     kern = {"auto": g.KERNEL_AUTO, "rolling": g.KERNEL_ROLLING, "rowpar": g.KERNEL_ROWPAR,
             "lane": g.KERNEL_LANE}[a.kernel]
     mq, mt = int(wl.jobs["qlen"].max()), int(wl.jobs["tlen"].max())
+    if a.class_times:
+        ctx.set_timing(2)
     dt = 0.0
     for _ in range(a.reps):
         torch.cuda.synchronize()
@@ -55,6 +59,8 @@ def main():
                          schedule=sched, kernel=kern)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
+    if a.class_times:
+        print("class ms/jobs:", " ".join(f"{ms:.3f}/{jobs}" for ms, jobs in ctx.class_times()))
     bad = int((status != 0).sum())
     print(f"jobs {wl.n} max_qlen {mq} max_tlen {mt} last_batch_ms {dt * 1e3:.3f} job_errors {bad}")
     if bad:

@@ -98,6 +98,7 @@ const char *g3x_strerror(int code);
 #define G3X_KERNEL_ROWPAR  2  /* one row per step: columns on lanes, F by shuffle scan */
 #define G3X_KERNEL_LANE    3  /* one job per lane: the scalar row loop, 8-column blocks */
 #define G3X_KERNEL_LANE16  4  /* two jobs per lane in int16x2 (jobs whose scores fit 16 bits) */
+#define G3X_KERNEL_LANE2   5  /* one job per lane, rows i and i+1 in flight together */
 
 typedef struct {
     int32_t schedule;     /* G3X_SCHED_* */
@@ -155,7 +156,8 @@ typedef struct {
     int32_t width;        /* widest query of the class (the last class: unbounded) */
     int32_t lanes;        /* 1 = lane-per-job kernel; 4, 8, 16, 32 = row-parallel groups */
     int32_t tile;         /* row-parallel: cells per lane per tile (5, 9, 13); lane kernel: 0
-                             (int32, one job per lane) or 2 (int16x2, two jobs per lane) */
+                             (int32, one job per lane), 2 (int16x2, two jobs per lane) or 4
+                             (int32, one job per lane with two of its rows in flight) */
     int32_t warp_batch;   /* 1: a warp takes its jobs together and waits for all of them */
     int32_t refill;       /* lane kernel: idle lanes that trigger a refill wave (1-32) */
 } g3x_tile_t;

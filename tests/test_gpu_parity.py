@@ -10,14 +10,15 @@ from tests.gpu_util import run_batch
 
 pytestmark = pytest.mark.gpu
 
-R, P, LN, L16 = g.KERNEL_ROLLING, g.KERNEL_ROWPAR, g.KERNEL_LANE, g.KERNEL_LANE16
+R, P, LN, L16, L2 = g.KERNEL_ROLLING, g.KERNEL_ROWPAR, g.KERNEL_LANE, g.KERNEL_LANE16, g.KERNEL_LANE2
 # (schedule, kernel, lanes, tile)
 SCHEDULES = [(g.SCHED_PLAIN, R, 0, 0), (g.SCHED_SORTED, R, 8, 0), (g.SCHED_SORTED, R, 16, 0),
              (g.SCHED_SORTED, R, 32, 0), (g.SCHED_PLAIN, P, 0, 9)] + \
             [(g.SCHED_SORTED, P, l, t) for l in (4, 8, 16, 32) for t in (5, 9, 13)] + \
             [(g.SCHED_SORTED, LN, 1, rf) for rf in (1, 8, 32)] + \
-            [(g.SCHED_SORTED, L16, 1, rf) for rf in (1, 8, 32)]
-NAMES = {R: "roll", P: "row", LN: "lane", L16: "lane16"}
+            [(g.SCHED_SORTED, L16, 1, rf) for rf in (1, 8, 32)] + \
+            [(g.SCHED_SORTED, L2, 1, rf) for rf in (1, 8, 32)]
+NAMES = {R: "roll", P: "row", LN: "lane", L16: "lane16", L2: "lane2"}
 IDS = [f"{'plain' if s == 0 else 'pers'}-{NAMES[k]}-g{l}-c{t}" for s, k, l, t in SCHEDULES]
 
 
@@ -28,7 +29,7 @@ def lane_fits(jobs, score, kernel):
     mn = np.minimum(jobs["qlen"], jobs["tlen"]).astype(np.int64)
     hmax = jobs["h0"].astype(np.int64) + max(max_sc, 0) * mn
     ok = (jobs["h0"] >= 0) & (jobs["qlen"] < 65535)
-    if kernel == LN:
+    if kernel in (LN, L2):
         return ok & (hmax < 32768)
     k = 0
     while (1 << k) < 1 + max_sc and k < 15:
@@ -40,7 +41,7 @@ def lane_fits(jobs, score, kernel):
 def check_status(jobs, score, kernel, status):
     """Mask of the jobs whose outputs are compared: all of them, except the jobs a lane-per-job
     kernel must reject (which must carry G3X_ERR_TOO_LONG)."""
-    if kernel in (LN, L16):
+    if kernel in (LN, L16, L2):
         fits = lane_fits(jobs, score, kernel)
         assert (status[~fits] == g.G3X_ERR_TOO_LONG).all()
         assert (status[fits] == 0).all(), np.unique(status[fits])
@@ -54,7 +55,7 @@ def check_status(jobs, score, kernel, status):
 @pytest.mark.parametrize("name", golden_io.job_sets())
 def test_gpu_matches_golden(name, sched, kernel, lanes, tile):
     u8, jobs, score, ext = golden_io.load_jobs(name)
-    if kernel in (LN, L16) and jobs["qlen"].max() > 1000:
+    if kernel in (LN, L16, L2) and jobs["qlen"].max() > 1000:
         pytest.skip("the lane-per-job kernels hold each lane's query in shared memory (short queries)")
     out, status, cells = run_batch(u8, jobs, score, sched, lanes, tile=tile, kernel=kernel)
     keep = check_status(jobs, score, kernel, status)
@@ -65,7 +66,7 @@ def test_gpu_matches_golden(name, sched, kernel, lanes, tile):
 @pytest.mark.parametrize("sched,kernel,lanes,tile", SCHEDULES, ids=IDS)
 @pytest.mark.parametrize("kind,n,w", [(1, 30000, 100), (2, 15000, 100), (4, 150, 100), (4, 150, 500)])
 def test_gpu_matches_oracle_fresh(kind, n, w, sched, kernel, lanes, tile):
-    if kernel in (LN, L16) and kind == 4:
+    if kernel in (LN, L16, L2) and kind == 4:
         pytest.skip("the lane-per-job kernels hold each lane's query in shared memory (short queries)")
     wl = g.synth(kind, n, seed=0x6A5 + 100 * kind + w, w=w, unrelated=0.2 if kind == 2 else 0.0)
     sc = g.default_score()
@@ -79,8 +80,8 @@ def test_gpu_matches_oracle_fresh(kind, n, w, sched, kernel, lanes, tile):
 
 # Width classes on the lane-per-job kernels (int16x2 and int32) with the row-parallel kernel
 # as the last class: the scheduler routes every job a lane class cannot hold to the last class.
-LANE_TILES = [(20, 1, 2, 0, 1), (36, 1, 2, 0, 32), (72, 1, 0, 0, 8), (144, 1, 2, 0, 32),
-              (288, 1, 2, 0, 8), (1 << 30, 32, 9, 0, 1)]
+LANE_TILES = [(20, 1, 2, 0, 1), (36, 1, 2, 0, 32), (72, 1, 0, 0, 8), (144, 1, 4, 0, 32),
+              (288, 1, 4, 0, 8), (1 << 30, 32, 9, 0, 1)]
 
 
 @pytest.mark.parametrize("name", golden_io.job_sets())
