@@ -137,9 +137,10 @@ G3X_HD int32_t int16_shift(int32_t max_sc) {
 
 // A job fits the int16x2 kernel when every value of its DP, H << k included, stays below 2^15:
 // 0 <= H <= h0 + max_sc * min(qlen, tlen) (E and F are bounded by H), and the penalties keep
-// M - o - e above -2^15.
+// M - o - e and F - 8 e_ins above -2^15.
 G3X_HD bool job_fits_int16(const JobConst& c, int32_t max_sc) {
     if (c.h0 < 0 || c.qlen >= 65535 || c.oe_del >= 16384 || c.oe_ins >= 16384) return false;
+    if (c.e_ins > 4095 || c.e_del > 4095) return false;
     const int64_t mn = c.qlen < c.tlen ? c.qlen : c.tlen;
     const int64_t hmax = (int64_t)c.h0 + (int64_t)(max_sc > 0 ? max_sc : 0) * mn;
     return (hmax << int16_shift(max_sc)) < 32768;

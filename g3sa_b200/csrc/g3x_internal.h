@@ -72,7 +72,7 @@ int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScorePara
 constexpr int32_t kKernelRolling = 1;   // anti-diagonal wavefront, rows on lanes
 constexpr int32_t kKernelRowpar = 2;    // one row per step, columns on lanes
 constexpr int32_t kKernelLane = 3;      // one job per lane
-constexpr int32_t kKernelLane16 = 4;    // two jobs per lane, int16x2
+constexpr int32_t kKernelLane16 = 4;    // one job per lane, int16x2 pair-column blocks
 constexpr int32_t kKernelLane2 = 5;     // one job per lane, two rows in flight
 
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);

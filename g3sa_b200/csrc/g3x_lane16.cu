@@ -1,27 +1,25 @@
-// g3x_lane16.cu -- lane-per-job-pair sm_100a kernel for batched ksw_extend2 in int16x2
+// g3x_lane16.cu -- lane-per-job sm_100a kernel for batched ksw_extend2 in int16x2
 // (bwa/src/ksw.cu:303-401).
 //
-// Each lane runs TWO jobs of the batch at once, one in each 16-bit half of its registers, with
-// the Blackwell DPX int16x2 instructions: one __viaddmin_s16x2 / __vimax3_s16x2 /
-// __viaddmax_s16x2 computes the same step of the recurrence for both jobs.  The two jobs are
-// consecutive in the scheduler's order (similar query length, similar row count), start
-// together and advance one row per step each, so they are always on the same row; each half
-// keeps its own band [beg, end) (ksw.cu:338-340, 388-391), its own row bookkeeping
-// (ksw.cu:371-386) and its own output.  A lane walks the union of the two bands in aligned
-// blocks of eight columns: blocks inside both bands unmasked, the others with per-half masks
-// that leave a half's state and row buffer untouched outside its band.  The warp is
-// row-synchronous as in the int32 lane kernel.
+// The same row-synchronous lane-per-job design as the int32 lane kernel (g3x_lane.cu): each
+// lane runs its job through the reference's row loop, all lanes start rows together, a row is
+// walked in aligned 8-column blocks (first and last block masked to the band, the blocks
+// between unmasked), and the row-end bookkeeping (ksw.cu:371-391) runs for all lanes together.
+// What differs is the arithmetic of the unmasked blocks: the row buffer (ksw.cu:310) holds, for
+// each 8-column block, four int16x2 words of H and four of E, word p holding columns p and p+4.
+// One Blackwell DPX int16x2 instruction (__viaddmin_s16x2, __vimax3_s16x2, __viaddmax_s16x2)
+// then does one step of the recurrence for two cells of the row, and the words need no
+// unpacking or packing.  F runs through the block in its unrolled form,
+// F(t) = max(F_in - t e_ins, V(t)), V(t+1) = max(V(t) - e_ins, T(t)): both halves compute the
+// prefix V over their four columns at once, and the high half then takes in V(4) from the low.
+// The masked blocks and the row end use int32 arithmetic on the same words.
 //
-// Exactness of the 16-bit arithmetic: a job runs here only when every value of its DP fits,
-// i.e. 0 <= h0 and K * (h0 + max_score * min(qlen, tlen)) < 2^15, with K the smallest power
-// of two >= 1 + max_score.  Then H, E, F < 2^15 / K, M = H ? H + S : 0 is written as
-// min(H + S, K * H) (equal when H > 0, <= 0 when H == 0, and every use clips it to 0 like the
-// reference's 0), and no sum or difference leaves the int16 range.  The scheduler routes every
-// other job to an int32 kernel.
-//
-// Shared memory per lane: the two jobs' row buffers (ksw.cu:310) as a plane of H words
-// (H_a | H_b << 16) and a plane of E words, lane-interleaved like the int32 lane kernel's
-// (slot k of lane L is word ((k/4)*32 + L)*4 + k%4), and each job's query as 4-bit codes.
+// Exactness of the 16-bit arithmetic: a job runs here only when every value of its DP fits
+// (job_fits_int16): 0 <= h0, K * (h0 + max_score * min(qlen, tlen)) < 2^15 with K the smallest
+// power of two >= 1 + max_score, and the gap penalties small enough that every difference stays
+// above -2^15.  Then M = H ? H + S : 0 is min(H + S, K H) (equal when H > 0, <= 0 when H == 0,
+// and every use clips it to 0 like the reference's 0).  The scheduler routes every other job
+// to an int32 kernel.
 #include <cuda_runtime.h>
 #include "g3x_core.h"
 #include "g3x_internal.h"
@@ -33,29 +31,71 @@ namespace {
 
 constexpr int kLB = 8;
 
-__host__ __device__ inline int pair_eh_words(int qcap) { return (qcap + 8 + kLB + 3) & ~3; }
-__host__ __device__ inline int pair_nib_words(int len) { return (len + 7) / 8 + 2; }
-__host__ __device__ inline size_t pair_warp_bytes(int qcap) {
-    return (size_t)128 * (2 * pair_eh_words(qcap) + 2 * pair_nib_words(qcap));
+// Blocks per lane: columns up to qcap + 16 (block loads reach (end-1)|7, the row-end scans
+// column end <= qcap, the column-of-maximum scan one block further).
+__host__ __device__ inline int pc_blocks(int qcap) { return (qcap + 7) / 8 + 2; }
+__host__ __device__ inline int pc_nib_words(int len) { return (len + 7) / 8 + 2; }
+__host__ __device__ inline size_t pc_warp_bytes(int qcap) {
+    return (size_t)32 * pc_blocks(qcap) * 32 + (size_t)128 * pc_nib_words(qcap);
 }
 
-__device__ __forceinline__ int ehw(int k, int L) { return (((k >> 2) * 32 + L) << 2) + (k & 3); }
-
-// Scores of column byte t of both jobs as int16x2: byte t of a (job a) and byte t of b (job b),
-// each sign-extended to 16 bits, in one prmt.
-template <int t>
-__device__ __forceinline__ uint32_t pair_score(uint32_t a, uint32_t b) {
-    constexpr uint32_t sel = (uint32_t)t | ((8u | t) << 4) | ((4u + t) << 8) | ((8u | (4u + t)) << 12);
+template <uint32_t SEL>
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b) {
     uint32_t r;
-    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "n"(sel));
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "n"(SEL));
     return r;
 }
 
-__device__ __forceinline__ int32_t half_of(uint32_t w, int x) {
-    return x ? (int32_t)(int16_t)(w >> 16) : (int32_t)(int16_t)(w & 0xFFFFu);
+// Scores of columns p and p+4 of a block as int16x2: byte p of lo and byte p of hi, each
+// sign-extended to 16 bits.
+template <int p>
+__device__ __forceinline__ uint32_t pair_score(uint32_t lo, uint32_t hi) {
+    constexpr uint32_t sel = (uint32_t)p | ((8u | p) << 4) | ((4u + p) << 8) | ((8u | (4u + p)) << 12);
+    return prmt<sel>(lo, hi);
 }
 
-struct HalfJob {
+template <int t>
+__device__ __forceinline__ int32_t sbyte(uint32_t x) {
+    constexpr uint32_t sel = (uint32_t)t | ((8u | t) << 4) | ((8u | t) << 8) | ((8u | t) << 12);
+    uint32_t r;
+    asm("prmt.b32 %0, %1, 0, %2;" : "=r"(r) : "r"(x), "n"(sel));
+    return (int32_t)r;
+}
+
+__device__ __forceinline__ int32_t score_of(uint32_t lo, uint32_t hi, int t) {
+    switch (t) {
+        case 0: return sbyte<0>(lo);
+        case 1: return sbyte<1>(lo);
+        case 2: return sbyte<2>(lo);
+        case 3: return sbyte<3>(lo);
+        case 4: return sbyte<0>(hi);
+        case 5: return sbyte<1>(hi);
+        case 6: return sbyte<2>(hi);
+        default: return sbyte<3>(hi);
+    }
+}
+
+// The warp's row buffers: per lane and block, a uint4 of H pairs and a uint4 of E pairs.
+struct Planes {
+    uint4* H;
+    uint4* E;
+    uint32_t* H32;   // the same words, one at a time
+    uint32_t* E32;
+};
+
+__device__ __forceinline__ int word_of(int c, int L) { return ((((c >> 3) << 5) + L) << 2) + (c & 3); }
+
+__device__ __forceinline__ int32_t get_col(const uint32_t* P, int c, int L) {
+    const uint32_t w = P[word_of(c, L)];
+    return (int32_t)((c & 4) ? (w >> 16) : (w & 0xFFFFu));
+}
+
+__device__ __forceinline__ void set_col(uint32_t* P, int c, int L, int32_t v) {
+    uint32_t& w = P[word_of(c, L)];
+    w = (c & 4) ? ((w & 0x0000FFFFu) | ((uint32_t)v << 16)) : ((w & 0xFFFF0000u) | ((uint32_t)v & 0xFFFFu));
+}
+
+struct LaneJob {
     int job;                 // -1 = none
     int32_t qlen, tlen, w, h0;
     uint32_t t_off;
@@ -65,87 +105,109 @@ struct HalfJob {
     uint32_t tx, tn, px, pn; // target chunk K.next >> 4 and the next one
 };
 
-// Row state of both halves.
-struct PairRow {
-    int32_t beg[2], end[2];  // per half; halves without a row: beg = end = 0
-    int32_t m[2], mjb[2];
-    uint32_t H1, F;          // int16x2 running H(i, j-1) and F(i, j)
-    uint32_t plo[2], phi[2]; // per half: this row's scores by query code
+struct RowState {
+    int32_t beg, end, h1, f, m, mjb;
+    uint32_t plo, phi;
+    uint32_t hlast;          // high half: H of the last column done (int16x2 carry)
 };
 
 struct PairConst {
     uint32_t noe_del, ne_del, noe_ins, ne_ins;   // negated penalties in both halves
-    int32_t kshift;
+    uint32_t nt[4];          // (-p e_ins, -(p+4) e_ins)
+    uint32_t cv[4];          // (-2^15, -(p+1) e_ins)
+    uint32_t kmul;           // 2^k: M = min(H + S, H * 2^k)
 };
 
-// Per-half mask of the halves whose band holds column col (a band may be empty, beg >= end).
-__device__ __forceinline__ uint32_t pair_mask(const PairRow& r, int32_t col) {
-    const bool va = col >= r.beg[0] && col < r.end[0];
-    const bool vb = col >= r.beg[1] && col < r.end[1];
-    return (va ? 0x0000FFFFu : 0u) | (vb ? 0xFFFF0000u : 0u);
-}
-
-template <bool kMasked>
-__device__ __forceinline__ void pair_block(uint32_t* __restrict__ Hp, uint32_t* __restrict__ Ep,
-                                           const uint32_t* __restrict__ qa, const uint32_t* __restrict__ qb,
-                                           int lane, int32_t jb, PairRow& r, const PairConst& pc) {
-    const int at = ehw(jb, lane);
-    const uint4 h0 = *reinterpret_cast<const uint4*>(Hp + at);
-    const uint4 h1 = *reinterpret_cast<const uint4*>(Hp + at + 128);
-    const uint4 e0 = *reinterpret_cast<const uint4*>(Ep + at);
-    const uint4 e1 = *reinterpret_cast<const uint4*>(Ep + at + 128);
-    const uint32_t Hw[kLB] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
-    const uint32_t Ew[kLB] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-    const uint32_t wa = qa[(jb >> 3) * 32 + lane], wb = qb[(jb >> 3) * 32 + lane];
-    const uint32_t sa_lo = __byte_perm(r.plo[0], r.phi[0], wa), sa_hi = __byte_perm(r.plo[0], r.phi[0], wa >> 16);
-    const uint32_t sb_lo = __byte_perm(r.plo[1], r.phi[1], wb), sb_hi = __byte_perm(r.plo[1], r.phi[1], wb >> 16);
-    uint32_t oH[kLB], oE[kLB], hv[kLB];
-    uint32_t H1 = r.H1, F = r.F;
+// A masked block in int32 (ksw.cu:346-370): cells outside [r.beg, r.end) keep their words.
+__device__ __forceinline__ void block_masked(const Planes& P, const uint32_t* __restrict__ qn, int lane,
+                                             int32_t jb, RowState& r, const ScoreParams& sp) {
+    const int at = ((jb >> 3) << 5) + lane;
+    const uint4 hq = P.H[at], eq = P.E[at];
+    const uint32_t hw[4] = {hq.x, hq.y, hq.z, hq.w}, ew[4] = {eq.x, eq.y, eq.z, eq.w};
+    const uint32_t qw = qn[(jb >> 3) * 32 + lane];
+    const uint32_t sc_lo = __byte_perm(r.plo, r.phi, qw);
+    const uint32_t sc_hi = __byte_perm(r.plo, r.phi, qw >> 16);
+    int32_t oh[kLB], oe[kLB], hv[kLB];
+    int32_t h1 = r.h1, f = r.f;
 #pragma unroll
     for (int t = 0; t < kLB; ++t) {
-        uint32_t S;
-        switch (t & 3) {
-            case 0: S = pair_score<0>(t < 4 ? sa_lo : sa_hi, t < 4 ? sb_lo : sb_hi); break;
-            case 1: S = pair_score<1>(t < 4 ? sa_lo : sa_hi, t < 4 ? sb_lo : sb_hi); break;
-            case 2: S = pair_score<2>(t < 4 ? sa_lo : sa_hi, t < 4 ? sb_lo : sb_hi); break;
-            default: S = pair_score<3>(t < 4 ? sa_lo : sa_hi, t < 4 ? sb_lo : sb_hi); break;
-        }
-        const uint32_t H = Hw[t], E = Ew[t];
-        const uint32_t M = __viaddmin_s16x2(H, S, H << pc.kshift);
-        const uint32_t h = __vimax3_s16x2(M, E, F);
-        const uint32_t te = __viaddmax_s16x2(M, pc.noe_del, 0u);
-        const uint32_t en = __viaddmax_s16x2(E, pc.ne_del, te);
-        const uint32_t tf = __viaddmax_s16x2(M, pc.noe_ins, 0u);
-        const uint32_t fn = __viaddmax_s16x2(F, pc.ne_ins, tf);
-        if (kMasked) {
-            const uint32_t m2 = pair_mask(r, jb + t);
-            oH[t] = (H1 & m2) | (H & ~m2);
-            oE[t] = (en & m2) | (E & ~m2);
-            hv[t] = h | ~m2;                       // -1 in a half outside its band
-            F = (fn & m2) | (F & ~m2);
-            H1 = (h & m2) | (H1 & ~m2);
-        } else {
-            oH[t] = H1;
-            oE[t] = en;
-            hv[t] = h;
-            F = fn;
-            H1 = h;
-        }
+        const int32_t hd = (int32_t)(t < 4 ? (hw[t & 3] & 0xFFFFu) : (hw[t & 3] >> 16));
+        const int32_t ed = (int32_t)(t < 4 ? (ew[t & 3] & 0xFFFFu) : (ew[t & 3] >> 16));
+        const int32_t s = score_of(sc_lo, sc_hi, t);
+        const int32_t M = addmin_i32(hd, s, hd * 256);
+        const int32_t h = max3_i32(M, ed, f);
+        const int32_t te = addmax_i32(M, -sp.oe_del, 0);
+        const int32_t e2 = addmax_i32(ed, -sp.e_del, te);
+        const int32_t tf = addmax_i32(M, -sp.oe_ins, 0);
+        const int32_t fn = addmax_i32(f, -sp.e_ins, tf);
+        const int32_t col = jb + t;
+        const bool valid = col >= r.beg && col < r.end;
+        oh[t] = valid ? h1 : hd;
+        oe[t] = valid ? e2 : ed;
+        hv[t] = valid ? h : -1;
+        if (valid) { f = fn; h1 = h; }
     }
-    *reinterpret_cast<uint4*>(Hp + at) = make_uint4(oH[0], oH[1], oH[2], oH[3]);
-    *reinterpret_cast<uint4*>(Hp + at + 128) = make_uint4(oH[4], oH[5], oH[6], oH[7]);
-    *reinterpret_cast<uint4*>(Ep + at) = make_uint4(oE[0], oE[1], oE[2], oE[3]);
-    *reinterpret_cast<uint4*>(Ep + at + 128) = make_uint4(oE[4], oE[5], oE[6], oE[7]);
-    const uint32_t bm = __vimax3_s16x2(__vimax3_s16x2(hv[0], hv[1], hv[2]), __vimax3_s16x2(hv[3], hv[4], hv[5]),
-                                       __vimax3_s16x2(hv[6], hv[7], hv[7]));
-    const int32_t ba = (int32_t)(int16_t)(bm & 0xFFFFu), bb = (int32_t)(int16_t)(bm >> 16);
-    if (ba >= r.m[0]) { r.m[0] = ba; r.mjb[0] = jb; }   // ties: the later block holds the later column
-    if (bb >= r.m[1]) { r.m[1] = bb; r.mjb[1] = jb; }
-    r.H1 = H1;
-    r.F = F;
+    uint4 nh, ne;
+    nh.x = (uint32_t)oh[0] | ((uint32_t)oh[4] << 16); nh.y = (uint32_t)oh[1] | ((uint32_t)oh[5] << 16);
+    nh.z = (uint32_t)oh[2] | ((uint32_t)oh[6] << 16); nh.w = (uint32_t)oh[3] | ((uint32_t)oh[7] << 16);
+    ne.x = (uint32_t)oe[0] | ((uint32_t)oe[4] << 16); ne.y = (uint32_t)oe[1] | ((uint32_t)oe[5] << 16);
+    ne.z = (uint32_t)oe[2] | ((uint32_t)oe[6] << 16); ne.w = (uint32_t)oe[3] | ((uint32_t)oe[7] << 16);
+    P.H[at] = nh;
+    P.E[at] = ne;
+    const int32_t bm = max3_i32(max3_i32(hv[0], hv[1], hv[2]), max3_i32(hv[3], hv[4], hv[5]),
+                                hv[6] > hv[7] ? hv[6] : hv[7]);
+    if (bm >= r.m) { r.m = bm; r.mjb = jb; }   // ties: the later block holds the later column
+    r.h1 = h1;
+    r.f = f;
+    r.hlast = (uint32_t)h1 << 16;
 }
 
-__device__ __forceinline__ JobConst half_const(const HalfJob& J, const ScoreParams& sp) {
+// An unmasked block in int16x2.  Pair p = columns (p, p+4).  The H word written for column c
+// is H(i, c-1): pairs 1..3 take the h pairs of 0..2, pair 0 takes (H(i, jb-1), h(3)).
+__device__ __forceinline__ void block_mid(const Planes& P, const uint32_t* __restrict__ qn, int lane,
+                                          int32_t jb, RowState& r, const PairConst& pc, int32_t e_ins8) {
+    const int at = ((jb >> 3) << 5) + lane;
+    const uint4 hq = P.H[at], eq = P.E[at];
+    const uint32_t H2[4] = {hq.x, hq.y, hq.z, hq.w}, E2[4] = {eq.x, eq.y, eq.z, eq.w};
+    const uint32_t qw = qn[(jb >> 3) * 32 + lane];
+    const uint32_t sc_lo = __byte_perm(r.plo, r.phi, qw);
+    const uint32_t sc_hi = __byte_perm(r.plo, r.phi, qw >> 16);
+    const uint32_t S2[4] = {pair_score<0>(sc_lo, sc_hi), pair_score<1>(sc_lo, sc_hi),
+                            pair_score<2>(sc_lo, sc_hi), pair_score<3>(sc_lo, sc_hi)};
+    uint32_t M2[4], L2[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        M2[p] = __viaddmin_s16x2(H2[p], S2[p], H2[p] * pc.kmul);
+        const uint32_t T2 = __viaddmax_s16x2(M2[p], pc.noe_ins, 0u);
+        // per half: the prefix of V over its own four columns, started at 0
+        L2[p] = p == 0 ? T2 : __viaddmax_s16x2(L2[p - 1], pc.ne_ins, T2);
+    }
+    // (V(p+1), V(p+5)): the high half takes in V(4) = low half of L2[3]
+    const uint32_t v4 = prmt<0x1010>(L2[3], L2[3]);
+    uint32_t Vf[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) Vf[p] = __viaddmax_s16x2(v4, pc.cv[p], L2[p]);
+    const uint32_t fin2 = (uint32_t)r.f * 0x00010001u;
+    uint32_t h2[4], oe[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const uint32_t vp = p == 0 ? prmt<0x1044>(L2[3], 0u) : Vf[p - 1];   // (V(p), V(p+4))
+        const uint32_t F2 = __viaddmax_s16x2(fin2, pc.nt[p], vp);
+        h2[p] = __vimax3_s16x2(M2[p], E2[p], F2);
+        const uint32_t te = __viaddmax_s16x2(M2[p], pc.noe_del, 0u);
+        oe[p] = __viaddmax_s16x2(E2[p], pc.ne_del, te);
+    }
+    P.H[at] = make_uint4(prmt<0x5432>(r.hlast, h2[3]), h2[0], h2[1], h2[2]);
+    P.E[at] = make_uint4(oe[0], oe[1], oe[2], oe[3]);
+    const uint32_t bm2 = __vimax3_s16x2(__vimax3_s16x2(h2[0], h2[1], h2[2]), h2[3], h2[3]);
+    const int32_t blo = (int32_t)(bm2 & 0xFFFFu), bhi = (int32_t)(bm2 >> 16);
+    const int32_t bm = blo > bhi ? blo : bhi;
+    if (bm >= r.m) { r.m = bm; r.mjb = jb; }
+    r.f = addmax_i32(r.f, -e_ins8, (int32_t)(Vf[3] >> 16));              // F(8)
+    r.hlast = h2[3];
+}
+
+__device__ __forceinline__ JobConst job_const(const LaneJob& J, const ScoreParams& sp) {
     JobConst c;
     c.qlen = J.qlen; c.tlen = J.tlen; c.w = J.w; c.h0 = J.h0;
     c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
@@ -153,128 +215,9 @@ __device__ __forceinline__ JobConst half_const(const HalfJob& J, const ScorePara
     return c;
 }
 
-// Row begin of half X (ksw.cu:335-345); sets the half's band, first-column H and score pool.
-template <int X>
-__device__ __forceinline__ void half_begin(HalfJob& J, PairRow& r, const LaunchDesc& d, const ScoreParams& sp,
-                                           const uint2* pools, int32_t& h1) {
-    h1 = 0;
-    r.beg[X] = r.end[X] = 0;
-    r.plo[X] = r.phi[X] = 0;
-    if (J.job < 0 || J.K.stop) return;
-    const int32_t i = J.K.next;
-    int32_t beg = J.beg > i - J.w ? J.beg : i - J.w;
-    int32_t end = J.end < i + J.w + 1 ? J.end : i + J.w + 1;
-    if (end > J.qlen) end = J.qlen;
-    if (beg == 0) {
-        const int32_t h = J.h0 - (sp.o_del + sp.e_del * (i + 1));
-        h1 = h > 0 ? h : 0;
-    }
-    r.beg[X] = beg;
-    r.end[X] = end;
-    if ((i & 15) == 0 && i > 0) {
-        J.tx = J.px; J.tn = J.pn;
-        const int ch = (i >> 4) + 1;
-        if ((ch << 4) < J.tlen) load16(d.codes, d.nmask, J.t_off, J.tlen, ch, J.trev, J.px, J.pn);
-    }
-    uint32_t code = (J.tx >> ((i & 15) << 1)) & 3u;
-    if ((J.tn >> (i & 15)) & 1u) code = 4;
-    const uint2 p = pools[code];
-    r.plo[X] = p.x;
-    r.phi[X] = p.y;
-}
-
-// Row end of half X (ksw.cu:371-391), then the job's output when it stops.
-template <int X>
-__device__ __forceinline__ void half_end(HalfJob& J, const PairRow& r, uint32_t* Hp, uint32_t* Ep, int lane,
-                                         const LaunchDesc& d, const ScoreParams& sp) {
-    if (J.job < 0) return;
-    if (!J.K.stop) {
-        const uint32_t keep = X ? 0x0000FFFFu : 0xFFFF0000u;
-        const int32_t beg = r.beg[X], end = r.end[X];
-        const bool nonempty = beg < end;
-        const int32_t h1 = half_of(r.H1, X);
-        {   // eh[end] = {h1, 0} (ksw.cu:371), in this half only
-            const int at = ehw(end, lane);
-            Hp[at] = (Hp[at] & keep) | ((uint32_t)(h1 & 0xFFFF) << (16 * X));
-            Ep[at] = Ep[at] & keep;
-        }
-        RowDone rd;
-        rd.m = r.m[X];
-        rd.mj = -1;
-        if (rd.m > 0) {
-            const int32_t lo = r.mjb[X] > beg ? r.mjb[X] : beg;
-            const int32_t hi = r.mjb[X] + kLB < end ? r.mjb[X] + kLB : end;
-            for (int32_t c = hi - 1; c >= lo; --c)
-                if (half_of(Hp[ehw(c + 1, lane)], X) == rd.m) { rd.mj = c; break; }
-        }
-        rd.gval = (nonempty ? end : beg) == J.qlen ? h1 : -1;
-        rd.ncells = nonempty ? end - beg : 0;
-        const JobConst c = half_const(J, sp);
-        commit_row(J.K, c, rd);
-        if (!J.K.stop) {
-            int32_t j = beg;
-            while (j < end && half_of(Hp[ehw(j, lane)], X) == 0 && half_of(Ep[ehw(j, lane)], X) == 0) ++j;
-            const int32_t nb = j;
-            j = end;
-            while (j >= nb && half_of(Hp[ehw(j, lane)], X) == 0 && half_of(Ep[ehw(j, lane)], X) == 0) --j;
-            J.beg = nb;
-            J.end = j + 2 < J.qlen ? j + 2 : J.qlen;
-        }
-    }
-    if (J.K.stop) {
-        const Commit& K = J.K;
-        d.out[J.job] = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};
-        d.status[J.job] = G3X_OK;
-        if (d.cells) d.cells[J.job] = (int32_t)K.cells;
-        J.job = -1;
-    }
-}
-
-// Sets up half J for `job` (ksw.cu:305-333); false (status written) when the job does not
-// belong to this kernel.
-__device__ __forceinline__ bool half_stage(HalfJob& J, int job, const LaunchDesc& d, const ScoreParams& sp) {
-    const g3x_job_t jb = d.jobs[job];
-    JobConst c;
-    c.qlen = jb.qlen; c.tlen = jb.tlen; c.h0 = jb.h0;
-    c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
-    c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
-    c.w = clamp_w(jb.w, c.qlen, sp.max_sc, sp.end_bonus, sp.o_del, sp.e_del, sp.o_ins, sp.e_ins);
-    if (c.qlen > d.qmax || c.tlen > d.tmax || !job_fits_int16(c, sp.max_sc)) {
-        d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
-        d.status[job] = G3X_ERR_TOO_LONG;
-        if (d.cells) d.cells[job] = 0;
-        J.job = -1;
-        return false;
-    }
-    J.job = job;
-    J.qlen = c.qlen; J.tlen = c.tlen; J.w = c.w; J.h0 = c.h0;
-    J.t_off = jb.t_off;
-    J.trev = (jb.flags & G3X_JOB_TREV) != 0;
-    commit_init(J.K, c);
-    J.beg = 0; J.end = c.qlen;
-    J.tx = J.tn = J.px = J.pn = 0;
-    if (c.tlen > 0) load16(d.codes, d.nmask, J.t_off, c.tlen, 0, J.trev, J.tx, J.tn);
-    if (c.tlen > 16) load16(d.codes, d.nmask, J.t_off, c.tlen, 1, J.trev, J.px, J.pn);
-    return true;
-}
-
-// The warp writes job `job`'s query codes into half plane q of lane L.
-__device__ __forceinline__ void stage_query(uint32_t* q, int L, int job, int lane, const LaunchDesc& d) {
-    const g3x_job_t jb = d.jobs[job];
-    const int qlen = jb.qlen;
-    const bool qrev = (jb.flags & G3X_JOB_QREV) != 0;
-    for (int ch = lane; (ch << 4) < qlen; ch += 32) {
-        uint32_t x, nb;
-        load16(d.codes, d.nmask, jb.q_off, qlen, ch, qrev, x, nb);
-        const uint64_t v = nibbles16(x, nb);
-        q[(2 * ch) * 32 + L] = (uint32_t)v;
-        q[(2 * ch + 1) * 32 + L] = (uint32_t)(v >> 32);
-    }
-}
-
 }  // namespace
 
-size_t lane16_smem_per_warp(int qcap) { return pair_warp_bytes(qcap); }
+size_t lane16_smem_per_warp(int qcap) { return pc_warp_bytes(qcap); }
 
 __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams sp) {
     extern __shared__ __align__(16) char smem[];
@@ -289,12 +232,15 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int qcap = d.qmax;
-    uint32_t* base = reinterpret_cast<uint32_t*>(smem + (size_t)warp * pair_warp_bytes(qcap));
-    uint32_t* Hp = base;
-    uint32_t* Ep = Hp + 32 * pair_eh_words(qcap);
-    uint32_t* qa = Ep + 32 * pair_eh_words(qcap);
-    uint32_t* qb = qa + 32 * pair_nib_words(qcap);
+    const int qcap = d.qmax, tcap = d.tmax;
+    const int nbc = pc_blocks(qcap);
+    char* base = smem + (size_t)warp * pc_warp_bytes(qcap);
+    Planes P;
+    P.H = reinterpret_cast<uint4*>(base);
+    P.E = P.H + 32 * nbc;
+    P.H32 = reinterpret_cast<uint32_t*>(P.H);
+    P.E32 = reinterpret_cast<uint32_t*>(P.E);
+    uint32_t* qn = reinterpret_cast<uint32_t*>(P.E + 32 * nbc);
     const int n = d.count ? *d.count : d.n;
     const int* order = d.order ? d.order + (d.order_off ? *d.order_off : 0) : nullptr;
     const int refill = d.warp_batch ? 32 : (d.refill > 0 ? d.refill : 1);
@@ -303,102 +249,165 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
     pc.ne_del = (uint32_t)(uint16_t)(-sp.e_del) * 0x00010001u;
     pc.noe_ins = (uint32_t)(uint16_t)(-sp.oe_ins) * 0x00010001u;
     pc.ne_ins = (uint32_t)(uint16_t)(-sp.e_ins) * 0x00010001u;
-    pc.kshift = int16_shift(sp.max_sc);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        pc.nt[p] = (uint32_t)(uint16_t)(-p * sp.e_ins) | ((uint32_t)(uint16_t)(-(p + 4) * sp.e_ins) << 16);
+        pc.cv[p] = 0x8000u | ((uint32_t)(uint16_t)(-(p + 1) * sp.e_ins) << 16);
+    }
+    pc.kmul = 1u << int16_shift(sp.max_sc);
+    const int32_t e_ins8 = 8 * sp.e_ins;
 
-    HalfJob A, B;
-    A.job = B.job = -1;
+    LaneJob J;
+    J.job = -1;
     bool exhausted = false;
     unsigned long long busy = 0, idle = 0, waves = 0;
     for (;;) {
-        // ---- refill wave: every lane whose two jobs are done takes the next two jobs ----
-        const unsigned idle_mask = __ballot_sync(0xFFFFFFFFu, A.job < 0 && B.job < 0);
+        // ---- refill wave: the warp stages one new job for every idle lane, together ----
+        const unsigned idle_mask = __ballot_sync(0xFFFFFFFFu, J.job < 0);
         if (!exhausted && __popc(idle_mask) >= (idle_mask == 0xFFFFFFFFu ? 1 : refill)) {
             const int want = __popc(idle_mask);
             int first = 0;
-            if (lane == 0) first = atomicAdd(d.queue, 2 * want);
+            if (lane == 0) first = atomicAdd(d.queue, want);
             first = __shfl_sync(0xFFFFFFFFu, first, 0);
-            if (first + 2 * want >= n) exhausted = true;
+            if (first + want >= n) exhausted = true;
             ++waves;
-            int ja = -1, jbj = -1;
+            int my_job = -1;
             if ((idle_mask >> lane) & 1u) {
-                const int slot = first + 2 * __popc(idle_mask & ((1u << lane) - 1u));
-                if (slot < n && half_stage(A, order ? order[slot] : slot, d, sp)) ja = A.job;
-                if (slot + 1 < n && half_stage(B, order ? order[slot + 1] : slot + 1, d, sp)) jbj = B.job;
+                const int slot = first + __popc(idle_mask & ((1u << lane) - 1u));
+                if (slot < n) {
+                    const int job = order ? order[slot] : slot;
+                    const g3x_job_t jb = d.jobs[job];
+                    JobConst c;
+                    c.qlen = jb.qlen; c.tlen = jb.tlen; c.h0 = jb.h0;
+                    c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
+                    c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
+                    c.w = clamp_w(jb.w, c.qlen, sp.max_sc, sp.end_bonus, sp.o_del, sp.e_del, sp.o_ins, sp.e_ins);
+                    if (c.qlen > qcap || c.tlen > tcap || !job_fits_int16(c, sp.max_sc)) {
+                        d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
+                        d.status[job] = G3X_ERR_TOO_LONG;
+                        if (d.cells) d.cells[job] = 0;
+                    } else {
+                        my_job = job;
+                        J.job = job;
+                        J.qlen = c.qlen; J.tlen = c.tlen; J.w = c.w; J.h0 = c.h0;
+                        J.t_off = jb.t_off;
+                        J.trev = (jb.flags & G3X_JOB_TREV) != 0;
+                        commit_init(J.K, c);
+                        J.beg = 0; J.end = c.qlen;
+                        J.tx = J.tn = J.px = J.pn = 0;
+                        if (c.tlen > 0) load16(d.codes, d.nmask, J.t_off, c.tlen, 0, J.trev, J.tx, J.tn);
+                        if (c.tlen > 16) load16(d.codes, d.nmask, J.t_off, c.tlen, 1, J.trev, J.px, J.pn);
+                    }
+                }
             }
-            unsigned m = __ballot_sync(0xFFFFFFFFu, ja >= 0 || jbj >= 0);
+            unsigned m = __ballot_sync(0xFFFFFFFFu, my_job >= 0);
             while (m) {
                 const int L = __ffs(m) - 1;
                 m &= m - 1;
-                const int job_a = __shfl_sync(0xFFFFFFFFu, ja, L);
-                const int job_b = __shfl_sync(0xFFFFFFFFu, jbj, L);
-                JobConst ca, cb;
-                ca.qlen = cb.qlen = 0; ca.h0 = cb.h0 = 0;
-                ca.oe_ins = cb.oe_ins = sp.oe_ins; ca.e_ins = cb.e_ins = sp.e_ins;
-                if (job_a >= 0) { stage_query(qa, L, job_a, lane, d); ca.qlen = d.jobs[job_a].qlen; ca.h0 = d.jobs[job_a].h0; }
-                if (job_b >= 0) { stage_query(qb, L, job_b, lane, d); cb.qlen = d.jobs[job_b].qlen; cb.h0 = d.jobs[job_b].h0; }
-                const int top = (ca.qlen > cb.qlen ? ca.qlen : cb.qlen) + 1;
-                for (int k = lane; k <= top; k += 32) {
-                    const uint32_t va = job_a >= 0 ? (uint32_t)init_h(k, ca) & 0xFFFFu : 0u;
-                    const uint32_t vb = job_b >= 0 ? (uint32_t)init_h(k, cb) & 0xFFFFu : 0u;
-                    Hp[ehw(k, L)] = va | (vb << 16);
-                    Ep[ehw(k, L)] = 0u;
+                const int job = __shfl_sync(0xFFFFFFFFu, my_job, L);
+                const g3x_job_t jb = d.jobs[job];
+                const int qlen = jb.qlen;
+                const bool qrev = (jb.flags & G3X_JOB_QREV) != 0;
+                for (int ch = lane; (ch << 4) < qlen; ch += 32) {
+                    uint32_t x, nb;
+                    load16(d.codes, d.nmask, jb.q_off, qlen, ch, qrev, x, nb);
+                    const uint64_t v = nibbles16(x, nb);
+                    qn[(2 * ch) * 32 + L] = (uint32_t)v;
+                    qn[(2 * ch + 1) * 32 + L] = (uint32_t)(v >> 32);
+                }
+                // row -1 (ksw.cu:317-319): H pairs from the closed form, E = 0
+                JobConst c;
+                c.qlen = qlen; c.h0 = jb.h0; c.oe_ins = sp.oe_ins; c.e_ins = sp.e_ins;
+                const int words = (((qlen + 1) >> 3) + 1) * 4;
+                for (int k = lane; k < words; k += 32) {
+                    const int b = k >> 2, p = k & 3;
+                    const int32_t lo = init_h(8 * b + p, c), hi = init_h(8 * b + p + 4, c);
+                    P.H32[((b << 5) + L) * 4 + p] = ((uint32_t)lo & 0xFFFFu) | ((uint32_t)hi << 16);
+                    P.E32[((b << 5) + L) * 4 + p] = 0u;
                 }
             }
             __syncwarp();
         }
-        const bool active = A.job >= 0 || B.job >= 0;
+        const bool active = J.job >= 0;
         if (!__any_sync(0xFFFFFFFFu, active)) {
             if (exhausted) break;
             continue;
         }
+        const bool run = active && !J.K.stop;
 
-        // ---- row begin for both halves ----
-        PairRow r;
-        int32_t ha, hb;
-        half_begin<0>(A, r, d, sp, pools, ha);
-        half_begin<1>(B, r, d, sp, pools, hb);
-        r.H1 = ((uint32_t)ha & 0xFFFFu) | ((uint32_t)hb << 16);
-        r.F = 0;
-        r.m[0] = r.m[1] = 0;
-        r.mjb[0] = r.mjb[1] = -1;
-        const bool na = r.beg[0] < r.end[0], nb = r.beg[1] < r.end[1];
-        // union of the two bands, and the blocks inside both
-        int nh = 0, nf = 0, nt = 0;
-        int32_t ub0 = 0, fb0 = 0, fb1 = 0;
-        if (na || nb) {
-            const int32_t ubeg = na && nb ? min(r.beg[0], r.beg[1]) : (na ? r.beg[0] : r.beg[1]);
-            const int32_t uend = na && nb ? max(r.end[0], r.end[1]) : (na ? r.end[0] : r.end[1]);
-            ub0 = ubeg & ~(kLB - 1);
-            if (na && nb) {
-                fb0 = (max(r.beg[0], r.beg[1]) + kLB - 1) & ~(kLB - 1);
-                fb1 = min(r.end[0], r.end[1]) & ~(kLB - 1);
+        // ---- row begin (ksw.cu:335-345) ----
+        RowState r;
+        r.beg = 0; r.end = 0; r.h1 = 0; r.f = 0; r.m = 0; r.mjb = -1; r.plo = 0; r.phi = 0; r.hlast = 0;
+        if (run) {
+            const int32_t i = J.K.next;
+            r.beg = J.beg > i - J.w ? J.beg : i - J.w;
+            r.end = J.end < i + J.w + 1 ? J.end : i + J.w + 1;
+            if (r.end > J.qlen) r.end = J.qlen;
+            if (r.beg == 0) {
+                const int32_t h = J.h0 - (sp.o_del + sp.e_del * (i + 1));
+                r.h1 = h > 0 ? h : 0;
             }
-            if (na && nb && fb1 > fb0) {
-                nh = (fb0 - ub0) >> 3;
-                nf = (fb1 - fb0) >> 3;
-                nt = (uend - fb1 + kLB - 1) >> 3;
-            } else {
-                nh = (uend - ub0 + kLB - 1) >> 3;
-                fb0 = fb1 = ub0 + nh * kLB;
+            if ((i & 15) == 0 && i > 0) {
+                J.tx = J.px; J.tn = J.pn;
+                const int ch = (i >> 4) + 1;
+                if ((ch << 4) < J.tlen) load16(d.codes, d.nmask, J.t_off, J.tlen, ch, J.trev, J.px, J.pn);
+            }
+            uint32_t code = (J.tx >> ((i & 15) << 1)) & 3u;
+            if ((J.tn >> (i & 15)) & 1u) code = 4;
+            const uint2 p = pools[code];
+            r.plo = p.x;
+            r.phi = p.y;
+        }
+        const bool nonempty = run && r.beg < r.end;
+        const int32_t jb0 = r.beg & ~(kLB - 1);
+        const int nblk = nonempty ? ((r.end - 1) >> 3) - (r.beg >> 3) + 1 : 0;
+        const int kmax = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nblk);
+        busy += nblk;
+        idle += kmax - nblk;
+
+        // ---- masked first block, unmasked middle blocks in int16x2, masked last block ----
+        if (nblk > 0) block_masked(P, qn, lane, jb0, r, sp);
+        for (int k = 1; k < kmax - 1; ++k)
+            if (k < nblk - 1) block_mid(P, qn, lane, jb0 + k * kLB, r, pc, e_ins8);
+        if (nblk > 2) r.h1 = (int32_t)(r.hlast >> 16);
+        if (nblk > 1) block_masked(P, qn, lane, jb0 + (nblk - 1) * kLB, r, sp);
+
+        // ---- row end (ksw.cu:371-391) ----
+        if (run) {
+            const int32_t beg = r.beg, end = r.end;
+            set_col(P.H32, end, lane, r.h1);
+            set_col(P.E32, end, lane, 0);
+            RowDone rd;
+            rd.m = r.m;
+            rd.mj = -1;
+            if (r.m > 0) {
+                // the last column of the winning block that reaches the maximum; H(i, c) is in
+                // the H word of column c+1
+                const int32_t lo = r.mjb > beg ? r.mjb : beg;
+                const int32_t hi = r.mjb + kLB < end ? r.mjb + kLB : end;
+                for (int32_t c = hi - 1; c >= lo; --c)
+                    if (get_col(P.H32, c + 1, lane) == r.m) { rd.mj = c; break; }
+            }
+            rd.gval = (nonempty ? end : beg) == J.qlen ? r.h1 : -1;
+            rd.ncells = nonempty ? end - beg : 0;
+            commit_row(J.K, job_const(J, sp), rd);
+            if (!J.K.stop) {
+                int32_t j = beg;
+                while (j < end && get_col(P.H32, j, lane) == 0 && get_col(P.E32, j, lane) == 0) ++j;
+                const int32_t nb = j;
+                j = end;
+                while (j >= nb && get_col(P.H32, j, lane) == 0 && get_col(P.E32, j, lane) == 0) --j;
+                J.beg = nb;
+                J.end = j + 2 < J.qlen ? j + 2 : J.qlen;
             }
         }
-        const int kh = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nh);
-        const int kf = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nf);
-        const int kt = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nt);
-        busy += nh + nf + nt;
-        idle += (kh + kf + kt) - (nh + nf + nt);
-
-        // ---- the union's blocks: masked head, unmasked middle, masked tail ----
-        for (int k = 0; k < kh; ++k)
-            if (k < nh) pair_block<true>(Hp, Ep, qa, qb, lane, ub0 + k * kLB, r, pc);
-        for (int k = 0; k < kf; ++k)
-            if (k < nf) pair_block<false>(Hp, Ep, qa, qb, lane, fb0 + k * kLB, r, pc);
-        for (int k = 0; k < kt; ++k)
-            if (k < nt) pair_block<true>(Hp, Ep, qa, qb, lane, fb1 + k * kLB, r, pc);
-
-        // ---- row end for both halves ----
-        half_end<0>(A, r, Hp, Ep, lane, d, sp);
-        half_end<1>(B, r, Hp, Ep, lane, d, sp);
+        if (active && J.K.stop) {
+            const Commit& K = J.K;
+            d.out[J.job] = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};
+            d.status[J.job] = G3X_OK;
+            if (d.cells) d.cells[J.job] = (int32_t)K.cells;
+            J.job = -1;
+        }
         __syncwarp();
     }
     if (d.stats) {
@@ -409,7 +418,7 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
 }
 
 int launch_lane16(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
-    const size_t wb = pair_warp_bytes(d.qmax);
+    const size_t wb = pc_warp_bytes(d.qmax);
     size_t max_smem = 0;
     if (allow_max_smem(lane16_kernel, &max_smem) != cudaSuccess) return G3X_ERR_CUDA;
     if (wb > max_smem) return G3X_ERR_TOO_LONG;

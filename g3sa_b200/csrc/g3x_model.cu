@@ -19,6 +19,7 @@ namespace g3x {
 constexpr int kF = 5, kH = 64;
 constexpr int oW1 = 0, ob1 = oW1 + kH * kF, oW2 = ob1 + kH, ob2 = oW2 + kH * kH, oW3 = ob2 + kH,
               ob3 = oW3 + kH, kParams = ob3 + 1;
+static_assert(oW2 % 4 == 0 && kH % 4 == 0, "W2 rows load as float4");
 static_assert(kParams == G3X_MLP_PARAMS, "parameter count");
 
 // ---- features ---------------------------------------------------------------------------
@@ -76,7 +77,7 @@ __global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
 __global__ void __launch_bounds__(256) predict_kernel(const float* __restrict__ params,
                                                       const float* __restrict__ feat, int n,
                                                       float* __restrict__ out) {
-    __shared__ float w[kParams];
+    __shared__ __align__(16) float w[kParams];
     for (int t = threadIdx.x; t < kParams; t += blockDim.x) w[t] = params[t];
     __syncthreads();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -95,8 +96,16 @@ __global__ void __launch_bounds__(256) predict_kernel(const float* __restrict__ 
     float y = w[ob3];
     for (int u = 0; u < kH; ++u) {
         float a = w[ob2 + u];
+        // the row of W2 four weights per (broadcast) load; the sum keeps its order
+        const float4* row = reinterpret_cast<const float4*>(w + oW2 + u * kH);
 #pragma unroll
-        for (int q = 0; q < kH; ++q) a = fmaf(w[oW2 + u * kH + q], h1[q], a);
+        for (int q = 0; q < kH / 4; ++q) {
+            const float4 c = row[q];
+            a = fmaf(c.x, h1[4 * q], a);
+            a = fmaf(c.y, h1[4 * q + 1], a);
+            a = fmaf(c.z, h1[4 * q + 2], a);
+            a = fmaf(c.w, h1[4 * q + 3], a);
+        }
         y = fmaf(w[oW3 + u], fmaxf(a, 0.0f), y);
     }
     out[k] = y;

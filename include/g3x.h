@@ -97,7 +97,8 @@ const char *g3x_strerror(int code);
 #define G3X_KERNEL_ROLLING 1  /* anti-diagonal wavefront: rows on lanes, 4-cell lane steps */
 #define G3X_KERNEL_ROWPAR  2  /* one row per step: columns on lanes, F by shuffle scan */
 #define G3X_KERNEL_LANE    3  /* one job per lane: the scalar row loop, 8-column blocks */
-#define G3X_KERNEL_LANE16  4  /* two jobs per lane in int16x2 (jobs whose scores fit 16 bits) */
+#define G3X_KERNEL_LANE16  4  /* one job per lane, two cells per int16x2 instruction (jobs whose
+                                 scores fit 16 bits) */
 #define G3X_KERNEL_LANE2   5  /* one job per lane, rows i and i+1 in flight together */
 
 typedef struct {
@@ -148,7 +149,7 @@ int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t *score, const g3
    `warp_batch` = 1 makes a warp pull one job per group at once and wait for all of them
    (jobs then balance by the schedule's cost order), 0 lets each group refill on its own;
    the lane-per-job kernels (lanes = 1) refill their idle lanes in waves of at least `refill`.
-   A lane class with tile = 2 runs two jobs per lane in int16x2; the scheduler sends a job whose
+   A lane class with tile = 2 runs its middle blocks in int16x2; the scheduler sends a job whose
    scores do not provably fit a lane class's arithmetic (16-bit fields, h0 >= 0) to the last
    class instead. */
 #define G3X_MAX_CLASSES 8
@@ -156,7 +157,7 @@ typedef struct {
     int32_t width;        /* widest query of the class (the last class: unbounded) */
     int32_t lanes;        /* 1 = lane-per-job kernel; 4, 8, 16, 32 = row-parallel groups */
     int32_t tile;         /* row-parallel: cells per lane per tile (5, 9, 13); lane kernel: 0
-                             (int32, one job per lane), 2 (int16x2, two jobs per lane) or 4
+                             (int32, one job per lane), 2 (int16x2, two cells per instruction) or 4
                              (int32, one job per lane with two of its rows in flight) */
     int32_t warp_batch;   /* 1: a warp takes its jobs together and waits for all of them */
     int32_t refill;       /* lane kernel: idle lanes that trigger a refill wave (1-32) */
@@ -165,7 +166,7 @@ typedef struct {
 int g3x_get_tiles(g3x_ctx *ctx, g3x_tile_t *h_tiles, int32_t *n);
 int g3x_set_tiles(g3x_ctx *ctx, const g3x_tile_t *h_tiles, int32_t n);
 /* Fits the width classes to the given jobs (device buffers) and tunes them: the class widths
-   become max_qlen * (k/7)^1.5 for k = 1..7 (rounded up to 8 columns, duplicates dropped) plus
+   become max_qlen * ((k + 0.5) / 7.5)^2 for k = 1..7 (rounded up to 8 columns, duplicates dropped) plus
    the unbounded class; then every candidate configuration of each class is timed on the class's
    jobs and the fastest kept in the context; h_tiles/n receive the table.  Blocks.  Outputs of
    the trial runs are discarded. */

@@ -35,7 +35,8 @@ def lane_fits(jobs, score, kernel):
     while (1 << k) < 1 + max_sc and k < 15:
         k += 1
     oe_del, oe_ins = int(score["o_del"][0] + score["e_del"][0]), int(score["o_ins"][0] + score["e_ins"][0])
-    return ok & ((hmax << k) < 32768) & (oe_del < 16384) & (oe_ins < 16384)
+    small = oe_del < 16384 and oe_ins < 16384 and int(score["e_ins"][0]) <= 4095 and int(score["e_del"][0]) <= 4095
+    return ok & ((hmax << k) < 32768) & small
 
 
 def check_status(jobs, score, kernel, status):
