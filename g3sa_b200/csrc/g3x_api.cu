@@ -183,6 +183,7 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
         LaunchDesc d = base;
         d.kernel = tt.lanes[k] != 1 ? kKernelRowpar : tt.tile[k] == 2 ? kKernelLane16
                  : tt.tile[k] == 4 ? kKernelLane2 : kKernelLane;
+        d.ring = tt.lanes[k] == 1 && tt.tile[k] >= 64 ? tt.tile[k] : 0;
         d.lanes = tt.lanes[k];
         d.tile = tt.tile[k];
         d.warp_batch = tt.warp_batch[k];
@@ -404,7 +405,7 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
         const g3x_tile_t& t = h[k];
         const bool lane = t.lanes == 1;
         if ((!lane && t.lanes != 4 && t.lanes != 8 && t.lanes != 16 && t.lanes != 32) ||
-            (!lane && t.tile != 5 && t.tile != 9 && t.tile != 13) || (lane && t.tile != 0 && t.tile != 2 && t.tile != 4) ||
+            (!lane && t.tile != 5 && t.tile != 9 && t.tile != 13) || (lane && t.tile != 0 && t.tile != 2 && t.tile != 4 && (t.tile < 64 || t.tile % 16)) ||
             t.width < 1 ||
             (k && t.width <= h[k - 1].width) || (t.warp_batch != 0 && t.warp_batch != 1) ||
             (lane && (t.refill < 1 || t.refill > 32)))
@@ -507,6 +508,10 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
         pred = ctx->sched.pred;
     }
     if (rc == G3X_OK) rc = g3x::schedule_jobs(ctx->sched, d_jobs, n, sp, pred, ctx->tiles, st);
+    // ring of the lane kernel's ring form: every band of the batch, 2w + 16 columns, rounded up
+    int32_t wmax = 0, ring = 0;
+    if (rc == G3X_OK) rc = g3x::batch_max_w(d_jobs, n, sp, ctx->d_queue + 32, &wmax, st);
+    if (rc == G3X_OK && wmax > 0) ring = (2 * wmax + 16 + 15) & ~15;
     int32_t oc[2 * g3x::kMaxBuckets];
     if (rc == G3X_OK && cudaMemcpy(oc, ctx->sched.bucket_oc, sizeof(oc), cudaMemcpyDeviceToHost) != cudaSuccess)
         rc = G3X_ERR_CUDA;
@@ -527,6 +532,10 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
             for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 2, 0, rf};
         if (!last && g3x::lane2_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen)) <= 200 * 1024)
             for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 4, 0, rf};
+        // the ring form of the lane kernel, where the band is narrower than the class's queries
+        if (!last && ring > 0 && ring < g3x::class_qcap(ctx->tiles, k, max_qlen) + 19 &&
+            g3x::lane_ring_smem_per_warp(ring) <= 200 * 1024)
+            for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, ring, 0, rf};
         for (int l : {4, 8, 16, 32})
             for (int c : {5, 9, 13}) {
                 const int S = l * c;

@@ -43,6 +43,7 @@ struct LaunchDesc {
     int32_t warp_batch;    // persistent row-parallel: 1 = a warp pulls one job per group at
                            // once and waits for all of them; 0 = each group refills alone
     int32_t refill;        // lane-per-job kernel: idle lanes that trigger a refill wave
+    int32_t ring;          // lane-per-job kernel: 0, or the columns of its row-buffer ring
 };
 
 // Tile configurations by job width class (ascending width; the last class is unbounded).
@@ -68,6 +69,9 @@ struct SchedScratch {
 };
 int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScoreParams& sp,
                   const float* pred, const TileTable& tt, cudaStream_t st);
+// Largest band width w (after the clamp of ksw.cu:321-329) over n jobs; blocks.
+int batch_max_w(const g3x_job_t* jobs, int n, const ScoreParams& sp, int32_t* d_tmp, int32_t* h_out,
+                cudaStream_t st);
 
 constexpr int32_t kKernelRolling = 1;   // anti-diagonal wavefront, rows on lanes
 constexpr int32_t kKernelRowpar = 2;    // one row per step, columns on lanes
@@ -100,6 +104,7 @@ int launch_lane16(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t strea
 int launch_lane2(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 size_t lane2_smem_per_warp(int qcap);
 size_t lane16_smem_per_warp(int qcap);
+size_t lane_ring_smem_per_warp(int ring);
 size_t lane_smem_per_warp(int qcap, int tcap);
 
 // Device scratch of one seed-level call (capacity >= n seeds).

@@ -23,6 +23,14 @@
 // planes in global memory, sixteen codes at a time, one chunk ahead.  Idle lanes are refilled
 // in waves at row boundaries: when at least `refill` lanes of the warp are idle, the whole warp
 // stages one new job per idle lane together.
+//
+// Ring variant (kRing, for queries longer than the band): a row only touches columns
+// [beg, end] inside [i-w, i+w+1], columns left of beg are never read again (beg never
+// decreases), and a column right of every band so far still holds its row -1 value.  So the
+// row buffer and the query codes live in rings of R >= 2w+16 columns (column c in slot
+// c mod R): the valid columns a row reads or writes span at most 2w+2, so no two of them share
+// a slot, and every column entering the band for the first time is given its row -1 value
+// (ksw.cu:317-319) first.  Shared memory then no longer grows with the query.
 #include <cuda_runtime.h>
 #include "g3x_core.h"
 #include "g3x_internal.h"
@@ -51,6 +59,7 @@ __device__ __forceinline__ int32_t sbyte(uint32_t x) {
 
 struct LaneJob {
     int job;                 // job index, -1 = none
+    int32_t hi, qc;          // ring: last column given its row -1 value, query chunks loaded
     int32_t qlen, tlen, w, h0;
     uint32_t t_off;
     int32_t trev;
@@ -75,20 +84,21 @@ struct BlockIn {
     uint32_t qw;
 };
 
+// sb: the block's slot (its first column, or that column mod R for a ring).
 __device__ __forceinline__ BlockIn load_block(const uint32_t* __restrict__ eh, const uint32_t* __restrict__ qn,
-                                              int lane, int32_t jb) {
-    const uint32_t* ep = eh + ehw(jb, lane);
+                                              int lane, int32_t sb) {
+    const uint32_t* ep = eh + ehw(sb, lane);
     BlockIn b;
     b.wa = *reinterpret_cast<const uint4*>(ep);
     b.wb = *reinterpret_cast<const uint4*>(ep + 128);
-    b.qw = qn[(jb >> 3) * 32 + lane];
+    b.qw = qn[(sb >> 3) * 32 + lane];
     return b;
 }
 
 template <bool kMasked>
 __device__ __forceinline__ void lane_block(uint32_t* __restrict__ eh, const BlockIn& in,
-                                           int lane, int32_t jb, RowState& r, const ScoreParams& sp) {
-    uint32_t* ep = eh + ehw(jb, lane);
+                                           int lane, int32_t jb, int32_t sb, RowState& r, const ScoreParams& sp) {
+    uint32_t* ep = eh + ehw(sb, lane);
     const uint4 wa = in.wa, wb = in.wb;
     const uint32_t wv[kLB] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
     const uint32_t qw = in.qw;
@@ -148,9 +158,9 @@ struct InsSteps {
 // the only value a block hands to the next through a dependency chain is F_in itself (one
 // operation per block instead of eight).
 __device__ __forceinline__ void lane_block_mid(uint32_t* __restrict__ eh, const BlockIn& in, int lane,
-                                               int32_t jb, RowState& r, const ScoreParams& sp,
+                                               int32_t jb, int32_t sb, RowState& r, const ScoreParams& sp,
                                                const InsSteps& ins) {
-    uint32_t* ep = eh + ehw(jb, lane);
+    uint32_t* ep = eh + ehw(sb, lane);
     const uint32_t wv[kLB] = {in.wa.x, in.wa.y, in.wa.z, in.wa.w, in.wb.x, in.wb.y, in.wb.z, in.wb.w};
     const uint32_t sc_lo = __byte_perm(r.plo, r.phi, in.qw);
     const uint32_t sc_hi = __byte_perm(r.plo, r.phi, in.qw >> 16);
@@ -209,8 +219,15 @@ __host__ __device__ inline size_t lane_warp_bytes(int qcap) {
     return (size_t)128 * (lane_eh_words(qcap) + lane_nib_words(qcap));
 }
 
-size_t lane_smem_per_warp(int qcap, int tcap) { (void)tcap; return lane_warp_bytes(qcap); }
+// A ring of R columns: R row-buffer slots and R/8 query words per lane.
+__host__ __device__ inline size_t ring_warp_bytes(int R) { return (size_t)128 * (R + R / 8); }
 
+size_t lane_smem_per_warp(int qcap, int tcap) { (void)tcap; return lane_warp_bytes(qcap); }
+size_t lane_ring_smem_per_warp(int ring) { return ring_warp_bytes(ring); }
+
+__device__ __forceinline__ int32_t wrap_slot(int32_t s, int32_t R) { return s >= R ? s - R : s; }
+
+template <bool kRing>
 __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp) {
     extern __shared__ __align__(16) char smem[];
     __shared__ uint2 pools[5];
@@ -225,9 +242,11 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int qcap = d.qmax, tcap = d.tmax;
-    uint32_t* base = reinterpret_cast<uint32_t*>(smem + (size_t)warp * lane_warp_bytes(qcap));
+    const int32_t R = kRing ? d.ring : 1;                        // ring columns (multiple of 16)
+    uint32_t* base = reinterpret_cast<uint32_t*>(
+        smem + (size_t)warp * (kRing ? ring_warp_bytes(R) : lane_warp_bytes(qcap)));
     uint32_t* eh = base;                                         // [slot*32 + lane]
-    uint32_t* qn = eh + 32 * lane_eh_words(qcap);                // [word*32 + lane]
+    uint32_t* qn = eh + 32 * (kRing ? R : lane_eh_words(qcap));  // [word*32 + lane]
     const int n = d.count ? *d.count : d.n;
     const int* order = d.order ? d.order + (d.order_off ? *d.order_off : 0) : nullptr;
     const int refill = d.warp_batch ? 32 : (d.refill > 0 ? d.refill : 1);
@@ -262,7 +281,8 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                     c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
                     c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
                     c.w = clamp_w(jb.w, c.qlen, sp.max_sc, sp.end_bonus, sp.o_del, sp.e_del, sp.o_ins, sp.e_ins);
-                    if (c.qlen > qcap || c.tlen > tcap || !job_fits_lane(c, sp.max_sc)) {
+                    if (c.qlen > qcap || c.tlen > tcap || !job_fits_lane(c, sp.max_sc) ||
+                        (kRing && 2 * c.w + 16 > R)) {
                         d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
                         d.status[job] = G3X_ERR_TOO_LONG;
                         if (d.cells) d.cells[job] = 0;
@@ -274,6 +294,11 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                         J.trev = (jb.flags & G3X_JOB_TREV) != 0;
                         commit_init(J.K, c);
                         J.beg = 0; J.end = c.qlen;
+                        if (kRing) {   // staged below: columns 0 .. min(qlen + 1, R - 1), query chunks
+                            J.hi = c.qlen + 1 < R - 1 ? c.qlen + 1 : R - 1;
+                            const int32_t qc = (c.qlen + 15) >> 4;
+                            J.qc = qc < (R >> 4) ? qc : (R >> 4);
+                        }
                         J.tx = J.tn = J.px = J.pn = 0;
                         if (c.tlen > 0) load16(d.codes, d.nmask, J.t_off, c.tlen, 0, J.trev, J.tx, J.tn);
                         if (c.tlen > 16) load16(d.codes, d.nmask, J.t_off, c.tlen, 1, J.trev, J.px, J.pn);
@@ -288,7 +313,9 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                 const g3x_job_t jb = d.jobs[job];
                 const int qlen = jb.qlen;
                 const bool qrev = (jb.flags & G3X_JOB_QREV) != 0;
-                for (int ch = lane; (ch << 4) < qlen; ch += 32) {
+                const int qchunks = kRing ? ((qlen + 15) >> 4 < (R >> 4) ? (qlen + 15) >> 4 : (R >> 4))
+                                          : (qlen + 15) >> 4;
+                for (int ch = lane; ch < qchunks; ch += 32) {
                     uint32_t x, nb;
                     load16(d.codes, d.nmask, jb.q_off, qlen, ch, qrev, x, nb);
                     const uint64_t v = nibbles16(x, nb);
@@ -297,7 +324,8 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                 }
                 JobConst c;
                 c.qlen = qlen; c.h0 = jb.h0; c.oe_ins = sp.oe_ins; c.e_ins = sp.e_ins;
-                for (int k = lane; k <= qlen + 1; k += 32) eh[ehw(k, L)] = (uint32_t)init_h(k, c) << 16;
+                const int top = kRing ? (qlen + 1 < R - 1 ? qlen + 1 : R - 1) : qlen + 1;
+                for (int k = lane; k <= top; k += 32) eh[ehw(k, L)] = (uint32_t)init_h(k, c) << 16;
             }
             __syncwarp();
         }
@@ -331,9 +359,32 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
             const uint2 p = pools[code];
             r.plo = p.x;
             r.phi = p.y;
+            if (kRing && r.beg < r.end) {
+                // columns entering the band for the first time get their row -1 value
+                if (J.hi < r.end - 1) {
+                    JobConst c;
+                    c.qlen = J.qlen; c.h0 = J.h0; c.oe_ins = sp.oe_ins; c.e_ins = sp.e_ins;
+                    for (int32_t col = J.hi + 1; col < r.end; ++col)
+                        eh[ehw(col % R, lane)] = (uint32_t)init_h(col, c) << 16;
+                    J.hi = r.end - 1;
+                }
+                // query codes of the 16-column chunks up to the band's last block
+                const int32_t need = (r.end - 1) >> 4;
+                while (J.qc <= need) {
+                    uint32_t x, nb;
+                    const g3x_job_t jd = d.jobs[J.job];
+                    load16(d.codes, d.nmask, jd.q_off, J.qlen, J.qc, (jd.flags & G3X_JOB_QREV) != 0, x, nb);
+                    const uint64_t v = nibbles16(x, nb);
+                    const int32_t wq = (2 * J.qc) % (kRing ? (R >> 3) : 1);
+                    qn[wq * 32 + lane] = (uint32_t)v;
+                    qn[(wq + 1) * 32 + lane] = (uint32_t)(v >> 32);
+                    ++J.qc;
+                }
+            }
         }
         const bool nonempty = run && r.beg < r.end;
         const int32_t jb0 = r.beg & ~(kLB - 1);
+        const int32_t sb0 = kRing ? jb0 % R : jb0;                     // slot of the first block
         const int nblk = nonempty ? ((r.end - 1) >> 3) - (r.beg >> 3) + 1 : 0;
         const int kmax = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nblk);
         busy += nblk;
@@ -342,25 +393,27 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
         // ---- the row's blocks: masked first block, unmasked middle, masked last block ----
         // Each middle block's words are loaded one block ahead (blocks never overlap, so the
         // load may precede the previous block's store).
+        // slots advance with the columns; a ring wraps at R
+        auto slot_at = [&](int k) { return kRing ? wrap_slot(sb0 + k * kLB, R) : jb0 + k * kLB; };
         BlockIn next;
-        if (nblk > 2) next = load_block(eh, qn, lane, jb0 + kLB);
-        if (nblk > 0) lane_block<true>(eh, load_block(eh, qn, lane, jb0), lane, jb0, r, sp);
+        if (nblk > 2) next = load_block(eh, qn, lane, slot_at(1));
+        if (nblk > 0) lane_block<true>(eh, load_block(eh, qn, lane, sb0), lane, jb0, sb0, r, sp);
         for (int k = 1; k < kmax - 1; ++k) {
             if (k < nblk - 1) {
                 const BlockIn cur = next;
-                if (k + 1 < nblk - 1) next = load_block(eh, qn, lane, jb0 + (k + 1) * kLB);
-                lane_block_mid(eh, cur, lane, jb0 + k * kLB, r, sp, ins);
+                if (k + 1 < nblk - 1) next = load_block(eh, qn, lane, slot_at(k + 1));
+                lane_block_mid(eh, cur, lane, jb0 + k * kLB, slot_at(k), r, sp, ins);
             }
         }
         if (nblk > 1) {
-            const int32_t jl = jb0 + (nblk - 1) * kLB;
-            lane_block<true>(eh, load_block(eh, qn, lane, jl), lane, jl, r, sp);
+            const int32_t jl = jb0 + (nblk - 1) * kLB, sl = slot_at(nblk - 1);
+            lane_block<true>(eh, load_block(eh, qn, lane, sl), lane, jl, sl, r, sp);
         }
 
         // ---- row end (ksw.cu:371-391) ----
         if (run) {
             const int32_t beg = r.beg, end = r.end;
-            if (end >= 0) eh[ehw(end, lane)] = (uint32_t)r.h1 << 16;
+            if (end >= 0) eh[ehw(kRing ? end % R : end, lane)] = (uint32_t)r.h1 << 16;
             RowDone rd;
             rd.m = r.m;
             rd.mj = -1;
@@ -370,9 +423,11 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                 const int32_t mjb = r.mjb;
                 const int32_t lo = mjb > beg ? mjb : beg;
                 const int32_t hi = mjb + kLB < end ? mjb + kLB : end;
-                const uint4 a = *reinterpret_cast<const uint4*>(eh + ehw(mjb, lane));
-                const uint4 b = *reinterpret_cast<const uint4*>(eh + ehw(mjb + 4, lane));
-                const uint32_t hs[kLB] = {a.y, a.z, a.w, b.x, b.y, b.z, b.w, eh[ehw(mjb + 8, lane)]};
+                const int32_t ms = kRing ? mjb % R : mjb;
+                const uint4 a = *reinterpret_cast<const uint4*>(eh + ehw(ms, lane));
+                const uint4 b = *reinterpret_cast<const uint4*>(eh + ehw(ms + 4, lane));
+                const int32_t m8 = kRing ? wrap_slot(ms + 8, R) : ms + 8;
+                const uint32_t hs[kLB] = {a.y, a.z, a.w, b.x, b.y, b.z, b.w, eh[ehw(m8, lane)]};
 #pragma unroll
                 for (int t = 0; t < kLB; ++t) {
                     const int32_t c = mjb + t;
@@ -385,10 +440,20 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
             commit_row(J.K, c, rd);
             if (!J.K.stop) {
                 int32_t j = beg;
-                while (j < end && eh[ehw(j, lane)] == 0u) ++j;
+                if (kRing) {
+                    int32_t s = beg % R;
+                    while (j < end && eh[ehw(s, lane)] == 0u) { ++j; s = wrap_slot(s + 1, R); }
+                } else {
+                    while (j < end && eh[ehw(j, lane)] == 0u) ++j;
+                }
                 const int32_t nb = j;
                 j = end;
-                while (j >= nb && eh[ehw(j, lane)] == 0u) --j;
+                if (kRing) {
+                    int32_t s = end % R;
+                    while (j >= nb && eh[ehw(s, lane)] == 0u) { --j; s = s == 0 ? R - 1 : s - 1; }
+                } else {
+                    while (j >= nb && eh[ehw(j, lane)] == 0u) --j;
+                }
                 J.beg = nb;
                 J.end = j + 2 < J.qlen ? j + 2 : J.qlen;
             }
@@ -409,10 +474,11 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
     }
 }
 
-int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
-    const size_t wb = lane_warp_bytes(d.qmax);
+template <bool kRing>
+static int launch_lane_t(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
+    const size_t wb = kRing ? ring_warp_bytes(d.ring) : lane_warp_bytes(d.qmax);
     size_t max_smem = 0;
-    if (allow_max_smem(lane_kernel, &max_smem) != cudaSuccess) return G3X_ERR_CUDA;
+    if (allow_max_smem(lane_kernel<kRing>, &max_smem) != cudaSuccess) return G3X_ERR_CUDA;
     if (wb > max_smem) return G3X_ERR_TOO_LONG;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return G3X_ERR_CUDA;
@@ -425,13 +491,22 @@ int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream)
         const size_t smem = (size_t)wpb * wb;
         if (smem > max_smem) break;
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane_kernel, 32 * wpb, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane_kernel<kRing>, 32 * wpb, smem);
         if (per_sm * wpb >= best_warps) { best_warps = per_sm * wpb; best_wpb = wpb; best_blocks = per_sm; }
     }
     const size_t smem = (size_t)best_wpb * wb;
     int blocks = d.blocks > 0 ? d.blocks : sms * (best_blocks > 0 ? best_blocks : 1);
-    lane_kernel<<<blocks, 32 * best_wpb, smem, stream>>>(d, sp);
+    lane_kernel<kRing><<<blocks, 32 * best_wpb, smem, stream>>>(d, sp);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
+
+// The ring form when the launch names a ring (d.ring > 0, a multiple of 16, at least 64).
+int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
+    if (d.ring > 0) {
+        if (d.ring < 64 || d.ring % 16) return G3X_ERR_INVALID;
+        return launch_lane_t<true>(d, sp, stream);
+    }
+    return launch_lane_t<false>(d, sp, stream);
 }
 
 }  // namespace g3x

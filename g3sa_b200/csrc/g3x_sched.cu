@@ -47,7 +47,8 @@ __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScorePara
         c.qlen = jb.qlen; c.tlen = jb.tlen; c.h0 = jb.h0; c.w = w;
         c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
         c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
-        const bool fits = tt.tile[b] == 2 ? job_fits_int16(c, sp.max_sc) : job_fits_lane(c, sp.max_sc);
+        bool fits = tt.tile[b] == 2 ? job_fits_int16(c, sp.max_sc) : job_fits_lane(c, sp.max_sc);
+        if (tt.tile[b] >= 64 && 2 * w + 16 > tt.tile[b]) fits = false;   // band wider than the ring
         if (!fits) b = tt.n - 1;
     }
     // log2 of the row count, 0..16; four bins per doubling, more rows -> earlier bin
@@ -100,7 +101,28 @@ __global__ void scatter_kernel(const int32_t* __restrict__ bin, int n, int32_t* 
     order[at] = k;
 }
 
+__global__ void max_w_kernel(const g3x_job_t* __restrict__ jobs, int n, ScoreParams sp, int32_t* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t w = 0;
+    if (k < n) {
+        const g3x_job_t jb = jobs[k];
+        w = clamp_w(jb.w, jb.qlen, sp.max_sc, sp.end_bonus, sp.o_del, sp.e_del, sp.o_ins, sp.e_ins);
+    }
+    w = (int32_t)__reduce_max_sync(0xFFFFFFFFu, (unsigned)(w > 0 ? w : 0));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, w);
+}
+
 }  // namespace
+
+int batch_max_w(const g3x_job_t* jobs, int n, const ScoreParams& sp, int32_t* d_tmp, int32_t* h_out,
+                cudaStream_t st) {
+    if (cudaMemsetAsync(d_tmp, 0, sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
+    max_w_kernel<<<(n + 255) / 256, 256, 0, st>>>(jobs, n, sp, d_tmp);
+    if (cudaMemcpyAsync(h_out, d_tmp, sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return G3X_ERR_CUDA;
+    return G3X_OK;
+}
 
 int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScoreParams& sp,
                   const float* pred, const TileTable& tt, cudaStream_t st) {

@@ -157,4 +157,4 @@ def test_learned_schedule_gains_over_length_sorted():
         idle[sched] = waited / (busy + waited)
         assert (status.cpu().numpy() == 0).all()
         np.testing.assert_array_equal(out.cpu().numpy(), ref)
-    assert idle[g.SCHED_LEARNED] < idle[g.SCHED_SORTED] - 0.03, idle
+    assert idle[g.SCHED_LEARNED] < idle[g.SCHED_SORTED] - 0.02, idle

@@ -147,3 +147,50 @@ def test_gpu_lane_classes_route_jobs_beyond_16_bits():
     torch.cuda.synchronize()
     assert (status.cpu().numpy() == 0).all()
     np.testing.assert_array_equal(out.cpu().numpy(), ref)
+
+
+# The ring form of the lane kernel (row buffer and query codes in rings of 224 columns, for
+# bands of w <= 104) on long queries; w = 500 jobs do not fit the ring and go to the last class.
+RING_TILES = [(1000, 1, 224, 0, 8), (3000, 1, 224, 0, 32), (6000, 1, 224, 0, 1), (1 << 30, 32, 9, 0, 1)]
+
+
+@pytest.mark.parametrize("name", ["cfg4_w100", "cfg4_w500", "cfg1", "stale", "edge"])
+def test_gpu_ring_classes_exact(name):
+    import torch
+    from tests.gpu_util import to_dev
+    u8, jobs, score, ext = golden_io.load_jobs(name)
+    ctx = g.Context(0)
+    ctx.set_tiles([(max(64, int(jobs["qlen"].max()) // 2), 1, 224, 0, 8)] + RING_TILES[1:]
+                  if name not in ("cfg4_w100", "cfg4_w500") else RING_TILES)
+    codes, nmask = g.pack_planes(u8)
+    d_jobs, d_codes, d_nmask = to_dev(jobs), to_dev(codes), to_dev(nmask)
+    n = len(jobs)
+    out = torch.full((n, 6), -777, dtype=torch.int32, device="cuda")
+    status = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+    ctx.extend_batch(score, d_jobs, n, d_codes, d_nmask, out, status, int(jobs["qlen"].max()),
+                     int(jobs["tlen"].max()), schedule=g.SCHED_SORTED)
+    torch.cuda.synchronize()
+    assert (status.cpu().numpy() == 0).all()
+    np.testing.assert_array_equal(out.cpu().numpy(), ext)
+
+
+def test_gpu_ring_long_fresh():
+    """Fresh long-segment jobs (qlen log-uniform 500-5,000, w = 100) through ring classes."""
+    import torch
+    from tests.gpu_util import to_dev
+    wl = g.synth(4, 400, seed=0x41A6, w=100, unrelated=0.0)
+    sc = g.default_score()
+    ref, rcells, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
+    ctx = g.Context(0)
+    ctx.set_tiles(RING_TILES)
+    codes, nmask = wl.planes()
+    d_jobs, d_codes, d_nmask = to_dev(wl.jobs), to_dev(codes), to_dev(nmask)
+    out = torch.full((wl.n, 6), -777, dtype=torch.int32, device="cuda")
+    status = torch.full((wl.n,), 99, dtype=torch.int32, device="cuda")
+    cells = torch.full((wl.n,), -1, dtype=torch.int32, device="cuda")
+    ctx.extend_batch(sc, d_jobs, wl.n, d_codes, d_nmask, out, status, int(wl.jobs["qlen"].max()),
+                     int(wl.jobs["tlen"].max()), schedule=g.SCHED_SORTED, d_cells=cells)
+    torch.cuda.synchronize()
+    assert (status.cpu().numpy() == 0).all()
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)
+    assert (cells.cpu().numpy() == rcells).all()
