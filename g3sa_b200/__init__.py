@@ -383,13 +383,25 @@ class Context:
     def extend_seeds_stream(self, opt, seeds, codes, nmask, n_bases, regs, status, max_qlen,
                             max_tlen, chunk=65536, schedule=SCHED_SORTED, lanes=0, tile=0,
                             kernel=KERNEL_AUTO):
-        """g3x_extend_seeds_stream on host arrays (numpy or pinned torch tensors)."""
+        """g3x_extend_seeds_stream on host arrays: numpy DSEED_DT records, or a pinned torch
+        tensor holding them (any dtype: the seed count is its byte size / 48)."""
+        if isinstance(seeds, np.ndarray):
+            if seeds.dtype != DSEED_DT:
+                raise ValueError("seeds must be DSEED_DT records (device_seeds())")
+            n_seeds = len(seeds)
+        elif hasattr(seeds, "element_size"):
+            nbytes = seeds.numel() * seeds.element_size()
+            if nbytes % DSEED_DT.itemsize:
+                raise ValueError("seed tensor size is not a whole number of g3x_seed_t records")
+            n_seeds = nbytes // DSEED_DT.itemsize
+        else:
+            n_seeds = len(seeds)
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
             schedule, max_qlen, max_tlen, lanes)
         opts["tile"], opts["kernel"] = tile, kernel
         hp = lambda a: a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr()  # noqa: E731
-        rc = lib().g3x_extend_seeds_stream(self._h, opt.ctypes.data, hp(seeds), len(seeds), hp(codes),
+        rc = lib().g3x_extend_seeds_stream(self._h, opt.ctypes.data, hp(seeds), n_seeds, hp(codes),
                                            hp(nmask), int(n_bases), hp(regs), hp(status), int(chunk),
                                            opts.ctypes.data)
         _check(rc, "g3x_extend_seeds_stream")

@@ -238,6 +238,50 @@ static int run_scheduled(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParams
     return launch_classes(ctx, base, sp, st);
 }
 
+// A seed-level wave through the width classes: the wave's jobs (a subset of the seed job
+// array) sorted like a batch (length-sorted, or by the model's predictions), then one
+// persistent launch per class.
+struct ClassWave {
+    g3x_ctx* ctx;
+    bool learned;
+};
+
+static int run_class_wave(void* user, const LaunchDesc& d, const ScoreParams& sp, cudaStream_t st) {
+    const ClassWave* w = static_cast<const ClassWave*>(user);
+    g3x_ctx* ctx = w->ctx;
+    const float* pred = nullptr;
+    int rc;
+    if (w->learned) {
+        if ((rc = model_features(d.jobs, d.n, d.codes, d.nmask, ctx->sched.feat, st, d.order, d.count))) return rc;
+        if ((rc = model_predict(ctx->model.params, ctx->sched.feat, d.n, ctx->sched.pred, st))) return rc;
+        pred = ctx->sched.pred;
+    }
+    if ((rc = schedule_jobs(ctx->sched, d.jobs, d.n, sp, pred, ctx->tiles, st, d.order, d.count))) return rc;
+    if (cudaMemsetAsync(ctx->d_queue, 0, kMaxBuckets * sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
+    LaunchDesc base = d;
+    base.order = nullptr; base.count = nullptr; base.order_off = nullptr; base.queue = nullptr;
+    return launch_classes(ctx, base, sp, st);
+}
+
+// Whether a seed-level call goes through the width classes, and how to run its waves.
+static int seed_waves(g3x_ctx* ctx, const g3x_batch_opts_t* opts, const LaunchDesc& proto, int64_t n,
+                      ClassWave* cw, WaveRunner* wr, const WaveRunner** out) {
+    *out = nullptr;
+    if (!(proto.persistent && proto.kernel == kKernelRowpar && opts->kernel == G3X_KERNEL_AUTO &&
+          opts->lanes == 0 && opts->tile == 0))
+        return opts->schedule == G3X_SCHED_LEARNED ? G3X_ERR_INVALID : G3X_OK;
+    const bool learned = opts->schedule == G3X_SCHED_LEARNED;
+    if (learned && (!ctx->model.params || !ctx->model.trained)) return G3X_ERR_NOT_TRAINED;
+    int rc = alloc_sched(ctx->sched, n);
+    if (rc) return rc;
+    cw->ctx = ctx;
+    cw->learned = learned;
+    wr->run = run_class_wave;
+    wr->user = cw;
+    *out = wr;
+    return G3X_OK;
+}
+
 }  // namespace g3x
 
 extern "C" {
@@ -595,8 +639,12 @@ int g3x_extend_seeds(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_seed_t* d_see
     proto.cells = nullptr;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
     if ((rc = g3x::alloc_seed_scratch(ctx->seeds, n))) return rc;
+    g3x::ClassWave cw;
+    g3x::WaveRunner wr;
+    const g3x::WaveRunner* runner = nullptr;
+    if ((rc = g3x::seed_waves(ctx, opts, proto, n, &cw, &wr, &runner))) return rc;
     return g3x::extend_seeds(ctx->seeds, *opt, sp, d_seeds, n, d_codes, d_nmask, d_regs, d_status,
-                             proto, (cudaStream_t)stream);
+                             proto, (cudaStream_t)stream, runner);
 }
 
 int g3x_extend_seeds_stream(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_seed_t* h_seeds,
@@ -614,8 +662,12 @@ int g3x_extend_seeds_stream(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_seed_t
     if ((rc = g3x::batch_proto(opts, nullptr, &proto))) return rc;
     proto.cells = nullptr;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    g3x::ClassWave cw;
+    g3x::WaveRunner wr;
+    const g3x::WaveRunner* runner = nullptr;
+    if ((rc = g3x::seed_waves(ctx, opts, proto, chunk > 0 ? chunk : 65536, &cw, &wr, &runner))) return rc;
     return g3x::extend_seeds_stream(ctx->seeds, g3x::alloc_seed_scratch, *opt, sp, h_seeds, n,
-                                    h_codes, h_nmask, n_bases, h_regs, h_status, chunk, proto);
+                                    h_codes, h_nmask, n_bases, h_regs, h_status, chunk, proto, runner);
 }
 
 int g3x_features(g3x_ctx* ctx, const g3x_job_t* d_jobs, int32_t n, const uint32_t* d_codes,

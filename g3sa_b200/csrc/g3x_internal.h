@@ -67,8 +67,11 @@ struct SchedScratch {
     float *feat = nullptr, *pred = nullptr;
     int64_t cap = 0;
 };
+// Sorts jobs 0..n-1, or with `subset` the *subset_n jobs subset[0..] (device arrays, at most
+// n), into width classes; s.order receives job indices.
 int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScoreParams& sp,
-                  const float* pred, const TileTable& tt, cudaStream_t st);
+                  const float* pred, const TileTable& tt, cudaStream_t st,
+                  const int32_t* subset = nullptr, const int32_t* subset_n = nullptr);
 // Largest band width w (after the clamp of ksw.cu:321-329) over n jobs; blocks.
 int batch_max_w(const g3x_job_t* jobs, int n, const ScoreParams& sp, int32_t* d_tmp, int32_t* h_out,
                 cudaStream_t st);
@@ -117,14 +120,22 @@ struct SeedScratch {
     int64_t cap;
 };
 
+// Runs one wave of a seed-level call: d names the wave's job array (d.n entries) and its jobs
+// (d.order[0 .. *d.count)); by default one launch of d.kernel over them.
+struct WaveRunner {
+    int (*run)(void* user, const LaunchDesc& d, const ScoreParams& sp, cudaStream_t st);
+    void* user;
+};
+
 int extend_seeds(const SeedScratch& ws, const g3x_opt_t& opt, const ScoreParams& sp,
                  const g3x_seed_t* seeds, int n, const uint32_t* codes, const uint32_t* nmask,
-                 g3x_reg_t* regs, int32_t* status, const LaunchDesc& proto, cudaStream_t st);
+                 g3x_reg_t* regs, int32_t* status, const LaunchDesc& proto, cudaStream_t st,
+                 const WaveRunner* runner = nullptr);
 int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), const g3x_opt_t& opt,
                         const ScoreParams& sp, const g3x_seed_t* h_seeds, int64_t n,
                         const uint32_t* h_codes, const uint32_t* h_nmask, int64_t n_bases,
                         g3x_reg_t* h_regs, int32_t* h_status, int32_t chunk,
-                        const LaunchDesc& proto);
+                        const LaunchDesc& proto, const WaveRunner* runner = nullptr);
 int score_params(const g3x_score_t* s, ScoreParams* sp);
 
 // Learned cost model state (device buffers; g3x_model.cu).
@@ -141,7 +152,8 @@ int model_alloc(ModelState& M, int batch);
 void model_free(ModelState& M);
 int model_init(ModelState& M, uint64_t seed);
 int model_features(const g3x_job_t* jobs, int n, const uint32_t* codes, const uint32_t* nmask,
-                   float* feat, cudaStream_t st);
+                   float* feat, cudaStream_t st,
+                   const int32_t* subset = nullptr, const int32_t* subset_n = nullptr);
 int model_predict(const float* params, const float* feat, int n, float* out, cudaStream_t st);
 int model_gradient(ModelState& M, const float* X, const float* T, int B, float* h_grad,
                    float* h_loss, cudaStream_t st);

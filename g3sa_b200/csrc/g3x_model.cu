@@ -29,9 +29,11 @@ static_assert(kParams == G3X_MLP_PARAMS, "parameter count");
 // mismatch).  One thread per job.
 __global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
                                 const uint32_t* __restrict__ codes,
-                                const uint32_t* __restrict__ nmask, float* __restrict__ feat) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+                                const uint32_t* __restrict__ nmask, float* __restrict__ feat,
+                                const int32_t* __restrict__ subset, const int32_t* __restrict__ subset_n) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n || (subset_n && k >= *subset_n)) return;
+    if (subset) k = subset[k];              // features of job subset[k], stored at that job
     const g3x_job_t jb = jobs[k];
     const bool qrev = (jb.flags & G3X_JOB_QREV) != 0, trev = (jb.flags & G3X_JOB_TREV) != 0;
     int gc = 0, nq = 0;
@@ -260,9 +262,9 @@ __global__ void perm_kernel(int* __restrict__ idx, int n, unsigned long long see
 // ---- host side ---------------------------------------------------------------------------
 
 int model_features(const g3x_job_t* jobs, int n, const uint32_t* codes, const uint32_t* nmask,
-                   float* feat, cudaStream_t st) {
+                   float* feat, cudaStream_t st, const int32_t* subset, const int32_t* subset_n) {
     if (n <= 0) return G3X_OK;
-    features_kernel<<<(n + 255) / 256, 256, 0, st>>>(jobs, n, codes, nmask, feat);
+    features_kernel<<<(n + 255) / 256, 256, 0, st>>>(jobs, n, codes, nmask, feat, subset, subset_n);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }
 

@@ -27,12 +27,17 @@ constexpr int kLevels = kSchedLevels;  // key levels per bucket: 64 row-count x 
 constexpr int kRowBins = 64, kWidthBins = 32;
 static_assert(kRowBins * kWidthBins == kLevels, "key layout");
 
+// Job of sort position k: k itself, or subset[k] when sorting a subset of *subset_n jobs.
+__device__ __forceinline__ int job_at(int k, const int32_t* subset) { return subset ? subset[k] : k; }
+
 __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScoreParams sp,
                             const float* __restrict__ pred, TileTable tt,
-                            int32_t* __restrict__ bin, int32_t* __restrict__ hist) {
+                            int32_t* __restrict__ bin, int32_t* __restrict__ hist,
+                            const int32_t* __restrict__ subset, const int32_t* __restrict__ subset_n) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const g3x_job_t jb = jobs[k];
+    if (k >= n || (subset_n && k >= *subset_n)) return;
+    const int job = job_at(k, subset);
+    const g3x_job_t jb = jobs[job];
     const int w = clamp_w(jb.w, jb.qlen, sp.max_sc, sp.end_bonus, sp.o_del, sp.e_del, sp.o_ins, sp.e_ins);
     const int wide = jb.qlen < 2 * w + 1 ? jb.qlen : 2 * w + 1;
     // A class stages queries up to its width (the last class any query), and its tile covers
@@ -52,7 +57,7 @@ __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScorePara
         if (!fits) b = tt.n - 1;
     }
     // log2 of the row count, 0..16; four bins per doubling, more rows -> earlier bin
-    float lr = pred ? pred[k] - log2f((float)(wide > 1 ? wide : 1)) : log2f(1.0f + (float)jb.tlen);
+    float lr = pred ? pred[job] - log2f((float)(wide > 1 ? wide : 1)) : log2f(1.0f + (float)jb.tlen);
     int rb = (int)((16.0f - lr) * (kRowBins / 16.0f));
     rb = rb < 0 ? 0 : (rb >= kRowBins ? kRowBins - 1 : rb);
     // eight-column blocks of the widest row, wider -> earlier bin
@@ -94,11 +99,12 @@ __global__ void scan_kernel(const int32_t* __restrict__ hist, int nb, int32_t* _
 }
 
 __global__ void scatter_kernel(const int32_t* __restrict__ bin, int n, int32_t* __restrict__ cursor,
-                               int32_t* __restrict__ order) {
+                               int32_t* __restrict__ order, const int32_t* __restrict__ subset,
+                               const int32_t* __restrict__ subset_n) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    if (k >= n || (subset_n && k >= *subset_n)) return;
     const int at = atomicAdd(cursor + bin[k], 1);
-    order[at] = k;
+    order[at] = job_at(k, subset);
 }
 
 __global__ void max_w_kernel(const g3x_job_t* __restrict__ jobs, int n, ScoreParams sp, int32_t* out) {
@@ -125,13 +131,14 @@ int batch_max_w(const g3x_job_t* jobs, int n, const ScoreParams& sp, int32_t* d_
 }
 
 int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScoreParams& sp,
-                  const float* pred, const TileTable& tt, cudaStream_t st) {
+                  const float* pred, const TileTable& tt, cudaStream_t st, const int32_t* subset,
+                  const int32_t* subset_n) {
     const int nbins = tt.n * kLevels;
     if (cudaMemsetAsync(s.hist, 0, nbins * sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
     const int tb = 256, nb = (n + tb - 1) / tb;
-    cost_kernel<<<nb, tb, 0, st>>>(jobs, n, sp, pred, tt, s.bin, s.hist);
+    cost_kernel<<<nb, tb, 0, st>>>(jobs, n, sp, pred, tt, s.bin, s.hist, subset, subset_n);
     scan_kernel<<<1, 1024, 0, st>>>(s.hist, nbins, s.cursor, s.bucket_oc, tt.n);
-    scatter_kernel<<<nb, tb, 0, st>>>(s.bin, n, s.cursor, s.order);
+    scatter_kernel<<<nb, tb, 0, st>>>(s.bin, n, s.cursor, s.order, subset, subset_n);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }
 

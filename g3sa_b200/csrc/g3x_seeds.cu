@@ -154,7 +154,8 @@ __global__ void right_finish_kernel(const g3x_seed_t* __restrict__ seeds, int n,
 
 int extend_seeds(const SeedScratch& ws, const g3x_opt_t& opt, const ScoreParams& sp,
                  const g3x_seed_t* seeds, int n, const uint32_t* codes, const uint32_t* nmask,
-                 g3x_reg_t* regs, int32_t* status, const LaunchDesc& proto, cudaStream_t st) {
+                 g3x_reg_t* regs, int32_t* status, const LaunchDesc& proto, cudaStream_t st,
+                 const WaveRunner* runner) {
     if (n == 0) return G3X_OK;
     // counters: [0] left wave 1, [1] left wave 2, [2] right wave 1, [3] right wave 2;
     // queue counters of the four persistent launches at [8 .. 11]
@@ -166,7 +167,7 @@ int extend_seeds(const SeedScratch& ws, const g3x_opt_t& opt, const ScoreParams&
         LaunchDesc d = proto;
         d.jobs = jobs; d.codes = codes; d.nmask = nmask; d.out = ext; d.status = jst;
         d.cells = nullptr; d.order = order; d.count = count; d.queue = queue; d.n = n;
-        return launch_extend(d, sp, st);
+        return runner ? runner->run(runner->user, d, sp, st) : launch_extend(d, sp, st);
     };
     int rc;
     if ((rc = wave(ws.ljobs, ws.lext, ws.lstatus, ws.order[0], ws.counters + 0, ws.counters + 8))) return rc;

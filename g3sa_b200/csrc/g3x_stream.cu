@@ -51,7 +51,7 @@ int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), con
                         const ScoreParams& sp, const g3x_seed_t* h_seeds, int64_t n,
                         const uint32_t* h_codes, const uint32_t* h_nmask, int64_t n_bases,
                         g3x_reg_t* h_regs, int32_t* h_status, int32_t chunk,
-                        const LaunchDesc& proto) {
+                        const LaunchDesc& proto, const WaveRunner* runner) {
     if (chunk <= 0) chunk = 65536;
     const int64_t nchunks = (n + chunk - 1) / chunk;
     std::vector<ChunkRange> ranges((size_t)nchunks);
@@ -124,7 +124,7 @@ int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), con
             break;
         }
         if ((rc = extend_seeds(ws, opt, sp, s.d_seeds, (int)R.count, s.d_codes, s.d_nmask, s.d_regs,
-                               s.d_status, proto, comp_st)))
+                               s.d_status, proto, comp_st, runner)))
             break;
         if (cudaMemcpyAsync(s.h_regs, s.d_regs, R.count * sizeof(g3x_reg_t), cudaMemcpyDeviceToHost, comp_st) ||
             cudaMemcpyAsync(s.h_status, s.d_status, R.count * sizeof(int32_t), cudaMemcpyDeviceToHost, comp_st) ||

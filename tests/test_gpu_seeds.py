@@ -86,3 +86,34 @@ def test_seeds_stream_matches_device_form(chunk):
     assert (status == 0).all()
     for f in FIELDS:
         assert (regs[f] == ref[f]).all(), f
+
+
+@pytest.mark.parametrize("sched", [g.SCHED_SORTED, g.SCHED_LEARNED])
+def test_seeds_through_lane_classes(sched):
+    """Each wave of the seed-level call sorted into width classes that run the lane-per-job
+    kernels (int32, int16x2, ring), length-sorted or by a model's predictions."""
+    import torch
+    from tests.gpu_util import to_dev
+    wl = g.synth(2, 20000, seed=0x5EED5, w=100, unrelated=0.2)
+    opt_cpu = nat.opt_from_score(g.default_score(), w=100)
+    ref = nat.oracle_seeds(wl.seeds, wl.u8, opt_cpu)
+    c = g.Context(0)
+    c.set_tiles([(16, 1, 2, 0, 32), (56, 1, 0, 0, 32), (128, 1, 2, 0, 8), (176, 1, 432, 0, 1),
+                 (1 << 30, 32, 9, 0, 1)])
+    if sched == g.SCHED_LEARNED:
+        c.mlp_init(3)
+        c.mlp_set_params(c.mlp_params())
+    codes, nmask = wl.planes()
+    ds = g.device_seeds(wl.seeds)
+    n = len(ds)
+    d_seeds, d_codes, d_nmask = to_dev(ds), to_dev(codes), to_dev(nmask)
+    d_regs = torch.zeros(n * g.REG_DT.itemsize, dtype=torch.uint8, device="cuda")
+    d_status = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+    mq = int(wl.seeds["l_query"].max())
+    mt = int((wl.seeds["rmax1"] - wl.seeds["rmax0"]).max())
+    c.extend_seeds(g.default_opt(w=100), d_seeds, n, d_codes, d_nmask, d_regs, d_status, mq, mt, sched, 0)
+    torch.cuda.synchronize()
+    regs = d_regs.cpu().numpy().view(g.REG_DT)
+    assert (d_status.cpu().numpy() == 0).all()
+    for f in FIELDS:
+        assert (regs[f] == ref[f]).all(), f
