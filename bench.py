@@ -34,7 +34,7 @@ METRIC = "ksw_extend2 GCUPS & extensions/s on 1 B200, learned vs plain schedule,
 # DRAM bytes (read + write) per launch of each kernel at this workload's size, from the ncu
 # captures summarised under profiles/ (a 100k-seed case scaled by 5, the DRAM traffic of a
 # launch growing with the jobs it stages).  None until a capture of that kernel exists.
-TRAFFIC_PER_LAUNCH = {("lane", 232): 27.9e6}
+TRAFFIC_PER_LAUNCH = {("lane", 232): 27.9e6, ("lane16", 232): 34.4e6}
 WORKLOADS = {
     # name: (synth kind, units, w, unrelated, description)
     "cfg2": (2, 500000, 100, 0.2,

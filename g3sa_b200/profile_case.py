@@ -1,5 +1,12 @@
 """Small profiling case: one synthetic batch extended a few times through one schedule.
 
+    python -m g3sa_b200.profile_case --seed-stream [--units 2000000] [--chunk 262144]
+
+runs the seed-level band-retry stream instead (config 5): the generator's seeds, the planes and
+the regions in pinned host memory, g3x_extend_seeds_stream once with the plain kernel and once
+through the width classes (tuned on a job batch of the same generator), both timed, their
+regions compared.
+
     python -m g3sa_b200.profile_case [--kind 2] [--units 100000] [--schedule sorted]
                                      [--kernel auto] [--tiles WIDTH:LANES:TILE:WB:REFILL,...]
                                      [--reps 2]
@@ -33,7 +40,11 @@ def main():
     ap.add_argument("--class-times", action="store_true",
                     help="run the width classes one after another and print each one's time")
     ap.add_argument("--seed", type=int, default=0x6A5 + 2)
+    ap.add_argument("--seed-stream", action="store_true")
+    ap.add_argument("--chunk", type=int, default=262144)
     a = ap.parse_args()
+    if a.seed_stream:
+        return seed_stream(a)
     import torch
     wl = g.synth(a.kind, a.units, seed=a.seed, w=a.w, unrelated=a.unrelated)
     codes, nmask = wl.planes()
@@ -64,6 +75,48 @@ def main():
     bad = int((status != 0).sum())
     print(f"jobs {wl.n} max_qlen {mq} max_tlen {mt} last_batch_ms {dt * 1e3:.3f} job_errors {bad}")
     if bad:
+        raise SystemExit(1)
+
+
+def seed_stream(a):
+    import torch
+    units = a.units if a.units != 100000 else 2000000
+    wl = g.synth(2, units, seed=a.seed, w=a.w, unrelated=a.unrelated)
+    codes, nmask = wl.planes()
+    ds = g.device_seeds(wl.seeds)
+    n = len(ds)
+    pin = lambda x: torch.from_numpy(np.ascontiguousarray(x).view(np.uint8).copy()).pin_memory()  # noqa: E731
+    h_seeds, h_codes, h_nmask = pin(ds), pin(codes), pin(nmask)
+    h_regs = torch.zeros(n * g.REG_DT.itemsize, dtype=torch.uint8).pin_memory()
+    h_status = torch.full((n,), 99, dtype=torch.int32).pin_memory()
+    mq = int(wl.seeds["l_query"].max())
+    mt = int((wl.seeds["rmax1"] - wl.seeds["rmax0"]).max())
+    ctx = g.Context(0)
+    tw = g.synth(2, 200000, seed=a.seed + 1, w=a.w, unrelated=a.unrelated)
+    tc, tn = tw.planes()
+    dev = torch.device("cuda", 0)
+    td = [torch.from_numpy(np.ascontiguousarray(x).view(np.uint8).copy()).to(dev) for x in (tw.jobs, tc, tn)]
+    ctx.autotune(g.default_score(), td[0], tw.n, td[1], td[2], int(tw.jobs["qlen"].max()),
+                 int(tw.jobs["tlen"].max()))
+    opt = g.default_opt(w=a.w)
+    regs = {}
+    for name, sched, chunk in (("plain", g.SCHED_PLAIN, 65536), ("sorted", g.SCHED_SORTED, a.chunk)):
+        dt = 0.0
+        for _ in range(max(a.reps, 1)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.extend_seeds_stream(opt, h_seeds, h_codes, h_nmask, len(wl.u8), h_regs, h_status, mq, mt,
+                                    chunk=chunk, schedule=sched)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+        if (h_status.numpy() != 0).any():
+            raise SystemExit(f"{name}: seed errors")
+        regs[name] = h_regs.numpy().view(g.REG_DT).copy()
+        print(f"{name}: chunk {chunk} seeds {n} last_call_ms {dt * 1e3:.1f} seeds_per_s {n / dt:.4g}")
+    same = all((regs["plain"][f] == regs["sorted"][f]).all()
+               for f in ("rb", "re", "qb", "qe", "score", "truesc", "w"))
+    print(f"regions identical: {same}")
+    if not same:
         raise SystemExit(1)
 
 
