@@ -302,28 +302,20 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                         J.tx = J.tn = J.px = J.pn = 0;
                         if (c.tlen > 0) load16(d.codes, d.nmask, J.t_off, c.tlen, 0, J.trev, J.tx, J.tn);
                         if (c.tlen > 16) load16(d.codes, d.nmask, J.t_off, c.tlen, 1, J.trev, J.px, J.pn);
+                        const int32_t qch = (c.qlen + 15) >> 4;
+                        stage_own_query(d.codes, d.nmask, jb.q_off, c.qlen, (jb.flags & G3X_JOB_QREV) != 0,
+                                        kRing ? (qch < (R >> 4) ? qch : (R >> 4)) : qch, qn, lane);
                     }
                 }
             }
+            // row -1 of every new job (ksw.cu:317-319), the whole warp on one job at a time
             unsigned m = __ballot_sync(0xFFFFFFFFu, my_job >= 0);
             while (m) {
                 const int L = __ffs(m) - 1;
                 m &= m - 1;
-                const int job = __shfl_sync(0xFFFFFFFFu, my_job, L);
-                const g3x_job_t jb = d.jobs[job];
-                const int qlen = jb.qlen;
-                const bool qrev = (jb.flags & G3X_JOB_QREV) != 0;
-                const int qchunks = kRing ? ((qlen + 15) >> 4 < (R >> 4) ? (qlen + 15) >> 4 : (R >> 4))
-                                          : (qlen + 15) >> 4;
-                for (int ch = lane; ch < qchunks; ch += 32) {
-                    uint32_t x, nb;
-                    load16(d.codes, d.nmask, jb.q_off, qlen, ch, qrev, x, nb);
-                    const uint64_t v = nibbles16(x, nb);
-                    qn[(2 * ch) * 32 + L] = (uint32_t)v;
-                    qn[(2 * ch + 1) * 32 + L] = (uint32_t)(v >> 32);
-                }
+                const int qlen = __shfl_sync(0xFFFFFFFFu, J.qlen, L);
                 JobConst c;
-                c.qlen = qlen; c.h0 = jb.h0; c.oe_ins = sp.oe_ins; c.e_ins = sp.e_ins;
+                c.qlen = qlen; c.h0 = __shfl_sync(0xFFFFFFFFu, J.h0, L); c.oe_ins = sp.oe_ins; c.e_ins = sp.e_ins;
                 const int top = kRing ? (qlen + 1 < R - 1 ? qlen + 1 : R - 1) : qlen + 1;
                 for (int k = lane; k <= top; k += 32) eh[ehw(k, L)] = (uint32_t)init_h(k, c) << 16;
             }

@@ -12,7 +12,8 @@
 // unpacking or packing.  F runs through the block in its unrolled form,
 // F(t) = max(F_in - t e_ins, V(t)), V(t+1) = max(V(t) - e_ins, T(t)): both halves compute the
 // prefix V over their four columns at once, and the high half then takes in V(4) from the low.
-// The masked blocks and the row end use int32 arithmetic on the same words.
+// The first and last block of a row run the same arithmetic with per-half masks (block_edge),
+// and the row end finds the next band eight columns at a time.
 //
 // Exactness of the 16-bit arithmetic: a job runs here only when every value of its DP fits
 // (job_fits_int16): 0 <= h0, K * (h0 + max_score * min(qlen, tlen)) < 2^15 with K the smallest
@@ -54,27 +55,6 @@ __device__ __forceinline__ uint32_t pair_score(uint32_t lo, uint32_t hi) {
     return prmt<sel>(lo, hi);
 }
 
-template <int t>
-__device__ __forceinline__ int32_t sbyte(uint32_t x) {
-    constexpr uint32_t sel = (uint32_t)t | ((8u | t) << 4) | ((8u | t) << 8) | ((8u | t) << 12);
-    uint32_t r;
-    asm("prmt.b32 %0, %1, 0, %2;" : "=r"(r) : "r"(x), "n"(sel));
-    return (int32_t)r;
-}
-
-__device__ __forceinline__ int32_t score_of(uint32_t lo, uint32_t hi, int t) {
-    switch (t) {
-        case 0: return sbyte<0>(lo);
-        case 1: return sbyte<1>(lo);
-        case 2: return sbyte<2>(lo);
-        case 3: return sbyte<3>(lo);
-        case 4: return sbyte<0>(hi);
-        case 5: return sbyte<1>(hi);
-        case 6: return sbyte<2>(hi);
-        default: return sbyte<3>(hi);
-    }
-}
-
 // The warp's row buffers: per lane and block, a uint4 of H pairs and a uint4 of E pairs.
 struct Planes {
     uint4* H;
@@ -84,11 +64,6 @@ struct Planes {
 };
 
 __device__ __forceinline__ int word_of(int c, int L) { return ((((c >> 3) << 5) + L) << 2) + (c & 3); }
-
-__device__ __forceinline__ int32_t get_col(const uint32_t* P, int c, int L) {
-    const uint32_t w = P[word_of(c, L)];
-    return (int32_t)((c & 4) ? (w >> 16) : (w & 0xFFFFu));
-}
 
 __device__ __forceinline__ void set_col(uint32_t* P, int c, int L, int32_t v) {
     uint32_t& w = P[word_of(c, L)];
@@ -117,50 +92,6 @@ struct PairConst {
     uint32_t cv[4];          // (-2^15, -(p+1) e_ins)
     uint32_t kmul;           // 2^k: M = min(H + S, H * 2^k)
 };
-
-// A masked block in int32 (ksw.cu:346-370): cells outside [r.beg, r.end) keep their words.
-__device__ __forceinline__ void block_masked(const Planes& P, const uint32_t* __restrict__ qn, int lane,
-                                             int32_t jb, RowState& r, const ScoreParams& sp) {
-    const int at = ((jb >> 3) << 5) + lane;
-    const uint4 hq = P.H[at], eq = P.E[at];
-    const uint32_t hw[4] = {hq.x, hq.y, hq.z, hq.w}, ew[4] = {eq.x, eq.y, eq.z, eq.w};
-    const uint32_t qw = qn[(jb >> 3) * 32 + lane];
-    const uint32_t sc_lo = __byte_perm(r.plo, r.phi, qw);
-    const uint32_t sc_hi = __byte_perm(r.plo, r.phi, qw >> 16);
-    int32_t oh[kLB], oe[kLB], hv[kLB];
-    int32_t h1 = r.h1, f = r.f;
-#pragma unroll
-    for (int t = 0; t < kLB; ++t) {
-        const int32_t hd = (int32_t)(t < 4 ? (hw[t & 3] & 0xFFFFu) : (hw[t & 3] >> 16));
-        const int32_t ed = (int32_t)(t < 4 ? (ew[t & 3] & 0xFFFFu) : (ew[t & 3] >> 16));
-        const int32_t s = score_of(sc_lo, sc_hi, t);
-        const int32_t M = addmin_i32(hd, s, hd * 256);
-        const int32_t h = max3_i32(M, ed, f);
-        const int32_t te = addmax_i32(M, -sp.oe_del, 0);
-        const int32_t e2 = addmax_i32(ed, -sp.e_del, te);
-        const int32_t tf = addmax_i32(M, -sp.oe_ins, 0);
-        const int32_t fn = addmax_i32(f, -sp.e_ins, tf);
-        const int32_t col = jb + t;
-        const bool valid = col >= r.beg && col < r.end;
-        oh[t] = valid ? h1 : hd;
-        oe[t] = valid ? e2 : ed;
-        hv[t] = valid ? h : -1;
-        if (valid) { f = fn; h1 = h; }
-    }
-    uint4 nh, ne;
-    nh.x = (uint32_t)oh[0] | ((uint32_t)oh[4] << 16); nh.y = (uint32_t)oh[1] | ((uint32_t)oh[5] << 16);
-    nh.z = (uint32_t)oh[2] | ((uint32_t)oh[6] << 16); nh.w = (uint32_t)oh[3] | ((uint32_t)oh[7] << 16);
-    ne.x = (uint32_t)oe[0] | ((uint32_t)oe[4] << 16); ne.y = (uint32_t)oe[1] | ((uint32_t)oe[5] << 16);
-    ne.z = (uint32_t)oe[2] | ((uint32_t)oe[6] << 16); ne.w = (uint32_t)oe[3] | ((uint32_t)oe[7] << 16);
-    P.H[at] = nh;
-    P.E[at] = ne;
-    const int32_t bm = max3_i32(max3_i32(hv[0], hv[1], hv[2]), max3_i32(hv[3], hv[4], hv[5]),
-                                hv[6] > hv[7] ? hv[6] : hv[7]);
-    if (bm >= r.m) { r.m = bm; r.mjb = jb; }   // ties: the later block holds the later column
-    r.h1 = h1;
-    r.f = f;
-    r.hlast = (uint32_t)h1 << 16;
-}
 
 // An unmasked block in int16x2.  Pair p = columns (p, p+4).  The H word written for column c
 // is H(i, c-1): pairs 1..3 take the h pairs of 0..2, pair 0 takes (H(i, jb-1), h(3)).
@@ -207,6 +138,88 @@ __device__ __forceinline__ void block_mid(const Planes& P, const uint32_t* __res
     r.hlast = h2[3];
 }
 
+// Bit t set when column b+t (b a multiple of 8) has a non-zero H or E word.  Every half-word
+// is reduced to 0 or 1 by an unsigned min, then the four pairs are summed with weights 1-8 (no
+// carry: each half stays below 16), which leaves columns 0-3 in bits 0-3 and 4-7 in bits 16-19.
+__device__ __forceinline__ uint32_t nonzero_cols(const Planes& P, int32_t b, int lane) {
+    const int at = ((b >> 3) << 5) + lane;
+    const uint4 hq = P.H[at], eq = P.E[at];
+    const uint32_t one = 0x00010001u;
+    const uint32_t z0 = __vimin3_u16x2(hq.x | eq.x, one, one), z1 = __vimin3_u16x2(hq.y | eq.y, one, one);
+    const uint32_t z2 = __vimin3_u16x2(hq.z | eq.z, one, one), z3 = __vimin3_u16x2(hq.w | eq.w, one, one);
+    const uint32_t s = z0 + 2u * z1 + 4u * z2 + 8u * z3;
+    return (s & 0xFu) | ((s >> 12) & 0xF0u);
+}
+
+// The first or last block of a row in int16x2 (ksw.cu:346-370 for the columns of [r.beg, r.end)
+// in it).  ge[o] holds, per pair word, 0xFFFF in each half whose column offset is >= o.
+//  * Columns left of the band get H = 0, so their M <= 0 and their F contribution is 0; with
+//    F_in = r.f (0 at a row's first column) the unrolled F of every band column is exact.
+//  * The H word of the band's first column is H(i, beg-1), as the scalar loop writes it.
+//  * Words right of column end keep their stale values (the band can regrow into them); the
+//    row end then sets column end's words as the reference does (ksw.cu:371).
+//  * The row maximum takes band columns only (every band H is >= 0, the rest are cleared).
+// On return r.h1 = H of the last band column of the block and r.hlast holds it in its high half.
+__device__ __forceinline__ void block_edge(const Planes& P, const uint32_t* __restrict__ qn, int lane,
+                                           int32_t jb, RowState& r, const PairConst& pc, int32_t e_ins8,
+                                           const uint4* __restrict__ ge) {
+    const int at = ((jb >> 3) << 5) + lane;
+    const uint4 hq = P.H[at], eq = P.E[at];
+    const int lo = r.beg > jb ? r.beg - jb : 0;
+    const int hi = r.end - jb < kLB ? r.end - jb : kLB;
+    const uint4 ga = ge[lo], gh = ge[hi], gw = ge[hi + 1];
+    const uint32_t A[4] = {ga.x, ga.y, ga.z, ga.w};
+    const uint32_t V[4] = {ga.x & ~gh.x, ga.y & ~gh.y, ga.z & ~gh.z, ga.w & ~gh.w};
+    const uint32_t W[4] = {~gw.x, ~gw.y, ~gw.z, ~gw.w};
+    const uint32_t Hq[4] = {hq.x, hq.y, hq.z, hq.w}, E2[4] = {eq.x, eq.y, eq.z, eq.w};
+    const uint32_t qw = qn[(jb >> 3) * 32 + lane];
+    const uint32_t sc_lo = __byte_perm(r.plo, r.phi, qw);
+    const uint32_t sc_hi = __byte_perm(r.plo, r.phi, qw >> 16);
+    const uint32_t S2[4] = {pair_score<0>(sc_lo, sc_hi), pair_score<1>(sc_lo, sc_hi),
+                            pair_score<2>(sc_lo, sc_hi), pair_score<3>(sc_lo, sc_hi)};
+    uint32_t M2[4], L2[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const uint32_t H2 = Hq[p] & V[p];
+        M2[p] = __viaddmin_s16x2(H2, S2[p], H2 * pc.kmul);
+        const uint32_t T2 = __viaddmax_s16x2(M2[p], pc.noe_ins, 0u);
+        L2[p] = p == 0 ? T2 : __viaddmax_s16x2(L2[p - 1], pc.ne_ins, T2);
+    }
+    const uint32_t v4 = prmt<0x1010>(L2[3], L2[3]);
+    uint32_t Vf[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) Vf[p] = __viaddmax_s16x2(v4, pc.cv[p], L2[p]);
+    const uint32_t fin2 = (uint32_t)r.f * 0x00010001u;
+    const uint32_t hin2 = (r.hlast >> 16) * 0x00010001u;
+    uint32_t h2[4], hw[4], nh[4], ne[4], hm[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const uint32_t vp = p == 0 ? prmt<0x1044>(L2[3], 0u) : Vf[p - 1];
+        const uint32_t F2 = __viaddmax_s16x2(fin2, pc.nt[p], vp);
+        h2[p] = __vimax3_s16x2(M2[p], E2[p], F2);
+        const uint32_t te = __viaddmax_s16x2(M2[p], pc.noe_del, 0u);
+        const uint32_t oe = __viaddmax_s16x2(E2[p], pc.ne_del, te);
+        hw[p] = (h2[p] & A[p]) | (hin2 & ~A[p]);    // left of the band: H(i, beg-1)
+        ne[p] = (oe & W[p]) | (E2[p] & ~W[p]);
+        hm[p] = h2[p] & V[p];
+    }
+    nh[0] = prmt<0x5432>(r.hlast, hw[3]);
+    nh[1] = hw[0]; nh[2] = hw[1]; nh[3] = hw[2];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) nh[p] = (nh[p] & W[p]) | (Hq[p] & ~W[p]);
+    P.H[at] = make_uint4(nh[0], nh[1], nh[2], nh[3]);
+    P.E[at] = make_uint4(ne[0], ne[1], ne[2], ne[3]);
+    const uint32_t bm2 = __vimax3_s16x2(__vimax3_s16x2(hm[0], hm[1], hm[2]), hm[3], hm[3]);
+    const int32_t blo = (int32_t)(bm2 & 0xFFFFu), bhi = (int32_t)(bm2 >> 16);
+    const int32_t bm = blo > bhi ? blo : bhi;
+    if (bm >= r.m) { r.m = bm; r.mjb = jb; }
+    r.f = addmax_i32(r.f, -e_ins8, (int32_t)(Vf[3] >> 16));              // F(8)
+    const int t = hi - 1;
+    const uint32_t wl = (t & 2) ? ((t & 1) ? h2[3] : h2[2]) : ((t & 1) ? h2[1] : h2[0]);
+    r.h1 = (int32_t)((t & 4) ? (wl >> 16) : (wl & 0xFFFFu));
+    r.hlast = (uint32_t)r.h1 << 16;
+}
+
 __device__ __forceinline__ JobConst job_const(const LaneJob& J, const ScoreParams& sp) {
     JobConst c;
     c.qlen = J.qlen; c.tlen = J.tlen; c.w = J.w; c.h0 = J.h0;
@@ -222,6 +235,14 @@ size_t lane16_smem_per_warp(int qcap) { return pc_warp_bytes(qcap); }
 __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams sp) {
     extern __shared__ __align__(16) char smem[];
     __shared__ uint2 pools[5];
+    __shared__ uint4 ge[10];
+    if (threadIdx.x < 10) {
+        const int o = threadIdx.x;
+        uint32_t g[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) g[p] = (p >= o ? 0x0000FFFFu : 0u) | (p + 4 >= o ? 0xFFFF0000u : 0u);
+        ge[o] = make_uint4(g[0], g[1], g[2], g[3]);
+    }
     if (threadIdx.x < 5) {
         uint32_t lo[5], hi[5];
         score_pools(sp, lo, hi);
@@ -297,27 +318,20 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
                         J.tx = J.tn = J.px = J.pn = 0;
                         if (c.tlen > 0) load16(d.codes, d.nmask, J.t_off, c.tlen, 0, J.trev, J.tx, J.tn);
                         if (c.tlen > 16) load16(d.codes, d.nmask, J.t_off, c.tlen, 1, J.trev, J.px, J.pn);
+                        stage_own_query(d.codes, d.nmask, jb.q_off, c.qlen, (jb.flags & G3X_JOB_QREV) != 0,
+                                        (c.qlen + 15) >> 4, qn, lane);
                     }
                 }
             }
+            // row -1 of every new job (ksw.cu:317-319), the whole warp on one job at a time:
+            // H pairs from the closed form, E = 0
             unsigned m = __ballot_sync(0xFFFFFFFFu, my_job >= 0);
             while (m) {
                 const int L = __ffs(m) - 1;
                 m &= m - 1;
-                const int job = __shfl_sync(0xFFFFFFFFu, my_job, L);
-                const g3x_job_t jb = d.jobs[job];
-                const int qlen = jb.qlen;
-                const bool qrev = (jb.flags & G3X_JOB_QREV) != 0;
-                for (int ch = lane; (ch << 4) < qlen; ch += 32) {
-                    uint32_t x, nb;
-                    load16(d.codes, d.nmask, jb.q_off, qlen, ch, qrev, x, nb);
-                    const uint64_t v = nibbles16(x, nb);
-                    qn[(2 * ch) * 32 + L] = (uint32_t)v;
-                    qn[(2 * ch + 1) * 32 + L] = (uint32_t)(v >> 32);
-                }
-                // row -1 (ksw.cu:317-319): H pairs from the closed form, E = 0
+                const int qlen = __shfl_sync(0xFFFFFFFFu, J.qlen, L);
                 JobConst c;
-                c.qlen = qlen; c.h0 = jb.h0; c.oe_ins = sp.oe_ins; c.e_ins = sp.e_ins;
+                c.qlen = qlen; c.h0 = __shfl_sync(0xFFFFFFFFu, J.h0, L); c.oe_ins = sp.oe_ins; c.e_ins = sp.e_ins;
                 const int words = (((qlen + 1) >> 3) + 1) * 4;
                 for (int k = lane; k < words; k += 32) {
                     const int b = k >> 2, p = k & 3;
@@ -366,11 +380,11 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
         idle += kmax - nblk;
 
         // ---- masked first block, unmasked middle blocks in int16x2, masked last block ----
-        if (nblk > 0) block_masked(P, qn, lane, jb0, r, sp);
+        r.hlast = (uint32_t)r.h1 << 16;
+        if (nblk > 0) block_edge(P, qn, lane, jb0, r, pc, e_ins8, ge);
         for (int k = 1; k < kmax - 1; ++k)
             if (k < nblk - 1) block_mid(P, qn, lane, jb0 + k * kLB, r, pc, e_ins8);
-        if (nblk > 2) r.h1 = (int32_t)(r.hlast >> 16);
-        if (nblk > 1) block_masked(P, qn, lane, jb0 + (nblk - 1) * kLB, r, sp);
+        if (nblk > 1) block_edge(P, qn, lane, jb0 + (nblk - 1) * kLB, r, pc, e_ins8, ge);
 
         // ---- row end (ksw.cu:371-391) ----
         if (run) {
@@ -382,23 +396,53 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
             rd.mj = -1;
             if (r.m > 0) {
                 // the last column of the winning block that reaches the maximum; H(i, c) is in
-                // the H word of column c+1
-                const int32_t lo = r.mjb > beg ? r.mjb : beg;
-                const int32_t hi = r.mjb + kLB < end ? r.mjb + kLB : end;
-                for (int32_t c = hi - 1; c >= lo; --c)
-                    if (get_col(P.H32, c + 1, lane) == r.m) { rd.mj = c; break; }
+                // the H word of column c+1: columns mjb+1 .. mjb+7 of the block (pairs 1-3 low,
+                // pairs 0-3 high) and column mjb+8, the first of the next block
+                const int32_t mjb = r.mjb;
+                const int32_t lo = mjb > beg ? mjb : beg;
+                const int32_t hi = mjb + kLB < end ? mjb + kLB : end;
+                const int at = ((mjb >> 3) << 5) + lane;
+                const uint4 hq = P.H[at];
+                const uint32_t nx = P.H[at + 32].x;
+                const uint32_t hs[kLB] = {hq.y, hq.z, hq.w, hq.x >> 16, hq.y >> 16, hq.z >> 16, hq.w >> 16, nx};
+#pragma unroll
+                for (int t = 0; t < kLB; ++t) {
+                    const int32_t c = mjb + t;
+                    if (c >= lo && c < hi && (int32_t)(hs[t] & 0xFFFFu) == r.m) rd.mj = c;
+                }
             }
             rd.gval = (nonempty ? end : beg) == J.qlen ? r.h1 : -1;
             rd.ncells = nonempty ? end - beg : 0;
             commit_row(J.K, job_const(J, sp), rd);
             if (!J.K.stop) {
-                int32_t j = beg;
-                while (j < end && get_col(P.H32, j, lane) == 0 && get_col(P.E32, j, lane) == 0) ++j;
-                const int32_t nb = j;
-                j = end;
-                while (j >= nb && get_col(P.H32, j, lane) == 0 && get_col(P.E32, j, lane) == 0) --j;
+                // ksw.cu:388-391, eight columns at a time: the first column of [beg, end) whose
+                // H or E word is non-zero (beg itself when the band is empty) ...
+                int32_t nb = beg < end ? end : beg;
+                for (int32_t b = beg & ~(kLB - 1); b < end; b += kLB) {
+                    uint32_t mk = nonzero_cols(P, b, lane);
+                    if (b < beg) mk &= ~0u << (beg - b);
+                    if (mk) {
+                        const int32_t j = b + __ffs(mk) - 1;
+                        nb = j < end ? j : end;
+                        break;
+                    }
+                }
+                // ... and the last column of [nb, end] whose word is non-zero (nb - 1 if none;
+                // end itself when end < nb)
+                int32_t last = end < nb ? end : nb - 1;
+                if (end >= nb) {
+                    for (int32_t b = end & ~(kLB - 1); b >= (nb & ~(kLB - 1)); b -= kLB) {
+                        uint32_t mk = nonzero_cols(P, b, lane);
+                        if (end - b < kLB - 1) mk &= (2u << (end - b)) - 1u;
+                        if (b < nb) mk &= ~0u << (nb - b);
+                        if (mk) {
+                            last = b + 31 - __clz(mk);
+                            break;
+                        }
+                    }
+                }
                 J.beg = nb;
-                J.end = j + 2 < J.qlen ? j + 2 : J.qlen;
+                J.end = last + 2 < J.qlen ? last + 2 : J.qlen;
             }
         }
         if (active && J.K.stop) {

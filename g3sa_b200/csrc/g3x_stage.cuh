@@ -107,6 +107,32 @@ __device__ __forceinline__ uint64_t nibbles16(uint32_t x, uint32_t nb) {
     return t | (n << 2);
 }
 
+// Chunks 0 .. nch-1 of the calling lane's own query as 4-bit codes into its column of a
+// lane-interleaved word array (chunk ch in words 2ch and 2ch+1, word k of lane L at
+// qn[k * 32 + L]).  The lanes of a refill wave each stage their own job at the same time, four
+// chunks in flight per lane, so a wave waits for about one global-memory latency per four
+// chunks whatever the number of new jobs.
+__device__ __forceinline__ void stage_own_query(const uint32_t* __restrict__ codes,
+                                                const uint32_t* __restrict__ nmask, uint32_t q_off,
+                                                int qlen, bool qrev, int nch, uint32_t* qn, int lane) {
+    for (int c0 = 0; c0 < nch; c0 += 4) {
+        uint32_t x[4], nb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            x[u] = 0u; nb[u] = 0u;
+            if (c0 + u < nch) load16(codes, nmask, q_off, qlen, c0 + u, qrev, x[u], nb[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (c0 + u < nch) {
+                const uint64_t v = nibbles16(x[u], nb[u]);
+                qn[(2 * (c0 + u)) * 32 + lane] = (uint32_t)v;
+                qn[(2 * (c0 + u) + 1) * 32 + lane] = (uint32_t)(v >> 32);
+            }
+        }
+    }
+}
+
 // Score rows as byte-permute pools: bytes 0-3 = codes 0-3, bytes 4-7 = N.
 __device__ __forceinline__ void score_pools(const ScoreParams& sp, uint32_t (&lo)[5],
                                             uint32_t (&hi)[5]) {
