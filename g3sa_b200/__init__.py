@@ -142,6 +142,15 @@ def lib():
         L.g3x_graph_capture.argtypes = [P, P, P, I32, P, P, P, P, P, ctypes.POINTER(P)]
         L.g3x_graph_launch.argtypes = [P, P]
         L.g3x_graph_destroy.argtypes = [P]
+        I64 = ctypes.c_int64
+        L.g3x_pipe_create.argtypes = [P, P, I32, I32, I64, I64, ctypes.POINTER(P)]
+        L.g3x_pipe_create.restype = ctypes.c_int
+        L.g3x_pipe_submit.argtypes = [P, P, I32, P, I64, P, I64, I32, I32, P, P, P]
+        L.g3x_pipe_submit.restype = ctypes.c_int
+        L.g3x_pipe_wait.argtypes = [P, P]
+        L.g3x_pipe_wait.restype = ctypes.c_int
+        L.g3x_pipe_destroy.argtypes = [P]
+        L.g3x_pipe_destroy.restype = ctypes.c_int
         L.g3x_int_peak.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
         L.g3x_int_peak.restype = ctypes.c_int
         L.g3x_pack_codes.argtypes = [P, ctypes.c_int64, P, P, ctypes.c_int64]
@@ -405,6 +414,52 @@ class Context:
                                            hp(nmask), int(n_bases), hp(regs), hp(status), int(chunk),
                                            opts.ctypes.data)
         _check(rc, "g3x_extend_seeds_stream")
+
+
+def _host_ptr(a):
+    return a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr()
+
+
+def _nbytes(a):
+    return a.nbytes if isinstance(a, np.ndarray) else a.numel() * a.element_size()
+
+
+class Pipe:
+    """g3x_pipe: batches in host memory (numpy arrays or pinned torch tensors), extended with
+    the context's schedule while the neighbouring batches' copies run.  submit() returns at
+    once; wait(stream) makes `stream` wait for every submitted batch, after which the output
+    buffers hold the results.  Host buffers must stay alive and unchanged until then."""
+
+    def __init__(self, ctx, score, schedule, max_jobs, max_code_words, max_nmask_words):
+        self._score = np.ascontiguousarray(score)
+        self._ctx = ctx
+        h = ctypes.c_void_p()
+        _check(lib().g3x_pipe_create(ctx._h, self._score.ctypes.data, int(schedule), int(max_jobs),
+                                     int(max_code_words), int(max_nmask_words), ctypes.byref(h)),
+               "g3x_pipe_create")
+        self._h = h.value
+
+    def submit(self, jobs, n, codes, nmask, max_qlen, max_tlen, out, status, stream=None):
+        """jobs: JOB_DT records (or their bytes); codes/nmask: the uint32 planes (or their
+        bytes); out: n x 6 int32 (g3x_ext_t); status: n int32."""
+        rc = lib().g3x_pipe_submit(self._h, _host_ptr(jobs), int(n), _host_ptr(codes), _nbytes(codes) // 4,
+                                   _host_ptr(nmask), _nbytes(nmask) // 4, int(max_qlen), int(max_tlen),
+                                   _host_ptr(out), _host_ptr(status), _stream(stream))
+        _check(rc, "g3x_pipe_submit")
+
+    def wait(self, stream=None):
+        _check(lib().g3x_pipe_wait(self._h, _stream(stream)), "g3x_pipe_wait")
+
+    def close(self):
+        if self._h:
+            lib().g3x_pipe_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Graph:

@@ -25,6 +25,8 @@ struct g3x_ctx {
 
 namespace g3x {
 
+int ctx_device(const g3x_ctx* ctx) { return ctx->device; }
+
 int score_params(const g3x_score_t* s, ScoreParams* sp) {
     if (!s) return G3X_ERR_INVALID;
     if (s->m != 5 || s->e_del <= 0 || s->e_ins <= 0 || s->o_del < 0 || s->o_ins < 0)

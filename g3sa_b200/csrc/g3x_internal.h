@@ -137,6 +137,7 @@ int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), con
                         g3x_reg_t* h_regs, int32_t* h_status, int32_t chunk,
                         const LaunchDesc& proto, const WaveRunner* runner = nullptr);
 int score_params(const g3x_score_t* s, ScoreParams* sp);
+int ctx_device(const g3x_ctx* ctx);   // the CUDA device a context is bound to
 
 // Learned cost model state (device buffers; g3x_model.cu).
 struct ModelState {

@@ -248,6 +248,32 @@ int g3x_extend_seeds_stream(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t
                             int64_t n_bases, g3x_reg_t *h_regs, int32_t *h_status,
                             int32_t chunk, const g3x_batch_opts_t *opts);
 
+/* ---- host-resident batches, pipelined --------------------------------------------------- */
+/* No counterpart in the reference (its batches stay on the device between pipeline stages).
+   A pipe extends batches of jobs that live in host memory with the context's schedule and
+   width classes, overlapping each batch's copies with its neighbours' extension.  It owns two
+   device buffer sets of max_jobs jobs, max_code_words code-plane words and max_nmask_words
+   N-plane words, and three streams.  g3x_pipe_submit returns at once: the batch's inputs are
+   copied to the next set once the work queued on `stream` before the call is done, the batch
+   is extended when they arrive (g3x_ksw_extend2_batch with `schedule`, kernel AUTO), and its
+   outputs and per-job statuses are copied to h_out / h_status.  Consecutive submits alternate
+   sets, so batch k+1's input copies and batch k-1's output copies run while batch k is
+   extended.  g3x_pipe_wait makes `stream` wait for every batch submitted so far: host buffers
+   of a batch must stay valid and unchanged until then, and pinned host memory is needed for
+   the copies to overlap.  Batches run one at a time on the context's scratch; other calls on
+   the same context belong after g3x_pipe_wait.  The first submit of a larger batch may
+   allocate context scratch.  G3X_ERR_INVALID for a batch beyond the pipe's sizes. */
+typedef struct g3x_pipe g3x_pipe;
+int g3x_pipe_create(g3x_ctx *ctx, const g3x_score_t *score, int32_t schedule, int32_t max_jobs,
+                    int64_t max_code_words, int64_t max_nmask_words, g3x_pipe **out);
+int g3x_pipe_submit(g3x_pipe *p, const g3x_job_t *h_jobs, int32_t n, const uint32_t *h_codes,
+                    int64_t code_words, const uint32_t *h_nmask, int64_t nmask_words,
+                    int32_t max_qlen, int32_t max_tlen, g3x_ext_t *h_out, int32_t *h_status,
+                    void *stream);
+int g3x_pipe_wait(g3x_pipe *p, void *stream);
+/* Waits for the pipe's batches on the host, then frees it. */
+int g3x_pipe_destroy(g3x_pipe *p);
+
 /* ---- CUDA graphs ------------------------------------------------------------------------- */
 /* Captures one g3x_ksw_extend2_batch call (all of its kernels and memsets, on the
    context's streams) into an executable CUDA graph bound to these buffers and options;
