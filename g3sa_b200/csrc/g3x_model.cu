@@ -76,7 +76,7 @@ __global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
 
 // ---- inference ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256) predict_kernel(const float* __restrict__ params,
+__global__ void __launch_bounds__(256, 2) predict_kernel(const float* __restrict__ params,
                                                       const float* __restrict__ feat, int n,
                                                       float* __restrict__ out) {
     __shared__ __align__(16) float w[kParams];
@@ -95,20 +95,30 @@ __global__ void __launch_bounds__(256) predict_kernel(const float* __restrict__ 
         for (int f = 0; f < kF; ++f) a = fmaf(w[oW1 + u * kF + f], x[f], a);
         h1[u] = fmaxf(a, 0.0f);
     }
+    // Four hidden units at a time: four independent accumulation chains (each unit's sum in
+    // the order of its row), rows of W2 four weights per broadcast load, y summed in unit order.
     float y = w[ob3];
-    for (int u = 0; u < kH; ++u) {
-        float a = w[ob2 + u];
-        // the row of W2 four weights per (broadcast) load; the sum keeps its order
-        const float4* row = reinterpret_cast<const float4*>(w + oW2 + u * kH);
+    for (int u0 = 0; u0 < kH; u0 += 4) {
+        float a[4];
+        const float4* row[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            a[j] = w[ob2 + u0 + j];
+            row[j] = reinterpret_cast<const float4*>(w + oW2 + (u0 + j) * kH);
+        }
 #pragma unroll
         for (int q = 0; q < kH / 4; ++q) {
-            const float4 c = row[q];
-            a = fmaf(c.x, h1[4 * q], a);
-            a = fmaf(c.y, h1[4 * q + 1], a);
-            a = fmaf(c.z, h1[4 * q + 2], a);
-            a = fmaf(c.w, h1[4 * q + 3], a);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float4 c = row[j][q];
+                a[j] = fmaf(c.x, h1[4 * q], a[j]);
+                a[j] = fmaf(c.y, h1[4 * q + 1], a[j]);
+                a[j] = fmaf(c.z, h1[4 * q + 2], a[j]);
+                a[j] = fmaf(c.w, h1[4 * q + 3], a[j]);
+            }
         }
-        y = fmaf(w[oW3 + u], fmaxf(a, 0.0f), y);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) y = fmaf(w[oW3 + u0 + j], fmaxf(a[j], 0.0f), y);
     }
     out[k] = y;
 }

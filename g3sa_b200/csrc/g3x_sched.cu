@@ -65,7 +65,9 @@ __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScorePara
     wb = kWidthBins - 1 - (wb < kWidthBins - 1 ? wb : kWidthBins - 1);
     const int bn = b * kLevels + rb * kWidthBins + wb;
     bin[k] = bn;
-    atomicAdd(hist + bn, 1);
+    // one atomic per distinct bin of the warp (a batch has few populated bins)
+    const unsigned peers = __match_any_sync(__activemask(), bn);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(hist + bn, __popc(peers));
 }
 
 // Exclusive scan of the nb bins in one block; also each bucket's (offset, count).
@@ -103,7 +105,13 @@ __global__ void scatter_kernel(const int32_t* __restrict__ bin, int n, int32_t* 
                                const int32_t* __restrict__ subset_n) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n || (subset_n && k >= *subset_n)) return;
-    const int at = atomicAdd(cursor + bin[k], 1);
+    const int bn = bin[k];
+    // the warp's jobs of one bin take consecutive slots with one atomic
+    const unsigned peers = __match_any_sync(__activemask(), bn);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    int at = 0;
+    if (lane == leader) at = atomicAdd(cursor + bn, __popc(peers));
+    at = __shfl_sync(peers, at, leader) + __popc(peers & ((1u << lane) - 1u));
     order[at] = job_at(k, subset);
 }
 
