@@ -60,6 +60,10 @@ SYNTH_PARAMS_DT = np.dtype([("kind", "<i4"), ("n", "<i4"), ("w", "<i4"), ("a", "
                             ("threads", "<i4"), ("pad_", "<i4"), ("unrelated", "<f8"),
                             ("seed", "<u8")])
 assert SCORE_DT.itemsize == 56 and JOB_DT.itemsize == 24 and EXT_DT.itemsize == 24
+# g3x_refinfo_t
+REFINFO_DT = np.dtype([("l_pac", "<i8"), ("ref_off", "<i8"), ("n_seqs", "<i4"), ("pad_", "<i4"),
+                       ("d_anns", "<u8")])
+assert REFINFO_DT.itemsize == 32
 assert SEED_DT.itemsize == 56 and OPT_DT.itemsize == 72 and DSEED_DT.itemsize == 48
 assert REG_DT.itemsize == 40
 
@@ -143,6 +147,8 @@ def lib():
         L.g3x_graph_launch.argtypes = [P, P]
         L.g3x_graph_destroy.argtypes = [P]
         I64 = ctypes.c_int64
+        L.g3x_chain2aln.argtypes = [P, P, P, P, I32, P, I32, P, I32, P, P, P, P, P, P, P]
+        L.g3x_chain2aln.restype = ctypes.c_int
         L.g3x_pipe_create.argtypes = [P, P, I32, I32, I64, I64, ctypes.POINTER(P)]
         L.g3x_pipe_create.restype = ctypes.c_int
         L.g3x_pipe_submit.argtypes = [P, P, I32, P, I64, P, I64, I32, I32, P, P, P]
@@ -388,6 +394,21 @@ class Context:
                                     _ptr(d_nmask), _ptr(d_regs), _ptr(d_status), opts.ctypes.data,
                                     _stream(stream))
         _check(rc, "g3x_extend_seeds")
+
+    def chain2aln(self, opt, l_pac, ref_off, d_anns, n_seqs, d_reads, n_reads, d_chains, n_chains,
+                  d_seeds, n_seeds, d_codes, d_nmask, d_regs, d_nregs, d_status,
+                  schedule=SCHED_SORTED, lanes=0, tile=0, kernel=KERNEL_AUTO, stream=None):
+        """g3x_chain2aln on device buffers (records of g3sa_b200.chains: READ_DT, CHAIN_DT,
+        CSEED_DT, ANN_DT in; ALNREG_DT per seed slot, nregs and status per read out)."""
+        ri = np.zeros(1, REFINFO_DT)
+        ri["l_pac"], ri["ref_off"], ri["n_seqs"], ri["d_anns"] = l_pac, ref_off, n_seqs, _ptr(d_anns)
+        opts = np.zeros(1, BATCH_OPTS_DT)
+        opts["schedule"], opts["lanes"], opts["tile"], opts["kernel"] = schedule, lanes, tile, kernel
+        rc = lib().g3x_chain2aln(self._h, opt.ctypes.data, ri.ctypes.data, _ptr(d_reads), int(n_reads),
+                                 _ptr(d_chains), int(n_chains), _ptr(d_seeds), int(n_seeds), _ptr(d_codes),
+                                 _ptr(d_nmask), _ptr(d_regs), _ptr(d_nregs), _ptr(d_status), opts.ctypes.data,
+                                 _stream(stream))
+        _check(rc, "g3x_chain2aln")
 
     def extend_seeds_stream(self, opt, seeds, codes, nmask, n_bases, regs, status, max_qlen,
                             max_tlen, chunk=65536, schedule=SCHED_SORTED, lanes=0, tile=0,

@@ -14,6 +14,7 @@ struct g3x_ctx {
     g3x::SeedScratch seeds;      // seed-level scratch, grown on demand
     g3x::ModelState model;       // learned cost model
     g3x::SchedScratch sched;     // job order and width classes of a persistent batch
+    g3x::ChainScratch chain;     // chain-level call state
     g3x::TileTable tiles;        // width classes and their kernel configurations
     unsigned long long* d_stats; // occupancy counters of the last persistent batch
     cudaStream_t side[g3x::kMaxBuckets];   // one stream per width class
@@ -26,6 +27,7 @@ struct g3x_ctx {
 namespace g3x {
 
 int ctx_device(const g3x_ctx* ctx) { return ctx->device; }
+ChainScratch& ctx_chain(g3x_ctx* ctx) { return ctx->chain; }
 
 int score_params(const g3x_score_t* s, ScoreParams* sp) {
     if (!s) return G3X_ERR_INVALID;
@@ -339,6 +341,7 @@ int g3x_ctx_destroy(g3x_ctx* c) {
     g3x::free_seed_scratch(c->seeds);
     g3x::model_free(c->model);
     g3x::free_sched(c->sched);
+    g3x::free_chain_scratch(c->chain);
     for (int k = 0; k < g3x::kMaxBuckets; ++k) {
         cudaStreamDestroy(c->side[k]);
         cudaEventDestroy(c->join[k]);

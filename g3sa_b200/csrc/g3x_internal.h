@@ -139,6 +139,23 @@ int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), con
 int score_params(const g3x_score_t* s, ScoreParams* sp);
 int ctx_device(const g3x_ctx* ctx);   // the CUDA device a context is bound to
 
+// Scratch of the chain-level call (g3x_chain.cu), grown on demand.
+struct ChainScratch {
+    int64_t* win = nullptr;          // per chain: reference window [r0, r1)
+    uint64_t* srt = nullptr;         // per seed: its chain's processing keys
+    void* state = nullptr;           // per read: 16-byte walk state
+    g3x_seed_t* wseeds = nullptr;    // per wave: the queued seeds ...
+    int32_t* wsrc = nullptr;         // ... their (read, chain, seed)
+    g3x_reg_t* wregs = nullptr;      // ... and their extension results
+    int32_t* wstatus = nullptr;
+    int32_t* count = nullptr;        // seeds queued by the wave
+    int32_t* maxlen = nullptr;       // longest read and window of the call
+    int32_t* h_count = nullptr;      // pinned: count, or the two bounds
+    int64_t reads = 0, chains = 0, seeds = 0;
+};
+ChainScratch& ctx_chain(g3x_ctx* ctx);
+void free_chain_scratch(ChainScratch& w);
+
 // Learned cost model state (device buffers; g3x_model.cu).
 struct ModelState {
     float *params = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;

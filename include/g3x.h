@@ -248,6 +248,77 @@ int g3x_extend_seeds_stream(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t
                             int64_t n_bases, g3x_reg_t *h_regs, int32_t *h_status,
                             int32_t chunk, const g3x_batch_opts_t *opts);
 
+/* ---- chain-level extension: mem_chain2aln --------------------------------------------- */
+/* Records of the chain-level call, with the fields mem_chain2aln reads or sets
+   (bwa/src/bwa.h:202-247, bwa/src/bntseq.h:42-65).  The reference sequence lives in the
+   code planes as 2*l_pac bases starting at base ref_off: the forward strand of every contig
+   (contig k at anns[k].offset, anns[k].len bases), then its reverse complement, so reference
+   position p >= l_pac holds 3 - forward[2*l_pac - 1 - p] (what bns_get_seq_gpu returns for
+   the reverse strand, bwa/src/bntseq.cu:39-60).  Every base index (reads, reference) must be
+   below 2^32. */
+typedef struct {
+    int64_t rbeg;         /* seed start in [0, 2*l_pac) */
+    int32_t qbeg, len, score;
+    int32_t pad_;
+} g3x_cseed_t;            /* mem_seed_t, 24 bytes */
+
+typedef struct {
+    int32_t seed_beg, n;  /* seeds [seed_beg, seed_beg + n) of the seed array */
+    int32_t rid;
+    float frac_rep;
+} g3x_chain_t;            /* mem_chain_t, 16 bytes */
+
+typedef struct {
+    int64_t read_off;     /* base index of read[0] in the planes */
+    int32_t l_query;
+    int32_t chain_beg, n_chains;   /* the read's chains, processed in this order */
+    int32_t pad_;
+} g3x_read_t;             /* 24 bytes */
+
+typedef struct {
+    int64_t offset;       /* first forward position of the contig */
+    int32_t len;
+    int32_t pad_;
+} g3x_ann_t;              /* bntann1_t, 16 bytes */
+
+typedef struct {
+    int64_t l_pac;        /* forward length of the reference */
+    int64_t ref_off;      /* base index of reference position 0 in the planes */
+    int32_t n_seqs;       /* contigs */
+    int32_t pad_;
+    const g3x_ann_t *d_anns;   /* n_seqs contigs, device memory, increasing offsets */
+} g3x_refinfo_t;          /* 32 bytes */
+
+typedef struct {
+    int64_t rb, re;       /* [rb, re) on the reference (2*l_pac coordinates) */
+    int32_t qb, qe;       /* [qb, qe) on the read */
+    int32_t rid, score, truesc, w, seedcov, seedlen0;
+    float frac_rep;
+    int32_t pad_;
+} g3x_alnreg_t;           /* mem_alnreg_t fields mem_chain2aln sets, 56 bytes */
+
+/* mem_chain2aln (bwa/src/aux.cu:178-315) for every chain of n_reads reads.  A read's chains
+   run in order on the read's region list: each chain's reference window is the span its seeds
+   can reach (cal_max_gap, aux.cu:168-205) clipped to the first seed's contig and strand
+   (bns_fetch_seq_gpu, bwa/src/bntseq.cu:62-87); its seeds run by decreasing (score, index)
+   (aux.cu:207-212); a seed inside an earlier region of the read, with no long enough
+   earlier seed of the chain overlapping it on another diagonal, is skipped (aux.cu:214-245);
+   every other seed is extended left and right with band retry (as g3x_extend_seeds) and gives
+   one region with its seed coverage (aux.cu:247-314).  A read's chains must be contiguous in
+   d_chains and their seeds contiguous in d_seeds, one chain after the other: read r's
+   regions go to d_regs[chains[chain_beg].seed_beg ...] (at most one per seed), their number
+   to d_nregs[r], a per-read status to d_status[r] (G3X_OK; G3X_ERR_INVALID for a read whose
+   records break these rules; G3X_ERR_TOO_LONG when an extension exceeds the job limits, the
+   read's processing stopping there).  Runs in waves, one extended seed per read per wave,
+   the waves' extensions through the context's schedule (opts as g3x_extend_seeds); the
+   host waits for `stream` once per wave to read the wave's size.  Allocates context scratch
+   for larger calls. */
+int g3x_chain2aln(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_refinfo_t *ref,
+                  const g3x_read_t *d_reads, int32_t n_reads, const g3x_chain_t *d_chains,
+                  int32_t n_chains, const g3x_cseed_t *d_seeds, int32_t n_seeds,
+                  const uint32_t *d_codes, const uint32_t *d_nmask, g3x_alnreg_t *d_regs,
+                  int32_t *d_nregs, int32_t *d_status, const g3x_batch_opts_t *opts, void *stream);
+
 /* ---- host-resident batches, pipelined --------------------------------------------------- */
 /* No counterpart in the reference (its batches stay on the device between pipeline stages).
    A pipe extends batches of jobs that live in host memory with the context's schedule and

@@ -2,7 +2,9 @@
 # Builds oracle/_ref/libksw_ref.so: the reference's own ksw_extend2, compiled from its
 # source file where it lies (bwa/src/ksw.cu, lines 299-401 = eh_t + ksw_extend2) as host
 # C++, the reference's own band-retry lines of mem_chain2aln (bwa/src/aux.cu:253-255,
-# 258-301, 309), plus the ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
+# 258-301, 309), the whole of mem_chain2aln with the window fetch it calls
+# (bwa/src/aux.cu:168-175, 178-315; bwa/src/bntseq.cu:5, 7-87), plus the ctypes batch driver
+# ref_wrap.cpp.  The source lines are streamed from the
 # reference tree into the compiler; no reference source is copied into this repository.
 # Usage: sh oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -eu
@@ -42,7 +44,27 @@ fi
 { grep -m1 '^#define MAX_BAND_TRY' "$AUXH"; cat "$HERE/ref_seed_head.inc"; \
   sed -n '253,255p;258,301p;309p' "$AUX"; echo '}'; } | tr -d '\r' | \
     $CXX -O3 -fPIC -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/seed_ref_fn.o"
+# The chain level: the reference's own mem_chain2aln with cal_max_gap (aux.cu:168-175,
+# 178-315) and the window fetch it calls (bntseq.cu:5, 7-87), between ref_chain_head.inc and
+# ref_chain_tail.inc.
+BNS="$REF/bwa/src/bntseq.cu"
+A168=$(sed -n '168p' "$AUX" | tr -d '\r')
+A178=$(sed -n '178p' "$AUX" | tr -d '\r' | cut -c1-30)
+A315=$(sed -n '315p' "$AUX" | tr -d '\r')
+B5=$(sed -n '5p' "$BNS" | tr -d '\r' | cut -c1-16)
+B7=$(sed -n '7p' "$BNS" | tr -d '\r')
+B87=$(sed -n '87p' "$BNS" | tr -d '\r')
+if [ "$A168" != "__device__ static inline int cal_max_gap(const mem_opt_t *opt, int qlen)" ] || \
+   [ "$A178" != "__device__ void mem_chain2aln(" ] || [ "$A315" != "}" ] || \
+   [ "$B5" != "#define _get_pac" ] || [ "$B7" != "__device__ int bns_pos2rid_gpu(const bntseq_t *bns, int64_t pos_f)" ] || \
+   [ "$B87" != "}" ]; then
+    echo "build_ref.sh: unexpected content at aux.cu:168/178/315 or bntseq.cu:5/7/87; refusing to build" >&2
+    exit 3
+fi
+{ grep -m1 '^#define MAX_BAND_TRY' "$AUXH"; cat "$HERE/ref_chain_head.inc"; sed -n '5p;7,87p' "$BNS"; \
+  sed -n '168,175p;178,315p' "$AUX"; cat "$HERE/ref_chain_tail.inc"; } | tr -d '\r' | \
+    $CXX -O3 -fPIC -std=c++17 -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/chain_ref_fn.o"
 $CXX -O3 -fPIC -shared -std=c++17 "$HERE/ref_wrap.cpp" "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" \
-    -o "$OUT/libksw_ref.so" -lpthread
-rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o"
+    "$OUT/chain_ref_fn.o" -o "$OUT/libksw_ref.so" -lpthread
+rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" "$OUT/chain_ref_fn.o"
 echo "built $OUT/libksw_ref.so"

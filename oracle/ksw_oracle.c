@@ -403,3 +403,166 @@ void g3o_stale_scan(const g3o_job *jobs, int64_t n, const uint8_t *codes, const 
         free(tb);
     }
 }
+
+/* ---------------------------------------------------------------------------------- */
+/* Chain level: mem_chain2aln (aux.cu:178-315) with the window fetch of                 */
+/* bns_fetch_seq_gpu (bntseq.cu:62-87).  The reference is given as one sequence of      */
+/* 2*l_pac codes at codes[ref_off]: the forward strand, then its reverse complement     */
+/* (position p >= l_pac holds 3 - forward[2*l_pac - 1 - p], what bns_get_seq_gpu reads  */
+/* for the reverse strand, bntseq.cu:39-60), so a window [b, e) is codes[ref_off + b].  */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct { int64_t rbeg; int32_t qbeg, len, score, pad_; } g3o_cseed;      /* mem_seed_t */
+typedef struct { int32_t seed_beg, n, rid; float frac_rep; } g3o_chain;           /* mem_chain_t */
+typedef struct { int64_t read_off; int32_t l_query, chain_beg, n_chains, pad_; } g3o_read;
+typedef struct { int64_t offset; int32_t len, pad_; } g3o_ann;                     /* bntann1_t */
+typedef struct {                                                                    /* mem_alnreg_t */
+    int64_t rb, re;
+    int32_t qb, qe, rid, score, truesc, w, seedcov, seedlen0;
+    float frac_rep;
+    int32_t pad_;
+} g3o_alnreg;
+
+/* The contig holding forward position pos_f: the last one whose offset is <= pos_f
+   (bns_pos2rid_gpu, bntseq.cu:7-21). */
+static int g3o_pos2rid(const g3o_ann *anns, int n_seqs, int64_t pos_f)
+{
+    int lo = 0, hi = n_seqs;           /* first index with offset > pos_f, in [lo, hi] */
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (anns[mid].offset <= pos_f) lo = mid + 1; else hi = mid;
+    }
+    return lo > 0 ? lo - 1 : 0;
+}
+
+/* bns_fetch_seq_gpu's clipping of the window [*b, *e) to the contig (and strand) of
+   position mid (bntseq.cu:62-80). */
+static void g3o_clip_window(const g3o_ann *anns, int n_seqs, int64_t l_pac, int64_t *b,
+                            int64_t mid, int64_t *e)
+{
+    if (*e < *b) { int64_t t = *b; *b = *e; *e = t; }
+    const int rev = mid >= l_pac;
+    const int rid = g3o_pos2rid(anns, n_seqs, rev ? (l_pac << 1) - 1 - mid : mid);
+    int64_t lo = anns[rid].offset, hi = lo + anns[rid].len;
+    if (rev) { const int64_t t = lo; lo = (l_pac << 1) - hi; hi = (l_pac << 1) - t; }
+    if (*b < lo) *b = lo;
+    if (*e > hi) *e = hi;
+}
+
+static int g3o_cmp_u64(const void *x, const void *y)
+{
+    const uint64_t a = *(const uint64_t *)x, b = *(const uint64_t *)y;
+    return a < b ? -1 : a > b;
+}
+
+/* Is seed s (almost) inside region p: fully contained, not much longer than p's seed, and
+   on p's diagonal band ahead of or behind the seed (aux.cu:217-231). */
+static int g3o_around(const g3o_opt *opt, int l_query, const g3o_cseed *s, const g3o_alnreg *p)
+{
+    if (s->rbeg < p->rb || s->rbeg + s->len > p->re || s->qbeg < p->qb || s->qbeg + s->len > p->qe)
+        return 0;
+    if (s->len - p->seedlen0 > .1 * l_query) return 0;
+    int qd = s->qbeg - p->qb;
+    int64_t rd = s->rbeg - p->rb;
+    int gap = g3o_cal_max_gap(opt, (int)(qd < rd ? qd : rd));
+    int w = gap < p->w ? gap : p->w;
+    if (qd - rd < w && rd - qd < w) return 1;
+    qd = p->qe - (s->qbeg + s->len);
+    rd = p->re - (s->rbeg + s->len);
+    gap = g3o_cal_max_gap(opt, (int)(qd < rd ? qd : rd));
+    w = gap < p->w ? gap : p->w;
+    return qd - rd < w && rd - qd < w;
+}
+
+/* One chain of a read; av/nav = the read's regions so far, appended to. */
+static void g3o_chain2aln_one(const g3o_opt *opt, const uint8_t *codes, int64_t ref_off,
+                              int64_t l_pac, const g3o_ann *anns, int n_seqs, int64_t read_off,
+                              int l_query, const g3o_chain *c, const g3o_cseed *all_seeds,
+                              g3o_alnreg *av, int32_t *nav, int64_t *cells)
+{
+    const int n = c->n;
+    if (n == 0) return;
+    const g3o_cseed *cs = all_seeds + c->seed_beg;
+    /* the widest span any seed can reach (aux.cu:186-205) */
+    int64_t r0 = l_pac << 1, r1 = 0;
+    for (int i = 0; i < n; ++i) {
+        const g3o_cseed *t = &cs[i];
+        const int tail = l_query - t->qbeg - t->len;
+        const int64_t b = t->rbeg - (t->qbeg + g3o_cal_max_gap(opt, t->qbeg));
+        const int64_t e = t->rbeg + t->len + (tail + g3o_cal_max_gap(opt, tail));
+        if (b < r0) r0 = b;
+        if (e > r1) r1 = e;
+    }
+    if (r0 < 0) r0 = 0;
+    if (r1 > l_pac << 1) r1 = l_pac << 1;
+    if (r0 < l_pac && l_pac < r1) {              /* one strand only: the first seed's */
+        if (cs[0].rbeg < l_pac) r1 = l_pac; else r0 = l_pac;
+    }
+    g3o_clip_window(anns, n_seqs, l_pac, &r0, cs[0].rbeg, &r1);
+
+    /* seeds by decreasing (score, index) (aux.cu:207-212); a key set to 0 marks a skip */
+    uint64_t *srt = (uint64_t *)malloc((size_t)n * sizeof(uint64_t));
+    for (int i = 0; i < n; ++i) srt[i] = (uint64_t)cs[i].score << 32 | (uint64_t)i;
+    qsort(srt, (size_t)n, sizeof(uint64_t), g3o_cmp_u64);
+
+    for (int k = n - 1; k >= 0; --k) {
+        const g3o_cseed *s = &cs[(uint32_t)srt[k]];
+        int i = 0;
+        while (i < *nav && !g3o_around(opt, l_query, s, &av[i])) ++i;
+        if (i < *nav) {
+            /* contained: extend anyway only when an earlier, long enough seed overlaps it on
+               another diagonal (aux.cu:234-244) */
+            int j;
+            for (j = k + 1; j < n; ++j) {
+                if (srt[j] == 0) continue;
+                const g3o_cseed *t = &cs[(uint32_t)srt[j]];
+                if (t->len < s->len * .95) continue;
+                if (s->qbeg <= t->qbeg && s->qbeg + s->len - t->qbeg >= s->len >> 2 &&
+                    t->qbeg - s->qbeg != t->rbeg - s->rbeg) break;
+                if (t->qbeg <= s->qbeg && t->qbeg + t->len - s->qbeg >= s->len >> 2 &&
+                    s->qbeg - t->qbeg != s->rbeg - t->rbeg) break;
+            }
+            if (j == n) { srt[k] = 0; continue; }
+        }
+        g3o_alnreg *a = &av[(*nav)++];
+        memset(a, 0, sizeof(*a));
+        g3o_seed gs;
+        gs.read_off = read_off; gs.win_off = ref_off + r0; gs.rmax0 = r0; gs.rmax1 = r1;
+        gs.rbeg = s->rbeg; gs.l_query = l_query; gs.qbeg = s->qbeg; gs.len = s->len;
+        g3o_reg r;
+        g3o_extend_seed(opt, codes, &gs, &r);            /* aux.cu:253-301, 309 */
+        if (cells) *cells += r.cells;
+        a->rb = r.rb; a->re = r.re; a->qb = r.qb; a->qe = r.qe;
+        a->score = r.score; a->truesc = r.truesc; a->w = r.w;
+        a->rid = c->rid;
+        for (int t = 0; t < n; ++t) {                    /* seedcov, aux.cu:303-307 */
+            const g3o_cseed *u = &cs[t];
+            if (u->qbeg >= a->qb && u->qbeg + u->len <= a->qe && u->rbeg >= a->rb &&
+                u->rbeg + u->len <= a->re)
+                a->seedcov += u->len;
+        }
+        a->seedlen0 = s->len;
+        a->frac_rep = c->frac_rep;
+    }
+    free(srt);
+}
+
+/* Every read's chains in order; read r's regions go to regs[chains[chain_beg].seed_beg ...]
+   (a read yields at most one region per seed), their number to nregs[r]. */
+void g3o_chain2aln_reads(const g3o_opt *opt, const uint8_t *codes, int64_t ref_off, int64_t l_pac,
+                         const g3o_ann *anns, int n_seqs, const g3o_read *reads, int64_t n_reads,
+                         const g3o_chain *chains, const g3o_cseed *seeds, g3o_alnreg *regs,
+                         int32_t *nregs, int64_t *cells)
+{
+    for (int64_t r = 0; r < n_reads; ++r) {
+        const g3o_read *rd = &reads[r];
+        int32_t nav = 0;
+        if (rd->n_chains > 0) {
+            g3o_alnreg *av = regs + chains[rd->chain_beg].seed_beg;
+            for (int ch = 0; ch < rd->n_chains; ++ch)
+                g3o_chain2aln_one(opt, codes, ref_off, l_pac, anns, n_seqs, rd->read_off, rd->l_query,
+                                  &chains[rd->chain_beg + ch], seeds, av, &nav, cells ? cells + r : NULL);
+        }
+        nregs[r] = nav;
+    }
+}

@@ -41,6 +41,9 @@ def oracle():
         _oracle.g3o_extend_batch.argtypes = [ctypes.c_void_p, ctypes.c_int64] + [ctypes.c_void_p] * 5 + [ctypes.c_int]
         _oracle.g3o_extend_seeds.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_void_p]
         _oracle.g3o_ksw_extend2.restype = ctypes.c_int
+        P, I64 = ctypes.c_void_p, ctypes.c_int64
+        _oracle.g3o_chain2aln_reads.argtypes = [P, P, I64, I64, P, ctypes.c_int, P, I64, P, P, P, P, P]
+        _oracle.g3o_chain2aln_reads.restype = None
     return _oracle
 
 
@@ -54,6 +57,9 @@ def ref():
         _ref = ctypes.CDLL(REF_SO)
         _ref.g3r_ksw_extend2_batch.argtypes = [ctypes.c_void_p, ctypes.c_int64] + [ctypes.c_void_p] * 3 + [ctypes.c_int]
         _ref.g3r_extend_seeds.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_void_p]
+        P, I64 = ctypes.c_void_p, ctypes.c_int64
+        _ref.g3r_chain2aln_reads.argtypes = [P, P, I64, I64, P, ctypes.c_int, P, I64, P, P, P, P]
+        _ref.g3r_chain2aln_reads.restype = ctypes.c_int
     return _ref
 
 
@@ -149,3 +155,49 @@ def ref_seeds(seeds, u8, opt):
     ref().g3r_extend_seeds(ro.ctypes.data, np.ascontiguousarray(u8).ctypes.data,
                            np.ascontiguousarray(seeds).ctypes.data, len(seeds), out.ctypes.data)
     return out
+
+
+def _chain_args(wl):
+    u8 = np.ascontiguousarray(wl.u8)
+    parts = [np.ascontiguousarray(x) for x in (wl.anns, wl.reads, wl.chains, wl.seeds)]
+    return u8, parts
+
+
+def oracle_chains(wl, opt):
+    """(regions ALNREG_DT per seed slot, nregs per read, DP cells per read) from the C
+    restatement of mem_chain2aln."""
+    from g3sa_b200.chains import ALNREG_DT
+    u8, (anns, reads, chains, seeds) = _chain_args(wl)
+    regs = np.zeros(max(len(seeds), 1), ALNREG_DT)
+    nregs = np.zeros(len(reads), np.int32)
+    cells = np.zeros(len(reads), np.int64)
+    oracle().g3o_chain2aln_reads(opt.ctypes.data, u8.ctypes.data, wl.ref_off, wl.l_pac,
+                                 anns.ctypes.data, len(anns), reads.ctypes.data, len(reads),
+                                 chains.ctypes.data, seeds.ctypes.data, regs.ctypes.data,
+                                 nregs.ctypes.data, cells.ctypes.data)
+    return regs, nregs, cells
+
+
+def ref_chains(wl, opt):
+    """(regions, nregs) from the reference's own mem_chain2aln (oracle/_ref)."""
+    from g3sa_b200.chains import ALNREG_DT
+    u8, (anns, reads, chains, seeds) = _chain_args(wl)
+    ro = np.zeros(1, REF_OPT_DT)
+    for f in ("a", "o_del", "e_del", "o_ins", "e_ins", "pen_clip5", "pen_clip3", "w", "zdrop", "mat"):
+        ro[f] = opt[f]
+    regs = np.zeros(max(len(seeds), 1), ALNREG_DT)
+    nregs = np.zeros(len(reads), np.int32)
+    ref().g3r_chain2aln_reads(ro.ctypes.data, u8.ctypes.data, wl.ref_off, wl.l_pac, anns.ctypes.data,
+                              len(anns), reads.ctypes.data, len(reads), chains.ctypes.data,
+                              seeds.ctypes.data, regs.ctypes.data, nregs.ctypes.data)
+    return regs, nregs
+
+
+def region_rows(regs, nregs, chains, reads):
+    """The regions each read produced, as one array in read order."""
+    out = []
+    for r in range(len(reads)):
+        if nregs[r]:
+            b = int(chains[reads["chain_beg"][r]]["seed_beg"])
+            out.append(regs[b:b + int(nregs[r])])
+    return np.concatenate(out) if out else regs[:0]
