@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["chains"])
     ap.add_argument("--schedule", default="auto", choices=["auto", "plain", "sorted", "learned"])
     ap.add_argument("--seed", type=int, default=0x6A5 + 2)
     return ap.parse_args()
@@ -170,6 +170,176 @@ def run_reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+CHAIN_READS = 60000
+CHAIN_DESC = ("mem_chain2aln over 60k synthetic reads (100/150/250 bp, divergence U[0,5%], small "
+              "indels) on a 12-contig random reference: each read's true chain of exact-match seeds "
+              "plus 0-2 spurious chains; seed order, containment skip, left/right extension with band "
+              "retry, seed coverage; w=100, a=1 b=4 o=6 e=1 zdrop=100")
+
+
+def ref_chains_threaded(wl, opt_cpu, threads):
+    """The reference's own mem_chain2aln (oracle/_ref) over the reads, split into `threads`
+    slices of reads run side by side (their regions go to disjoint seed slots)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from g3sa_b200.chains import ALNREG_DT
+    from tests import native as nat
+    lib = nat.ref()
+    ro = np.zeros(1, nat.REF_OPT_DT)
+    for f in ("a", "o_del", "e_del", "o_ins", "e_ins", "pen_clip5", "pen_clip3", "w", "zdrop", "mat"):
+        ro[f] = opt_cpu[f]
+    u8 = np.ascontiguousarray(wl.u8)
+    anns, chains, seeds = (np.ascontiguousarray(x) for x in (wl.anns, wl.chains, wl.seeds))
+    regs = np.zeros(max(len(seeds), 1), ALNREG_DT)
+    nregs = np.zeros(wl.n_reads, np.int32)
+    bounds = np.linspace(0, wl.n_reads, threads + 1).astype(np.int64)
+
+    def part(i):
+        a, b = int(bounds[i]), int(bounds[i + 1])
+        rd = np.ascontiguousarray(wl.reads[a:b])
+        nr = np.zeros(b - a, np.int32)
+        lib.g3r_chain2aln_reads(ro.ctypes.data, u8.ctypes.data, wl.ref_off, wl.l_pac, anns.ctypes.data,
+                                len(anns), rd.ctypes.data, b - a, chains.ctypes.data, seeds.ctypes.data,
+                                regs.ctypes.data, nr.ctypes.data)
+        nregs[a:b] = nr
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(part, range(threads)))
+    return time.perf_counter() - t0, regs, nregs
+
+
+def run_chain_workload(args, ws, rank):
+    """`--workload chains`: the chain-level call (g3x_chain2aln), one step = every read of the
+    batch; GCUPS from the oracle's DP cell count of the extensions the reads make."""
+    import g3sa_b200 as g
+    from g3sa_b200.chains import ALNREG_DT, synth_chains
+    from tests import native as nat
+    if args.impl == "reference" and rank != 0:
+        return
+    wl = synth_chains(CHAIN_READS, seed=args.seed + 1000 * rank)
+    opt_cpu = nat.opt_from_score(g.default_score())
+    oregs, onregs, ocells = nat.oracle_chains(wl, opt_cpu)
+    cells = int(ocells.sum())
+    threads = os.cpu_count() or 1
+    metric = "mem_chain2aln GCUPS & reads/s on 1 B200, bit-exact"
+    cfg = {"workload": CHAIN_DESC, "reads": wl.n_reads, "chains": len(wl.chains), "seeds": len(wl.seeds),
+           "regions": int(onregs.sum()), "cells": cells}
+    if args.impl == "reference":
+        kind = "reference" if nat.have_ref() else "port"
+        times = []
+        for it in range(args.warmup + args.steps):
+            if kind == "reference":
+                dt, _, _ = ref_chains_threaded(wl, opt_cpu, threads)
+            else:
+                t0 = time.perf_counter()
+                nat.oracle_chains(wl, opt_cpu)
+                dt = time.perf_counter() - t0
+            if it >= args.warmup:
+                times.append(dt)
+        t = sum(times) / len(times)
+        gcups = cells / t / 1e9
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": round(gcups, 4), "unit": "GCUPS",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded)", "config": cfg, "reads_per_s": round(wl.n_reads / t, 1),
+            "cpu_baseline": {"value": round(gcups, 4), "unit": "GCUPS", "cores": threads if kind == "reference" else 1,
+                             "kind": kind, "sample": "whole workload per step"},
+            "e2e": {"value": round(gcups, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+            flush=True)
+        return
+    import torch
+    from g3sa_b200 import build
+    build.build_lib()
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    codes, nmask = wl.planes()
+    host = {k: torch.from_numpy(np.ascontiguousarray(v).view(np.uint8).copy()).pin_memory()
+            for k, v in (("reads", wl.reads), ("chains", wl.chains), ("seeds", wl.seeds),
+                         ("anns", wl.anns), ("codes", codes), ("nmask", nmask))}
+    d = {k: v.to(dev) for k, v in host.items()}
+    n_seeds = len(wl.seeds)
+    d_regs = torch.zeros(n_seeds * ALNREG_DT.itemsize, dtype=torch.uint8, device=dev)
+    d_nregs = torch.zeros(wl.n_reads, dtype=torch.int32, device=dev)
+    d_status = torch.zeros(wl.n_reads, dtype=torch.int32, device=dev)
+    h_regs = torch.zeros_like(d_regs, device="cpu").pin_memory()
+    h_nregs = torch.zeros_like(d_nregs, device="cpu").pin_memory()
+    h_status = torch.zeros_like(d_status, device="cpu").pin_memory()
+    ctx = g.Context(local)
+    # width classes of int16x2 lane kernels up to the longest read, the row-parallel kernel last
+    tiles = [(16, 1, 4, 0, 32)] + [(wd, 1, 2, 0, 32) for wd in (32, 56, 88, 128, 176, 256)] + [(1 << 30, 32, 9, 0, 1)]
+    ctx.set_tiles(tiles)
+    opt = g.default_opt()
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def call(src):
+        ctx.chain2aln(opt, wl.l_pac, wl.ref_off, src["anns"], len(wl.anns), src["reads"], wl.n_reads,
+                      src["chains"], len(wl.chains), src["seeds"], n_seeds, src["codes"], src["nmask"],
+                      d_regs, d_nregs, d_status, schedule=g.SCHED_SORTED, stream=stream)
+
+    call(d)
+    torch.cuda.synchronize()
+    regs = d_regs.cpu().numpy().view(ALNREG_DT)
+    nregs = d_nregs.cpu().numpy()
+    exact = bool((d_status == 0).all()) and np.array_equal(nregs, onregs) and np.array_equal(
+        nat.region_rows(regs, nregs, wl.chains, wl.reads), nat.region_rows(oregs, onregs, wl.chains, wl.reads))
+    if not exact:
+        raise SystemExit("chain-level results differ from the oracle")
+    clocks = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    clocks.start()
+    ms = timed_steps(lambda: call(d), args.steps, args.warmup, stream, flush)
+    clk = clocks.stop()
+
+    def e2e_step():
+        for k in d:
+            d[k].copy_(host[k], non_blocking=True)
+        call(d)
+        h_regs.copy_(d_regs, non_blocking=True)
+        h_nregs.copy_(d_nregs, non_blocking=True)
+        h_status.copy_(d_status, non_blocking=True)
+
+    e2e_ms = timed_steps(e2e_step, max(3, args.steps // 4), args.warmup, stream, flush)
+    t = sum(ms) / len(ms)
+    te = sum(e2e_ms) / len(e2e_ms)
+    (t, te), (tot_cells, tot_reads) = combine_ranks(dist, [t, te], [cells, wl.n_reads], dev)
+    if rank != 0:
+        return
+    peak_gcups = ctx.int_peak() / 8 / 1e9
+    cpu_t, _, _ = ref_chains_threaded(wl, opt_cpu, threads) if nat.have_ref() else (None, None, None)
+    gcups = tot_cells / (t * 1e-3) / 1e9
+    bi = sum(v.numel() for v in host.values())
+    bo = h_regs.numel() + 4 * (h_nregs.numel() + h_status.numel())
+    print(json.dumps({
+        "metric": metric, "value": round(gcups, 3), "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)", "config": cfg,
+        "reads_per_s": round(tot_reads / (t * 1e-3), 1),
+        "e2e": {"value": round(tot_cells / (te * 1e-3) / 1e9, 3), "unit": "GCUPS", "ms_per_step": round(te, 4),
+                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
+        "roofline": {"bound": "int_alu", "achieved": round(gcups / max(ws, 1), 3), "peak": round(peak_gcups, 3),
+                     "unit": "GCUPS", "frac": round(gcups / max(ws, 1) / peak_gcups, 4), "traffic": None,
+                     "note": "the whole call (waves of seed-level extension through the width classes) "
+                             "against the int-ALU cells/s peak"},
+        "cpu_baseline": None if cpu_t is None else {
+            "value": round(cells / cpu_t / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
+            "sample": "whole rank-0 workload, one pass, the reference's own mem_chain2aln"},
+        "clocks": clk, "outputs_equal_oracle": exact,
+        # per step: prep, resolve and finish, the five seed-level passes and four extension
+        # waves of (cost, scan, scatter, one launch per width class)
+        "gpu_launches": args.steps * (3 + 5 + 4 * (3 + len(tiles))), "width_classes": tiles,
+    }), flush=True)
+
+
 def combine_ranks(dist, times, counts, device):
     """Every rank calls this with its own step times and counts: returns the max over ranks
     of each time (the slowest replica sets the pace) and the sum over ranks of each count.
@@ -242,6 +412,9 @@ def timed_pipeline(submit, wait, k, w, stream, flush):
 def main():
     args = parse()
     ws, rank, local = dist_setup()
+    if args.workload == "chains":
+        run_chain_workload(args, ws, rank)
+        return
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
         return

@@ -1,19 +1,23 @@
 // g3x_chain.cu -- mem_chain2aln (bwa/src/aux.cu:178-315) for batches of reads on the GPU.
 //
 // The reference runs one read's chains, and within a chain its seeds, one after the other:
-// whether a seed is extended depends on the regions its read already has.  Here reads run
-// side by side and seeds in waves:
-//   prep    : one thread per read: each chain's reference window (aux.cu:186-205 and the
-//             contig clipping of bns_fetch_seq_gpu, bwa/src/bntseq.cu:62-80) and its seeds'
-//             processing order (keys score << 32 | index, aux.cu:207-210);
-//   decide  : one thread per read: walks the read's seeds in order from where the last wave
-//             stopped, skipping every seed the containment test rejects (aux.cu:214-245),
-//             and queues the first seed to extend;
-//   extend  : the queued seeds through g3x_extend_seeds (left and right extension with band
-//             retry, aux.cu:253-309), i.e. the context's width classes;
-//   commit  : one thread per queued seed: the region with its seed coverage (aux.cu:247-256,
-//             303-314) appended to its read's regions, which the next decide reads.
-// The host reads each wave's size back; the waves end when no read queues a seed.
+// whether a seed is extended depends on the regions its read already has.  But a seed's
+// extension itself depends only on the seed, its chain's reference window and the read, not
+// on any other seed.  So every seed of the batch is extended at once, and the order-dependent
+// decisions are replayed afterwards on the results:
+//   prep     : one thread per read: each chain's reference window (aux.cu:186-205 and the
+//              contig clipping of bns_fetch_seq_gpu, bwa/src/bntseq.cu:62-80), its seeds'
+//              processing order (keys score << 32 | index, aux.cu:207-210), and a seed-level
+//              record per seed;
+//   extend   : all seeds through g3x_extend_seeds (left and right extension with band retry,
+//              aux.cu:253-309), i.e. one batch through the context's width classes;
+//   resolve  : one thread per read: the seeds in order with the containment test and its
+//              overlap rescue (aux.cu:214-245) against the read's regions so far; a seed that
+//              passes takes its extension result and gives a region with its seed coverage
+//              (aux.cu:247-256, 303-314).
+// The results of the seeds the reference skips are computed and discarded: more DP cells
+// than the reference's (the price of one batch instead of one batch per region of the most
+// prolific read), the same regions.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include "g3x_internal.h"
@@ -71,8 +75,9 @@ __global__ void prep_kernel(const g3x_read_t* __restrict__ reads, int n_reads,
                             const g3x_chain_t* __restrict__ chains, int n_chains,
                             const g3x_cseed_t* __restrict__ seeds, int n_seeds, g3x_opt_t opt,
                             int64_t l_pac, const g3x_ann_t* __restrict__ anns, int n_seqs,
-                            int64_t* __restrict__ win, uint64_t* __restrict__ srt,
-                            ReadState* __restrict__ state, int32_t* __restrict__ maxlen) {
+                            int64_t ref_off, int64_t* __restrict__ win, uint64_t* __restrict__ srt,
+                            g3x_seed_t* __restrict__ xseeds, ReadState* __restrict__ state,
+                            int32_t* __restrict__ maxlen) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_reads) return;
     const g3x_read_t rd = reads[r];
@@ -91,7 +96,7 @@ __global__ void prep_kernel(const g3x_read_t* __restrict__ reads, int n_reads,
                  s.rbeg + s.len <= (l_pac << 1);
         }
     }
-    if (!ok) {
+    if (!ok) {   // its seeds keep the all-zero records, which make no jobs
         st.status = G3X_ERR_INVALID;
         st.chain = rd.chain_beg + (rd.n_chains > 0 ? rd.n_chains : 0);
         state[r] = st;
@@ -133,6 +138,19 @@ __global__ void prep_kernel(const g3x_read_t* __restrict__ reads, int n_reads,
         uint64_t* key = srt + ch.seed_beg;
         for (int i = 0; i < ch.n; ++i) key[i] = (uint64_t)cs[i].score << 32 | (uint64_t)i;
         sort_keys(key, ch.n);
+        for (int i = 0; i < ch.n; ++i) {                    // every seed's extension record
+            g3x_seed_t q;
+            q.read_off = (uint32_t)rd.read_off;
+            q.win_off = (uint32_t)(ref_off + r0);
+            q.l_query = rd.l_query;
+            q.qbeg = cs[i].qbeg;
+            q.len = cs[i].len;
+            q.pad_ = 0;
+            q.rbeg = cs[i].rbeg;
+            q.rmax0 = r0;
+            q.rmax1 = r1;
+            xseeds[ch.seed_beg + i] = q;
+        }
     }
     if (rd.n_chains > 0) st.k = chains[rd.chain_beg].n - 1;
     atomicMax(maxlen, rd.l_query);
@@ -155,97 +173,65 @@ __device__ bool around(const g3x_opt_t& opt, int l_query, const g3x_cseed_t& s, 
     return qd - rd < w && rd - qd < w;
 }
 
-__global__ void decide_kernel(const g3x_read_t* __restrict__ reads, int n_reads,
-                              const g3x_chain_t* __restrict__ chains, const g3x_cseed_t* __restrict__ seeds,
-                              g3x_opt_t opt, int64_t ref_off, const int64_t* __restrict__ win,
-                              uint64_t* __restrict__ srt, ReadState* __restrict__ state,
-                              const g3x_alnreg_t* __restrict__ regs, g3x_seed_t* __restrict__ wseeds,
-                              int32_t* __restrict__ wsrc, int32_t* __restrict__ count) {
+__global__ void resolve_kernel(const g3x_read_t* __restrict__ reads, int n_reads,
+                               const g3x_chain_t* __restrict__ chains, const g3x_cseed_t* __restrict__ seeds,
+                               g3x_opt_t opt, uint64_t* __restrict__ srt, ReadState* __restrict__ state,
+                               const g3x_reg_t* __restrict__ xregs, const int32_t* __restrict__ xstatus,
+                               g3x_alnreg_t* __restrict__ regs) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_reads) return;
     ReadState st = state[r];
     const g3x_read_t rd = reads[r];
     const int end = rd.chain_beg + rd.n_chains;
     if (st.status != G3X_OK || st.chain >= end) return;
-    const g3x_alnreg_t* av = regs + chains[rd.chain_beg].seed_beg;
-    for (;;) {
-        while (st.k < 0) {
-            if (++st.chain >= end) { state[r] = st; return; }
-            st.k = chains[st.chain].n - 1;
-        }
-        const g3x_chain_t ch = chains[st.chain];
+    g3x_alnreg_t* av = regs + chains[rd.chain_beg].seed_beg;
+    for (int ci = rd.chain_beg; ci < end; ++ci) {
+        const g3x_chain_t ch = chains[ci];
         const g3x_cseed_t* cs = seeds + ch.seed_beg;
         uint64_t* key = srt + ch.seed_beg;
-        const int k = st.k--;
-        const g3x_cseed_t s = cs[(uint32_t)key[k]];
-        int i = 0;
-        while (i < st.nreg && !around(opt, rd.l_query, s, av[i])) ++i;
-        if (i < st.nreg) {
-            // extended anyway only when an earlier seed of the chain, at least 95% as long,
-            // overlaps it by a quarter on another diagonal (aux.cu:234-244)
-            int j;
-            for (j = k + 1; j < ch.n; ++j) {
-                if (key[j] == 0) continue;
-                const g3x_cseed_t t = cs[(uint32_t)key[j]];
-                if (t.len < s.len * .95) continue;
-                if (s.qbeg <= t.qbeg && s.qbeg + s.len - t.qbeg >= s.len >> 2 &&
-                    t.qbeg - s.qbeg != t.rbeg - s.rbeg) break;
-                if (t.qbeg <= s.qbeg && t.qbeg + t.len - s.qbeg >= s.len >> 2 &&
-                    s.qbeg - t.qbeg != s.rbeg - t.rbeg) break;
+        for (int k = ch.n - 1; k >= 0; --k) {
+            const int si = (int)(uint32_t)key[k];
+            const g3x_cseed_t s = cs[si];
+            int i = 0;
+            while (i < st.nreg && !around(opt, rd.l_query, s, av[i])) ++i;
+            if (i < st.nreg) {
+                // extended anyway only when an earlier seed of the chain, at least 95% as
+                // long, overlaps it by a quarter on another diagonal (aux.cu:234-244)
+                int j;
+                for (j = k + 1; j < ch.n; ++j) {
+                    if (key[j] == 0) continue;
+                    const g3x_cseed_t t = cs[(uint32_t)key[j]];
+                    if (t.len < s.len * .95) continue;
+                    if (s.qbeg <= t.qbeg && s.qbeg + s.len - t.qbeg >= s.len >> 2 &&
+                        t.qbeg - s.qbeg != t.rbeg - s.rbeg) break;
+                    if (t.qbeg <= s.qbeg && t.qbeg + t.len - s.qbeg >= s.len >> 2 &&
+                        s.qbeg - t.qbeg != s.rbeg - t.rbeg) break;
+                }
+                if (j == ch.n) { key[k] = 0; continue; }
             }
-            if (j == ch.n) { key[k] = 0; continue; }
+            const int64_t xi = (int64_t)ch.seed_beg + si;
+            if (xstatus[xi] != G3X_OK) {                // an extension beyond the job limits
+                st.status = xstatus[xi];
+                state[r] = st;
+                return;
+            }
+            const g3x_reg_t x = xregs[xi];
+            g3x_alnreg_t a;
+            a.rb = x.rb; a.re = x.re; a.qb = x.qb; a.qe = x.qe;
+            a.rid = ch.rid; a.score = x.score; a.truesc = x.truesc; a.w = x.w;
+            a.seedcov = 0;
+            for (int t = 0; t < ch.n; ++t) {            // aux.cu:303-307
+                const g3x_cseed_t u = cs[t];
+                if (u.qbeg >= a.qb && u.qbeg + u.len <= a.qe && u.rbeg >= a.rb && u.rbeg + u.len <= a.re)
+                    a.seedcov += u.len;
+            }
+            a.seedlen0 = s.len;
+            a.frac_rep = ch.frac_rep;
+            a.pad_ = 0;
+            av[st.nreg++] = a;
         }
-        const int64_t r0 = win[2 * st.chain], r1 = win[2 * st.chain + 1];
-        g3x_seed_t q;
-        q.read_off = (uint32_t)rd.read_off;
-        q.win_off = (uint32_t)(ref_off + r0);
-        q.l_query = rd.l_query;
-        q.qbeg = s.qbeg;
-        q.len = s.len;
-        q.pad_ = 0;
-        q.rbeg = s.rbeg;
-        q.rmax0 = r0;
-        q.rmax1 = r1;
-        const int at = atomicAdd(count, 1);
-        wseeds[at] = q;
-        wsrc[3 * at] = r;
-        wsrc[3 * at + 1] = st.chain;
-        wsrc[3 * at + 2] = ch.seed_beg + (int32_t)(uint32_t)key[k];
-        state[r] = st;
-        return;
     }
-}
-
-__global__ void commit_kernel(const g3x_read_t* __restrict__ reads, const g3x_chain_t* __restrict__ chains,
-                              const g3x_cseed_t* __restrict__ seeds, const int32_t* __restrict__ wsrc,
-                              const g3x_reg_t* __restrict__ wregs, const int32_t* __restrict__ wstatus,
-                              const int32_t* __restrict__ count, ReadState* __restrict__ state,
-                              g3x_alnreg_t* __restrict__ regs) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= *count) return;
-    const int r = wsrc[3 * e], ci = wsrc[3 * e + 1], si = wsrc[3 * e + 2];
-    ReadState st = state[r];
-    if (wstatus[e] != G3X_OK) {
-        st.status = wstatus[e];
-        state[r] = st;
-        return;
-    }
-    const g3x_reg_t x = wregs[e];
-    const g3x_chain_t ch = chains[ci];
-    g3x_alnreg_t a;
-    a.rb = x.rb; a.re = x.re; a.qb = x.qb; a.qe = x.qe;
-    a.rid = ch.rid; a.score = x.score; a.truesc = x.truesc; a.w = x.w;
-    a.seedcov = 0;
-    for (int i = 0; i < ch.n; ++i) {                // aux.cu:303-307
-        const g3x_cseed_t t = seeds[ch.seed_beg + i];
-        if (t.qbeg >= a.qb && t.qbeg + t.len <= a.qe && t.rbeg >= a.rb && t.rbeg + t.len <= a.re)
-            a.seedcov += t.len;
-    }
-    a.seedlen0 = seeds[si].len;
-    a.frac_rep = ch.frac_rep;
-    a.pad_ = 0;
-    regs[chains[reads[r].chain_beg].seed_beg + st.nreg] = a;
-    ++st.nreg;
+    st.chain = end;
     state[r] = st;
 }
 
@@ -260,26 +246,24 @@ __global__ void finish_kernel(const ReadState* __restrict__ state, int n_reads, 
 }  // namespace
 
 void free_chain_scratch(ChainScratch& w) {
-    cudaFree(w.win); cudaFree(w.srt); cudaFree(w.state); cudaFree(w.wseeds); cudaFree(w.wsrc);
-    cudaFree(w.wregs); cudaFree(w.wstatus); cudaFree(w.count); cudaFree(w.maxlen);
-    cudaFreeHost(w.h_count);
+    cudaFree(w.win); cudaFree(w.srt); cudaFree(w.state); cudaFree(w.xseeds); cudaFree(w.xregs);
+    cudaFree(w.xstatus); cudaFree(w.maxlen);
+    cudaFreeHost(w.h_maxlen);
     w = ChainScratch();
 }
 
 static int alloc_chain_scratch(ChainScratch& w, int64_t reads, int64_t chains, int64_t seeds) {
-    if (w.count && reads <= w.reads && chains <= w.chains && seeds <= w.seeds) return G3X_OK;
+    if (w.maxlen && reads <= w.reads && chains <= w.chains && seeds <= w.seeds) return G3X_OK;
     const int64_t R = std::max(reads, w.reads), C = std::max(chains, w.chains), S = std::max(seeds, w.seeds);
     free_chain_scratch(w);
     bool ok = cudaMalloc(&w.win, std::max<int64_t>(C, 1) * 2 * sizeof(int64_t)) == cudaSuccess &&
               cudaMalloc(&w.srt, std::max<int64_t>(S, 1) * sizeof(uint64_t)) == cudaSuccess &&
               cudaMalloc(&w.state, std::max<int64_t>(R, 1) * 16) == cudaSuccess &&
-              cudaMalloc(&w.wseeds, std::max<int64_t>(R, 1) * sizeof(g3x_seed_t)) == cudaSuccess &&
-              cudaMalloc(&w.wsrc, std::max<int64_t>(R, 1) * 3 * sizeof(int32_t)) == cudaSuccess &&
-              cudaMalloc(&w.wregs, std::max<int64_t>(R, 1) * sizeof(g3x_reg_t)) == cudaSuccess &&
-              cudaMalloc(&w.wstatus, std::max<int64_t>(R, 1) * sizeof(int32_t)) == cudaSuccess &&
-              cudaMalloc(&w.count, sizeof(int32_t)) == cudaSuccess &&
+              cudaMalloc(&w.xseeds, std::max<int64_t>(S, 1) * sizeof(g3x_seed_t)) == cudaSuccess &&
+              cudaMalloc(&w.xregs, std::max<int64_t>(S, 1) * sizeof(g3x_reg_t)) == cudaSuccess &&
+              cudaMalloc(&w.xstatus, std::max<int64_t>(S, 1) * sizeof(int32_t)) == cudaSuccess &&
               cudaMalloc(&w.maxlen, 2 * sizeof(int32_t)) == cudaSuccess &&
-              cudaMallocHost(&w.h_count, 2 * sizeof(int32_t)) == cudaSuccess;
+              cudaMallocHost(&w.h_maxlen, 2 * sizeof(int32_t)) == cudaSuccess;
     if (!ok) { free_chain_scratch(w); cudaGetLastError(); return G3X_ERR_NOMEM; }
     w.reads = R; w.chains = C; w.seeds = S;
     return G3X_OK;
@@ -309,33 +293,30 @@ extern "C" int g3x_chain2aln(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_refin
     const cudaStream_t st = (cudaStream_t)stream;
     const int tb = 128, nb = (n_reads + tb - 1) / tb;
     ReadState* state = static_cast<ReadState*>(w.state);
-    if (cudaMemsetAsync(w.maxlen, 0, 2 * sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
+    // all-zero seed records (an empty read and seed: no extension jobs) for every seed that no
+    // valid read's chain sets
+    if (cudaMemsetAsync(w.maxlen, 0, 2 * sizeof(int32_t), st) != cudaSuccess ||
+        (n_seeds > 0 && cudaMemsetAsync(w.xseeds, 0, sizeof(g3x_seed_t) * (size_t)n_seeds, st) != cudaSuccess))
+        return G3X_ERR_CUDA;
     prep_kernel<<<nb, tb, 0, st>>>(d_reads, n_reads, d_chains, n_chains, d_seeds, n_seeds, *opt, ref->l_pac,
-                                   ref->d_anns, ref->n_seqs, w.win, w.srt, state, w.maxlen);
+                                   ref->d_anns, ref->n_seqs, ref->ref_off, w.win, w.srt, w.xseeds, state,
+                                   w.maxlen);
     if (cudaPeekAtLastError() != cudaSuccess ||
-        cudaMemcpyAsync(w.h_count, w.maxlen, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(w.h_maxlen, w.maxlen, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return G3X_ERR_CUDA;
-    // the extension waves' options: the caller's schedule and kernel choice, with length
-    // bounds from the batch itself
-    g3x_batch_opts_t xo = *opts;
-    xo.max_qlen = std::max<int32_t>(w.h_count[0], 1);
-    xo.max_tlen = std::max<int32_t>(w.h_count[1], 1);
-    xo.d_cells = nullptr;
-    // every wave extends at least one seed and every seed is visited once
-    for (int64_t wave = 0; wave <= n_seeds; ++wave) {
-        if (cudaMemsetAsync(w.count, 0, sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
-        decide_kernel<<<nb, tb, 0, st>>>(d_reads, n_reads, d_chains, d_seeds, *opt, ref->ref_off, w.win,
-                                         w.srt, state, d_regs, w.wseeds, w.wsrc, w.count);
-        if (cudaMemcpyAsync(w.h_count, w.count, sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess)
-            return G3X_ERR_CUDA;
-        const int32_t cnt = *w.h_count;
-        if (cnt == 0) break;
-        if ((rc = g3x_extend_seeds(ctx, opt, w.wseeds, cnt, d_codes, d_nmask, w.wregs, w.wstatus, &xo, stream)))
+    if (n_seeds > 0) {
+        // every seed extended in one batch: the caller's schedule and kernel choice, with length
+        // bounds from the batch itself
+        g3x_batch_opts_t xo = *opts;
+        xo.max_qlen = std::max<int32_t>(w.h_maxlen[0], 1);
+        xo.max_tlen = std::max<int32_t>(w.h_maxlen[1], 1);
+        xo.d_cells = nullptr;
+        if ((rc = g3x_extend_seeds(ctx, opt, w.xseeds, n_seeds, d_codes, d_nmask, w.xregs, w.xstatus, &xo,
+                                   stream)))
             return rc;
-        commit_kernel<<<(cnt + tb - 1) / tb, tb, 0, st>>>(d_reads, d_chains, d_seeds, w.wsrc, w.wregs, w.wstatus,
-                                                          w.count, state, d_regs);
+        resolve_kernel<<<nb, tb, 0, st>>>(d_reads, n_reads, d_chains, d_seeds, *opt, w.srt, state, w.xregs,
+                                          w.xstatus, d_regs);
         if (cudaPeekAtLastError() != cudaSuccess) return G3X_ERR_CUDA;
     }
     finish_kernel<<<nb, tb, 0, st>>>(state, n_reads, d_nregs, d_status);

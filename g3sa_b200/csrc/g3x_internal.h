@@ -144,13 +144,11 @@ struct ChainScratch {
     int64_t* win = nullptr;          // per chain: reference window [r0, r1)
     uint64_t* srt = nullptr;         // per seed: its chain's processing keys
     void* state = nullptr;           // per read: 16-byte walk state
-    g3x_seed_t* wseeds = nullptr;    // per wave: the queued seeds ...
-    int32_t* wsrc = nullptr;         // ... their (read, chain, seed)
-    g3x_reg_t* wregs = nullptr;      // ... and their extension results
-    int32_t* wstatus = nullptr;
-    int32_t* count = nullptr;        // seeds queued by the wave
+    g3x_seed_t* xseeds = nullptr;    // per seed: its seed-level extension record ...
+    g3x_reg_t* xregs = nullptr;      // ... and result
+    int32_t* xstatus = nullptr;
     int32_t* maxlen = nullptr;       // longest read and window of the call
-    int32_t* h_count = nullptr;      // pinned: count, or the two bounds
+    int32_t* h_maxlen = nullptr;     // pinned copy of the two bounds
     int64_t reads = 0, chains = 0, seeds = 0;
 };
 ChainScratch& ctx_chain(g3x_ctx* ctx);

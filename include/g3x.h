@@ -309,10 +309,13 @@ typedef struct {
    regions go to d_regs[chains[chain_beg].seed_beg ...] (at most one per seed), their number
    to d_nregs[r], a per-read status to d_status[r] (G3X_OK; G3X_ERR_INVALID for a read whose
    records break these rules; G3X_ERR_TOO_LONG when an extension exceeds the job limits, the
-   read's processing stopping there).  Runs in waves, one extended seed per read per wave,
-   the waves' extensions through the context's schedule (opts as g3x_extend_seeds); the
-   host waits for `stream` once per wave to read the wave's size.  Allocates context scratch
-   for larger calls. */
+   read's processing stopping there).  A seed's extension depends on nothing but the seed,
+   its chain's window and the read, so every seed of the batch is extended in one batch
+   through the context's schedule (opts->schedule, lanes, tile, kernel as for
+   g3x_extend_seeds; max_qlen / max_tlen are taken from the batch) and the reads' decisions
+   are replayed on the results: the same regions as the reference, more DP cells (the
+   results of the seeds it skips are discarded).  The host waits for `stream` once, after
+   the windows are known.  Allocates context scratch for larger calls. */
 int g3x_chain2aln(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_refinfo_t *ref,
                   const g3x_read_t *d_reads, int32_t n_reads, const g3x_chain_t *d_chains,
                   int32_t n_chains, const g3x_cseed_t *d_seeds, int32_t n_seeds,
