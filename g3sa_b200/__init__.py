@@ -149,6 +149,12 @@ def lib():
         I64 = ctypes.c_int64
         L.g3x_chain2aln.argtypes = [P, P, P, P, I32, P, I32, P, I32, P, P, P, P, P, P, P]
         L.g3x_chain2aln.restype = ctypes.c_int
+        L.g3x_pac_to_planes.argtypes = [P, I64, P, P, I64, P]
+        L.g3x_pac_to_planes.restype = ctypes.c_int
+        L.g3x_pack_codes_device.argtypes = [P, I64, P, P, I64, P]
+        L.g3x_pack_codes_device.restype = ctypes.c_int
+        L.g3x_pair_generate.argtypes = [P, P, P, I32, P, I32, P, I32, P, I32, P, P, P, P]
+        L.g3x_pair_generate.restype = ctypes.c_int
         L.g3x_pipe_create.argtypes = [P, P, I32, I32, I64, I64, ctypes.POINTER(P)]
         L.g3x_pipe_create.restype = ctypes.c_int
         L.g3x_pipe_submit.argtypes = [P, P, I32, P, I64, P, I64, I32, I32, P, P, P]
@@ -443,6 +449,32 @@ def _host_ptr(a):
 
 def _nbytes(a):
     return a.nbytes if isinstance(a, np.ndarray) else a.numel() * a.element_size()
+
+
+def pac_to_planes(d_pac, l_pac, d_codes, d_nmask, base, stream=None):
+    """g3x_pac_to_planes: bwa's packed reference (device bytes) to forward + reverse-complement
+    planes at base index `base`."""
+    _check(lib().g3x_pac_to_planes(_ptr(d_pac), int(l_pac), _ptr(d_codes), _ptr(d_nmask), int(base),
+                                   _stream(stream)), "g3x_pac_to_planes")
+
+
+def pack_codes_device(d_seq, n, d_codes, d_nmask, base, stream=None):
+    """g3x_pack_codes_device: n u8 codes (device) to the planes at base index `base`."""
+    _check(lib().g3x_pack_codes_device(_ptr(d_seq), int(n), _ptr(d_codes), _ptr(d_nmask), int(base),
+                                       _stream(stream)), "g3x_pack_codes_device")
+
+
+def pair_generate(opt, l_pac, ref_off, d_anns, n_seqs, d_reads, n_reads, d_chains, n_chains, d_seeds,
+                  n_seeds, d_recs, n_recs, d_out, d_rid, d_status, stream=None):
+    """g3x_pair_generate: per seed record (SEEDREC_DT) its g3x_seed_t (DSEED_DT) and contig id."""
+    ri = np.zeros(1, REFINFO_DT)
+    ri["l_pac"], ri["ref_off"], ri["n_seqs"], ri["d_anns"] = l_pac, ref_off, n_seqs, _ptr(d_anns)
+    _check(lib().g3x_pair_generate(opt.ctypes.data, ri.ctypes.data, _ptr(d_reads), int(n_reads), _ptr(d_chains),
+                                   int(n_chains), _ptr(d_seeds), int(n_seeds), _ptr(d_recs), int(n_recs),
+                                   _ptr(d_out), _ptr(d_rid), _ptr(d_status), _stream(stream)), "g3x_pair_generate")
+
+
+SEEDREC_DT = np.dtype([("read", "<i4"), ("chain", "<i4"), ("seed", "<i4")])
 
 
 class Pipe:

@@ -171,3 +171,13 @@ def synth_chains(n_reads, seed=1, n_contigs=12, contig_len=(20000, 120000), a=1,
         s = np.array(seeds, np.int64)
         S["rbeg"], S["qbeg"], S["len"], S["score"] = s[:, 0], s[:, 1], s[:, 2], s[:, 3]
     return ChainWorkload(u8, l_pac, anns, R, C, S)
+
+
+def pac_of(fwd):
+    """bwa's packed reference of forward codes 0-3: base k in byte k >> 2, bits ((~k) & 3) << 1
+    (bwa/src/bntseq.cu:4-5)."""
+    fwd = np.asarray(fwd, np.uint8)
+    k = np.arange(len(fwd), dtype=np.int64)
+    pac = np.zeros(len(fwd) // 4 + 1, np.uint8)
+    np.bitwise_or.at(pac, k >> 2, ((fwd & 3).astype(np.uint8) << ((~k & 3) << 1).astype(np.uint8)))
+    return pac

@@ -322,6 +322,42 @@ int g3x_chain2aln(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_refinfo_t *ref,
                   const uint32_t *d_codes, const uint32_t *d_nmask, g3x_alnreg_t *d_regs,
                   int32_t *d_nregs, int32_t *d_status, const g3x_batch_opts_t *opts, void *stream);
 
+/* ---- the stage's inputs from the reference's own data ----------------------------------- */
+/* The packed reference (bwa's pac: base k in byte k >> 2, bits ((~k) & 3) << 1,
+   bwa/src/bntseq.cu:4-5) as the 2*l_pac bases that g3x_chain2aln and g3x_pair_generate read:
+   the forward strand, then its reverse complement (bns_get_seq_gpu, bwa/src/bntseq.cu:39-60),
+   written to the planes at base index `base`.  Device buffers; asynchronous on `stream` (the
+   current device).  Only the planes' words holding bases [base, base + 2*l_pac) are written,
+   and in the first and last of them only those bases. */
+int g3x_pac_to_planes(const uint8_t *d_pac, int64_t l_pac, uint32_t *d_codes, uint32_t *d_nmask,
+                      int64_t base, void *stream);
+
+/* g3x_pack_codes on device buffers: len u8 codes (0-3 bases, anything else N) to bases
+   [base, base + len) of the planes, e.g. the batch's reads (the reference's d_seq) in one
+   call; their read_off is then base + d_seq_offset[r].  Same word rule as above. */
+int g3x_pack_codes_device(const uint8_t *d_seq, int64_t len, uint32_t *d_codes, uint32_t *d_nmask,
+                          int64_t base, void *stream);
+
+/* One seed of one chain of one read, as the reference's seed_record_t names it (seqID,
+   chainID, seedID; bwa/src/bwa.h:272-287), with chain and seed absolute indices into the
+   chain and seed arrays (seed relative to its chain). */
+typedef struct {
+    int32_t read, chain, seed;
+} g3x_seedrec_t;          /* 12 bytes */
+
+/* ExtendingPairGenerate (bwa/src/aux.cu:2101-2189) for n_recs seed records: the chain's
+   reference window (aux.cu:2134-2156, clipped by bns_fetch_seq_gpu to the first seed's contig
+   and strand) as a g3x_seed_t for g3x_extend_seeds (which reads the sequences in place and
+   reverses the left side itself), and the window's contig id in d_rid (what the reference
+   writes to the region's rid).  d_status[i]: G3X_OK, or G3X_ERR_INVALID for a record that
+   indexes outside its arrays (its g3x_seed_t then makes no extension jobs).  Asynchronous on
+   `stream` (the current device). */
+int g3x_pair_generate(const g3x_opt_t *opt, const g3x_refinfo_t *ref, const g3x_read_t *d_reads,
+                      int32_t n_reads, const g3x_chain_t *d_chains, int32_t n_chains,
+                      const g3x_cseed_t *d_seeds, int32_t n_seeds, const g3x_seedrec_t *d_recs,
+                      int32_t n_recs, g3x_seed_t *d_out, int32_t *d_rid, int32_t *d_status,
+                      void *stream);
+
 /* ---- host-resident batches, pipelined --------------------------------------------------- */
 /* No counterpart in the reference (its batches stay on the device between pipeline stages).
    A pipe extends batches of jobs that live in host memory with the context's schedule and
