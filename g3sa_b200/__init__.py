@@ -149,6 +149,8 @@ def lib():
         I64 = ctypes.c_int64
         L.g3x_chain2aln.argtypes = [P, P, P, P, I32, P, I32, P, I32, P, P, P, P, P, P, P]
         L.g3x_chain2aln.restype = ctypes.c_int
+        L.g3x_ksw_global2_batch.argtypes = [P, P, P, I32, P, P, I32, I32, I32, P, P, I32, P, P, P]
+        L.g3x_ksw_global2_batch.restype = ctypes.c_int
         L.g3x_pac_to_planes.argtypes = [P, I64, P, P, I64, P]
         L.g3x_pac_to_planes.restype = ctypes.c_int
         L.g3x_pack_codes_device.argtypes = [P, I64, P, P, I64, P]
@@ -415,6 +417,14 @@ class Context:
                                  _ptr(d_nmask), _ptr(d_regs), _ptr(d_nregs), _ptr(d_status), opts.ctypes.data,
                                  _stream(stream))
         _check(rc, "g3x_chain2aln")
+
+    def global_batch(self, score, d_jobs, n, d_codes, d_nmask, max_qlen, max_tlen, max_w, d_score, d_cigar,
+                     cigar_stride, d_n_cigar, d_status, stream=None):
+        """g3x_ksw_global2_batch on device buffers (JOB_DT jobs; the job's w is the band)."""
+        _check(lib().g3x_ksw_global2_batch(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
+                                           _ptr(d_nmask), int(max_qlen), int(max_tlen), int(max_w), _ptr(d_score),
+                                           _ptr(d_cigar), int(cigar_stride), _ptr(d_n_cigar), _ptr(d_status),
+                                           _stream(stream)), "g3x_ksw_global2_batch")
 
     def extend_seeds_stream(self, opt, seeds, codes, nmask, n_bases, regs, status, max_qlen,
                             max_tlen, chunk=65536, schedule=SCHED_SORTED, lanes=0, tile=0,

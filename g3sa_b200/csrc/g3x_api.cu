@@ -15,6 +15,7 @@ struct g3x_ctx {
     g3x::ModelState model;       // learned cost model
     g3x::SchedScratch sched;     // job order and width classes of a persistent batch
     g3x::ChainScratch chain;     // chain-level call state
+    g3x::GlobalScratch global;   // global-alignment backtrack bytes
     g3x::TileTable tiles;        // width classes and their kernel configurations
     unsigned long long* d_stats; // occupancy counters of the last persistent batch
     cudaStream_t side[g3x::kMaxBuckets];   // one stream per width class
@@ -28,6 +29,7 @@ namespace g3x {
 
 int ctx_device(const g3x_ctx* ctx) { return ctx->device; }
 ChainScratch& ctx_chain(g3x_ctx* ctx) { return ctx->chain; }
+GlobalScratch& ctx_global(g3x_ctx* ctx) { return ctx->global; }
 
 int score_params(const g3x_score_t* s, ScoreParams* sp) {
     if (!s) return G3X_ERR_INVALID;
@@ -342,6 +344,8 @@ int g3x_ctx_destroy(g3x_ctx* c) {
     g3x::model_free(c->model);
     g3x::free_sched(c->sched);
     g3x::free_chain_scratch(c->chain);
+    cudaFree(c->global.z);
+    cudaFree(c->global.queue);
     for (int k = 0; k < g3x::kMaxBuckets; ++k) {
         cudaStreamDestroy(c->side[k]);
         cudaEventDestroy(c->join[k]);

@@ -152,6 +152,14 @@ struct ChainScratch {
     int64_t reads = 0, chains = 0, seeds = 0;
 };
 ChainScratch& ctx_chain(g3x_ctx* ctx);
+
+// Direction bytes of the global-alignment backtrack (g3x_global.cu), grown on demand.
+struct GlobalScratch {
+    uint8_t* z = nullptr;
+    int32_t* queue = nullptr;
+    int64_t bytes = 0;
+};
+GlobalScratch& ctx_global(g3x_ctx* ctx);
 void free_chain_scratch(ChainScratch& w);
 
 // Learned cost model state (device buffers; g3x_model.cu).

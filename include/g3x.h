@@ -358,6 +358,24 @@ int g3x_pair_generate(const g3x_opt_t *opt, const g3x_refinfo_t *ref, const g3x_
                       int32_t n_recs, g3x_seed_t *d_out, int32_t *d_rid, int32_t *d_status,
                       void *stream);
 
+/* ---- banded global alignment with backtrack ------------------------------------------- */
+/* n calls of ksw_global2 (bwa/src/ksw.cu:706-809) as traceback_baseline issues them
+   (bwa/src/aux.cu:2794-2830): job k aligns its query (q_off, qlen) globally to its target
+   (t_off, tlen) inside the band |i - j| <= w (the job's w; h0 unused; G3X_JOB_QREV/TREV read
+   the planes reversed).  d_score[k] = the reference's return value; the CIGAR (BAM order,
+   len << 4 | op, 0 = M, 1 = I, 2 = D, runs merged as push_cigar does, ksw.cu:694-704) goes to
+   d_cigar[k * cigar_stride ...] and its length to d_n_cigar[k].  When no alignment inside the
+   band reaches the last cell (score <= -2^29) the reference's backtrack reads direction bytes
+   it never wrote; here the CIGAR is then empty.  d_status[k]: G3X_OK; G3X_ERR_TOO_LONG for a
+   job beyond max_qlen / max_tlen / max_w or whose CIGAR exceeds cigar_stride (empty CIGAR;
+   qlen + tlen + 2 always suffices).  Scratch: max_tlen x min(max_qlen, 2 max_w + 1) bytes per
+   resident warp (at most 8 GiB, fewer warps beyond), allocated in the context for larger
+   calls.  Asynchronous on `stream`. */
+int g3x_ksw_global2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
+                          const uint32_t *d_codes, const uint32_t *d_nmask, int32_t max_qlen,
+                          int32_t max_tlen, int32_t max_w, int32_t *d_score, uint32_t *d_cigar,
+                          int32_t cigar_stride, int32_t *d_n_cigar, int32_t *d_status, void *stream);
+
 /* ---- host-resident batches, pipelined --------------------------------------------------- */
 /* No counterpart in the reference (its batches stay on the device between pipeline stages).
    A pipe extends batches of jobs that live in host memory with the context's schedule and

@@ -3,7 +3,8 @@
 # source file where it lies (bwa/src/ksw.cu, lines 299-401 = eh_t + ksw_extend2) as host
 # C++, the reference's own band-retry lines of mem_chain2aln (bwa/src/aux.cu:253-255,
 # 258-301, 309), the whole of mem_chain2aln with the window fetch it calls
-# (bwa/src/aux.cu:168-175, 178-315; bwa/src/bntseq.cu:5, 7-87), plus the ctypes batch driver
+# (bwa/src/aux.cu:168-175, 178-315; bwa/src/bntseq.cu:5, 7-87), the banded global alignment
+# with backtrack (bwa/src/ksw.cu:299-301, 548, 694-809), plus the ctypes batch driver
 # ref_wrap.cpp.  The source lines are streamed from the
 # reference tree into the compiler; no reference source is copied into this repository.
 # Usage: sh oracle/build_ref.sh [reference_root]   (default /root/reference)
@@ -64,7 +65,20 @@ fi
 { grep -m1 '^#define MAX_BAND_TRY' "$AUXH"; cat "$HERE/ref_chain_head.inc"; sed -n '5p;7,87p' "$BNS"; \
   sed -n '168,175p;178,315p' "$AUX"; cat "$HERE/ref_chain_tail.inc"; } | tr -d '\r' | \
     $CXX -O3 -fPIC -std=c++17 -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/chain_ref_fn.o"
+# Banded global alignment: eh_t, MINUS_INF, push_cigar and ksw_global2 (ksw.cu:299-301, 548,
+# 694-704, 706-809) between ref_global_head.inc and ref_global_tail.inc.
+K548=$(sed -n '548p' "$SRC" | tr -d '\r' | sed 's/^ *//')
+K694=$(sed -n '694p' "$SRC" | tr -d '\r' | cut -c1-49)
+K706=$(sed -n '706p' "$SRC" | tr -d '\r' | cut -c1-26)
+K809=$(sed -n '809p' "$SRC" | tr -d '\r')
+if [ "$K548" != "#define MINUS_INF -0x40000000" ] || [ "$K694" != "__device__ static inline uint32_t *push_cigar(int" ] || \
+   [ "$K706" != "__device__ int ksw_global2" ] || [ "$K809" != "}" ]; then
+    echo "build_ref.sh: unexpected content at ksw.cu:548/694/706/809; refusing to build" >&2
+    exit 3
+fi
+{ cat "$HERE/ref_global_head.inc"; sed -n '299,301p;548p;694,704p;706,809p' "$SRC"; cat "$HERE/ref_global_tail.inc"; } | \
+    tr -d '\r' | $CXX -O3 -fPIC -std=c++17 -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/global_ref_fn.o"
 $CXX -O3 -fPIC -shared -std=c++17 "$HERE/ref_wrap.cpp" "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" \
-    "$OUT/chain_ref_fn.o" -o "$OUT/libksw_ref.so" -lpthread
-rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" "$OUT/chain_ref_fn.o"
+    "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" -o "$OUT/libksw_ref.so" -lpthread
+rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o"
 echo "built $OUT/libksw_ref.so"

@@ -566,3 +566,103 @@ void g3o_chain2aln_reads(const g3o_opt *opt, const uint8_t *codes, int64_t ref_o
         nregs[r] = nav;
     }
 }
+
+/* ---------------------------------------------------------------------------------- */
+/* Banded global alignment with backtrack: ksw_global2 (ksw.cu:706-809) and the CIGAR  */
+/* run merging of push_cigar (ksw.cu:694-704).  Outside the band the DP holds          */
+/* -0x40000000 (ksw.cu:548).                                                            */
+/* ---------------------------------------------------------------------------------- */
+
+#define G3O_NEG_INF (-0x40000000)
+
+static void g3o_push_op(uint32_t *cig, int *n, int op, int len)
+{
+    if (*n > 0 && (int)(cig[*n - 1] & 0xf) == op) cig[*n - 1] += (uint32_t)len << 4;
+    else cig[(*n)++] = (uint32_t)len << 4 | (uint32_t)op;
+}
+
+/* Score of the best global alignment in the band |i - j| <= w; with cigar != NULL the
+   CIGAR (BAM order: len << 4 | op, 0 = M, 1 = I, 2 = D) goes there (room for qlen + tlen + 2
+   operations) and its length to *n_cigar, 0 when no alignment in the band reaches the last
+   cell (score <= -2^29).  *cells receives the DP cells (may be NULL). */
+int g3o_ksw_global2(int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                    const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins, int w,
+                    int *n_cigar, uint32_t *cigar, int64_t *cells)
+{
+    const int oe_del = o_del + e_del, oe_ins = o_ins + e_ins;
+    const int ncol = qlen < 2 * w + 1 ? qlen : 2 * w + 1;
+    uint8_t *z = cigar && ncol > 0 && tlen > 0 ? (uint8_t *)malloc((size_t)ncol * tlen) : NULL;
+    int32_t *H = (int32_t *)malloc(sizeof(int32_t) * ((size_t)qlen + 1));
+    int32_t *E = (int32_t *)malloc(sizeof(int32_t) * ((size_t)qlen + 1));
+    int64_t nc = 0;
+    H[0] = 0; E[0] = G3O_NEG_INF;                           /* the first row */
+    for (int j = 1; j <= qlen; ++j) {
+        H[j] = j <= w ? -(o_ins + e_ins * j) : G3O_NEG_INF;
+        E[j] = G3O_NEG_INF;
+    }
+    for (int i = 0; i < tlen; ++i) {
+        const int beg = i > w ? i - w : 0, end = i + w + 1 < qlen ? i + w + 1 : qlen;
+        const int8_t *row = mat + target[i] * 5;
+        int32_t f = G3O_NEG_INF;
+        int32_t h1 = beg == 0 ? -(o_del + e_del * (i + 1)) : G3O_NEG_INF;
+        for (int j = beg; j < end; ++j) {
+            /* H[j] = H(i-1, j-1), E[j] = E(i, j), f = F(i, j), h1 = H(i, j-1) */
+            const int32_t m = H[j] + row[query[j]];
+            int32_t e = E[j];
+            H[j] = h1;
+            uint8_t d = m >= e ? 0 : 1;
+            int32_t h = m >= e ? m : e;
+            if (h < f) { d = 2; h = f; }
+            h1 = h;
+            int32_t t = m - oe_del;
+            e -= e_del;
+            if (e > t) d |= 1 << 2; else e = t;
+            E[j] = e;
+            t = m - oe_ins;
+            f -= e_ins;
+            if (f > t) d |= 2 << 4; else f = t;
+            if (z) z[(size_t)i * ncol + (j - beg)] = d;
+        }
+        nc += end > beg ? end - beg : 0;
+        H[end] = h1; E[end] = G3O_NEG_INF;
+    }
+    const int score = H[qlen];
+    if (cigar && score <= G3O_NEG_INF / 2) {
+        /* no alignment inside the band reaches the last cell: the reference's backtrack then
+           walks direction bytes it never wrote (undefined); here the CIGAR is empty */
+        *n_cigar = 0;
+    } else if (cigar) {
+        int n = 0, which = 0;
+        int i = tlen - 1, k = (i + w + 1 < qlen ? i + w + 1 : qlen) - 1;
+        while (i >= 0 && k >= 0) {
+            which = z[(size_t)i * ncol + (k - (i > w ? i - w : 0))] >> (which << 1) & 3;
+            if (which == 0) { g3o_push_op(cigar, &n, 0, 1); --i; --k; }
+            else if (which == 1) { g3o_push_op(cigar, &n, 2, 1); --i; }
+            else { g3o_push_op(cigar, &n, 1, 1); --k; }
+        }
+        if (i >= 0) g3o_push_op(cigar, &n, 2, i + 1);
+        if (k >= 0) g3o_push_op(cigar, &n, 1, k + 1);
+        for (int a = 0; a < n >> 1; ++a) {
+            const uint32_t t = cigar[a]; cigar[a] = cigar[n - 1 - a]; cigar[n - 1 - a] = t;
+        }
+        *n_cigar = n;
+    }
+    free(z); free(H); free(E);
+    if (cells) *cells = nc;
+    return score;
+}
+
+/* n global alignments over one code buffer (jobs as g3o_job, flags ignored; h0 unused):
+   scores, CIGARs at cigar[k * stride] (stride >= qlen + tlen + 2), their lengths. */
+void g3o_global_batch(const g3o_job *jobs, int64_t n, const uint8_t *codes, const g3o_score *sc,
+                      int32_t *score, uint32_t *cigar, int32_t stride, int32_t *n_cigar, int64_t *cells)
+{
+    for (int64_t k = 0; k < n; ++k) {
+        const g3o_job *j = &jobs[k];
+        int nc = 0;
+        score[k] = g3o_ksw_global2(j->qlen, codes + j->q_off, j->tlen, codes + j->t_off, sc->mat, sc->o_del,
+                                   sc->e_del, sc->o_ins, sc->e_ins, j->w, &nc, cigar + (size_t)k * stride,
+                                   cells ? cells + k : NULL);
+        n_cigar[k] = nc;
+    }
+}

@@ -44,6 +44,8 @@ def oracle():
         P, I64 = ctypes.c_void_p, ctypes.c_int64
         _oracle.g3o_chain2aln_reads.argtypes = [P, P, I64, I64, P, ctypes.c_int, P, I64, P, P, P, P, P]
         _oracle.g3o_chain2aln_reads.restype = None
+        _oracle.g3o_global_batch.argtypes = [P, I64, P, P, P, P, ctypes.c_int32, P, P]
+        _oracle.g3o_global_batch.restype = None
     return _oracle
 
 
@@ -60,6 +62,8 @@ def ref():
         P, I64 = ctypes.c_void_p, ctypes.c_int64
         _ref.g3r_chain2aln_reads.argtypes = [P, P, I64, I64, P, ctypes.c_int, P, I64, P, P, P, P]
         _ref.g3r_chain2aln_reads.restype = ctypes.c_int
+        _ref.g3r_global_batch.argtypes = [P, I64, P, P, P, P, ctypes.c_int32, P]
+        _ref.g3r_global_batch.restype = ctypes.c_int
     return _ref
 
 
@@ -201,3 +205,61 @@ def region_rows(regs, nregs, chains, reads):
             b = int(chains[reads["chain_beg"][r]]["seed_beg"])
             out.append(regs[b:b + int(nregs[r])])
     return np.concatenate(out) if out else regs[:0]
+
+
+NEG_HALF = -0x40000000 // 2
+
+
+def global_jobs(n, seed, max_len=160, ws=(0, 1, 3, 5, 17, 50, 100), n_frac=0.1):
+    """n (query, target) pairs for banded global alignment: targets are the queries with a few
+    substitutions and 1-base indels; some queries carry N codes.  Returns (CPU_JOB_DT jobs,
+    u8 codes)."""
+    rng = np.random.default_rng(seed)
+    jobs = np.zeros(n, CPU_JOB_DT)
+    bufs, off = [], 0
+    for k in range(n):
+        ql = int(rng.integers(0, max_len))
+        q = rng.integers(0, 5 if rng.random() < n_frac else 4, ql).astype(np.uint8)
+        t = list(q)
+        for _ in range(int(rng.integers(0, 6))):
+            if not t:
+                break
+            p, u = int(rng.integers(0, len(t))), rng.random()
+            if u < 0.5:
+                t[p] = int(rng.integers(0, 4))
+            elif u < 0.75:
+                del t[p]
+            else:
+                t.insert(p, int(rng.integers(0, 4)))
+        t = np.array(t, np.uint8)
+        jobs[k]["q_off"], jobs[k]["t_off"] = off, off + len(q)
+        bufs += [q, t]
+        off += len(q) + len(t)
+        jobs[k]["qlen"], jobs[k]["tlen"] = len(q), len(t)
+        jobs[k]["w"] = int(rng.choice(ws))
+    return jobs, (np.concatenate(bufs) if bufs else np.zeros(1, np.uint8))
+
+
+def _global(fn, jobs, u8, score, stride, with_cells):
+    n = len(jobs)
+    sc = cpu_score(score)
+    s = np.zeros(n, np.int32)
+    c = np.zeros(max(n * stride, 1), np.uint32)
+    nc = np.zeros(n, np.int32)
+    args = [np.ascontiguousarray(jobs).ctypes.data, n, np.ascontiguousarray(u8).ctypes.data, sc.ctypes.data,
+            s.ctypes.data, c.ctypes.data, stride, nc.ctypes.data]
+    cells = np.zeros(n, np.int64)
+    if with_cells:
+        args.append(cells.ctypes.data)
+    fn(*args)
+    return s, c.reshape(n, stride) if n else c[:0].reshape(0, stride), nc, cells
+
+
+def oracle_global(jobs, u8, score, stride):
+    """(score, cigar [n, stride], n_cigar, cells) from the C restatement of ksw_global2."""
+    return _global(oracle().g3o_global_batch, jobs, u8, score, stride, True)
+
+
+def ref_global(jobs, u8, score, stride):
+    """(score, cigar, n_cigar) from the reference's own ksw_global2."""
+    return _global(ref().g3r_global_batch, jobs, u8, score, stride, False)[:3]
