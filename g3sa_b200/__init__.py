@@ -28,7 +28,7 @@ G3X_ERR_NOMEM = -7
 G3X_ERR_NOT_TRAINED = -8
 
 SCHED_PLAIN, SCHED_SORTED, SCHED_LEARNED = 0, 1, 2
-JOB_QREV, JOB_TREV = 1, 2
+JOB_QREV, JOB_TREV, JOB_MDRC = 1, 2, 4
 
 # ---- record types (byte-identical to the C structs) -------------------------------------
 SCORE_DT = np.dtype([("mat", "i1", 25), ("pad_", "i1", 3), ("m", "<i4"), ("o_del", "<i4"),
@@ -149,7 +149,7 @@ def lib():
         I64 = ctypes.c_int64
         L.g3x_chain2aln.argtypes = [P, P, P, P, I32, P, I32, P, I32, P, P, P, P, P, P, P]
         L.g3x_chain2aln.restype = ctypes.c_int
-        L.g3x_ksw_global2_batch.argtypes = [P, P, P, I32, P, P, I32, I32, I32, P, P, I32, P, P, P]
+        L.g3x_ksw_global2_batch.argtypes = [P, P, P, I32, P, P, I32, I32, I32, P, P, I32, P, P, P, I32, P, P]
         L.g3x_ksw_global2_batch.restype = ctypes.c_int
         L.g3x_pac_to_planes.argtypes = [P, I64, P, P, I64, P]
         L.g3x_pac_to_planes.restype = ctypes.c_int
@@ -419,12 +419,14 @@ class Context:
         _check(rc, "g3x_chain2aln")
 
     def global_batch(self, score, d_jobs, n, d_codes, d_nmask, max_qlen, max_tlen, max_w, d_score, d_cigar,
-                     cigar_stride, d_n_cigar, d_status, stream=None):
-        """g3x_ksw_global2_batch on device buffers (JOB_DT jobs; the job's w is the band)."""
+                     cigar_stride, d_n_cigar, d_status, d_nm=None, d_md=None, md_stride=0, stream=None):
+        """g3x_ksw_global2_batch on device buffers (JOB_DT jobs; the job's w is the band; NM/MD
+        when d_nm and d_md are given)."""
         _check(lib().g3x_ksw_global2_batch(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
                                            _ptr(d_nmask), int(max_qlen), int(max_tlen), int(max_w), _ptr(d_score),
-                                           _ptr(d_cigar), int(cigar_stride), _ptr(d_n_cigar), _ptr(d_status),
-                                           _stream(stream)), "g3x_ksw_global2_batch")
+                                           _ptr(d_cigar), int(cigar_stride), _ptr(d_n_cigar), _ptr(d_nm),
+                                           _ptr(d_md), int(md_stride), _ptr(d_status), _stream(stream)),
+               "g3x_ksw_global2_batch")
 
     def extend_seeds_stream(self, opt, seeds, codes, nmask, n_bases, regs, status, max_qlen,
                             max_tlen, chunk=65536, schedule=SCHED_SORTED, lanes=0, tile=0,

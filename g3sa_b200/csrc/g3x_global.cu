@@ -12,7 +12,8 @@
 // continuing in bits 2 and 4-5) goes to global scratch, laid out [row][band column][lane] per
 // warp so that the 32 lanes of a step write one 32-byte sector.  The backtrack then walks each
 // lane's bytes from the last cell (ksw.cu:783-806) and writes the CIGAR, merging runs as
-// push_cigar does (ksw.cu:694-704).
+// push_cigar does (ksw.cu:694-704); on request NM and the MD string follow, as the traceback
+// stage computes them (bwa/src/aux.cu:2831-2860).
 #include <cuda_runtime.h>
 #include <algorithm>
 #include "g3x_core.h"
@@ -36,8 +37,20 @@ struct GlobalDesc {
     uint8_t* z;            // direction bytes: per warp slot zwarp bytes
     int64_t zwarp;
     int32_t* queue;
-    int32_t n, qmax, tmax, wmax, ncol, ring, stride;
+    int32_t* nm;           // optional: NM per job
+    char* md;              // optional: MD string per job, md_stride bytes each
+    int32_t n, qmax, tmax, wmax, ncol, ring, stride, md_stride;
 };
+
+// Appends the decimal digits of v (>= 0) to buf[l ...] while they fit below cap.
+__device__ __forceinline__ bool put_uint(char* buf, int& l, int cap, int v) {
+    char tmp[12];
+    int k = 0;
+    do { tmp[k++] = (char)('0' + v % 10); v /= 10; } while (v);
+    if (l + k >= cap) return false;
+    while (k) buf[l++] = tmp[--k];
+    return true;
+}
 
 __device__ __forceinline__ int32_t sbyte0(uint32_t x) { return (int32_t)(int8_t)(x & 0xFFu); }
 
@@ -62,14 +75,15 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
         if (first >= d.n) break;
         const int job = first + lane;
         int32_t qlen = 0, tlen = 0, w = 0;
-        uint32_t t_off = 0;
+        uint32_t t_off = 0, flags = 0;
         bool trev = false, live = false;
         if (job < d.n) {
             const g3x_job_t jb = d.jobs[job];
-            qlen = jb.qlen; tlen = jb.tlen; w = jb.w;
+            qlen = jb.qlen; tlen = jb.tlen; w = jb.w; flags = jb.flags;
             t_off = jb.t_off; trev = (jb.flags & G3X_JOB_TREV) != 0;
             if (qlen > d.qmax || tlen > d.tmax || w < 0 || w > d.wmax) {
                 d.score[job] = 0; d.n_cigar[job] = 0; d.status[job] = G3X_ERR_TOO_LONG;
+                if (d.nm) { d.nm[job] = 0; d.md[(int64_t)job * d.md_stride] = 0; }
             } else {
                 live = true;
                 stage_own_query(d.codes, d.nmask, jb.q_off, qlen, (jb.flags & G3X_JOB_QREV) != 0,
@@ -163,7 +177,58 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
                 }
             }
             d.n_cigar[job] = full || bad ? 0 : n;
-            d.status[job] = full ? G3X_ERR_TOO_LONG : bad ? G3X_ERR_INTERNAL : G3X_OK;
+            int32_t stj = full ? G3X_ERR_TOO_LONG : bad ? G3X_ERR_INTERNAL : G3X_OK;
+            if (d.nm && stj == G3X_OK) {
+                // NM and MD along the CIGAR (aux.cu:2831-2860): the query from its codes in shared
+                // memory, the target from the planes 16 codes at a time
+                const char* alpha = (flags & 4u) ? "TGCAN" : "ACGTN";
+                char* md = d.md + (int64_t)job * d.md_stride;
+                int x = 0, y = 0, u = 0, n_mm = 0, n_gap = 0, l = 0, cy = -1;
+                uint32_t ty = 0, tyn = 0;
+                bool ok = true;
+                auto qcode = [&](int p) -> uint32_t {
+                    const uint32_t nib = (qn[(p >> 3) * 32 + lane] >> ((p & 7) << 2)) & 0xFu;
+                    return (nib & 4u) ? 4u : nib;
+                };
+                auto tcode = [&](int p) -> uint32_t {
+                    if ((p >> 4) != cy) { cy = p >> 4; load16(d.codes, d.nmask, t_off, tlen, cy, trev, ty, tyn); }
+                    return ((tyn >> (p & 15)) & 1u) ? 4u : (ty >> ((p & 15) << 1)) & 3u;
+                };
+                for (int k = 0; k < n && ok; ++k) {
+                    const int op = (int)(cg[k] & 0xFu), len = (int)(cg[k] >> 4);
+                    if (op == 0) {
+                        for (int i = 0; i < len && ok; ++i) {
+                            const uint32_t tc = tcode(y + i);
+                            if (qcode(x + i) != tc) {
+                                ok = put_uint(md, l, d.md_stride - 1, u);
+                                if (ok && l + 1 < d.md_stride) md[l++] = alpha[tc]; else ok = false;
+                                ++n_mm; u = 0;
+                            } else ++u;
+                        }
+                        x += len; y += len;
+                    } else if (op == 2) {
+                        if (k > 0 && k < n - 1) {
+                            ok = put_uint(md, l, d.md_stride - 1, u);
+                            if (ok && l + 1 < d.md_stride) md[l++] = '^'; else ok = false;
+                            for (int i = 0; i < len && ok; ++i) {
+                                if (l + 1 < d.md_stride) md[l++] = alpha[tcode(y + i)]; else ok = false;
+                            }
+                            u = 0; n_gap += len;
+                        }
+                        y += len;
+                    } else if (op == 1) {
+                        x += len; n_gap += len;
+                    }
+                }
+                ok = ok && put_uint(md, l, d.md_stride - 1, u);
+                md[ok ? l : 0] = 0;
+                d.nm[job] = ok ? n_mm + n_gap : 0;
+                if (!ok) stj = G3X_ERR_TOO_LONG;
+            } else if (d.nm) {
+                d.nm[job] = 0;
+                d.md[(int64_t)job * d.md_stride] = 0;
+            }
+            d.status[job] = stj;
         }
         __syncwarp();
     }
@@ -176,10 +241,12 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
 extern "C" int g3x_ksw_global2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs, int32_t n,
                                      const uint32_t* d_codes, const uint32_t* d_nmask, int32_t max_qlen,
                                      int32_t max_tlen, int32_t max_w, int32_t* d_score, uint32_t* d_cigar,
-                                     int32_t cigar_stride, int32_t* d_n_cigar, int32_t* d_status, void* stream) {
+                                     int32_t cigar_stride, int32_t* d_n_cigar, int32_t* d_nm, char* d_md,
+                                     int32_t md_stride, int32_t* d_status, void* stream) {
     using namespace g3x;
     if (!ctx || !score || n < 0 || max_qlen < 0 || max_tlen < 0 || max_w < 0 || cigar_stride <= 0)
         return G3X_ERR_INVALID;
+    if ((d_nm != nullptr) != (d_md != nullptr) || (d_nm && md_stride < 2)) return G3X_ERR_INVALID;
     if (n == 0) return G3X_OK;
     if (!d_jobs || !d_codes || !d_nmask || !d_score || !d_cigar || !d_n_cigar || !d_status) return G3X_ERR_INVALID;
     ScoreParams sp;
@@ -190,6 +257,7 @@ extern "C" int g3x_ksw_global2_batch(g3x_ctx* ctx, const g3x_score_t* score, con
     GlobalDesc d;
     d.jobs = d_jobs; d.codes = d_codes; d.nmask = d_nmask; d.score = d_score; d.cigar = d_cigar;
     d.n_cigar = d_n_cigar; d.status = d_status; d.n = n;
+    d.nm = d_nm; d.md = d_md; d.md_stride = md_stride;
     d.qmax = std::max(max_qlen, 1); d.tmax = std::max(max_tlen, 1); d.wmax = max_w;
     d.ncol = std::max(1, std::min(d.qmax, 2 * max_w + 1));
     d.ring = ((2 * max_w + 3) + 3) & ~3;

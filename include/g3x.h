@@ -368,13 +368,19 @@ int g3x_pair_generate(const g3x_opt_t *opt, const g3x_refinfo_t *ref, const g3x_
    band reaches the last cell (score <= -2^29) the reference's backtrack reads direction bytes
    it never wrote; here the CIGAR is then empty.  d_status[k]: G3X_OK; G3X_ERR_TOO_LONG for a
    job beyond max_qlen / max_tlen / max_w or whose CIGAR exceeds cigar_stride (empty CIGAR;
-   qlen + tlen + 2 always suffices).  Scratch: max_tlen x min(max_qlen, 2 max_w + 1) bytes per
-   resident warp (at most 8 GiB, fewer warps beyond), allocated in the context for larger
+   qlen + tlen + 2 always suffices).  With d_nm and d_md (both or neither), NM and the MD
+   string follow as the traceback stage computes them after ksw_global2 (bwa/src/aux.cu:2831-2860;
+   bases as "ACGTN", or "TGCAN" for jobs with G3X_JOB_MDRC): d_nm[k], and the NUL-terminated MD
+   at d_md[k * md_stride] (G3X_ERR_TOO_LONG and an empty string when it does not fit;
+   4 (qlen + tlen) + 16 bytes always do).  Scratch: max_tlen x min(max_qlen, 2 max_w + 1) bytes
+   per resident warp (at most 8 GiB, fewer warps beyond), allocated in the context for larger
    calls.  Asynchronous on `stream`. */
+#define G3X_JOB_MDRC 4u   /* MD prints the reverse-strand alphabet "TGCAN" */
 int g3x_ksw_global2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
                           const uint32_t *d_codes, const uint32_t *d_nmask, int32_t max_qlen,
                           int32_t max_tlen, int32_t max_w, int32_t *d_score, uint32_t *d_cigar,
-                          int32_t cigar_stride, int32_t *d_n_cigar, int32_t *d_status, void *stream);
+                          int32_t cigar_stride, int32_t *d_n_cigar, int32_t *d_nm, char *d_md,
+                          int32_t md_stride, int32_t *d_status, void *stream);
 
 /* ---- host-resident batches, pipelined --------------------------------------------------- */
 /* No counterpart in the reference (its batches stay on the device between pipeline stages).

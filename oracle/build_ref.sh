@@ -4,8 +4,8 @@
 # C++, the reference's own band-retry lines of mem_chain2aln (bwa/src/aux.cu:253-255,
 # 258-301, 309), the whole of mem_chain2aln with the window fetch it calls
 # (bwa/src/aux.cu:168-175, 178-315; bwa/src/bntseq.cu:5, 7-87), the banded global alignment
-# with backtrack (bwa/src/ksw.cu:299-301, 548, 694-809), plus the ctypes batch driver
-# ref_wrap.cpp.  The source lines are streamed from the
+# with backtrack (bwa/src/ksw.cu:299-301, 548, 694-809) and the NM/MD block of the traceback
+# stage (bwa/src/aux.cu:2830-2861), plus the ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
 # reference tree into the compiler; no reference source is copied into this repository.
 # Usage: sh oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -eu
@@ -78,7 +78,17 @@ if [ "$K548" != "#define MINUS_INF -0x40000000" ] || [ "$K694" != "__device__ st
 fi
 { cat "$HERE/ref_global_head.inc"; sed -n '299,301p;548p;694,704p;706,809p' "$SRC"; cat "$HERE/ref_global_tail.inc"; } | \
     tr -d '\r' | $CXX -O3 -fPIC -std=c++17 -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/global_ref_fn.o"
+# NM and MD of the traceback stage (aux.cu:2830-2861) inside the host function of
+# ref_nmmd_head.inc / ref_nmmd_tail.inc.
+A2830=$(sed -n '2830p' "$AUX" | tr -d '\r' | sed 's/^ *//')
+A2862=$(sed -n '2862p' "$AUX" | tr -d '\r' | sed 's/^ *//')
+if [ "$A2830" != "int NM;" ] || [ "$A2862" != "// write output" ]; then
+    echo "build_ref.sh: unexpected content at aux.cu:2830/2862; refusing to build" >&2
+    exit 3
+fi
+{ cat "$HERE/ref_nmmd_head.inc"; sed -n '2830,2861p' "$AUX"; cat "$HERE/ref_nmmd_tail.inc"; } | tr -d '\r' | \
+    $CXX -O3 -fPIC -std=c++17 -x c++ -c - -o "$OUT/nmmd_ref_fn.o"
 $CXX -O3 -fPIC -shared -std=c++17 "$HERE/ref_wrap.cpp" "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" \
-    "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" -o "$OUT/libksw_ref.so" -lpthread
-rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o"
+    "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o" -o "$OUT/libksw_ref.so" -lpthread
+rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o"
 echo "built $OUT/libksw_ref.so"

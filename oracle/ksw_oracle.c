@@ -22,6 +22,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <pthread.h>
+#include <stdio.h>
 
 typedef struct { int32_t h, e; } g3o_eh;          /* ksw.cu:299-301 */
 
@@ -665,4 +666,52 @@ void g3o_global_batch(const g3o_job *jobs, int64_t n, const uint8_t *codes, cons
                                    cells ? cells + k : NULL);
         n_cigar[k] = nc;
     }
+}
+
+/* NM and MD of a global alignment, as the traceback stage computes them after ksw_global2
+   (aux.cu:2831-2860): along the CIGAR, a mismatch in an M run adds to NM and writes the run of
+   matches before it and the target base; a D that is neither the first nor the last operation
+   writes the matches before it, '^' and the deleted target bases, and adds its length to NM;
+   an I adds its length to NM only.  Bases print as "ACGTN", or "TGCAN" when rc.  md gets the
+   NUL-terminated string (room for 4 * (qlen + tlen) + 16 bytes); returns NM. */
+int g3o_nm_md(const uint32_t *cigar, int n_cigar, const uint8_t *query, const uint8_t *target, int rc,
+              char *md)
+{
+    const char *base = rc ? "TGCAN" : "ACGTN";
+    int x = 0, y = 0, u = 0, n_mm = 0, n_gap = 0, l = 0;
+    for (int k = 0; k < n_cigar; ++k) {
+        const int op = cigar[k] & 0xf, len = (int)(cigar[k] >> 4);
+        if (op == 0) {
+            for (int i = 0; i < len; ++i) {
+                if (query[x + i] != target[y + i]) {
+                    l += sprintf(md + l, "%d", u);
+                    md[l++] = base[target[y + i]];
+                    ++n_mm; u = 0;
+                } else ++u;
+            }
+            x += len; y += len;
+        } else if (op == 2) {
+            if (k > 0 && k < n_cigar - 1) {
+                l += sprintf(md + l, "%d", u);
+                md[l++] = '^';
+                for (int i = 0; i < len; ++i) md[l++] = base[target[y + i]];
+                u = 0; n_gap += len;
+            }
+            y += len;
+        } else if (op == 1) {
+            x += len; n_gap += len;
+        }
+    }
+    l += sprintf(md + l, "%d", u);
+    md[l] = 0;
+    return n_mm + n_gap;
+}
+
+/* NM and MD for every job of a global batch (flags bit 2 = the "TGCAN" alphabet). */
+void g3o_nm_md_batch(const g3o_job *jobs, int64_t n, const uint8_t *codes, const uint32_t *cigar,
+                     int32_t stride, const int32_t *n_cigar, int32_t *nm, char *md, int32_t md_stride)
+{
+    for (int64_t k = 0; k < n; ++k)
+        nm[k] = g3o_nm_md(cigar + (size_t)k * stride, n_cigar[k], codes + jobs[k].q_off, codes + jobs[k].t_off,
+                          (jobs[k].flags & 4) != 0, md + (size_t)k * md_stride);
 }

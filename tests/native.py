@@ -46,6 +46,8 @@ def oracle():
         _oracle.g3o_chain2aln_reads.restype = None
         _oracle.g3o_global_batch.argtypes = [P, I64, P, P, P, P, ctypes.c_int32, P, P]
         _oracle.g3o_global_batch.restype = None
+        _oracle.g3o_nm_md_batch.argtypes = [P, I64, P, P, ctypes.c_int32, P, P, P, ctypes.c_int32]
+        _oracle.g3o_nm_md_batch.restype = None
     return _oracle
 
 
@@ -64,6 +66,8 @@ def ref():
         _ref.g3r_chain2aln_reads.restype = ctypes.c_int
         _ref.g3r_global_batch.argtypes = [P, I64, P, P, P, P, ctypes.c_int32, P]
         _ref.g3r_global_batch.restype = ctypes.c_int
+        _ref.g3r_nm_md_batch.argtypes = [P, I64, P, P, ctypes.c_int32, P, P, P, ctypes.c_int32]
+        _ref.g3r_nm_md_batch.restype = ctypes.c_int
     return _ref
 
 
@@ -263,3 +267,23 @@ def oracle_global(jobs, u8, score, stride):
 def ref_global(jobs, u8, score, stride):
     """(score, cigar, n_cigar) from the reference's own ksw_global2."""
     return _global(ref().g3r_global_batch, jobs, u8, score, stride, False)[:3]
+
+
+def _nm_md(fn, jobs, u8, cigar, n_cigar, md_stride):
+    n = len(jobs)
+    nm = np.zeros(n, np.int32)
+    md = np.zeros((max(n, 1), md_stride), np.uint8)
+    cig = np.ascontiguousarray(cigar, np.uint32)
+    fn(np.ascontiguousarray(jobs).ctypes.data, n, np.ascontiguousarray(u8).ctypes.data, cig.ctypes.data,
+       cig.shape[1], np.ascontiguousarray(n_cigar, np.int32).ctypes.data, nm.ctypes.data, md.ctypes.data, md_stride)
+    return nm, [bytes(md[k]).split(b"\0")[0].decode() for k in range(n)]
+
+
+def oracle_nm_md(jobs, u8, cigar, n_cigar, md_stride):
+    """(NM, MD strings) from the C restatement of the traceback stage's NM/MD block."""
+    return _nm_md(oracle().g3o_nm_md_batch, jobs, u8, cigar, n_cigar, md_stride)
+
+
+def ref_nm_md(jobs, u8, cigar, n_cigar, md_stride):
+    """(NM, MD strings) from the reference's own NM/MD block (aux.cu:2830-2861)."""
+    return _nm_md(ref().g3r_nm_md_batch, jobs, u8, cigar, n_cigar, md_stride)

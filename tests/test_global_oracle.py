@@ -29,3 +29,18 @@ def test_oracle_global_equals_reference(seed):
         ops = c1[k, :n1[k]]
         ln, op = ops >> 4, ops & 0xF
         assert ln[op != 2].sum() == jobs["qlen"][k] and ln[op != 1].sum() == jobs["tlen"][k]
+
+
+@pytest.mark.skipif(not nat.have_ref(), reason="oracle/_ref not built (no reference tree)")
+@pytest.mark.parametrize("seed", [4, 5])
+def test_oracle_nm_md_equals_reference(seed):
+    jobs, u8 = nat.global_jobs(2000, seed)
+    jobs["flags"][::3] = 4                      # the reverse-strand alphabet on a third of them
+    stride = int((jobs["qlen"] + jobs["tlen"]).max()) + 2
+    s, c, n, _ = nat.oracle_global(jobs, u8, g.default_score(), stride)
+    md_stride = 4 * stride + 16
+    nm1, md1 = nat.oracle_nm_md(jobs, u8, c, n, md_stride)
+    nm2, md2 = nat.ref_nm_md(jobs, u8, c, n, md_stride)
+    assert np.array_equal(nm1, nm2)
+    assert md1 == md2
+    assert any("^" in m for m in md1) and any(set("TGCA") & set(m) for m in md1) and (nm1 > 0).any()

@@ -80,3 +80,34 @@ def test_gpu_global_limits():
     assert (st[fits] == 0).all() and np.array_equal(s2[fits], s1[fits]) and np.array_equal(n2[fits], n1[fits])
     long_ = ~over & (n1 > stride)
     assert long_.any() and (st[long_] == g.G3X_ERR_TOO_LONG).all() and (n2[long_] == 0).all()
+
+
+def test_gpu_global_nm_md():
+    """NM and MD (the traceback stage's block after ksw_global2) equal the oracle's, itself
+    pinned to the reference's own block (tests/test_global_oracle.py)."""
+    import torch
+    cj, u8 = nat.global_jobs(3000, 21, max_len=200)
+    cj["flags"][::3] = g.JOB_MDRC
+    jobs = gpu_jobs(cj)
+    jobs["flags"] = cj["flags"]
+    n = len(cj)
+    stride = int((cj["qlen"] + cj["tlen"]).max()) + 2
+    md_stride = 4 * stride + 16
+    s1, c1, n1, _ = nat.oracle_global(cj, u8, g.default_score(), stride)
+    nm1, md1 = nat.oracle_nm_md(cj, u8, c1, n1, md_stride)
+    codes, nmask = g.pack_planes(u8)
+    d_score = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d_cig = torch.zeros(n * stride, dtype=torch.int32, device="cuda")
+    d_nc = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d_st = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+    d_nm = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    d_md = torch.zeros(n * md_stride, dtype=torch.uint8, device="cuda")
+    ctx().global_batch(g.default_score(), to_dev(jobs), n, to_dev(codes), to_dev(nmask), int(cj["qlen"].max()),
+                       int(cj["tlen"].max()), int(cj["w"].max()), d_score, d_cig, stride, d_nc, d_st,
+                       d_nm=d_nm, d_md=d_md, md_stride=md_stride)
+    torch.cuda.synchronize()
+    assert (d_st.cpu().numpy() == 0).all()
+    assert np.array_equal(d_nm.cpu().numpy(), nm1)
+    md = d_md.cpu().numpy().reshape(n, md_stride)
+    md2 = [bytes(md[k]).split(b"\0")[0].decode() for k in range(n)]
+    assert md2 == md1
