@@ -529,16 +529,17 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
     base.jobs = d_jobs; base.codes = d_codes; base.nmask = d_nmask; base.out = out; base.status = status;
     base.n = n; base.qmax = max_qlen; base.tmax = max_tlen;
     cudaStream_t st = nullptr;
-    // Class widths follow the batch: up to seven classes at max_qlen * ((k + 0.5) / 7.5)^2,
+    // Class widths follow the batch: up to seven classes at max_qlen times the fractions below,
     // rounded up to eight columns, then the unbounded class.  A class's shared memory per job is
-    // sized by its width, so the steps grow with the width (8k(k+1)-like for max_qlen 231:
-    // 16, 32, 56, 88, 128, 176, 232, the fastest of the layouts measured on the benchmark batch).
+    // sized by its width: the steps grow at the low end, where rows are short and few cells lie,
+    // and stay dense at the top, where shared memory bounds the resident warps (for max_qlen 231:
+    // 32, 56, 88, 128, 168, 200, 232, the fastest of the layouts measured on the benchmark batch).
     {
+        static const double kFrac[7] = {0.138, 0.241, 0.379, 0.552, 0.724, 0.862, 1.0};
         g3x::TileTable t;
         t.n = 0;
         for (int k = 1; k <= 7; ++k) {
-            const double f = (k + 0.5) / 7.5;
-            int wk = (int)(max_qlen * f * f + 0.999);
+            int wk = (int)(max_qlen * kFrac[k - 1] + 0.999);
             wk = std::max(8, (wk + 7) & ~7);
             if (t.n && wk <= t.width[t.n - 1]) continue;
             t.width[t.n] = wk;

@@ -166,7 +166,8 @@ typedef struct {
 int g3x_get_tiles(g3x_ctx *ctx, g3x_tile_t *h_tiles, int32_t *n);
 int g3x_set_tiles(g3x_ctx *ctx, const g3x_tile_t *h_tiles, int32_t n);
 /* Fits the width classes to the given jobs (device buffers) and tunes them: the class widths
-   become max_qlen * ((k + 0.5) / 7.5)^2 for k = 1..7 (rounded up to 8 columns, duplicates dropped) plus
+   become max_qlen x (0.138, 0.241, 0.379, 0.552, 0.724, 0.862, 1) (rounded up to 8 columns,
+   duplicates dropped) plus
    the unbounded class; then every candidate configuration of each class is timed on the class's
    jobs and the fastest kept in the context; h_tiles/n receive the table.  Blocks.  Outputs of
    the trial runs are discarded. */
