@@ -360,9 +360,11 @@ def run_global_workload(args, ws, rank):
     sc = g.default_score()
     s_o, c_o, n_o, cells_o = nat.oracle_global(cj, u8, sc, stride)
     cells = int(cells_o.sum())
+    # the GPU's CIGAR slots hold the longest CIGAR of the batch (a caller sizes them likewise)
+    gstride = int(n_o.max()) + 2
     threads = os.cpu_count() or 1
     metric = "ksw_global2 GCUPS & alignments/s on 1 B200, bit-exact"
-    cfg = {"workload": GLOBAL_DESC, "jobs": n, "cells": cells}
+    cfg = {"workload": GLOBAL_DESC, "jobs": n, "cells": cells, "cigar_slots": int(n_o.max()) + 2}
 
     def ref_time():
         bounds = np.linspace(0, n, threads + 1).astype(np.int64)
@@ -415,7 +417,7 @@ def run_global_workload(args, ws, rank):
             for k, v in (("jobs", jobs), ("codes", codes), ("nmask", nmask))}
     d = {k: v.to(dev) for k, v in host.items()}
     d_score = torch.zeros(n, dtype=torch.int32, device=dev)
-    d_cig = torch.zeros(n * stride, dtype=torch.int32, device=dev)
+    d_cig = torch.zeros(n * gstride, dtype=torch.int32, device=dev)
     d_nc = torch.zeros(n, dtype=torch.int32, device=dev)
     d_st = torch.zeros(n, dtype=torch.int32, device=dev)
     h_out = [torch.zeros_like(x, device="cpu").pin_memory() for x in (d_score, d_cig, d_nc, d_st)]
@@ -425,12 +427,12 @@ def run_global_workload(args, ws, rank):
     mq, mt, mw = int(cj["qlen"].max()), int(cj["tlen"].max()), int(cj["w"].max())
 
     def call():
-        ctx.global_batch(sc, d["jobs"], n, d["codes"], d["nmask"], mq, mt, mw, d_score, d_cig, stride, d_nc, d_st,
+        ctx.global_batch(sc, d["jobs"], n, d["codes"], d["nmask"], mq, mt, mw, d_score, d_cig, gstride, d_nc, d_st,
                          stream=stream)
 
     call()
     torch.cuda.synchronize()
-    cig = d_cig.cpu().numpy().view(np.uint32).reshape(n, stride)
+    cig = d_cig.cpu().numpy().view(np.uint32).reshape(n, gstride)
     nc = d_nc.cpu().numpy()
     exact = bool((d_st == 0).all()) and np.array_equal(d_score.cpu().numpy(), s_o) and np.array_equal(nc, n_o) and \
         all(np.array_equal(cig[k, :nc[k]], c_o[k, :n_o[k]]) for k in range(n))

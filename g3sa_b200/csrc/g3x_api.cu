@@ -31,6 +31,21 @@ int ctx_device(const g3x_ctx* ctx) { return ctx->device; }
 ChainScratch& ctx_chain(g3x_ctx* ctx) { return ctx->chain; }
 GlobalScratch& ctx_global(g3x_ctx* ctx) { return ctx->global; }
 
+static int alloc_sched(SchedScratch& s, int64_t n);
+
+// The jobs in decreasing order of row count, then of widest row (the counting sort of the
+// scheduled batches with one class), so that the jobs a warp takes together are alike.
+int cost_order(g3x_ctx* ctx, const g3x_job_t* jobs, int n, const ScoreParams& sp, cudaStream_t st,
+               const int32_t** order) {
+    int rc = alloc_sched(ctx->sched, n);
+    if (rc) return rc;
+    TileTable t;
+    t.n = 1; t.width[0] = 0x7FFFFFFF; t.lanes[0] = 32; t.tile[0] = 9; t.warp_batch[0] = 0; t.refill[0] = 1;
+    if ((rc = schedule_jobs(ctx->sched, jobs, n, sp, nullptr, t, st))) return rc;
+    *order = ctx->sched.order;
+    return G3X_OK;
+}
+
 int score_params(const g3x_score_t* s, ScoreParams* sp) {
     if (!s) return G3X_ERR_INVALID;
     if (s->m != 5 || s->e_del <= 0 || s->e_ins <= 0 || s->o_del < 0 || s->o_ins < 0)

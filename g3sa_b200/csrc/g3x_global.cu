@@ -1,8 +1,9 @@
 // g3x_global.cu -- banded global alignment with backtrack (ksw_global2, bwa/src/ksw.cu:706-809)
 // for batches of alignments on the GPU.
 //
-// One job per lane.  A warp takes 32 jobs at a time and runs their target rows together
-// (row i of every job in the same step); in a row each lane walks its own band
+// One job per lane.  The jobs are first ordered by decreasing row count and row width (the
+// scheduler's counting sort); a warp takes 32 consecutive ones and runs their target rows
+// together (row i of every job in the same step); in a row each lane walks its own band
 // [max(i-w, 0), min(i+w+1, qlen)) column by column (the reference's scalar recurrence, in int32
 // with -2^30 outside the band, ksw.cu:548).  The band has a fixed width and never trims, so the
 // row buffer of H(i-1, j-1) and E(i, j) (ksw.cu:299-301) is a ring of R >= 2w+3 columns per lane
@@ -37,6 +38,7 @@ struct GlobalDesc {
     uint8_t* z;            // direction bytes: per warp slot zwarp bytes
     int64_t zwarp;
     int32_t* queue;
+    const int32_t* order;  // queue slot -> job, jobs alike in row count and width together
     int32_t* nm;           // optional: NM per job
     char* md;              // optional: MD string per job, md_stride bytes each
     int32_t n, qmax, tmax, wmax, ncol, ring, stride, md_stride;
@@ -73,7 +75,7 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
         if (lane == 0) first = atomicAdd(d.queue, 32);
         first = __shfl_sync(0xFFFFFFFFu, first, 0);
         if (first >= d.n) break;
-        const int job = first + lane;
+        const int job = first + lane < d.n ? d.order[first + lane] : d.n;
         int32_t qlen = 0, tlen = 0, w = 0;
         uint32_t t_off = 0, flags = 0;
         bool trev = false, live = false;
@@ -290,6 +292,7 @@ extern "C" int g3x_ksw_global2_batch(g3x_ctx* ctx, const g3x_score_t* score, con
     d.z = gs.z;
     d.queue = gs.queue;
     const cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = cost_order(ctx, d_jobs, n, sp, st, &d.order))) return rc;
     if (cudaMemsetAsync(gs.queue, 0, sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
     global_kernel<<<blocks, 32 * wpb, wpb * warp_smem, st>>>(d, sp);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;

@@ -160,6 +160,9 @@ struct GlobalScratch {
     int64_t bytes = 0;
 };
 GlobalScratch& ctx_global(g3x_ctx* ctx);
+// The context's job order by decreasing row count and row width (its scheduling scratch).
+int cost_order(g3x_ctx* ctx, const g3x_job_t* jobs, int n, const ScoreParams& sp, cudaStream_t st,
+               const int32_t** order);
 void free_chain_scratch(ChainScratch& w);
 
 // Learned cost model state (device buffers; g3x_model.cu).

@@ -375,7 +375,8 @@ int g3x_pair_generate(const g3x_opt_t *opt, const g3x_refinfo_t *ref, const g3x_
    at d_md[k * md_stride] (G3X_ERR_TOO_LONG and an empty string when it does not fit;
    4 (qlen + tlen) + 16 bytes always do).  Scratch: max_tlen x min(max_qlen, 2 max_w + 1) bytes
    per resident warp (at most 8 GiB, fewer warps beyond), allocated in the context for larger
-   calls.  Asynchronous on `stream`. */
+   calls; the jobs are ordered by size with the context's scheduling scratch, so calls on one
+   context belong on one stream.  Asynchronous on `stream`. */
 #define G3X_JOB_MDRC 4u   /* MD prints the reverse-strand alphabet "TGCAN" */
 int g3x_ksw_global2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
                           const uint32_t *d_codes, const uint32_t *d_nmask, int32_t max_qlen,
