@@ -5,7 +5,9 @@
 # 258-301, 309), the whole of mem_chain2aln with the window fetch it calls
 # (bwa/src/aux.cu:168-175, 178-315; bwa/src/bntseq.cu:5, 7-87), the banded global alignment
 # with backtrack (bwa/src/ksw.cu:299-301, 548, 694-809) and the NM/MD block of the traceback
-# stage (bwa/src/aux.cu:2830-2861), plus the ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
+# stage (bwa/src/aux.cu:2830-2861), the striped local alignment ksw_align2 with ksw_qinit and
+# ksw_i16 (bwa/src/ksw.cu:5, 18-292 less its trap line 276; bwa/src/ksw.h:7-29), plus the
+# ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
 # reference tree into the compiler; no reference source is copied into this repository.
 # Usage: sh oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -eu
@@ -88,7 +90,29 @@ if [ "$A2830" != "int NM;" ] || [ "$A2862" != "// write output" ]; then
 fi
 { cat "$HERE/ref_nmmd_head.inc"; sed -n '2830,2861p' "$AUX"; cat "$HERE/ref_nmmd_tail.inc"; } | tr -d '\r' | \
     $CXX -O3 -fPIC -std=c++17 -x c++ -c - -o "$OUT/nmmd_ref_fn.o"
+# Striped local alignment: ksw.h:7-29 (flags and types), ksw.cu:5 (g_defr), 18-275 and 277-292
+# (ksw_qinit, the m128i helpers, ksw_i16, revseq, ksw_align2 without its trap line 276) between
+# ref_sw_head.inc and ref_sw_tail.inc.
+KSWH="$REF/bwa/src/ksw.h"
+K5=$(sed -n '5p' "$SRC" | tr -d '\r' | cut -c1-32)
+K18=$(sed -n '18p' "$SRC" | tr -d '\r' | cut -c1-35)
+K155=$(sed -n '155p' "$SRC" | tr -d '\r' | cut -c1-33)
+K271=$(sed -n '271p' "$SRC" | tr -d '\r' | cut -c1-29)
+K276=$(sed -n '276p' "$SRC" | tr -d '\r')
+K292=$(sed -n '292p' "$SRC" | tr -d '\r')
+H7=$(sed -n '7p' "$KSWH" | tr -d '\r' | cut -c1-17)
+H29=$(sed -n '29p' "$KSWH" | tr -d '\r')
+if [ "$K5" != "__device__ const kswr_t g_defr =" ] || [ "$K18" != "static __device__ kswq_t* ksw_qinit" ] || \
+   [ "$K155" != "static __device__ kswr_t ksw_i16(" ] || [ "$K271" != "__device__ kswr_t ksw_align2(" ] || \
+   [ "$K276" != 'printf("this part of code for long reads is under development \n"); __trap();' ] || \
+   [ "$K292" != "}" ] || [ "$H7" != "#define KSW_XBYTE" ] || [ "$H29" != "} kswr_t;" ]; then
+    echo "build_ref.sh: unexpected content at ksw.cu:5/18/155/271/276/292 or ksw.h:7/29; refusing to build" >&2
+    exit 3
+fi
+{ cat "$HERE/ref_sw_head.inc"; sed -n '7,29p' "$KSWH"; sed -n '5p;18,275p;277,292p' "$SRC"; cat "$HERE/ref_sw_tail.inc"; } | \
+    tr -d '\r' | $CXX -O3 -fPIC -std=c++17 -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/sw_ref_fn.o"
 $CXX -O3 -fPIC -shared -std=c++17 "$HERE/ref_wrap.cpp" "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" \
-    "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o" -o "$OUT/libksw_ref.so" -lpthread
-rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o"
+    "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o" "$OUT/sw_ref_fn.o" -o "$OUT/libksw_ref.so" -lpthread
+rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o" \
+    "$OUT/sw_ref_fn.o"
 echo "built $OUT/libksw_ref.so"

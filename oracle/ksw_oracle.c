@@ -715,3 +715,171 @@ void g3o_nm_md_batch(const g3o_job *jobs, int64_t n, const uint8_t *codes, const
         nm[k] = g3o_nm_md(cigar + (size_t)k * stride, n_cigar[k], codes + jobs[k].q_off, codes + jobs[k].t_off,
                           (jobs[k].flags & 4) != 0, md + (size_t)k * md_stride);
 }
+
+/* ---------------------------------------------------------------------------------- */
+/* Striped local Smith-Waterman with 16-bit cells: ksw_align2 (ksw.cu:271-292) over the  */
+/* query profile of ksw_qinit (ksw.cu:18-64, two-byte cells) and the pass of ksw_i16     */
+/* (ksw.cu:155-262).  The reference stops ksw_align2 at its first line (ksw.cu:276); this */
+/* restates the function as written after that line.                                    */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct { int32_t score, te, qe, score2, te2, tb, qb; } g3o_swr;   /* kswr_t, ksw.h:24-29 */
+#define G3O_XSTOP  0x20000
+#define G3O_XSUBO  0x40000
+#define G3O_XSTART 0x80000
+
+/* The vector helpers of ksw.cu:66-153 act on eight int16 lanes: a plain add whose int result
+   is stored back into int16 (wraps), a signed max, and "subtract, 0 if not positive" computed in
+   int before the store. */
+static int16_t g3o_sub0(int16_t a, int16_t b) { const int v = (int)a - (int)b; return (int16_t)(v > 0 ? v : 0); }
+
+/* One pass of ksw_i16.  Lane k of vector j of the striped profile holds query position
+   j + k * slen (score 0 past the query); the row loop, the lazy-F loop of at most 16 rounds
+   that leaves E alone, the per-row maximum, the list of row maxima at or above minsc
+   (XSUBO) and the stop at endsc (XSTOP) follow ksw.cu:190-239; the end position on the query
+   is the smallest position holding the best row's maximum (the scan of ksw.cu:244-248 reads
+   the cells as uint16), the second best score comes from the list entries more than
+   ceil(score / max(mat)) rows away from te (ksw.cu:249-256). */
+static g3o_swr g3o_sw16_pass(int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                             const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins, int xtra,
+                             int64_t *cells)
+{
+    g3o_swr r = { 0, -1, -1, -1, -1, -1, -1 };               /* g_defr, ksw.cu:5 */
+    const int slen = (qlen + 7) / 8, np = slen * 8;
+    int16_t *prof = (int16_t *)malloc(sizeof(int16_t) * 5 * (size_t)(np > 0 ? np : 1));
+    int16_t *H0 = (int16_t *)calloc((size_t)np + 8, sizeof(int16_t));
+    int16_t *H1 = (int16_t *)calloc((size_t)np + 8, sizeof(int16_t));
+    int16_t *E = (int16_t *)calloc((size_t)np + 8, sizeof(int16_t));
+    int16_t *Hmax = (int16_t *)calloc((size_t)np + 8, sizeof(int16_t));
+    uint64_t *b = NULL;
+    int n_b = 0, m_b = 0, gmax = 0, te = -1, maxmat = 0;
+    const int minsc = (xtra & G3O_XSUBO) ? xtra & 0xffff : 0x10000;
+    const int endsc = (xtra & G3O_XSTOP) ? xtra & 0xffff : 0x10000;
+    const int16_t oed = (int16_t)(o_del + e_del), ed = (int16_t)e_del;
+    const int16_t oei = (int16_t)(o_ins + e_ins), ei = (int16_t)e_ins;
+    for (int k = 0; k < 25; ++k) if (mat[k] > maxmat) maxmat = mat[k];
+    for (int a = 0; a < 5; ++a)
+        for (int j = 0; j < slen; ++j)
+            for (int k = 0; k < 8; ++k) {
+                const int pos = j + k * slen;
+                prof[((size_t)a * slen + j) * 8 + k] = pos < qlen ? mat[a * 5 + query[pos]] : 0;
+            }
+    int64_t nc = 0;
+    for (int i = 0; i < tlen; ++i) {
+        const int16_t *S = prof + (size_t)target[i] * slen * 8;
+        int16_t h[8], f[8], mx[8];
+        for (int k = 0; k < 8; ++k) {                        /* the last vector moved up a lane */
+            h[k] = k == 0 || slen == 0 ? 0 : H0[(size_t)(slen - 1) * 8 + k - 1];
+            f[k] = 0; mx[k] = 0;
+        }
+        for (int j = 0; j < slen; ++j) {
+            for (int k = 0; k < 8; ++k) {
+                const size_t at = (size_t)j * 8 + k;
+                int16_t v = (int16_t)(h[k] + S[at]);
+                if (E[at] > v) v = E[at];
+                if (f[k] > v) v = f[k];
+                if (v > mx[k]) mx[k] = v;
+                H1[at] = v;
+                int16_t e = g3o_sub0(E[at], ed), t = g3o_sub0(v, oed);
+                E[at] = e > t ? e : t;
+                f[k] = g3o_sub0(f[k], ei); t = g3o_sub0(v, oei);
+                if (t > f[k]) f[k] = t;
+                h[k] = H0[at];
+            }
+        }
+        nc += qlen;
+        for (int round = 0; round < 16; ++round) {          /* lazy F */
+            for (int k = 7; k > 0; --k) f[k] = f[k - 1];
+            f[0] = 0;
+            for (int j = 0; j < slen; ++j) {
+                int any = 0;
+                for (int k = 0; k < 8; ++k) {
+                    const size_t at = (size_t)j * 8 + k;
+                    int16_t v = H1[at] > f[k] ? H1[at] : f[k];
+                    H1[at] = v;
+                    v = g3o_sub0(v, oei);
+                    f[k] = g3o_sub0(f[k], ei);
+                    any |= f[k] > v;
+                }
+                if (!any) goto lazy_done;
+            }
+        }
+lazy_done:;
+        int imax = mx[0];
+        for (int k = 1; k < 8; ++k) if (mx[k] > imax) imax = mx[k];
+        if (imax >= minsc) {
+            if (n_b == 0 || (int32_t)b[n_b - 1] + 1 != i) {
+                if (n_b == m_b) {
+                    m_b = m_b ? m_b << 1 : 8;
+                    b = (uint64_t *)realloc(b, 8 * (size_t)m_b);
+                }
+                b[n_b++] = (uint64_t)imax << 32 | (uint32_t)i;
+            } else if ((int)(b[n_b - 1] >> 32) < imax) {
+                b[n_b - 1] = (uint64_t)imax << 32 | (uint32_t)i;
+            }
+        }
+        if (imax > gmax) {
+            gmax = imax; te = i;
+            memcpy(Hmax, H1, sizeof(int16_t) * (size_t)np);
+            if (gmax >= endsc) break;
+        }
+        int16_t *sw = H0; H0 = H1; H1 = sw;
+    }
+    r.score = gmax; r.te = te;
+    int best = -1;
+    for (int x = 0; x < np; ++x) {
+        const int v = (uint16_t)Hmax[x], pos = x / 8 + x % 8 * slen;
+        if (v > best) { best = v; r.qe = pos; }
+        else if (v == best && pos < r.qe) r.qe = pos;
+    }
+    if (n_b > 0) {
+        const int c = (r.score + maxmat - 1) / maxmat, low = te - c, high = te + c;
+        for (int x = 0; x < n_b; ++x) {
+            const int e = (int32_t)b[x];
+            if ((e < low || e > high) && (int)(b[x] >> 32) > r.score2) { r.score2 = (int)(b[x] >> 32); r.te2 = e; }
+        }
+    }
+    free(prof); free(H0); free(H1); free(E); free(Hmax); free(b);
+    if (cells) *cells += nc;
+    return r;
+}
+
+/* ksw_align2 with 16-bit cells (ksw.cu:271-292): the forward pass; with XSTART (and, under
+   XSUBO, a score reaching xtra & 0xffff) a second pass over the query prefix 0..qe and the
+   target with its prefix 0..te reversed, stopping at the first score, gives the start
+   positions when it finds the same score.  qlen >= 1; *cells (may be NULL) receives the cells
+   of both passes (query length x target rows entered, padding lanes not counted). */
+g3o_swr g3o_ksw_align2(int qlen, const uint8_t *query, int tlen, const uint8_t *target, const int8_t *mat,
+                       int o_del, int e_del, int o_ins, int e_ins, int xtra, int64_t *cells)
+{
+    int64_t nc = 0;
+    g3o_swr r = g3o_sw16_pass(qlen, query, tlen, target, mat, o_del, e_del, o_ins, e_ins, xtra, &nc);
+    if ((xtra & G3O_XSTART) && !((xtra & G3O_XSUBO) && r.score < (xtra & 0xffff))) {
+        const int lq = r.qe + 1, lt = r.te + 1;
+        uint8_t *rq = (uint8_t *)malloc((size_t)lq + 1), *rt = (uint8_t *)malloc((size_t)tlen + 1);
+        for (int k = 0; k < lq; ++k) rq[k] = query[lq - 1 - k];
+        for (int k = 0; k < tlen; ++k) rt[k] = k < lt ? target[lt - 1 - k] : target[k];
+        const g3o_swr rr = g3o_sw16_pass(lq, rq, tlen, rt, mat, o_del, e_del, o_ins, e_ins,
+                                         G3O_XSTOP | r.score, &nc);
+        if (r.score == rr.score) { r.tb = r.te - rr.te; r.qb = r.qe - rr.qe; }
+        free(rq); free(rt);
+    }
+    if (cells) *cells = nc;
+    return r;
+}
+
+/* n local alignments over one code buffer (jobs as g3o_job: G3O_QREV / G3O_TREV read the
+   sequence backwards; h0 and w unused), one xtra for all. */
+void g3o_sw_batch(const g3o_job *jobs, int64_t n, const uint8_t *codes, const g3o_score *sc, int xtra,
+                  g3o_swr *out, int64_t *cells)
+{
+    for (int64_t k = 0; k < n; ++k) {
+        const g3o_job *jb = &jobs[k];
+        uint8_t *qb = NULL, *tb = NULL;
+        const uint8_t *q = g3o_view(codes + jb->q_off, jb->qlen, jb->flags & G3O_QREV, &qb);
+        const uint8_t *t = g3o_view(codes + jb->t_off, jb->tlen, jb->flags & G3O_TREV, &tb);
+        out[k] = g3o_ksw_align2(jb->qlen, q, jb->tlen, t, sc->mat, sc->o_del, sc->e_del, sc->o_ins, sc->e_ins,
+                                xtra, cells ? cells + k : NULL);
+        free(qb); free(tb);
+    }
+}

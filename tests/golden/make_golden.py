@@ -13,6 +13,10 @@ Inputs are seeded synthetic jobs (g3sa_b200.synth) plus hand-built edge cases.
 Files:
     jobs_<name>.npz   u8 (one byte per base), jobs (JOB_DT), score (SCORE_DT), ext (n x 6)
     seeds_<name>.npz  u8, seeds (SEED_DT), opt (CPU_OPT_DT), reg (CPU_REG_DT)
+    sw_<name>.npz     u8, jobs (JOB_DT), score, xtras (flag sets), out (flag sets x n kswr_t)
+                      from the reference's own ksw_align2 (its trap line left out)
+
+`python tests/golden/make_golden.py --sw` rewrites the sw_ files only.
 """
 import ctypes
 import os
@@ -138,6 +142,74 @@ def save_seeds(name, wl, opt):
     print(f"seeds_{name}: {len(wl.seeds)} seeds")
 
 
+SW_XTRAS = (0, nat.KSW_XSTART, nat.KSW_XSUBO | 20, nat.KSW_XSTART | nat.KSW_XSUBO | 30, nat.KSW_XSTOP | 15,
+            nat.KSW_XSUBO, nat.KSW_XSTART | nat.KSW_XSUBO | 400)
+
+
+def sw_edge_jobs(rng):
+    """Edge cases of the striped local alignment: one-base queries, empty and one-base targets,
+    all-N queries, identical pairs, query lengths on the 8-lane segment boundaries up to 256,
+    long targets, tandem repeats (ties for the end position), several copies of the query in
+    one target (second-best scores), sequences stored backwards."""
+    b = JobBuilder()
+    rnd = lambda n: rng.integers(0, 4, n).astype(np.uint8)  # noqa: E731
+    for t in ([], [0], [1], [4], list(rnd(30)), list(rnd(300))):
+        b.add([0], t, 0, 0)
+    b.add(rnd(5), [], 0, 0)
+    b.add([4] * 20, rnd(60), 0, 0)
+    b.add(rnd(40), [4] * 40, 0, 0)
+    for ql in (100, 199, 256):
+        q = rnd(ql)
+        b.add(q, q, 0, 0)
+    for ql in (7, 8, 9, 15, 16, 17, 63, 64, 65, 127, 128, 129, 200, 255, 256):
+        q = rnd(ql)
+        t = np.concatenate([rnd(int(rng.integers(0, 40))), nat._mutate(rng, q, 0.05), rnd(int(rng.integers(0, 40)))])
+        b.add(q, t, 0, 0)
+    q = rnd(150)
+    b.add(q, np.concatenate([rnd(1200), q, rnd(1500)]), 0, 0)
+    rep = np.tile(np.array([0, 1, 2, 3], np.uint8), 30)
+    b.add(rep, np.tile(np.array([0, 1, 2, 3], np.uint8), 45), 0, 0)
+    b.add(np.tile(np.array([2, 2, 1], np.uint8), 20), np.tile(np.array([2, 1], np.uint8), 50), 0, 0)
+    for _ in range(6):
+        q = rnd(int(rng.integers(20, 90)))
+        parts = []
+        for _c in range(int(rng.integers(2, 5))):
+            parts += [rnd(int(rng.integers(5, 200))), nat._mutate(rng, q, rng.random() * 0.2)]
+        b.add(q, np.concatenate(parts + [rnd(30)]), 0, 0)
+    for _ in range(6):
+        q = rnd(int(rng.integers(30, 180)))
+        t = np.concatenate([rnd(20), nat._mutate(rng, q, 0.05), rnd(20)])
+        b.add(q[::-1].copy(), t[::-1].copy(), 0, 0, flags=3)
+        b.add(q[::-1].copy(), t, 0, 0, flags=1)
+    return b
+
+
+def save_sw(name, u8, jobs, score):
+    cj = nat.cpu_jobs(jobs)
+    out = np.stack([nat.ref_sw(cj, u8, score, x) for x in SW_XTRAS]) if len(jobs) else np.zeros((0,), nat.SWR_DT)
+    np.savez_compressed(os.path.join(HERE, f"sw_{name}.npz"), u8=u8, jobs=jobs, score=score,
+                        xtras=np.array(SW_XTRAS, np.int32), out=out)
+    print(f"sw_{name}: {len(jobs)} jobs x {len(SW_XTRAS)} flag sets")
+
+
+def sw_main(rng):
+    sc = g.default_score()
+    u8, jobs = sw_edge_jobs(rng).build()
+    save_sw("edge", u8, jobs, sc)
+    cj, u8 = nat.sw_jobs(400, 0x5EED, rev_frac=0.2)
+    save_sw("seeds", u8, _gpu_jobs(cj), sc)
+    sc2 = g.default_score(a=2, b=3, o_del=5, e_del=2, o_ins=4, e_ins=3)
+    cj, u8 = nat.sw_jobs(300, 0x5EED + 1)
+    save_sw("score2", u8, _gpu_jobs(cj), sc2)
+
+
+def _gpu_jobs(cj):
+    jobs = np.zeros(len(cj), g.JOB_DT)
+    for f in ("q_off", "t_off", "qlen", "tlen", "flags"):
+        jobs[f] = cj[f]
+    return jobs
+
+
 def main():
     if not nat.have_ref():
         sys.exit("oracle/_ref/libksw_ref.so missing: run sh oracle/build_ref.sh first")
@@ -164,7 +236,13 @@ def main():
     for w in (100, 5):
         wl = g.synth(2, 1500, seed=0x6A5 + 5 + w, w=w, unrelated=0.2)
         save_seeds(f"cfg5_w{w}", wl, nat.opt_from_score(sc, w=w))
+    sw_main(np.random.default_rng(2026))
 
 
 if __name__ == "__main__":
-    main()
+    if "--sw" in sys.argv:
+        if not nat.have_ref():
+            sys.exit("oracle/_ref/libksw_ref.so missing: run sh oracle/build_ref.sh first")
+        sw_main(np.random.default_rng(2026))
+    else:
+        main()

@@ -23,3 +23,12 @@ def load_jobs(name):
 def load_seeds(name):
     z = np.load(os.path.join(GOLDEN, f"seeds_{name}.npz"))
     return z["u8"], z["seeds"], z["opt"], z["reg"]
+
+
+def sw_sets():
+    return sorted(os.path.basename(p)[3:-4] for p in glob.glob(os.path.join(GOLDEN, "sw_*.npz")))
+
+
+def load_sw(name):
+    z = np.load(os.path.join(GOLDEN, f"sw_{name}.npz"))
+    return z["u8"], z["jobs"], z["score"], z["xtras"], z["out"]

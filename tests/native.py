@@ -48,6 +48,8 @@ def oracle():
         _oracle.g3o_global_batch.restype = None
         _oracle.g3o_nm_md_batch.argtypes = [P, I64, P, P, ctypes.c_int32, P, P, P, ctypes.c_int32]
         _oracle.g3o_nm_md_batch.restype = None
+        _oracle.g3o_sw_batch.argtypes = [P, I64, P, P, ctypes.c_int, P, P]
+        _oracle.g3o_sw_batch.restype = None
     return _oracle
 
 
@@ -68,6 +70,8 @@ def ref():
         _ref.g3r_global_batch.restype = ctypes.c_int
         _ref.g3r_nm_md_batch.argtypes = [P, I64, P, P, ctypes.c_int32, P, P, P, ctypes.c_int32]
         _ref.g3r_nm_md_batch.restype = ctypes.c_int
+        _ref.g3r_sw_batch.argtypes = [P, I64, P, P, ctypes.c_int, P]
+        _ref.g3r_sw_batch.restype = ctypes.c_int
     return _ref
 
 
@@ -287,3 +291,84 @@ def oracle_nm_md(jobs, u8, cigar, n_cigar, md_stride):
 def ref_nm_md(jobs, u8, cigar, n_cigar, md_stride):
     """(NM, MD strings) from the reference's own NM/MD block (aux.cu:2830-2861)."""
     return _nm_md(ref().g3r_nm_md_batch, jobs, u8, cigar, n_cigar, md_stride)
+
+
+# kswr_t (bwa/src/ksw.h:24-29) == g3o_swr == g3x_swr_t
+SWR_DT = np.dtype([("score", "<i4"), ("te", "<i4"), ("qe", "<i4"), ("score2", "<i4"), ("te2", "<i4"),
+                   ("tb", "<i4"), ("qb", "<i4")])
+KSW_XSTOP, KSW_XSUBO, KSW_XSTART = 0x20000, 0x40000, 0x80000
+
+
+def _mutate(rng, seq, div):
+    """seq with substitutions, 1-3 base insertions and deletions at rate div."""
+    out = []
+    for b in seq:
+        u = rng.random()
+        if u < div * 0.7:
+            out.append(int(rng.integers(0, 4)))
+        elif u < div * 0.85:
+            continue
+        elif u < div:
+            out.append(int(b))
+            out.extend(int(x) for x in rng.integers(0, 4, int(rng.integers(1, 4))))
+        else:
+            out.append(int(b))
+    return np.array(out, np.uint8)
+
+
+def sw_jobs(n, seed, flank=50, seed_len=(19, 60), related=0.5, n_frac=0.05, rev_frac=0.0, max_q=199):
+    """n seed-window pairs as mem_seed_sw cuts them (aux.cu:117-143): a seed of seed_len bases
+    with up to `flank` bases either side on the read (the query) and on the reference (the
+    target); the flanks agree with divergence U[0, 10%] for a `related` fraction of the pairs
+    and are unrelated otherwise; some queries carry N codes.  Query and target stay below
+    max_q + 1 bases.  A `rev_frac` fraction of the jobs has both sequences stored backwards
+    (flags 1 | 2).  Returns (CPU_JOB_DT jobs, u8 codes)."""
+    rng = np.random.default_rng(seed)
+    jobs = np.zeros(n, CPU_JOB_DT)
+    bufs, off = [], 0
+    for k in range(n):
+        L = int(rng.integers(seed_len[0], seed_len[1]))
+        core = rng.integers(0, 4, L).astype(np.uint8)
+        a, b = int(rng.integers(0, flank + 1)), int(rng.integers(0, flank + 1))
+        ql, qr = rng.integers(0, 4, a).astype(np.uint8), rng.integers(0, 4, b).astype(np.uint8)
+        q = np.concatenate([ql, core, qr])
+        if rng.random() < related:
+            div = rng.random() * 0.1
+            tl, tr = _mutate(rng, ql, div), _mutate(rng, qr, div)
+        else:
+            tl = rng.integers(0, 4, int(rng.integers(0, flank + 1))).astype(np.uint8)
+            tr = rng.integers(0, 4, int(rng.integers(0, flank + 1))).astype(np.uint8)
+        t = np.concatenate([tl, _mutate(rng, core, 0.02), tr])
+        q, t = q[:max_q], t[:max_q]
+        if rng.random() < n_frac and len(q):
+            q[rng.integers(0, len(q), int(rng.integers(1, 4)))] = 4
+        flags = 3 if rng.random() < rev_frac else 0
+        if flags:
+            q, t = q[::-1].copy(), t[::-1].copy()
+        jobs[k]["q_off"], jobs[k]["t_off"] = off, off + len(q)
+        jobs[k]["qlen"], jobs[k]["tlen"], jobs[k]["flags"] = len(q), len(t), flags
+        bufs += [q, t]
+        off += len(q) + len(t)
+    return jobs, (np.concatenate(bufs) if bufs else np.zeros(1, np.uint8))
+
+
+def _sw(fn, jobs, u8, score, xtra, with_cells):
+    n = len(jobs)
+    out = np.zeros(max(n, 1), SWR_DT)
+    args = [np.ascontiguousarray(jobs).ctypes.data, n, np.ascontiguousarray(u8).ctypes.data,
+            cpu_score(score).ctypes.data, int(xtra), out.ctypes.data]
+    cells = np.zeros(max(n, 1), np.int64)
+    if with_cells:
+        args.append(cells.ctypes.data)
+    fn(*args)
+    return out[:n], cells[:n]
+
+
+def oracle_sw(jobs, u8, score, xtra):
+    """(kswr_t records, cells) from the C restatement of ksw_align2."""
+    return _sw(oracle().g3o_sw_batch, jobs, u8, score, xtra, True)
+
+
+def ref_sw(jobs, u8, score, xtra):
+    """kswr_t records from the reference's own ksw_align2 (its trap line left out)."""
+    return _sw(ref().g3r_sw_batch, jobs, u8, score, xtra, False)[0]

@@ -1,0 +1,47 @@
+"""The oracle's striped local alignment (g3o_ksw_align2 in oracle/ksw_oracle.c: ksw_align2,
+ksw_qinit and ksw_i16 of bwa/src/ksw.cu:18-292) against the committed golden vectors of the
+reference's own ksw_align2 (tests/golden/sw_*.npz, made by tests/golden/make_golden.py) and
+against the compiled reference itself on fresh seeded windows.  Every kswr_t field is compared
+(score, te, qe, score2, te2, tb, qb) under each flag set: plain, XSTART (start positions),
+XSUBO (second-best score), XSTOP (stop at a score) and their combinations."""
+import numpy as np
+import pytest
+
+import g3sa_b200 as g
+from tests import golden_io
+from tests import native as nat
+
+
+@pytest.mark.parametrize("name", golden_io.sw_sets())
+def test_oracle_sw_matches_golden(name):
+    u8, jobs, score, xtras, out = golden_io.load_sw(name)
+    cj = nat.cpu_jobs(jobs)
+    for x, want in zip(xtras, out):
+        got, _ = nat.oracle_sw(cj, u8, score, int(x))
+        bad = np.nonzero(got != want)[0]
+        assert bad.size == 0, f"xtra {int(x):#x}: jobs {bad[:5]}: {got[bad[:2]]} vs {want[bad[:2]]}"
+
+
+def test_golden_sw_covers_the_paths():
+    """The fixtures exercise second-best scores, start positions, early stops and ties."""
+    u8, jobs, score, xtras, out = golden_io.load_sw("edge")
+    by = dict(zip((int(x) for x in xtras), out))
+    assert (by[nat.KSW_XSUBO]["score2"] > 0).any()
+    assert (by[nat.KSW_XSTART]["tb"] > 0).any() and (by[nat.KSW_XSTART]["qb"] > 0).any()
+    assert (by[nat.KSW_XSTOP | 15]["score"] < by[0]["score"]).any()
+    assert (by[0]["score"] == 0).any() and (by[0]["te"] == -1).any()
+    assert jobs["qlen"].max() == 256 and (jobs["tlen"] == 0).any()
+
+
+@pytest.mark.skipif(not nat.have_ref(), reason="oracle/_ref not built (no reference tree)")
+@pytest.mark.parametrize("seed", [1, 2])
+def test_oracle_sw_equals_reference(seed):
+    cj, u8 = nat.sw_jobs(1500, 0xA11 + seed, rev_frac=0.25, related=0.6)
+    sc = g.default_score()
+    for x in (0, nat.KSW_XSTART, nat.KSW_XSTART | nat.KSW_XSUBO | 25, nat.KSW_XSUBO | 8, nat.KSW_XSTOP | 30):
+        a, cells = nat.oracle_sw(cj, u8, sc, x)
+        b = nat.ref_sw(cj, u8, sc, x)
+        bad = np.nonzero(a != b)[0]
+        assert bad.size == 0, f"xtra {x:#x}: jobs {bad[:5]}"
+        rows = cj["tlen"] > 0                  # every pass enters at least one target row
+        assert (cells[rows] >= cj["qlen"][rows]).all()
