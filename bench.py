@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["chains", "global"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["chains", "global", "seedsw"])
     ap.add_argument("--schedule", default="auto", choices=["auto", "plain", "sorted", "learned"])
     ap.add_argument("--seed", type=int, default=0x6A5 + 2)
     return ap.parse_args()
@@ -477,6 +477,138 @@ def run_global_workload(args, ws, rank):
     }), flush=True)
 
 
+SW_JOBS = 200000
+SW_DESC = ("ksw_align2 (16-bit striped local SW, KSW_XSTART as mem_seed_sw calls it) over 200k synthetic "
+           "seed windows as mem_seed_sw cuts them: seed U[19,60) bases with U[0,50] bases either side on the "
+           "read and the reference, half the flanks related (divergence U[0,10%]), half unrelated, core 2%, "
+           "5% of queries with N codes; a=1 b=4 o=6 e=1")
+
+
+def run_sw_workload(args, ws, rank):
+    """`--workload seedsw`: g3x_ksw_align2_batch with KSW_XSTART, one step = every window of the
+    batch once (forward pass and start-position pass); GCUPS from the oracle's cell count
+    (query length x target rows entered, both passes)."""
+    import g3sa_b200 as g
+    from concurrent.futures import ThreadPoolExecutor
+    from tests import native as nat
+    if args.impl == "reference" and rank != 0:
+        return
+    cj, u8 = nat.sw_windows(SW_JOBS, args.seed + 2000 + 1000 * rank)
+    n = len(cj)
+    sc = g.default_score()
+    xtra = g.KSW_XSTART
+    want, cells_o = nat.oracle_sw(cj, u8, sc, xtra)
+    cells = int(cells_o.sum())
+    threads = os.cpu_count() or 1
+    metric = "ksw_align2 GCUPS & alignments/s on 1 B200, bit-exact"
+    cfg = {"workload": SW_DESC, "jobs": n, "cells": cells, "xtra": "KSW_XSTART"}
+
+    def ref_time():
+        bounds = np.linspace(0, n, threads + 1).astype(np.int64)
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda i: nat.ref_sw(cj[bounds[i]:bounds[i + 1]], u8, sc, xtra), range(threads)))
+        return time.perf_counter() - t0
+
+    if args.impl == "reference":
+        kind = "reference" if nat.have_ref() else "port"
+        times = []
+        for it in range(args.warmup + args.steps):
+            if kind == "reference":
+                dt = ref_time()
+            else:
+                t0 = time.perf_counter()
+                nat.oracle_sw(cj, u8, sc, xtra)
+                dt = time.perf_counter() - t0
+            if it >= args.warmup:
+                times.append(dt)
+        t = sum(times) / len(times)
+        gcups = cells / t / 1e9
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": round(gcups, 4), "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int16x2", "data": "synthetic (seeded)", "config": cfg,
+            "alignments_per_s": round(n / t, 1),
+            "cpu_baseline": {"value": round(gcups, 4), "unit": "GCUPS", "cores": threads if kind == "reference" else 1,
+                             "kind": kind, "sample": "whole workload per step"},
+            "e2e": {"value": round(gcups, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+            flush=True)
+        return
+    import torch
+    from g3sa_b200 import build
+    build.build_lib()
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    jobs = np.zeros(n, g.JOB_DT)
+    for f in ("q_off", "t_off", "qlen", "tlen", "flags"):
+        jobs[f] = cj[f]
+    codes, nmask = g.pack_planes(u8)
+    host = {k: torch.from_numpy(np.ascontiguousarray(v).view(np.uint8).copy()).pin_memory()
+            for k, v in (("jobs", jobs), ("codes", codes), ("nmask", nmask))}
+    d = {k: v.to(dev) for k, v in host.items()}
+    d_out = torch.zeros(n * 7, dtype=torch.int32, device=dev)
+    d_st = torch.zeros(n, dtype=torch.int32, device=dev)
+    h_out = [torch.zeros_like(x, device="cpu").pin_memory() for x in (d_out, d_st)]
+    ctx = g.Context(local)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    mt = int(cj["tlen"].max())
+
+    def call():
+        ctx.align2_batch(sc, d["jobs"], n, d["codes"], d["nmask"], xtra, mt, d_out, d_st, stream=stream)
+
+    call()
+    torch.cuda.synchronize()
+    got = d_out.cpu().numpy().view(g.SWR_DT)
+    exact = bool((d_st == 0).all()) and np.array_equal(got, want)
+    if not exact:
+        raise SystemExit("local alignments differ from the oracle")
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = timed_steps(call, args.steps, args.warmup, stream, flush)
+    clk = clocks.stop()
+
+    def e2e_step():
+        for k in d:
+            d[k].copy_(host[k], non_blocking=True)
+        call()
+        for h, x in zip(h_out, (d_out, d_st)):
+            h.copy_(x, non_blocking=True)
+
+    e2e_ms = timed_steps(e2e_step, max(3, args.steps // 4), args.warmup, stream, flush)
+    t, te = sum(ms) / len(ms), sum(e2e_ms) / len(e2e_ms)
+    (t, te), (tot_cells, tot_n) = combine_ranks(dist, [t, te], [cells, n], dev)
+    if rank != 0:
+        return
+    peak_gcups = ctx.int_peak() / 8 / 1e9
+    cpu_t = ref_time() if nat.have_ref() else None
+    gcups = tot_cells / (t * 1e-3) / 1e9
+    bi = sum(v.numel() for v in host.values())
+    bo = sum(h.numel() * 4 for h in h_out)
+    print(json.dumps({
+        "metric": metric, "value": round(gcups, 3), "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int16x2", "data": "synthetic (seeded generator)", "config": cfg,
+        "alignments_per_s": round(tot_n / (t * 1e-3), 1),
+        "e2e": {"value": round(tot_cells / (te * 1e-3) / 1e9, 3), "unit": "GCUPS", "ms_per_step": round(te, 4),
+                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
+        "roofline": {"bound": "int_alu", "achieved": round(gcups / max(ws, 1), 3), "peak": round(peak_gcups, 3),
+                     "unit": "GCUPS", "frac": round(gcups / max(ws, 1) / peak_gcups, 4), "traffic": None,
+                     "note": "cells per second of the step against the int-ALU cells/s peak (8 ops per cell)"},
+        "cpu_baseline": None if cpu_t is None else {
+            "value": round(cells / cpu_t / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
+            "sample": "whole rank-0 workload, one pass, the reference's own ksw_align2 (trap line left out)"},
+        "clocks": clk, "outputs_equal_oracle": exact, "gpu_launches": 6 * args.steps,
+    }), flush=True)
+
+
 def combine_ranks(dist, times, counts, device):
     """Every rank calls this with its own step times and counts: returns the max over ranks
     of each time (the slowest replica sets the pace) and the sum over ranks of each count.
@@ -554,6 +686,9 @@ def main():
         return
     if args.workload == "global":
         run_global_workload(args, ws, rank)
+        return
+    if args.workload == "seedsw":
+        run_sw_workload(args, ws, rank)
         return
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)

@@ -38,6 +38,10 @@ JOB_DT = np.dtype([("q_off", "<u4"), ("t_off", "<u4"), ("qlen", "<u2"), ("tlen",
                    ("h0", "<i4"), ("w", "<i4"), ("flags", "<u4")])
 EXT_DT = np.dtype([("score", "<i4"), ("qle", "<i4"), ("tle", "<i4"), ("gtle", "<i4"),
                    ("gscore", "<i4"), ("max_off", "<i4")])
+# g3x_swr_t == kswr_t (bwa/src/ksw.h:24-29)
+SWR_DT = np.dtype([("score", "<i4"), ("te", "<i4"), ("qe", "<i4"), ("score2", "<i4"), ("te2", "<i4"),
+                   ("tb", "<i4"), ("qb", "<i4")])
+KSW_XBYTE, KSW_XSTOP, KSW_XSUBO, KSW_XSTART = 0x10000, 0x20000, 0x40000, 0x80000
 SEED_DT = np.dtype([("read_off", "<i8"), ("win_off", "<i8"), ("rmax0", "<i8"), ("rmax1", "<i8"),
                     ("rbeg", "<i8"), ("l_query", "<i4"), ("qbeg", "<i4"), ("len", "<i4"),
                     ("pad_", "<i4")])
@@ -151,6 +155,8 @@ def lib():
         L.g3x_chain2aln.restype = ctypes.c_int
         L.g3x_ksw_global2_batch.argtypes = [P, P, P, I32, P, P, I32, I32, I32, P, P, I32, P, P, P, I32, P, P]
         L.g3x_ksw_global2_batch.restype = ctypes.c_int
+        L.g3x_ksw_align2_batch.argtypes = [P, P, P, I32, P, P, I32, I32, P, P, P]
+        L.g3x_ksw_align2_batch.restype = ctypes.c_int
         L.g3x_pac_to_planes.argtypes = [P, I64, P, P, I64, P]
         L.g3x_pac_to_planes.restype = ctypes.c_int
         L.g3x_pack_codes_device.argtypes = [P, I64, P, P, I64, P]
@@ -427,6 +433,14 @@ class Context:
                                            _ptr(d_cigar), int(cigar_stride), _ptr(d_n_cigar), _ptr(d_nm),
                                            _ptr(d_md), int(md_stride), _ptr(d_status), _stream(stream)),
                "g3x_ksw_global2_batch")
+
+    def align2_batch(self, score, d_jobs, n, d_codes, d_nmask, xtra, max_tlen, d_out, d_status, stream=None):
+        """g3x_ksw_align2_batch on device buffers: JOB_DT jobs, SWR_DT results (kswr_t), the
+        KSW_X* flags in xtra."""
+        _check(lib().g3x_ksw_align2_batch(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
+                                          _ptr(d_nmask), int(xtra), int(max_tlen), _ptr(d_out), _ptr(d_status),
+                                          _stream(stream)),
+               "g3x_ksw_align2_batch")
 
     def extend_seeds_stream(self, opt, seeds, codes, nmask, n_bases, regs, status, max_qlen,
                             max_tlen, chunk=65536, schedule=SCHED_SORTED, lanes=0, tile=0,

@@ -16,6 +16,7 @@ struct g3x_ctx {
     g3x::SchedScratch sched;     // job order and width classes of a persistent batch
     g3x::ChainScratch chain;     // chain-level call state
     g3x::GlobalScratch global;   // global-alignment backtrack bytes
+    g3x::SwScratch sw;           // striped local alignment: job order, XSUBO row maxima
     g3x::TileTable tiles;        // width classes and their kernel configurations
     unsigned long long* d_stats; // occupancy counters of the last persistent batch
     cudaStream_t side[g3x::kMaxBuckets];   // one stream per width class
@@ -30,6 +31,7 @@ namespace g3x {
 int ctx_device(const g3x_ctx* ctx) { return ctx->device; }
 ChainScratch& ctx_chain(g3x_ctx* ctx) { return ctx->chain; }
 GlobalScratch& ctx_global(g3x_ctx* ctx) { return ctx->global; }
+SwScratch& ctx_sw(g3x_ctx* ctx) { return ctx->sw; }
 
 static int alloc_sched(SchedScratch& s, int64_t n);
 
@@ -361,6 +363,8 @@ int g3x_ctx_destroy(g3x_ctx* c) {
     g3x::free_chain_scratch(c->chain);
     cudaFree(c->global.z);
     cudaFree(c->global.queue);
+    cudaFree(c->sw.buf);
+    cudaFree(c->sw.sub);
     for (int k = 0; k < g3x::kMaxBuckets; ++k) {
         cudaStreamDestroy(c->side[k]);
         cudaEventDestroy(c->join[k]);

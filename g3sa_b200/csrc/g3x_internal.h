@@ -160,6 +160,13 @@ struct GlobalScratch {
     int64_t bytes = 0;
 };
 GlobalScratch& ctx_global(g3x_ctx* ctx);
+// Scratch of the striped local alignment: sort arrays and counters (int32), XSUBO row maxima.
+struct SwScratch {
+    int32_t* buf = nullptr;
+    uint32_t* sub = nullptr;
+    int64_t cap = 0, sub_cap = 0;
+};
+SwScratch& ctx_sw(g3x_ctx* ctx);
 // The context's job order by decreasing row count and row width (its scheduling scratch).
 int cost_order(g3x_ctx* ctx, const g3x_job_t* jobs, int n, const ScoreParams& sp, cudaStream_t st,
                const int32_t** order);

@@ -384,6 +384,35 @@ int g3x_ksw_global2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
                           int32_t cigar_stride, int32_t *d_n_cigar, int32_t *d_nm, char *d_md,
                           int32_t md_stride, int32_t *d_status, void *stream);
 
+/* ---- striped local alignment with 16-bit cells --------------------------------------- */
+/* n calls of ksw_align2 (bwa/src/ksw.cu:271-292 with ksw_qinit :18-64 and ksw_i16 :155-262),
+   the local alignment mem_seed_sw runs on the window around a short seed (bwa/src/aux.cu:
+   117-143); the reference stops ksw_align2 at its first statement (ksw.cu:276), and this is
+   the function as written after it, with 16-bit cells (the only kind its ksw_i16 reads).
+   Job k aligns its query (q_off, qlen) locally to its target (t_off, tlen) (h0 and w unused;
+   G3X_JOB_QREV/TREV read the planes reversed); d_out[k] is the kswr_t: best score, its end on
+   the target (te) and query (qe); with G3X_KSW_XSUBO (minimum score in xtra & 0xffff) the
+   best row maximum more than ceil(score / max(mat)) rows from te (score2, te2); with
+   G3X_KSW_XSTART the start positions (tb, qb) from the reversed pass, when it finds the same
+   score; with G3X_KSW_XSTOP (score in xtra & 0xffff) the pass stops once the best score
+   reaches it.  Fields not computed are -1 (g_defr, ksw.cu:5).  d_status[k]: G3X_OK;
+   G3X_ERR_INVALID for qlen 0 (the reference reads before its buffers); G3X_ERR_TOO_LONG for
+   qlen > 256 or, under XSUBO, tlen > max_tlen.  Returns G3X_ERR_INVALID for G3X_KSW_XBYTE (the
+   reference fills an 8-bit profile and reads it as 16-bit cells) and G3X_ERR_SCORE for gap
+   costs above 32767 or, under XSUBO, a matrix without a positive score.  Scratch in the
+   context (the job order; under XSUBO 4 bytes per job and target row); calls on one context
+   belong on one stream.  Asynchronous on `stream`. */
+typedef struct {
+    int32_t score, te, qe, score2, te2, tb, qb;   /* == kswr_t, bwa/src/ksw.h:24-29 */
+} g3x_swr_t;
+#define G3X_KSW_XBYTE  0x10000   /* bwa/src/ksw.h:7-10 */
+#define G3X_KSW_XSTOP  0x20000
+#define G3X_KSW_XSUBO  0x40000
+#define G3X_KSW_XSTART 0x80000
+int g3x_ksw_align2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
+                         const uint32_t *d_codes, const uint32_t *d_nmask, int32_t xtra, int32_t max_tlen,
+                         g3x_swr_t *d_out, int32_t *d_status, void *stream);
+
 /* ---- host-resident batches, pipelined --------------------------------------------------- */
 /* No counterpart in the reference (its batches stay on the device between pipeline stages).
    A pipe extends batches of jobs that live in host memory with the context's schedule and

@@ -372,3 +372,66 @@ def oracle_sw(jobs, u8, score, xtra):
 def ref_sw(jobs, u8, score, xtra):
     """kswr_t records from the reference's own ksw_align2 (its trap line left out)."""
     return _sw(ref().g3r_sw_batch, jobs, u8, score, xtra, False)[0]
+
+
+def _mutate_many(rng, seq, owner, rate, n_owner):
+    """Vectorised _mutate over a concatenation: seq[k] belongs to sequence owner[k] and mutates
+    at rate[k].  Returns (new concatenation, new length of each of the n_owner sequences)."""
+    u = rng.random(len(seq))
+    sub = u < rate * 0.7
+    dele = (u >= rate * 0.7) & (u < rate * 0.85)
+    ins = (u >= rate * 0.85) & (u < rate)
+    s = seq.copy()
+    s[sub] = rng.integers(0, 4, int(sub.sum()))
+    extra = np.where(ins, rng.integers(1, 4, len(seq)), 0)
+    counts = np.where(dele, 0, 1 + extra)
+    out = np.repeat(s, counts)
+    first = np.cumsum(counts) - counts                 # where each kept base lands
+    is_ins = np.ones(len(out), bool)
+    is_ins[first[~dele]] = False
+    out[is_ins] = rng.integers(0, 4, int(is_ins.sum()))
+    lens = np.bincount(owner, weights=counts, minlength=n_owner).astype(np.int64)
+    return out.astype(np.uint8), lens
+
+
+def sw_windows(n, seed, flank=50, seed_len=(19, 60), related=0.5, n_frac=0.05):
+    """The shapes of sw_jobs, generated without a per-job loop (for large batches): seeds of
+    seed_len bases with up to `flank` bases either side; related flanks with divergence
+    U[0, 10%], unrelated ones random; the core with 2% divergence; some queries with N codes.
+    Returns (CPU_JOB_DT jobs, u8 codes), query and target of a job adjacent."""
+    rng = np.random.default_rng(seed)
+    L = rng.integers(seed_len[0], seed_len[1], n)
+    A, B = rng.integers(0, flank + 1, n), rng.integers(0, flank + 1, n)
+    ql = A + L + B
+    q = rng.integers(0, 4, int(ql.sum())).astype(np.uint8)
+    qo = np.cumsum(ql) - ql
+    owner = np.repeat(np.arange(n), ql)
+    pos = np.arange(len(q)) - np.repeat(qo, ql)
+    in_core = (pos >= np.repeat(A, ql)) & (pos < np.repeat(A + L, ql))
+    rel = rng.random(n) < related
+    div = rng.random(n) * 0.1
+    rate = np.where(in_core, 0.02, np.repeat(div, ql))
+    # unrelated jobs: their flanks are replaced by random bases of random length after mutation
+    keep_src = in_core | np.repeat(rel, ql)
+    t, tl = _mutate_many(rng, q[keep_src], owner[keep_src], rate[keep_src], n)
+    ua, ub = rng.integers(0, flank + 1, n), rng.integers(0, flank + 1, n)
+    ua, ub = np.where(rel, 0, ua), np.where(rel, 0, ub)
+    total_t = tl + ua + ub
+    tbuf = rng.integers(0, 4, int(total_t.sum())).astype(np.uint8)
+    to = np.cumsum(total_t) - total_t
+    src_o = np.cumsum(tl) - tl
+    dst = np.repeat(to + ua - src_o, tl) + np.arange(len(t))
+    tbuf[dst] = t
+    nq = rng.random(n) < n_frac
+    for k in np.nonzero(nq)[0][:]:
+        hit = rng.integers(0, ql[k], int(rng.integers(1, 4)))
+        q[qo[k] + hit] = 4
+    total = ql + total_t
+    base = np.cumsum(total) - total
+    u8 = np.empty(int(total.sum()), np.uint8)
+    u8[np.repeat(base - qo, ql) + np.arange(len(q))] = q
+    u8[np.repeat(base + ql - to, total_t) + np.arange(len(tbuf))] = tbuf
+    jobs = np.zeros(n, CPU_JOB_DT)
+    jobs["q_off"], jobs["t_off"] = base, base + ql
+    jobs["qlen"], jobs["tlen"] = ql, total_t
+    return jobs, u8
