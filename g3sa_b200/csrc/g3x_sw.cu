@@ -6,10 +6,12 @@
 // Four lanes per job (a quad), eight jobs per warp.  ksw_i16 works on vectors of eight 16-bit
 // cells; here a vector is the quad's four int16x2 words (lane p holds cells 2p and 2p+1), so
 // each vector step of the reference is one DPX/SIMD instruction per lane:
-//   adds (wrapping int16 add)        -> __vadd2
-//   max, max of three                -> __vmaxs2, __vimax3_s16x2
+//   adds, then max with E and F      -> __viaddmax_s16x2(H, S, max(E, F))
+//   max of non-negative cells        -> __vimax_s16x2_relu
 //   "subtract, 0 if not positive"    -> __viaddmax_s16x2_relu with the negated penalty
-//   the one-lane shift                -> one quad shuffle and a byte permute
+//   "any cell of F beats H - oe"      -> max(F, H - oe) != H - oe
+//   the one-cell shift                -> one quad shuffle and a byte permute
+// (only DPX forms: the SIMD-video intrinsics are instruction sequences on this architecture).
 // The query profile is not stored: segment j's word of lane p is the score of the row's target
 // base against query positions j + 2p*slen and j + (2p+1)*slen, one sign-extending byte
 // permute (prmt) of the score row by a selector built once per job.  The job's H and E rows
@@ -116,6 +118,118 @@ struct PassOut {
     int score, te, qe;
 };
 
+// Slot cases 0..31 of the unrolled segment loops.  A loop enters at the warp's first used slot
+// with one jump (a switch on a warp-uniform value) and falls through the rest.
+#define G3X_SW_CASES(F) F(0) F(1) F(2) F(3) F(4) F(5) F(6) F(7) F(8) F(9) F(10) F(11) F(12) F(13) F(14) \
+    F(15) F(16) F(17) F(18) F(19) F(20) F(21) F(22) F(23) F(24) F(25) F(26) F(27) F(28) F(29) F(30) F(31)
+
+// The row loop of one pass over registers H, E (slot MAXSEG - slen + j = segment j).  UNI: every
+// live quad of the warp has the same slot base, so no slot needs a per-quad guard; a quad that
+// is not running computes on slots it never reads back.
+template <int MAXSEG, bool UNI, bool SYM>
+__device__ __forceinline__ void sw_rows(const SwDesc& d, bool live, int tlen, Rows& rows, int minsc, int endsc,
+                                        uint32_t* sub, int& n_b, uint32_t (&H)[MAXSEG], uint32_t (&E)[MAXSEG],
+                                        const uint32_t (&sel2)[MAXSEG / 2], int base, int base_min, uint32_t* hm,
+                                        const uint32_t* tab, int lane, int& gmax, int& te) {
+    const int p = lane & 3;
+    const unsigned qmask = 0xFu << (lane & ~3);
+    int last_row = -2, last_v = 0;
+    bool run = live;
+    for (int i = 0;; ++i) {
+        run = run && i < tlen;
+        if (!__any_sync(kFull, run)) break;
+        uint32_t lo = 0u, hi = 0u;
+        if (run) {
+            const uint32_t t = rows.code(d.codes, d.nmask, i);
+            lo = tab[2 * t]; hi = tab[2 * t + 1];
+        }
+        uint32_t hd = shift_up(H[MAXSEG - 1], p);
+        uint32_t f = 0u, mx = 0u;
+        // the row (ksw.cu:193-208): M = H(i-1, j-1) + S, H = max(M, E, F), E' and F' from H
+        switch (base_min) {
+#define G3X_SW_MAIN(S)                                                                               \
+    case S:                                                                                          \
+        if constexpr (S < MAXSEG) {                                                                  \
+            if (UNI || S >= base) {                                                                  \
+                const uint32_t sc = prmt(lo, hi, (S & 1) ? sel2[S >> 1] >> 16 : sel2[S >> 1]);         \
+                const uint32_t h = __viaddmax_s16x2(hd, sc, __vimax_s16x2_relu(E[S], f));            \
+                mx = __vimax_s16x2_relu(mx, h);                                                      \
+                hd = H[S];                                                                           \
+                H[S] = h;                                                                            \
+                const uint32_t td = __viaddmax_s16x2_relu(h, d.noedel, 0u);                          \
+                E[S] = __viaddmax_s16x2(E[S], d.nedel, td);                                          \
+                f = __viaddmax_s16x2(f, d.neins, SYM ? td : __viaddmax_s16x2_relu(h, d.noeins, 0u)); \
+            }                                                                                        \
+        }
+            G3X_SW_CASES(G3X_SW_MAIN)
+#undef G3X_SW_MAIN
+            default: break;
+        }
+        // lazy F (ksw.cu:209-220): at most 16 rounds of the F vector moved up one cell, then
+        // H = max(H, F) segment by segment, E untouched, until a segment where no cell's F - e
+        // beats its H - (o + e).  One ballot per segment gives every quad its stop.
+        f = run ? f : 0u;
+        // A quad that stops gets F = 0, which leaves its H unchanged and keeps it stopped; a quad
+        // whose first segment is later (not UNI) waits with its F; the warp leaves when no quad
+        // goes on.
+        for (int round = 0; round < 16; ++round) {
+            f = shift_up(f, p);
+            switch (base_min) {
+#define G3X_SW_LAZY(S)                                                                               \
+    case S:                                                                                          \
+        if constexpr (S < MAXSEG) {                                                                  \
+            bool go;                                                                                 \
+            const bool at = UNI || S >= base;                                                        \
+            if (at) {                                                                                \
+                const uint32_t h = __vimax_s16x2_relu(H[S], f);                                      \
+                H[S] = h;                                                                            \
+                f = __viaddmax_s16x2_relu(f, d.neins, 0u);                                           \
+                const uint32_t hp = __viaddmax_s16x2_relu(h, d.noeins, 0u);                          \
+                go = __vimax_s16x2_relu(f, hp) != hp;                                                \
+            } else {                                                                                 \
+                go = f != 0u;                                                                        \
+            }                                                                                        \
+            const unsigned bal = __ballot_sync(kFull, go);                                           \
+            if (at && !(bal & qmask)) f = 0u;                                                        \
+            if (!bal) goto lazy_done;                                                                \
+        }
+                G3X_SW_CASES(G3X_SW_LAZY)
+#undef G3X_SW_LAZY
+                default: break;
+            }
+        }
+    lazy_done:
+        uint32_t m2 = __vimax_s16x2_relu(mx, __shfl_xor_sync(kFull, mx, 1));
+        m2 = __vimax_s16x2_relu(m2, __shfl_xor_sync(kFull, m2, 2));
+        const int im = max((int)(int16_t)(m2 & 0xFFFFu), (int)(int16_t)(m2 >> 16));
+        if (run) {
+            if (sub && im >= minsc && p == 0) {     // ksw.cu:223-232
+                if (n_b == 0 || last_row + 1 != i) {
+                    sub[n_b++] = (uint32_t)im << 16 | (uint32_t)i;
+                    last_row = i; last_v = im;
+                } else if (last_v < im) {
+                    sub[n_b - 1] = (uint32_t)im << 16 | (uint32_t)i;
+                    last_row = i; last_v = im;
+                }
+            }
+            if (im > gmax) {                        // ksw.cu:233-238
+                gmax = im; te = i;
+                switch (base_min) {
+#define G3X_SW_SNAP(S)                                                                               \
+    case S:                                                                                          \
+        if constexpr (S < MAXSEG) {                                                                  \
+            if (UNI || S >= base) hm[S * 32 + lane] = H[S];                                          \
+        }
+                    G3X_SW_CASES(G3X_SW_SNAP)
+#undef G3X_SW_SNAP
+                    default: break;
+                }
+                if (gmax >= endsc) run = false;
+            }
+        }
+    }
+}
+
 // One pass of ksw_i16 (ksw.cu:155-262) for the quad's job (live), query codes qcode(pos) for
 // pos < qlen.  With `sub`, row maxima >= minsc go to the job's list (ksw.cu:223-232; lane p = 0
 // keeps it) and *nb receives its length.
@@ -123,10 +237,11 @@ template <int MAXSEG, typename QCode>
 __device__ __forceinline__ PassOut sw_pass(const SwDesc& d, bool live, int qlen, int tlen, QCode qcode, Rows rows,
                                            int minsc, int endsc, uint32_t* sub, int* nb, uint32_t* hm,
                                            const uint32_t* tab, int lane) {
-    const int p = lane & 3, quad = lane >> 2;
+    const int p = lane & 3;
     const int slen = live ? (qlen + 7) >> 3 : 0;
     const int base = MAXSEG - slen;
     const int base_min = (int)__reduce_min_sync(kFull, (unsigned)base);
+    const bool uni = __all_sync(kFull, !live || base == base_min);
     uint32_t H[MAXSEG], E[MAXSEG], sel2[MAXSEG / 2];
 #pragma unroll
     for (int s = 0; s < MAXSEG; s += 2) {
@@ -146,74 +261,14 @@ __device__ __forceinline__ PassOut sw_pass(const SwDesc& d, bool live, int qlen,
         H[s] = H[s + 1] = 0u;
         E[s] = E[s + 1] = 0u;
     }
-    int gmax = 0, te = -1, n_b = 0, last_row = -2, last_v = 0;
-    bool run = live;
-    for (int i = 0;; ++i) {
-        run = run && i < tlen;
-        if (!__any_sync(kFull, run)) break;
-        uint32_t lo = 0u, hi = 0u;
-        if (run) {
-            const uint32_t t = rows.code(d.codes, d.nmask, i);
-            lo = tab[2 * t]; hi = tab[2 * t + 1];
-        }
-        uint32_t hd = shift_up(H[MAXSEG - 1], p);
-        uint32_t f = 0u, mx = 0u;
-#pragma unroll
-        for (int s = 0; s < MAXSEG; ++s) {
-            if (s >= base_min && run && s >= base) {
-                const uint32_t sc = prmt(lo, hi, (s & 1) ? sel2[s >> 1] >> 16 : sel2[s >> 1]);
-                const uint32_t h = __vimax3_s16x2(__vadd2(hd, sc), E[s], f);
-                mx = __vmaxs2(mx, h);
-                hd = H[s];
-                H[s] = h;
-                E[s] = __viaddmax_s16x2_relu(E[s], d.nedel, __vadd2(h, d.noedel));
-                f = __viaddmax_s16x2_relu(f, d.neins, __vadd2(h, d.noeins));
-            }
-        }
-        // lazy F (ksw.cu:209-220): at most 16 rounds, E untouched, out at the first segment
-        // where no cell's F beats its H
-        bool lz = run;
-        for (int round = 0; round < 16 && __any_sync(kFull, lz); ++round) {
-            f = shift_up(f, p);
-#pragma unroll
-            for (int s = 0; s < MAXSEG; ++s) {
-                if (s >= base_min) {
-                    const bool act = lz && s >= base;
-                    bool gt = false;
-                    if (act) {
-                        uint32_t h = __vmaxs2(H[s], f);
-                        H[s] = h;
-                        h = __viaddmax_s16x2_relu(h, d.noeins, 0u);
-                        f = __viaddmax_s16x2_relu(f, d.neins, 0u);
-                        gt = __vcmpgts2(f, h) != 0u;
-                    }
-                    const unsigned bal = __ballot_sync(kFull, gt);
-                    if (act) lz = ((bal >> (quad * 4)) & 0xFu) != 0u;
-                    if (!__any_sync(kFull, lz)) goto lazy_done;
-                }
-            }
-        }
-    lazy_done:
-        int im = run ? max((int)(int16_t)(mx & 0xFFFFu), (int)(int16_t)(mx >> 16)) : 0;
-        im = quad_max(im);
-        if (run) {
-            if (sub && im >= minsc && p == 0) {     // ksw.cu:223-232
-                if (n_b == 0 || last_row + 1 != i) {
-                    sub[n_b++] = (uint32_t)im << 16 | (uint32_t)i;
-                    last_row = i; last_v = im;
-                } else if (last_v < im) {
-                    sub[n_b - 1] = (uint32_t)im << 16 | (uint32_t)i;
-                    last_row = i; last_v = im;
-                }
-            }
-            if (im > gmax) {                        // ksw.cu:233-238
-                gmax = im; te = i;
-#pragma unroll
-                for (int s = 0; s < MAXSEG; ++s)
-                    if (s >= base) hm[s * 32 + lane] = H[s];
-                if (gmax >= endsc) run = false;
-            }
-        }
+    int gmax = 0, te = -1, n_b = 0;
+    // SYM: equal insertion and deletion costs, so E and F share H - (o + e)
+    if (d.noedel == d.noeins) {
+        if (uni) sw_rows<MAXSEG, true, true>(d, live, tlen, rows, minsc, endsc, sub, n_b, H, E, sel2, base, base_min, hm, tab, lane, gmax, te);
+        else sw_rows<MAXSEG, false, true>(d, live, tlen, rows, minsc, endsc, sub, n_b, H, E, sel2, base, base_min, hm, tab, lane, gmax, te);
+    } else {
+        if (uni) sw_rows<MAXSEG, true, false>(d, live, tlen, rows, minsc, endsc, sub, n_b, H, E, sel2, base, base_min, hm, tab, lane, gmax, te);
+        else sw_rows<MAXSEG, false, false>(d, live, tlen, rows, minsc, endsc, sub, n_b, H, E, sel2, base, base_min, hm, tab, lane, gmax, te);
     }
     __syncwarp();
     // end on the query: the smallest position holding the best row's largest cell, cells read
