@@ -163,6 +163,8 @@ def lib():
         L.g3x_pack_codes_device.restype = ctypes.c_int
         L.g3x_pair_generate.argtypes = [P, P, P, I32, P, I32, P, I32, P, I32, P, P, P, P]
         L.g3x_pair_generate.restype = ctypes.c_int
+        L.g3x_traceback_pairs.argtypes = [P, P, P, I32, P, I32, P, I32, P, P, P]
+        L.g3x_traceback_pairs.restype = ctypes.c_int
         L.g3x_pipe_create.argtypes = [P, P, I32, I32, I64, I64, ctypes.POINTER(P)]
         L.g3x_pipe_create.restype = ctypes.c_int
         L.g3x_pipe_submit.argtypes = [P, P, I32, P, I64, P, I64, I32, I32, P, P, P]
@@ -501,6 +503,19 @@ def pair_generate(opt, l_pac, ref_off, d_anns, n_seqs, d_reads, n_reads, d_chain
 
 
 SEEDREC_DT = np.dtype([("read", "<i4"), ("chain", "<i4"), ("seed", "<i4")])
+# g3x_alnrec_t: one alignment of the traceback stage (read, absolute region index)
+ALNREC_DT = np.dtype([("read", "<i4"), ("reg", "<i4")])
+
+
+def traceback_pairs(opt, l_pac, ref_off, d_reads, n_reads, d_regs, n_regs, d_recs, n_recs, d_jobs, d_status,
+                    stream=None):
+    """g3x_traceback_pairs: per alignment record (ALNREC_DT) the ksw_global2 job (JOB_DT) of its
+    region, as the traceback stage prepares it."""
+    ri = np.zeros(1, REFINFO_DT)
+    ri["l_pac"], ri["ref_off"] = l_pac, ref_off
+    _check(lib().g3x_traceback_pairs(opt.ctypes.data, ri.ctypes.data, _ptr(d_reads), int(n_reads), _ptr(d_regs),
+                                     int(n_regs), _ptr(d_recs), int(n_recs), _ptr(d_jobs), _ptr(d_status),
+                                     _stream(stream)), "g3x_traceback_pairs")
 
 
 class Pipe:

@@ -18,6 +18,8 @@
 
 namespace g3x {
 
+constexpr int kTracebackBandCap = 500;   // GLOBALSW_BANDWITH_CUTOFF, bwa/src/aux.cuh:428
+
 namespace {
 
 // bwa's pac order: base k in byte k >> 2, bits ((~k) & 3) << 1
@@ -142,11 +144,90 @@ __global__ void pair_kernel(g3x_opt_t opt, int64_t l_pac, int64_t ref_off, const
     status[i] = G3X_OK;
 }
 
+// Band width of the traceback stage's pair (aux.cu:506-513, infer_bw).
+__device__ int infer_bw(int l1, int l2, int score, int a, int q, int r) {
+    if (l1 == l2 && l1 * a - score < (q + r - a) << 1) return 0;
+    const int w = (int)((double)((l1 < l2 ? l1 : l2) * a - score - q) / r + 2.);
+    const int d = l1 > l2 ? l1 - l2 : l2 - l1;
+    return w < d ? d : w;
+}
+
+// FINALIZEALN_preprocessing2_kernel (aux.cu:2698-2745) and the band cap of traceback_baseline
+// (aux.cu:2810-2812) for one alignment record: the region's query and reference slices as a
+// ksw_global2 job.
+__global__ void tb_pair_kernel(g3x_opt_t opt, int64_t l_pac, int64_t ref_off, const g3x_read_t* __restrict__ reads,
+                               int n_reads, const g3x_alnreg_t* __restrict__ regs, int n_regs,
+                               const g3x_alnrec_t* __restrict__ recs, int n_recs, g3x_job_t* __restrict__ jobs,
+                               int32_t* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_recs) return;
+    const g3x_alnrec_t rc = recs[i];
+    g3x_job_t jb = {};
+    jobs[i] = jb;                                     // an empty job unless the record is valid
+    status[i] = G3X_ERR_INVALID;
+    if (rc.read < 0 || rc.read >= n_reads || rc.reg < 0 || rc.reg >= n_regs) return;
+    const g3x_read_t rd = reads[rc.read];
+    const g3x_alnreg_t g = regs[rc.reg];
+    const int lq = g.qe - g.qb;
+    if (lq < 0 || g.qb < 0 || rd.read_off + g.qb + (int64_t)lq > 0xFFFFFFFFLL) return;
+    // the reference slice as bns_get_seq_gpu returns it (bntseq.cu:39-60)
+    int64_t beg = g.rb, end = g.re, rlen = 0;
+    if (end < beg) { const int64_t t = beg; beg = end; end = t; }
+    if (end > l_pac << 1) end = l_pac << 1;
+    if (beg < 0) beg = 0;
+    if (beg >= l_pac || end <= l_pac) rlen = end - beg;
+    if (lq > 65535 || rlen > 65535) { status[i] = G3X_ERR_TOO_LONG; return; }
+    // the band (aux.cu:2711-2737), stored as uint16 (aux.cu:2745), at most 500 (aux.cu:2812)
+    int w = 0;
+    if ((int64_t)lq != g.re - g.rb) {
+        const g3x_score_t& sc = opt.score;
+        const int l2 = (int)(g.re - g.rb);
+        const int wd = infer_bw(lq, l2, g.score, opt.a, sc.o_del, sc.e_del);
+        const int wi = infer_bw(lq, l2, g.score, opt.a, sc.o_ins, sc.e_ins);
+        w = wd > wi ? wd : wi;
+        const int half = ((lq + 1) >> 1) * opt.a;
+        const int max_ins = (int)((double)(half - sc.o_ins) / sc.e_ins + 1.);
+        const int max_del = (int)((double)(half - sc.o_del) / sc.e_del + 1.);
+        int max_gap = max_ins > max_del ? max_ins : max_del;
+        max_gap = max_gap > 1 ? max_gap : 1;
+        const int dl = (int)rlen > lq ? (int)rlen - lq : lq - (int)rlen;
+        const int hi = (max_gap + dl + 1) >> 1;
+        w = w < hi ? w : hi;
+        w = w > dl + 3 ? w : dl + 3;
+    }
+    w = (uint16_t)w;
+    jb.q_off = (uint32_t)(rd.read_off + g.qb);
+    jb.t_off = (uint32_t)(ref_off + beg);
+    jb.qlen = (uint16_t)lq;
+    jb.tlen = (uint16_t)rlen;
+    jb.w = w < kTracebackBandCap ? w : kTracebackBandCap;
+    jb.flags = g.rb >= l_pac ? G3X_JOB_MDRC : 0u;
+    jobs[i] = jb;
+    status[i] = G3X_OK;
+}
+
 }  // namespace
 
 }  // namespace g3x
 
 extern "C" {
+
+int g3x_traceback_pairs(const g3x_opt_t* opt, const g3x_refinfo_t* ref, const g3x_read_t* d_reads, int32_t n_reads,
+                        const g3x_alnreg_t* d_regs, int32_t n_regs, const g3x_alnrec_t* d_recs, int32_t n_recs,
+                        g3x_job_t* d_jobs, int32_t* d_status, void* stream) {
+    if (!opt || !ref || n_recs < 0 || n_reads < 0 || n_regs < 0) return G3X_ERR_INVALID;
+    if (n_recs == 0) return G3X_OK;
+    if (!d_reads || !d_regs || !d_recs || !d_jobs || !d_status || ref->l_pac <= 0 || ref->ref_off < 0 ||
+        ref->ref_off + 2 * ref->l_pac > 0xFFFFFFFFLL)
+        return G3X_ERR_INVALID;
+    g3x::ScoreParams sp;
+    const int rc = g3x::score_params(&opt->score, &sp);
+    if (rc) return rc;
+    const int tb = 128;
+    g3x::tb_pair_kernel<<<(n_recs + tb - 1) / tb, tb, 0, (cudaStream_t)stream>>>(
+        *opt, ref->l_pac, ref->ref_off, d_reads, n_reads, d_regs, n_regs, d_recs, n_recs, d_jobs, d_status);
+    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
 
 int g3x_pac_to_planes(const uint8_t* d_pac, int64_t l_pac, uint32_t* d_codes, uint32_t* d_nmask,
                       int64_t base, void* stream) {

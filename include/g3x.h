@@ -359,6 +359,32 @@ int g3x_pair_generate(const g3x_opt_t *opt, const g3x_refinfo_t *ref, const g3x_
                       int32_t n_recs, g3x_seed_t *d_out, int32_t *d_rid, int32_t *d_status,
                       void *stream);
 
+/* One alignment of the traceback stage, as its seed_record_t names it (seqID, regID;
+   bwa/src/bwa.h:272-287), with the region as an absolute index into the region array. */
+typedef struct {
+    int32_t read, reg;
+} g3x_alnrec_t;           /* 8 bytes */
+
+/* The pair preparation of the traceback stage for n_recs alignment records:
+   FINALIZEALN_preprocessing2_kernel (bwa/src/aux.cu:2698-2745) and the band cap of
+   traceback_baseline (aux.cu:2810-2812, GLOBALSW_BANDWITH_CUTOFF = 500, aux.cuh:428).  Record
+   i's region (d_regs[reg], e.g. from g3x_chain2aln) becomes the g3x_ksw_global2_batch job
+   d_jobs[i]: query = read [qb, qe) at d_reads[read].read_off + qb, target = the reference slice
+   [rb, re) as bns_get_seq_gpu returns it (bwa/src/bntseq.cu:39-60: bounds swapped if reversed,
+   clipped to [0, 2 l_pac), empty when it spans the forward/reverse boundary) at ref_off + beg;
+   w = 0 when qe - qb == re - rb, else the larger infer_bw (aux.cu:506-513) of the deletion and
+   insertion costs for the region's score, at most (max_gap + |tlen - qlen| + 1) / 2, at least
+   |tlen - qlen| + 3, then kept as the reference's uint16 and capped at 500; G3X_JOB_MDRC when
+   rb >= l_pac.  (The reference's reversal kernel FINALIZEALN_reverseSeq_kernel, aux.cu:
+   2755-2790, writes reversed copies that nothing reads, so the slices go in as they are.)
+   d_status[i]: G3X_OK; G3X_ERR_INVALID for a record outside its arrays or a region with
+   qe < qb (empty job); G3X_ERR_TOO_LONG when a slice is longer than 65535 bases.  Asynchronous
+   on `stream` (the current device). */
+int g3x_traceback_pairs(const g3x_opt_t *opt, const g3x_refinfo_t *ref, const g3x_read_t *d_reads,
+                        int32_t n_reads, const g3x_alnreg_t *d_regs, int32_t n_regs,
+                        const g3x_alnrec_t *d_recs, int32_t n_recs, g3x_job_t *d_jobs, int32_t *d_status,
+                        void *stream);
+
 /* ---- banded global alignment with backtrack ------------------------------------------- */
 /* n calls of ksw_global2 (bwa/src/ksw.cu:706-809) as traceback_baseline issues them
    (bwa/src/aux.cu:2794-2830): job k aligns its query (q_off, qlen) globally to its target

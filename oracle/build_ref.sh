@@ -6,8 +6,9 @@
 # (bwa/src/aux.cu:168-175, 178-315; bwa/src/bntseq.cu:5, 7-87), the banded global alignment
 # with backtrack (bwa/src/ksw.cu:299-301, 548, 694-809) and the NM/MD block of the traceback
 # stage (bwa/src/aux.cu:2830-2861), the striped local alignment ksw_align2 with ksw_qinit and
-# ksw_i16 (bwa/src/ksw.cu:5, 18-292 less its trap line 276; bwa/src/ksw.h:7-29), plus the
-# ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
+# ksw_i16 (bwa/src/ksw.cu:5, 18-292 less its trap line 276; bwa/src/ksw.h:7-29), the pair
+# preparation of the traceback stage (bwa/src/aux.cu:506-513, 2698-2737; bwa/src/bntseq.cu:5,
+# 39-60), plus the ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
 # reference tree into the compiler; no reference source is copied into this repository.
 # Usage: sh oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -eu
@@ -111,8 +112,27 @@ if [ "$K5" != "__device__ const kswr_t g_defr =" ] || [ "$K18" != "static __devi
 fi
 { cat "$HERE/ref_sw_head.inc"; sed -n '7,29p' "$KSWH"; sed -n '5p;18,275p;277,292p' "$SRC"; cat "$HERE/ref_sw_tail.inc"; } | \
     tr -d '\r' | $CXX -O3 -fPIC -std=c++17 -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/sw_ref_fn.o"
+# Pair preparation of the traceback stage: bntseq.cu:5, 39-60 (_get_pac, bns_get_seq_gpu),
+# aux.cu:506-513 (infer_bw) and the per-record lines of FINALIZEALN_preprocessing2_kernel
+# (aux.cu:2698-2737) between ref_tbpair_head.inc, ref_tbpair_mid.inc and ref_tbpair_tail.inc.
+T506=$(sed -n '506p' "$AUX" | tr -d '\r' | sed 's/^ *//;s/ *$//')
+T513=$(sed -n '513p' "$AUX" | tr -d '\r' | sed 's/^ *//;s/ *$//')
+T2698=$(sed -n '2698p' "$AUX" | tr -d '\r' | sed 's/^ *//;s/ *$//')
+T2737=$(sed -n '2737p' "$AUX" | tr -d '\r' | sed 's/^ *//;s/ *$//')
+B39=$(sed -n '39p' "$BNS" | tr -d '\r' | cut -c1-35)
+B60=$(sed -n '60p' "$BNS" | tr -d '\r')
+if [ "$T506" != "__device__ static inline int infer_bw(int l1, int l2, int score, int a, int q, int r)" ] || \
+   [ "$T513" != "}" ] || [ "$T2698" != "int64_t rb = d_regs[seqID].a[alnID].rb;" ] || [ "$T2737" != "}" ] || \
+   [ "$B39" != "__device__ uint8_t *bns_get_seq_gpu" ] || [ "$B60" != "}" ]; then
+    echo "build_ref.sh: unexpected content at aux.cu:506/513/2698/2737 or bntseq.cu:39/60; refusing to build" >&2
+    exit 3
+fi
+{ cat "$HERE/ref_tbpair_head.inc"; sed -n '5p;39,60p' "$BNS"; sed -n '506,513p' "$AUX"; cat "$HERE/ref_tbpair_mid.inc"; \
+  sed -n '2698,2737p' "$AUX"; cat "$HERE/ref_tbpair_tail.inc"; } | tr -d '\r' | \
+    $CXX -O3 -fPIC -std=c++17 -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/tbpair_ref_fn.o"
 $CXX -O3 -fPIC -shared -std=c++17 "$HERE/ref_wrap.cpp" "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" \
-    "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o" "$OUT/sw_ref_fn.o" -o "$OUT/libksw_ref.so" -lpthread
+    "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o" "$OUT/sw_ref_fn.o" "$OUT/tbpair_ref_fn.o" \
+    -o "$OUT/libksw_ref.so" -lpthread
 rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o" \
-    "$OUT/sw_ref_fn.o"
+    "$OUT/sw_ref_fn.o" "$OUT/tbpair_ref_fn.o"
 echo "built $OUT/libksw_ref.so"

@@ -883,3 +883,70 @@ void g3o_sw_batch(const g3o_job *jobs, int64_t n, const uint8_t *codes, const g3
         free(qb); free(tb);
     }
 }
+
+/* ---------------------------------------------------------------------------------- */
+/* Pair preparation of the traceback stage: FINALIZEALN_preprocessing2_kernel            */
+/* (aux.cu:2698-2745) with infer_bw (aux.cu:506-513) and bns_get_seq_gpu                 */
+/* (bntseq.cu:39-60).                                                                    */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct { int32_t a, o_del, e_del, o_ins, e_ins; } g3o_tbopt;
+
+/* Band width a global alignment of l1 and l2 bases with this score needs (aux.cu:506-513):
+   0 for equal lengths that leave no room for two gaps, else (min(l1,l2) a - score - q) / r + 2
+   (the double truncated), at least |l1 - l2|. */
+static int g3o_infer_bw(int l1, int l2, int score, int a, int q, int r)
+{
+    if (l1 == l2 && l1 * a - score < (q + r - a) << 1) return 0;
+    int w = (int)((double)((l1 < l2 ? l1 : l2) * a - score - q) / r + 2.);
+    const int d = l1 > l2 ? l1 - l2 : l2 - l1;
+    return w < d ? d : w;
+}
+
+/* Per record k (read recs[2k], region recs[2k+1]): the query read[qb, qe) (its code-buffer
+   offset and length), the reference slice [rb, re) as bns_get_seq_gpu returns it (bounds
+   swapped if reversed, clipped to [0, 2 l_pac), empty when it spans the forward/reverse
+   boundary) to tgt[k * tstride ...] with its length, and the band width: 0 when the query and
+   [rb, re) have equal lengths, else the larger infer_bw of the deletion and insertion costs,
+   at most (max_gap + |rlen - lq| + 1) / 2 with max_gap the larger of the insertion and
+   deletion gaps half the query can pay for (at least 1), at least |rlen - lq| + 3; stored as
+   uint16 (aux.cu:2745).  rb_out[k] = rb (the stage prints the reverse-strand alphabet in MD
+   when rb >= l_pac). */
+void g3o_tb_pairs(const g3o_tbopt *opt, const uint8_t *codes, int64_t ref_off, int64_t l_pac,
+                  const g3o_read *reads, const g3o_alnreg *regs, const int32_t *recs, int64_t n,
+                  int64_t *q_off, int32_t *qlen, uint8_t *tgt, int32_t tstride, int32_t *tlen, int32_t *w,
+                  int64_t *rb_out)
+{
+    for (int64_t k = 0; k < n; ++k) {
+        const g3o_read *rd = &reads[recs[2 * k]];
+        const g3o_alnreg *g = &regs[recs[2 * k + 1]];
+        const int lq = g->qe - g->qb;
+        int64_t beg = g->rb, end = g->re, rlen = 0;
+        if (end < beg) { const int64_t t = beg; beg = end; end = t; }
+        if (end > l_pac << 1) end = l_pac << 1;
+        if (beg < 0) beg = 0;
+        if (beg >= l_pac || end <= l_pac) rlen = end - beg;
+        q_off[k] = rd->read_off + g->qb;
+        qlen[k] = lq;
+        tlen[k] = (int32_t)rlen;
+        for (int64_t x = 0; x < rlen && x < tstride; ++x) tgt[k * tstride + x] = codes[ref_off + beg + x];
+        int bw = 0;
+        if ((int64_t)lq != g->re - g->rb) {
+            const int l2 = (int)(g->re - g->rb);
+            const int wd = g3o_infer_bw(lq, l2, g->score, opt->a, opt->o_del, opt->e_del);
+            const int wi = g3o_infer_bw(lq, l2, g->score, opt->a, opt->o_ins, opt->e_ins);
+            bw = wd > wi ? wd : wi;
+            const int half = ((lq + 1) >> 1) * opt->a;
+            const int max_ins = (int)((double)(half - opt->o_ins) / opt->e_ins + 1.);
+            const int max_del = (int)((double)(half - opt->o_del) / opt->e_del + 1.);
+            int max_gap = max_ins > max_del ? max_ins : max_del;
+            if (max_gap < 1) max_gap = 1;
+            const int dl = (int)rlen > lq ? (int)rlen - lq : lq - (int)rlen;
+            const int hi = (max_gap + dl + 1) >> 1;
+            if (bw > hi) bw = hi;
+            if (bw < dl + 3) bw = dl + 3;
+        }
+        w[k] = (uint16_t)bw;
+        rb_out[k] = g->rb;
+    }
+}

@@ -50,6 +50,8 @@ def oracle():
         _oracle.g3o_nm_md_batch.restype = None
         _oracle.g3o_sw_batch.argtypes = [P, I64, P, P, ctypes.c_int, P, P]
         _oracle.g3o_sw_batch.restype = None
+        _oracle.g3o_tb_pairs.argtypes = [P, P, I64, I64, P, P, P, I64, P, P, P, ctypes.c_int32, P, P, P]
+        _oracle.g3o_tb_pairs.restype = None
     return _oracle
 
 
@@ -72,6 +74,8 @@ def ref():
         _ref.g3r_nm_md_batch.restype = ctypes.c_int
         _ref.g3r_sw_batch.argtypes = [P, I64, P, P, ctypes.c_int, P]
         _ref.g3r_sw_batch.restype = ctypes.c_int
+        _ref.g3r_tb_pairs.argtypes = [P, P, I64, I64, P, P, P, I64, P, P, P, ctypes.c_int32, P, P, P]
+        _ref.g3r_tb_pairs.restype = ctypes.c_int
     return _ref
 
 
@@ -435,3 +439,44 @@ def sw_windows(n, seed, flank=50, seed_len=(19, 60), related=0.5, n_frac=0.05):
     jobs["q_off"], jobs["t_off"] = base, base + ql
     jobs["qlen"], jobs["tlen"] = ql, total_t
     return jobs, u8
+
+
+TBOPT_DT = np.dtype([("a", "<i4"), ("o_del", "<i4"), ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4")])
+
+
+def tb_records(wl, nregs):
+    """(read, region index) for every region a chain-level call wrote: read r's regions start at
+    its first chain's first seed slot."""
+    recs = []
+    for r, rd in enumerate(wl.reads):
+        if rd["n_chains"] == 0:
+            continue
+        beg = int(wl.chains[rd["chain_beg"]]["seed_beg"])
+        recs += [(r, beg + i) for i in range(int(nregs[r]))]
+    return np.array(recs, np.int32).reshape(-1, 2)
+
+
+def _tb(fn, opt, u8, ref_off, l_pac, reads, regs, recs, tstride):
+    n = len(recs)
+    o = np.zeros(1, TBOPT_DT)
+    for f in ("a", "o_del", "e_del", "o_ins", "e_ins"):
+        o[f] = opt[f]
+    q_off = np.zeros(max(n, 1), np.int64)
+    qlen, tlen, w = (np.zeros(max(n, 1), np.int32) for _ in range(3))
+    rb = np.zeros(max(n, 1), np.int64)
+    tgt = np.zeros((max(n, 1), tstride), np.uint8)
+    fn(o.ctypes.data, np.ascontiguousarray(u8).ctypes.data, int(ref_off), int(l_pac), np.ascontiguousarray(reads).ctypes.data,
+       np.ascontiguousarray(regs).ctypes.data, np.ascontiguousarray(recs, np.int32).ctypes.data, n, q_off.ctypes.data,
+       qlen.ctypes.data, tgt.ctypes.data, tstride, tlen.ctypes.data, w.ctypes.data, rb.ctypes.data)
+    return q_off[:n], qlen[:n], tgt[:n], tlen[:n], w[:n], rb[:n]
+
+
+def oracle_tb_pairs(opt, u8, ref_off, l_pac, reads, regs, recs, tstride):
+    """(q_off, qlen, target bases [n, tstride], tlen, w, rb) from the C restatement of the
+    traceback stage's pair preparation."""
+    return _tb(oracle().g3o_tb_pairs, opt, u8, ref_off, l_pac, reads, regs, recs, tstride)
+
+
+def ref_tb_pairs(opt, u8, ref_off, l_pac, reads, regs, recs, tstride):
+    """The same from the reference's own FINALIZEALN_preprocessing2 lines (aux.cu:2698-2737)."""
+    return _tb(ref().g3r_tb_pairs, opt, u8, ref_off, l_pac, reads, regs, recs, tstride)
