@@ -157,6 +157,8 @@ def lib():
         L.g3x_ksw_global2_batch.restype = ctypes.c_int
         L.g3x_ksw_align2_batch.argtypes = [P, P, P, I32, P, P, I32, I32, P, P, P]
         L.g3x_ksw_align2_batch.restype = ctypes.c_int
+        L.g3x_flt_chained_seeds.argtypes = [P, P, I32, P, P, I32, P, I32, P, I32, P, P, P, P, P]
+        L.g3x_flt_chained_seeds.restype = ctypes.c_int
         L.g3x_pac_to_planes.argtypes = [P, I64, P, P, I64, P]
         L.g3x_pac_to_planes.restype = ctypes.c_int
         L.g3x_pack_codes_device.argtypes = [P, I64, P, P, I64, P]
@@ -443,6 +445,17 @@ class Context:
                                           _ptr(d_nmask), int(xtra), int(max_tlen), _ptr(d_out), _ptr(d_status),
                                           _stream(stream)),
                "g3x_ksw_align2_batch")
+
+    def flt_chained_seeds(self, opt, min_chain_weight, l_pac, ref_off, d_anns, n_seqs, d_reads, n_reads, d_chains,
+                          n_chains, d_seeds, n_seeds, d_codes, d_nmask, d_status, d_sw_score=None, stream=None):
+        """g3x_flt_chained_seeds on device buffers (the chain and seed arrays change in place)."""
+        ri = np.zeros(1, REFINFO_DT)
+        ri["l_pac"], ri["ref_off"], ri["n_seqs"], ri["d_anns"] = l_pac, ref_off, n_seqs, _ptr(d_anns)
+        _check(lib().g3x_flt_chained_seeds(self._h, opt.ctypes.data, int(min_chain_weight), ri.ctypes.data,
+                                           _ptr(d_reads), int(n_reads), _ptr(d_chains), int(n_chains), _ptr(d_seeds),
+                                           int(n_seeds), _ptr(d_codes), _ptr(d_nmask), _ptr(d_sw_score),
+                                           _ptr(d_status), _stream(stream)),
+               "g3x_flt_chained_seeds")
 
     def extend_seeds_stream(self, opt, seeds, codes, nmask, n_bases, regs, status, max_qlen,
                             max_tlen, chunk=65536, schedule=SCHED_SORTED, lanes=0, tile=0,

@@ -94,12 +94,13 @@ def _sample_read(rng, ref2, p, seg_end, lq, d):
 
 
 def synth_chains(n_reads, seed=1, n_contigs=12, contig_len=(20000, 120000), a=1,
-                 div=0.05, min_seed=19, spurious=0.6, edge=0.15):
+                 div=0.05, min_seed=19, spurious=0.6, edge=0.15, read_lens=None):
     """Reads sampled from a random reference (substitutions at up to `div`, small indels),
     each with its true chain (exact-match seeds along the read's alignment, some split into
     overlapping pieces) and, with probability `spurious`, one or two chains of short seeds at
     random loci.  A fraction `edge` of the reads lies within a read length of a contig end, so
-    windows are clipped to contigs and strands."""
+    windows are clipped to contigs and strands.  Read lengths are 100/150/250 (0.4/0.4/0.2), or
+    drawn uniformly from `read_lens`."""
     rng = np.random.default_rng(seed)
     lens = rng.integers(contig_len[0], contig_len[1], n_contigs)
     offs = np.concatenate([[0], np.cumsum(lens)[:-1]])
@@ -116,7 +117,7 @@ def synth_chains(n_reads, seed=1, n_contigs=12, contig_len=(20000, 120000), a=1,
     read_chunks, reads, chains, seeds = [], [], [], []
     base = 2 * l_pac
     for r in range(n_reads):
-        lq = int(rng.choice([100, 150, 250], p=[0.4, 0.4, 0.2]))
+        lq = int(rng.choice([100, 150, 250], p=[0.4, 0.4, 0.2])) if read_lens is None else int(rng.choice(read_lens))
         sg = int(rng.integers(0, len(seg_b)))
         span = lq + 8
         lo, hi = int(seg_b[sg]), int(seg_e[sg]) - span

@@ -365,6 +365,7 @@ int g3x_ctx_destroy(g3x_ctx* c) {
     cudaFree(c->global.queue);
     cudaFree(c->sw.buf);
     cudaFree(c->sw.sub);
+    cudaFree(c->sw.flt);
     for (int k = 0; k < g3x::kMaxBuckets; ++k) {
         cudaStreamDestroy(c->side[k]);
         cudaEventDestroy(c->join[k]);

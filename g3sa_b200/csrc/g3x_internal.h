@@ -165,6 +165,8 @@ struct SwScratch {
     int32_t* buf = nullptr;
     uint32_t* sub = nullptr;
     int64_t cap = 0, sub_cap = 0;
+    uint8_t* flt = nullptr;        // the seed filter: its jobs, results and per-read values
+    int64_t flt_cap = 0;
 };
 SwScratch& ctx_sw(g3x_ctx* ctx);
 // The context's job order by decreasing row count and row width (its scheduling scratch).

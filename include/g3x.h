@@ -439,6 +439,26 @@ int g3x_ksw_align2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t
                          const uint32_t *d_codes, const uint32_t *d_nmask, int32_t xtra, int32_t max_tlen,
                          g3x_swr_t *d_out, int32_t *d_status, void *stream);
 
+/* The seed filter of long reads: mem_flt_chained_seeds (bwa/src/aux.cu:145-162) for every read,
+   as CHAINFILTERING_flt_chained_seeds_kernel runs it (aux.cu:1991-2030), with the window score
+   of mem_seed_sw (aux.cu:117-143).  A read is left alone when min_l = 1.1 * min_chain_weight
+   (5.5 * logf(l_query) when min_chain_weight is 0) exceeds 0.05 * l_query; otherwise each seed
+   shorter than 200 bases whose window (the seed +-50 bases on the read and the reference,
+   clipped to the read, to [0, 2 l_pac), to the strand and the contig of the seed's middle) is
+   below 200 bases on both gets the score of ksw_align2 over that window, and each chain keeps,
+   in order, the seeds without a window (their score becoming len * a) and those scoring at least
+   (int)(a * min_l + .499).  d_chains[].n and d_seeds are changed in place, as the reference
+   changes its chains; the same layout rules as g3x_chain2aln (a read's chains contiguous, their
+   seeds within the seed array).  d_sw_score (optional): per seed its window score, -1 without a
+   window, -2 for seeds of reads left alone.  d_status[r]: G3X_OK, or G3X_ERR_INVALID for a read
+   whose records lie outside their arrays (its chains untouched).  Only the score of ksw_align2
+   is used, which its first pass alone decides, so the start-position pass is not run.  Scratch
+   in the context; asynchronous on `stream`. */
+int g3x_flt_chained_seeds(g3x_ctx *ctx, const g3x_opt_t *opt, int32_t min_chain_weight, const g3x_refinfo_t *ref,
+                          const g3x_read_t *d_reads, int32_t n_reads, g3x_chain_t *d_chains, int32_t n_chains,
+                          g3x_cseed_t *d_seeds, int32_t n_seeds, const uint32_t *d_codes, const uint32_t *d_nmask,
+                          int32_t *d_sw_score, int32_t *d_status, void *stream);
+
 /* ---- host-resident batches, pipelined --------------------------------------------------- */
 /* No counterpart in the reference (its batches stay on the device between pipeline stages).
    A pipe extends batches of jobs that live in host memory with the context's schedule and

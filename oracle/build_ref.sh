@@ -8,7 +8,8 @@
 # stage (bwa/src/aux.cu:2830-2861), the striped local alignment ksw_align2 with ksw_qinit and
 # ksw_i16 (bwa/src/ksw.cu:5, 18-292 less its trap line 276; bwa/src/ksw.h:7-29), the pair
 # preparation of the traceback stage (bwa/src/aux.cu:506-513, 2698-2737; bwa/src/bntseq.cu:5,
-# 39-60), plus the ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
+# 39-60), the seed filter of long reads (bwa/src/aux.cu:117-162 with bwa/src/bntseq.cu:7-87),
+# plus the ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
 # reference tree into the compiler; no reference source is copied into this repository.
 # Usage: sh oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -eu
@@ -130,9 +131,30 @@ fi
 { cat "$HERE/ref_tbpair_head.inc"; sed -n '5p;39,60p' "$BNS"; sed -n '506,513p' "$AUX"; cat "$HERE/ref_tbpair_mid.inc"; \
   sed -n '2698,2737p' "$AUX"; cat "$HERE/ref_tbpair_tail.inc"; } | tr -d '\r' | \
     $CXX -O3 -fPIC -std=c++17 -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/tbpair_ref_fn.o"
+# The seed filter of long reads: the MEM_SHORT_* / MEM_*_COEF constants (aux.cuh), ksw.h:7-31
+# (flags, types, the ksw_align2 prototype), bntseq.cu:5, 7-87 (the window fetch) and
+# aux.cu:117-162 (mem_seed_sw, mem_flt_chained_seeds) between ref_seedflt_head.inc and
+# ref_seedflt_tail.inc; the call to ksw_align2 links to the unit above.
+F117=$(sed -n '117p' "$AUX" | tr -d '\r' | cut -c1-27)
+F143=$(sed -n '143p' "$AUX" | tr -d '\r')
+F145=$(sed -n '145p' "$AUX" | tr -d '\r' | cut -c1-38)
+F162=$(sed -n '162p' "$AUX" | tr -d '\r')
+H31=$(sed -n '31p' "$KSWH" | tr -d '\r' | cut -c1-29)
+if [ "$F117" != "__device__ int mem_seed_sw(" ] || [ "$F143" != "}" ] || \
+   [ "$F145" != "__device__ void mem_flt_chained_seeds(" ] || [ "$F162" != "}" ] || \
+   [ "$H31" != "__device__ kswr_t ksw_align2(" ]; then
+    echo "build_ref.sh: unexpected content at aux.cu:117/143/145/162 or ksw.h:31; refusing to build" >&2
+    exit 3
+fi
+{ cat "$HERE/ref_seedflt_head.inc"; \
+  grep -m1 '^#define MEM_SHORT_EXT' "$AUXH"; grep -m1 '^#define MEM_SHORT_LEN' "$AUXH"; \
+  grep -m1 '^#define MEM_HSP_COEF' "$AUXH"; grep -m1 '^#define MEM_MINSC_COEF' "$AUXH"; \
+  grep -m1 '^#define MEM_SEEDSW_COEF' "$AUXH"; sed -n '7,31p' "$KSWH"; sed -n '5p;7,87p' "$BNS"; \
+  sed -n '117,162p' "$AUX"; cat "$HERE/ref_seedflt_tail.inc"; } | tr -d '\r' | \
+    $CXX -O3 -fPIC -std=c++17 -x c++ -include "$HERE/ref_shim.h" -c - -o "$OUT/seedflt_ref_fn.o"
 $CXX -O3 -fPIC -shared -std=c++17 "$HERE/ref_wrap.cpp" "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" \
     "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o" "$OUT/sw_ref_fn.o" "$OUT/tbpair_ref_fn.o" \
-    -o "$OUT/libksw_ref.so" -lpthread
+    "$OUT/seedflt_ref_fn.o" -o "$OUT/libksw_ref.so" -lpthread
 rm -f "$OUT/ksw_ref_fn.o" "$OUT/seed_ref_fn.o" "$OUT/chain_ref_fn.o" "$OUT/global_ref_fn.o" "$OUT/nmmd_ref_fn.o" \
-    "$OUT/sw_ref_fn.o" "$OUT/tbpair_ref_fn.o"
+    "$OUT/sw_ref_fn.o" "$OUT/tbpair_ref_fn.o" "$OUT/seedflt_ref_fn.o"
 echo "built $OUT/libksw_ref.so"

@@ -23,6 +23,7 @@
 #include <string.h>
 #include <pthread.h>
 #include <stdio.h>
+#include <math.h>
 
 typedef struct { int32_t h, e; } g3o_eh;          /* ksw.cu:299-301 */
 
@@ -948,5 +949,78 @@ void g3o_tb_pairs(const g3o_tbopt *opt, const uint8_t *codes, int64_t ref_off, i
         }
         w[k] = (uint16_t)bw;
         rb_out[k] = g->rb;
+    }
+}
+
+/* ---------------------------------------------------------------------------------- */
+/* The seed filter of long reads: mem_seed_sw (aux.cu:117-143) and                      */
+/* mem_flt_chained_seeds (aux.cu:144-162, as CHAINFILTERING_flt_chained_seeds_kernel      */
+/* runs it per read, aux.cu:1991-2030).                                                  */
+/* ---------------------------------------------------------------------------------- */
+
+#define G3O_SHORT_EXT 50            /* MEM_SHORT_EXT, aux.cuh:396 */
+#define G3O_SHORT_LEN 200           /* MEM_SHORT_LEN, aux.cuh:397 */
+
+/* The local alignment score of the window around a short seed, or -1 when the seed or its
+   window is long enough to skip it (aux.cu:117-143): the seed +-50 bases on the read and on
+   the reference (clipped to the read, to [0, 2 l_pac) and to the strand of the seed's middle),
+   both below 200 bases, the reference window clipped to the contig of the middle
+   (bns_fetch_seq_gpu), then ksw_align2 with KSW_XSTART; only the score is used.  *cells (may
+   be NULL) grows by the cells of both passes. */
+int g3o_seed_sw(const g3o_opt *opt, const uint8_t *codes, int64_t ref_off, int64_t l_pac, const g3o_ann *anns,
+                int n_seqs, int l_query, const uint8_t *query, const g3o_cseed *s, int64_t *cells)
+{
+    if (s->len >= G3O_SHORT_LEN) return -1;
+    int qb = s->qbeg, qe = s->qbeg + s->len;
+    int64_t rb = s->rbeg, re = s->rbeg + s->len;
+    const int64_t mid = (rb + re) >> 1;
+    qb -= G3O_SHORT_EXT; if (qb < 0) qb = 0;
+    qe += G3O_SHORT_EXT; if (qe > l_query) qe = l_query;
+    rb -= G3O_SHORT_EXT; if (rb < 0) rb = 0;
+    re += G3O_SHORT_EXT; if (re > l_pac << 1) re = l_pac << 1;
+    if (rb < l_pac && l_pac < re) {
+        if (mid < l_pac) re = l_pac; else rb = l_pac;
+    }
+    if (qe - qb >= G3O_SHORT_LEN || re - rb >= G3O_SHORT_LEN) return -1;
+    g3o_clip_window(anns, n_seqs, l_pac, &rb, mid, &re);
+    const int tlen = (int)(re - rb);
+    int64_t nc = 0;
+    const g3o_swr x = g3o_ksw_align2(qe - qb, query + qb, tlen > 0 ? tlen : 0, codes + ref_off + rb, opt->mat,
+                                     opt->o_del, opt->e_del, opt->o_ins, opt->e_ins, G3O_XSTART, &nc);
+    if (cells) *cells += nc;
+    return x.score;
+}
+
+/* mem_flt_chained_seeds for every read: reads whose min_l = 1.1 * min_chain_weight (or, with
+   no minimum chain weight, 5.5 * logf(l_query)) exceeds 0.05 * l_query are left alone;
+   otherwise every seed of every chain gets its window score, and a chain keeps, in order, the
+   seeds whose score is -1 (their score becoming len * a) or at least
+   (int)(a * min_l + .499).  chains[].n and the seeds are changed in place; sw_score[i]
+   receives seed i's window score (-2 for seeds of reads left alone). */
+void g3o_flt_chained_seeds(const g3o_opt *opt, int min_chain_weight, const uint8_t *codes, int64_t ref_off,
+                           int64_t l_pac, const g3o_ann *anns, int n_seqs, const g3o_read *reads, int64_t n_reads,
+                           g3o_chain *chains, g3o_cseed *seeds, int32_t *sw_score, int64_t *cells)
+{
+    for (int64_t r = 0; r < n_reads; ++r) {
+        const g3o_read *rd = &reads[r];
+        const int lq = rd->l_query;
+        const double min_l = min_chain_weight ? 1.1f * min_chain_weight : 5.5f * logf((float)lq);
+        const int min_hsp = (int)(opt->a * min_l + .499);
+        if (min_l > 0.05f * lq) continue;
+        for (int c = 0; c < rd->n_chains; ++c) {
+            g3o_chain *ch = &chains[rd->chain_beg + c];
+            g3o_cseed *sd = seeds + ch->seed_beg;
+            int k = 0;
+            for (int j = 0; j < ch->n; ++j) {
+                g3o_cseed s = sd[j];
+                s.score = g3o_seed_sw(opt, codes, ref_off, l_pac, anns, n_seqs, lq, codes + rd->read_off, &s, cells);
+                if (sw_score) sw_score[ch->seed_beg + j] = s.score;
+                if (s.score < 0 || s.score >= min_hsp) {
+                    if (s.score < 0) s.score = s.len * opt->a;
+                    sd[k++] = s;
+                }
+            }
+            ch->n = k;
+        }
     }
 }

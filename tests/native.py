@@ -52,6 +52,8 @@ def oracle():
         _oracle.g3o_sw_batch.restype = None
         _oracle.g3o_tb_pairs.argtypes = [P, P, I64, I64, P, P, P, I64, P, P, P, ctypes.c_int32, P, P, P]
         _oracle.g3o_tb_pairs.restype = None
+        _oracle.g3o_flt_chained_seeds.argtypes = [P, ctypes.c_int, P, I64, I64, P, ctypes.c_int, P, I64, P, P, P, P]
+        _oracle.g3o_flt_chained_seeds.restype = None
     return _oracle
 
 
@@ -76,6 +78,8 @@ def ref():
         _ref.g3r_sw_batch.restype = ctypes.c_int
         _ref.g3r_tb_pairs.argtypes = [P, P, I64, I64, P, P, P, I64, P, P, P, ctypes.c_int32, P, P, P]
         _ref.g3r_tb_pairs.restype = ctypes.c_int
+        _ref.g3r_flt_chained_seeds.argtypes = [P, ctypes.c_int, P, I64, I64, P, ctypes.c_int, P, I64, P, P]
+        _ref.g3r_flt_chained_seeds.restype = ctypes.c_int
     return _ref
 
 
@@ -480,3 +484,27 @@ def oracle_tb_pairs(opt, u8, ref_off, l_pac, reads, regs, recs, tstride):
 def ref_tb_pairs(opt, u8, ref_off, l_pac, reads, regs, recs, tstride):
     """The same from the reference's own FINALIZEALN_preprocessing2 lines (aux.cu:2698-2737)."""
     return _tb(ref().g3r_tb_pairs, opt, u8, ref_off, l_pac, reads, regs, recs, tstride)
+
+
+def oracle_flt_seeds(wl, opt, min_chain_weight=0):
+    """(chains, seeds, window scores, cells) after the C restatement of mem_flt_chained_seeds:
+    copies of the workload's chain and seed arrays, changed as the reference changes them in
+    place; window score -1 for seeds it skips, -2 for seeds of reads it leaves alone."""
+    ch, sd = wl.chains.copy(), wl.seeds.copy()
+    sw = np.full(max(len(sd), 1), -2, np.int32)
+    cells = np.zeros(1, np.int64)
+    oracle().g3o_flt_chained_seeds(opt.ctypes.data, int(min_chain_weight), wl.u8.ctypes.data, int(wl.ref_off),
+                                   int(wl.l_pac), np.ascontiguousarray(wl.anns).ctypes.data, len(wl.anns),
+                                   np.ascontiguousarray(wl.reads).ctypes.data, len(wl.reads), ch.ctypes.data,
+                                   sd.ctypes.data, sw.ctypes.data, cells.ctypes.data)
+    return ch, sd, sw[:len(sd)], int(cells[0])
+
+
+def ref_flt_seeds(wl, opt, min_chain_weight=0):
+    """(chains, seeds) after the reference's own mem_flt_chained_seeds (aux.cu:145-162)."""
+    ch, sd = wl.chains.copy(), wl.seeds.copy()
+    ref().g3r_flt_chained_seeds(opt.ctypes.data, int(min_chain_weight), wl.u8.ctypes.data, int(wl.ref_off),
+                                int(wl.l_pac), np.ascontiguousarray(wl.anns).ctypes.data, len(wl.anns),
+                                np.ascontiguousarray(wl.reads).ctypes.data, len(wl.reads), ch.ctypes.data,
+                                sd.ctypes.data)
+    return ch, sd
