@@ -5,7 +5,8 @@
 // scheduler's counting sort); a warp takes 32 consecutive ones and runs their target rows
 // together (row i of every job in the same step); in a row each lane walks its own band
 // [max(i-w, 0), min(i+w+1, qlen)) column by column (the reference's scalar recurrence, in int32
-// with -2^30 outside the band, ksw.cu:548).  The band has a fixed width and never trims, so the
+// with -2^30 outside the band, ksw.cu:548; see Ring for the int16 form of short batches).  The
+// band has a fixed width and never trims, so the
 // row buffer of H(i-1, j-1) and E(i, j) (ksw.cu:299-301) is a ring of R >= 2w+3 columns per lane
 // in shared memory: a row reads columns [beg, end) and writes column end, and a column enters
 // the ring either from the first row's fill (columns 0..w) or from the row end that precedes its
@@ -56,13 +57,45 @@ __device__ __forceinline__ bool put_uint(char* buf, int& l, int cap, int v) {
 
 __device__ __forceinline__ int32_t sbyte0(uint32_t x) { return (int32_t)(int8_t)(x & 0xFFu); }
 
+// The ring's H and E: int32 pairs with the reference's -2^30 outside the band, or, for batches
+// whose every value fits (compact_fits), int16 pairs in one word with -2^14 outside the band.
+// Every value outside the band is that constant plus a sum of scores and penalties, the same sum
+// in both forms, and every value inside stays above -2^13 while every value outside stays below
+// it: each comparison goes the same way in both, and a score from outside the band maps back to
+// the reference's -2^30 plus the same sum.
+template <bool C16> struct Ring;
+template <> struct Ring<false> {
+    static constexpr int32_t kNeg = kNegInf;
+    static constexpr int kSlotBytes = 8;
+    int2* p;
+    __device__ __forceinline__ int2 ld(int k) const { return p[k]; }
+    __device__ __forceinline__ void st(int k, int32_t h, int32_t e) const { p[k] = make_int2(h, e); }
+};
+template <> struct Ring<true> {
+    static constexpr int32_t kNeg = -0x4000;
+    static constexpr int kSlotBytes = 4;
+    uint32_t* p;
+    __device__ __forceinline__ int2 ld(int k) const {
+        const uint32_t v = p[k];
+        return make_int2((int32_t)(int16_t)(v & 0xFFFFu), (int32_t)v >> 16);
+    }
+    __device__ __forceinline__ void st(int k, int32_t h, int32_t e) const {
+        p[k] = (uint32_t)(uint16_t)h | ((uint32_t)e << 16);
+    }
+};
+
+template <bool C16>
 __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp) {
     extern __shared__ __align__(16) char smem[];
+    using RingT = Ring<C16>;
+    constexpr int32_t kNeg = RingT::kNeg;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int nq = (d.qmax + 7) / 8 + 1;                       // query words (8 codes each)
-    uint32_t* qn = reinterpret_cast<uint32_t*>(smem + (size_t)warp * ((size_t)nq * 128 + (size_t)d.ring * 256));
-    int2* he = reinterpret_cast<int2*>(qn + nq * 32);          // ring slot s of lane L: he[s*32 + L]
+    uint32_t* qn = reinterpret_cast<uint32_t*>(
+        smem + (size_t)warp * ((size_t)nq * 128 + (size_t)d.ring * 32 * RingT::kSlotBytes));
+    RingT he;                                                   // ring slot s of lane L: index s*32 + L
+    he.p = reinterpret_cast<decltype(he.p)>(qn + nq * 32);
     const int wslot = blockIdx.x * (blockDim.x >> 5) + warp;
     uint8_t* z = d.z + (int64_t)wslot * d.zwarp;
     uint32_t lo[5], hi[5];
@@ -93,7 +126,7 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
                 // the first row (ksw.cu:721-724): columns 0..min(w, qlen)
                 const int top = qlen < w ? qlen : w;
                 for (int j = 0; j <= top; ++j)
-                    he[(j % R) * 32 + lane] = make_int2(j == 0 ? 0 : -(oe_ins + sp.e_ins * (j - 1)), kNegInf);
+                    he.st((j % R) * 32 + lane, j == 0 ? 0 : -(oe_ins + sp.e_ins * (j - 1)), kNeg);
             }
         }
         __syncwarp();
@@ -103,11 +136,11 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
             const bool run = live && i < tlen;
             int beg = 0, end = 0;
             uint32_t plo = 0, phi = 0;
-            int32_t h1 = kNegInf, f = kNegInf;
+            int32_t h1 = kNeg, f = kNeg;
             if (run) {
                 beg = i > w ? i - w : 0;
                 end = i + w + 1 < qlen ? i + w + 1 : qlen;
-                h1 = beg == 0 ? -(sp.o_del + sp.e_del * (i + 1)) : kNegInf;
+                h1 = beg == 0 ? -(sp.o_del + sp.e_del * (i + 1)) : kNeg;
                 if ((i & 15) == 0) load16(d.codes, d.nmask, t_off, tlen, i >> 4, trev, tx, tn);
                 uint32_t code = (tx >> ((i & 15) << 1)) & 3u;
                 if ((tn >> (i & 15)) & 1u) code = 4;
@@ -123,7 +156,7 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
                     const int j = beg + t;
                     if (t == 0 || (j & 7) == 0) qw = qn[(j >> 3) * 32 + lane];
                     const int32_t sc = sbyte0(__byte_perm(plo, phi, (qw >> ((j & 7) << 2)) & 0xFu));
-                    int2 c = he[s * 32 + lane];
+                    int2 c = he.ld(s * 32 + lane);
                     const int32_t m = c.x + sc;
                     int32_t e = c.y;
                     c.x = h1;
@@ -135,7 +168,7 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
                     e -= sp.e_del;
                     if (e > tt) dir |= 1u << 2; else e = tt;
                     c.y = e;
-                    he[s * 32 + lane] = c;
+                    he.st(s * 32 + lane, c.x, c.y);
                     tt = m - oe_ins;
                     f -= sp.e_ins;
                     if (f > tt) dir |= 2u << 4; else f = tt;
@@ -143,16 +176,17 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
                     s = s + 1 == R ? 0 : s + 1;
                 }
             }
-            if (run) he[(end % R) * 32 + lane] = make_int2(h1, kNegInf);   // ksw.cu:779
+            if (run) he.st((end % R) * 32 + lane, h1, kNeg);   // ksw.cu:779
             __syncwarp();
         }
         // score and backtrack (ksw.cu:781-806)
         if (live) {
             // H of column qlen: written by the last row's end when its band reaches qlen, else
             // still the first row's value
-            const int32_t init = qlen == 0 ? 0 : (qlen <= w ? -(oe_ins + sp.e_ins * (qlen - 1)) : kNegInf);
-            const int32_t score = tlen > 0 && tlen + w >= qlen ? he[(qlen % R) * 32 + lane].x : init;
-            d.score[job] = score;
+            const int32_t init = qlen == 0 ? 0 : (qlen <= w ? -(oe_ins + sp.e_ins * (qlen - 1)) : kNeg);
+            const int32_t score = tlen > 0 && tlen + w >= qlen ? he.ld((qlen % R) * 32 + lane).x : init;
+            const bool finite = score > kNeg / 2;
+            d.score[job] = finite ? score : kNegInf + (score - kNeg);
             uint32_t* cg = d.cigar + (int64_t)job * d.stride;
             int n = 0;
             bool full = false;
@@ -162,7 +196,7 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
                 else full = true;
             };
             bool bad = false;
-            if (score > kNegInf / 2) {
+            if (finite) {
                 int i = tlen - 1, k = (i + w + 1 < qlen ? i + w + 1 : qlen) - 1, which = 0;
                 while (i >= 0 && k >= 0 && !full) {
                     const int bi = i > w ? i - w : 0;
@@ -264,15 +298,23 @@ extern "C" int g3x_ksw_global2_batch(g3x_ctx* ctx, const g3x_score_t* score, con
     d.ncol = std::max(1, std::min(d.qmax, 2 * max_w + 1));
     d.ring = ((2 * max_w + 3) + 3) & ~3;
     d.stride = cigar_stride;
+    // int16 ring when every value of the batch fits: |inside-band values| <= bound <= 8000
+    int max_abs = 0;
+    for (int k = 0; k < 25; ++k) max_abs = std::max(max_abs, std::abs((int)sp.mat[k]));
+    const int64_t bound = 2 * (int64_t)std::max(sp.o_del, sp.o_ins) +
+                          (int64_t)std::max(sp.e_del, sp.e_ins) * (d.qmax + d.tmax + 2) +
+                          (int64_t)max_abs * (std::min(d.qmax, d.tmax) + 1);
+    const bool c16 = bound <= 8000;
+    auto kern = c16 ? global_kernel<true> : global_kernel<false>;
     const int nq = (d.qmax + 7) / 8 + 1;
-    const size_t warp_smem = (size_t)nq * 128 + (size_t)d.ring * 256;
+    const size_t warp_smem = (size_t)nq * 128 + (size_t)d.ring * 32 * (c16 ? 4 : 8);
     size_t max_smem = 0;
-    if (allow_max_smem(global_kernel, &max_smem) != cudaSuccess) return G3X_ERR_CUDA;
+    if (allow_max_smem(kern, &max_smem) != cudaSuccess) return G3X_ERR_CUDA;
     if (warp_smem > max_smem) return G3X_ERR_TOO_LONG;
     const int wpb = 2 * warp_smem <= max_smem ? 2 : 1;
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, global_kernel, 32 * wpb, wpb * warp_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, wpb * warp_smem);
     int blocks = sms * std::max(per_sm, 1);
     // direction bytes: tmax rows x ncol columns x 32 lanes per resident warp, at most 8 GiB
     d.zwarp = (int64_t)d.tmax * d.ncol * 32;
@@ -294,6 +336,6 @@ extern "C" int g3x_ksw_global2_batch(g3x_ctx* ctx, const g3x_score_t* score, con
     const cudaStream_t st = (cudaStream_t)stream;
     if ((rc = cost_order(ctx, d_jobs, n, sp, st, &d.order))) return rc;
     if (cudaMemsetAsync(gs.queue, 0, sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
-    global_kernel<<<blocks, 32 * wpb, wpb * warp_smem, st>>>(d, sp);
+    kern<<<blocks, 32 * wpb, wpb * warp_smem, st>>>(d, sp);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }

@@ -111,3 +111,37 @@ def test_gpu_global_nm_md():
     md = d_md.cpu().numpy().reshape(n, md_stride)
     md2 = [bytes(md[k]).split(b"\0")[0].decode() for k in range(n)]
     assert md2 == md1
+
+
+@pytest.mark.parametrize("long_len", [0, 3500])
+def test_gpu_global_both_ring_forms(long_len):
+    """Short batches keep H and E as int16 pairs (-2^14 outside the band), batches with long
+    sequences as int32 pairs (the reference's -2^30): both equal the oracle, scores from outside
+    the band included (jobs whose band misses the last cell)."""
+    cj, u8 = nat.global_jobs(1500, 21 + long_len, max_len=120, ws=(0, 1, 3, 10, 40))
+    if long_len:
+        rng = np.random.default_rng(long_len)
+        extra = []
+        for k in range(6):
+            q = rng.integers(0, 4, long_len - 300 * k).astype(np.uint8)
+            t = q.copy()
+            t[rng.integers(0, len(t), 40)] = rng.integers(0, 4, 40)
+            extra.append((q, t[: len(t) - 20 * k]))
+        off = len(u8)
+        ej = np.zeros(len(extra), cj.dtype)
+        parts = [u8]
+        for k, (q, t) in enumerate(extra):
+            ej[k]["q_off"], ej[k]["t_off"], ej[k]["qlen"], ej[k]["tlen"], ej[k]["w"] = off, off + len(q), len(q), len(t), 60
+            parts += [q, t]
+            off += len(q) + len(t)
+        cj, u8 = np.concatenate([cj, ej]), np.concatenate(parts)
+    # a few jobs whose band cannot reach the last cell: query much longer than target + w
+    out_of_band = (cj["qlen"] > cj["tlen"] + cj["w"])
+    stride = int((cj["qlen"] + cj["tlen"]).max()) + 2
+    s1, c1, n1, _ = nat.oracle_global(cj, u8, g.default_score(), stride)
+    s2, c2, n2, st = run_global(gpu_jobs(cj), u8, stride)
+    assert (st == 0).all(), np.unique(st)
+    assert np.array_equal(s1, s2)
+    assert np.array_equal(n1, n2)
+    assert all(np.array_equal(c1[k, :n1[k]], c2[k, :n2[k]]) for k in range(len(cj)))
+    assert out_of_band.any() and (s1[out_of_band] < -(1 << 29)).any()
