@@ -1,7 +1,8 @@
 """Benchmark of the B200 ksw_extend2 batch path (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cfg2|cfg1|cfg4] [--schedule auto|plain|sorted|learned]
+                    [--workload cfg2|cfg1|cfg4|chains|global|seedsw]
+                    [--schedule auto|plain|sorted|learned]
 
 A step extends every job of one synthetic batch once: the uneven left+right extension
 workload (about 1M jobs from 500k seeds on 100/150/250 bp reads, 20% unrelated targets,
@@ -16,6 +17,12 @@ step), so scaling is weak and `value` is the sum over ranks / the slowest rank's
 --impl reference times the reference's own CPU ksw_extend2 (oracle/_ref, compiled from
 bwa/src/ksw.cu) on all host threads over the same workload, or the C restatement of it
 when oracle/_ref is absent.
+
+The other workloads measure the rows around the extension, each against the reference's own
+CPU code for it: `chains` the chain-level call (g3x_chain2aln, mem_chain2aln over 60k reads),
+`global` banded global alignment with backtrack (g3x_ksw_global2_batch, ksw_global2 over 200k
+region pairs), `seedsw` the striped local alignment (g3x_ksw_align2_batch, ksw_align2 over
+200k seed windows).
 """
 import argparse
 import json
