@@ -167,7 +167,8 @@ __device__ __forceinline__ void sw_rows(const SwDesc& d, bool live, int tlen, Ro
         }
         // lazy F (ksw.cu:209-220): at most 16 rounds of the F vector moved up one cell, then
         // H = max(H, F) segment by segment, E untouched, until a segment where no cell's F - e
-        // beats its H - (o + e).  One ballot per segment gives every quad its stop.
+        // beats its H - (o + e).  One ballot per segment gives every quad its stop; the warp
+        // looks for the end every other segment (a stopped quad's steps change nothing).
         f = run ? f : 0u;
         // A quad that stops gets F = 0, which leaves its H unchanged and keeps it stopped; a quad
         // whose first segment is later (not UNI) waits with its F; the warp leaves when no quad
@@ -191,7 +192,7 @@ __device__ __forceinline__ void sw_rows(const SwDesc& d, bool live, int tlen, Ro
             }                                                                                        \
             const unsigned bal = __ballot_sync(kFull, go);                                           \
             if (at && !(bal & qmask)) f = 0u;                                                        \
-            if (!bal) goto lazy_done;                                                                \
+            if ((S & 1) && !bal) goto lazy_done;                                                     \
         }
                 G3X_SW_CASES(G3X_SW_LAZY)
 #undef G3X_SW_LAZY
