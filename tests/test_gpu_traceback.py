@@ -33,7 +33,7 @@ def gpu_pairs(wl, regs, recs, opt):
 def check_pairs(wl, regs, recs, opt, jobs, st):
     opt_cpu = nat.opt_from_score(g.default_score(), w=int(opt["w"][0]))
     q_off, qlen, tgt, tlen, w, rb = nat.oracle_tb_pairs(opt_cpu, wl.u8, wl.ref_off, wl.l_pac, wl.reads, regs,
-                                                        recs, 1024)
+                                                        recs, 4096)
     ok = st == 0
     assert ok.all(), np.unique(st)
     assert np.array_equal(jobs["q_off"], q_off) and np.array_equal(jobs["qlen"], qlen)
@@ -57,6 +57,7 @@ def test_gpu_traceback_pairs_match_oracle(seed, edge):
     jobs, st = gpu_pairs(wl, allregs, allrecs, opt)
     check_pairs(wl, allregs, allrecs, opt, jobs, st)
     assert (jobs["w"] > 0).any() and (jobs["w"] == 0).any() and (jobs["tlen"] == 0).any()
+    assert (jobs["w"] == 500).any()                      # the band cap of traceback_baseline
 
 
 def test_gpu_traceback_pairs_reject_bad_records():

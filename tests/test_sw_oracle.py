@@ -45,3 +45,17 @@ def test_oracle_sw_equals_reference(seed):
         assert bad.size == 0, f"xtra {x:#x}: jobs {bad[:5]}"
         rows = cj["tlen"] > 0                  # every pass enters at least one target row
         assert (cells[rows] >= cj["qlen"][rows]).all()
+
+
+@pytest.mark.skipif(not nat.have_ref(), reason="oracle/_ref not built (no reference tree)")
+def test_oracle_sw_long_queries_equal_reference():
+    """Queries of 257-500 bases (KSW_MAX_QLEN, bwa/src/ksw.h:11; beyond the GPU kernel's 256):
+    the restatement still equals the reference, so the GPU limit is the kernel's, not the
+    oracle's."""
+    cj, u8 = nat.sw_jobs(300, 0xB16, flank=200, seed_len=(60, 120), max_q=500)
+    assert cj["qlen"].max() > 256
+    sc = g.default_score()
+    for x in (0, nat.KSW_XSTART | nat.KSW_XSUBO | 30):
+        a, _ = nat.oracle_sw(cj, u8, sc, x)
+        b = nat.ref_sw(cj, u8, sc, x)
+        assert np.array_equal(a, b), hex(x)

@@ -23,6 +23,8 @@ def edge_regions(wl, first, n, seed):
         regs[k]["rb"], regs[k]["re"] = rb, rb + ln
         if k % 7 == 0:                                   # spans the forward/reverse boundary
             regs[k]["rb"], regs[k]["re"] = wl.l_pac - 20, wl.l_pac + 30
+        if k % 11 == 5:                                  # far longer than the query: band > 500
+            regs[k]["re"] = regs[k]["rb"] + int(rng.integers(1500, 3000))
         qb = int(rng.integers(0, 50))
         ql = ln if (k % 5 == 0 and ln > 0) else int(rng.integers(1, 200))   # equal lengths every fifth
         regs[k]["qb"], regs[k]["qe"] = qb, qb + ql
@@ -40,12 +42,13 @@ def test_oracle_tb_pairs_equal_reference(seed, edge, w):
     recs = nat.tb_records(wl, nregs)
     extra, erecs = edge_regions(wl, len(regs), 500, seed)
     allregs, allrecs = np.concatenate([regs, extra]), np.concatenate([recs, erecs])
-    a = nat.oracle_tb_pairs(opt, wl.u8, wl.ref_off, wl.l_pac, wl.reads, allregs, allrecs, 1024)
-    b = nat.ref_tb_pairs(opt, wl.u8, wl.ref_off, wl.l_pac, wl.reads, allregs, allrecs, 1024)
+    a = nat.oracle_tb_pairs(opt, wl.u8, wl.ref_off, wl.l_pac, wl.reads, allregs, allrecs, 4096)
+    b = nat.ref_tb_pairs(opt, wl.u8, wl.ref_off, wl.l_pac, wl.reads, allregs, allrecs, 4096)
     for x, y, name in zip(a, b, ("q_off", "qlen", "tgt", "tlen", "w", "rb")):
         assert np.array_equal(x, y), name
     q_off, qlen, tgt, tlen, w, rb = a
     assert (w == 0).any() and (w > 0).any() and (tlen == 0).any() and (rb >= wl.l_pac).any()
+    assert (w > 500).any()                               # the traceback stage caps these at 500
 
 
 @pytest.mark.skipif(not nat.have_ref(), reason="oracle/_ref not built (no reference tree)")
@@ -58,7 +61,7 @@ def test_oracle_tb_pairs_other_scoring():
     recs = nat.tb_records(wl, nregs)
     extra, erecs = edge_regions(wl, len(regs), 400, 9)
     allregs, allrecs = np.concatenate([regs, extra]), np.concatenate([recs, erecs])
-    a = nat.oracle_tb_pairs(opt, wl.u8, wl.ref_off, wl.l_pac, wl.reads, allregs, allrecs, 1024)
-    b = nat.ref_tb_pairs(opt, wl.u8, wl.ref_off, wl.l_pac, wl.reads, allregs, allrecs, 1024)
+    a = nat.oracle_tb_pairs(opt, wl.u8, wl.ref_off, wl.l_pac, wl.reads, allregs, allrecs, 4096)
+    b = nat.ref_tb_pairs(opt, wl.u8, wl.ref_off, wl.l_pac, wl.reads, allregs, allrecs, 4096)
     for x, y, name in zip(a, b, ("q_off", "qlen", "tgt", "tlen", "w", "rb")):
         assert np.array_equal(x, y), name
