@@ -427,7 +427,6 @@ def run_global_workload(args, ws, rank):
     d_cig = torch.zeros(n * gstride, dtype=torch.int32, device=dev)
     d_nc = torch.zeros(n, dtype=torch.int32, device=dev)
     d_st = torch.zeros(n, dtype=torch.int32, device=dev)
-    h_out = [torch.zeros_like(x, device="cpu").pin_memory() for x in (d_score, d_cig, d_nc, d_st)]
     ctx = g.Context(local)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -450,15 +449,19 @@ def run_global_workload(args, ws, rank):
     ms = timed_steps(call, args.steps, args.warmup, stream, flush)
     clk = clocks.stop()
 
-    def e2e_step():
-        for k in d:
-            d[k].copy_(host[k], non_blocking=True)
-        call()
-        for h, x in zip(h_out, (d_score, d_cig, d_nc, d_st)):
-            h.copy_(x, non_blocking=True)
+    # end to end: two contexts, streams and buffer sets, so one batch's copies overlap the
+    # other's alignment
+    def run_g(cx, dd, outs, st):
+        cx.global_batch(sc, dd["jobs"], n, dd["codes"], dd["nmask"], mq, mt, mw, outs[0], outs[1], gstride,
+                        outs[2], outs[3], stream=st)
 
-    e2e_ms = timed_steps(e2e_step, max(3, args.steps // 4), args.warmup, stream, flush)
-    t, te = sum(ms) / len(ms), sum(e2e_ms) / len(e2e_ms)
+    submit, wait, sets = two_set_pipeline(lambda i: ctx if i == 0 else g.Context(local), host,
+                                          (d_score, d_cig, d_nc, d_st), run_g)
+    te = timed_pipeline(submit, wait, max(3, args.steps // 4), args.warmup, stream, flush)
+    torch.cuda.synchronize()
+    for st_, dd, outs, h_outs, cx in sets:     # both sets' last batches came back intact
+        exact = exact and np.array_equal(h_outs[0].numpy(), s_o) and bool((h_outs[3] == 0).all())
+    t = sum(ms) / len(ms)
     (t, te), (tot_cells, tot_n) = combine_ranks(dist, [t, te], [cells, n], dev)
     if rank != 0:
         return
@@ -466,14 +469,15 @@ def run_global_workload(args, ws, rank):
     cpu_t = ref_time() if nat.have_ref() else None
     gcups = tot_cells / (t * 1e-3) / 1e9
     bi = sum(v.numel() for v in host.values())
-    bo = sum(h.numel() * 4 for h in h_out)
+    bo = sum(h.numel() * h.element_size() for h in sets[0][3])
     print(json.dumps({
         "metric": metric, "value": round(gcups, 3), "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)", "config": cfg,
         "alignments_per_s": round(tot_n / (t * 1e-3), 1),
         "e2e": {"value": round(tot_cells / (te * 1e-3) / 1e9, 3), "unit": "GCUPS", "ms_per_step": round(te, 4),
-                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
+                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+                "overlap": "two contexts, streams and buffer sets: a batch's copies overlap the other set's batch"},
         "roofline": {"bound": "int_alu", "achieved": round(gcups / max(ws, 1), 3), "peak": round(peak_gcups, 3),
                      "unit": "GCUPS", "frac": round(gcups / max(ws, 1) / peak_gcups, 4), "traffic": None,
                      "note": "cells per second of the global kernel against the int-ALU cells/s peak (8 ops per cell)"},
@@ -562,7 +566,6 @@ def run_sw_workload(args, ws, rank):
     d = {k: v.to(dev) for k, v in host.items()}
     d_out = torch.zeros(n * 7, dtype=torch.int32, device=dev)
     d_st = torch.zeros(n, dtype=torch.int32, device=dev)
-    h_out = [torch.zeros_like(x, device="cpu").pin_memory() for x in (d_out, d_st)]
     ctx = g.Context(local)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -582,15 +585,15 @@ def run_sw_workload(args, ws, rank):
     ms = timed_steps(call, args.steps, args.warmup, stream, flush)
     clk = clocks.stop()
 
-    def e2e_step():
-        for k in d:
-            d[k].copy_(host[k], non_blocking=True)
-        call()
-        for h, x in zip(h_out, (d_out, d_st)):
-            h.copy_(x, non_blocking=True)
+    def run_s(cx, dd, outs, st):
+        cx.align2_batch(sc, dd["jobs"], n, dd["codes"], dd["nmask"], xtra, mt, outs[0], outs[1], stream=st)
 
-    e2e_ms = timed_steps(e2e_step, max(3, args.steps // 4), args.warmup, stream, flush)
-    t, te = sum(ms) / len(ms), sum(e2e_ms) / len(e2e_ms)
+    submit, wait, sets = two_set_pipeline(lambda i: ctx if i == 0 else g.Context(local), host, (d_out, d_st), run_s)
+    te = timed_pipeline(submit, wait, max(3, args.steps // 4), args.warmup, stream, flush)
+    torch.cuda.synchronize()
+    for st_, dd, outs, h_outs, cx in sets:     # both sets' last batches came back intact
+        exact = exact and np.array_equal(h_outs[0].numpy().view(g.SWR_DT), want) and bool((h_outs[1] == 0).all())
+    t = sum(ms) / len(ms)
     (t, te), (tot_cells, tot_n) = combine_ranks(dist, [t, te], [cells, n], dev)
     if rank != 0:
         return
@@ -598,14 +601,15 @@ def run_sw_workload(args, ws, rank):
     cpu_t = ref_time() if nat.have_ref() else None
     gcups = tot_cells / (t * 1e-3) / 1e9
     bi = sum(v.numel() for v in host.values())
-    bo = sum(h.numel() * 4 for h in h_out)
+    bo = sum(h.numel() * h.element_size() for h in sets[0][3])
     print(json.dumps({
         "metric": metric, "value": round(gcups, 3), "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int16x2", "data": "synthetic (seeded generator)", "config": cfg,
         "alignments_per_s": round(tot_n / (t * 1e-3), 1),
         "e2e": {"value": round(tot_cells / (te * 1e-3) / 1e9, 3), "unit": "GCUPS", "ms_per_step": round(te, 4),
-                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
+                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+                "overlap": "two contexts, streams and buffer sets: a batch's copies overlap the other set's batch"},
         "roofline": {"bound": "int_alu", "achieved": round(gcups / max(ws, 1), 3), "peak": round(peak_gcups, 3),
                      "unit": "GCUPS", "frac": round(gcups / max(ws, 1) / peak_gcups, 4), "traffic": None,
                      "note": "cells per second of the step against the int-ALU cells/s peak (8 ops per cell)"},
@@ -614,6 +618,40 @@ def run_sw_workload(args, ws, rank):
             "sample": "whole rank-0 workload, one pass, the reference's own ksw_align2 (trap line left out)"},
         "clocks": clk, "outputs_equal_oracle": exact, "gpu_launches": 6 * args.steps,
     }), flush=True)
+
+
+def two_set_pipeline(make_ctx, host, outs_like, run):
+    """A caller's pipeline over the public API: batches alternate between two contexts, each
+    with its own stream and device buffer set; batch k's host->device copies (pinned), its
+    call `run(ctx, d, outs, stream)` and its device->host copies are enqueued on its set's
+    stream, so they overlap the other set's batch.  Returns (submit, wait, sets) for
+    timed_pipeline; each set is (stream, d, outs, h_outs)."""
+    import torch
+    sets = []
+    for i in range(2):
+        st = torch.cuda.Stream()
+        d = {k: torch.empty(v.shape, dtype=v.dtype, device="cuda") for k, v in host.items()}
+        outs = [torch.empty_like(x) for x in outs_like]
+        h_outs = [torch.empty(x.shape, dtype=x.dtype).pin_memory() for x in outs]
+        sets.append((st, d, outs, h_outs, make_ctx(i)))
+    k = [0]
+
+    def submit():
+        st, d, outs, h_outs, cx = sets[k[0] % 2]
+        k[0] += 1
+        st.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(st):
+            for name in d:
+                d[name].copy_(host[name], non_blocking=True)
+            run(cx, d, outs, st)
+            for h, x in zip(h_outs, outs):
+                h.copy_(x, non_blocking=True)
+
+    def wait(stream):
+        for st in sets:
+            stream.wait_stream(st[0])
+
+    return submit, wait, sets
 
 
 def combine_ranks(dist, times, counts, device):
