@@ -75,16 +75,48 @@ def dist_setup():
 
 
 class ClockSampler:
-    """nvidia-smi SM clock / throttle-reason samples while the timed region runs."""
+    """SM clock / throttle-reason samples while the timed region runs: NVML read every 10 ms
+    from a thread (reads only), or nvidia-smi at 200 ms where NVML cannot be loaded."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, gpu):
         self.gpu, self.rows, self.proc = gpu, [], None
+        self.nvml, self.samples, self.stop_flag = None, [], threading.Event()
+
+    def _nvml_loop(self, nv, h):
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception:   # noqa: BLE001 -- a failed read is a missing sample
+                pass
+            self.stop_flag.wait(0.01)
 
     def start(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+            if len(vis) > self.gpu and vis[self.gpu].isdigit():         # the visible device's index
+                h = nv.nvmlDeviceGetHandleByIndex(int(vis[self.gpu]))
+            elif len(vis) > self.gpu and vis[self.gpu].startswith("GPU-"):
+                h = nv.nvmlDeviceGetHandleByUUID(vis[self.gpu])
+            else:
+                h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.nvml = nv
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            return
+        except Exception:   # noqa: BLE001 -- fall back to nvidia-smi
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
@@ -100,6 +132,22 @@ class ClockSampler:
             self.rows.append([x.strip() for x in line.split(",")])
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=2)
+            nv, reasons = self.nvml, set()
+            for _, _, bits in self.samples:
+                for name, const in self.REASONS:
+                    if bits & getattr(nv, const, 0):
+                        reasons.add(name)
+            sm = [c for c, _, _ in self.samples]
+            try:
+                nv.nvmlShutdown()
+            except Exception:   # noqa: BLE001
+                pass
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": max(m for _, m, _ in self.samples) if self.samples else None,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
