@@ -8,11 +8,19 @@
  *   - band-retry driver:      bwa/src/aux.cu:250-301   (left/right extension of one seed,
  *                                                       MAX_BAND_TRY = 2, aux.cuh:401)
  *   - cal_max_gap:            bwa/src/aux.cu:168-175
+ *   - mem_chain2aln:          bwa/src/aux.cu:178-315 with the window fetch of
+ *                             bwa/src/bntseq.cu:7-87
+ *   - ksw_global2 + NM/MD:    bwa/src/ksw.cu:694-809, bwa/src/aux.cu:2830-2861
+ *   - traceback pairs:        bwa/src/aux.cu:506-513, 2698-2745 (FINALIZEALN_preprocessing2)
+ *   - ksw_align2 (16-bit):    bwa/src/ksw.cu:18-64, 155-262, 271-292 (ksw_qinit, ksw_i16)
+ *   - seed filter:            bwa/src/aux.cu:117-162 (mem_seed_sw, mem_flt_chained_seeds)
  *
- * Parity pin: tests/test_oracle.py checks this restatement against the reference's own
- * ksw_extend2 compiled from its source (oracle/build_ref.sh -> oracle/_ref/libksw_ref.so)
- * on seeded jobs, and against the committed golden vectors in tests/golden/ that were
- * generated from that compiled reference.
+ * Parity pin: each restatement is checked against the reference's own lines compiled from
+ * its source (oracle/build_ref.sh -> oracle/_ref/libksw_ref.so) on seeded inputs and edge
+ * cases (tests/test_oracle.py, test_chain_oracle.py, test_global_oracle.py,
+ * test_tbpair_oracle.py, test_sw_oracle.py, test_seedflt_oracle.py), and against the
+ * committed golden vectors in tests/golden/ that were generated from that compiled
+ * reference.
  *
  * Extra output not present in the reference: the number of DP cells evaluated
  * (the trip count of the inner loop at ksw.cu:346, summed over the executed rows,
