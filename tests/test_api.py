@@ -80,7 +80,6 @@ def test_bad_arguments_return_codes(lib):
 def test_widened_entry_points_reject_bad_arguments(lib):
     """The entry points of the rows around the extension check their arguments before any CUDA
     call: no context, negative counts, missing buffers and refused flags return codes."""
-    P = ctypes.c_void_p
     sc = g.default_score()
     assert lib.g3x_ksw_global2_batch(None, sc.ctypes.data, None, 1, None, None, 10, 10, 5, None, None, 4, None,
                                      None, None, 0, None, None) == g.G3X_ERR_INVALID
