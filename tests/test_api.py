@@ -109,3 +109,17 @@ def test_ctx_without_gpu_is_an_error_not_a_crash(lib):
         pytest.skip("GPU present")
     h = ctypes.c_void_p()
     assert lib.g3x_ctx_create(ctypes.byref(h), 0) == g.G3X_ERR_CUDA
+
+
+@pytest.mark.parametrize("compiler,std", [("gcc", "-std=c99"), ("g++", "-std=c++11")])
+def test_header_compiles_as_c_and_cpp(tmp_path, compiler, std):
+    """include/g3x.h is a plain C header (the boundary a cgo / JNI / ctypes stub binds): it
+    compiles on its own as C99 and as C++11, without CUDA or torch headers."""
+    import shutil
+    import subprocess
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not installed")
+    src = tmp_path / ("probe.c" if compiler == "gcc" else "probe.cpp")
+    src.write_text('#include "g3x.h"\nint probe(void) { return G3X_OK + (int)sizeof(g3x_job_t); }\n')
+    subprocess.check_call([compiler, std, "-Wall", "-Werror", "-fsyntax-only",
+                           "-I", os.path.join(ROOT, "include"), str(src)])
