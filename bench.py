@@ -395,6 +395,11 @@ def run_chain_workload(args, ws, rank):
     }), flush=True)
 
 
+# DRAM bytes (read + write) per launch of the dominant kernel of each workload below, from ncu
+# captures of these workloads (global_kernel: 0.427 GB read + 1.010 GB written; sw_kernel<16>:
+# 18.9 MB read, nothing written back but the outputs)
+GLOBAL_DRAM_BYTES = 1_436_724_000
+SW_DRAM_BYTES = 18_913_024
 GLOBAL_JOBS = 200000
 GLOBAL_DESC = ("ksw_global2 with backtrack over 200k synthetic region pairs as the traceback stage issues "
                "them: query U[0,250) bases, target = query with up to 5 substitutions/1-base indels, 10% "
@@ -527,8 +532,11 @@ def run_global_workload(args, ws, rank):
                 "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                 "overlap": "two contexts, streams and buffer sets: a batch's copies overlap the other set's batch"},
         "roofline": {"bound": "int_alu", "achieved": round(gcups / max(ws, 1), 3), "peak": round(peak_gcups, 3),
-                     "unit": "GCUPS", "frac": round(gcups / max(ws, 1) / peak_gcups, 4), "traffic": None,
-                     "note": "cells per second of the global kernel against the int-ALU cells/s peak (8 ops per cell)"},
+                     "unit": "GCUPS", "frac": round(gcups / max(ws, 1) / peak_gcups, 4),
+                     "traffic": GLOBAL_DRAM_BYTES,
+                     "note": "cells per second of the global kernel against the int-ALU cells/s peak (8 ops per cell); "
+                             "traffic: DRAM bytes read + written by one global_kernel launch of this workload "
+                             "(an ncu capture of it): the direction bytes"},
         "cpu_baseline": None if cpu_t is None else {
             "value": round(cells / cpu_t / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
             "sample": "whole rank-0 workload, one pass, the reference's own ksw_global2"},
@@ -659,8 +667,11 @@ def run_sw_workload(args, ws, rank):
                 "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                 "overlap": "two contexts, streams and buffer sets: a batch's copies overlap the other set's batch"},
         "roofline": {"bound": "int_alu", "achieved": round(gcups / max(ws, 1), 3), "peak": round(peak_gcups, 3),
-                     "unit": "GCUPS", "frac": round(gcups / max(ws, 1) / peak_gcups, 4), "traffic": None,
-                     "note": "cells per second of the step against the int-ALU cells/s peak (8 ops per cell)"},
+                     "unit": "GCUPS", "frac": round(gcups / max(ws, 1) / peak_gcups, 4),
+                     "traffic": SW_DRAM_BYTES,
+                     "note": "cells per second of the step against the int-ALU cells/s peak (8 ops per cell); "
+                             "traffic: DRAM bytes of one sw_kernel<16> launch (the class with 83% of the cells) of "
+                             "this workload (an ncu capture of it): job headers and planes"},
         "cpu_baseline": None if cpu_t is None else {
             "value": round(cells / cpu_t / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
             "sample": "whole rank-0 workload, one pass, the reference's own ksw_align2 (trap line left out)"},
