@@ -176,6 +176,7 @@ __global__ void tb_pair_kernel(g3x_opt_t opt, int64_t l_pac, int64_t ref_off, co
     if (end > l_pac << 1) end = l_pac << 1;
     if (beg < 0) beg = 0;
     if (beg >= l_pac || end <= l_pac) rlen = end - beg;
+    if (rlen < 0) return;           // [rb, re) wholly outside [0, 2 l_pac): no slice (invalid)
     if (lq > 65535 || rlen > 65535) { status[i] = G3X_ERR_TOO_LONG; return; }
     // the band (aux.cu:2711-2737), stored as uint16 (aux.cu:2745), at most 500 (aux.cu:2812)
     int w = 0;

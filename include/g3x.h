@@ -377,8 +377,8 @@ typedef struct {
    |tlen - qlen| + 3, then kept as the reference's uint16 and capped at 500; G3X_JOB_MDRC when
    rb >= l_pac.  (The reference's reversal kernel FINALIZEALN_reverseSeq_kernel, aux.cu:
    2755-2790, writes reversed copies that nothing reads, so the slices go in as they are.)
-   d_status[i]: G3X_OK; G3X_ERR_INVALID for a record outside its arrays or a region with
-   qe < qb (empty job); G3X_ERR_TOO_LONG when a slice is longer than 65535 bases.  Asynchronous
+   d_status[i]: G3X_OK; G3X_ERR_INVALID for a record outside its arrays, a region with qe < qb
+   or one wholly outside [0, 2 l_pac) (empty job); G3X_ERR_TOO_LONG when a slice is longer than 65535 bases.  Asynchronous
    on `stream` (the current device). */
 int g3x_traceback_pairs(const g3x_opt_t *opt, const g3x_refinfo_t *ref, const g3x_read_t *d_reads,
                         int32_t n_reads, const g3x_alnreg_t *d_regs, int32_t n_regs,

@@ -16,7 +16,15 @@ Files:
     sw_<name>.npz     u8, jobs (JOB_DT), score, xtras (flag sets), out (flag sets x n kswr_t)
                       from the reference's own ksw_align2 (its trap line left out)
 
-`python tests/golden/make_golden.py --sw` rewrites the sw_ files only.
+    chains_<name>.npz the chain workload (u8, l_pac, anns, reads, chains, seeds), opt, and the
+                      reference's mem_chain2aln regions and counts
+    global_<name>.npz jobs, u8, score and the reference's ksw_global2 score, CIGAR, NM and MD
+    tbpairs_<name>.npz the chain workload, regions, records and the reference's pair preparation
+    seedflt_<name>.npz the chain workload with long reads, opt, min chain weight, and the chains
+                      and seeds after the reference's mem_flt_chained_seeds
+
+`python tests/golden/make_golden.py --sw` rewrites the sw_ files only, `--rows` the chains_,
+global_, tbpairs_ and seedflt_ files only.
 """
 import ctypes
 import os
@@ -210,6 +218,65 @@ def _gpu_jobs(cj):
     return jobs
 
 
+def _wl_arrays(wl):
+    return dict(u8=wl.u8, l_pac=np.int64(wl.l_pac), anns=wl.anns, reads=wl.reads, chains=wl.chains, seeds=wl.seeds)
+
+
+def save_chains(name, wl, opt):
+    regs, nregs = nat.ref_chains(wl, opt)
+    np.savez_compressed(os.path.join(HERE, f"chains_{name}.npz"), opt=opt, regs=regs, nregs=nregs, **_wl_arrays(wl))
+    print(f"chains_{name}: {len(wl.reads)} reads, {int(nregs.sum())} regions")
+    return regs, nregs
+
+
+def save_global(name, jobs, u8, score):
+    stride = int((jobs["qlen"] + jobs["tlen"]).max()) + 2
+    sc, cig, nc = nat.ref_global(jobs, u8, score, stride)
+    md_stride = 4 * stride + 16
+    nm, md = nat.ref_nm_md(jobs, u8, cig, nc, md_stride)
+    np.savez_compressed(os.path.join(HERE, f"global_{name}.npz"), jobs=jobs, u8=u8, score=score, out_score=sc,
+                        cigar=cig, n_cigar=nc, nm=nm, md=np.array(md, dtype=object).astype(str))
+    print(f"global_{name}: {len(jobs)} pairs")
+
+
+def save_tbpairs(name, wl, opt, regs, recs):
+    q_off, qlen, tgt, tlen, w, rb = nat.ref_tb_pairs(opt, wl.u8, wl.ref_off, wl.l_pac, wl.reads, regs, recs, 4096)
+    tcat = np.concatenate([tgt[k, :tlen[k]] for k in range(len(recs))]) if len(recs) else np.zeros(0, np.uint8)
+    np.savez_compressed(os.path.join(HERE, f"tbpairs_{name}.npz"), opt=opt, regs=regs, recs=recs, q_off=q_off,
+                        qlen=qlen, tgt=tcat, tlen=tlen, w=w, rb=rb, **_wl_arrays(wl))
+    print(f"tbpairs_{name}: {len(recs)} records")
+
+
+def save_seedflt(name, wl, opt, mcw):
+    ch, sd = nat.ref_flt_seeds(wl, opt, mcw)
+    np.savez_compressed(os.path.join(HERE, f"seedflt_{name}.npz"), opt=opt, mcw=np.int32(mcw), out_chains=ch,
+                        out_seeds=sd, **_wl_arrays(wl))
+    print(f"seedflt_{name}: {len(wl.reads)} reads, {int(ch['n'].sum())} of {int(wl.chains['n'].sum())} seeds kept")
+
+
+def rows_main():
+    """Golden vectors of the rows around the extension: chain level, global alignment with
+    NM/MD, traceback pairs, seed filter (small references so the files stay small)."""
+    from g3sa_b200.chains import synth_chains
+    from tests.test_tbpair_oracle import edge_regions
+    sc = g.default_score()
+    small = dict(n_contigs=4, contig_len=(6000, 16000))
+    wl = synth_chains(300, seed=0x6C, edge=0.3, **small)
+    opt = nat.opt_from_score(sc, w=100)
+    regs, nregs = save_chains("edge", wl, opt)
+    recs = nat.tb_records(wl, nregs)
+    extra, erecs = edge_regions(wl, len(regs), 200, 0x6C)
+    save_tbpairs("edge", wl, opt, np.concatenate([regs, extra]), np.concatenate([recs, erecs]))
+    cj, u8 = nat.global_jobs(600, 0x61, max_len=160)
+    save_global("mixed", cj, u8, sc)
+    sc2 = g.default_score(a=2, b=3, o_del=5, e_del=2, o_ins=4, e_ins=3)
+    cj, u8 = nat.global_jobs(300, 0x62, max_len=120, ws=(0, 2, 9, 30))
+    save_global("score2", cj, u8, sc2)
+    wl = synth_chains(80, seed=0x5F, read_lens=(100, 720, 750, 1000, 1500), div=0.03, edge=0.3, **small)
+    save_seedflt("long", wl, opt, 0)
+    save_seedflt("mcw", wl, opt, 25)
+
+
 def main():
     if not nat.have_ref():
         sys.exit("oracle/_ref/libksw_ref.so missing: run sh oracle/build_ref.sh first")
@@ -237,12 +304,16 @@ def main():
         wl = g.synth(2, 1500, seed=0x6A5 + 5 + w, w=w, unrelated=0.2)
         save_seeds(f"cfg5_w{w}", wl, nat.opt_from_score(sc, w=w))
     sw_main(np.random.default_rng(2026))
+    rows_main()
 
 
 if __name__ == "__main__":
-    if "--sw" in sys.argv:
+    if "--sw" in sys.argv or "--rows" in sys.argv:
         if not nat.have_ref():
             sys.exit("oracle/_ref/libksw_ref.so missing: run sh oracle/build_ref.sh first")
-        sw_main(np.random.default_rng(2026))
+        if "--sw" in sys.argv:
+            sw_main(np.random.default_rng(2026))
+        if "--rows" in sys.argv:
+            rows_main()
     else:
         main()

@@ -32,3 +32,20 @@ def sw_sets():
 def load_sw(name):
     z = np.load(os.path.join(GOLDEN, f"sw_{name}.npz"))
     return z["u8"], z["jobs"], z["score"], z["xtras"], z["out"]
+
+
+def load_rows(kind, name):
+    """The golden file of a row around the extension (chains_, global_, tbpairs_, seedflt_) as a
+    dict of arrays."""
+    z = np.load(os.path.join(GOLDEN, f"{kind}_{name}.npz"))
+    return {k: z[k] for k in z.files}
+
+
+def row_sets(kind):
+    return sorted(os.path.basename(p)[len(kind) + 1:-4] for p in glob.glob(os.path.join(GOLDEN, f"{kind}_*.npz")))
+
+
+def workload(d):
+    """The ChainWorkload stored in a golden file."""
+    from g3sa_b200.chains import ChainWorkload
+    return ChainWorkload(d["u8"], int(d["l_pac"]), d["anns"], d["reads"], d["chains"], d["seeds"])

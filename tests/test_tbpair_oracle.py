@@ -29,6 +29,9 @@ def edge_regions(wl, first, n, seed):
         ql = ln if (k % 5 == 0 and ln > 0) else int(rng.integers(1, 200))   # equal lengths every fifth
         regs[k]["qb"], regs[k]["qe"] = qb, qb + ql
         regs[k]["score"] = int(rng.integers(-10, 200))
+        lo, hi = sorted((int(regs[k]["rb"]), int(regs[k]["re"])))
+        if hi < 0 or lo >= L2:         # a slice wholly outside [0, 2 l_pac): the reference asks its
+            regs[k]["rb"], regs[k]["re"] = 0, 40   # arena for a negative size; not a region
     recs = np.stack([rng.integers(0, len(wl.reads), n), np.arange(first, first + n)], 1).astype(np.int32)
     return regs, recs
 
