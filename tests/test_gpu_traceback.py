@@ -62,9 +62,11 @@ def test_gpu_traceback_pairs_match_oracle(seed, edge):
 
 def test_gpu_traceback_pairs_reject_bad_records():
     wl = synth_chains(50, seed=2)
-    regs = np.zeros(3, ALNREG_DT)
+    regs = np.zeros(4, ALNREG_DT)
     regs["rb"], regs["re"], regs["qb"], regs["qe"] = 10, 40, 5, 2   # qe < qb
-    recs = np.array([[0, 0], [len(wl.reads), 1], [0, 7], [-1, 0]], np.int32)
+    L2 = 2 * wl.l_pac                                              # a slice wholly past the reference
+    regs[3]["rb"], regs[3]["re"], regs[3]["qb"], regs[3]["qe"] = L2 + 10, L2 + 50, 0, 10
+    recs = np.array([[0, 0], [len(wl.reads), 1], [0, 7], [-1, 0], [0, 3]], np.int32)
     jobs, st = gpu_pairs(wl, regs, recs, g.default_opt())
     assert (st == g.G3X_ERR_INVALID).all()
     assert (jobs["qlen"] == 0).all() and (jobs["tlen"] == 0).all()
