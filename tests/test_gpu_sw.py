@@ -108,3 +108,26 @@ def test_gpu_sw_rejects_bad_calls():
     got, st = run_sw(jobs[:0], u8, g.default_score(), 0)   # an empty batch is a no-op
     assert len(got) == 0
     torch.cuda.synchronize()
+
+
+def test_gpu_sw_edge_of_int16_domain():
+    """Cells up to 127 * 256 (+ one score) in int16 lanes: identical and mutated 256-base pairs
+    under a = 127 equal the oracle, the identical ones at exactly 127 * 256."""
+    rng = np.random.default_rng(0xE17)
+    parts, rows, off = [], [], 0
+    for k in range(64):
+        q = rng.integers(0, 4, 256 - (k % 5)).astype(np.uint8)
+        t = q.copy() if k % 2 == 0 else nat._mutate(rng, q, 0.03)[:256]
+        rows.append((off, off + len(q), len(q), len(t)))
+        parts += [q, t]
+        off += len(q) + len(t)
+    jobs = np.zeros(len(rows), g.JOB_DT)
+    jobs["q_off"], jobs["t_off"], jobs["qlen"], jobs["tlen"] = np.array(rows).T
+    u8 = np.concatenate(parts)
+    sc = g.default_score(a=127, b=1, o_del=1, e_del=1, o_ins=1, e_ins=1)
+    for x in (0, g.KSW_XSTART):
+        want, _ = nat.oracle_sw(nat.cpu_jobs(jobs), u8, sc, x)
+        got, st = run_sw(jobs, u8, sc, x)
+        assert (st == 0).all()
+        assert np.array_equal(got, want)
+        assert int(got["score"][0]) == 127 * 256

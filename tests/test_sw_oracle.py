@@ -59,3 +59,20 @@ def test_oracle_sw_long_queries_equal_reference():
         a, _ = nat.oracle_sw(cj, u8, sc, x)
         b = nat.ref_sw(cj, u8, sc, x)
         assert np.array_equal(a, b), hex(x)
+
+
+@pytest.mark.skipif(not nat.have_ref(), reason="oracle/_ref not built (no reference tree)")
+def test_oracle_sw_edge_of_int16_domain():
+    """The GPU kernel's domain (queries up to 256 bases, any int8 matrix) keeps every cell at most
+    127 * 256 + 127 < 2^15: the largest match score on identical 256-base sequences reaches
+    127 * 256 exactly, and the reference's wrapping int16 adds agree with the oracle there."""
+    rng = np.random.default_rng(0xE16)
+    q = rng.integers(0, 4, 256).astype(np.uint8)
+    u8 = np.concatenate([q, q])
+    jobs = np.zeros(1, nat.CPU_JOB_DT)
+    jobs["q_off"], jobs["t_off"], jobs["qlen"], jobs["tlen"] = 0, 256, 256, 256
+    sc = g.default_score(a=127, b=1, o_del=1, e_del=1, o_ins=1, e_ins=1)
+    for x in (0, nat.KSW_XSTART):
+        a, _ = nat.oracle_sw(jobs, u8, sc, x)
+        b = nat.ref_sw(jobs, u8, sc, x)
+        assert np.array_equal(a, b) and int(a["score"][0]) == 127 * 256
