@@ -2,6 +2,7 @@
 
     libg3x.so      product library: sm_100a kernels + C-ABI host code (nvcc)
     libg3x_emu.so  CPU model of the kernels' warp protocol, loaded by tests only (g++)
+    libg3x_emu16.so CPU model of the int16x2 lane kernel's per-lane logic, tests only (nvcc)
     libg3x_synth.so seeded synthetic workload generator + multi-threaded plane packer (g++)
 
 Run as ``python -m g3sa_b200.build``.  The oracle libraries are built by oracle/Makefile
@@ -55,6 +56,18 @@ def build_emu(force=False):
     return out
 
 
+def build_emu16(force=False):
+    """CPU model of the int16x2 lane kernel's per-lane logic (host code built by nvcc, whose
+    headers give the DPX intrinsics host versions)."""
+    out = os.path.join(HERE, "libg3x_emu16.so")
+    deps = [os.path.join(CSRC, f) for f in ("g3x_emu16.cu", "g3x_lane16.cuh", "g3x_core.h", "g3x_internal.h")]
+    if not force and not _stale(out, deps):
+        return out
+    _run([NVCC] + ARCH + ["-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-o", out,
+                          os.path.join(CSRC, "g3x_emu16.cu")])
+    return out
+
+
 def build_synth(force=False):
     out = os.path.join(HERE, "libg3x_synth.so")
     deps = [os.path.join(CSRC, "g3x_synth.cpp"), os.path.join(HERE, "..", "include", "g3x.h")]
@@ -70,6 +83,7 @@ def main(argv=None):
     force = "--force" in argv
     build_lib(force=force, verbose_ptxas="--ptxas-v" in argv)
     build_emu(force=force)
+    build_emu16(force=force)
     build_synth(force=force)
 
 

@@ -1,0 +1,388 @@
+// g3x_lane16.cuh -- per-lane logic of the int16x2 lane-per-job kernel for batched ksw_extend2
+// (bwa/src/ksw.cu:303-401), shared by the sm_100a kernel (g3x_lane16.cu) and its CPU model
+// (g3x_emu16.cu, test-only).
+//
+// One lane runs one job through the reference's row loop.  The lane's row buffer (ksw.cu:310,
+// eh[j] = {H(i-1, j-1), E(i, j)} before row i) lives in shared memory as int16 fields grouped in
+// 8-column blocks: per block four int16x2 words of H and four of E, word p holding columns
+// jb+p (low half) and jb+p+4 (high half).  A row is walked in aligned blocks; every step of the
+// recurrence is one Blackwell DPX int16x2 instruction for two cells.
+//
+// The recurrence of ksw.cu:346-370, per column j of row i:
+//   M = H(i-1,j-1) ? H(i-1,j-1) + S : 0;  H = max(M, E, F);
+//   E' = max(E - e_del, max(M - oe_del, 0));  F' = max(F - e_ins, max(M - oe_ins, 0)).
+// E and F are computed from M, never from H, so inside a row F is a max-plus prefix over the
+// row's M values: with T(t) = max(M(t) - oe_ins, 0) and V(t) = max_{s<t} T(s) - (t-1-s) e_ins,
+//   F(t) = max(F_in - t e_ins, V(t))           (F_in = F entering the block).
+// A block computes each half's own prefix of T over its four columns (the L words: low half
+// over columns 0-3, high half over 4-7), then F(4) = max(F_in - 4e, V(4)) with V(4) the low
+// half's full prefix, and every F of the block from the pair (F_in, F(4)):
+//   (F(p), F(p+4)) = max((F_in, F(4)) - p e, L[p-1]),     F(8) = max(F(4) - 4e, L[3].hi).
+//
+// Exactness in 16 bits: a job runs here only when every value of its DP fits (job_fits_int16):
+// 0 <= h0, K (h0 + max_score min(qlen, tlen)) < 2^15 with K the smallest power of two
+// >= 1 + max_score, small gap penalties.  Then M = H ? H + S : 0 equals min(H + S, K H) where
+// H > 0 and is <= 0 where H == 0, which every use clips to 0 as the reference's 0.
+//
+// Band edges.  Columns left of beg are never read again (beg only grows), and the reference's
+// trim (ksw.cu:388-389) only moves beg past columns whose H and E words are zero, so every such
+// "dead" column holds zeros -- except those the band clamp beg >= i - w (ksw.cu:338) cuts off.
+// The first block of a row therefore zeroes the H and E words left of beg as it loads them; a
+// dead column then computes M <= 0, T = 0, E' = 0, F = 0 and H = 0, so it adds nothing to F or
+// to the row maximum and writes zeros back, and the H word of column beg (H(i, beg-1), 0 for
+// beg > 0 as ksw.cu:344-345 sets it) comes out right.  The last block keeps the words right of
+// column end as they were (the band can grow back into them, ksw.cu:390-391), and leaves
+// columns >= end out of the row maximum.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "g3x_core.h"
+
+namespace g3x {
+namespace l16 {
+
+constexpr int kLB = 8;   // columns per block
+
+// Blocks per lane: columns up to qcap + 8 (block loads reach (end - 1) | 7 <= qcap - 1 | 7, the
+// row end writes column end <= qcap, the column-of-maximum search reads one block past the
+// winning block, which starts at most at (qcap - 1) & ~7).
+G3X_HD int blocks_of(int qcap) { return (qcap + 7) / 8 + 1; }
+G3X_HD int nib_words(int qcap) { return 2 * ((qcap + 15) / 16); }
+G3X_HD size_t warp_bytes(int qcap) {
+    return (size_t)32 * blocks_of(qcap) * 32 + (size_t)128 * nib_words(qcap);
+}
+
+// PTX prmt (default mode): result byte k = byte (s_k & 7) of {b, a}, sign-replicated when s_k & 8.
+G3X_HD uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+#if defined(__CUDA_ARCH__)
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+    return r;
+#else
+    const uint64_t v = (uint64_t)a | ((uint64_t)b << 32);
+    uint32_t r = 0;
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t s = (sel >> (4 * k)) & 15u;
+        uint32_t byte = (uint32_t)(v >> (8 * (s & 7u))) & 0xFFu;
+        if (s & 8u) byte = (byte & 0x80u) ? 0xFFu : 0u;
+        r |= byte << (8 * k);
+    }
+    return r;
+#endif
+}
+
+G3X_HD int ffs32(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __ffs(x);
+#else
+    return x ? __builtin_ctz(x) + 1 : 0;
+#endif
+}
+G3X_HD int clz32(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __clz(x);
+#else
+    return x ? __builtin_clz(x) : 32;
+#endif
+}
+
+// Scores of columns p and p+4 of a block as int16x2: byte p of lo and byte p of hi, each
+// sign-extended to 16 bits.
+template <int p>
+G3X_HD uint32_t pair_score(uint32_t lo, uint32_t hi) {
+    constexpr uint32_t sel = (uint32_t)p | ((8u | p) << 4) | ((4u + p) << 8) | ((8u | (4u + p)) << 12);
+    return prmt(lo, hi, sel);
+}
+
+// Lane-interleaved layout: block b of lane L at uint4 index b * 32 + L; the 32-bit word of
+// column c is word (c & 3) of its block's uint4, in the half (c & 4).
+G3X_HD int word_of(int c, int L) { return ((((c >> 3) << 5) + L) << 2) + (c & 3); }
+
+struct Planes {
+    uint4* H;
+    uint4* E;
+    uint32_t* H32;
+    uint32_t* E32;
+    const uint32_t* qn;   // query codes, 8 nibbles per word, word k of lane L at qn[k * 32 + L]
+};
+
+G3X_HD void set_col(uint32_t* P, int c, int L, int32_t v) {
+    uint32_t& w = P[word_of(c, L)];
+    w = (c & 4) ? ((w & 0x0000FFFFu) | ((uint32_t)v << 16)) : ((w & 0xFFFF0000u) | ((uint32_t)v & 0xFFFFu));
+}
+
+// Constants of the recurrence, replicated in both halves.
+struct PairConst {
+    uint32_t noe_del, ne_del, noe_ins, ne_ins;
+    uint32_t nt[4];     // -p e_ins
+    uint32_t n4;        // -4 e_ins
+    uint32_t kmul;      // 2^k: M = min(H + S, H * 2^k)
+};
+
+G3X_HD uint32_t rep16(int32_t v) { return ((uint32_t)v & 0xFFFFu) * 0x00010001u; }
+
+G3X_HD PairConst pair_const(const ScoreParams& sp) {
+    PairConst pc;
+    pc.noe_del = rep16(-sp.oe_del);
+    pc.ne_del = rep16(-sp.e_del);
+    pc.noe_ins = rep16(-sp.oe_ins);
+    pc.ne_ins = rep16(-sp.e_ins);
+    for (int p = 0; p < 4; ++p) pc.nt[p] = rep16(-p * sp.e_ins);
+    pc.n4 = rep16(-4 * sp.e_ins);
+    pc.kmul = 1u << int16_shift(sp.max_sc);
+    return pc;
+}
+
+// Masks per column offset o (0..9) within a block: in each pair word, 0xFFFF in each half whose
+// column offset (p, p + 4) is >= o.
+G3X_HD uint32_t ge_word(int o, int p) {
+    return (p >= o ? 0x0000FFFFu : 0u) | (p + 4 >= o ? 0xFFFF0000u : 0u);
+}
+
+// State of one row of one lane.
+struct RowState {
+    int32_t beg, end, h1;
+    uint32_t plo, phi;   // the row's score pools (target code vs query codes 0-3 and N)
+    uint32_t fr;         // high half: F entering the next block
+    uint32_t hlast;      // high half: H of the column before the next block
+    int32_t key;         // row maximum << 16 | block index of its last block reaching it
+};
+
+// The block arithmetic on loaded (and masked) words; returns the new H and E words, the H of
+// the block's columns (h2), and advances fr and hlast.  kSym: oe_del == oe_ins, so the E step
+// reuses max(M - oe_ins, 0).
+template <bool kSym>
+G3X_HD void block_core(const uint32_t (&H2)[4], const uint32_t (&E2)[4], uint32_t qw, RowState& r,
+                       const PairConst& pc, uint32_t (&nh)[4], uint32_t (&ne)[4], uint32_t (&h2)[4]) {
+    const uint32_t sc_lo = prmt(r.plo, r.phi, qw);   // prmt reads selector bits 0-15 only
+    const uint32_t sc_hi = prmt(r.plo, r.phi, qw >> 16);
+    const uint32_t S2[4] = {pair_score<0>(sc_lo, sc_hi), pair_score<1>(sc_lo, sc_hi),
+                            pair_score<2>(sc_lo, sc_hi), pair_score<3>(sc_lo, sc_hi)};
+    uint32_t M2[4], T2[4], L2[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        M2[p] = __viaddmin_s16x2(H2[p], S2[p], H2[p] * pc.kmul);
+        T2[p] = __viaddmax_s16x2(M2[p], pc.noe_ins, 0u);
+        L2[p] = p == 0 ? T2[0] : __viaddmax_s16x2(L2[p - 1], pc.ne_ins, T2[p]);
+    }
+    // (F_in, F(4)), then every F of the block
+    const uint32_t fin = prmt(r.fr, r.fr, 0x3232u);
+    const uint32_t x = __viaddmax_s16x2(fin, pc.n4, L2[3]);                  // low half: F(4)
+    const uint32_t fp = prmt(r.fr, x, 0x5432u);
+    r.fr = __viaddmax_s16x2(fp, pc.n4, L2[3]);                              // high half: F(8)
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const uint32_t F2 = p == 0 ? fp : __viaddmax_s16x2(fp, pc.nt[p], L2[p - 1]);
+        h2[p] = __vimax3_s16x2(M2[p], E2[p], F2);
+        const uint32_t te = kSym ? T2[p] : __viaddmax_s16x2(M2[p], pc.noe_del, 0u);
+        ne[p] = __viaddmax_s16x2(E2[p], pc.ne_del, te);
+    }
+    nh[0] = prmt(r.hlast, h2[3], 0x5432u);
+    nh[1] = h2[0]; nh[2] = h2[1]; nh[3] = h2[2];
+    r.hlast = h2[3];
+}
+
+// Row maximum of a block (of the given H words) into the running key.
+G3X_HD void block_max(const uint32_t (&hm)[4], int32_t kb, RowState& r) {
+    const uint32_t b2 = __vimax3_s16x2(__vimax3_s16x2(hm[0], hm[1], hm[2]), hm[3], hm[3]);
+    const uint32_t bx = __vimax3_s16x2(b2, prmt(b2, b2, 0x1032u), b2);   // max in both halves
+    const int32_t key = (int32_t)prmt((uint32_t)kb, bx, 0x7610u);        // (max << 16) | kb
+    r.key = r.key > key ? r.key : key;
+}
+
+// A block strictly inside the row.
+template <bool kSym>
+G3X_HD void block_mid(const Planes& P, int lane, int32_t jb, RowState& r, const PairConst& pc) {
+    const int at = ((jb >> 3) << 5) + lane;
+    const uint4 hq = P.H[at], eq = P.E[at];
+    const uint32_t H2[4] = {hq.x, hq.y, hq.z, hq.w}, E2[4] = {eq.x, eq.y, eq.z, eq.w};
+    uint32_t nh[4], ne[4], h2[4];
+    block_core<kSym>(H2, E2, P.qn[(jb >> 3) * 32 + lane], r, pc, nh, ne, h2);
+    P.H[at] = make_uint4(nh[0], nh[1], nh[2], nh[3]);
+    P.E[at] = make_uint4(ne[0], ne[1], ne[2], ne[3]);
+    block_max(h2, jb >> 3, r);
+}
+
+// The first block of a row with two or more blocks: the words left of beg are zeroed on load.
+template <bool kSym>
+G3X_HD void block_first(const Planes& P, int lane, int32_t jb, RowState& r, const PairConst& pc,
+                        const uint4* ge) {
+    const int at = ((jb >> 3) << 5) + lane;
+    const uint4 hq = P.H[at], eq = P.E[at];
+    const uint4 A = ge[r.beg - jb];
+    const uint32_t H2[4] = {hq.x & A.x, hq.y & A.y, hq.z & A.z, hq.w & A.w};
+    const uint32_t E2[4] = {eq.x & A.x, eq.y & A.y, eq.z & A.z, eq.w & A.w};
+    uint32_t nh[4], ne[4], h2[4];
+    block_core<kSym>(H2, E2, P.qn[(jb >> 3) * 32 + lane], r, pc, nh, ne, h2);
+    P.H[at] = make_uint4(nh[0], nh[1], nh[2], nh[3]);
+    P.E[at] = make_uint4(ne[0], ne[1], ne[2], ne[3]);
+    block_max(h2, jb >> 3, r);
+}
+
+// The last block of a row (first == true: also its first, the row's only block): columns right of
+// end keep their words, columns >= end stay out of the row maximum, r.h1 = H(i, end - 1).
+template <bool kSym>
+G3X_HD void block_last(const Planes& P, int lane, int32_t jb, bool first, RowState& r,
+                       const PairConst& pc, const uint4* ge) {
+    const int at = ((jb >> 3) << 5) + lane;
+    const uint4 hq = P.H[at], eq = P.E[at];
+    const uint4 A = ge[first ? r.beg - jb : 0];
+    const int hi = r.end - jb;                       // 1 .. 8
+    const uint4 gv = ge[hi], gw = ge[hi + 1];
+    const uint32_t Hq[4] = {hq.x, hq.y, hq.z, hq.w}, Eq[4] = {eq.x, eq.y, eq.z, eq.w};
+    const uint32_t Am[4] = {A.x, A.y, A.z, A.w}, V[4] = {~gv.x, ~gv.y, ~gv.z, ~gv.w};
+    const uint32_t W[4] = {~gw.x, ~gw.y, ~gw.z, ~gw.w};
+    uint32_t H2[4], E2[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) { H2[p] = Hq[p] & Am[p]; E2[p] = Eq[p] & Am[p]; }
+    uint32_t nh[4], ne[4], h2[4], hm[4];
+    block_core<kSym>(H2, E2, P.qn[(jb >> 3) * 32 + lane], r, pc, nh, ne, h2);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        nh[p] = (nh[p] & W[p]) | (Hq[p] & ~W[p]);   // columns <= end: new; beyond: as they were
+        ne[p] = (ne[p] & W[p]) | (Eq[p] & ~W[p]);
+        hm[p] = h2[p] & V[p];
+    }
+    P.H[at] = make_uint4(nh[0], nh[1], nh[2], nh[3]);
+    P.E[at] = make_uint4(ne[0], ne[1], ne[2], ne[3]);
+    block_max(hm, jb >> 3, r);
+    const int t = hi - 1;
+    const uint32_t wl = (t & 2) ? ((t & 1) ? h2[3] : h2[2]) : ((t & 1) ? h2[1] : h2[0]);
+    r.h1 = (int32_t)((t & 4) ? (wl >> 16) : (wl & 0xFFFFu));
+}
+
+// Bit t set when column b+t (b a multiple of 8) has a non-zero H or E word: every half-word is
+// reduced to 0 or 1 by an unsigned min, then the four pairs are summed with weights 1-8 (each
+// half stays below 16), which leaves columns 0-3 in bits 0-3 and 4-7 in bits 16-19.
+G3X_HD uint32_t nonzero_cols(const Planes& P, int32_t b, int lane) {
+    const int at = ((b >> 3) << 5) + lane;
+    const uint4 hq = P.H[at], eq = P.E[at];
+    const uint32_t one = 0x00010001u;
+    const uint32_t z0 = __vimin3_u16x2(hq.x | eq.x, one, one), z1 = __vimin3_u16x2(hq.y | eq.y, one, one);
+    const uint32_t z2 = __vimin3_u16x2(hq.z | eq.z, one, one), z3 = __vimin3_u16x2(hq.w | eq.w, one, one);
+    const uint32_t s = z0 + 2u * z1 + 4u * z2 + 8u * z3;
+    return (s & 0xFu) | ((s >> 12) & 0xF0u);
+}
+
+// The last column c in [lo, hi) of the block at mjb (lo, hi within mjb .. mjb + 8) with
+// H(i, c) == m, or -1.  H(i, c) sits in the H word of column c + 1: columns mjb .. mjb + 2 in
+// the low halves of words 1-3, mjb + 3 .. mjb + 6 in the high halves of words 0-3, mjb + 7 in
+// the low half of the next block's word 0.  Each half-word is reduced to 0 (equal) or 1.
+G3X_HD int32_t max_col(const Planes& P, int lane, int32_t mjb, int32_t lo, int32_t hi, int32_t m) {
+    const int at = ((mjb >> 3) << 5) + lane;
+    const uint4 hq = P.H[at];
+    const uint32_t nx = P.H32[(at + 32) << 2];
+    const uint32_t m2 = rep16(m), one = 0x00010001u;
+    const uint32_t z0 = __vimin3_u16x2(hq.x ^ m2, one, one), z1 = __vimin3_u16x2(hq.y ^ m2, one, one);
+    const uint32_t z2 = __vimin3_u16x2(hq.z ^ m2, one, one), z3 = __vimin3_u16x2(hq.w ^ m2, one, one);
+    const uint32_t zn = __vimin3_u16x2(nx ^ m2, one, one);
+    // bit t (low half: t = 0..3, high half: t = 4..7) = 1 where column mjb + t differs from m
+    const uint32_t s = z1 + 2u * z2 + 4u * z3 + 8u * prmt(z0, zn, 0x5432u);
+    const uint32_t ne = (s & 0xFu) | ((s >> 12) & 0xF0u);
+    const uint32_t range = (0xFFu >> (kLB - (hi - mjb))) & (0xFFu << (lo - mjb));
+    const uint32_t eq = ~ne & range;
+    return eq ? mjb + 31 - clz32(eq) : -1;
+}
+
+// Per-lane job state.
+struct LaneJob {
+    int job;                 // -1 = none
+    int32_t qlen, tlen, w, h0;
+    uint32_t t_off;
+    int32_t trev;
+    Commit K;
+    int32_t beg, end;        // band of the next row before the clamps of ksw.cu:338-340
+    uint32_t tx, tn, px, pn; // target chunk K.next >> 4 and the next one
+};
+
+G3X_HD JobConst job_const(const LaneJob& J, const ScoreParams& sp) {
+    JobConst c;
+    c.qlen = J.qlen; c.tlen = J.tlen; c.w = J.w; c.h0 = J.h0;
+    c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
+    c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
+    return c;
+}
+
+// Row begin (ksw.cu:335-345): the band after the clamps, the first column's h1, the pools of the
+// row's target code (target chunks as 2-bit fields x and N bits n, 16 rows per chunk).
+G3X_HD void row_begin(const LaneJob& J, const ScoreParams& sp, const uint2* pools, RowState& r) {
+    const int32_t i = J.K.next;
+    r.beg = J.beg > i - J.w ? J.beg : i - J.w;
+    r.end = J.end < i + J.w + 1 ? J.end : i + J.w + 1;
+    if (r.end > J.qlen) r.end = J.qlen;
+    r.h1 = 0;
+    if (r.beg == 0) {
+        const int32_t h = J.h0 - (sp.o_del + sp.e_del * (i + 1));
+        r.h1 = h > 0 ? h : 0;
+    }
+    uint32_t code = (J.tx >> ((i & 15) << 1)) & 3u;
+    if ((J.tn >> (i & 15)) & 1u) code = 4;
+    const uint2 p = pools[code];
+    r.plo = p.x;
+    r.phi = p.y;
+    r.fr = 0;
+    r.hlast = (uint32_t)r.h1 << 16;
+    r.key = 0;
+}
+
+// Row end (ksw.cu:371-391) for a running lane: column end's words, the row's bookkeeping, and
+// the band of the next row.
+G3X_HD void row_end(LaneJob& J, const Planes& P, int lane, const RowState& r, const ScoreParams& sp,
+                    bool nonempty) {
+    const int32_t beg = r.beg, end = r.end;
+    set_col(P.H32, end, lane, r.h1);
+    set_col(P.E32, end, lane, 0);
+    RowDone rd;
+    rd.m = r.key >> 16;
+    rd.mj = -1;
+    if (rd.m > 0) {
+        const int32_t mjb = (r.key & 0xFFFF) << 3;
+        rd.mj = max_col(P, lane, mjb, mjb > beg ? mjb : beg, mjb + kLB < end ? mjb + kLB : end, rd.m);
+    }
+    rd.gval = (nonempty ? end : beg) == J.qlen ? r.h1 : -1;
+    rd.ncells = nonempty ? end - beg : 0;
+    commit_row(J.K, job_const(J, sp), rd);
+    if (J.K.stop) return;
+    // ksw.cu:388-389, eight columns at a time: the first column of [beg, end) whose H or E word
+    // is non-zero (end when none; beg itself when the band is empty) ...
+    int32_t nb = beg < end ? end : beg;
+    for (int32_t b = beg & ~(kLB - 1); b < end; b += kLB) {
+        uint32_t mk = nonzero_cols(P, b, lane);
+        if (b < beg) mk &= ~0u << (beg - b);
+        if (mk) {
+            const int32_t j = b + ffs32(mk) - 1;
+            nb = j < end ? j : end;
+            break;
+        }
+    }
+    // ... and ksw.cu:390-391: the last column of [nb, end] whose word is non-zero (nb - 1 if none;
+    // end itself when end < nb)
+    int32_t last = end < nb ? end : nb - 1;
+    if (end >= nb) {
+        for (int32_t b = end & ~(kLB - 1); b >= (nb & ~(kLB - 1)); b -= kLB) {
+            uint32_t mk = nonzero_cols(P, b, lane);
+            if (end - b < kLB - 1) mk &= (2u << (end - b)) - 1u;
+            if (b < nb) mk &= ~0u << (nb - b);
+            if (mk) {
+                last = b + 31 - clz32(mk);
+                break;
+            }
+        }
+    }
+    J.beg = nb;
+    J.end = last + 2 < J.qlen ? last + 2 : J.qlen;
+}
+
+// All blocks of one row of one lane, in the order the kernel runs them.
+template <bool kSym>
+G3X_HD void row_blocks(const Planes& P, int lane, RowState& r, const PairConst& pc, const uint4* ge) {
+    if (r.beg >= r.end) return;
+    const int32_t jb0 = r.beg & ~(kLB - 1);
+    const int nblk = ((r.end - 1) >> 3) - (r.beg >> 3) + 1;
+    if (nblk > 1) block_first<kSym>(P, lane, jb0, r, pc, ge);
+    for (int k = 1; k < nblk - 1; ++k) block_mid<kSym>(P, lane, jb0 + k * kLB, r, pc);
+    block_last<kSym>(P, lane, jb0 + (nblk - 1) * kLB, nblk == 1, r, pc, ge);
+}
+
+}  // namespace l16
+}  // namespace g3x

@@ -17,6 +17,7 @@ def _built():
     """Build the native test libraries (CPU-only builds are cheap and idempotent)."""
     from g3sa_b200 import build
     build.build_emu()
+    build.build_emu16()
     build.build_synth()
     from tests import native
     native.build_oracle()

@@ -11,6 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "libg3x_oracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libksw_ref.so")
 EMU_SO = os.path.join(ROOT, "g3sa_b200", "libg3x_emu.so")
+EMU16_SO = os.path.join(ROOT, "g3sa_b200", "libg3x_emu16.so")
 
 # g3o_job / RefJob (oracle/ksw_oracle.c, oracle/ref_wrap.cpp)
 CPU_JOB_DT = np.dtype([("q_off", "<i8"), ("t_off", "<i8"), ("qlen", "<i4"), ("tlen", "<i4"),
@@ -25,7 +26,7 @@ CPU_REG_DT = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"
                        ("truesc", "<i4"), ("w", "<i4"), ("tries_left", "<i4"),
                        ("tries_right", "<i4"), ("pad_", "<i4"), ("cells", "<i8")])
 
-_oracle = _ref = _emu = None
+_oracle = _ref = _emu = _emu16 = None
 
 
 def build_oracle():
@@ -90,6 +91,26 @@ def emu():
         _emu.g3x_emu_extend_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 4
     return _emu
+
+
+def emu16_extend(jobs, u8, score):
+    """(ext[n,6], cells[n], status[n]) from the CPU model of the int16x2 lane kernel's per-lane
+    logic (libg3x_emu16.so); status -3 (too long) for jobs outside its int16 fit."""
+    global _emu16
+    if _emu16 is None:
+        _emu16 = ctypes.CDLL(EMU16_SO)
+        _emu16.g3x_emu16_extend.argtypes = [ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 5
+    n = len(jobs)
+    jobs = np.ascontiguousarray(jobs)
+    u8 = np.ascontiguousarray(u8)
+    score = np.ascontiguousarray(score)
+    out = np.zeros((n, 6), np.int32)
+    cells = np.zeros(n, np.int32)
+    status = np.zeros(n, np.int32)
+    rc = _emu16.g3x_emu16_extend(jobs.ctypes.data, n, u8.ctypes.data, score.ctypes.data, out.ctypes.data,
+                                 cells.ctypes.data, status.ctypes.data)
+    assert rc == 0
+    return out, cells, status
 
 
 def cpu_jobs(jobs):
