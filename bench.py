@@ -39,20 +39,38 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "ksw_extend2 GCUPS & extensions/s on 1 B200, learned vs plain schedule, bit-exact"
-# DRAM bytes (read + write) per launch of each kernel at this workload's size, from the ncu
-# captures summarised under profiles/ (a 100k-seed case scaled by 5, the DRAM traffic of a
-# launch growing with the jobs it stages).  None until a capture of that kernel exists.
-TRAFFIC_PER_LAUNCH = {("lane", 232): 27.9e6, ("lane16", 232): 34.4e6}
+# DRAM bytes (read + write) per job staged by the lane kernels, from the ncu capture of the
+# width classes' launches summarised in profiles/lane16_kernel_cfg2_classes.md (dram__bytes_read
+# + dram__bytes_write of each class launch / its job count, 100k-seed case): a launch's DRAM
+# traffic is its jobs' headers, query and target plane words and outputs, so it scales with the
+# jobs the launch stages.  Keyed by the class's widest query; None until a capture exists.
+TRAFFIC_PER_JOB = {}
 WORKLOADS = {
-    # name: (synth kind, units, w, unrelated, description)
+    # name: (synth kind, units, w, unrelated, description with {w})
     "cfg2": (2, 500000, 100, 0.2,
              "uneven left+right ksw_extend2 batch: ~1M jobs from 500k seeds on 100/150/250 bp "
-             "reads, divergence U[0,5%], 20% unrelated targets, w=100, a=1 b=4 o=6 e=1 zdrop=100"),
+             "reads, divergence U[0,5%], 20% unrelated targets, w={w}, a=1 b=4 o=6 e=1 zdrop=100"),
     "cfg1": (1, 100000, 100, 0.0,
-             "100k right-extension jobs, qlen U[1,150], 1% subs / 0.1% indels, w=100 flank"),
+             "100k right-extension jobs, qlen U[1,150], 1% subs / 0.1% indels, w={w} flank"),
     "cfg4": (4, 200000, 100, 0.0,
-             "200k long-segment jobs, qlen log-uniform [500,5000], divergence U[0.1%,1%], w=100"),
+             "200k long-segment jobs, qlen log-uniform [500,5000], divergence U[0.1%,1%], indels "
+             "up to 20 bp, w={w}"),
 }
+# Trace units of the learned model's training batch per workload (the generator's units: seeds
+# for cfg2, jobs otherwise), about 2M jobs where that stays within host memory.
+TRAIN_UNITS = {"cfg2": 1_000_000, "cfg1": 2_000_000, "cfg4": 200_000}
+
+
+def workload(args):
+    """(synth kind, units, w, unrelated fraction, description) of --workload with --w."""
+    kind_, units, w, unrel, desc = WORKLOADS[args.workload]
+    w = args.w if args.w else w
+    return kind_, units, w, unrel, desc.format(w=w)
+
+
+def bench_config(desc, n, cells):
+    """The `config` object both arms print for one workload (the same keys and values)."""
+    return {"workload": desc, "jobs": int(n), "cells": int(cells)}
 
 
 def parse():
@@ -64,6 +82,7 @@ def parse():
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["chains", "global", "seedsw"])
     ap.add_argument("--schedule", default="auto", choices=["auto", "plain", "sorted", "learned"])
     ap.add_argument("--seed", type=int, default=0x6A5 + 2)
+    ap.add_argument("--w", type=int, default=0, help="band width w of the job generator (0: the workload's)")
     return ap.parse_args()
 
 
@@ -199,7 +218,7 @@ def run_reference_arm(args, ws, rank):
     import g3sa_b200 as g
     if rank != 0:
         return
-    kind_, units, w, unrel, desc = WORKLOADS[args.workload]
+    kind_, units, w, unrel, desc = workload(args)
     wl = g.synth(kind_, units, seed=args.seed, w=w, unrelated=unrel)
     threads = os.cpu_count() or 1
     cells = useful_cells(wl)
@@ -215,7 +234,7 @@ def run_reference_arm(args, ws, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
-        "config": {"workload": desc, "jobs": wl.n, "cells": cells},
+        "config": bench_config(desc, wl.n, cells),
         "extensions_per_s": round(wl.n / t, 1),
         "cpu_baseline": {"value": round(gcups, 4), "unit": "GCUPS", "cores": threads, "kind": kind,
                          "sample": f"whole workload ({wl.n} jobs) per step"},
@@ -814,7 +833,7 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    kind_, units, w, unrel, desc = WORKLOADS[args.workload]
+    kind_, units, w, unrel, desc = workload(args)
     wl = g.synth(kind_, units, seed=args.seed + 1000 * rank, w=w, unrelated=unrel)
     codes, nmask = wl.planes()
     sc = g.default_score()
@@ -848,7 +867,7 @@ def main():
 
     # Learned cost model: trained on the GPU on plain-kernel traces of a held-out batch of the
     # same generator (another seed), about 2M jobs.
-    train_metrics = learn.train(ctx, n_train=max(1, 2_000_000 * units // max(n, 1)),
+    train_metrics = learn.train(ctx, n_train=TRAIN_UNITS[args.workload],
                                 seed_train=0xA11CE + rank, kind=kind_, w=w, unrelated=unrel)
     pred_err = learn.prediction_error(ctx, d_jobs, n, d_codes, d_nmask, cells_np)
 
@@ -894,7 +913,25 @@ def main():
     ms_learned = timed_steps(lambda: graphs["learned"].launch(stream), k2, 1, stream, flush)
     stats_learned = ctx.last_stats()
     ms_plain = timed_steps(lambda: batch(g.SCHED_PLAIN), k2, 1, stream, flush)
-    t_sorted, t_learned, t_plain = (sum(x) / len(x) for x in (ms_sorted, ms_learned, ms_plain))
+    # The plain kernel over the jobs in length-sorted order (longest query first, then longest
+    # target): the same one-block-per-job kernel, its blocks issued longest first so that the
+    # batch's tail is made of short jobs.  The order is computed once on the host, outside the
+    # timed region; the outputs come back in that order and are compared after un-permuting.
+    perm = np.lexsort((-wl.jobs["tlen"].astype(np.int64), -wl.jobs["qlen"].astype(np.int64)))
+    d_jobs_len = torch.from_numpy(np.ascontiguousarray(wl.jobs[perm]).view(np.uint8).copy()).to(dev)
+    d_out_len = torch.zeros_like(d_out)
+
+    def plain_sorted():
+        ctx.extend_batch(sc, d_jobs_len, n, d_codes, d_nmask, d_out_len, d_status, mq, mt,
+                         schedule=g.SCHED_PLAIN, stream=stream)
+
+    plain_sorted()
+    torch.cuda.synchronize()
+    if (d_status != 0).any() or not np.array_equal(d_out_len.cpu().numpy(), plain_out[perm]):
+        raise SystemExit("length-sorted plain batch differs from the plain kernel")
+    ms_plain_len = timed_steps(plain_sorted, k2, 1, stream, flush)
+    t_sorted, t_learned, t_plain, t_plain_len = (sum(x) / len(x) for x in (ms_sorted, ms_learned, ms_plain,
+                                                                            ms_plain_len))
 
     # Per-class launch durations of the learned batch (the same kernels the graph replays),
     # each from CUDA events on the class's own stream, while the other classes run beside it.
@@ -902,6 +939,11 @@ def main():
     member = np.searchsorted(widths, wl.jobs["qlen"].astype(np.int64), side="left")
     cls_jobs = np.bincount(member, minlength=len(tiles))
     cls_cells = np.bincount(member, weights=cells_np.astype(np.float64), minlength=len(tiles))
+    # Algorithmic HBM bytes of each class's jobs: 24 B header + 2-bit query and target + their
+    # N bits + 24 B of outputs per job.
+    q64, t64 = wl.jobs["qlen"].astype(np.int64), wl.jobs["tlen"].astype(np.int64)
+    job_bytes = 24 + (q64 + 3) // 4 + (t64 + 3) // 4 + (q64 + t64 + 7) // 8 + 24
+    cls_bytes = np.bincount(member, weights=job_bytes.astype(np.float64), minlength=len(tiles))
 
     def class_table(schedule, mode):
         ctx.set_timing(mode)
@@ -921,7 +963,9 @@ def main():
             mk = sum(ms_k) / len(ms_k)
             rows.append({"width": int(t[0]), "kernel": kernel_name(t), "jobs": int(cls_jobs[k]),
                          "cells": int(cls_cells[k]), "ms": round(mk, 4),
-                         "gcups": round(cls_cells[k] / (mk * 1e-3) / 1e9, 3)})
+                         "gcups": round(cls_cells[k] / (mk * 1e-3) / 1e9, 3),
+                         "arith": "int16x2" if kernel_name(t) == "lane16" else "int32",
+                         "alg_bytes": int(cls_bytes[k])})
         return rows
 
     # each class alone (its own kernel roofline), and side by side as the step runs them
@@ -949,14 +993,23 @@ def main():
     e2e_exact = bool((h_status == 0).all()) and np.array_equal(h_out.numpy(), plain_out)
     pipe.close()
 
-    (t_step, t_e2e, t_plain, t_sorted, t_learned), (tot_cells, tot_jobs) = combine_ranks(
-        dist, [t_step, t_e2e, t_plain, t_sorted, t_learned], [cells, n], dev)
+    (t_step, t_e2e, t_plain, t_plain_len, t_sorted, t_learned), (tot_cells, tot_jobs) = combine_ranks(
+        dist, [t_step, t_e2e, t_plain, t_plain_len, t_sorted, t_learned], [cells, n], dev)
+
 
     peak_ops = ctx.int_peak()
     if rank == 0:
         gcups = tot_cells / (t_step * 1e-3) / 1e9
-        peak_gcups = peak_ops / 8 / 1e9
+        # cells/s rooflines: 8 int ops per cell; an int16x2 instruction does two cells
+        peak32 = peak_ops / 8 / 1e9
+        peak_of = {"int32": peak32, "int16x2": 2 * peak32}
         dom = max(classes, key=lambda c: c["ms"])
+        dom_peak = peak_of[dom["arith"]]
+        # the step against the blend of its classes' rooflines: the time every class's cells
+        # would take at its own kernel's peak, over the measured step time
+        ideal_ms = sum(c["cells"] / (peak_of[c["arith"]] * 1e9) * 1e3 for c in classes)
+        tpj = TRAFFIC_PER_JOB.get(dom["width"])
+        int16_cells = sum(c["cells"] for c in classes if c["arith"] == "int16x2")
         try:
             with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
                 hbm_peak, hbm_src = float(json.load(fh)["hbm_gbs"]), "measured"
@@ -965,44 +1018,56 @@ def main():
         kind, cpu_t, cpu_out = cpu_reference(wl, os.cpu_count() or 1)
         cpu_gcups = cells / cpu_t / 1e9
         idle = lambda s: round(s[1] / max(1, s[0] + s[1]), 4)  # noqa: E731
+        gc = lambda t: round(tot_cells / (t * 1e-3) / 1e9, 3)  # noqa: E731
         line = {
             "metric": METRIC, "value": round(gcups, 3), "unit": "GCUPS", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_step, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int16x2 (int32 where the fit fails)" if int16_cells else "int32",
             "data": "synthetic (seeded generator, shapes of the benchmark configuration)",
-            "config": {"workload": desc, "jobs_per_gpu": n, "cells_per_gpu": cells,
-                       "schedule": args.schedule if args.schedule != "auto" else "learned",
-                       "launch": "one CUDA graph per step (features, MLP, counting sort, one persistent launch per width class)",
-                       "width_classes": tiles, "width_classes_sorted": tiles_of["sorted"],
-                       "max_qlen": mq, "max_tlen": mt,
-                       "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas x{ws}"},
+            "config": bench_config(desc, n, cells),
+            "setup": {"schedule": args.schedule if args.schedule != "auto" else "learned",
+                      "launch": "one CUDA graph per step (features, MLP, counting sort, one persistent launch per width class)",
+                      "width_classes": tiles, "width_classes_sorted": tiles_of["sorted"],
+                      "max_qlen": mq, "max_tlen": mt, "int16x2_cell_frac": round(int16_cells / max(cells, 1), 4),
+                      "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas x{ws}"},
             "extensions_per_s": round(tot_jobs / (t_step * 1e-3), 1),
-            "arms": {"learned": {"gcups": round(tot_cells / (t_learned * 1e-3) / 1e9, 3), "ms": round(t_learned, 4),
+            "arms": {"learned": {"gcups": gc(t_learned), "ms": round(t_learned, 4),
                                  "warp_idle_frac": idle(stats_learned)},
-                     "sorted": {"gcups": round(tot_cells / (t_sorted * 1e-3) / 1e9, 3), "ms": round(t_sorted, 4),
+                     "sorted": {"gcups": gc(t_sorted), "ms": round(t_sorted, 4),
                                 "warp_idle_frac": idle(stats_sorted),
                                 "class_ms": [c["ms"] for c in classes_sorted]},
-                     "plain": {"gcups": round(tot_cells / (t_plain * 1e-3) / 1e9, 3), "ms": round(t_plain, 4),
+                     "plain_sorted": {"gcups": gc(t_plain_len), "ms": round(t_plain_len, 4),
+                                      "kernel": "one 32-lane block per job, anti-diagonal wavefront, jobs by "
+                                                "decreasing query then target length (host order, untimed)"},
+                     "plain": {"gcups": gc(t_plain), "ms": round(t_plain, 4),
                                "kernel": "one 32-lane block per job, anti-diagonal wavefront, input order"}},
+            "speedup_learned_vs_plain_sorted": round(t_plain_len / t_learned, 3),
             "speedup_learned_vs_plain": round(t_plain / t_learned, 3),
             "speedup_learned_vs_sorted": round(t_sorted / t_learned, 3),
             "cost_model": {**train_metrics, "prediction_on_this_batch": pred_err},
             "autotune_s": round(t_tune, 2),
-            "e2e": {"value": round(tot_cells / (t_e2e * 1e-3) / 1e9, 3), "unit": "GCUPS",
+            "e2e": {"value": gc(t_e2e), "unit": "GCUPS",
                     "ms_per_step": round(t_e2e, 4), "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                     "api": "g3x_pipe_submit per step (pinned host buffers; copies overlap the "
                            "neighbouring steps' extension), g3x_pipe_wait after the K steps",
                     "outputs_equal_plain_kernel": e2e_exact},
             "roofline": {"bound": "int_alu", "kernel": f"{dom['kernel']} (width class {dom['width']})",
-                         "achieved": dom["gcups"], "peak": round(peak_gcups, 3), "unit": "GCUPS",
-                         "frac": round(dom["gcups"] / peak_gcups, 4),
-                         "traffic": TRAFFIC_PER_LAUNCH.get((dom["kernel"], dom["width"])),
+                         "achieved": dom["gcups"], "peak": round(dom_peak, 3), "unit": "GCUPS",
+                         "frac": round(dom["gcups"] / dom_peak, 4),
+                         "traffic": None if tpj is None else int(tpj * dom["jobs"]),
                          "traffic_unit": "DRAM bytes per launch",
+                         "alg_bytes": dom["alg_bytes"],
                          "algorithmic": "cells of the class launch (trip count of ksw.cu:346) / its "
                                         "CUDA-event duration, the class launched alone on the bench stream",
+                         "peak_def": f"{dom['arith']} cells/s roofline: measured 32-bit int ops/s / 8 ops per "
+                                     "cell" + (", x2 (two cells per int16x2 instruction)" if dom["arith"] == "int16x2" else ""),
+                         "peak_source": "measured live: g3x_int_peak (DPX VIMNMX3 chains, 32-bit int ops/s)",
+                         "int_ops_per_s": peak_ops, "int32_peak_gcups": round(peak32, 3),
+                         "int16x2_peak_gcups": round(2 * peak32, 3),
+                         "step_frac": round(ideal_ms / t_step, 4),
+                         "step_frac_def": "sum over classes of cells / that class kernel's roofline, over the step time",
                          "class_ms_side_by_side": [c["ms"] for c in classes_conc],
-                         "peak_source": "measured live: g3x_int_peak (DPX VIMNMX3 chains, 32-bit int ops/s) / 8 ops per cell",
-                         "int_ops_per_s": peak_ops, "step_frac": round(gcups / max(ws, 1) / peak_gcups, 4),
                          "classes": classes},
             "hbm_job_stream": {"achieved_gbs": round(bi / (t_step * 1e-3) / 1e9, 2), "peak_gbs": hbm_peak,
                                "frac": round(bi / (t_step * 1e-3) / 1e9 / hbm_peak, 5),

@@ -11,10 +11,11 @@
 # 39-60), the seed filter of long reads (bwa/src/aux.cu:117-162 with bwa/src/bntseq.cu:7-87),
 # plus the ctypes batch driver ref_wrap.cpp.  The source lines are streamed from the
 # reference tree into the compiler; no reference source is copied into this repository.
-# Usage: sh oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: sh oracle/build_ref.sh [reference_root]
+#   (default: $G3X_REFERENCE, else a checkout named "reference" beside this repository)
 set -eu
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${1:-${G3X_REFERENCE:-/root/reference}}
+REF=${1:-${G3X_REFERENCE:-$(cd "$HERE/../.." && pwd)/reference}}
 SRC="$REF/bwa/src/ksw.cu"
 OUT="$HERE/_ref"
 if [ ! -f "$SRC" ]; then
