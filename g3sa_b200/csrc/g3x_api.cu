@@ -165,18 +165,6 @@ static int alloc_sched(SchedScratch& s, int64_t n) {
     return G3X_OK;
 }
 
-// Default width classes: each uses the narrowest group whose tile (lanes x odd cells per lane)
-// covers the class width; the last class tiles wider rows.
-static void default_tiles(TileTable& t) {
-    const int w[] = {20, 36, 72, 144, 288, 0x7FFFFFFF};
-    const int l[] = {4, 4, 8, 16, 32, 32};
-    const int c[] = {5, 9, 9, 9, 9, 9};
-    t.n = 6;
-    for (int k = 0; k < t.n; ++k) {
-        t.width[k] = w[k]; t.lanes[k] = l[k]; t.tile[k] = c[k]; t.warp_batch[k] = 0; t.refill[k] = 1;
-    }
-}
-
 // Largest query a class stages: its width, except for the unbounded last class.
 int class_qcap(const TileTable& t, int k, int qmax) {
     return k == t.n - 1 ? qmax : std::min(qmax, t.width[k]);

@@ -57,6 +57,19 @@ struct TileTable {
     int32_t refill[kMaxBuckets];
 };
 
+// The width classes a new context starts with (and the no-alloc entry point always uses): each
+// runs the row-parallel kernel with the narrowest group whose tile (lanes x odd cells per lane)
+// covers the class width; the last class tiles wider rows.
+inline void default_tiles(TileTable& t) {
+    const int w[] = {20, 36, 72, 144, 288, 0x7FFFFFFF};
+    const int l[] = {4, 4, 8, 16, 32, 32};
+    const int c[] = {5, 9, 9, 9, 9, 9};
+    t.n = 6;
+    for (int k = 0; k < t.n; ++k) {
+        t.width[k] = w[k]; t.lanes[k] = l[k]; t.tile[k] = c[k]; t.warp_batch[k] = 0; t.refill[k] = 1;
+    }
+}
+
 // Sort bins per width class of schedule_jobs (its histogram holds kMaxBuckets * kSchedLevels).
 constexpr int kSchedLevels = 2048;
 

@@ -11,8 +11,16 @@
 // cudaFree would synchronise with the whole device; a caller that has reserved nearly all of
 // the GPU's memory for its index and batches up front (as the reference's pipeline does in
 // device_alloc) and has nothing left for a library to grow into; and a caller inside a
-// framework whose allocator owns all device memory.  The array is part of the library's
-// module image and is set up with it, so these calls only look its address up.
+// framework whose allocator owns all device memory.
+//
+// Set-up: CUDA loads a library's device code, and with it this array, on first use (lazy
+// module loading, the default unless CUDA_MODULE_LOADING=EAGER), and loading may allocate
+// device memory and synchronise.  So the first call on a device -- which also looks the array's
+// address up with cudaGetSymbolAddress, once per device -- belongs before the phase in which
+// nothing may allocate: one call with a small batch loads every kernel the entry point
+// launches, and a call with n = 0 does the address look-up alone.  The address is kept per
+// device index and belongs to the device's primary context (the one the runtime API uses):
+// the entry point assumes that context throughout, with no cudaDeviceReset between calls.
 //
 // Limits: at most G3X_NOALLOC_MAX_JOBS jobs per call (larger batches return
 // G3X_ERR_SCRATCH).  Every call on a device shares the one array, so calls that overlap on
@@ -58,17 +66,6 @@ int scratch_of(int device, int32_t** out) {
     return G3X_OK;
 }
 
-// The width classes g3x_ctx_create starts a context with.
-void fixed_tiles(TileTable& t) {
-    const int w[] = {20, 36, 72, 144, 288, 0x7FFFFFFF};
-    const int l[] = {4, 4, 8, 16, 32, 32};
-    const int c[] = {5, 9, 9, 9, 9, 9};
-    t.n = 6;
-    for (int k = 0; k < t.n; ++k) {
-        t.width[k] = w[k]; t.lanes[k] = l[k]; t.tile[k] = c[k]; t.warp_batch[k] = 0; t.refill[k] = 1;
-    }
-}
-
 }  // namespace
 
 }  // namespace g3x
@@ -81,15 +78,15 @@ extern "C" int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t* scor
     using namespace g3x;
     if (n < 0) return G3X_ERR_INVALID;
     if (n > G3X_NOALLOC_MAX_JOBS) return G3X_ERR_SCRATCH;
+    int rc;
+    if (cudaSetDevice(device) != cudaSuccess) return G3X_ERR_CUDA;
+    int32_t* s = nullptr;
+    if ((rc = scratch_of(device, &s))) return rc;
     if (n == 0) return G3X_OK;
     if (!d_jobs || !d_codes || !d_nmask || !d_out || !d_status) return G3X_ERR_INVALID;
     if (max_qlen < 0 || max_tlen < 0 || max_qlen > 65534 || max_tlen > 65535) return G3X_ERR_INVALID;
     ScoreParams sp;
-    int rc = score_params(score, &sp);
-    if (rc) return rc;
-    if (cudaSetDevice(device) != cudaSuccess) return G3X_ERR_CUDA;
-    int32_t* s = nullptr;
-    if ((rc = scratch_of(device, &s))) return rc;
+    if ((rc = score_params(score, &sp))) return rc;
     cudaStream_t st = (cudaStream_t)stream;
 
     // Sort scratch: schedule_jobs clears the histogram itself and writes the keys, cursors,
@@ -102,7 +99,7 @@ extern "C" int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t* scor
     sc.bucket_oc = s + kBucketAt;
     sc.cap = G3X_NOALLOC_MAX_JOBS;
     TileTable tt;
-    fixed_tiles(tt);
+    default_tiles(tt);
     if ((rc = schedule_jobs(sc, d_jobs, n, sp, nullptr, tt, st))) return rc;
     // The persistent kernels take jobs from a counter that must start at zero.
     if (cudaMemsetAsync(s + kQueueAt, 0, kMaxBuckets * sizeof(int32_t), st) != cudaSuccess)

@@ -130,10 +130,14 @@ int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
    the GPU's memory up front (as the reference's device_alloc does); a framework whose
    allocator owns all device memory.  It needs no context: its scratch (sort keys, job order,
    histogram, per-class job counters) is one static device array of the library, 8.13 MiB,
-   looked up once per device.  At most G3X_NOALLOC_MAX_JOBS jobs per call, else
-   G3X_ERR_SCRATCH.  All calls on a device share that array: calls that overlap on the GPU
-   (two streams, two host threads) race and corrupt each other's results, so serialise them.
-   Makes `device` current.  Asynchronous on `stream`. */
+   whose address the first call on a device looks up (cudaGetSymbolAddress).  CUDA loads the
+   library's kernels and that array lazily, on first use, and loading may allocate device memory
+   and synchronise: make one call with a small batch on each device before the phase in which
+   nothing may allocate (n = 0 does the address look-up alone).  The address belongs to the
+   device's primary context: no cudaDeviceReset between calls.  At most G3X_NOALLOC_MAX_JOBS
+   jobs per call, else G3X_ERR_SCRATCH.  All calls on a device share that array: calls that
+   overlap on the GPU (two streams, two host threads) race and corrupt each other's results,
+   so serialise them.  Makes `device` current.  Asynchronous on `stream`. */
 #define G3X_NOALLOC_MAX_JOBS 1048576
 int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t *score, const g3x_job_t *d_jobs,
                                   int32_t n, const uint32_t *d_codes, const uint32_t *d_nmask,
