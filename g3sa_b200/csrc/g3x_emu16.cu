@@ -53,17 +53,22 @@ int run_job(const g3x_job_t& jb, const uint8_t* u8, const ScoreParams& sp, const
     const bool qrev = (jb.flags & G3X_JOB_QREV) != 0, trev = (jb.flags & G3X_JOB_TREV) != 0;
     for (int k = 0; k < c.qlen; ++k)
         qn[(size_t)(k >> 3) * 32] |= (uint32_t)base_at(u8, jb.q_off, c.qlen, k, qrev) << ((k & 7) * 4);
-    for (int b = 0; b <= ((c.qlen + 1) >> 3); ++b) {
-        uint32_t* h = reinterpret_cast<uint32_t*>(&H[(size_t)b * 32]);
-        for (int p = 0; p < 4; ++p)
-            h[p] = ((uint32_t)init_h(8 * b + p, c) & 0xFFFFu) | ((uint32_t)init_h(8 * b + p + 4, c) << 16);
-    }
+    // stale words from an earlier job, as a lane of the kernel finds its row buffer
+    for (auto& v : H) v = make_uint4(0x1357u, 0x2468u, 0x1111u, 0x2222u);
+    for (auto& v : E) v = make_uint4(0x0123u, 0x0456u, 0x0789u, 0x0abcu);
     l16::Planes P;
     P.H = H.data(); P.E = E.data();
     P.H32 = reinterpret_cast<uint32_t*>(P.H);
     P.E32 = reinterpret_cast<uint32_t*>(P.E);
     P.qn = qn.data();
     const l16::PairConst pc = l16::pair_const(sp);
+    l16::init_row(P, 0, c.qlen, c.h0, sp, pc, ge);
+    for (int b = 0; b <= ((c.qlen + 1) >> 3); ++b) {      // the closed form against init_h
+        const uint32_t* h = reinterpret_cast<const uint32_t*>(&H[(size_t)b * 32]);
+        for (int p = 0; p < 4; ++p)
+            if (h[p] != (((uint32_t)init_h(8 * b + p, c) & 0xFFFFu) | ((uint32_t)init_h(8 * b + p + 4, c) << 16)))
+                return G3X_ERR_INTERNAL;
+    }
     l16::LaneJob J;
     J.job = 0;
     J.qlen = c.qlen; J.tlen = c.tlen; J.w = c.w; J.h0 = c.h0;
@@ -81,8 +86,12 @@ int run_job(const g3x_job_t& jb, const uint8_t* u8, const ScoreParams& sp, const
         l16::RowState r;
         l16::row_begin(J, sp, pools, r);
         const bool nonempty = r.beg < r.end;
-        l16::row_blocks<kSym>(P, 0, r, pc, ge);
-        l16::row_end(J, P, 0, r, sp, nonempty);
+        const int nblk = l16::blocks_in_row(r);
+        // the warp's widest row in the kernel can have more blocks than this lane's: vary it
+        const int kmax = nblk + (int)((i * 2654435761u + (uint32_t)jb.q_off) >> 30);
+        uint32_t mF, mL;
+        l16::row_blocks<kSym>(P, 0, r, pc, ge, nblk, kmax, mF, mL);
+        l16::row_end(J, P, 0, r, sp, nonempty, mF, mL);
     }
     const Commit& K = J.K;
     *out = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};

@@ -5,8 +5,8 @@
 // begin, the blocks of a row, the row end with its band trims) is in g3x_lane16.cuh, where the
 // arithmetic and the band handling are described.  This file is the warp around it:
 //  * refill waves: the warp takes a new job for every idle lane at once (one atomicAdd on the
-//    class's job queue), each new lane stages its query as 4-bit codes from the bit planes, and
-//    the warp writes row -1 of every new job's row buffer (ksw.cu:317-319) cooperatively;
+//    class's job queue), and each new lane stages its query as 4-bit codes from the bit planes
+//    and writes row -1 of its row buffer (ksw.cu:317-319);
 //  * row-synchronous rows: all lanes begin a row together, walk it block by block (a lane with a
 //    shorter row sits out the extra iterations), and end it together;
 //  * a lane whose job ends writes the job's outputs and status and idles until the next wave.
@@ -71,7 +71,6 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
             first = __shfl_sync(0xFFFFFFFFu, first, 0);
             if (first + want >= n) exhausted = true;
             ++waves;
-            int my_job = -1;
             if ((idle_mask >> lane) & 1u) {
                 const int slot = first + __popc(idle_mask & ((1u << lane) - 1u));
                 if (slot < n) {
@@ -87,36 +86,21 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
                         d.status[job] = G3X_ERR_TOO_LONG;
                         if (d.cells) d.cells[job] = 0;
                     } else {
-                        my_job = job;
                         J.job = job;
                         J.qlen = c.qlen; J.tlen = c.tlen; J.w = c.w; J.h0 = c.h0;
                         J.t_off = jb.t_off;
                         J.trev = (jb.flags & G3X_JOB_TREV) != 0;
                         commit_init(J.K, c);
                         J.beg = 0; J.end = c.qlen;
-                        J.tx = J.tn = J.px = J.pn = 0;
+                        J.tx = J.tn = 0;
+                        J.pv = J.pm = 0;
                         if (c.tlen > 0) load16(d.codes, d.nmask, J.t_off, c.tlen, 0, J.trev, J.tx, J.tn);
-                        if (c.tlen > 16) load16(d.codes, d.nmask, J.t_off, c.tlen, 1, J.trev, J.px, J.pn);
+                        if (c.tlen > 16) load16_raw(d.codes, d.nmask, J.t_off, c.tlen, 1, J.trev, J.pv, J.pm);
                         stage_own_query(d.codes, d.nmask, jb.q_off, c.qlen, (jb.flags & G3X_JOB_QREV) != 0,
                                         (c.qlen + 15) >> 4, qn, lane);
+                        // row -1 of the new job (ksw.cu:317-319), each new lane its own
+                        init_row(P, lane, c.qlen, c.h0, sp, pc, ge);
                     }
-                }
-            }
-            // row -1 of every new job (ksw.cu:317-319), the whole warp on one job at a time:
-            // H pairs from the closed form, E = 0, blocks 0 .. (qlen + 1) / 8
-            unsigned m = __ballot_sync(0xFFFFFFFFu, my_job >= 0);
-            while (m) {
-                const int L = __ffs(m) - 1;
-                m &= m - 1;
-                const int qlen = __shfl_sync(0xFFFFFFFFu, J.qlen, L);
-                JobConst c;
-                c.qlen = qlen; c.h0 = __shfl_sync(0xFFFFFFFFu, J.h0, L); c.oe_ins = sp.oe_ins; c.e_ins = sp.e_ins;
-                const int words = (((qlen + 1) >> 3) + 1) * 4;
-                for (int k = lane; k < words; k += 32) {
-                    const int b = k >> 2, p = k & 3;
-                    const int32_t lo = init_h(8 * b + p, c), hi = init_h(8 * b + p + 4, c);
-                    P.H32[((b << 5) + L) * 4 + p] = ((uint32_t)lo & 0xFFFFu) | ((uint32_t)hi << 16);
-                    P.E32[((b << 5) + L) * 4 + p] = 0u;
                 }
             }
             __syncwarp();
@@ -133,28 +117,25 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
         r.beg = 0; r.end = 0; r.h1 = 0; r.plo = 0; r.phi = 0; r.fr = 0; r.hlast = 0; r.key = 0;
         if (run) {
             const int32_t i = J.K.next;
-            if ((i & 15) == 0 && i > 0) {
-                J.tx = J.px; J.tn = J.pn;
+            if ((i & 15) == 0 && i > 0) {       // the prefetched chunk, then the next one's words
+                decode16(J.t_off, J.tlen, i >> 4, J.trev, J.pv, J.pm, J.tx, J.tn);
                 const int ch = (i >> 4) + 1;
-                if ((ch << 4) < J.tlen) load16(d.codes, d.nmask, J.t_off, J.tlen, ch, J.trev, J.px, J.pn);
+                if ((ch << 4) < J.tlen) load16_raw(d.codes, d.nmask, J.t_off, J.tlen, ch, J.trev, J.pv, J.pm);
             }
             row_begin(J, sp, pools, r);
         }
         const bool nonempty = run && r.beg < r.end;
-        const int32_t jb0 = r.beg & ~(kLB - 1);
-        const int nblk = nonempty ? ((r.end - 1) >> 3) - (r.beg >> 3) + 1 : 0;
+        const int nblk = run ? blocks_in_row(r) : 0;
         const int kmax = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nblk);
         busy += nblk;
         idle += kmax - nblk;
 
-        // ---- the row's blocks: masked first block, middle blocks, masked last block ----
-        if (nblk > 1) block_first<kSym>(P, lane, jb0, r, pc, ge);
-        for (int k = 1; k < kmax - 1; ++k)
-            if (k < nblk - 1) block_mid<kSym>(P, lane, jb0 + k * kLB, r, pc);
-        if (nblk > 0) block_last<kSym>(P, lane, jb0 + (nblk - 1) * kLB, nblk == 1, r, pc, ge);
+        // ---- the row's blocks: masked first block, middle blocks two at a time, masked last block ----
+        uint32_t mF, mL;
+        row_blocks<kSym>(P, lane, r, pc, ge, nblk, kmax, mF, mL);
 
         // ---- row end (ksw.cu:371-391) ----
-        if (run) row_end(J, P, lane, r, sp, nonempty);
+        if (run) row_end(J, P, lane, r, sp, nonempty, mF, mL);
         if (active && J.K.stop) {
             const Commit& K = J.K;
             d.out[J.job] = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};

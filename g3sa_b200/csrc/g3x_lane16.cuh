@@ -116,6 +116,7 @@ struct PairConst {
     uint32_t noe_del, ne_del, noe_ins, ne_ins;
     uint32_t nt[4];     // -p e_ins
     uint32_t n4;        // -4 e_ins
+    uint32_t ni[4];     // (-p e_ins, -(p + 4) e_ins)
     uint32_t kmul;      // 2^k: M = min(H + S, H * 2^k)
 };
 
@@ -129,6 +130,8 @@ G3X_HD PairConst pair_const(const ScoreParams& sp) {
     pc.ne_ins = rep16(-sp.e_ins);
     for (int p = 0; p < 4; ++p) pc.nt[p] = rep16(-p * sp.e_ins);
     pc.n4 = rep16(-4 * sp.e_ins);
+    for (int p = 0; p < 4; ++p)
+        pc.ni[p] = ((uint32_t)(-p * sp.e_ins) & 0xFFFFu) | ((uint32_t)(-(p + 4) * sp.e_ins) << 16);
     pc.kmul = 1u << int16_shift(sp.max_sc);
     return pc;
 }
@@ -148,38 +151,56 @@ struct RowState {
     int32_t key;         // row maximum << 16 | block index of its last block reaching it
 };
 
-// The block arithmetic on loaded (and masked) words; returns the new H and E words, the H of
-// the block's columns (h2), and advances fr and hlast.  kSym: oe_del == oe_ins, so the E step
-// reuses max(M - oe_ins, 0).
+// The part of a block that does not depend on F entering it: scores, M, each half's prefix of
+// T (L), and the E step, which uses M only.
+struct BlockA {
+    uint32_t M2[4], E2[4], L2[4];
+};
+
+// kSym: oe_del == oe_ins, so the E step reuses max(M - oe_ins, 0).
 template <bool kSym>
-G3X_HD void block_core(const uint32_t (&H2)[4], const uint32_t (&E2)[4], uint32_t qw, RowState& r,
-                       const PairConst& pc, uint32_t (&nh)[4], uint32_t (&ne)[4], uint32_t (&h2)[4]) {
+G3X_HD void phase_a(const uint32_t (&H2)[4], const uint32_t (&E2)[4], uint32_t qw, const RowState& r,
+                    const PairConst& pc, BlockA& a, uint32_t (&ne)[4]) {
     const uint32_t sc_lo = prmt(r.plo, r.phi, qw);   // prmt reads selector bits 0-15 only
     const uint32_t sc_hi = prmt(r.plo, r.phi, qw >> 16);
     const uint32_t S2[4] = {pair_score<0>(sc_lo, sc_hi), pair_score<1>(sc_lo, sc_hi),
                             pair_score<2>(sc_lo, sc_hi), pair_score<3>(sc_lo, sc_hi)};
-    uint32_t M2[4], T2[4], L2[4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
-        M2[p] = __viaddmin_s16x2(H2[p], S2[p], H2[p] * pc.kmul);
-        T2[p] = __viaddmax_s16x2(M2[p], pc.noe_ins, 0u);
-        L2[p] = p == 0 ? T2[0] : __viaddmax_s16x2(L2[p - 1], pc.ne_ins, T2[p]);
-    }
-    // (F_in, F(4)), then every F of the block
-    const uint32_t fin = prmt(r.fr, r.fr, 0x3232u);
-    const uint32_t x = __viaddmax_s16x2(fin, pc.n4, L2[3]);                  // low half: F(4)
-    const uint32_t fp = prmt(r.fr, x, 0x5432u);
-    r.fr = __viaddmax_s16x2(fp, pc.n4, L2[3]);                              // high half: F(8)
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        const uint32_t F2 = p == 0 ? fp : __viaddmax_s16x2(fp, pc.nt[p], L2[p - 1]);
-        h2[p] = __vimax3_s16x2(M2[p], E2[p], F2);
-        const uint32_t te = kSym ? T2[p] : __viaddmax_s16x2(M2[p], pc.noe_del, 0u);
+        a.E2[p] = E2[p];
+        a.M2[p] = __viaddmin_s16x2(H2[p], S2[p], H2[p] * pc.kmul);
+        const uint32_t T2 = __viaddmax_s16x2(a.M2[p], pc.noe_ins, 0u);
+        a.L2[p] = p == 0 ? T2 : __viaddmax_s16x2(a.L2[p - 1], pc.ne_ins, T2);
+        const uint32_t te = kSym ? T2 : __viaddmax_s16x2(a.M2[p], pc.noe_del, 0u);
         ne[p] = __viaddmax_s16x2(E2[p], pc.ne_del, te);
+    }
+}
+
+// The part that takes F in: (F_in, F(4)), every F and H of the block, the new H words; advances
+// fr and hlast.
+G3X_HD void phase_b(const BlockA& a, RowState& r, const PairConst& pc, uint32_t (&nh)[4], uint32_t (&h2)[4]) {
+    const uint32_t fin = prmt(r.fr, r.fr, 0x3232u);
+    const uint32_t x = __viaddmax_s16x2(fin, pc.n4, a.L2[3]);                // low half: F(4)
+    const uint32_t fp = prmt(r.fr, x, 0x5432u);
+    r.fr = __viaddmax_s16x2(fp, pc.n4, a.L2[3]);                             // high half: F(8)
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const uint32_t F2 = p == 0 ? fp : __viaddmax_s16x2(fp, pc.nt[p], a.L2[p - 1]);
+        h2[p] = __vimax3_s16x2(a.M2[p], a.E2[p], F2);
     }
     nh[0] = prmt(r.hlast, h2[3], 0x5432u);
     nh[1] = h2[0]; nh[2] = h2[1]; nh[3] = h2[2];
     r.hlast = h2[3];
+}
+
+// The whole block on loaded (and masked) words: the new H and E words and the H of the block's
+// columns (h2); advances fr and hlast.
+template <bool kSym>
+G3X_HD void block_core(const uint32_t (&H2)[4], const uint32_t (&E2)[4], uint32_t qw, RowState& r,
+                       const PairConst& pc, uint32_t (&nh)[4], uint32_t (&ne)[4], uint32_t (&h2)[4]) {
+    BlockA a;
+    phase_a<kSym>(H2, E2, qw, r, pc, a, ne);
+    phase_b(a, r, pc, nh, h2);
 }
 
 // Row maximum of a block (of the given H words) into the running key.
@@ -188,6 +209,17 @@ G3X_HD void block_max(const uint32_t (&hm)[4], int32_t kb, RowState& r) {
     const uint32_t bx = __vimax3_s16x2(b2, prmt(b2, b2, 0x1032u), b2);   // max in both halves
     const int32_t key = (int32_t)prmt((uint32_t)kb, bx, 0x7610u);        // (max << 16) | kb
     r.key = r.key > key ? r.key : key;
+}
+
+// Bit t set when column jb+t of a block's words (H and E pairs in registers) is non-zero: every
+// half-word is reduced to 0 or 1 by an unsigned min, then the four pairs are summed with weights
+// 1-8 (each half stays below 16), which leaves columns 0-3 in bits 0-3 and 4-7 in bits 16-19.
+G3X_HD uint32_t nonzero_mask(const uint32_t (&h)[4], const uint32_t (&e)[4]) {
+    const uint32_t one = 0x00010001u;
+    const uint32_t z0 = __vimin3_u16x2(h[0] | e[0], one, one), z1 = __vimin3_u16x2(h[1] | e[1], one, one);
+    const uint32_t z2 = __vimin3_u16x2(h[2] | e[2], one, one), z3 = __vimin3_u16x2(h[3] | e[3], one, one);
+    const uint32_t s = z0 + 2u * z1 + 4u * z2 + 8u * z3;
+    return (s & 0xFu) | ((s >> 12) & 0xF0u);
 }
 
 // A block strictly inside the row.
@@ -203,10 +235,45 @@ G3X_HD void block_mid(const Planes& P, int lane, int32_t jb, RowState& r, const 
     block_max(h2, jb >> 3, r);
 }
 
-// The first block of a row with two or more blocks: the words left of beg are zeroed on load.
+// Two consecutive blocks strictly inside the row, the second only when `second` (else nothing of
+// it is stored and the row state stays as the first block leaves it).  The F-independent
+// phases of both blocks come first, so the two blocks' instructions interleave.
 template <bool kSym>
-G3X_HD void block_first(const Planes& P, int lane, int32_t jb, RowState& r, const PairConst& pc,
-                        const uint4* ge) {
+G3X_HD void block_mid2(const Planes& P, int lane, int32_t jb, bool second, RowState& r, const PairConst& pc) {
+    const int at = ((jb >> 3) << 5) + lane;
+    const uint4 hq0 = P.H[at], eq0 = P.E[at], hq1 = P.H[at + 32], eq1 = P.E[at + 32];
+    const uint32_t qw0 = P.qn[(jb >> 3) * 32 + lane], qw1 = P.qn[((jb >> 3) + 1) * 32 + lane];
+    BlockA a0, a1;
+    uint32_t ne0[4], ne1[4];
+    {
+        const uint32_t H2[4] = {hq0.x, hq0.y, hq0.z, hq0.w}, E2[4] = {eq0.x, eq0.y, eq0.z, eq0.w};
+        phase_a<kSym>(H2, E2, qw0, r, pc, a0, ne0);
+    }
+    {
+        const uint32_t H2[4] = {hq1.x, hq1.y, hq1.z, hq1.w}, E2[4] = {eq1.x, eq1.y, eq1.z, eq1.w};
+        phase_a<kSym>(H2, E2, qw1, r, pc, a1, ne1);
+    }
+    uint32_t nh0[4], h20[4], nh1[4], h21[4];
+    phase_b(a0, r, pc, nh0, h20);
+    RowState r1 = r;
+    phase_b(a1, r1, pc, nh1, h21);
+    P.E[at] = make_uint4(ne0[0], ne0[1], ne0[2], ne0[3]);
+    P.H[at] = make_uint4(nh0[0], nh0[1], nh0[2], nh0[3]);
+    block_max(h20, jb >> 3, r);
+    if (second) {
+        P.E[at + 32] = make_uint4(ne1[0], ne1[1], ne1[2], ne1[3]);
+        P.H[at + 32] = make_uint4(nh1[0], nh1[1], nh1[2], nh1[3]);
+        r.fr = r1.fr;
+        r.hlast = r1.hlast;
+        block_max(h21, (jb >> 3) + 1, r);
+    }
+}
+
+// The first block of a row with two or more blocks: the words left of beg are zeroed on load.
+// Returns the columns of the block at or right of beg whose new H or E word is non-zero.
+template <bool kSym>
+G3X_HD uint32_t block_first(const Planes& P, int lane, int32_t jb, RowState& r, const PairConst& pc,
+                            const uint4* ge) {
     const int at = ((jb >> 3) << 5) + lane;
     const uint4 hq = P.H[at], eq = P.E[at];
     const uint4 A = ge[r.beg - jb];
@@ -217,12 +284,16 @@ G3X_HD void block_first(const Planes& P, int lane, int32_t jb, RowState& r, cons
     P.H[at] = make_uint4(nh[0], nh[1], nh[2], nh[3]);
     P.E[at] = make_uint4(ne[0], ne[1], ne[2], ne[3]);
     block_max(h2, jb >> 3, r);
+    return nonzero_mask(nh, ne) & (0xFFu << (r.beg - jb));
 }
 
 // The last block of a row (first == true: also its first, the row's only block): columns right of
-// end keep their words, columns >= end stay out of the row maximum, r.h1 = H(i, end - 1).
+// end keep their words, columns >= end stay out of the row maximum, r.h1 = H(i, end - 1).  When
+// column end is in the block its words become {h1, 0} here (ksw.cu:371): its H word is H(i, end-1)
+// as computed, its E word is cleared.  Returns the columns of the block up to column end whose
+// new H or E word is non-zero.
 template <bool kSym>
-G3X_HD void block_last(const Planes& P, int lane, int32_t jb, bool first, RowState& r,
+G3X_HD uint32_t block_last(const Planes& P, int lane, int32_t jb, bool first, RowState& r,
                        const PairConst& pc, const uint4* ge) {
     const int at = ((jb >> 3) << 5) + lane;
     const uint4 hq = P.H[at], eq = P.E[at];
@@ -231,7 +302,7 @@ G3X_HD void block_last(const Planes& P, int lane, int32_t jb, bool first, RowSta
     const uint4 gv = ge[hi], gw = ge[hi + 1];
     const uint32_t Hq[4] = {hq.x, hq.y, hq.z, hq.w}, Eq[4] = {eq.x, eq.y, eq.z, eq.w};
     const uint32_t Am[4] = {A.x, A.y, A.z, A.w}, V[4] = {~gv.x, ~gv.y, ~gv.z, ~gv.w};
-    const uint32_t W[4] = {~gw.x, ~gw.y, ~gw.z, ~gw.w};
+    const uint32_t G[4] = {gw.x, gw.y, gw.z, gw.w};   // columns right of end
     uint32_t H2[4], E2[4];
 #pragma unroll
     for (int p = 0; p < 4; ++p) { H2[p] = Hq[p] & Am[p]; E2[p] = Eq[p] & Am[p]; }
@@ -239,8 +310,8 @@ G3X_HD void block_last(const Planes& P, int lane, int32_t jb, bool first, RowSta
     block_core<kSym>(H2, E2, P.qn[(jb >> 3) * 32 + lane], r, pc, nh, ne, h2);
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
-        nh[p] = (nh[p] & W[p]) | (Hq[p] & ~W[p]);   // columns <= end: new; beyond: as they were
-        ne[p] = (ne[p] & W[p]) | (Eq[p] & ~W[p]);
+        nh[p] = (nh[p] & ~G[p]) | (Hq[p] & G[p]);   // columns <= end: new; beyond: as they were
+        ne[p] = (ne[p] & V[p]) | (Eq[p] & G[p]);    // columns < end: new; end: 0; beyond: as they were
         hm[p] = h2[p] & V[p];
     }
     P.H[at] = make_uint4(nh[0], nh[1], nh[2], nh[3]);
@@ -249,6 +320,7 @@ G3X_HD void block_last(const Planes& P, int lane, int32_t jb, bool first, RowSta
     const int t = hi - 1;
     const uint32_t wl = (t & 2) ? ((t & 1) ? h2[3] : h2[2]) : ((t & 1) ? h2[1] : h2[0]);
     r.h1 = (int32_t)((t & 4) ? (wl >> 16) : (wl & 0xFFFFu));
+    return nonzero_mask(nh, ne) & (0xFFu >> (7 - (hi < 8 ? hi : 7)));
 }
 
 // Bit t set when column b+t (b a multiple of 8) has a non-zero H or E word: every half-word is
@@ -292,7 +364,8 @@ struct LaneJob {
     int32_t trev;
     Commit K;
     int32_t beg, end;        // band of the next row before the clamps of ksw.cu:338-340
-    uint32_t tx, tn, px, pn; // target chunk K.next >> 4 and the next one
+    uint32_t tx, tn;         // target chunk K.next >> 4: 2-bit codes and N bits
+    uint64_t pv, pm;         // the plane words of the next chunk (kernel prefetch)
 };
 
 G3X_HD JobConst job_const(const LaneJob& J, const ScoreParams& sp) {
@@ -325,13 +398,42 @@ G3X_HD void row_begin(const LaneJob& J, const ScoreParams& sp, const uint2* pool
     r.key = 0;
 }
 
+// The row bookkeeping of ksw.cu:372-386 (the same as commit_row) with selects in place of
+// branches: to-end score, cell count, new maximum or z-drop, last row.
+G3X_HD void commit_row_sel(Commit& k, const JobConst& c, const RowDone& d) {
+    const int32_t i = k.next;
+    const bool g = d.gval >= 0;
+    k.max_ie = (g && !(k.gscore > d.gval)) ? i : k.max_ie;                  // ksw.cu:372-375
+    k.gscore = (g && d.gval > k.gscore) ? d.gval : k.gscore;
+    k.cells += d.ncells;
+    k.next = i + 1;
+    const bool up = d.m > k.best;                                            // ksw.cu:377-379
+    const int32_t di = i - k.best_i, dj = d.mj - k.best_j;                   // ksw.cu:380-386
+    const int32_t drop = di > dj ? k.best - d.m - (di - dj) * c.e_del : k.best - d.m - (dj - di) * c.e_ins;
+    const bool zstop = !up && c.zdrop > 0 && drop > c.zdrop;
+    const int32_t off = d.mj > i ? d.mj - i : i - d.mj;
+    k.max_off = up && off > k.max_off ? off : k.max_off;
+    k.best = up ? d.m : k.best;
+    k.best_i = up ? i : k.best_i;
+    k.best_j = up ? d.mj : k.best_j;
+    k.stop = d.m == 0 || zstop || k.next >= c.tlen;                         // ksw.cu:376, the row loop
+}
+
 // Row end (ksw.cu:371-391) for a running lane: column end's words, the row's bookkeeping, and
-// the band of the next row.
+// the band of the next row.  mF: the columns >= beg of the row's first block with a non-zero new
+// word (rows of two or more blocks); mL: those up to column end of its last block.  The first
+// non-zero column from beg and the last one back from end are almost always found in them; the
+// row buffer is read only when not.
 G3X_HD void row_end(LaneJob& J, const Planes& P, int lane, const RowState& r, const ScoreParams& sp,
-                    bool nonempty) {
+                    bool nonempty, uint32_t mF, uint32_t mL) {
     const int32_t beg = r.beg, end = r.end;
-    set_col(P.H32, end, lane, r.h1);
-    set_col(P.E32, end, lane, 0);
+    const int32_t jb0 = beg & ~(kLB - 1), jbl = (end - 1) & ~(kLB - 1);
+    // column end starts the block after the last one: its words {h1, 0} (ksw.cu:371)
+    const bool end_next = nonempty && end - jbl == kLB;
+    if (end_next) {
+        set_col(P.H32, end, lane, r.h1);
+        set_col(P.E32, end, lane, 0);
+    }
     RowDone rd;
     rd.m = r.key >> 16;
     rd.mj = -1;
@@ -341,31 +443,40 @@ G3X_HD void row_end(LaneJob& J, const Planes& P, int lane, const RowState& r, co
     }
     rd.gval = (nonempty ? end : beg) == J.qlen ? r.h1 : -1;
     rd.ncells = nonempty ? end - beg : 0;
-    commit_row(J.K, job_const(J, sp), rd);
+    commit_row_sel(J.K, job_const(J, sp), rd);
     if (J.K.stop) return;
-    // ksw.cu:388-389, eight columns at a time: the first column of [beg, end) whose H or E word
-    // is non-zero (end when none; beg itself when the band is empty) ...
-    int32_t nb = beg < end ? end : beg;
-    for (int32_t b = beg & ~(kLB - 1); b < end; b += kLB) {
-        uint32_t mk = nonzero_cols(P, b, lane);
-        if (b < beg) mk &= ~0u << (beg - b);
-        if (mk) {
-            const int32_t j = b + ffs32(mk) - 1;
-            nb = j < end ? j : end;
-            break;
+    // (a row that does not stop has a non-empty band)
+    // ksw.cu:388-389: the first column of [beg, end) whose H or E word is non-zero, else end
+    const uint32_t mk = jb0 < jbl ? mF : (mL & (0xFFu << (beg - jb0)) & (0xFFu >> (kLB - (end - jb0))));
+    int32_t nb = end;
+    if (mk) {
+        nb = jb0 + ffs32(mk) - 1;
+    } else {
+        for (int32_t b = jb0 + kLB; b < end; b += kLB) {
+            uint32_t m2 = nonzero_cols(P, b, lane);
+            if (end - b < kLB) m2 &= 0xFFu >> (kLB - (end - b));
+            if (m2) {
+                nb = b + ffs32(m2) - 1;
+                break;
+            }
         }
     }
-    // ... and ksw.cu:390-391: the last column of [nb, end] whose word is non-zero (nb - 1 if none;
-    // end itself when end < nb)
-    int32_t last = end < nb ? end : nb - 1;
-    if (end >= nb) {
-        for (int32_t b = end & ~(kLB - 1); b >= (nb & ~(kLB - 1)); b -= kLB) {
-            uint32_t mk = nonzero_cols(P, b, lane);
-            if (end - b < kLB - 1) mk &= (2u << (end - b)) - 1u;
-            if (b < nb) mk &= ~0u << (nb - b);
-            if (mk) {
-                last = b + 31 - clz32(mk);
-                break;
+    // ksw.cu:390-391: the last column of [nb, end] whose word is non-zero, else nb - 1
+    int32_t last = nb - 1;
+    if (end_next && r.h1 != 0) {
+        last = end;
+    } else if (nb <= jbl + kLB - 1) {
+        const uint32_t ml = nb > jbl ? mL & (0xFFu << (nb - jbl)) : mL;
+        if (ml) {
+            last = jbl + 31 - clz32(ml);
+        } else {
+            for (int32_t b = jbl - kLB; b >= (nb & ~(kLB - 1)); b -= kLB) {
+                uint32_t m2 = nonzero_cols(P, b, lane);
+                if (b < nb) m2 &= 0xFFu << (nb - b);
+                if (m2) {
+                    last = b + 31 - clz32(m2);
+                    break;
+                }
             }
         }
     }
@@ -374,14 +485,55 @@ G3X_HD void row_end(LaneJob& J, const Planes& P, int lane, const RowState& r, co
 }
 
 // All blocks of one row of one lane, in the order the kernel runs them.
+// The blocks of one row of one lane as the kernel's warp runs them: kmax (>= nblk) is the most
+// blocks any lane of the warp has in this row, and every lane walks the same iterations, doing
+// only its own blocks: the first (masked), the middle ones two at a time (one alone when an odd
+// number of them is left for the warp), the last (masked).  Returns the first block's and the
+// last block's non-zero column masks for row_end in mF, mL.
 template <bool kSym>
-G3X_HD void row_blocks(const Planes& P, int lane, RowState& r, const PairConst& pc, const uint4* ge) {
-    if (r.beg >= r.end) return;
+G3X_HD void row_blocks(const Planes& P, int lane, RowState& r, const PairConst& pc, const uint4* ge,
+                       int nblk, int kmax, uint32_t& mF, uint32_t& mL) {
+    mF = mL = 0;
     const int32_t jb0 = r.beg & ~(kLB - 1);
-    const int nblk = ((r.end - 1) >> 3) - (r.beg >> 3) + 1;
-    if (nblk > 1) block_first<kSym>(P, lane, jb0, r, pc, ge);
-    for (int k = 1; k < nblk - 1; ++k) block_mid<kSym>(P, lane, jb0 + k * kLB, r, pc);
-    block_last<kSym>(P, lane, jb0 + (nblk - 1) * kLB, nblk == 1, r, pc, ge);
+    if (nblk > 1) mF = block_first<kSym>(P, lane, jb0, r, pc, ge);
+    int k = 1;
+    for (; k + 1 < kmax - 1; k += 2)
+        if (k < nblk - 1) block_mid2<kSym>(P, lane, jb0 + k * kLB, k + 1 < nblk - 1, r, pc);
+    if (k < kmax - 1 && k < nblk - 1) block_mid<kSym>(P, lane, jb0 + k * kLB, r, pc);
+    if (nblk > 0) mL = block_last<kSym>(P, lane, jb0 + (nblk - 1) * kLB, nblk == 1, r, pc, ge);
+}
+
+// Blocks of a row with a non-empty band [beg, end).
+G3X_HD int blocks_in_row(const RowState& r) {
+    return r.beg < r.end ? ((r.end - 1) >> 3) - (r.beg >> 3) + 1 : 0;
+}
+
+// Row -1 of a new job in the lane's row buffer (ksw.cu:317-319), blocks 0 .. (qlen + 1) / 8:
+// H(-1, c) = h0 at column 0, then max(v1 - (c - 1) e_ins, 0) with v1 = max(h0 - oe_ins, 0) up to
+// column max(qlen, 1), zero beyond; E = 0.  Word p of block b holds columns 8b + p and 8b + p + 4:
+// max(base - p e, 0) and max(base - (p + 4) e, 0) with base = v1 - (8b - 1) e, the value of column
+// 8b, computed in int32 per block; a non-positive base leaves the block zero, and a positive one is
+// below 2^15 with base - 7 e above -2^15, so the int16 steps stay in range.
+G3X_HD void init_row(const Planes& P, int lane, int32_t qlen, int32_t h0, const ScoreParams& sp,
+                     const PairConst& pc, const uint4* ge) {
+    const int32_t v1 = h0 > sp.oe_ins ? h0 - sp.oe_ins : 0;
+    const int32_t lim = (qlen > 1 ? qlen : 1) + 1;          // first column that is zero
+    const int nb = ((qlen + 1) >> 3) + 1;
+    for (int b = 0; b < nb; ++b) {
+        const int32_t base = v1 + sp.e_ins - 8 * b * sp.e_ins;   // value of column 8b (when >= 1)
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
+        if (base > 0) {
+            const uint4 keep = ge[lim - 8 * b < 9 ? (lim - 8 * b > 0 ? lim - 8 * b : 0) : 9];
+            const uint32_t k2[4] = {~keep.x, ~keep.y, ~keep.z, ~keep.w};
+            const uint32_t b2 = rep16(base);
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+                w[p] = __viaddmax_s16x2(b2, pc.ni[p], 0u) & k2[p];
+        }
+        if (b == 0) w[0] = (w[0] & 0xFFFF0000u) | ((uint32_t)h0 & 0xFFFFu);
+        P.H[(b << 5) + lane] = make_uint4(w[0], w[1], w[2], w[3]);
+        P.E[(b << 5) + lane] = make_uint4(0u, 0u, 0u, 0u);
+    }
 }
 
 }  // namespace l16

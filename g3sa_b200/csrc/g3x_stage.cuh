@@ -60,36 +60,56 @@ __host__ __device__ inline size_t group_bytes(int qmax, int tmax) {
            (size_t)align16(5 * qstride_of(qmax)) + (size_t)align16(tgt_bytes(tmax));
 }
 
-// 16 bases of a sequence (bases 16*ch .. 16*ch+15, in the job's reading direction) as 16
-// 2-bit fields (x) and 16 N bits (nb).  Only plane words that hold valid bases are read.
-__device__ __forceinline__ void load16(const uint32_t* __restrict__ codes,
-                                       const uint32_t* __restrict__ nmask, uint32_t off,
-                                       int len, int ch, bool rev, uint32_t& x, uint32_t& nb) {
+// 16 bases of a sequence (bases 16*ch .. 16*ch+15, in the job's reading direction), in two
+// steps: load16_raw reads the plane words that hold them (only words with valid bases), and
+// decode16 turns those words into 16 2-bit fields (x) and 16 N bits (nb).  Split so that a
+// prefetch issues its loads long before the decode needs their data.
+__device__ __forceinline__ void load16_raw(const uint32_t* __restrict__ codes,
+                                           const uint32_t* __restrict__ nmask, uint32_t off,
+                                           int len, int ch, bool rev, uint64_t& v, uint64_t& m) {
     const int k0 = ch << 4;
     const int nv = len - k0 < 16 ? len - k0 : 16;
     if (!rev) {
         const uint32_t p0 = off + (uint32_t)k0;
         const uint32_t w = p0 >> 4, sh = p0 & 15u;
-        uint64_t v = __ldg(codes + w);
+        v = __ldg(codes + w);
         if (sh + (uint32_t)nv > 16u) v |= (uint64_t)__ldg(codes + w + 1) << 32;
-        x = (uint32_t)(v >> (sh << 1));
         const uint32_t nw = p0 >> 5, nsh = p0 & 31u;
-        uint64_t m = __ldg(nmask + nw);
+        m = __ldg(nmask + nw);
         if (nsh + (uint32_t)nv > 32u) m |= (uint64_t)__ldg(nmask + nw + 1) << 32;
-        nb = (uint32_t)(m >> nsh) & 0xFFFFu;
     } else {
         const uint32_t ph = off + (uint32_t)(len - 1 - k0);   // plane position of base k0
         const uint32_t w = ph >> 4, sh = ph & 15u;
-        uint64_t v = (uint64_t)__ldg(codes + w) << 32;
+        v = (uint64_t)__ldg(codes + w) << 32;
         if ((uint32_t)nv > sh + 1u) v |= __ldg(codes + w - 1);
-        uint32_t y = (uint32_t)(v >> ((sh << 1) + 2));        // field 15 = position ph
+        const uint32_t nw = ph >> 5, nsh = ph & 31u;
+        m = (uint64_t)__ldg(nmask + nw) << 32;
+        if ((uint32_t)nv > nsh + 1u) m |= __ldg(nmask + nw - 1);
+    }
+}
+
+__device__ __forceinline__ void decode16(uint32_t off, int len, int ch, bool rev, uint64_t v, uint64_t m,
+                                         uint32_t& x, uint32_t& nb) {
+    const int k0 = ch << 4;
+    if (!rev) {
+        const uint32_t p0 = off + (uint32_t)k0;
+        x = (uint32_t)(v >> ((p0 & 15u) << 1));
+        nb = (uint32_t)(m >> (p0 & 31u)) & 0xFFFFu;
+    } else {
+        const uint32_t ph = off + (uint32_t)(len - 1 - k0);
+        uint32_t y = (uint32_t)(v >> (((ph & 15u) << 1) + 2));  // field 15 = position ph
         y = __brev(y);                                          // field order reversed...
         x = ((y >> 1) & 0x55555555u) | ((y & 0x55555555u) << 1);  // ...and each field's bits
-        const uint32_t nw = ph >> 5, nsh = ph & 31u;
-        uint64_t m = (uint64_t)__ldg(nmask + nw) << 32;
-        if ((uint32_t)nv > nsh + 1u) m |= __ldg(nmask + nw - 1);
-        nb = __brev((uint32_t)(m >> (nsh + 17)) & 0xFFFFu) >> 16;
+        nb = __brev((uint32_t)(m >> ((ph & 31u) + 17)) & 0xFFFFu) >> 16;
     }
+}
+
+__device__ __forceinline__ void load16(const uint32_t* __restrict__ codes,
+                                       const uint32_t* __restrict__ nmask, uint32_t off,
+                                       int len, int ch, bool rev, uint32_t& x, uint32_t& nb) {
+    uint64_t v, m;
+    load16_raw(codes, nmask, off, len, ch, rev, v, m);
+    decode16(off, len, ch, rev, v, m, x, nb);
 }
 
 // 16 codes as 16 nibbles: the 2-bit code in bits 0-1, the N flag in bit 2.
