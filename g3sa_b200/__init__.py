@@ -54,7 +54,8 @@ REG_DT = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), (
                    ("truesc", "<i4"), ("w", "<i4"), ("tries_left", "u1"), ("tries_right", "u1"),
                    ("pad_", "u1", 2)])
 BATCH_OPTS_DT = np.dtype([("schedule", "<i4"), ("max_qlen", "<i4"), ("max_tlen", "<i4"),
-                          ("lanes", "<i4"), ("tile", "<i4"), ("kernel", "<i4"), ("d_cells", "<u8")])
+                          ("lanes", "<i4"), ("tile", "<i4"), ("kernel", "<i4"), ("d_cells", "<u8"),
+                          ("n_bases", "<i8")])
 KERNEL_AUTO, KERNEL_ROLLING, KERNEL_ROWPAR, KERNEL_LANE, KERNEL_LANE16, KERNEL_LANE2 = 0, 1, 2, 3, 4, 5
 TILE_DT = np.dtype([("width", "<i4"), ("lanes", "<i4"), ("tile", "<i4"), ("warp_batch", "<i4"),
                     ("refill", "<i4")])
@@ -133,7 +134,7 @@ def lib():
         L.g3x_extend_seeds_stream.argtypes = [P, P, P, ctypes.c_int64, P, P, ctypes.c_int64, P, P,
                                               I32, P]
         L.g3x_extend_seeds_stream.restype = ctypes.c_int
-        L.g3x_features.argtypes = [P, P, I32, P, P, P, P]
+        L.g3x_features.argtypes = [P, P, I32, P, P, ctypes.c_int64, P, P]
         L.g3x_mlp_init.argtypes = [P, ctypes.c_uint64]
         L.g3x_mlp_train.argtypes = [P, P, P, I32, I32, I32, ctypes.c_float, ctypes.c_uint64, P]
         L.g3x_mlp_gradient.argtypes = [P, P, P, I32, P, P]
@@ -142,10 +143,11 @@ def lib():
         L.g3x_mlp_set_params.argtypes = [P, P]
         L.g3x_get_tiles.argtypes = [P, P, P]
         L.g3x_set_tiles.argtypes = [P, P, I32]
-        L.g3x_autotune.argtypes = [P, P, P, I32, P, P, I32, I32, P, P]
-        L.g3x_autotune_schedule.argtypes = [P, I32, P, P, I32, P, P, I32, I32, P, P]
+        L.g3x_autotune.argtypes = [P, P, P, I32, P, P, ctypes.c_int64, I32, I32, P, P]
+        L.g3x_autotune_schedule.argtypes = [P, I32, P, P, I32, P, P, ctypes.c_int64, I32, I32, P, P]
         L.g3x_last_stats.argtypes = [P, P]
         L.g3x_set_timing.argtypes = [P, I32]
+        L.g3x_set_step_limit.argtypes = [P, ctypes.c_int64]
         L.g3x_class_times.argtypes = [P, P, P, P]
         L.g3x_graph_capture.argtypes = [P, P, P, I32, P, P, P, P, P, ctypes.POINTER(P)]
         L.g3x_graph_launch.argtypes = [P, P]
@@ -293,13 +295,14 @@ class Context:
 
     def capture_batch(self, score, d_jobs, n, d_codes, d_nmask, d_out, d_status, max_qlen,
                       max_tlen, schedule=SCHED_SORTED, lanes=0, d_cells=None, tile=0,
-                      kernel=KERNEL_AUTO):
+                      kernel=KERNEL_AUTO, n_bases=None):
         """g3x_graph_capture of one batch; returns a Graph whose launch() replays it."""
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
             schedule, max_qlen, max_tlen, lanes)
         opts["tile"], opts["kernel"] = tile, kernel
         opts["d_cells"] = _ptr(d_cells) if d_cells is not None else 0
+        opts["n_bases"] = plane_bases(d_codes, d_nmask, n_bases)
         h = ctypes.c_void_p()
         _check(lib().g3x_graph_capture(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
                                        _ptr(d_nmask), _ptr(d_out), _ptr(d_status), opts.ctypes.data,
@@ -307,9 +310,10 @@ class Context:
         return Graph(h)
 
     # ---- learned cost model ----
-    def features(self, d_jobs, n, d_codes, d_nmask, d_feat, stream=None):
+    def features(self, d_jobs, n, d_codes, d_nmask, d_feat, stream=None, n_bases=None):
         _check(lib().g3x_features(self._h, _ptr(d_jobs), int(n), _ptr(d_codes), _ptr(d_nmask),
-                                  _ptr(d_feat), _stream(stream)), "g3x_features")
+                                  plane_bases(d_codes, d_nmask, n_bases), _ptr(d_feat), _stream(stream)),
+               "g3x_features")
 
     def mlp_init(self, seed):
         _check(lib().g3x_mlp_init(self._h, int(seed)), "g3x_mlp_init")
@@ -352,11 +356,13 @@ class Context:
         t = np.array([tuple(x) for x in tiles], TILE_DT)
         _check(lib().g3x_set_tiles(self._h, t.ctypes.data, len(t)), "g3x_set_tiles")
 
-    def autotune(self, score, d_jobs, n, d_codes, d_nmask, max_qlen, max_tlen, schedule=SCHED_SORTED):
+    def autotune(self, score, d_jobs, n, d_codes, d_nmask, max_qlen, max_tlen, schedule=SCHED_SORTED,
+                 n_bases=None):
         t = np.zeros(8, TILE_DT)
         k = ctypes.c_int32()
         _check(lib().g3x_autotune_schedule(self._h, int(schedule), score.ctypes.data, _ptr(d_jobs), int(n),
-                                           _ptr(d_codes), _ptr(d_nmask), int(max_qlen), int(max_tlen),
+                                           _ptr(d_codes), _ptr(d_nmask), plane_bases(d_codes, d_nmask, n_bases),
+                                           int(max_qlen), int(max_tlen),
                                            t.ctypes.data, ctypes.addressof(k)), "g3x_autotune_schedule")
         return [tuple(int(v) for v in row) for row in t[:k.value]]
 
@@ -364,6 +370,10 @@ class Context:
         s = np.zeros(3, np.uint64)
         _check(lib().g3x_last_stats(self._h, s.ctypes.data), "g3x_last_stats")
         return [int(v) for v in s]
+
+    def set_step_limit(self, limit):
+        """g3x_set_step_limit: the plain kernel's per-job step bound (0: its own bound)."""
+        _check(lib().g3x_set_step_limit(self._h, ctypes.c_int64(int(limit))), "g3x_set_step_limit")
 
     def set_timing(self, mode):
         """0 off; 1: CUDA events around every class launch of later scheduled batches (classes
@@ -387,13 +397,14 @@ class Context:
 
     def extend_batch(self, score, d_jobs, n, d_codes, d_nmask, d_out, d_status, max_qlen,
                      max_tlen, schedule=SCHED_PLAIN, lanes=0, d_cells=None, stream=None,
-                     tile=0, kernel=KERNEL_AUTO):
+                     tile=0, kernel=KERNEL_AUTO, n_bases=None):
         """g3x_ksw_extend2_batch on torch device tensors (or raw device pointers)."""
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
             schedule, max_qlen, max_tlen, lanes)
         opts["tile"], opts["kernel"] = tile, kernel
         opts["d_cells"] = _ptr(d_cells) if d_cells is not None else 0
+        opts["n_bases"] = plane_bases(d_codes, d_nmask, n_bases)
         rc = lib().g3x_ksw_extend2_batch(self._h, score.ctypes.data, _ptr(d_jobs), int(n),
                                          _ptr(d_codes), _ptr(d_nmask), _ptr(d_out),
                                          _ptr(d_status), opts.ctypes.data, _stream(stream))
@@ -402,12 +413,13 @@ class Context:
 
     def extend_seeds(self, opt, d_seeds, n, d_codes, d_nmask, d_regs, d_status, max_qlen,
                      max_tlen, schedule=SCHED_SORTED, lanes=0, stream=None, tile=0,
-                     kernel=KERNEL_AUTO):
+                     kernel=KERNEL_AUTO, n_bases=None):
         """g3x_extend_seeds: left + right extension with band retry on device buffers."""
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
             schedule, max_qlen, max_tlen, lanes)
         opts["tile"], opts["kernel"] = tile, kernel
+        opts["n_bases"] = plane_bases(d_codes, d_nmask, n_bases)
         rc = lib().g3x_extend_seeds(self._h, opt.ctypes.data, _ptr(d_seeds), int(n), _ptr(d_codes),
                                     _ptr(d_nmask), _ptr(d_regs), _ptr(d_status), opts.ctypes.data,
                                     _stream(stream))
@@ -415,13 +427,14 @@ class Context:
 
     def chain2aln(self, opt, l_pac, ref_off, d_anns, n_seqs, d_reads, n_reads, d_chains, n_chains,
                   d_seeds, n_seeds, d_codes, d_nmask, d_regs, d_nregs, d_status,
-                  schedule=SCHED_SORTED, lanes=0, tile=0, kernel=KERNEL_AUTO, stream=None):
+                  schedule=SCHED_SORTED, lanes=0, tile=0, kernel=KERNEL_AUTO, stream=None, n_bases=None):
         """g3x_chain2aln on device buffers (records of g3sa_b200.chains: READ_DT, CHAIN_DT,
         CSEED_DT, ANN_DT in; ALNREG_DT per seed slot, nregs and status per read out)."""
         ri = np.zeros(1, REFINFO_DT)
         ri["l_pac"], ri["ref_off"], ri["n_seqs"], ri["d_anns"] = l_pac, ref_off, n_seqs, _ptr(d_anns)
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["lanes"], opts["tile"], opts["kernel"] = schedule, lanes, tile, kernel
+        opts["n_bases"] = plane_bases(d_codes, d_nmask, n_bases)
         rc = lib().g3x_chain2aln(self._h, opt.ctypes.data, ri.ctypes.data, _ptr(d_reads), int(n_reads),
                                  _ptr(d_chains), int(n_chains), _ptr(d_seeds), int(n_seeds), _ptr(d_codes),
                                  _ptr(d_nmask), _ptr(d_regs), _ptr(d_nregs), _ptr(d_status), opts.ctypes.data,
@@ -477,6 +490,7 @@ class Context:
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
             schedule, max_qlen, max_tlen, lanes)
         opts["tile"], opts["kernel"] = tile, kernel
+        opts["n_bases"] = n_bases
         hp = lambda a: a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr()  # noqa: E731
         rc = lib().g3x_extend_seeds_stream(self._h, opt.ctypes.data, hp(seeds), n_seeds, hp(codes),
                                            hp(nmask), int(n_bases), hp(regs), hp(status), int(chunk),
@@ -588,6 +602,16 @@ class Graph:
             self.close()
         except Exception:
             pass
+
+
+def plane_bases(d_codes, d_nmask, n_bases=None):
+    """The bases a pair of planes holds: n_bases when given, else what the two buffers' sizes
+    cover (16 bases per code word, 32 per N-mask word); raw pointers need n_bases."""
+    if n_bases is not None:
+        return int(n_bases)
+    if isinstance(d_codes, int) or isinstance(d_nmask, int):
+        raise ValueError("n_bases is needed for planes given as raw pointers")
+    return min(_nbytes(d_codes) // 4 * 16, _nbytes(d_nmask) // 4 * 32, 1 << 32)
 
 
 def _ptr(t):

@@ -12,6 +12,7 @@ struct g3x_ctx {
     int sms;
     int32_t* d_queue;            // persistent-kernel job counters
     g3x::SeedScratch seeds;      // seed-level scratch, grown on demand
+    g3x::StreamScratch stream;   // chunked seed stream: buffer sets, staging, streams
     g3x::ModelState model;       // learned cost model
     g3x::SchedScratch sched;     // job order and width classes of a persistent batch
     g3x::ChainScratch chain;     // chain-level call state
@@ -24,6 +25,7 @@ struct g3x_ctx {
     int timing;                             // bracket class launches with timing events
     cudaEvent_t cls0[g3x::kMaxBuckets], cls1[g3x::kMaxBuckets];
     int cls_timed[g3x::kMaxBuckets];        // 1 when the last batch recorded class k
+    int64_t step_limit;                     // g3x_set_step_limit (0: the kernels' own bound)
 };
 
 namespace g3x {
@@ -70,7 +72,9 @@ int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d) {
     if (!opts) return G3X_ERR_INVALID;
     if (opts->max_qlen < 0 || opts->max_tlen < 0 || opts->max_qlen > 65534 || opts->max_tlen > 65535)
         return G3X_ERR_INVALID;
+    if (opts->n_bases < 1 || opts->n_bases > 0x100000000ll) return G3X_ERR_INVALID;
     memset(d, 0, sizeof(*d));
+    d->n_bases = opts->n_bases;
     d->qmax = opts->max_qlen;
     d->tmax = opts->max_tlen;
     d->cells = opts->d_cells;
@@ -238,7 +242,8 @@ static int run_scheduled(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParams
     const float* pred = nullptr;
     if (learned) {
         if (!ctx->model.params || !ctx->model.trained) return G3X_ERR_NOT_TRAINED;
-        if ((rc = model_features(base.jobs, base.n, base.codes, base.nmask, ctx->sched.feat, st))) return rc;
+        if ((rc = model_features(base.jobs, base.n, base.codes, base.nmask, base.n_bases, ctx->sched.feat, st)))
+            return rc;
         if ((rc = model_predict(ctx->model.params, ctx->sched.feat, base.n, ctx->sched.pred, st))) return rc;
         pred = ctx->sched.pred;
     }
@@ -263,7 +268,8 @@ static int run_class_wave(void* user, const LaunchDesc& d, const ScoreParams& sp
     const float* pred = nullptr;
     int rc;
     if (w->learned) {
-        if ((rc = model_features(d.jobs, d.n, d.codes, d.nmask, ctx->sched.feat, st, d.order, d.count))) return rc;
+        if ((rc = model_features(d.jobs, d.n, d.codes, d.nmask, d.n_bases, ctx->sched.feat, st, d.order, d.count)))
+            return rc;
         if ((rc = model_predict(ctx->model.params, ctx->sched.feat, d.n, ctx->sched.pred, st))) return rc;
         pred = ctx->sched.pred;
     }
@@ -346,6 +352,7 @@ int g3x_ctx_destroy(g3x_ctx* c) {
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
     g3x::free_seed_scratch(c->seeds);
+    g3x::free_stream_scratch(c->stream);
     g3x::model_free(c->model);
     g3x::free_sched(c->sched);
     g3x::free_chain_scratch(c->chain);
@@ -383,6 +390,7 @@ int g3x_ksw_extend2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_
     cudaStream_t st = (cudaStream_t)stream;
     d.jobs = d_jobs; d.codes = d_codes; d.nmask = d_nmask; d.out = d_out; d.status = d_status;
     d.n = n;
+    d.step_limit = ctx->step_limit;
     // Persistent batches without a fixed kernel shape go through the scheduler.
     if (d.persistent && d.kernel == g3x::kKernelRowpar && opts->kernel == G3X_KERNEL_AUTO &&
         opts->lanes == 0 && opts->tile == 0)
@@ -483,6 +491,12 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
     return G3X_OK;
 }
 
+int g3x_set_step_limit(g3x_ctx* ctx, int64_t limit) {
+    if (!ctx || limit < 0) return G3X_ERR_INVALID;
+    ctx->step_limit = limit;
+    return G3X_OK;
+}
+
 int g3x_set_timing(g3x_ctx* ctx, int32_t on) {
     if (!ctx || on < 0 || on > 2) return G3X_ERR_INVALID;
     ctx->timing = on;
@@ -516,9 +530,10 @@ int g3x_last_stats(g3x_ctx* ctx, uint64_t* h) {
 }
 
 int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* score, const g3x_job_t* d_jobs,
-                          int32_t n, const uint32_t* d_codes, const uint32_t* d_nmask, int32_t max_qlen,
-                          int32_t max_tlen, g3x_tile_t* h_tiles, int32_t* n_tiles) {
+                          int32_t n, const uint32_t* d_codes, const uint32_t* d_nmask, int64_t n_bases,
+                          int32_t max_qlen, int32_t max_tlen, g3x_tile_t* h_tiles, int32_t* n_tiles) {
     if (!ctx || !d_jobs || !d_codes || !d_nmask || n <= 0) return G3X_ERR_INVALID;
+    if (n_bases < 1 || n_bases > 0x100000000ll) return G3X_ERR_INVALID;
     if (schedule != G3X_SCHED_SORTED && schedule != G3X_SCHED_LEARNED) return G3X_ERR_INVALID;
     if (schedule == G3X_SCHED_LEARNED && (!ctx->model.params || !ctx->model.trained)) return G3X_ERR_NOT_TRAINED;
     g3x::ScoreParams sp;
@@ -535,7 +550,7 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
     g3x::LaunchDesc base;
     memset(&base, 0, sizeof(base));
     base.jobs = d_jobs; base.codes = d_codes; base.nmask = d_nmask; base.out = out; base.status = status;
-    base.n = n; base.qmax = max_qlen; base.tmax = max_tlen;
+    base.n = n; base.qmax = max_qlen; base.tmax = max_tlen; base.n_bases = n_bases;
     cudaStream_t st = nullptr;
     // Class widths follow the batch: up to seven classes at max_qlen times the fractions below,
     // rounded up to eight columns, then the unbounded class.  A class's shared memory per job is
@@ -565,7 +580,7 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
     cudaEventCreate(&e1);
     const float* pred = nullptr;
     if (schedule == G3X_SCHED_LEARNED) {
-        rc = g3x::model_features(d_jobs, n, d_codes, d_nmask, ctx->sched.feat, st);
+        rc = g3x::model_features(d_jobs, n, d_codes, d_nmask, n_bases, ctx->sched.feat, st);
         if (rc == G3X_OK) rc = g3x::model_predict(ctx->model.params, ctx->sched.feat, n, ctx->sched.pred, st);
         pred = ctx->sched.pred;
     }
@@ -637,9 +652,9 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
 }
 
 int g3x_autotune(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs, int32_t n,
-                 const uint32_t* d_codes, const uint32_t* d_nmask, int32_t max_qlen,
+                 const uint32_t* d_codes, const uint32_t* d_nmask, int64_t n_bases, int32_t max_qlen,
                  int32_t max_tlen, g3x_tile_t* h_tiles, int32_t* n_tiles) {
-    return g3x_autotune_schedule(ctx, G3X_SCHED_SORTED, score, d_jobs, n, d_codes, d_nmask, max_qlen,
+    return g3x_autotune_schedule(ctx, G3X_SCHED_SORTED, score, d_jobs, n, d_codes, d_nmask, n_bases, max_qlen,
                                  max_tlen, h_tiles, n_tiles);
 }
 
@@ -677,22 +692,25 @@ int g3x_extend_seeds_stream(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_seed_t
     int rc = g3x::score_params(&opt->score, &sp);
     if (rc) return rc;
     g3x::LaunchDesc proto;
-    if ((rc = g3x::batch_proto(opts, nullptr, &proto))) return rc;
+    g3x_batch_opts_t so = *opts;          // the planes' length is this call's n_bases
+    so.n_bases = n_bases > 0 ? n_bases : 1;
+    if ((rc = g3x::batch_proto(&so, nullptr, &proto))) return rc;
     proto.cells = nullptr;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
     g3x::ClassWave cw;
     g3x::WaveRunner wr;
     const g3x::WaveRunner* runner = nullptr;
     if ((rc = g3x::seed_waves(ctx, opts, proto, chunk > 0 ? chunk : 65536, &cw, &wr, &runner))) return rc;
-    return g3x::extend_seeds_stream(ctx->seeds, g3x::alloc_seed_scratch, *opt, sp, h_seeds, n,
+    return g3x::extend_seeds_stream(ctx->stream, ctx->seeds, g3x::alloc_seed_scratch, *opt, sp, h_seeds, n,
                                     h_codes, h_nmask, n_bases, h_regs, h_status, chunk, proto, runner);
 }
 
 int g3x_features(g3x_ctx* ctx, const g3x_job_t* d_jobs, int32_t n, const uint32_t* d_codes,
-                 const uint32_t* d_nmask, float* d_feat, void* stream) {
+                 const uint32_t* d_nmask, int64_t n_bases, float* d_feat, void* stream) {
     if (!ctx || n < 0 || (n && (!d_jobs || !d_codes || !d_nmask || !d_feat))) return G3X_ERR_INVALID;
+    if (n_bases < 0 || n_bases > 0x100000000ll) return G3X_ERR_INVALID;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
-    return g3x::model_features(d_jobs, n, d_codes, d_nmask, d_feat, (cudaStream_t)stream);
+    return g3x::model_features(d_jobs, n, d_codes, d_nmask, n_bases, d_feat, (cudaStream_t)stream);
 }
 
 int g3x_mlp_init(g3x_ctx* ctx, uint64_t seed) {

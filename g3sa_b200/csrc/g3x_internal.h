@@ -44,7 +44,15 @@ struct LaunchDesc {
                            // once and waits for all of them; 0 = each group refills alone
     int32_t refill;        // lane-per-job kernel: idle lanes that trigger a refill wave
     int32_t ring;          // lane-per-job kernel: 0, or the columns of its row-buffer ring
+    int64_t n_bases;       // bases the planes hold: jobs reaching past them are refused
+    int64_t step_limit;    // plain (rolling) kernel: per-job step bound, 0 = the default bound
 };
+
+// A job whose query or target reaches past the planes' n_bases bases is refused before any of
+// its bases is read (per-job G3X_ERR_INVALID).
+__host__ __device__ __forceinline__ bool job_in_planes(const g3x_job_t& jb, int64_t n_bases) {
+    return (int64_t)jb.q_off + jb.qlen <= n_bases && (int64_t)jb.t_off + jb.tlen <= n_bases;
+}
 
 // Tile configurations by job width class (ascending width; the last class is unbounded).
 constexpr int kMaxBuckets = 8;
@@ -144,7 +152,28 @@ int extend_seeds(const SeedScratch& ws, const g3x_opt_t& opt, const ScoreParams&
                  const g3x_seed_t* seeds, int n, const uint32_t* codes, const uint32_t* nmask,
                  g3x_reg_t* regs, int32_t* status, const LaunchDesc& proto, cudaStream_t st,
                  const WaveRunner* runner = nullptr);
-int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), const g3x_opt_t& opt,
+// Device buffer sets, pinned staging and streams of the chunked seed stream (g3x_stream.cu),
+// kept in the context between calls and grown on demand.
+struct StreamSet {
+    g3x_seed_t* d_seeds = nullptr;
+    uint32_t* d_codes = nullptr;
+    uint32_t* d_nmask = nullptr;
+    g3x_reg_t* d_regs = nullptr;
+    int32_t* d_status = nullptr;
+    g3x_seed_t* h_seeds = nullptr;   // pinned staging
+    g3x_reg_t* h_regs = nullptr;
+    int32_t* h_status = nullptr;
+    cudaEvent_t h2d = nullptr, done = nullptr;
+    int64_t pending = -1;            // chunk whose results sit in this set
+};
+struct StreamScratch {
+    StreamSet set[2];
+    cudaStream_t copy_st = nullptr, comp_st = nullptr;
+    int64_t seeds = 0, code_words = 0, mask_words = 0;   // capacities of each set
+};
+void free_stream_scratch(StreamScratch& s);
+
+int extend_seeds_stream(StreamScratch& ss, SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), const g3x_opt_t& opt,
                         const ScoreParams& sp, const g3x_seed_t* h_seeds, int64_t n,
                         const uint32_t* h_codes, const uint32_t* h_nmask, int64_t n_bases,
                         g3x_reg_t* h_regs, int32_t* h_status, int32_t chunk,
@@ -201,7 +230,7 @@ int model_alloc(ModelState& M, int batch);
 void model_free(ModelState& M);
 int model_init(ModelState& M, uint64_t seed);
 int model_features(const g3x_job_t* jobs, int n, const uint32_t* codes, const uint32_t* nmask,
-                   float* feat, cudaStream_t st,
+                   int64_t n_bases, float* feat, cudaStream_t st,
                    const int32_t* subset = nullptr, const int32_t* subset_n = nullptr);
 int model_predict(const float* params, const float* feat, int n, float* out, cudaStream_t st);
 int model_gradient(ModelState& M, const float* X, const float* T, int B, float* h_grad,

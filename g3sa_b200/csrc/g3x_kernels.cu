@@ -80,7 +80,8 @@ __global__ void __launch_bounds__(256) extend_kernel(LaunchDesc d, ScoreParams s
                     // Every step either advances a row or moves a lane between states; the
                     // oldest unfinished row always advances, so this bound is never reached
                     // by a correct run.  It turns a logic error into a per-job status.
-                    gj.limit = 8LL * ((long long)gj.c.tlen + 2) * ((long long)gj.c.qlen + 8) + 4096;
+                    gj.limit = d.step_limit > 0 ? d.step_limit
+                                                : 8LL * ((long long)gj.c.tlen + 2) * ((long long)gj.c.qlen + 8) + 4096;
                     lane_init(L, r, gj.c.tlen);
                     err = G3X_OK;
                     break;

@@ -85,6 +85,10 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
                         d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
                         d.status[job] = G3X_ERR_TOO_LONG;
                         if (d.cells) d.cells[job] = 0;
+                    } else if (!job_in_planes(jb, d.n_bases)) {   // reaches past the planes: unread
+                        d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
+                        d.status[job] = G3X_ERR_INVALID;
+                        if (d.cells) d.cells[job] = 0;
                     } else {
                         J.job = job;
                         J.qlen = c.qlen; J.tlen = c.tlen; J.w = c.w; J.h0 = c.h0;

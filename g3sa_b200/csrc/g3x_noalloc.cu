@@ -73,11 +73,12 @@ int scratch_of(int device, int32_t** out) {
 extern "C" int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t* score,
                                              const g3x_job_t* d_jobs, int32_t n,
                                              const uint32_t* d_codes, const uint32_t* d_nmask,
-                                             g3x_ext_t* d_out, int32_t* d_status,
+                                             int64_t n_bases, g3x_ext_t* d_out, int32_t* d_status,
                                              int32_t max_qlen, int32_t max_tlen, void* stream) {
     using namespace g3x;
     if (n < 0) return G3X_ERR_INVALID;
     if (n > G3X_NOALLOC_MAX_JOBS) return G3X_ERR_SCRATCH;
+    if (n > 0 && (n_bases < 1 || n_bases > 0x100000000ll)) return G3X_ERR_INVALID;
     int rc;
     if (cudaSetDevice(device) != cudaSuccess) return G3X_ERR_CUDA;
     int32_t* s = nullptr;
@@ -111,6 +112,7 @@ extern "C" int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t* scor
         d.jobs = d_jobs; d.codes = d_codes; d.nmask = d_nmask; d.out = d_out; d.status = d_status;
         d.n = n;
         d.tmax = max_tlen;
+        d.n_bases = n_bases;
         d.qmax = k == tt.n - 1 ? max_qlen : (max_qlen < tt.width[k] ? max_qlen : tt.width[k]);
         d.kernel = kKernelRowpar;
         d.lanes = tt.lanes[k];

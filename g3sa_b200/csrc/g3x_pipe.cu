@@ -15,6 +15,7 @@
 // stream wait for every submitted batch.  The extension of all batches is serialised on the
 // comp stream, so the context's scratch is used by one batch at a time.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <string.h>
 #include <new>
 #include "g3x_internal.h"
@@ -148,6 +149,8 @@ int g3x_pipe_submit(g3x_pipe* p, const g3x_job_t* h_jobs, int32_t n, const uint3
     opts.max_qlen = max_qlen;
     opts.max_tlen = max_tlen;
     opts.kernel = G3X_KERNEL_AUTO;
+    // the planes hold the bases their copied words cover
+    opts.n_bases = std::min<int64_t>(std::min<int64_t>(code_words * 16, nmask_words * 32), 0x100000000ll);
     int rc = g3x_ksw_extend2_batch(p->ctx, &p->score, s.d_jobs, n, s.d_codes, s.d_nmask, s.d_out,
                                    s.d_status, &opts, p->comp);
     if (rc) return rc;

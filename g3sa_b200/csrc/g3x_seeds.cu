@@ -28,7 +28,7 @@ __device__ __forceinline__ void push(int32_t* order, int32_t* count, int32_t k) 
 }
 
 __global__ void left_jobs_kernel(const g3x_seed_t* __restrict__ seeds, int n, g3x_opt_t opt,
-                                 g3x_job_t* jobs, int32_t* order, int32_t* count,
+                                 int64_t n_bases, g3x_job_t* jobs, int32_t* order, int32_t* count,
                                  g3x_reg_t* regs, int32_t* status) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -45,6 +45,12 @@ __global__ void left_jobs_kernel(const g3x_seed_t* __restrict__ seeds, int n, g3
     if (s.qbeg < 0 || s.len < 0 || s.qbeg + s.len > s.l_query || tl < 0 || tr < 0 ||
         s.qbeg > 65534 || s.l_query - s.qbeg - s.len > 65534 || tl > 65535 || tr > 65535) {
         status[k] = G3X_ERR_TOO_LONG;
+        regs[k] = a;
+        return;
+    }
+    // the read and the window must lie in the planes: no job of this seed reads past them
+    if ((int64_t)s.read_off + s.l_query > n_bases || (int64_t)s.win_off + (s.rmax1 - s.rmax0) > n_bases) {
+        status[k] = G3X_ERR_INVALID;
         regs[k] = a;
         return;
     }
@@ -161,7 +167,8 @@ int extend_seeds(const SeedScratch& ws, const g3x_opt_t& opt, const ScoreParams&
     // queue counters of the four persistent launches at [8 .. 11]
     if (cudaMemsetAsync(ws.counters, 0, 16 * sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
     const int tb = 256, nb = (n + tb - 1) / tb;
-    left_jobs_kernel<<<nb, tb, 0, st>>>(seeds, n, opt, ws.ljobs, ws.order[0], ws.counters + 0, regs, status);
+    left_jobs_kernel<<<nb, tb, 0, st>>>(seeds, n, opt, proto.n_bases, ws.ljobs, ws.order[0], ws.counters + 0,
+                                        regs, status);
     auto wave = [&](g3x_job_t* jobs, g3x_ext_t* ext, int32_t* jst, int32_t* order, int32_t* count,
                     int32_t* queue) -> int {
         LaunchDesc d = proto;

@@ -182,10 +182,12 @@ __device__ bool stage_job(int job, const LaunchDesc& d, const ScoreParams& sp,
     // be negative is eh[0].h = h0 (ksw.cu:317), and for h0 <= -max_score the two forms agree
     // too (both <= 0, which every use clips to 0).  Seed scores in between are rejected.
     const bool bad_h0 = jb.h0 < 0 && jb.h0 > -sp.max_sc;
-    if (qlen > d.qmax || tlen > d.tmax || qlen > 65534 || bad_h0) {
+    // a job reaching past the planes is refused before any of its bases is read
+    const bool outside = !job_in_planes(jb, d.n_bases);
+    if (qlen > d.qmax || tlen > d.tmax || qlen > 65534 || bad_h0 || outside) {
         if (r == 0) {
             d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
-            d.status[job] = bad_h0 ? G3X_ERR_INVALID : G3X_ERR_TOO_LONG;
+            d.status[job] = bad_h0 || outside ? G3X_ERR_INVALID : G3X_ERR_TOO_LONG;
             if (d.cells) d.cells[job] = 0;
         }
         return false;

@@ -111,11 +111,15 @@ typedef struct {
     int32_t tile;         /* row-parallel: cells per lane per tile (5, 9 or 13), 0 = tuned */
     int32_t kernel;       /* G3X_KERNEL_* */
     int32_t *d_cells;     /* optional per-job DP cell count (trip count of ksw.cu:346) */
-} g3x_batch_opts_t;       /* 32 bytes */
+    int64_t n_bases;      /* bases the planes hold (required, 1 .. 2^32): a job or seed reaching
+                             past it is refused with a per-job G3X_ERR_INVALID, unread */
+} g3x_batch_opts_t;       /* 40 bytes */
 
 /* n jobs; outputs to d_out[k] and d_status[k] (G3X_OK or a G3X_ERR_* per job: TOO_LONG for a
    job beyond max_qlen/max_tlen or beyond what a fixed lane kernel holds, INVALID for a seed
-   score -max_score < h0 < 0, which callers of ksw_extend2 never pass).
+   score -max_score < h0 < 0, which callers of ksw_extend2 never pass, or for a job whose query
+   or target reaches past opts->n_bases: q_off + qlen or t_off + tlen > n_bases; such a job's
+   bases are never read).
    Replaces n calls of ksw_extend2 (bwa/src/ksw.h:33) issued by localExtending
    (bwa/src/aux.cu:2289-2382). Asynchronous on `stream`. */
 int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs,
@@ -137,12 +141,14 @@ int g3x_ksw_extend2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
    device's primary context: no cudaDeviceReset between calls.  At most G3X_NOALLOC_MAX_JOBS
    jobs per call, else G3X_ERR_SCRATCH.  All calls on a device share that array: calls that
    overlap on the GPU (two streams, two host threads) race and corrupt each other's results,
-   so serialise them.  Makes `device` current.  Asynchronous on `stream`. */
+   so serialise them.  n_bases: the bases the planes hold, as g3x_batch_opts_t.n_bases (jobs
+   reaching past them get G3X_ERR_INVALID, unread).  Makes `device` current.  Asynchronous on
+   `stream`. */
 #define G3X_NOALLOC_MAX_JOBS 1048576
 int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t *score, const g3x_job_t *d_jobs,
                                   int32_t n, const uint32_t *d_codes, const uint32_t *d_nmask,
-                                  g3x_ext_t *d_out, int32_t *d_status, int32_t max_qlen,
-                                  int32_t max_tlen, void *stream);
+                                  int64_t n_bases, g3x_ext_t *d_out, int32_t *d_status,
+                                  int32_t max_qlen, int32_t max_tlen, void *stream);
 
 /* ---- schedule tuning ----------------------------------------------------------------------- */
 /* The persistent schedules split a batch into width classes: a job belongs to the first class
@@ -173,18 +179,18 @@ int g3x_set_tiles(g3x_ctx *ctx, const g3x_tile_t *h_tiles, int32_t n);
    become max_qlen x (0.138, 0.241, 0.379, 0.552, 0.724, 0.862, 1) (rounded up to 8 columns,
    duplicates dropped) plus
    the unbounded class; then every candidate configuration of each class is timed on the class's
-   jobs and the fastest kept in the context; h_tiles/n receive the table.  Blocks.  Outputs of
-   the trial runs are discarded. */
+   jobs and the fastest kept in the context; h_tiles/n receive the table.  n_bases: the bases the
+   planes hold, as g3x_batch_opts_t.n_bases.  Blocks.  Outputs of the trial runs are discarded. */
 int g3x_autotune(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
-                 const uint32_t *d_codes, const uint32_t *d_nmask, int32_t max_qlen,
+                 const uint32_t *d_codes, const uint32_t *d_nmask, int64_t n_bases, int32_t max_qlen,
                  int32_t max_tlen, g3x_tile_t *h_tiles, int32_t *n_tiles);
 /* The same, with the jobs ordered as `schedule` (G3X_SCHED_SORTED or G3X_SCHED_LEARNED, which
    needs a trained model) orders them, so the choices fit that schedule; g3x_autotune is the
    G3X_SCHED_SORTED form. */
 int g3x_autotune_schedule(g3x_ctx *ctx, int32_t schedule, const g3x_score_t *score,
                           const g3x_job_t *d_jobs, int32_t n, const uint32_t *d_codes,
-                          const uint32_t *d_nmask, int32_t max_qlen, int32_t max_tlen,
-                          g3x_tile_t *h_tiles, int32_t *n_tiles);
+                          const uint32_t *d_nmask, int64_t n_bases, int32_t max_qlen,
+                          int32_t max_tlen, g3x_tile_t *h_tiles, int32_t *n_tiles);
 /* Occupancy counters of the last persistent batch on this context: h_stats[0] = group-rows
    computed, [1] = group-rows a group waited for the other groups of its warp (warp_batch),
    [2] = warp batches.  Synchronises the context's device. */
@@ -247,7 +253,8 @@ int g3x_extend_seeds(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t *d_see
    words they reference are copied to the GPU while the previous chunk is extended (two
    device buffer sets, a copy stream and a compute stream), and the regions come back to
    h_regs/h_status.  Host buffers should be pinned for the copies to overlap.  Blocks until
-   all chunks are done. */
+   all chunks are done.  The buffer sets, pinned staging and streams stay in the context,
+   grown when a call needs more, so repeated calls allocate nothing. */
 int g3x_extend_seeds_stream(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t *h_seeds,
                             int64_t n, const uint32_t *h_codes, const uint32_t *h_nmask,
                             int64_t n_bases, g3x_reg_t *h_regs, int32_t *h_status,
@@ -504,16 +511,19 @@ int g3x_graph_destroy(g3x_graph *graph);
 
 /* ---- learned cost model ------------------------------------------------------------------ */
 /* A 5 -> 64 -> 64 -> 1 ReLU MLP (fp32) per context that predicts a job's work from five
-   features: qlen/128, tlen/256, h0/64, query GC fraction, and the mismatch fraction of the
-   first min(32, qlen, tlen) bases next to the seed.  Trained on the GPU by the library's own
+   features: qlen/128, tlen/256, h0/64, and the ungapped extension along the seed's diagonal
+   over the first min(qlen, tlen) bases (from h0, +1 per identical base pair, -4 per other pair,
+   N counting as other): its best score / 64 and the number of bases at which it is first
+   reached / 128.  Trained on the GPU by the library's own
    forward/backward/Adam kernels; G3X_SCHED_LEARNED orders jobs by its prediction.  No
    counterpart in the reference (its extension stage has no scheduler). */
 #define G3X_MLP_FEATURES 5
 #define G3X_MLP_PARAMS 4609   /* W1[64][5] b1[64] W2[64][64] b2[64] W3[64] b3 */
 
-/* d_feat[k*5 .. k*5+4] = features of job k. */
+/* d_feat[k*5 .. k*5+4] = features of job k; a job reaching past the planes' n_bases bases reads
+   none of them (its diagonal features are those of an empty overlap). */
 int g3x_features(g3x_ctx *ctx, const g3x_job_t *d_jobs, int32_t n, const uint32_t *d_codes,
-                 const uint32_t *d_nmask, float *d_feat, void *stream);
+                 const uint32_t *d_nmask, int64_t n_bases, float *d_feat, void *stream);
 /* Fresh He-style parameters from `seed`; clears the optimiser state. */
 int g3x_mlp_init(g3x_ctx *ctx, uint64_t seed);
 /* Mini-batch Adam on mean squared error over n samples (d_feat n x 5, d_target n); the
@@ -529,6 +539,13 @@ int g3x_mlp_get_params(g3x_ctx *ctx, float *h_params);
 int g3x_mlp_set_params(g3x_ctx *ctx, const float *h_params);
 
 /* ---- diagnostics ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference: the plain kernel (G3X_SCHED_PLAIN) bounds the steps it spends
+   on one job (its wavefront protocol advances a row or a lane every step, so a correct run never
+   reaches the bound); a job that reaches it ends with the per-job status G3X_ERR_TIMEOUT and the
+   batch goes on.  This sets that bound to `limit` steps for later batches of the context (0: the
+   kernel's own bound, 8 (tlen + 2)(qlen + 8) + 4096), so tests can make it run out on normal jobs. */
+int g3x_set_step_limit(g3x_ctx *ctx, int64_t limit);
 
 /* Measured 32-bit integer ALU throughput of the context's GPU (ops/s): independent chains of
    the 3-input DPX maximum on every SM.  The cells/s roofline is this figure / 8 (ops per DP

@@ -20,7 +20,7 @@ def to_dev(a):
 
 
 def run_batch(u8, jobs, score, schedule=g.SCHED_PLAIN, lanes=0, max_qlen=None, max_tlen=None,
-              tile=0, kernel=g.KERNEL_AUTO):
+              tile=0, kernel=g.KERNEL_AUTO, n_bases=None):
     """Returns (ext[n,6], status[n], cells[n]) from the GPU."""
     import torch
     n = len(jobs)
@@ -32,12 +32,13 @@ def run_batch(u8, jobs, score, schedule=g.SCHED_PLAIN, lanes=0, max_qlen=None, m
     mq = int(jobs["qlen"].max()) if max_qlen is None else max_qlen
     mt = int(jobs["tlen"].max()) if max_tlen is None else max_tlen
     ctx().extend_batch(score, d_jobs, n, d_codes, d_nmask, out, status, mq, mt,
-                       schedule=schedule, lanes=lanes, d_cells=cells, tile=tile, kernel=kernel)
+                       schedule=schedule, lanes=lanes, d_cells=cells, tile=tile, kernel=kernel,
+                       n_bases=n_bases)
     torch.cuda.synchronize()
     return out.cpu().numpy(), status.cpu().numpy(), cells.cpu().numpy()
 
 
-def run_seeds(u8, seeds, opt, schedule=g.SCHED_SORTED, lanes=0):
+def run_seeds(u8, seeds, opt, schedule=g.SCHED_SORTED, lanes=0, n_bases=None):
     """Seed-level extension on the GPU: returns (regs REG_DT, status)."""
     import torch
     codes, nmask = g.pack_planes(u8)
@@ -48,6 +49,7 @@ def run_seeds(u8, seeds, opt, schedule=g.SCHED_SORTED, lanes=0):
     d_status = torch.full((n,), 99, dtype=torch.int32, device="cuda")
     mq = int(seeds["l_query"].max())
     mt = int((seeds["rmax1"] - seeds["rmax0"]).max())
-    ctx().extend_seeds(opt, d_seeds, n, d_codes, d_nmask, d_regs, d_status, mq, mt, schedule, lanes)
+    ctx().extend_seeds(opt, d_seeds, n, d_codes, d_nmask, d_regs, d_status, mq, mt, schedule, lanes,
+                       n_bases=n_bases)
     torch.cuda.synchronize()
     return d_regs.cpu().numpy().view(g.REG_DT), d_status.cpu().numpy()

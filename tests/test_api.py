@@ -42,6 +42,34 @@ def test_record_sizes():
     assert g.SCORE_DT.itemsize == 56
     assert g.JOB_DT.itemsize == 24
     assert g.EXT_DT.itemsize == 24
+    assert g.BATCH_OPTS_DT.itemsize == 40
+
+
+def test_batch_opts_layout_matches_header(tmp_path):
+    """The options record the bindings build has the C struct's size and field offsets."""
+    import subprocess
+    src = tmp_path / "opts.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "g3x.h"\nint main(void) {\n'
+                   '  printf("%zu %zu %zu %zu\\n", sizeof(g3x_batch_opts_t), offsetof(g3x_batch_opts_t, kernel),\n'
+                   '         offsetof(g3x_batch_opts_t, d_cells), offsetof(g3x_batch_opts_t, n_bases));\n'
+                   '  return 0;\n}\n')
+    exe = tmp_path / "opts"
+    subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    size, kern, cells, nb = (int(v) for v in subprocess.check_output([str(exe)]).split())
+    dt = g.BATCH_OPTS_DT
+    assert (size, kern, cells, nb) == (dt.itemsize, dt.fields["kernel"][1], dt.fields["d_cells"][1],
+                                       dt.fields["n_bases"][1])
+
+
+def test_noalloc_rejects_a_missing_plane_length(lib):
+    fn = lib.g3x_ksw_extend2_batch_noalloc
+    fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                   ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                   ctypes.c_int32, ctypes.c_void_p]
+    dummy = ctypes.c_void_p(16)
+    sc = g.default_score()
+    for nb in (0, -5, (1 << 32) + 1):
+        assert fn(0, sc.ctypes.data, dummy, 10, dummy, dummy, nb, dummy, dummy, 100, 300, None) == g.G3X_ERR_INVALID
 
 
 def test_pack_codes_roundtrip(lib):

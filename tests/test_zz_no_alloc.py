@@ -18,7 +18,7 @@ def _bind():
     lib = g.lib()
     fn = lib.g3x_ksw_extend2_batch_noalloc
     P, I32 = ctypes.c_void_p, ctypes.c_int32
-    fn.argtypes = [ctypes.c_int, P, P, I32, P, P, P, P, I32, I32, P]
+    fn.argtypes = [ctypes.c_int, P, P, I32, P, P, ctypes.c_int64, P, P, I32, I32, P]
     fn.restype = ctypes.c_int
     return fn
 
@@ -28,7 +28,7 @@ def test_noalloc_rejects_batches_beyond_its_scratch():
     fn = _bind()
     sc = g.default_score()
     dummy = ctypes.c_void_p(16)
-    rc = fn(0, sc.ctypes.data, dummy, G3X_NOALLOC_MAX_JOBS + 1, dummy, dummy, dummy, dummy,
+    rc = fn(0, sc.ctypes.data, dummy, G3X_NOALLOC_MAX_JOBS + 1, dummy, dummy, 1 << 20, dummy, dummy,
             100, 300, None)
     assert rc == G3X_ERR_SCRATCH
     assert b"1048576" in g.lib().g3x_strerror(rc)
@@ -43,7 +43,7 @@ def test_noalloc_matches_oracle_and_sorted_batch_on_two_calls():
     fn = _bind()
     sc = g.default_score()
     # set-up call: looks the scratch array's address up on this device
-    assert fn(0, sc.ctypes.data, None, 0, None, None, None, None, 0, 0, None) == 0
+    assert fn(0, sc.ctypes.data, None, 0, None, None, 0, None, None, 0, 0, None) == 0
     batches = [g.synth(2, 1500, seed=0x5EED1, w=100, unrelated=0.2),
                g.synth(1, 2500, seed=0x5EED2, w=100, unrelated=0.2)]
     for call, wl in enumerate(batches):
@@ -62,7 +62,8 @@ def test_noalloc_matches_oracle_and_sorted_batch_on_two_calls():
         torch.cuda.synchronize()
         free0 = torch.cuda.mem_get_info()[0]
         rc = fn(0, sc.ctypes.data, d_jobs.data_ptr(), n, d_codes.data_ptr(), d_nmask.data_ptr(),
-                out.data_ptr(), status.data_ptr(), mq, mt, ctypes.c_void_p(stream.cuda_stream))
+                g.plane_bases(d_codes, d_nmask), out.data_ptr(), status.data_ptr(), mq, mt,
+                ctypes.c_void_p(stream.cuda_stream))
         assert rc == 0, g.lib().g3x_strerror(rc)
         torch.cuda.synchronize()
         free1 = torch.cuda.mem_get_info()[0]
