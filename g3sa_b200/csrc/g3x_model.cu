@@ -24,54 +24,45 @@ static_assert(kParams == G3X_MLP_PARAMS, "parameter count");
 
 // ---- features ---------------------------------------------------------------------------
 
-// Per job: qlen/128, tlen/256, h0/64, GC fraction of the query, and the mismatch fraction of
-// the first min(32, qlen, tlen) bases of query and target next to the seed (N counts as a
-// mismatch).  One thread per job.
+// Per job: qlen/128, tlen/256, h0/64, and the ungapped extension along the seed's diagonal
+// over the first min(qlen, tlen) bases (from h0, +1 per identical base pair, -4 per other pair):
+// its best score / 64 and the bases at which that score is first reached / 128.  Where the
+// diagonal's score peaks tells how far the alignment runs before z-drop, and how high, how wide
+// its band grows.  One thread per job.
 __global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
                                 const uint32_t* __restrict__ codes,
-                                const uint32_t* __restrict__ nmask, float* __restrict__ feat,
+                                const uint32_t* __restrict__ nmask, int64_t n_bases, float* __restrict__ feat,
                                 const int32_t* __restrict__ subset, const int32_t* __restrict__ subset_n) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n || (subset_n && k >= *subset_n)) return;
     if (subset) k = subset[k];              // features of job subset[k], stored at that job
     const g3x_job_t jb = jobs[k];
     const bool qrev = (jb.flags & G3X_JOB_QREV) != 0, trev = (jb.flags & G3X_JOB_TREV) != 0;
-    int gc = 0, nq = 0;
-    for (int ch = 0; (ch << 4) < jb.qlen; ++ch) {
-        uint32_t x, nb;
-        load16(codes, nmask, jb.q_off, jb.qlen, ch, qrev, x, nb);
-        const int nv = jb.qlen - (ch << 4) < 16 ? jb.qlen - (ch << 4) : 16;
-        const uint32_t valid = nv == 16 ? 0xFFFFu : ((1u << nv) - 1u);
-        // code 1 (C) or 2 (G): the two bits of the field differ
-        const uint32_t diff = (x ^ (x >> 1)) & 0x55555555u;
-        uint32_t gcm = 0;
-#pragma unroll
-        for (int t = 0; t < 16; ++t) gcm |= ((diff >> (2 * t)) & 1u) << t;
-        gc += __popc(gcm & ~nb & valid);
-        nq += __popc(~nb & valid);
-    }
-    const int k0 = jb.qlen < jb.tlen ? jb.qlen : jb.tlen;
-    const int kk = k0 < 32 ? k0 : 32;
-    int mism = 0;
+    // The ungapped extension along the seed's diagonal: from h0, +1 per identical base pair and
+    // -4 per other pair (N on either side counts as different) over the first min(qlen, tlen)
+    // bases; its best score and the number of bases at which it is first reached.
+    // (a job reaching past the planes reads nothing: its diagonal stays at h0)
+    const int kk = !job_in_planes(jb, n_bases) ? 0 : (jb.qlen < jb.tlen ? jb.qlen : jb.tlen);
+    int32_t sc = jb.h0, best = jb.h0, best_at = 0;
     for (int ch = 0; (ch << 4) < kk; ++ch) {
-        uint32_t xq, nq2, xt, nt;
-        load16(codes, nmask, jb.q_off, jb.qlen, ch, qrev, xq, nq2);
+        uint32_t xq, nq, xt, nt;
+        load16(codes, nmask, jb.q_off, jb.qlen, ch, qrev, xq, nq);
         load16(codes, nmask, jb.t_off, jb.tlen, ch, trev, xt, nt);
         const int nv = kk - (ch << 4) < 16 ? kk - (ch << 4) : 16;
-        const uint32_t valid = nv == 16 ? 0xFFFFu : ((1u << nv) - 1u);
         const uint32_t d2 = xq ^ xt;
         const uint32_t dd = (d2 | (d2 >> 1)) & 0x55555555u;
-        uint32_t mm = 0;
-#pragma unroll
-        for (int t = 0; t < 16; ++t) mm |= ((dd >> (2 * t)) & 1u) << t;
-        mism += __popc((mm | nq2 | nt) & valid);
+        for (int t = 0; t < nv; ++t) {
+            const bool diff = ((dd >> (2 * t)) & 1u) || ((nq | nt) >> t) & 1u;
+            sc += diff ? -4 : 1;
+            if (sc > best) { best = sc; best_at = (ch << 4) + t + 1; }
+        }
     }
     float* f = feat + (size_t)k * kF;
     f[0] = jb.qlen * (1.0f / 128.0f);
     f[1] = jb.tlen * (1.0f / 256.0f);
     f[2] = jb.h0 * (1.0f / 64.0f);
-    f[3] = nq ? (float)gc / (float)nq : 0.0f;
-    f[4] = kk ? (float)mism / (float)kk : 0.0f;
+    f[3] = best * (1.0f / 64.0f);
+    f[4] = best_at * (1.0f / 128.0f);
 }
 
 // ---- inference ---------------------------------------------------------------------------
@@ -272,9 +263,9 @@ __global__ void perm_kernel(int* __restrict__ idx, int n, unsigned long long see
 // ---- host side ---------------------------------------------------------------------------
 
 int model_features(const g3x_job_t* jobs, int n, const uint32_t* codes, const uint32_t* nmask,
-                   float* feat, cudaStream_t st, const int32_t* subset, const int32_t* subset_n) {
+                   int64_t n_bases, float* feat, cudaStream_t st, const int32_t* subset, const int32_t* subset_n) {
     if (n <= 0) return G3X_OK;
-    features_kernel<<<(n + 255) / 256, 256, 0, st>>>(jobs, n, codes, nmask, feat, subset, subset_n);
+    features_kernel<<<(n + 255) / 256, 256, 0, st>>>(jobs, n, codes, nmask, n_bases, feat, subset, subset_n);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }
 

@@ -41,20 +41,28 @@ def traces(ctx, n, seed, kind=1, w=100, unrelated=0.2, score=None):
     return feat, target, cells.cpu().numpy()
 
 
-def train(ctx, n_train=2_000_000, seed_train=0xA11CE, epochs=4, batch=4096, lr=2e-3, init_seed=17,
+def lr_schedule(lr, epochs):
+    """The learning rate of each epoch: lr for the first two, then halved every epoch."""
+    return [lr * 0.5 ** max(0, e - 1) for e in range(epochs)]
+
+
+def train(ctx, n_train=2_000_000, seed_train=0xA11CE, epochs=5, batch=4096, lr=2e-3, init_seed=17,
           kind=1, w=100, unrelated=0.2):
-    """Trains the context's model on the traces of n_train generator units; returns a metrics
-    dict."""
+    """Trains the context's model on the traces of n_train generator units, one g3x_mlp_train
+    call per epoch (the Adam state carries over) with the rate of lr_schedule; returns a
+    metrics dict."""
     t0 = time.perf_counter()
     feat, target, _ = traces(ctx, n_train, seed_train, kind=kind, w=w, unrelated=unrelated)
     m = int(target.shape[0])
     t1 = time.perf_counter()
     ctx.mlp_init(init_seed)
-    losses = ctx.mlp_train(feat, target, m, epochs, batch, lr, seed=init_seed)
+    rates = lr_schedule(lr, epochs)
+    losses = [float(ctx.mlp_train(feat, target, m, 1, batch, r, seed=init_seed + e)[0])
+              for e, r in enumerate(rates)]
     t2 = time.perf_counter()
     return {"traces": m, "trace_kind": kind, "trace_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3),
-            "epochs": epochs, "batch": batch, "lr": lr, "loss_curve": [round(float(x), 5) for x in losses],
-            "params": g.MLP_PARAMS}
+            "epochs": epochs, "batch": batch, "lr": [round(r, 6) for r in rates],
+            "loss_curve": [round(x, 5) for x in losses], "params": g.MLP_PARAMS}
 
 
 def prediction_error(ctx, d_jobs, n, d_codes, d_nmask, cells):

@@ -55,8 +55,10 @@ def loss_and_grad(p, X, T):
 
 
 def features(jobs, u8):
-    """Per job: qlen/128, tlen/256, h0/64, query GC fraction (N excluded), and the mismatch
-    fraction of the first min(32, qlen, tlen) bases of query and target (N = mismatch)."""
+    """Per job: qlen/128, tlen/256, h0/64, and the ungapped extension along the seed's diagonal
+    over the first min(qlen, tlen) bases -- from h0, +1 per identical base pair, -4 per other
+    pair (N on either side counts as different) -- as its best score / 64 and the number of
+    bases at which that score is first reached / 128 (0 when it is h0 itself)."""
     out = np.zeros((len(jobs), F), np.float64)
     for k, jb in enumerate(jobs):
         q = u8[jb["q_off"]:jb["q_off"] + jb["qlen"]]
@@ -65,10 +67,9 @@ def features(jobs, u8):
             q = q[::-1]
         if jb["flags"] & 2:
             t = t[::-1]
-        nn = q[q < 4]
-        gc = np.count_nonzero((nn == 1) | (nn == 2))
-        kk = min(32, len(q), len(t))
-        mism = np.count_nonzero((q[:kk] != t[:kk]) | (q[:kk] > 3) | (t[:kk] > 3))
-        out[k] = (jb["qlen"] / 128, jb["tlen"] / 256, jb["h0"] / 64,
-                  gc / len(nn) if len(nn) else 0.0, mism / kk if kk else 0.0)
+        kk = min(len(q), len(t))
+        same = (q[:kk] == t[:kk]) & (q[:kk] < 4) & (t[:kk] < 4)
+        s = int(jb["h0"]) + np.concatenate([[0], np.cumsum(np.where(same, 1, -4))])
+        at = int(np.argmax(s))
+        out[k] = (jb["qlen"] / 128, jb["tlen"] / 256, jb["h0"] / 64, s[at] / 64, at / 128)
     return out
