@@ -1,7 +1,7 @@
 """Benchmark of the B200 ksw_extend2 batch path (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cfg2|cfg1|cfg4|chains|global|seedsw]
+                    [--workload cfg2|cfg1|cfg4|cfg5|chains|global|seedsw] [--w W]
                     [--schedule auto|plain|sorted|learned]
 
 A step extends every job of one synthetic batch once: the uneven left+right extension
@@ -17,6 +17,10 @@ step), so scaling is weak and `value` is the sum over ranks / the slowest rank's
 --impl reference times the reference's own CPU ksw_extend2 (oracle/_ref, compiled from
 bwa/src/ksw.cu) on all host threads over the same workload, or the C restatement of it
 when oracle/_ref is absent.
+
+`cfg5` is the seed-level band-retry stream (g3x_extend_seeds_stream, 2M seeds from host memory
+in 64k-job chunks), learned width classes against the plain kernel, its regions compared with the
+reference's own band-retry lines on the whole stream.
 
 The other workloads measure the rows around the extension, each against the reference's own
 CPU code for it: `chains` the chain-level call (g3x_chain2aln, mem_chain2aln over 60k reads),
@@ -79,7 +83,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["chains", "global", "seedsw"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg5", "chains", "global", "seedsw"])
     ap.add_argument("--schedule", default="auto", choices=["auto", "plain", "sorted", "learned"])
     ap.add_argument("--seed", type=int, default=0x6A5 + 2)
     ap.add_argument("--w", type=int, default=0, help="band width w of the job generator (0: the workload's)")
@@ -411,6 +415,184 @@ def run_chain_workload(args, ws, rank):
         # per step: prep, resolve and finish, the five seed-level passes and four extension
         # waves of (cost, scan, scatter, one launch per width class)
         "gpu_launches": args.steps * (3 + 5 + 4 * (3 + len(tiles))), "width_classes": tiles,
+    }), flush=True)
+
+
+CFG5_SEEDS = 2_000_000
+CFG5_CHUNK = 32768       # seeds per chunk: 64k extension jobs, a left and a right one per seed
+CFG5_DESC = ("band-retry stream: 2M seeds of the uneven left+right generator (100/150/250 bp reads, divergence "
+             "U[0,5%], 20% unrelated targets) = 4M ksw_extend2 jobs before retries, each side run with w=100 "
+             "and again with w=200 when the score changed and max_off >= 3w/4 (at most 2 tries), from pinned "
+             "host memory in 64k-job chunks (32k seeds) with double-buffered copies; a=1 b=4 o=6 e=1 zdrop=100")
+
+
+def seeds_threaded(fn, seeds, u8, opt, threads):
+    """fn (the oracle's or the reference's seed driver) over `threads` slices of the seeds run side
+    by side (the ctypes calls release the interpreter lock); returns the concatenated records."""
+    from concurrent.futures import ThreadPoolExecutor
+    bounds = np.linspace(0, len(seeds), threads + 1).astype(np.int64)
+    parts = [np.ascontiguousarray(seeds[bounds[i]:bounds[i + 1]]) for i in range(threads)]
+    with ThreadPoolExecutor(threads) as ex:
+        outs = list(ex.map(lambda p: fn(p, u8, opt), parts))
+    return np.concatenate(outs)
+
+
+def run_cfg5_workload(args, ws, rank):
+    """`--workload cfg5`: the seed-level band-retry stream (g3x_extend_seeds_stream) over 2M seeds
+    in 64k-job chunks, the learned width-class schedule against the plain kernel; the regions
+    are compared with the reference's own band-retry lines on the whole stream."""
+    import g3sa_b200 as g
+    from tests import native as nat
+    if args.impl == "reference" and rank != 0:
+        return
+    wl = g.synth(2, CFG5_SEEDS, seed=args.seed + 1000 * rank, w=100, unrelated=0.2)
+    sc = g.default_score()
+    opt_cpu = nat.opt_from_score(sc, w=100)
+    threads = os.cpu_count() or 1
+    oreg = seeds_threaded(nat.oracle_seeds, wl.seeds, wl.u8, opt_cpu, threads)
+    cells = int(oreg["cells"].sum())
+    n = len(wl.seeds)
+    cfg = bench_config(CFG5_DESC, n, cells)
+    kind = "reference" if nat.have_ref() else "port"
+    cpu_fn = nat.ref_seeds if kind == "reference" else nat.oracle_seeds
+    if args.impl == "reference":
+        times = []
+        for it in range(args.warmup + min(args.steps, 3)):
+            t0 = time.perf_counter()
+            seeds_threaded(cpu_fn, wl.seeds, wl.u8, opt_cpu, threads)
+            if it >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        t = sum(times) / len(times)
+        gcups = cells / t / 1e9
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": round(gcups, 4), "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": len(times), "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)", "config": cfg,
+            "seeds_per_s": round(n / t, 1),
+            "cpu_baseline": {"value": round(gcups, 4), "unit": "GCUPS", "cores": threads, "kind": kind,
+                             "sample": "whole workload per step (the reference's band-retry lines, threads over seed slices)"},
+            "e2e": {"value": round(gcups, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+            flush=True)
+        return
+    import torch
+    from g3sa_b200 import build, learn
+    build.build_lib()
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    codes, nmask = wl.planes()
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).pin_memory()  # noqa: E731
+    h_seeds, h_codes, h_nmask = pin(g.device_seeds(wl.seeds)), pin(codes), pin(nmask)
+    h_regs = torch.zeros(n * g.REG_DT.itemsize, dtype=torch.uint8).pin_memory()
+    h_status = torch.full((n,), 99, dtype=torch.int32).pin_memory()
+    mq = int(wl.seeds["l_query"].max())
+    mt = int((wl.seeds["rmax1"] - wl.seeds["rmax0"]).max())
+    ctx = g.Context(local)
+    # the cost model on traces of a held-out job batch of the generator, and width classes tuned
+    # for the learned order on another such batch
+    train_metrics = learn.train(ctx, n_train=TRAIN_UNITS["cfg2"], seed_train=0xA11CE + rank, kind=2, w=100,
+                                unrelated=0.2)
+    tw = g.synth(2, 200000, seed=args.seed + 7 + 1000 * rank, w=100, unrelated=0.2)
+    tc, tn = tw.planes()
+    td = [torch.from_numpy(np.ascontiguousarray(x).view(np.uint8).copy()).to(dev) for x in (tw.jobs, tc, tn)]
+    tiles = ctx.autotune(sc, td[0], tw.n, td[1], td[2], int(tw.jobs["qlen"].max()), int(tw.jobs["tlen"].max()),
+                         schedule=g.SCHED_LEARNED)
+    del td
+    opt = g.default_opt(w=100)
+    stream = torch.cuda.current_stream(dev)
+
+    def call(sched):
+        ctx.extend_seeds_stream(opt, h_seeds, h_codes, h_nmask, len(wl.u8), h_regs, h_status, mq, mt,
+                                chunk=CFG5_CHUNK, schedule=sched)
+
+    # the region fields mem_chain2aln sets; the try counts are the library's and the oracle's own
+    fields = ("rb", "re", "qb", "qe", "score", "truesc", "w")
+    regs = {}
+    for name, sched in (("plain", g.SCHED_PLAIN), ("learned", g.SCHED_LEARNED)):
+        h_status.fill_(99)
+        call(sched)
+        if (h_status.numpy() != 0).any():
+            raise SystemExit(f"{name}: seed errors in the stream")
+        regs[name] = h_regs.numpy().view(g.REG_DT).copy()
+    t0 = time.perf_counter()
+    ref_reg = seeds_threaded(cpu_fn, wl.seeds, wl.u8, opt_cpu, threads) if rank == 0 else None
+    cpu_t = time.perf_counter() - t0
+    same_plain = all(np.array_equal(regs["plain"][f], regs["learned"][f]) for f in fields + ("tries_left", "tries_right"))
+    same_plain = same_plain and all(np.array_equal(regs["learned"][f], oreg[f]) for f in ("tries_left", "tries_right"))
+    same_ref = ref_reg is None or all(np.array_equal(regs["learned"][f], ref_reg[f]) for f in fields)
+    if not (same_plain and same_ref):
+        raise SystemExit("stream regions differ between schedules or from the reference")
+
+    def timed(sched, k, w):
+        for _ in range(w):
+            call(sched)
+        ms = []
+        for _ in range(k):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call(sched)          # blocks until every chunk's regions are back in host memory
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return sum(ms) / len(ms)
+
+    clocks = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    clocks.start()
+    t_learned = timed(g.SCHED_LEARNED, args.steps, args.warmup)
+    clk = clocks.stop()
+    k2 = max(2, args.steps // 2)
+    t_plain = timed(g.SCHED_PLAIN, k2, 1)
+    t_sorted = timed(g.SCHED_SORTED, k2, 1)
+    (t_learned, t_plain, t_sorted), (tot_cells, tot_n) = combine_ranks(dist, [t_learned, t_plain, t_sorted],
+                                                                       [cells, n], dev)
+    if rank != 0:
+        return
+    gcups = tot_cells / (t_learned * 1e-3) / 1e9
+    peak16 = 2 * ctx.int_peak() / 8 / 1e9
+    bi = h_seeds.numel() + h_codes.numel() + h_nmask.numel()
+    bo = h_regs.numel() + 4 * h_status.numel()
+    gc = lambda t: round(tot_cells / (t * 1e-3) / 1e9, 3)  # noqa: E731
+    chunks = (n + CFG5_CHUNK - 1) // CFG5_CHUNK
+    print(json.dumps({
+        "metric": METRIC, "value": round(gcups, 3), "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t_learned, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int16x2 (int32 where the fit fails)", "data": "synthetic (seeded generator)",
+        "config": cfg,
+        "setup": {"chunk_seeds": CFG5_CHUNK, "chunks": chunks, "width_classes": tiles,
+                  "note": "the workload lives in host memory: every step copies each chunk's seeds and plane "
+                          "words in and its regions out (pinned, double-buffered); value and e2e are the same "
+                          "measurement"},
+        "seeds_per_s": round(tot_n / (t_learned * 1e-3), 1),
+        "extensions_per_s": round(int(regs["learned"]["tries_left"].sum() + regs["learned"]["tries_right"].sum())
+                                  / (t_learned * 1e-3), 1),
+        "arms": {"learned": {"gcups": gc(t_learned), "ms": round(t_learned, 4)},
+                 "sorted": {"gcups": gc(t_sorted), "ms": round(t_sorted, 4)},
+                 "plain": {"gcups": gc(t_plain), "ms": round(t_plain, 4),
+                           "kernel": "one 32-lane block per job, anti-diagonal wavefront"}},
+        "speedup_learned_vs_plain": round(t_plain / t_learned, 3),
+        "speedup_learned_vs_sorted": round(t_sorted / t_learned, 3),
+        "cost_model": train_metrics,
+        "e2e": {"value": round(gcups, 3), "unit": "GCUPS", "ms_per_step": round(t_learned, 4),
+                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+                "api": "g3x_extend_seeds_stream per step (pinned host seeds, planes and regions)"},
+        "roofline": {"bound": "int_alu", "achieved": round(gcups / max(ws, 1), 3), "peak": round(peak16, 3),
+                     "unit": "GCUPS", "frac": round(gcups / max(ws, 1) / peak16, 4), "traffic": None,
+                     "note": "the whole stream (copies, seed waves, band retries) against the int16x2 cells/s "
+                             "roofline (measured 32-bit int ops/s / 8 ops per cell x 2)"},
+        "cpu_baseline": {"value": round(cells / cpu_t / 1e9, 4), "unit": "GCUPS", "cores": threads, "kind": kind,
+                         "sample": "whole rank-0 workload, one pass: the reference's band-retry lines, threads over seed slices",
+                         "gpu_regions_identical": same_ref},
+        "clocks": clk, "outputs_equal_plain_kernel": same_plain,
+        "gpu_launches": None,
     }), flush=True)
 
 
@@ -812,6 +994,9 @@ def main():
         return
     if args.workload == "seedsw":
         run_sw_workload(args, ws, rank)
+        return
+    if args.workload == "cfg5":
+        run_cfg5_workload(args, ws, rank)
         return
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)

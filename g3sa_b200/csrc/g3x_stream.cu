@@ -5,7 +5,8 @@
 // plane words to one of two device buffer sets on a copy stream, and runs the seed-level
 // pipeline of g3x_seeds.cu on a compute stream that waits for the copy.  While chunk k is
 // extended, chunk k+1 is copied into the other set.  Results come back through pinned
-// staging buffers.
+// staging buffers.  The buffer sets, staging and streams live in the context and are grown
+// on demand, so repeated calls allocate nothing.
 #include <cuda_runtime.h>
 #include <string.h>
 #include <algorithm>
@@ -24,31 +25,52 @@ struct ChunkRange {
     int64_t bases;        // bases copied
 };
 
-struct Set {
-    g3x_seed_t* d_seeds = nullptr;
-    uint32_t* d_codes = nullptr;
-    uint32_t* d_nmask = nullptr;
-    g3x_reg_t* d_regs = nullptr;
-    int32_t* d_status = nullptr;
-    g3x_seed_t* h_seeds = nullptr;   // pinned staging
-    g3x_reg_t* h_regs = nullptr;
-    int32_t* h_status = nullptr;
-    cudaEvent_t h2d = nullptr, done = nullptr;
-    int64_t pending = -1;            // chunk whose results sit in this set
-};
-
-void release(Set& s) {
+void release(StreamSet& s) {
     cudaFree(s.d_seeds); cudaFree(s.d_codes); cudaFree(s.d_nmask); cudaFree(s.d_regs);
     cudaFree(s.d_status);
     cudaFreeHost(s.h_seeds); cudaFreeHost(s.h_regs); cudaFreeHost(s.h_status);
     if (s.h2d) cudaEventDestroy(s.h2d);
     if (s.done) cudaEventDestroy(s.done);
+    s = StreamSet();
+}
+
+// Buffer sets for chunks of `chunk` seeds and the given plane words, kept when large enough.
+int grow_stream(StreamScratch& ss, int64_t chunk, int64_t code_words, int64_t mask_words) {
+    if (!ss.copy_st && (cudaStreamCreateWithFlags(&ss.copy_st, cudaStreamNonBlocking) != cudaSuccess ||
+                        cudaStreamCreateWithFlags(&ss.comp_st, cudaStreamNonBlocking) != cudaSuccess))
+        return G3X_ERR_CUDA;
+    if (chunk <= ss.seeds && code_words <= ss.code_words && mask_words <= ss.mask_words) return G3X_OK;
+    chunk = std::max(chunk, ss.seeds);
+    code_words = std::max(code_words, ss.code_words);
+    mask_words = std::max(mask_words, ss.mask_words);
+    bool ok = true;
+    for (int b = 0; b < 2 && ok; ++b) {
+        StreamSet& s = ss.set[b];
+        release(s);
+        ok = cudaMalloc(&s.d_seeds, chunk * sizeof(g3x_seed_t)) == cudaSuccess &&
+             cudaMalloc(&s.d_codes, code_words * sizeof(uint32_t)) == cudaSuccess &&
+             cudaMalloc(&s.d_nmask, mask_words * sizeof(uint32_t)) == cudaSuccess &&
+             cudaMalloc(&s.d_regs, chunk * sizeof(g3x_reg_t)) == cudaSuccess &&
+             cudaMalloc(&s.d_status, chunk * sizeof(int32_t)) == cudaSuccess &&
+             cudaMallocHost(&s.h_seeds, chunk * sizeof(g3x_seed_t)) == cudaSuccess &&
+             cudaMallocHost(&s.h_regs, chunk * sizeof(g3x_reg_t)) == cudaSuccess &&
+             cudaMallocHost(&s.h_status, chunk * sizeof(int32_t)) == cudaSuccess &&
+             cudaEventCreateWithFlags(&s.h2d, cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (!ok) {
+        for (int b = 0; b < 2; ++b) release(ss.set[b]);
+        ss.seeds = ss.code_words = ss.mask_words = 0;
+        return G3X_ERR_NOMEM;
+    }
+    ss.seeds = chunk; ss.code_words = code_words; ss.mask_words = mask_words;
+    return G3X_OK;
 }
 
 }  // namespace
 
-int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), const g3x_opt_t& opt,
-                        const ScoreParams& sp, const g3x_seed_t* h_seeds, int64_t n,
+int extend_seeds_stream(StreamScratch& ss, SeedScratch& ws, int (*grow)(SeedScratch&, int64_t),
+                        const g3x_opt_t& opt, const ScoreParams& sp, const g3x_seed_t* h_seeds, int64_t n,
                         const uint32_t* h_codes, const uint32_t* h_nmask, int64_t n_bases,
                         g3x_reg_t* h_regs, int32_t* h_status, int32_t chunk,
                         const LaunchDesc& proto, const WaveRunner* runner) {
@@ -74,27 +96,12 @@ int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), con
     }
     int rc = grow(ws, chunk);
     if (rc) return rc;
-    const int64_t code_words = (max_bases + 15) / 16 + 2, mask_words = (max_bases + 31) / 32 + 2;
-    Set sets[2];
-    cudaStream_t copy_st = nullptr, comp_st = nullptr;
-    bool ok = cudaStreamCreateWithFlags(&copy_st, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaStreamCreateWithFlags(&comp_st, cudaStreamNonBlocking) == cudaSuccess;
-    for (int b = 0; b < 2 && ok; ++b) {
-        Set& s = sets[b];
-        ok = cudaMalloc(&s.d_seeds, chunk * sizeof(g3x_seed_t)) == cudaSuccess &&
-             cudaMalloc(&s.d_codes, code_words * sizeof(uint32_t)) == cudaSuccess &&
-             cudaMalloc(&s.d_nmask, mask_words * sizeof(uint32_t)) == cudaSuccess &&
-             cudaMalloc(&s.d_regs, chunk * sizeof(g3x_reg_t)) == cudaSuccess &&
-             cudaMalloc(&s.d_status, chunk * sizeof(int32_t)) == cudaSuccess &&
-             cudaMallocHost(&s.h_seeds, chunk * sizeof(g3x_seed_t)) == cudaSuccess &&
-             cudaMallocHost(&s.h_regs, chunk * sizeof(g3x_reg_t)) == cudaSuccess &&
-             cudaMallocHost(&s.h_status, chunk * sizeof(int32_t)) == cudaSuccess &&
-             cudaEventCreateWithFlags(&s.h2d, cudaEventDisableTiming) == cudaSuccess &&
-             cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) == cudaSuccess;
-    }
-    rc = ok ? G3X_OK : G3X_ERR_NOMEM;
+    if ((rc = grow_stream(ss, chunk, (max_bases + 15) / 16 + 2, (max_bases + 31) / 32 + 2))) return rc;
+    StreamSet* sets = ss.set;
+    cudaStream_t copy_st = ss.copy_st, comp_st = ss.comp_st;
+    for (int b = 0; b < 2; ++b) sets[b].pending = -1;
     const int64_t total_code_words = (n_bases + 15) / 16, total_mask_words = (n_bases + 31) / 32;
-    auto drain = [&](Set& s) -> int {
+    auto drain = [&](StreamSet& s) -> int {
         if (s.pending < 0) return G3X_OK;
         if (cudaEventSynchronize(s.done) != cudaSuccess) return G3X_ERR_CUDA;
         const ChunkRange& R = ranges[(size_t)s.pending];
@@ -104,7 +111,7 @@ int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), con
         return G3X_OK;
     };
     for (int64_t c = 0; c < nchunks && rc == G3X_OK; ++c) {
-        Set& s = sets[c & 1];
+        StreamSet& s = sets[c & 1];
         const ChunkRange& R = ranges[(size_t)c];
         if ((rc = drain(s))) break;                      // set free: its last chunk is done
         for (int64_t k = 0; k < R.count; ++k) {
@@ -123,8 +130,10 @@ int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), con
             rc = G3X_ERR_CUDA;
             break;
         }
+        LaunchDesc cp = proto;                 // the chunk's planes: its copied words, re-based
+        cp.n_bases = std::min<int64_t>(cw * 16, mw * 32);
         if ((rc = extend_seeds(ws, opt, sp, s.d_seeds, (int)R.count, s.d_codes, s.d_nmask, s.d_regs,
-                               s.d_status, proto, comp_st, runner)))
+                               s.d_status, cp, comp_st, runner)))
             break;
         if (cudaMemcpyAsync(s.h_regs, s.d_regs, R.count * sizeof(g3x_reg_t), cudaMemcpyDeviceToHost, comp_st) ||
             cudaMemcpyAsync(s.h_status, s.d_status, R.count * sizeof(int32_t), cudaMemcpyDeviceToHost, comp_st) ||
@@ -138,12 +147,16 @@ int extend_seeds_stream(SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), con
         int r2 = drain(sets[b]);
         if (rc == G3X_OK) rc = r2;
     }
-    if (comp_st) cudaStreamSynchronize(comp_st);
-    if (copy_st) cudaStreamSynchronize(copy_st);
-    for (int b = 0; b < 2; ++b) release(sets[b]);
-    if (comp_st) cudaStreamDestroy(comp_st);
-    if (copy_st) cudaStreamDestroy(copy_st);
+    cudaStreamSynchronize(comp_st);
+    cudaStreamSynchronize(copy_st);
     return rc;
+}
+
+void free_stream_scratch(StreamScratch& ss) {
+    for (int b = 0; b < 2; ++b) release(ss.set[b]);
+    if (ss.comp_st) cudaStreamDestroy(ss.comp_st);
+    if (ss.copy_st) cudaStreamDestroy(ss.copy_st);
+    ss = StreamScratch();
 }
 
 }  // namespace g3x
