@@ -155,11 +155,11 @@ def lib():
         I64 = ctypes.c_int64
         L.g3x_chain2aln.argtypes = [P, P, P, P, I32, P, I32, P, I32, P, P, P, P, P, P, P]
         L.g3x_chain2aln.restype = ctypes.c_int
-        L.g3x_ksw_global2_batch.argtypes = [P, P, P, I32, P, P, I32, I32, I32, P, P, I32, P, P, P, I32, P, P]
+        L.g3x_ksw_global2_batch.argtypes = [P, P, P, I32, P, P, I64, I32, I32, I32, P, P, I32, P, P, P, I32, P, P]
         L.g3x_ksw_global2_batch.restype = ctypes.c_int
-        L.g3x_ksw_align2_batch.argtypes = [P, P, P, I32, P, P, I32, I32, P, P, P]
+        L.g3x_ksw_align2_batch.argtypes = [P, P, P, I32, P, P, I64, I32, I32, P, P, P]
         L.g3x_ksw_align2_batch.restype = ctypes.c_int
-        L.g3x_flt_chained_seeds.argtypes = [P, P, I32, P, P, I32, P, I32, P, I32, P, P, P, P, P]
+        L.g3x_flt_chained_seeds.argtypes = [P, P, I32, P, P, I32, P, I32, P, I32, P, P, I64, P, P, P]
         L.g3x_flt_chained_seeds.restype = ctypes.c_int
         L.g3x_pac_to_planes.argtypes = [P, I64, P, P, I64, P]
         L.g3x_pac_to_planes.restype = ctypes.c_int
@@ -442,31 +442,37 @@ class Context:
         _check(rc, "g3x_chain2aln")
 
     def global_batch(self, score, d_jobs, n, d_codes, d_nmask, max_qlen, max_tlen, max_w, d_score, d_cigar,
-                     cigar_stride, d_n_cigar, d_status, d_nm=None, d_md=None, md_stride=0, stream=None):
+                     cigar_stride, d_n_cigar, d_status, d_nm=None, d_md=None, md_stride=0, stream=None,
+                     n_bases=None):
         """g3x_ksw_global2_batch on device buffers (JOB_DT jobs; the job's w is the band; NM/MD
         when d_nm and d_md are given)."""
         _check(lib().g3x_ksw_global2_batch(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
-                                           _ptr(d_nmask), int(max_qlen), int(max_tlen), int(max_w), _ptr(d_score),
+                                           _ptr(d_nmask), plane_bases(d_codes, d_nmask, n_bases), int(max_qlen),
+                                           int(max_tlen), int(max_w), _ptr(d_score),
                                            _ptr(d_cigar), int(cigar_stride), _ptr(d_n_cigar), _ptr(d_nm),
                                            _ptr(d_md), int(md_stride), _ptr(d_status), _stream(stream)),
                "g3x_ksw_global2_batch")
 
-    def align2_batch(self, score, d_jobs, n, d_codes, d_nmask, xtra, max_tlen, d_out, d_status, stream=None):
+    def align2_batch(self, score, d_jobs, n, d_codes, d_nmask, xtra, max_tlen, d_out, d_status, stream=None,
+                     n_bases=None):
         """g3x_ksw_align2_batch on device buffers: JOB_DT jobs, SWR_DT results (kswr_t), the
         KSW_X* flags in xtra."""
         _check(lib().g3x_ksw_align2_batch(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
-                                          _ptr(d_nmask), int(xtra), int(max_tlen), _ptr(d_out), _ptr(d_status),
+                                          _ptr(d_nmask), plane_bases(d_codes, d_nmask, n_bases), int(xtra),
+                                          int(max_tlen), _ptr(d_out), _ptr(d_status),
                                           _stream(stream)),
                "g3x_ksw_align2_batch")
 
     def flt_chained_seeds(self, opt, min_chain_weight, l_pac, ref_off, d_anns, n_seqs, d_reads, n_reads, d_chains,
-                          n_chains, d_seeds, n_seeds, d_codes, d_nmask, d_status, d_sw_score=None, stream=None):
+                          n_chains, d_seeds, n_seeds, d_codes, d_nmask, d_status, d_sw_score=None, stream=None,
+                          n_bases=None):
         """g3x_flt_chained_seeds on device buffers (the chain and seed arrays change in place)."""
         ri = np.zeros(1, REFINFO_DT)
         ri["l_pac"], ri["ref_off"], ri["n_seqs"], ri["d_anns"] = l_pac, ref_off, n_seqs, _ptr(d_anns)
         _check(lib().g3x_flt_chained_seeds(self._h, opt.ctypes.data, int(min_chain_weight), ri.ctypes.data,
                                            _ptr(d_reads), int(n_reads), _ptr(d_chains), int(n_chains), _ptr(d_seeds),
-                                           int(n_seeds), _ptr(d_codes), _ptr(d_nmask), _ptr(d_sw_score),
+                                           int(n_seeds), _ptr(d_codes), _ptr(d_nmask),
+                                           plane_bases(d_codes, d_nmask, n_bases), _ptr(d_sw_score),
                                            _ptr(d_status), _stream(stream)),
                "g3x_flt_chained_seeds")
 

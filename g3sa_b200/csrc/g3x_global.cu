@@ -43,6 +43,7 @@ struct GlobalDesc {
     int32_t* nm;           // optional: NM per job
     char* md;              // optional: MD string per job, md_stride bytes each
     int32_t n, qmax, tmax, wmax, ncol, ring, stride, md_stride;
+    int64_t n_bases;       // bases the planes hold: jobs reaching past them are refused
 };
 
 // Appends the decimal digits of v (>= 0) to buf[l ...] while they fit below cap.
@@ -116,8 +117,9 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
             const g3x_job_t jb = d.jobs[job];
             qlen = jb.qlen; tlen = jb.tlen; w = jb.w; flags = jb.flags;
             t_off = jb.t_off; trev = (jb.flags & G3X_JOB_TREV) != 0;
-            if (qlen > d.qmax || tlen > d.tmax || w < 0 || w > d.wmax) {
-                d.score[job] = 0; d.n_cigar[job] = 0; d.status[job] = G3X_ERR_TOO_LONG;
+            const bool outside = !job_in_planes(jb, d.n_bases);   // refused before any base is read
+            if (qlen > d.qmax || tlen > d.tmax || w < 0 || w > d.wmax || outside) {
+                d.score[job] = 0; d.n_cigar[job] = 0; d.status[job] = outside ? G3X_ERR_INVALID : G3X_ERR_TOO_LONG;
                 if (d.nm) { d.nm[job] = 0; d.md[(int64_t)job * d.md_stride] = 0; }
             } else {
                 live = true;
@@ -275,7 +277,7 @@ __global__ void __launch_bounds__(64) global_kernel(GlobalDesc d, ScoreParams sp
 }  // namespace g3x
 
 extern "C" int g3x_ksw_global2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs, int32_t n,
-                                     const uint32_t* d_codes, const uint32_t* d_nmask, int32_t max_qlen,
+                                     const uint32_t* d_codes, const uint32_t* d_nmask, int64_t n_bases, int32_t max_qlen,
                                      int32_t max_tlen, int32_t max_w, int32_t* d_score, uint32_t* d_cigar,
                                      int32_t cigar_stride, int32_t* d_n_cigar, int32_t* d_nm, char* d_md,
                                      int32_t md_stride, int32_t* d_status, void* stream) {
@@ -284,6 +286,7 @@ extern "C" int g3x_ksw_global2_batch(g3x_ctx* ctx, const g3x_score_t* score, con
         return G3X_ERR_INVALID;
     if ((d_nm != nullptr) != (d_md != nullptr) || (d_nm && md_stride < 2)) return G3X_ERR_INVALID;
     if (n == 0) return G3X_OK;
+    if (n_bases < 1 || n_bases > 0x100000000ll) return G3X_ERR_INVALID;
     if (!d_jobs || !d_codes || !d_nmask || !d_score || !d_cigar || !d_n_cigar || !d_status) return G3X_ERR_INVALID;
     ScoreParams sp;
     int rc = score_params(score, &sp);
@@ -293,7 +296,7 @@ extern "C" int g3x_ksw_global2_batch(g3x_ctx* ctx, const g3x_score_t* score, con
     GlobalDesc d;
     d.jobs = d_jobs; d.codes = d_codes; d.nmask = d_nmask; d.score = d_score; d.cigar = d_cigar;
     d.n_cigar = d_n_cigar; d.status = d_status; d.n = n;
-    d.nm = d_nm; d.md = d_md; d.md_stride = md_stride;
+    d.nm = d_nm; d.md = d_md; d.md_stride = md_stride; d.n_bases = n_bases;
     d.qmax = std::max(max_qlen, 1); d.tmax = std::max(max_tlen, 1); d.wmax = max_w;
     d.ncol = std::max(1, std::min(d.qmax, 2 * max_w + 1));
     d.ring = ((2 * max_w + 3) + 3) & ~3;

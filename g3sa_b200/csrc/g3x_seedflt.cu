@@ -136,15 +136,15 @@ __global__ void sfl_keep_kernel(int32_t a, const g3x_read_t* __restrict__ reads,
 extern "C" int g3x_flt_chained_seeds(g3x_ctx* ctx, const g3x_opt_t* opt, int32_t min_chain_weight,
                                      const g3x_refinfo_t* ref, const g3x_read_t* d_reads, int32_t n_reads,
                                      g3x_chain_t* d_chains, int32_t n_chains, g3x_cseed_t* d_seeds, int32_t n_seeds,
-                                     const uint32_t* d_codes, const uint32_t* d_nmask, int32_t* d_sw_score,
-                                     int32_t* d_status, void* stream) {
+                                     const uint32_t* d_codes, const uint32_t* d_nmask, int64_t n_bases,
+                                     int32_t* d_sw_score, int32_t* d_status, void* stream) {
     using namespace g3x;
     if (!ctx || !opt || !ref || n_reads < 0 || n_chains < 0 || n_seeds < 0 || min_chain_weight < 0)
         return G3X_ERR_INVALID;
     if (n_reads == 0) return G3X_OK;
     if (!d_reads || !d_status || (n_chains && !d_chains) || (n_seeds && (!d_seeds || !d_codes || !d_nmask)) ||
         ref->l_pac <= 0 || ref->n_seqs <= 0 || !ref->d_anns || ref->ref_off < 0 ||
-        ref->ref_off + 2 * ref->l_pac > 0xFFFFFFFFLL)
+        ref->ref_off + 2 * ref->l_pac > 0xFFFFFFFFLL || (n_seeds && (n_bases < 1 || n_bases > 0x100000000ll)))
         return G3X_ERR_INVALID;
     ScoreParams sp;
     int rc = score_params(&opt->score, &sp);
@@ -173,7 +173,8 @@ extern "C" int g3x_flt_chained_seeds(g3x_ctx* ctx, const g3x_opt_t* opt, int32_t
                                         d_reads, n_reads, d_chains, n_chains, d_seeds, n_seeds, jobs, flag, min_hsp);
     if (cudaPeekAtLastError() != cudaSuccess) return G3X_ERR_CUDA;
     if (n_seeds > 0 &&
-        (rc = g3x_ksw_align2_batch(ctx, &opt->score, jobs, n_seeds, d_codes, d_nmask, 0, 0, sw, sw_st, stream)))
+        (rc = g3x_ksw_align2_batch(ctx, &opt->score, jobs, n_seeds, d_codes, d_nmask, n_bases, 0, 0, sw, sw_st,
+                                   stream)))
         return rc;
     sfl_keep_kernel<<<nb, tb, 0, st>>>(opt->a, d_reads, n_reads, d_chains, d_seeds, sw, sw_st, flag, min_hsp,
                                         d_sw_score, d_status);

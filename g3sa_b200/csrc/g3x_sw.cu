@@ -58,6 +58,7 @@ struct SwDesc {
     int32_t xtra, maxmat;
     uint32_t tab[10];          // per target base: score bytes (lo: codes 0-3, hi: N, then 0)
     uint32_t nedel, noedel, neins, noeins;   // -e_del, -(o_del+e_del), ... as int16x2
+    int64_t n_bases;           // bases the planes hold: jobs reaching past them are refused
 };
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t c) {
@@ -328,6 +329,7 @@ __global__ void __launch_bounds__(128) sw_kernel(SwDesc d) {
             qlen = jb.qlen; tlen = jb.tlen;
             int st = G3X_OK;
             if (qlen < 1) st = G3X_ERR_INVALID;     // the reference reads before its buffers
+            else if (!job_in_planes(jb, d.n_bases)) st = G3X_ERR_INVALID;   // past the planes: unread
             else if (qlen > QMAX || (subo && tlen > d.sub_stride)) st = G3X_ERR_TOO_LONG;
             if (st != G3X_OK) {
                 if (p == 0) {
@@ -458,7 +460,8 @@ int launch_class(const SwDesc& d0, const int32_t* range, int32_t* queue, int sms
 }  // namespace g3x
 
 extern "C" int g3x_ksw_align2_batch(g3x_ctx* ctx, const g3x_score_t* score, const g3x_job_t* d_jobs, int32_t n,
-                                    const uint32_t* d_codes, const uint32_t* d_nmask, int32_t xtra, int32_t max_tlen,
+                                    const uint32_t* d_codes, const uint32_t* d_nmask, int64_t n_bases, int32_t xtra,
+                                    int32_t max_tlen,
                                     g3x_swr_t* d_out, int32_t* d_status, void* stream) {
     using namespace g3x;
     if (!ctx || !score || n < 0 || max_tlen < 0) return G3X_ERR_INVALID;
@@ -466,6 +469,7 @@ extern "C" int g3x_ksw_align2_batch(g3x_ctx* ctx, const g3x_score_t* score, cons
     if (xtra & G3X_KSW_XBYTE) return G3X_ERR_INVALID;
     if (n == 0) return G3X_OK;
     if (!d_jobs || !d_codes || !d_nmask || !d_out || !d_status) return G3X_ERR_INVALID;
+    if (n_bases < 1 || n_bases > 0x100000000ll) return G3X_ERR_INVALID;
     ScoreParams sp;
     int rc = score_params(score, &sp);
     if (rc) return rc;
@@ -509,7 +513,7 @@ extern "C" int g3x_ksw_align2_batch(g3x_ctx* ctx, const g3x_score_t* score, cons
     d.out = d_out; d.status = d_status;
     d.sub = subo ? s.sub : nullptr;
     d.sub_stride = subo ? std::max(max_tlen, 1) : 0;
-    d.xtra = xtra; d.maxmat = sp.max_sc;
+    d.xtra = xtra; d.maxmat = sp.max_sc; d.n_bases = n_bases;
     for (int a = 0; a < 5; ++a) {
         uint32_t lo = 0;
         for (int c = 0; c < 4; ++c) lo |= (uint32_t)(uint8_t)sp.mat[a * 5 + c] << (8 * c);

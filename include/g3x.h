@@ -400,7 +400,8 @@ int g3x_traceback_pairs(const g3x_opt_t *opt, const g3x_refinfo_t *ref, const g3
 /* n calls of ksw_global2 (bwa/src/ksw.cu:706-809) as traceback_baseline issues them
    (bwa/src/aux.cu:2794-2830): job k aligns its query (q_off, qlen) globally to its target
    (t_off, tlen) inside the band |i - j| <= w (the job's w; h0 unused; G3X_JOB_QREV/TREV read
-   the planes reversed).  d_score[k] = the reference's return value; the CIGAR (BAM order,
+   the planes reversed; a job reaching past the planes' n_bases bases gets G3X_ERR_INVALID,
+   unread).  d_score[k] = the reference's return value; the CIGAR (BAM order,
    len << 4 | op, 0 = M, 1 = I, 2 = D, runs merged as push_cigar does, ksw.cu:694-704) goes to
    d_cigar[k * cigar_stride ...] and its length to d_n_cigar[k].  When no alignment inside the
    band reaches the last cell (score <= -2^29) the reference's backtrack reads direction bytes
@@ -416,7 +417,7 @@ int g3x_traceback_pairs(const g3x_opt_t *opt, const g3x_refinfo_t *ref, const g3
    context belong on one stream.  Asynchronous on `stream`. */
 #define G3X_JOB_MDRC 4u   /* MD prints the reverse-strand alphabet "TGCAN" */
 int g3x_ksw_global2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
-                          const uint32_t *d_codes, const uint32_t *d_nmask, int32_t max_qlen,
+                          const uint32_t *d_codes, const uint32_t *d_nmask, int64_t n_bases, int32_t max_qlen,
                           int32_t max_tlen, int32_t max_w, int32_t *d_score, uint32_t *d_cigar,
                           int32_t cigar_stride, int32_t *d_n_cigar, int32_t *d_nm, char *d_md,
                           int32_t md_stride, int32_t *d_status, void *stream);
@@ -427,7 +428,8 @@ int g3x_ksw_global2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_
    117-143); the reference stops ksw_align2 at its first statement (ksw.cu:276), and this is
    the function as written after it, with 16-bit cells (the only kind its ksw_i16 reads).
    Job k aligns its query (q_off, qlen) locally to its target (t_off, tlen) (h0 and w unused;
-   G3X_JOB_QREV/TREV read the planes reversed); d_out[k] is the kswr_t: best score, its end on
+   G3X_JOB_QREV/TREV read the planes reversed; a job reaching past the planes' n_bases bases gets
+   G3X_ERR_INVALID, unread); d_out[k] is the kswr_t: best score, its end on
    the target (te) and query (qe); with G3X_KSW_XSUBO (minimum score in xtra & 0xffff) the
    best row maximum more than ceil(score / max(mat)) rows from te (score2, te2); with
    G3X_KSW_XSTART the start positions (tb, qb) from the reversed pass, when it finds the same
@@ -447,8 +449,8 @@ typedef struct {
 #define G3X_KSW_XSUBO  0x40000
 #define G3X_KSW_XSTART 0x80000
 int g3x_ksw_align2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t *d_jobs, int32_t n,
-                         const uint32_t *d_codes, const uint32_t *d_nmask, int32_t xtra, int32_t max_tlen,
-                         g3x_swr_t *d_out, int32_t *d_status, void *stream);
+                         const uint32_t *d_codes, const uint32_t *d_nmask, int64_t n_bases, int32_t xtra,
+                         int32_t max_tlen, g3x_swr_t *d_out, int32_t *d_status, void *stream);
 
 /* The seed filter of long reads: mem_flt_chained_seeds (bwa/src/aux.cu:145-162) for every read,
    as CHAINFILTERING_flt_chained_seeds_kernel runs it (aux.cu:1991-2030), with the window score
@@ -460,7 +462,8 @@ int g3x_ksw_align2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t
    in order, the seeds without a window (their score becoming len * a) and those scoring at least
    (int)(a * min_l + .499).  d_chains[].n and d_seeds are changed in place, as the reference
    changes its chains; the same layout rules as g3x_chain2aln (a read's chains contiguous, their
-   seeds within the seed array).  d_sw_score (optional): per seed its window score, -1 without a
+   seeds within the seed array; n_bases: the bases the planes hold, windows reaching past them
+   are not aligned).  d_sw_score (optional): per seed its window score, -1 without a
    window, -2 for seeds of reads left alone.  d_status[r]: G3X_OK, or G3X_ERR_INVALID for a read
    whose records lie outside their arrays (its chains untouched).  Only the score of ksw_align2
    is used, which its first pass alone decides, so the start-position pass is not run.  Scratch
@@ -468,7 +471,7 @@ int g3x_ksw_align2_batch(g3x_ctx *ctx, const g3x_score_t *score, const g3x_job_t
 int g3x_flt_chained_seeds(g3x_ctx *ctx, const g3x_opt_t *opt, int32_t min_chain_weight, const g3x_refinfo_t *ref,
                           const g3x_read_t *d_reads, int32_t n_reads, g3x_chain_t *d_chains, int32_t n_chains,
                           g3x_cseed_t *d_seeds, int32_t n_seeds, const uint32_t *d_codes, const uint32_t *d_nmask,
-                          int32_t *d_sw_score, int32_t *d_status, void *stream);
+                          int64_t n_bases, int32_t *d_sw_score, int32_t *d_status, void *stream);
 
 /* ---- host-resident batches, pipelined --------------------------------------------------- */
 /* No counterpart in the reference (its batches stay on the device between pipeline stages).

@@ -109,9 +109,9 @@ def test_widened_entry_points_reject_bad_arguments(lib):
     """The entry points of the rows around the extension check their arguments before any CUDA
     call: no context, negative counts, missing buffers and refused flags return codes."""
     sc = g.default_score()
-    assert lib.g3x_ksw_global2_batch(None, sc.ctypes.data, None, 1, None, None, 10, 10, 5, None, None, 4, None,
-                                     None, None, 0, None, None) == g.G3X_ERR_INVALID
-    assert lib.g3x_ksw_align2_batch(None, sc.ctypes.data, None, 1, None, None, 0, 0, None, None, None) == \
+    assert lib.g3x_ksw_global2_batch(None, sc.ctypes.data, None, 1, None, None, 1000, 10, 10, 5, None, None, 4,
+                                     None, None, None, 0, None, None) == g.G3X_ERR_INVALID
+    assert lib.g3x_ksw_align2_batch(None, sc.ctypes.data, None, 1, None, None, 1000, 0, 0, None, None, None) == \
         g.G3X_ERR_INVALID
     opt = g.default_opt()
     ri = np.zeros(1, g.REFINFO_DT)
@@ -123,7 +123,7 @@ def test_widened_entry_points_reject_bad_arguments(lib):
     assert lib.g3x_traceback_pairs(opt.ctypes.data, ri.ctypes.data, None, 1, None, 1, None, 3, None, None,
                                    None) == g.G3X_ERR_INVALID
     assert lib.g3x_flt_chained_seeds(None, opt.ctypes.data, 0, ri.ctypes.data, None, 1, None, 0, None, 0, None,
-                                     None, None, None, None) == g.G3X_ERR_INVALID
+                                     None, 1000, None, None, None) == g.G3X_ERR_INVALID
     assert lib.g3x_chain2aln(None, opt.ctypes.data, ri.ctypes.data, None, 1, None, 0, None, 0, None, None, None,
                              None, None, None, None) == g.G3X_ERR_INVALID
     assert lib.g3x_pair_generate(opt.ctypes.data, ri.ctypes.data, None, 1, None, 1, None, 1, None, -2, None, None,

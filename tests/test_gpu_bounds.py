@@ -114,3 +114,65 @@ def test_plain_kernel_step_limit_ends_jobs_with_timeout():
     assert (status == 0).all()
     np.testing.assert_array_equal(out, ref)
     np.testing.assert_array_equal(cells, rcells)
+
+
+def move_past(jobs, n_bases):
+    """Some queries and targets moved to end one base or more past n_bases bases; their mask."""
+    jobs = jobs.copy()
+    k = np.arange(len(jobs))
+    q, t = jobs["qlen"].astype(np.int64), jobs["tlen"].astype(np.int64)
+    bq = (k % 5 == 1) & (q > 0)
+    bt = (k % 7 == 2) & (t > 0) & ~bq
+    jobs["q_off"][bq] = n_bases - q[bq] + 1
+    jobs["t_off"][bt] = n_bases - t[bt] + 1 + (k[bt] % 4) * 500
+    return jobs, bq | bt
+
+
+def test_global_alignment_refuses_jobs_past_the_planes():
+    import torch
+    from tests.gpu_util import to_dev
+    cj, u8 = nat.global_jobs(2000, 31, max_len=160)
+    stride = int((cj["qlen"] + cj["tlen"]).max()) + 2
+    s_o, c_o, n_o, _ = nat.oracle_global(cj, u8, g.default_score(), stride)
+    jobs = np.zeros(len(cj), g.JOB_DT)
+    for f in ("q_off", "t_off", "qlen", "tlen", "w"):
+        jobs[f] = cj[f]
+    jobs, bad = move_past(jobs, len(u8))
+    n = len(jobs)
+    codes, nmask = g.pack_planes(u8)
+    d_score = torch.zeros(n, dtype=torch.int32, device="cuda")
+    d_cig = torch.zeros(n * stride, dtype=torch.int32, device="cuda")
+    d_nc = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    d_st = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+    ctx().global_batch(g.default_score(), to_dev(jobs), n, to_dev(codes), to_dev(nmask), int(jobs["qlen"].max()),
+                       int(jobs["tlen"].max()), int(jobs["w"].max()), d_score, d_cig, stride, d_nc, d_st,
+                       n_bases=len(u8))
+    torch.cuda.synchronize()
+    st, sc_, nc = d_st.cpu().numpy(), d_score.cpu().numpy(), d_nc.cpu().numpy()
+    assert (st[bad] == g.G3X_ERR_INVALID).all() and (nc[bad] == 0).all()
+    assert (st[~bad] == 0).all()
+    np.testing.assert_array_equal(sc_[~bad], s_o[~bad])
+    np.testing.assert_array_equal(nc[~bad], n_o[~bad])
+
+
+def test_striped_alignment_refuses_jobs_past_the_planes():
+    import torch
+    from tests.gpu_util import to_dev
+    cj, u8 = nat.sw_jobs(2000, 41)
+    sc = g.default_score()
+    want, _ = nat.oracle_sw(cj, u8, sc, g.KSW_XSTART)
+    jobs = np.zeros(len(cj), g.JOB_DT)
+    for f in ("q_off", "t_off", "qlen", "tlen", "flags"):
+        jobs[f] = cj[f]
+    jobs, bad = move_past(jobs, len(u8))
+    n = len(jobs)
+    codes, nmask = g.pack_planes(u8)
+    d_out = torch.full((n * 7,), -777, dtype=torch.int32, device="cuda")
+    d_st = torch.full((n,), 99, dtype=torch.int32, device="cuda")
+    ctx().align2_batch(sc, to_dev(jobs), n, to_dev(codes), to_dev(nmask), g.KSW_XSTART, int(jobs["tlen"].max()),
+                       d_out, d_st, n_bases=len(u8))
+    torch.cuda.synchronize()
+    out, st = d_out.cpu().numpy().view(g.SWR_DT), d_st.cpu().numpy()
+    assert (st[bad] == g.G3X_ERR_INVALID).all()
+    assert (st[~bad] == 0).all()
+    np.testing.assert_array_equal(out[~bad], want.astype(g.SWR_DT)[~bad])
