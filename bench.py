@@ -43,12 +43,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "ksw_extend2 GCUPS & extensions/s on 1 B200, learned vs plain schedule, bit-exact"
-# DRAM bytes (read + write) per job staged by the lane kernels, from the ncu capture of the
-# width classes' launches summarised in profiles/lane16_kernel_cfg2_classes.md (dram__bytes_read
-# + dram__bytes_write of each class launch / its job count, 100k-seed case): a launch's DRAM
-# traffic is its jobs' headers, query and target plane words and outputs, so it scales with the
-# jobs the launch stages.  Keyed by the class's widest query; None until a capture exists.
-TRAFFIC_PER_JOB = {}
+# DRAM bytes (read + write) per job staged by the int16x2 lane kernel, from the ncu capture of the
+# width classes' launches summarised in profiles/lane16_kernel_cfg2_class_traffic.md
+# (dram__bytes_read + dram__bytes_write of each class launch / its job count, 100k-seed case of the
+# config-2 generator): a launch's DRAM traffic is its jobs' headers, query and target plane words
+# and outputs, so it scales with the jobs the launch stages.  Keyed by the class's widest query.
+TRAFFIC_PER_JOB = {32: 280.2, 56: 324.3, 88: 371.5, 128: 386.2, 168: 559.3, 200: 579.3, 232: 612.5}
 WORKLOADS = {
     # name: (synth kind, units, w, unrelated, description with {w})
     "cfg2": (2, 500000, 100, 0.2,
@@ -1193,7 +1193,7 @@ def main():
         # the step against the blend of its classes' rooflines: the time every class's cells
         # would take at its own kernel's peak, over the measured step time
         ideal_ms = sum(c["cells"] / (peak_of[c["arith"]] * 1e9) * 1e3 for c in classes)
-        tpj = TRAFFIC_PER_JOB.get(dom["width"])
+        tpj = TRAFFIC_PER_JOB.get(dom["width"]) if dom["kernel"] == "lane16" and args.workload == "cfg2" else None
         int16_cells = sum(c["cells"] for c in classes if c["arith"] == "int16x2")
         try:
             with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -1242,6 +1242,9 @@ def main():
                          "frac": round(dom["gcups"] / dom_peak, 4),
                          "traffic": None if tpj is None else int(tpj * dom["jobs"]),
                          "traffic_unit": "DRAM bytes per launch",
+                         "traffic_source": "ncu dram__bytes_read + dram__bytes_write per job of this class "
+                                           "(profiles/lane16_kernel_cfg2_class_traffic.md, 100k-seed case) x the "
+                                           "class's jobs" if tpj is not None else None,
                          "alg_bytes": dom["alg_bytes"],
                          "algorithmic": "cells of the class launch (trip count of ksw.cu:346) / its "
                                         "CUDA-event duration, the class launched alone on the bench stream",

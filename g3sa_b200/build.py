@@ -3,6 +3,8 @@
     libg3x.so      product library: sm_100a kernels + C-ABI host code (nvcc)
     libg3x_emu.so  CPU model of the kernels' warp protocol, loaded by tests only (g++)
     libg3x_emu16.so CPU model of the int16x2 lane kernel's per-lane logic, tests only (nvcc)
+    libg3x_phase.so the product library with phase clocks in the int16x2 lane kernel
+                   (python -m g3sa_b200.build --phase-clocks; profile_case --phase-clocks)
     libg3x_synth.so seeded synthetic workload generator + multi-threaded plane packer (g++)
 
 Run as ``python -m g3sa_b200.build``.  The oracle libraries are built by oracle/Makefile
@@ -46,6 +48,19 @@ def build_lib(force=False, verbose_ptxas=False):
     return out
 
 
+def build_phase_lib(force=False):
+    """libg3x_phase.so: the product library with the int16x2 lane kernel's phase clocks compiled
+    in (-DG3X_PHASE_CLOCKS), for profile_case --phase-clocks only."""
+    out = os.path.join(HERE, "libg3x_phase.so")
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    deps.append(os.path.join(HERE, "..", "include", "g3x.h"))
+    if not force and not _stale(out, deps):
+        return out
+    _run([NVCC] + ARCH + ["-lineinfo", "-O3", "-std=c++17", "-DG3X_PHASE_CLOCKS", "-Xcompiler", "-fPIC", "-shared",
+                          "-o", out] + [os.path.join(CSRC, f) for f in CU_SOURCES])
+    return out
+
+
 def build_emu(force=False):
     out = os.path.join(HERE, "libg3x_emu.so")
     deps = [os.path.join(CSRC, "g3x_emu.cpp"), os.path.join(CSRC, "g3x_core.h")]
@@ -82,6 +97,8 @@ def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
     force = "--force" in argv
     build_lib(force=force, verbose_ptxas="--ptxas-v" in argv)
+    if "--phase-clocks" in argv:
+        build_phase_lib(force=force)
     build_emu(force=force)
     build_emu16(force=force)
     build_synth(force=force)

@@ -18,6 +18,26 @@
 #include "g3x_lane16.cuh"
 #include "g3x_stage.cuh"
 
+// Phase clocks (profiling builds only, -DG3X_PHASE_CLOCKS): each warp adds the SM clock cycles
+// it spends in each phase of its row loop -- refill wave, row begin, the row's blocks, row end,
+// output -- to g3x_phase_clocks[class][phase], the class taken as qcap / 32 (capped at 7); slot
+// 5 counts warp rows and slot 6 the warp's block iterations.  A __syncwarp before each reading
+// makes a phase's time the warp's.  The product library is built without it.
+#ifdef G3X_PHASE_CLOCKS
+__device__ unsigned long long g3x_phase_clocks[8][8];
+extern "C" int g3x_phase_clocks_read(unsigned long long* h, int reset) {
+    if (cudaMemcpyFromSymbol(h, g3x_phase_clocks, sizeof(g3x_phase_clocks)) != cudaSuccess) return G3X_ERR_CUDA;
+    if (reset) {
+        static const unsigned long long zero[8][8] = {};
+        if (cudaMemcpyToSymbol(g3x_phase_clocks, zero, sizeof(zero)) != cudaSuccess) return G3X_ERR_CUDA;
+    }
+    return G3X_OK;
+}
+#define G3X_PHASE(k) do { __syncwarp(); const long long t1_ = clock64(); ph_[k] += t1_ - t0_; t0_ = t1_; } while (0)
+#else
+#define G3X_PHASE(k) do { } while (0)
+#endif
+
 namespace g3x {
 
 size_t lane16_smem_per_warp(int qcap) { return l16::warp_bytes(qcap); }
@@ -61,7 +81,14 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
     J.job = -1;
     bool exhausted = false;
     unsigned long long busy = 0, idle = 0, waves = 0;
+#ifdef G3X_PHASE_CLOCKS
+    unsigned long long ph_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long t0_ = clock64();
+#endif
     for (;;) {
+#ifdef G3X_PHASE_CLOCKS
+        t0_ = clock64();
+#endif
         // ---- refill wave: the warp stages one new job for every idle lane, together ----
         const unsigned idle_mask = __ballot_sync(0xFFFFFFFFu, J.job < 0);
         if (!exhausted && __popc(idle_mask) >= (idle_mask == 0xFFFFFFFFu ? 1 : refill)) {
@@ -109,6 +136,7 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
             }
             __syncwarp();
         }
+        G3X_PHASE(0);
         const bool active = J.job >= 0;
         if (!__any_sync(0xFFFFFFFFu, active)) {
             if (exhausted) break;
@@ -128,6 +156,7 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
             }
             row_begin(J, sp, pools, r);
         }
+        G3X_PHASE(1);
         const bool nonempty = run && r.beg < r.end;
         const int nblk = run ? blocks_in_row(r) : 0;
         const int kmax = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nblk);
@@ -139,7 +168,9 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
         row_blocks<kSym>(P, lane, r, pc, ge, nblk, kmax, mF, mL);
 
         // ---- row end (ksw.cu:371-391) ----
+        G3X_PHASE(2);
         if (run) row_end(J, P, lane, r, sp, nonempty, mF, mL);
+        G3X_PHASE(3);
         if (active && J.K.stop) {
             const Commit& K = J.K;
             d.out[J.job] = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};
@@ -148,7 +179,18 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
             J.job = -1;
         }
         __syncwarp();
+#ifdef G3X_PHASE_CLOCKS
+        G3X_PHASE(4);
+        ph_[5] += 1;
+        ph_[6] += kmax;
+#endif
     }
+#ifdef G3X_PHASE_CLOCKS
+    if (lane == 0) {
+        const int ci = qcap / 32 < 8 ? qcap / 32 : 7;
+        for (int q = 0; q < 7; ++q) atomicAdd(&g3x_phase_clocks[ci][q], ph_[q]);
+    }
+#endif
     if (d.stats) {
         atomicAdd(d.stats + 0, busy);
         atomicAdd(d.stats + 1, idle);
