@@ -49,12 +49,21 @@ __global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
         load16(codes, nmask, jb.q_off, jb.qlen, ch, qrev, xq, nq);
         load16(codes, nmask, jb.t_off, jb.tlen, ch, trev, xt, nt);
         const int nv = kk - (ch << 4) < 16 ? kk - (ch << 4) : 16;
+        // bit t of m: base t of the chunk differs (2-bit codes differ, or N on either side)
         const uint32_t d2 = xq ^ xt;
-        const uint32_t dd = (d2 | (d2 >> 1)) & 0x55555555u;
-        for (int t = 0; t < nv; ++t) {
-            const bool diff = ((dd >> (2 * t)) & 1u) || ((nq | nt) >> t) & 1u;
-            sc += diff ? -4 : 1;
-            if (sc > best) { best = sc; best_at = (ch << 4) + t + 1; }
+        uint32_t m = (d2 | (d2 >> 1)) & 0x55555555u;
+        m = (m | (m >> 1)) & 0x33333333u;
+        m = (m | (m >> 2)) & 0x0F0F0F0Fu;
+        m = (m | (m >> 4)) & 0x00FF00FFu;
+        m = ((m | (m >> 8)) | nq | nt) & 0xFFFFu;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            if (t < nv) {
+                sc += 1 - 5 * (int32_t)((m >> t) & 1u);
+                const bool up = sc > best;
+                best = up ? sc : best;
+                best_at = up ? (ch << 4) + t + 1 : best_at;
+            }
         }
     }
     float* f = feat + (size_t)k * kF;
@@ -67,34 +76,47 @@ __global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
 
 // ---- inference ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256, 2) predict_kernel(const float* __restrict__ params,
+// Two jobs per thread (jobs k and k + 256 of the block's 512), so every weight read from shared
+// memory feeds both jobs' FMAs: the 64x64 layer's weights are read four at a time, and with one
+// job per thread the shared-memory instruction queue, not the FMA pipe, bounds the kernel.  Each
+// job's sums keep their order (each unit's row in order, y summed in unit order).
+__global__ void __launch_bounds__(256, 1) predict_kernel(const float* __restrict__ params,
                                                       const float* __restrict__ feat, int n,
                                                       float* __restrict__ out) {
     __shared__ __align__(16) float w[kParams];
     for (int t = threadIdx.x; t < kParams; t += blockDim.x) w[t] = params[t];
     __syncthreads();
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    float x[kF];
+    const int ka = blockIdx.x * 2 * blockDim.x + threadIdx.x, kb = ka + blockDim.x;
+    if (ka >= n) return;
+    const bool has_b = kb < n;
+    float xa[kF], xb[kF];
 #pragma unroll
-    for (int f = 0; f < kF; ++f) x[f] = feat[(size_t)k * kF + f];
-    float h1[kH];
+    for (int f = 0; f < kF; ++f) {
+        xa[f] = feat[(size_t)ka * kF + f];
+        xb[f] = has_b ? feat[(size_t)kb * kF + f] : 0.0f;
+    }
+    float ha[kH], hb[kH];
 #pragma unroll
     for (int u = 0; u < kH; ++u) {
-        float a = w[ob1 + u];
+        float a = w[ob1 + u], b = a;
 #pragma unroll
-        for (int f = 0; f < kF; ++f) a = fmaf(w[oW1 + u * kF + f], x[f], a);
-        h1[u] = fmaxf(a, 0.0f);
+        for (int f = 0; f < kF; ++f) {
+            const float c = w[oW1 + u * kF + f];
+            a = fmaf(c, xa[f], a);
+            b = fmaf(c, xb[f], b);
+        }
+        ha[u] = fmaxf(a, 0.0f);
+        hb[u] = fmaxf(b, 0.0f);
     }
-    // Four hidden units at a time: four independent accumulation chains (each unit's sum in
-    // the order of its row), rows of W2 four weights per broadcast load, y summed in unit order.
-    float y = w[ob3];
+    // four hidden units at a time: four independent accumulation chains per job, rows of W2
+    // four weights per broadcast load
+    float ya = w[ob3], yb = ya;
     for (int u0 = 0; u0 < kH; u0 += 4) {
-        float a[4];
+        float a[4], b[4];
         const float4* row[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            a[j] = w[ob2 + u0 + j];
+            a[j] = b[j] = w[ob2 + u0 + j];
             row[j] = reinterpret_cast<const float4*>(w + oW2 + (u0 + j) * kH);
         }
 #pragma unroll
@@ -102,16 +124,24 @@ __global__ void __launch_bounds__(256, 2) predict_kernel(const float* __restrict
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const float4 c = row[j][q];
-                a[j] = fmaf(c.x, h1[4 * q], a[j]);
-                a[j] = fmaf(c.y, h1[4 * q + 1], a[j]);
-                a[j] = fmaf(c.z, h1[4 * q + 2], a[j]);
-                a[j] = fmaf(c.w, h1[4 * q + 3], a[j]);
+                a[j] = fmaf(c.x, ha[4 * q], a[j]);
+                b[j] = fmaf(c.x, hb[4 * q], b[j]);
+                a[j] = fmaf(c.y, ha[4 * q + 1], a[j]);
+                b[j] = fmaf(c.y, hb[4 * q + 1], b[j]);
+                a[j] = fmaf(c.z, ha[4 * q + 2], a[j]);
+                b[j] = fmaf(c.z, hb[4 * q + 2], b[j]);
+                a[j] = fmaf(c.w, ha[4 * q + 3], a[j]);
+                b[j] = fmaf(c.w, hb[4 * q + 3], b[j]);
             }
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) y = fmaf(w[oW3 + u0 + j], fmaxf(a[j], 0.0f), y);
+        for (int j = 0; j < 4; ++j) {
+            ya = fmaf(w[oW3 + u0 + j], fmaxf(a[j], 0.0f), ya);
+            yb = fmaf(w[oW3 + u0 + j], fmaxf(b[j], 0.0f), yb);
+        }
     }
-    out[k] = y;
+    out[ka] = ya;
+    if (has_b) out[kb] = yb;
 }
 
 // ---- training: forward with saved activations, backward, Adam ----------------------------
@@ -271,7 +301,7 @@ int model_features(const g3x_job_t* jobs, int n, const uint32_t* codes, const ui
 
 int model_predict(const float* params, const float* feat, int n, float* out, cudaStream_t st) {
     if (n <= 0) return G3X_OK;
-    predict_kernel<<<(n + 255) / 256, 256, 0, st>>>(params, feat, n, out);
+    predict_kernel<<<(n + 511) / 512, 256, 0, st>>>(params, feat, n, out);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }
 
