@@ -35,7 +35,6 @@ ChainScratch& ctx_chain(g3x_ctx* ctx) { return ctx->chain; }
 GlobalScratch& ctx_global(g3x_ctx* ctx) { return ctx->global; }
 SwScratch& ctx_sw(g3x_ctx* ctx) { return ctx->sw; }
 
-static int alloc_sched(SchedScratch& s, int64_t n);
 
 // The jobs in decreasing order of row count, then of widest row (the counting sort of the
 // scheduled batches with one class), so that the jobs a warp takes together are alike.
@@ -122,7 +121,7 @@ int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d) {
     return G3X_OK;
 }
 
-static void free_seed_scratch(SeedScratch& w) {
+void free_seed_scratch(SeedScratch& w) {
     cudaFree(w.ljobs); cudaFree(w.rjobs); cudaFree(w.lext); cudaFree(w.rext);
     cudaFree(w.lstatus); cudaFree(w.rstatus);
     for (int k = 0; k < 4; ++k) cudaFree(w.order[k]);
@@ -147,13 +146,13 @@ int alloc_seed_scratch(SeedScratch& w, int64_t n) {
     return G3X_OK;
 }
 
-static void free_sched(SchedScratch& s) {
+void free_sched(SchedScratch& s) {
     cudaFree(s.bin); cudaFree(s.order); cudaFree(s.hist); cudaFree(s.cursor); cudaFree(s.bucket_oc);
     cudaFree(s.feat); cudaFree(s.pred);
     s = SchedScratch();
 }
 
-static int alloc_sched(SchedScratch& s, int64_t n) {
+int alloc_sched(SchedScratch& s, int64_t n) {
     if (n <= s.cap && s.order) return G3X_OK;
     free_sched(s);
     const int64_t cap = std::max<int64_t>(n, 1024);
@@ -176,15 +175,25 @@ int class_qcap(const TileTable& t, int k, int qmax) {
 
 // Runs the persistent row-parallel kernel over every width class of an ordered batch: one
 // launch per class on its own stream, forked from and joined back into `st`.
+static ClassRes ctx_res(g3x_ctx* ctx) {
+    return ClassRes{&ctx->sched, ctx->d_queue, ctx->side, ctx->fork, ctx->join, ctx->d_stats};
+}
+
 static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParams& sp, cudaStream_t st,
-                          int only = -1, const TileTable* tt_override = nullptr) {
+                          int only = -1, const TileTable* tt_override = nullptr, const ClassRes* res_in = nullptr) {
     const TileTable& tt = tt_override ? *tt_override : ctx->tiles;
-    if (cudaEventRecord(ctx->fork, st) != cudaSuccess) return G3X_ERR_CUDA;
+    const ClassRes res = res_in ? *res_in : ctx_res(ctx);
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st, &cap);
-    const bool timed = ctx->timing && cap == cudaStreamCaptureStatusNone && !tt_override;
-    // timing mode 2 runs the classes one after another on `st`, each timed alone
-    const bool serial = timed && ctx->timing == 2;
+    const bool timed = ctx->timing && cap == cudaStreamCaptureStatusNone && !tt_override && !res_in;
+    // timing mode 2 runs the classes one after another on `st`, each timed alone.  Resources
+    // without side streams chain the classes on `st` as programmatic dependent launches: each
+    // class kernel may start as soon as the one before it is running, so they run side by side
+    // as on separate streams.
+    const bool serial = (timed && ctx->timing == 2) || !res.side;
+    const bool chain = serial && !timed;
+    bool first = true;
+    if (!serial && cudaEventRecord(res.fork, st) != cudaSuccess) return G3X_ERR_CUDA;
     if (timed)
         for (int k = 0; k < kMaxBuckets; ++k) ctx->cls_timed[k] = 0;
     int rc = G3X_OK;
@@ -193,8 +202,8 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
     for (int kk = tt.n - 1; kk >= 0 && rc == G3X_OK; --kk) {
         const int k = kk;
         if (only >= 0 && k != only) continue;
-        cudaStream_t cs = serial ? st : ctx->side[k];
-        if (!serial && cudaStreamWaitEvent(cs, ctx->fork, 0) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
+        cudaStream_t cs = serial ? st : res.side[k];
+        if (!serial && cudaStreamWaitEvent(cs, res.fork, 0) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
         LaunchDesc d = base;
         d.kernel = tt.lanes[k] != 1 ? kKernelRowpar : tt.tile[k] == 2 ? kKernelLane16
                  : tt.tile[k] == 4 ? kKernelLane2 : kKernelLane;
@@ -206,11 +215,13 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
         d.persistent = 1;
         d.warps_per_block = 4;
         d.qmax = class_qcap(tt, k, base.qmax);
-        d.order = ctx->sched.order;
-        d.order_off = ctx->sched.bucket_oc + 2 * k;
-        d.count = ctx->sched.bucket_oc + 2 * k + 1;
-        d.queue = ctx->d_queue + k;
-        d.stats = ctx->d_stats;
+        d.order = res.sched->order;
+        d.order_off = res.sched->bucket_oc + 2 * k;
+        d.count = res.sched->bucket_oc + 2 * k + 1;
+        d.queue = res.queue + k;
+        d.stats = res.stats;
+        d.pdl = chain && !first;
+        first = false;
         if (timed && cudaEventRecord(ctx->cls0[k], cs) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
         if (d.kernel == kKernelLane) {
             rc = launch_lane(d, sp, cs);
@@ -227,8 +238,8 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
             else ctx->cls_timed[k] = 1;
         }
         if (serial) continue;
-        if (rc == G3X_OK && cudaEventRecord(ctx->join[k], cs) != cudaSuccess) rc = G3X_ERR_CUDA;
-        if (rc == G3X_OK && cudaStreamWaitEvent(st, ctx->join[k], 0) != cudaSuccess) rc = G3X_ERR_CUDA;
+        if (rc == G3X_OK && cudaEventRecord(res.join[k], cs) != cudaSuccess) rc = G3X_ERR_CUDA;
+        if (rc == G3X_OK && cudaStreamWaitEvent(st, res.join[k], 0) != cudaSuccess) rc = G3X_ERR_CUDA;
     }
     return rc;
 }
@@ -254,30 +265,24 @@ static int run_scheduled(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParams
     return launch_classes(ctx, base, sp, st);
 }
 
-// A seed-level wave through the width classes: the wave's jobs (a subset of the seed job
-// array) sorted like a batch (length-sorted, or by the model's predictions), then one
-// persistent launch per class.
-struct ClassWave {
-    g3x_ctx* ctx;
-    bool learned;
-};
-
-static int run_class_wave(void* user, const LaunchDesc& d, const ScoreParams& sp, cudaStream_t st) {
+int run_class_wave(void* user, const LaunchDesc& d, const ScoreParams& sp, cudaStream_t st) {
     const ClassWave* w = static_cast<const ClassWave*>(user);
     g3x_ctx* ctx = w->ctx;
+    const ClassRes res = w->res ? *w->res : ctx_res(ctx);
+    SchedScratch& sched = *res.sched;
     const float* pred = nullptr;
     int rc;
     if (w->learned) {
-        if ((rc = model_features(d.jobs, d.n, d.codes, d.nmask, d.n_bases, ctx->sched.feat, st, d.order, d.count)))
+        if ((rc = model_features(d.jobs, d.n, d.codes, d.nmask, d.n_bases, sched.feat, st, d.order, d.count)))
             return rc;
-        if ((rc = model_predict(ctx->model.params, ctx->sched.feat, d.n, ctx->sched.pred, st))) return rc;
-        pred = ctx->sched.pred;
+        if ((rc = model_predict(ctx->model.params, sched.feat, d.n, sched.pred, st))) return rc;
+        pred = sched.pred;
     }
-    if ((rc = schedule_jobs(ctx->sched, d.jobs, d.n, sp, pred, ctx->tiles, st, d.order, d.count))) return rc;
-    if (cudaMemsetAsync(ctx->d_queue, 0, kMaxBuckets * sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
+    if ((rc = schedule_jobs(sched, d.jobs, d.n, sp, pred, ctx->tiles, st, d.order, d.count))) return rc;
+    if (cudaMemsetAsync(res.queue, 0, kMaxBuckets * sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
     LaunchDesc base = d;
     base.order = nullptr; base.count = nullptr; base.order_off = nullptr; base.queue = nullptr;
-    return launch_classes(ctx, base, sp, st);
+    return launch_classes(ctx, base, sp, st, -1, nullptr, w->res);
 }
 
 // Whether a seed-level call goes through the width classes, and how to run its waves.
@@ -293,6 +298,7 @@ static int seed_waves(g3x_ctx* ctx, const g3x_batch_opts_t* opts, const LaunchDe
     if (rc) return rc;
     cw->ctx = ctx;
     cw->learned = learned;
+    cw->res = nullptr;
     wr->run = run_class_wave;
     wr->user = cw;
     *out = wr;
@@ -330,7 +336,7 @@ int g3x_ctx_create(g3x_ctx** out, int device) {
     memset(&c->seeds, 0, sizeof(c->seeds));
     c->device = device;
     cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
-    g3x::default_tiles(c->tiles);
+    g3x::context_tiles(c->tiles);
     bool ok = cudaMalloc(&c->d_queue, 64 * sizeof(int32_t)) == cudaSuccess &&
               cudaMalloc(&c->d_stats, 4 * sizeof(unsigned long long)) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
@@ -701,7 +707,7 @@ int g3x_extend_seeds_stream(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_seed_t
     g3x::WaveRunner wr;
     const g3x::WaveRunner* runner = nullptr;
     if ((rc = g3x::seed_waves(ctx, opts, proto, chunk > 0 ? chunk : 65536, &cw, &wr, &runner))) return rc;
-    return g3x::extend_seeds_stream(ctx->stream, ctx->seeds, g3x::alloc_seed_scratch, *opt, sp, h_seeds, n,
+    return g3x::extend_seeds_stream(ctx->stream, *opt, sp, h_seeds, n,
                                     h_codes, h_nmask, n_bases, h_regs, h_status, chunk, proto, runner);
 }
 

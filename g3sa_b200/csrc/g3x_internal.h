@@ -44,6 +44,8 @@ struct LaunchDesc {
                            // once and waits for all of them; 0 = each group refills alone
     int32_t refill;        // lane-per-job kernel: idle lanes that trigger a refill wave
     int32_t ring;          // lane-per-job kernel: 0, or the columns of its row-buffer ring
+    int32_t pdl;           // class kernels: 1 = launched as a programmatic dependent of the
+                           // class kernel before it on the stream (launch_class_kernel)
     int64_t n_bases;       // bases the planes hold: jobs reaching past them are refused
     int64_t step_limit;    // plain (rolling) kernel: per-job step bound, 0 = the default bound
 };
@@ -76,6 +78,19 @@ inline void default_tiles(TileTable& t) {
     for (int k = 0; k < t.n; ++k) {
         t.width[k] = w[k]; t.lanes[k] = l[k]; t.tile[k] = c[k]; t.warp_batch[k] = 0; t.refill[k] = 1;
     }
+}
+
+// The width classes a new context starts with: the int16x2 lane kernel (g3x_lane16.cu) over
+// seven classes of query length up to 256, refilling in waves of 8 lanes -- the layout the
+// autotuner settles on for reads of 100-250 bp -- then the row-parallel kernel for longer
+// queries and for jobs outside the int16 fit.
+inline void context_tiles(TileTable& t) {
+    const int w[] = {32, 56, 88, 128, 168, 200, 256};
+    t.n = 8;
+    for (int k = 0; k < 7; ++k) {
+        t.width[k] = w[k]; t.lanes[k] = 1; t.tile[k] = 2; t.warp_batch[k] = 0; t.refill[k] = 8;
+    }
+    t.width[7] = 0x7FFFFFFF; t.lanes[7] = 32; t.tile[7] = 9; t.warp_batch[7] = 0; t.refill[7] = 1;
 }
 
 // Sort bins per width class of schedule_jobs (its histogram holds kMaxBuckets * kSchedLevels).
@@ -121,6 +136,25 @@ inline cudaError_t allow_max_smem(F* fn, size_t* limit = nullptr) {
     if (limit) *limit = (size_t)dyn;
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
 }
+// Launches a width-class kernel fn<<<grid, block, smem, st>>>(d, sp).  With d.pdl it goes out
+// as a programmatic dependent of the kernel before it on `st`: it may start as soon as every
+// block of that kernel has called pdl_trigger(), so the classes of one stream run side by side
+// like launches on separate streams, without the streams.
+template <class K>
+inline cudaError_t launch_class_kernel(K* fn, int grid, int block, size_t smem, cudaStream_t st,
+                                       const LaunchDesc& d, const ScoreParams& sp) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = d.pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, fn, d, sp);
+}
 int launch_rolling(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_rowpar(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
@@ -141,6 +175,9 @@ struct SeedScratch {
     int64_t cap;
 };
 
+int alloc_seed_scratch(SeedScratch& w, int64_t n);   // grown to >= n seeds, kept when large enough
+void free_seed_scratch(SeedScratch& w);
+
 // Runs one wave of a seed-level call: d names the wave's job array (d.n entries) and its jobs
 // (d.order[0 .. *d.count)); by default one launch of d.kernel over them.
 struct WaveRunner {
@@ -152,8 +189,40 @@ int extend_seeds(const SeedScratch& ws, const g3x_opt_t& opt, const ScoreParams&
                  const g3x_seed_t* seeds, int n, const uint32_t* codes, const uint32_t* nmask,
                  g3x_reg_t* regs, int32_t* status, const LaunchDesc& proto, cudaStream_t st,
                  const WaveRunner* runner = nullptr);
-// Device buffer sets, pinned staging and streams of the chunked seed stream (g3x_stream.cu),
-// kept in the context between calls and grown on demand.
+// What one width-class pipeline uses: the sort scratch, the classes' job-queue counters
+// (kMaxBuckets), one stream per class and the events that fork the classes from the caller's
+// stream and join them back (side null: the classes chain on the caller's stream as
+// programmatic dependent launches), the occupancy counters (or none).  A context has one; the seed stream keeps one per
+// chunk it runs at a time.
+struct ClassRes {
+    SchedScratch* sched;
+    int32_t* queue;
+    cudaStream_t* side;
+    cudaEvent_t fork;
+    cudaEvent_t* join;
+    unsigned long long* stats;
+};
+int alloc_sched(SchedScratch& s, int64_t n);
+void free_sched(SchedScratch& s);
+
+// A seed-level wave through the width classes (g3x_api.cu): the wave's jobs sorted like a batch
+// (length-sorted, or by the cost model's predictions) with res's scratch, then one persistent
+// launch per class on res's streams (res null: the context's own).
+struct ClassWave {
+    g3x_ctx* ctx;
+    bool learned;
+    const ClassRes* res;
+};
+int run_class_wave(void* user, const LaunchDesc& d, const ScoreParams& sp, cudaStream_t st);
+
+// The chunked seed stream (g3x_stream.cu) runs kStreamLanes chunks at a time, each on its own
+// compute stream with its own device buffer set, pinned staging, seed scratch and width-class
+// scratch, so one chunk's latency-bound waves overlap the next chunks' work.  A lane chains its
+// classes on its own stream as programmatic dependent launches (they still run side by side),
+// so the whole stream stays within a few CUDA streams: more streams than the device's hardware
+// work queues alias onto the same queues and serialise.  Kept in the context between calls and
+// grown on demand.
+constexpr int kStreamLanes = 4;
 struct StreamSet {
     g3x_seed_t* d_seeds = nullptr;
     uint32_t* d_codes = nullptr;
@@ -165,15 +234,22 @@ struct StreamSet {
     int32_t* h_status = nullptr;
     cudaEvent_t h2d = nullptr, done = nullptr;
     int64_t pending = -1;            // chunk whose results sit in this set
+    cudaStream_t comp = nullptr;     // the lane's compute stream
+    SeedScratch seeds = {};          // the lane's seed-level scratch
+    SchedScratch sched;              // the lane's width-class sort scratch
+    int32_t* queue = nullptr;        // and job-queue counters
 };
 struct StreamScratch {
-    StreamSet set[2];
-    cudaStream_t copy_st = nullptr, comp_st = nullptr;
+    StreamSet set[kStreamLanes];
+    cudaStream_t copy_st = nullptr;
     int64_t seeds = 0, code_words = 0, mask_words = 0;   // capacities of each set
+    bool lanes_ready = false;        // streams, events and queues of the lanes created
 };
 void free_stream_scratch(StreamScratch& s);
 
-int extend_seeds_stream(StreamScratch& ss, SeedScratch& ws, int (*grow)(SeedScratch&, int64_t), const g3x_opt_t& opt,
+// runner: the class-wave runner of the call (its ClassWave user is copied per lane with the
+// lane's resources), or null for the call's single kernel.
+int extend_seeds_stream(StreamScratch& ss, const g3x_opt_t& opt,
                         const ScoreParams& sp, const g3x_seed_t* h_seeds, int64_t n,
                         const uint32_t* h_codes, const uint32_t* h_nmask, int64_t n_bases,
                         g3x_reg_t* h_regs, int32_t* h_status, int32_t chunk,

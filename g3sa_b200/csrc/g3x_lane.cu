@@ -229,6 +229,7 @@ __device__ __forceinline__ int32_t wrap_slot(int32_t s, int32_t R) { return s >=
 
 template <bool kRing>
 __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp) {
+    pdl_trigger();
     extern __shared__ __align__(16) char smem[];
     __shared__ uint2 pools[5];
     if (threadIdx.x < 5) {
@@ -463,11 +464,8 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
         }
         __syncwarp();
     }
-    if (d.stats) {
-        atomicAdd(d.stats + 0, busy);
-        atomicAdd(d.stats + 1, idle);
-        if (lane == 0) atomicAdd(d.stats + 2, waves);
-    }
+    if (d.stats) add_warp_stats(d.stats, busy, idle, waves, lane);
+    pdl_chain_end();
 }
 
 template <bool kRing>
@@ -492,8 +490,9 @@ static int launch_lane_t(const LaunchDesc& d, const ScoreParams& sp, cudaStream_
     }
     const size_t smem = (size_t)best_wpb * wb;
     int blocks = d.blocks > 0 ? d.blocks : sms * (best_blocks > 0 ? best_blocks : 1);
-    lane_kernel<kRing><<<blocks, 32 * best_wpb, smem, stream>>>(d, sp);
-    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+    if (launch_class_kernel(lane_kernel<kRing>, blocks, 32 * best_wpb, smem, stream, d, sp) != cudaSuccess)
+        return G3X_ERR_CUDA;
+    return G3X_OK;
 }
 
 // The ring form when the launch names a ring (d.ring > 0, a multiple of 16, at least 64).

@@ -44,6 +44,7 @@ size_t lane16_smem_per_warp(int qcap) { return l16::warp_bytes(qcap); }
 
 template <bool kSym>
 __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams sp) {
+    pdl_trigger();
     using namespace l16;
     extern __shared__ __align__(16) char smem[];
     __shared__ uint2 pools[5];
@@ -191,11 +192,8 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
         for (int q = 0; q < 7; ++q) atomicAdd(&g3x_phase_clocks[ci][q], ph_[q]);
     }
 #endif
-    if (d.stats) {
-        atomicAdd(d.stats + 0, busy);
-        atomicAdd(d.stats + 1, idle);
-        if (lane == 0) atomicAdd(d.stats + 2, waves);
-    }
+    if (d.stats) add_warp_stats(d.stats, busy, idle, waves, lane);
+    pdl_chain_end();
 }
 
 template <bool kSym>
@@ -218,8 +216,9 @@ static int launch_lane16_t(const LaunchDesc& d, const ScoreParams& sp, cudaStrea
     }
     const size_t smem = (size_t)best_wpb * wb;
     const int blocks = d.blocks > 0 ? d.blocks : sms * (best_blocks > 0 ? best_blocks : 1);
-    lane16_kernel<kSym><<<blocks, 32 * best_wpb, smem, stream>>>(d, sp);
-    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+    if (launch_class_kernel(lane16_kernel<kSym>, blocks, 32 * best_wpb, smem, stream, d, sp) != cudaSuccess)
+        return G3X_ERR_CUDA;
+    return G3X_OK;
 }
 
 // Gap opening and extension costs that agree between deletions and insertions (oe_del == oe_ins,

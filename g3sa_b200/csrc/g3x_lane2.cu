@@ -196,6 +196,7 @@ __device__ __forceinline__ void row_setup(Row& r, const Job& J, int32_t i, uint3
 size_t lane2_smem_per_warp(int qcap) { return warp_bytes(qcap); }
 
 __global__ void __launch_bounds__(128) lane2_kernel(LaunchDesc d, ScoreParams sp) {
+    pdl_trigger();
     extern __shared__ __align__(16) char smem[];
     __shared__ uint2 pools[5];
     if (threadIdx.x < 5) {
@@ -480,11 +481,8 @@ __global__ void __launch_bounds__(128) lane2_kernel(LaunchDesc d, ScoreParams sp
         }
         __syncwarp();
     }
-    if (d.stats) {
-        atomicAdd(d.stats + 0, busy);
-        atomicAdd(d.stats + 1, idle);
-        if (lane == 0) atomicAdd(d.stats + 2, waves);
-    }
+    if (d.stats) add_warp_stats(d.stats, busy, idle, waves, lane);
+    pdl_chain_end();
 }
 
 int launch_lane2(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream) {
@@ -506,8 +504,9 @@ int launch_lane2(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream
     }
     const size_t smem = (size_t)best_wpb * wb;
     const int blocks = d.blocks > 0 ? d.blocks : sms * (best_blocks > 0 ? best_blocks : 1);
-    lane2_kernel<<<blocks, 32 * best_wpb, smem, stream>>>(d, sp);
-    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+    if (launch_class_kernel(lane2_kernel, blocks, 32 * best_wpb, smem, stream, d, sp) != cudaSuccess)
+        return G3X_ERR_CUDA;
+    return G3X_OK;
 }
 
 }  // namespace g3x

@@ -205,6 +205,7 @@ __device__ __forceinline__ void dp_row(RowJob& J, const ScoreParams& sp, EhSlot3
 
 template <int G, int C>
 __global__ void __launch_bounds__(128) rowpar_kernel(LaunchDesc d, ScoreParams sp) {
+    pdl_trigger();
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31;
     const int r = lane & (G - 1);
@@ -313,6 +314,7 @@ __global__ void __launch_bounds__(128) rowpar_kernel(LaunchDesc d, ScoreParams s
         atomicAdd(d.stats + 1, idle_rows);
         if (gw == 0) atomicAdd(d.stats + 2, batches);
     }
+    pdl_chain_end();
 }
 
 template <int G, int C>
@@ -340,8 +342,9 @@ static int launch_rp(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t st
         blocks = (d.n + groups - 1) / groups;
         if (blocks == 0) return G3X_OK;
     }
-    rowpar_kernel<G, C><<<blocks, threads, smem, stream>>>(d, sp);
-    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+    if (launch_class_kernel(rowpar_kernel<G, C>, blocks, threads, smem, stream, d, sp) != cudaSuccess)
+        return G3X_ERR_CUDA;
+    return G3X_OK;
 }
 
 // C is odd: lane r's columns start 2*C*r words apart in the 8-byte row-buffer slots, so the

@@ -26,6 +26,7 @@ namespace {
 constexpr int kLevels = kSchedLevels;  // key levels per bucket: 64 row-count x 32 width bins
 constexpr int kRowBins = 64, kWidthBins = 32;
 static_assert(kRowBins * kWidthBins == kLevels, "key layout");
+static_assert(kLevels % 1024 == 0 && kMaxBuckets * kLevels <= 16 * 1024, "scan: 1..16 bins per thread");
 
 // Job of sort position k: k itself, or subset[k] when sorting a subset of *subset_n jobs.
 __device__ __forceinline__ int job_at(int k, const int32_t* subset) { return subset ? subset[k] : k; }
@@ -70,31 +71,52 @@ __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScorePara
     if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(hist + bn, __popc(peers));
 }
 
-// Exclusive scan of the nb bins in one block; also each bucket's (offset, count).
-__global__ void scan_kernel(const int32_t* __restrict__ hist, int nb, int32_t* __restrict__ cursor,
-                            int32_t* __restrict__ bucket_oc, int nbuckets) {
-    __shared__ int32_t part[1024];
-    const int per = (nb + 1023) / 1024;
-    const int t = threadIdx.x;
+// Exclusive scan of the nb bins in one block; also each bucket's (offset, count).  nb is a
+// multiple of 1024 with at most 16 bins per thread (nb = classes x kLevels): each thread sums
+// its consecutive bins with independent loads, the warps scan their sums with shuffles and warp
+// 0 scans the 32 warp totals.
+__global__ void __launch_bounds__(1024) scan_kernel(const int32_t* __restrict__ hist, int nb,
+                                                    int32_t* __restrict__ cursor, int32_t* __restrict__ bucket_oc,
+                                                    int nbuckets) {
+    __shared__ int32_t wsum[32];
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int per = nb >> 10;
+    int v[16];
     int s = 0;
-    for (int k = t * per; k < (t + 1) * per && k < nb; ++k) s += hist[k];
-    part[t] = s;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        v[k] = k < per ? hist[t * per + k] : 0;
+        s += v[k];
+    }
+    int inc = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) wsum[wid] = inc;
     __syncthreads();
-    for (int d = 1; d < 1024; d <<= 1) {
-        const int v = t >= d ? part[t - d] : 0;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
+    if (wid == 0) {
+        int w = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xFFFFFFFFu, w, o);
+            if (lane >= o) w += u;
+        }
+        wsum[lane] = w;                       // inclusive over warps
     }
-    int run = t ? part[t - 1] : 0;
-    for (int k = t * per; k < (t + 1) * per && k < nb; ++k) {
-        cursor[k] = run;
-        run += hist[k];
-    }
+    __syncthreads();
+    int run = (wid ? wsum[wid - 1] : 0) + inc - s;
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        if (k < per) {
+            cursor[t * per + k] = run;
+            run += v[k];
+        }
     __syncthreads();
     if (t < nbuckets) {
         const int lo = cursor[t * kLevels];
-        const int hi = t + 1 < nbuckets ? cursor[(t + 1) * kLevels] : part[1023];
+        const int hi = t + 1 < nbuckets ? cursor[(t + 1) * kLevels] : wsum[31];
         bucket_oc[2 * t] = lo;
         bucket_oc[2 * t + 1] = hi - lo;
     }

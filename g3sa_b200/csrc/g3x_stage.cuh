@@ -233,4 +233,32 @@ __device__ bool stage_job(int job, const LaunchDesc& d, const ScoreParams& sp,
     return true;
 }
 
+// Programmatic dependent launch in the width-class kernels.  pdl_trigger, first thing in the
+// kernel, lets the class kernel queued after this one on the stream start at once (its blocks
+// take the SMs this kernel's blocks leave as they run out of jobs).  pdl_chain_end, last thing:
+// one thread of block 0 waits for the kernel this one was launched after (no wait without a
+// programmatic launch), so a kernel of the chain completes only after the kernels before it,
+// and the work queued after the last class sees every class's outputs.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_chain_end() {
+    if (blockIdx.x == 0 && threadIdx.x == 0) asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Occupancy counters of a lane-per-job warp: the lanes' busy and idle block steps summed over
+// the warp first, so a warp adds to each counter once (every lane adding its own share put
+// tens of thousands of same-address atomics at the end of each launch).
+__device__ __forceinline__ void add_warp_stats(unsigned long long* stats, unsigned long long busy,
+                                               unsigned long long idle, unsigned long long waves, int lane) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        busy += __shfl_xor_sync(0xFFFFFFFFu, busy, o);
+        idle += __shfl_xor_sync(0xFFFFFFFFu, idle, o);
+    }
+    if (lane == 0) {
+        atomicAdd(stats + 0, busy);
+        atomicAdd(stats + 1, idle);
+        atomicAdd(stats + 2, waves);
+    }
+}
+
 }  // namespace g3x

@@ -1,12 +1,17 @@
-// g3x_stream.cu -- chunked, double-buffered seed-level extension from host memory.
+// g3x_stream.cu -- chunked seed-level extension from host memory, several chunks in flight.
 //
 // Host seeds are processed in chunks.  For each chunk the library finds the range of plane
-// bases its seeds reference, copies the chunk's seeds (re-based to that range) and those
-// plane words to one of two device buffer sets on a copy stream, and runs the seed-level
-// pipeline of g3x_seeds.cu on a compute stream that waits for the copy.  While chunk k is
-// extended, chunk k+1 is copied into the other set.  Results come back through pinned
-// staging buffers.  The buffer sets, staging and streams live in the context and are grown
-// on demand, so repeated calls allocate nothing.
+// bases its seeds reference, copies the chunk's seeds and those plane words to the device on a
+// copy stream, re-bases the seeds' plane offsets to the copied range on the device, and runs the
+// seed-level pipeline of g3x_seeds.cu on a compute stream that waits for the copy.
+// kStreamLanes chunks run at a time, chunk c on lane c % kStreamLanes: each lane has its own
+// compute stream, buffer set, pinned staging, seed scratch and sort scratch, and chains its
+// width classes on its stream as programmatic dependent launches (side by side, without side
+// streams), so the latency-bound waves of one chunk (a wave's longest job runs alone at the
+// end) overlap the next chunks' waves.  The host work of a chunk (its range,
+// its staging copy) overlaps the device work of the chunks before it.  Results come back
+// through the lane's pinned staging.  All of it lives in the context and is grown on demand,
+// so repeated calls allocate nothing.
 #include <cuda_runtime.h>
 #include <string.h>
 #include <algorithm>
@@ -25,28 +30,67 @@ struct ChunkRange {
     int64_t bases;        // bases copied
 };
 
-void release(StreamSet& s) {
+// The chunk's seeds' plane offsets, made relative to the copied range.
+__global__ void rebase_kernel(g3x_seed_t* __restrict__ s, int n, uint32_t base) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        s[k].read_off -= base;
+        s[k].win_off -= base;
+    }
+}
+
+// The lane's buffers and staging (not its stream, events and queue counters).
+void release_buffers(StreamSet& s) {
     cudaFree(s.d_seeds); cudaFree(s.d_codes); cudaFree(s.d_nmask); cudaFree(s.d_regs);
     cudaFree(s.d_status);
     cudaFreeHost(s.h_seeds); cudaFreeHost(s.h_regs); cudaFreeHost(s.h_status);
+    s.d_seeds = nullptr; s.d_codes = nullptr; s.d_nmask = nullptr; s.d_regs = nullptr;
+    s.d_status = nullptr; s.h_seeds = nullptr; s.h_regs = nullptr; s.h_status = nullptr;
+}
+
+void release_lane(StreamSet& s) {
+    release_buffers(s);
+    free_seed_scratch(s.seeds);
+    free_sched(s.sched);
+    cudaFree(s.queue);
     if (s.h2d) cudaEventDestroy(s.h2d);
     if (s.done) cudaEventDestroy(s.done);
+    if (s.comp) cudaStreamDestroy(s.comp);
     s = StreamSet();
 }
 
-// Buffer sets for chunks of `chunk` seeds and the given plane words, kept when large enough.
-int grow_stream(StreamScratch& ss, int64_t chunk, int64_t code_words, int64_t mask_words) {
-    if (!ss.copy_st && (cudaStreamCreateWithFlags(&ss.copy_st, cudaStreamNonBlocking) != cudaSuccess ||
-                        cudaStreamCreateWithFlags(&ss.comp_st, cudaStreamNonBlocking) != cudaSuccess))
+// Streams, events and queue counters of the lanes, made once per context.
+int make_lanes(StreamScratch& ss) {
+    if (ss.lanes_ready) return G3X_OK;
+    bool ok = cudaStreamCreateWithFlags(&ss.copy_st, cudaStreamNonBlocking) == cudaSuccess;
+    for (int l = 0; l < kStreamLanes && ok; ++l) {
+        StreamSet& s = ss.set[l];
+        ok = cudaStreamCreateWithFlags(&s.comp, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&s.h2d, cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) == cudaSuccess &&
+             cudaMalloc(&s.queue, kMaxBuckets * sizeof(int32_t)) == cudaSuccess;
+    }
+    if (!ok) {
+        free_stream_scratch(ss);
         return G3X_ERR_CUDA;
+    }
+    ss.lanes_ready = true;
+    return G3X_OK;
+}
+
+// Buffer sets for chunks of `chunk` seeds and the given plane words, kept when large enough.
+// The lanes must be idle.
+int grow_stream(StreamScratch& ss, int64_t chunk, int64_t code_words, int64_t mask_words) {
+    int rc = make_lanes(ss);
+    if (rc) return rc;
     if (chunk <= ss.seeds && code_words <= ss.code_words && mask_words <= ss.mask_words) return G3X_OK;
     chunk = std::max(chunk, ss.seeds);
     code_words = std::max(code_words, ss.code_words);
     mask_words = std::max(mask_words, ss.mask_words);
     bool ok = true;
-    for (int b = 0; b < 2 && ok; ++b) {
-        StreamSet& s = ss.set[b];
-        release(s);
+    for (int l = 0; l < kStreamLanes && ok; ++l) {
+        StreamSet& s = ss.set[l];
+        release_buffers(s);
         ok = cudaMalloc(&s.d_seeds, chunk * sizeof(g3x_seed_t)) == cudaSuccess &&
              cudaMalloc(&s.d_codes, code_words * sizeof(uint32_t)) == cudaSuccess &&
              cudaMalloc(&s.d_nmask, mask_words * sizeof(uint32_t)) == cudaSuccess &&
@@ -55,11 +99,10 @@ int grow_stream(StreamScratch& ss, int64_t chunk, int64_t code_words, int64_t ma
              cudaMallocHost(&s.h_seeds, chunk * sizeof(g3x_seed_t)) == cudaSuccess &&
              cudaMallocHost(&s.h_regs, chunk * sizeof(g3x_reg_t)) == cudaSuccess &&
              cudaMallocHost(&s.h_status, chunk * sizeof(int32_t)) == cudaSuccess &&
-             cudaEventCreateWithFlags(&s.h2d, cudaEventDisableTiming) == cudaSuccess &&
-             cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) == cudaSuccess;
+             alloc_seed_scratch(s.seeds, chunk) == G3X_OK && alloc_sched(s.sched, chunk) == G3X_OK;
     }
     if (!ok) {
-        for (int b = 0; b < 2; ++b) release(ss.set[b]);
+        for (int l = 0; l < kStreamLanes; ++l) release_buffers(ss.set[l]);
         ss.seeds = ss.code_words = ss.mask_words = 0;
         return G3X_ERR_NOMEM;
     }
@@ -67,94 +110,109 @@ int grow_stream(StreamScratch& ss, int64_t chunk, int64_t code_words, int64_t ma
     return G3X_OK;
 }
 
+// Range of plane bases chunk [first, first + count) reads; G3X_ERR_INVALID when a seed reaches
+// past the planes.
+int chunk_range(const g3x_seed_t* h_seeds, int64_t first, int64_t count, int64_t n_bases, ChunkRange& R) {
+    R.first = first;
+    R.count = count;
+    int64_t lo = INT64_MAX, hi = 0;
+    for (int64_t k = first; k < first + count; ++k) {
+        const g3x_seed_t& s = h_seeds[k];
+        lo = std::min<int64_t>(lo, std::min<int64_t>(s.read_off, s.win_off));
+        hi = std::max<int64_t>(hi, std::max<int64_t>((int64_t)s.read_off + s.l_query,
+                                                     (int64_t)s.win_off + (s.rmax1 - s.rmax0)));
+    }
+    if (hi > n_bases) return G3X_ERR_INVALID;
+    R.base = (uint32_t)(lo & ~(int64_t)31);
+    R.bases = hi - R.base;
+    return G3X_OK;
+}
+
 }  // namespace
 
-int extend_seeds_stream(StreamScratch& ss, SeedScratch& ws, int (*grow)(SeedScratch&, int64_t),
-                        const g3x_opt_t& opt, const ScoreParams& sp, const g3x_seed_t* h_seeds, int64_t n,
-                        const uint32_t* h_codes, const uint32_t* h_nmask, int64_t n_bases,
-                        g3x_reg_t* h_regs, int32_t* h_status, int32_t chunk,
-                        const LaunchDesc& proto, const WaveRunner* runner) {
+int extend_seeds_stream(StreamScratch& ss, const g3x_opt_t& opt, const ScoreParams& sp,
+                        const g3x_seed_t* h_seeds, int64_t n, const uint32_t* h_codes,
+                        const uint32_t* h_nmask, int64_t n_bases, g3x_reg_t* h_regs, int32_t* h_status,
+                        int32_t chunk, const LaunchDesc& proto, const WaveRunner* runner) {
     if (chunk <= 0) chunk = 65536;
     const int64_t nchunks = (n + chunk - 1) / chunk;
-    std::vector<ChunkRange> ranges((size_t)nchunks);
-    int64_t max_bases = 0;
-    for (int64_t c = 0; c < nchunks; ++c) {
-        ChunkRange& R = ranges[(size_t)c];
-        R.first = c * chunk;
-        R.count = std::min<int64_t>(chunk, n - R.first);
-        int64_t lo = INT64_MAX, hi = 0;
-        for (int64_t k = R.first; k < R.first + R.count; ++k) {
-            const g3x_seed_t& s = h_seeds[k];
-            lo = std::min<int64_t>(lo, std::min<int64_t>(s.read_off, s.win_off));
-            hi = std::max<int64_t>(hi, std::max<int64_t>((int64_t)s.read_off + s.l_query,
-                                                         (int64_t)s.win_off + (s.rmax1 - s.rmax0)));
-        }
-        if (hi > n_bases) return G3X_ERR_INVALID;
-        R.base = (uint32_t)(lo & ~(int64_t)31);
-        R.bases = hi - R.base;
-        max_bases = std::max(max_bases, R.bases);
-    }
-    int rc = grow(ws, chunk);
+    int rc = grow_stream(ss, chunk, 1, 1);     // plane words grow with the first chunk's range
     if (rc) return rc;
-    if ((rc = grow_stream(ss, chunk, (max_bases + 15) / 16 + 2, (max_bases + 31) / 32 + 2))) return rc;
-    StreamSet* sets = ss.set;
-    cudaStream_t copy_st = ss.copy_st, comp_st = ss.comp_st;
-    for (int b = 0; b < 2; ++b) sets[b].pending = -1;
+    // each lane's class waves run on the lane's own sort scratch and queue counters, the classes
+    // chained on the lane's stream
+    ClassRes res[kStreamLanes];
+    ClassWave cw[kStreamLanes];
+    WaveRunner wr[kStreamLanes];
+    const ClassWave* cw0 = runner ? static_cast<const ClassWave*>(runner->user) : nullptr;
+    std::vector<ChunkRange> pend(kStreamLanes);
+    for (int l = 0; l < kStreamLanes; ++l) {
+        StreamSet& s = ss.set[l];
+        s.pending = -1;
+        if (!runner) continue;
+        res[l] = ClassRes{&s.sched, s.queue, nullptr, nullptr, nullptr, nullptr};
+        cw[l] = ClassWave{cw0->ctx, cw0->learned, &res[l]};
+        wr[l] = WaveRunner{runner->run, &cw[l]};
+    }
     const int64_t total_code_words = (n_bases + 15) / 16, total_mask_words = (n_bases + 31) / 32;
-    auto drain = [&](StreamSet& s) -> int {
+    auto drain = [&](int l) -> int {
+        StreamSet& s = ss.set[l];
         if (s.pending < 0) return G3X_OK;
         if (cudaEventSynchronize(s.done) != cudaSuccess) return G3X_ERR_CUDA;
-        const ChunkRange& R = ranges[(size_t)s.pending];
+        const ChunkRange& R = pend[(size_t)l];
         memcpy(h_regs + R.first, s.h_regs, R.count * sizeof(g3x_reg_t));
         memcpy(h_status + R.first, s.h_status, R.count * sizeof(int32_t));
         s.pending = -1;
         return G3X_OK;
     };
     for (int64_t c = 0; c < nchunks && rc == G3X_OK; ++c) {
-        StreamSet& s = sets[c & 1];
-        const ChunkRange& R = ranges[(size_t)c];
-        if ((rc = drain(s))) break;                      // set free: its last chunk is done
-        for (int64_t k = 0; k < R.count; ++k) {
-            g3x_seed_t t = h_seeds[R.first + k];
-            t.read_off -= R.base;
-            t.win_off -= R.base;
-            s.h_seeds[k] = t;
+        const int l = (int)(c % kStreamLanes);
+        StreamSet& s = ss.set[l];
+        ChunkRange R;
+        if ((rc = chunk_range(h_seeds, c * chunk, std::min<int64_t>(chunk, n - c * chunk), n_bases, R))) break;
+        const int64_t cw0w = R.base / 16, mw0 = R.base / 32;
+        const int64_t cwn = std::min<int64_t>((R.bases + 15) / 16 + 1, total_code_words - cw0w);
+        const int64_t mwn = std::min<int64_t>((R.bases + 31) / 32 + 1, total_mask_words - mw0);
+        if (cwn > ss.code_words || mwn > ss.mask_words) {
+            // a wider range than the sets hold: let every lane finish, then grow them
+            for (int k = 0; k < kStreamLanes && rc == G3X_OK; ++k) rc = drain(k);
+            if (rc || (rc = grow_stream(ss, chunk, cwn + cwn / 4, mwn + mwn / 4))) break;
         }
-        const int64_t cw0 = R.base / 16, mw0 = R.base / 32;
-        const int64_t cw = std::min<int64_t>((R.bases + 15) / 16 + 1, total_code_words - cw0);
-        const int64_t mw = std::min<int64_t>((R.bases + 31) / 32 + 1, total_mask_words - mw0);
-        if (cudaMemcpyAsync(s.d_seeds, s.h_seeds, R.count * sizeof(g3x_seed_t), cudaMemcpyHostToDevice, copy_st) ||
-            cudaMemcpyAsync(s.d_codes, h_codes + cw0, cw * sizeof(uint32_t), cudaMemcpyHostToDevice, copy_st) ||
-            cudaMemcpyAsync(s.d_nmask, h_nmask + mw0, mw * sizeof(uint32_t), cudaMemcpyHostToDevice, copy_st) ||
-            cudaEventRecord(s.h2d, copy_st) || cudaStreamWaitEvent(comp_st, s.h2d, 0)) {
+        if ((rc = drain(l))) break;                      // lane free: its last chunk is done
+        memcpy(s.h_seeds, h_seeds + R.first, R.count * sizeof(g3x_seed_t));
+        if (cudaMemcpyAsync(s.d_seeds, s.h_seeds, R.count * sizeof(g3x_seed_t), cudaMemcpyHostToDevice,
+                            ss.copy_st) ||
+            cudaMemcpyAsync(s.d_codes, h_codes + cw0w, cwn * sizeof(uint32_t), cudaMemcpyHostToDevice, ss.copy_st) ||
+            cudaMemcpyAsync(s.d_nmask, h_nmask + mw0, mwn * sizeof(uint32_t), cudaMemcpyHostToDevice, ss.copy_st) ||
+            cudaEventRecord(s.h2d, ss.copy_st) || cudaStreamWaitEvent(s.comp, s.h2d, 0)) {
             rc = G3X_ERR_CUDA;
             break;
         }
+        rebase_kernel<<<(unsigned)((R.count + 255) / 256), 256, 0, s.comp>>>(s.d_seeds, (int)R.count, R.base);
         LaunchDesc cp = proto;                 // the chunk's planes: its copied words, re-based
-        cp.n_bases = std::min<int64_t>(cw * 16, mw * 32);
-        if ((rc = extend_seeds(ws, opt, sp, s.d_seeds, (int)R.count, s.d_codes, s.d_nmask, s.d_regs,
-                               s.d_status, cp, comp_st, runner)))
+        cp.n_bases = std::min<int64_t>(cwn * 16, mwn * 32);
+        if ((rc = extend_seeds(s.seeds, opt, sp, s.d_seeds, (int)R.count, s.d_codes, s.d_nmask, s.d_regs,
+                               s.d_status, cp, s.comp, runner ? &wr[l] : nullptr)))
             break;
-        if (cudaMemcpyAsync(s.h_regs, s.d_regs, R.count * sizeof(g3x_reg_t), cudaMemcpyDeviceToHost, comp_st) ||
-            cudaMemcpyAsync(s.h_status, s.d_status, R.count * sizeof(int32_t), cudaMemcpyDeviceToHost, comp_st) ||
-            cudaEventRecord(s.done, comp_st)) {
+        if (cudaMemcpyAsync(s.h_regs, s.d_regs, R.count * sizeof(g3x_reg_t), cudaMemcpyDeviceToHost, s.comp) ||
+            cudaMemcpyAsync(s.h_status, s.d_status, R.count * sizeof(int32_t), cudaMemcpyDeviceToHost, s.comp) ||
+            cudaEventRecord(s.done, s.comp)) {
             rc = G3X_ERR_CUDA;
             break;
         }
+        pend[(size_t)l] = R;
         s.pending = c;
     }
-    for (int b = 0; b < 2; ++b) {
-        int r2 = drain(sets[b]);
+    for (int l = 0; l < kStreamLanes; ++l) {
+        int r2 = drain(l);
         if (rc == G3X_OK) rc = r2;
     }
-    cudaStreamSynchronize(comp_st);
-    cudaStreamSynchronize(copy_st);
+    for (int l = 0; l < kStreamLanes; ++l) cudaStreamSynchronize(ss.set[l].comp);
+    cudaStreamSynchronize(ss.copy_st);
     return rc;
 }
 
 void free_stream_scratch(StreamScratch& ss) {
-    for (int b = 0; b < 2; ++b) release(ss.set[b]);
-    if (ss.comp_st) cudaStreamDestroy(ss.comp_st);
+    for (int l = 0; l < kStreamLanes; ++l) release_lane(ss.set[l]);
     if (ss.copy_st) cudaStreamDestroy(ss.copy_st);
     ss = StreamScratch();
 }

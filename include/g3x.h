@@ -173,6 +173,10 @@ typedef struct {
     int32_t refill;       /* lane kernel: idle lanes that trigger a refill wave (1-32) */
 } g3x_tile_t;
 
+/* A new context's classes: the int16x2 lane kernel (lanes 1, tile 2, refill 8) for queries up to
+   32, 56, 88, 128, 168, 200 and 256 bases, then 32-lane row-parallel groups (tile 9) for longer
+   queries and jobs outside the int16 fit.  g3x_autotune replaces them with classes fitted to a
+   batch. */
 int g3x_get_tiles(g3x_ctx *ctx, g3x_tile_t *h_tiles, int32_t *n);
 int g3x_set_tiles(g3x_ctx *ctx, const g3x_tile_t *h_tiles, int32_t n);
 /* Fits the width classes to the given jobs (device buffers) and tunes them: the class widths
@@ -250,11 +254,14 @@ int g3x_extend_seeds(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t *d_see
                      int32_t *d_status, const g3x_batch_opts_t *opts, void *stream);
 
 /* The same over n host seeds in chunks of `chunk` seeds: each chunk's seeds and the plane
-   words they reference are copied to the GPU while the previous chunk is extended (two
-   device buffer sets, a copy stream and a compute stream), and the regions come back to
-   h_regs/h_status.  Host buffers should be pinned for the copies to overlap.  Blocks until
-   all chunks are done.  The buffer sets, pinned staging and streams stay in the context,
-   grown when a call needs more, so repeated calls allocate nothing. */
+   words they reference are copied to the GPU while the chunks before it are extended (four
+   chunks in flight, each with its own device buffer set, pinned staging and compute stream,
+   beside one copy stream), and the regions come back to h_regs/h_status.  Host planes should
+   be pinned for the copies to overlap.  Blocks until all chunks are done.  A chunk with a
+   seed that reaches past n_bases ends the call with G3X_ERR_INVALID before anything of that
+   chunk is copied (the chunks before it have their results written).  The buffer sets,
+   staging and streams stay in the context, grown when a call needs more, so repeated calls
+   allocate nothing. */
 int g3x_extend_seeds_stream(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t *h_seeds,
                             int64_t n, const uint32_t *h_codes, const uint32_t *h_nmask,
                             int64_t n_bases, g3x_reg_t *h_regs, int32_t *h_status,

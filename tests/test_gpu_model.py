@@ -98,8 +98,10 @@ def test_warp_batched_classes_are_exact():
     sc = g.default_score()
     c = ctx()
     tiles = c.get_tiles()
+    rowpar = [(20, 4, 5, 0, 1), (36, 4, 9, 0, 1), (72, 8, 9, 0, 1), (144, 16, 9, 0, 1), (288, 32, 9, 0, 1),
+              (2147483647, 32, 9, 0, 1)]
     try:
-        c.set_tiles([(w, l, t, 1, r) for (w, l, t, _, r) in tiles])
+        c.set_tiles([(w, l, t, 1, r) for (w, l, t, _, r) in rowpar])
         ref, _, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
         out, status, _ = run_batch(wl.u8, wl.jobs, sc, g.SCHED_SORTED)
         assert (status == 0).all() and (out == ref).all()
