@@ -173,12 +173,16 @@ int class_qcap(const TileTable& t, int k, int qmax) {
     return k == t.n - 1 ? qmax : std::min(qmax, t.width[k]);
 }
 
-// Runs the persistent row-parallel kernel over every width class of an ordered batch: one
-// launch per class on its own stream, forked from and joined back into `st`.
+// The context's class resources.  The classes chain on the caller's stream as programmatic
+// dependent launches; only the per-class timing modes fork them onto the side streams (events
+// between chained launches would serialise them).
 static ClassRes ctx_res(g3x_ctx* ctx) {
-    return ClassRes{&ctx->sched, ctx->d_queue, ctx->side, ctx->fork, ctx->join, ctx->d_stats};
+    return ClassRes{&ctx->sched, ctx->d_queue, ctx->timing ? ctx->side : nullptr, ctx->fork, ctx->join,
+                    ctx->d_stats};
 }
 
+// Runs the persistent kernels over every width class of an ordered batch: one launch per class,
+// chained on `st` (or forked onto side streams from `st` and joined back).
 static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParams& sp, cudaStream_t st,
                           int only = -1, const TileTable* tt_override = nullptr, const ClassRes* res_in = nullptr) {
     const TileTable& tt = tt_override ? *tt_override : ctx->tiles;
