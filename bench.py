@@ -1034,6 +1034,7 @@ def main():
     d_out = torch.zeros((n, 6), dtype=torch.int32, device=dev)
     d_status = torch.zeros(n, dtype=torch.int32, device=dev)
     d_cells = torch.zeros(n, dtype=torch.int32, device=dev)
+    d_rows = torch.zeros(n, dtype=torch.int32, device=dev)
     h_out = torch.zeros((n, 6), dtype=torch.int32).pin_memory()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
     stream = torch.cuda.current_stream(dev)
@@ -1043,7 +1044,7 @@ def main():
                          schedule=schedule, stream=stream, **kw)
 
     # Useful cells of this batch: the kernels' own trip-count counters (plain kernel).
-    batch(g.SCHED_PLAIN, d_cells=d_cells)
+    batch(g.SCHED_PLAIN, d_cells=d_cells, d_rows=d_rows)
     torch.cuda.synchronize()
     if (d_status != 0).any():
         raise SystemExit("per-job status errors in the plain run")
@@ -1055,7 +1056,7 @@ def main():
     # same generator (another seed), about 2M jobs.
     train_metrics = learn.train(ctx, n_train=TRAIN_UNITS[args.workload],
                                 seed_train=0xA11CE + rank, kind=kind_, w=w, unrelated=unrel)
-    pred_err = learn.prediction_error(ctx, d_jobs, n, d_codes, d_nmask, cells_np)
+    pred_err = learn.prediction_error(ctx, wl.jobs, d_jobs, n, d_codes, d_nmask, d_rows.cpu().numpy())
 
     # Autotune the width classes on this batch for each schedule's own job order, and capture
     # each schedule's graph with its own tiles (a graph keeps the launch configuration it was

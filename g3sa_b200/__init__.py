@@ -55,7 +55,7 @@ REG_DT = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), (
                    ("pad_", "u1", 2)])
 BATCH_OPTS_DT = np.dtype([("schedule", "<i4"), ("max_qlen", "<i4"), ("max_tlen", "<i4"),
                           ("lanes", "<i4"), ("tile", "<i4"), ("kernel", "<i4"), ("d_cells", "<u8"),
-                          ("n_bases", "<i8")])
+                          ("n_bases", "<i8"), ("d_rows", "<u8")])
 KERNEL_AUTO, KERNEL_ROLLING, KERNEL_ROWPAR, KERNEL_LANE, KERNEL_LANE16, KERNEL_LANE2 = 0, 1, 2, 3, 4, 5
 TILE_DT = np.dtype([("width", "<i4"), ("lanes", "<i4"), ("tile", "<i4"), ("warp_batch", "<i4"),
                     ("refill", "<i4")])
@@ -295,7 +295,7 @@ class Context:
 
     def capture_batch(self, score, d_jobs, n, d_codes, d_nmask, d_out, d_status, max_qlen,
                       max_tlen, schedule=SCHED_SORTED, lanes=0, d_cells=None, tile=0,
-                      kernel=KERNEL_AUTO, n_bases=None):
+                      kernel=KERNEL_AUTO, n_bases=None, d_rows=None):
         """g3x_graph_capture of one batch; returns a Graph whose launch() replays it."""
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
@@ -303,6 +303,7 @@ class Context:
         opts["tile"], opts["kernel"] = tile, kernel
         opts["d_cells"] = _ptr(d_cells) if d_cells is not None else 0
         opts["n_bases"] = plane_bases(d_codes, d_nmask, n_bases)
+        opts["d_rows"] = _ptr(d_rows) if d_rows is not None else 0
         h = ctypes.c_void_p()
         _check(lib().g3x_graph_capture(self._h, score.ctypes.data, _ptr(d_jobs), int(n), _ptr(d_codes),
                                        _ptr(d_nmask), _ptr(d_out), _ptr(d_status), opts.ctypes.data,
@@ -397,7 +398,7 @@ class Context:
 
     def extend_batch(self, score, d_jobs, n, d_codes, d_nmask, d_out, d_status, max_qlen,
                      max_tlen, schedule=SCHED_PLAIN, lanes=0, d_cells=None, stream=None,
-                     tile=0, kernel=KERNEL_AUTO, n_bases=None):
+                     tile=0, kernel=KERNEL_AUTO, n_bases=None, d_rows=None):
         """g3x_ksw_extend2_batch on torch device tensors (or raw device pointers)."""
         opts = np.zeros(1, BATCH_OPTS_DT)
         opts["schedule"], opts["max_qlen"], opts["max_tlen"], opts["lanes"] = (
@@ -405,6 +406,7 @@ class Context:
         opts["tile"], opts["kernel"] = tile, kernel
         opts["d_cells"] = _ptr(d_cells) if d_cells is not None else 0
         opts["n_bases"] = plane_bases(d_codes, d_nmask, n_bases)
+        opts["d_rows"] = _ptr(d_rows) if d_rows is not None else 0
         rc = lib().g3x_ksw_extend2_batch(self._h, score.ctypes.data, _ptr(d_jobs), int(n),
                                          _ptr(d_codes), _ptr(d_nmask), _ptr(d_out),
                                          _ptr(d_status), opts.ctypes.data, _stream(stream))

@@ -77,6 +77,7 @@ int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d) {
     d->qmax = opts->max_qlen;
     d->tmax = opts->max_tlen;
     d->cells = opts->d_cells;
+    d->rows = opts->d_rows;
     if (opts->schedule != G3X_SCHED_PLAIN && opts->schedule != G3X_SCHED_SORTED &&
         opts->schedule != G3X_SCHED_LEARNED)
         return G3X_ERR_INVALID;

@@ -312,6 +312,7 @@ extern "C" int g3x_chain2aln(g3x_ctx* ctx, const g3x_opt_t* opt, const g3x_refin
         xo.max_qlen = std::max<int32_t>(w.h_maxlen[0], 1);
         xo.max_tlen = std::max<int32_t>(w.h_maxlen[1], 1);
         xo.d_cells = nullptr;
+        xo.d_rows = nullptr;
         if ((rc = g3x_extend_seeds(ctx, opt, w.xseeds, n_seeds, d_codes, d_nmask, w.xregs, w.xstatus, &xo,
                                    stream)))
             return rc;

@@ -26,6 +26,7 @@ struct LaunchDesc {
     g3x_ext_t* out;
     int32_t* status;
     int32_t* cells;        // optional
+    int32_t* rows;         // optional: rows of the row loop each job ran
     const int32_t* order;  // optional permutation: queue slot -> job index
     const int32_t* count;  // optional device-side job count (overrides n when set)
     int32_t* queue;        // persistent kernels: device counter (zeroed by the caller)

@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(256) extend_kernel(LaunchDesc d, ScoreParams s
                     d.out[gj.job] = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};
                     d.status[gj.job] = err;
                     if (d.cells) d.cells[gj.job] = (int32_t)K.cells;
+                    if (d.rows) d.rows[gj.job] = K.next;
                 }
                 gj.job = -1;
             }

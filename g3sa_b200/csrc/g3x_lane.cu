@@ -287,10 +287,12 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
                         d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
                         d.status[job] = G3X_ERR_TOO_LONG;
                         if (d.cells) d.cells[job] = 0;
+                        if (d.rows) d.rows[job] = 0;
                     } else if (!job_in_planes(jb, d.n_bases)) {   // reaches past the planes: unread
                         d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
                         d.status[job] = G3X_ERR_INVALID;
                         if (d.cells) d.cells[job] = 0;
+                        if (d.rows) d.rows[job] = 0;
                     } else {
                         my_job = job;
                         J.job = job;
@@ -460,6 +462,7 @@ __global__ void __launch_bounds__(128) lane_kernel(LaunchDesc d, ScoreParams sp)
             d.out[J.job] = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};
             d.status[J.job] = G3X_OK;
             if (d.cells) d.cells[J.job] = (int32_t)K.cells;
+            if (d.rows) d.rows[J.job] = K.next;
             J.job = -1;
         }
         __syncwarp();

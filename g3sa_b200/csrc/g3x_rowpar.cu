@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(128) rowpar_kernel(LaunchDesc d, ScoreParams s
                     d.out[J.job] = g3x_ext_t{K.best, K.best_j + 1, K.best_i + 1, K.max_ie + 1, K.gscore, K.max_off};
                     d.status[J.job] = J.err;
                     if (d.cells) d.cells[J.job] = (int32_t)K.cells;
+                    if (d.rows) d.rows[J.job] = K.next;
                 }
                 J.job = -1;
             }

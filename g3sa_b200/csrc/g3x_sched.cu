@@ -6,8 +6,10 @@
 //              min(qlen, 2w' + 1), w' the clamped band of ksw.cu:321-329); one persistent
 //              launch per class;
 //   a key    : the job's row count, then its widest row.  The row count is the length-sorted
-//              fallback's bound tlen, or, learned, the cost model's prediction of
-//              log2(1 + cells) less log2(widest row); the widest row is min(qlen, 2w' + 1).
+//              fallback's bound tlen, or, learned, that bound corrected by the cost model: the
+//              model predicts log2(1 + rows) less log2(1 + tlen), at most 0 (a job runs at most
+//              tlen rows), and the key's log2 row count is log2(1 + tlen) plus
+//              min(0, correction + 1); the widest row is min(qlen, 2w' + 1).
 //              A warp of a row-synchronous kernel takes consecutive jobs, so jobs of similar
 //              row count and similar row width run together, longest first.
 // A device counting sort over (bucket, key) bins -- histogram, exclusive scan, scatter --
@@ -25,6 +27,7 @@ namespace {
 
 constexpr int kLevels = kSchedLevels;  // key levels per bucket: 64 row-count x 32 width bins
 constexpr int kRowBins = 64, kWidthBins = 32;
+constexpr float kLearnedSlack = 1.0f;   // log2 rows the learned correction must exceed
 static_assert(kRowBins * kWidthBins == kLevels, "key layout");
 static_assert(kLevels % 1024 == 0 && kMaxBuckets * kLevels <= 16 * 1024, "scan: 1..16 bins per thread");
 
@@ -58,7 +61,14 @@ __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScorePara
         if (!fits) b = tt.n - 1;
     }
     // log2 of the row count, 0..16; four bins per doubling, more rows -> earlier bin
-    float lr = pred ? pred[job] - log2f((float)(wide > 1 ? wide : 1)) : log2f(1.0f + (float)jb.tlen);
+    // The learned correction is soft-thresholded by one halving: min(0, pred + 1).  A job moves
+    // ahead of the length order only where the network predicts that it ends before half its
+    // rows (a z-drop on an unrelated target), and by how much further; its error on jobs that
+    // run to their end (a few tenths of a halving, now and then one) leaves them in length order,
+    // which is already near the true order for them.  Continuous, so jobs of equal predicted rows
+    // stay together.
+    float lr = log2f(1.0f + (float)jb.tlen);
+    if (pred) lr += fminf(pred[job] + kLearnedSlack, 0.0f);
     int rb = (int)((16.0f - lr) * (kRowBins / 16.0f));
     rb = rb < 0 ? 0 : (rb >= kRowBins ? kRowBins - 1 : rb);
     // eight-column blocks of the widest row, wider -> earlier bin

@@ -173,7 +173,7 @@ int extend_seeds(const SeedScratch& ws, const g3x_opt_t& opt, const ScoreParams&
                     int32_t* queue) -> int {
         LaunchDesc d = proto;
         d.jobs = jobs; d.codes = codes; d.nmask = nmask; d.out = ext; d.status = jst;
-        d.cells = nullptr; d.order = order; d.count = count; d.queue = queue; d.n = n;
+        d.cells = nullptr; d.rows = nullptr; d.order = order; d.count = count; d.queue = queue; d.n = n;
         return runner ? runner->run(runner->user, d, sp, st) : launch_extend(d, sp, st);
     };
     int rc;

@@ -189,6 +189,7 @@ __device__ bool stage_job(int job, const LaunchDesc& d, const ScoreParams& sp,
             d.out[job] = g3x_ext_t{0, 0, 0, 0, 0, 0};
             d.status[job] = bad_h0 || outside ? G3X_ERR_INVALID : G3X_ERR_TOO_LONG;
             if (d.cells) d.cells[job] = 0;
+            if (d.rows) d.rows[job] = 0;
         }
         return false;
     }

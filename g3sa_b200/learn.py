@@ -1,10 +1,17 @@
 """Training workflow of the learned cost model (host orchestration over the C ABI).
 
 Traces come from the method itself: a held-out synthetic batch of the workload to be scheduled
-(same generator kind, another seed) is extended by the plain kernel, whose per-job cell counters are the targets
-(log2(1 + cells)); the features come from the library's feature kernel; the 5 -> 64 -> 64 -> 1
-MLP is trained on the GPU by the library's own forward/backward/Adam kernels
-(g3x_mlp_train).  Everything runs on the device; only the loss curve comes back.
+(same generator kind, another seed) is extended by the plain kernel, whose per-job row counters
+give the targets; the features come from the library's feature kernel; the 5 -> 64 -> 64 -> 1
+MLP is trained on the GPU by the library's own forward/backward/Adam kernels (g3x_mlp_train).
+
+The target is a correction to the length-sorted schedule's row bound: log2(1 + rows) less
+log2(1 + tlen), rows the trips of the row loop of ksw.cu:346 (the z-drop or an empty band ends
+it early).  A job that runs to its last row has a correction of exactly 0, whatever its length,
+so the network only learns where the z-drop ends a job early (a behaviour that looks the same at
+every length), and the scheduler, which adds min(0, prediction + 1) back onto log2(1 + tlen),
+keeps the length order wherever the network sees no end before half the rows.  Rows, not cells,
+because a row-synchronous warp runs as many steps as its longest job has rows.
 """
 import time
 
@@ -18,9 +25,18 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).cuda()
 
 
+def row_target(rows, tlen):
+    """The model's target: log2(1 + rows) - log2(1 + tlen) (numpy or torch, float32), <= 0."""
+    if hasattr(rows, "to"):
+        import torch
+        return torch.log2(1.0 + rows.to(torch.float32)) - torch.log2(1.0 + tlen.to(torch.float32))
+    return (np.log2(1.0 + rows.astype(np.float64)) - np.log2(1.0 + tlen.astype(np.float64))).astype(np.float32)
+
+
 def traces(ctx, n, seed, kind=1, w=100, unrelated=0.2, score=None):
     """(features [m,5] device, targets [m] device, cells numpy) from the m jobs the generator
-    `kind` makes for n units (jobs for kind 1, seeds for kind 2, segments for kind 4)."""
+    `kind` makes for n units (jobs for kind 1, seeds for kind 2, segments for kind 4); the
+    targets are row_target of the plain kernel's row counts."""
     import torch
     score = g.default_score() if score is None else score
     wl = g.synth(kind, n, seed=seed, w=w, unrelated=unrelated)
@@ -29,12 +45,14 @@ def traces(ctx, n, seed, kind=1, w=100, unrelated=0.2, score=None):
     out = torch.zeros((wl.n, 6), dtype=torch.int32, device="cuda")
     status = torch.zeros(wl.n, dtype=torch.int32, device="cuda")
     cells = torch.zeros(wl.n, dtype=torch.int32, device="cuda")
+    rows = torch.zeros(wl.n, dtype=torch.int32, device="cuda")
     ctx.extend_batch(score, d_jobs, wl.n, d_codes, d_nmask, out, status,
                      int(wl.jobs["qlen"].max()), int(wl.jobs["tlen"].max()),
-                     schedule=g.SCHED_PLAIN, d_cells=cells)
+                     schedule=g.SCHED_PLAIN, d_cells=cells, d_rows=rows)
     feat = torch.zeros((wl.n, g.MLP_FEATURES), dtype=torch.float32, device="cuda")
     ctx.features(d_jobs, wl.n, d_codes, d_nmask, feat)
-    target = torch.log2(1.0 + cells.to(torch.float32))
+    tlen = torch.from_numpy(wl.jobs["tlen"].astype(np.int32)).cuda()
+    target = row_target(rows, tlen)
     torch.cuda.synchronize()
     if (status != 0).any():
         raise RuntimeError("trace run reported job errors")
@@ -65,20 +83,24 @@ def train(ctx, n_train=2_000_000, seed_train=0xA11CE, epochs=5, batch=4096, lr=2
             "loss_curve": [round(x, 5) for x in losses], "params": g.MLP_PARAMS}
 
 
-def prediction_error(ctx, d_jobs, n, d_codes, d_nmask, cells):
-    """Per-job cell-count prediction error of the trained model on a batch whose measured
-    cells are `cells` (numpy): median / mean absolute relative error and log2 MAE."""
+def prediction_error(ctx, jobs, d_jobs, n, d_codes, d_nmask, rows):
+    """Per-job row-count prediction error of the trained model on a batch (host jobs `jobs`,
+    device copy d_jobs) whose measured row counts are `rows` (numpy): log2(1 + tlen) plus the
+    model's correction is its log2(1 + rows) estimate; median / mean absolute relative error
+    (the mean with each job's error capped at 10), log2 MAE and the log2 correlation."""
     import torch
     feat = torch.zeros((n, g.MLP_FEATURES), dtype=torch.float32, device="cuda")
     pred = torch.zeros(n, dtype=torch.float32, device="cuda")
     ctx.features(d_jobs, n, d_codes, d_nmask, feat)
     ctx.mlp_predict(feat, n, pred)
     torch.cuda.synchronize()
-    p = pred.cpu().numpy().astype(np.float64)
-    c = cells.astype(np.float64)
+    c = pred.cpu().numpy().astype(np.float64)
+    p = c + np.log2(1.0 + jobs["tlen"].astype(np.float64))
+    r = rows.astype(np.float64)
     est = np.exp2(p) - 1.0
-    rel = np.abs(est - c) / np.maximum(c, 1.0)
-    return {"median_rel_err": round(float(np.median(rel)), 4),
+    rel = np.abs(est - r) / np.maximum(r, 1.0)
+    return {"quantity": "rows of the row loop (ksw.cu:346) per job",
+            "median_rel_err": round(float(np.median(rel)), 4),
             "mean_rel_err": round(float(np.mean(np.minimum(rel, 10.0))), 4),
-            "log2_mae": round(float(np.mean(np.abs(p - np.log2(1.0 + c)))), 4),
-            "corr_log2": round(float(np.corrcoef(p, np.log2(1.0 + c))[0, 1]), 4)}
+            "log2_mae": round(float(np.mean(np.abs(p - np.log2(1.0 + r)))), 4),
+            "corr_log2": round(float(np.corrcoef(p, np.log2(1.0 + r))[0, 1]), 4)}

@@ -113,7 +113,9 @@ typedef struct {
     int32_t *d_cells;     /* optional per-job DP cell count (trip count of ksw.cu:346) */
     int64_t n_bases;      /* bases the planes hold (required, 1 .. 2^32): a job or seed reaching
                              past it is refused with a per-job G3X_ERR_INVALID, unread */
-} g3x_batch_opts_t;       /* 40 bytes */
+    int32_t *d_rows;      /* optional per-job row count: trips of the row loop of ksw.cu:346
+                             (the z-drop or an empty band ends it before tlen) */
+} g3x_batch_opts_t;       /* 48 bytes */
 
 /* n jobs; outputs to d_out[k] and d_status[k] (G3X_OK or a G3X_ERR_* per job: TOO_LONG for a
    job beyond max_qlen/max_tlen or beyond what a fixed lane kernel holds, INVALID for a seed
@@ -524,9 +526,12 @@ int g3x_graph_destroy(g3x_graph *graph);
    features: qlen/128, tlen/256, h0/64, and the ungapped extension along the seed's diagonal
    over the first min(qlen, tlen) bases (from h0, +1 per identical base pair, -4 per other pair,
    N counting as other): its best score / 64 and the number of bases at which it is first
-   reached / 128.  Trained on the GPU by the library's own
-   forward/backward/Adam kernels; G3X_SCHED_LEARNED orders jobs by its prediction.  No
-   counterpart in the reference (its extension stage has no scheduler). */
+   reached / 128.  Its output is a correction to the length bound: log2(1 + rows) less
+   log2(1 + tlen), rows the trips of the row loop of ksw.cu:346 (g3x_batch_opts_t.d_rows), 0 for
+   a job that runs to its last row.  Trained on the GPU by the library's own
+   forward/backward/Adam kernels; G3X_SCHED_LEARNED orders jobs by log2(1 + tlen) plus
+   min(0, prediction + 1): only a predicted end before half the rows moves a job.  No counterpart in the reference (its extension stage has no
+   scheduler). */
 #define G3X_MLP_FEATURES 5
 #define G3X_MLP_PARAMS 4609   /* W1[64][5] b1[64] W2[64][64] b2[64] W3[64] b3 */
 

@@ -20,8 +20,9 @@ def to_dev(a):
 
 
 def run_batch(u8, jobs, score, schedule=g.SCHED_PLAIN, lanes=0, max_qlen=None, max_tlen=None,
-              tile=0, kernel=g.KERNEL_AUTO, n_bases=None):
-    """Returns (ext[n,6], status[n], cells[n]) from the GPU."""
+              tile=0, kernel=g.KERNEL_AUTO, n_bases=None, with_rows=False):
+    """Returns (ext[n,6], status[n], cells[n]) from the GPU, and rows[n] after them with
+    with_rows."""
     import torch
     n = len(jobs)
     codes, nmask = g.pack_planes(u8)
@@ -29,13 +30,15 @@ def run_batch(u8, jobs, score, schedule=g.SCHED_PLAIN, lanes=0, max_qlen=None, m
     out = torch.full((n, 6), -777, dtype=torch.int32, device="cuda")
     status = torch.full((n,), 99, dtype=torch.int32, device="cuda")
     cells = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    rows = torch.full((n,), -1, dtype=torch.int32, device="cuda") if with_rows else None
     mq = int(jobs["qlen"].max()) if max_qlen is None else max_qlen
     mt = int(jobs["tlen"].max()) if max_tlen is None else max_tlen
     ctx().extend_batch(score, d_jobs, n, d_codes, d_nmask, out, status, mq, mt,
                        schedule=schedule, lanes=lanes, d_cells=cells, tile=tile, kernel=kernel,
-                       n_bases=n_bases)
+                       n_bases=n_bases, d_rows=rows)
     torch.cuda.synchronize()
-    return out.cpu().numpy(), status.cpu().numpy(), cells.cpu().numpy()
+    res = (out.cpu().numpy(), status.cpu().numpy(), cells.cpu().numpy())
+    return res + (rows.cpu().numpy(),) if with_rows else res
 
 
 def run_seeds(u8, seeds, opt, schedule=g.SCHED_SORTED, lanes=0, n_bases=None):

@@ -42,7 +42,7 @@ def test_record_sizes():
     assert g.SCORE_DT.itemsize == 56
     assert g.JOB_DT.itemsize == 24
     assert g.EXT_DT.itemsize == 24
-    assert g.BATCH_OPTS_DT.itemsize == 40
+    assert g.BATCH_OPTS_DT.itemsize == 48
 
 
 def test_batch_opts_layout_matches_header(tmp_path):
@@ -50,15 +50,16 @@ def test_batch_opts_layout_matches_header(tmp_path):
     import subprocess
     src = tmp_path / "opts.c"
     src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "g3x.h"\nint main(void) {\n'
-                   '  printf("%zu %zu %zu %zu\\n", sizeof(g3x_batch_opts_t), offsetof(g3x_batch_opts_t, kernel),\n'
-                   '         offsetof(g3x_batch_opts_t, d_cells), offsetof(g3x_batch_opts_t, n_bases));\n'
+                   '  printf("%zu %zu %zu %zu %zu\\n", sizeof(g3x_batch_opts_t), offsetof(g3x_batch_opts_t, kernel),\n'
+                   '         offsetof(g3x_batch_opts_t, d_cells), offsetof(g3x_batch_opts_t, n_bases),\n'
+                   '         offsetof(g3x_batch_opts_t, d_rows));\n'
                    '  return 0;\n}\n')
     exe = tmp_path / "opts"
     subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
-    size, kern, cells, nb = (int(v) for v in subprocess.check_output([str(exe)]).split())
+    size, kern, cells, nb, rows = (int(v) for v in subprocess.check_output([str(exe)]).split())
     dt = g.BATCH_OPTS_DT
-    assert (size, kern, cells, nb) == (dt.itemsize, dt.fields["kernel"][1], dt.fields["d_cells"][1],
-                                       dt.fields["n_bases"][1])
+    assert (size, kern, cells, nb, rows) == (dt.itemsize, dt.fields["kernel"][1], dt.fields["d_cells"][1],
+                                             dt.fields["n_bases"][1], dt.fields["d_rows"][1])
 
 
 def test_noalloc_rejects_a_missing_plane_length(lib):

@@ -71,12 +71,14 @@ def test_gpu_matches_oracle_fresh(kind, n, w, sched, kernel, lanes, tile):
         pytest.skip("the lane-per-job kernels hold each lane's query in shared memory (short queries)")
     wl = g.synth(kind, n, seed=0x6A5 + 100 * kind + w, w=w, unrelated=0.2 if kind == 2 else 0.0)
     sc = g.default_score()
-    ref, rcells, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
-    out, status, cells = run_batch(wl.u8, wl.jobs, sc, sched, lanes, tile=tile, kernel=kernel)
+    ref, rcells, rrows = nat.oracle_extend(wl.jobs, wl.u8, sc)
+    out, status, cells, rows = run_batch(wl.u8, wl.jobs, sc, sched, lanes, tile=tile, kernel=kernel,
+                                         with_rows=True)
     keep = check_status(wl.jobs, sc, kernel, status)
     bad = np.nonzero(((out != ref).any(1)) & keep)[0]
     assert bad.size == 0, f"jobs {bad[:5]}"
     assert (cells[keep] == rcells[keep]).all()
+    assert (rows[keep] == rrows[keep]).all()          # the row loop's trips (ksw.cu:346)
 
 
 # Width classes on the lane-per-job kernels (int16x2 and int32) with the row-parallel kernel

@@ -43,3 +43,20 @@ def test_cost_order_beats_length_order():
     e_cost = warp_efficiency(cost_key, rows, blocks, cls)
     assert e_cost > e_sorted + 0.08, (e_cost, e_sorted)
     assert e_cost > 0.9
+
+
+def test_learned_target_is_a_correction_below_the_length_bound():
+    """The cost model's training target, log2(1 + rows) less log2(1 + tlen), is never positive
+    (the row loop of ksw.cu:346 runs at most tlen times), exactly 0 for the jobs that run to
+    their last row, and clearly negative where the z-drop ends a job early (unrelated
+    targets)."""
+    from g3sa_b200 import learn
+    sc = g.default_score()
+    wl = g.synth(2, 4000, seed=0x7A26, w=100, unrelated=0.2)
+    _, _, rows = nat.oracle_extend(wl.jobs, wl.u8, sc)
+    tlen = wl.jobs["tlen"]
+    tgt = learn.row_target(np.asarray(rows), tlen)
+    assert tgt.dtype == np.float32 and (tgt <= 0).all()
+    full = rows == tlen
+    assert full.mean() > 0.5 and (tgt[full] == 0).all()
+    assert np.percentile(tgt[~full], 25) < -1.0      # a quarter of them end before half their rows
