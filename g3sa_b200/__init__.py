@@ -56,7 +56,7 @@ REG_DT = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), (
 BATCH_OPTS_DT = np.dtype([("schedule", "<i4"), ("max_qlen", "<i4"), ("max_tlen", "<i4"),
                           ("lanes", "<i4"), ("tile", "<i4"), ("kernel", "<i4"), ("d_cells", "<u8"),
                           ("n_bases", "<i8"), ("d_rows", "<u8")])
-KERNEL_AUTO, KERNEL_ROLLING, KERNEL_ROWPAR, KERNEL_LANE, KERNEL_LANE16, KERNEL_LANE2 = 0, 1, 2, 3, 4, 5
+KERNEL_AUTO, KERNEL_ROLLING, KERNEL_ROWPAR, KERNEL_LANE, KERNEL_LANE16, KERNEL_LANE2, KERNEL_BAND = 0, 1, 2, 3, 4, 5, 6
 TILE_DT = np.dtype([("width", "<i4"), ("lanes", "<i4"), ("tile", "<i4"), ("warp_batch", "<i4"),
                     ("refill", "<i4")])
 MLP_PARAMS, MLP_FEATURES = 4609, 5

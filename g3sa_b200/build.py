@@ -18,7 +18,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["g3x_kernels.cu", "g3x_api.cu", "g3x_peak.cu", "g3x_seeds.cu", "g3x_stream.cu", "g3x_rowpar.cu", "g3x_model.cu", "g3x_sched.cu", "g3x_lane.cu", "g3x_lane16.cu", "g3x_lane2.cu", "g3x_noalloc.cu", "g3x_pipe.cu", "g3x_chain.cu", "g3x_produce.cu", "g3x_global.cu", "g3x_sw.cu", "g3x_seedflt.cu"]
+CU_SOURCES = ["g3x_kernels.cu", "g3x_api.cu", "g3x_peak.cu", "g3x_seeds.cu", "g3x_stream.cu", "g3x_rowpar.cu", "g3x_model.cu", "g3x_sched.cu", "g3x_lane.cu", "g3x_lane16.cu", "g3x_lane2.cu", "g3x_band.cu", "g3x_noalloc.cu", "g3x_pipe.cu", "g3x_chain.cu", "g3x_produce.cu", "g3x_global.cu", "g3x_sw.cu", "g3x_seedflt.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 

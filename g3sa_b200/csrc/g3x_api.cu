@@ -81,13 +81,22 @@ int batch_proto(const g3x_batch_opts_t* opts, int32_t* queue, LaunchDesc* d) {
     if (opts->schedule != G3X_SCHED_PLAIN && opts->schedule != G3X_SCHED_SORTED &&
         opts->schedule != G3X_SCHED_LEARNED)
         return G3X_ERR_INVALID;
-    if (opts->kernel < G3X_KERNEL_AUTO || opts->kernel > G3X_KERNEL_LANE2) return G3X_ERR_INVALID;
+    if (opts->kernel < G3X_KERNEL_AUTO || opts->kernel > G3X_KERNEL_BAND) return G3X_ERR_INVALID;
     const bool plain = opts->schedule == G3X_SCHED_PLAIN;
     d->kernel = opts->kernel == G3X_KERNEL_AUTO ? (plain ? kKernelRolling : kKernelRowpar)
                 : opts->kernel == G3X_KERNEL_ROLLING ? kKernelRolling
                 : opts->kernel == G3X_KERNEL_ROWPAR ? kKernelRowpar
                 : opts->kernel == G3X_KERNEL_LANE ? kKernelLane
-                : opts->kernel == G3X_KERNEL_LANE16 ? kKernelLane16 : kKernelLane2;
+                : opts->kernel == G3X_KERNEL_LANE16 ? kKernelLane16
+                : opts->kernel == G3X_KERNEL_LANE2 ? kKernelLane2 : kKernelBand;
+    if (d->kernel == kKernelBand) {
+        // one job per warp; tile carries the window (256, 512 or 1024 columns, 0 = 1024)
+        const int win = opts->tile ? opts->tile : 1024;
+        if (win != 256 && win != 512 && win != 1024) return G3X_ERR_INVALID;
+        d->lanes = 32; d->tile = win; d->persistent = plain ? 0 : 1; d->warps_per_block = 4;
+        d->queue = plain ? nullptr : queue;
+        return G3X_OK;
+    }
     if (d->kernel == kKernelLane || d->kernel == kKernelLane16 || d->kernel == kKernelLane2) {
         if (plain) return G3X_ERR_INVALID;            // the lane kernels are persistent only
         d->lanes = 1; d->tile = d->kernel == kKernelLane16 ? 2 : d->kernel == kKernelLane2 ? 4 : 0;
@@ -210,8 +219,8 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
         cudaStream_t cs = serial ? st : res.side[k];
         if (!serial && cudaStreamWaitEvent(cs, res.fork, 0) != cudaSuccess) { rc = G3X_ERR_CUDA; break; }
         LaunchDesc d = base;
-        d.kernel = tt.lanes[k] != 1 ? kKernelRowpar : tt.tile[k] == 2 ? kKernelLane16
-                 : tt.tile[k] == 4 ? kKernelLane2 : kKernelLane;
+        d.kernel = tt.lanes[k] != 1 ? (tt.tile[k] >= 64 ? kKernelBand : kKernelRowpar)
+                 : tt.tile[k] == 2 ? kKernelLane16 : tt.tile[k] == 4 ? kKernelLane2 : kKernelLane;
         d.ring = tt.lanes[k] == 1 && tt.tile[k] >= 64 ? tt.tile[k] : 0;
         d.lanes = tt.lanes[k];
         d.tile = tt.tile[k];
@@ -234,6 +243,8 @@ static int launch_classes(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParam
             rc = launch_lane16(d, sp, cs);
         } else if (d.kernel == kKernelLane2) {
             rc = launch_lane2(d, sp, cs);
+        } else if (d.kernel == kKernelBand) {
+            rc = launch_band(d, sp, cs);
         } else {
             while (d.lanes < 32 && (32 / d.lanes) * group_smem_bytes(d.qmax, d.tmax) > 227 * 1024) d.lanes *= 2;
             rc = launch_rowpar(d, sp, cs);
@@ -484,8 +495,12 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
     for (int k = 0; k < n; ++k) {
         const g3x_tile_t& t = h[k];
         const bool lane = t.lanes == 1;
+        // the band kernel (32 lanes, a window of 256, 512 or 1024 columns) holds only bands that
+        // fit its window, so it cannot be the last class, which takes every job
+        const bool band = t.lanes == 32 && (t.tile == 256 || t.tile == 512 || t.tile == 1024) && k < n - 1;
         if ((!lane && t.lanes != 4 && t.lanes != 8 && t.lanes != 16 && t.lanes != 32) ||
-            (!lane && t.tile != 5 && t.tile != 9 && t.tile != 13) || (lane && t.tile != 0 && t.tile != 2 && t.tile != 4 && (t.tile < 64 || t.tile % 16)) ||
+            (!lane && !band && t.tile != 5 && t.tile != 9 && t.tile != 13) ||
+            (lane && t.tile != 0 && t.tile != 2 && t.tile != 4 && (t.tile < 64 || t.tile % 16)) ||
             t.width < 1 ||
             (k && t.width <= h[k - 1].width) || (t.warp_batch != 0 && t.warp_batch != 1) ||
             (lane && (t.refill < 1 || t.refill > 32)))
@@ -624,6 +639,11 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
         if (!last && ring > 0 && ring < g3x::class_qcap(ctx->tiles, k, max_qlen) + 19 &&
             g3x::lane_ring_smem_per_warp(ring) <= 200 * 1024)
             for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, ring, 0, rf};
+        // the band kernel (one warp per job), with the narrowest window that holds every band
+        if (!last && wmax > 0 && 2 * wmax + 2 <= 1024) {
+            const int win = 2 * wmax + 2 <= 256 ? 256 : 2 * wmax + 2 <= 512 ? 512 : 1024;
+            cands[nc++] = Cand{32, win, 0, 1};
+        }
         for (int l : {4, 8, 16, 32})
             for (int c : {5, 9, 13}) {
                 const int S = l * c;

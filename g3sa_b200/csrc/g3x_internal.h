@@ -118,6 +118,7 @@ constexpr int32_t kKernelRowpar = 2;    // one row per step, columns on lanes
 constexpr int32_t kKernelLane = 3;      // one job per lane
 constexpr int32_t kKernelLane16 = 4;    // one job per lane, int16x2 pair-column blocks
 constexpr int32_t kKernelLane2 = 5;     // one job per lane, two rows in flight
+constexpr int32_t kKernelBand = 6;      // one job per warp, the band's row buffer in registers
 
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 
@@ -161,6 +162,8 @@ int launch_rowpar(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t strea
 int launch_lane(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_lane16(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 int launch_lane2(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+int launch_band(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
+size_t band_smem_per_warp(int qcap);
 size_t lane2_smem_per_warp(int qcap);
 size_t lane16_smem_per_warp(int qcap);
 size_t lane_ring_smem_per_warp(int ring);

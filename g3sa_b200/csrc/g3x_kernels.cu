@@ -174,6 +174,7 @@ int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t strea
     if (d.kernel == kKernelLane) return launch_lane(d, sp, stream);
     if (d.kernel == kKernelLane16) return launch_lane16(d, sp, stream);
     if (d.kernel == kKernelLane2) return launch_lane2(d, sp, stream);
+    if (d.kernel == kKernelBand) return launch_band(d, sp, stream);
     return d.kernel == kKernelRowpar ? launch_rowpar(d, sp, stream) : launch_rolling(d, sp, stream);
 }
 

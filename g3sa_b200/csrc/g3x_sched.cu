@@ -59,6 +59,10 @@ __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScorePara
         bool fits = tt.tile[b] == 2 ? job_fits_int16(c, sp.max_sc) : job_fits_lane(c, sp.max_sc);
         if (tt.tile[b] >= 64 && 2 * w + 16 > tt.tile[b]) fits = false;   // band wider than the ring
         if (!fits) b = tt.n - 1;
+    } else if (tt.lanes[b] == 32 && tt.tile[b] >= 64 && b != tt.n - 1) {
+        // the band kernel: the band's 2w' + 2 entries fit its window, and every H stays below 2^21
+        const int64_t hmax = (int64_t)jb.qlen * sp.max_sc + (jb.h0 > 0 ? jb.h0 : 0);
+        if (2 * w + 2 > tt.tile[b] || hmax >= (1 << 21)) b = tt.n - 1;
     }
     // log2 of the row count, 0..16; four bins per doubling, more rows -> earlier bin
     // The learned correction is soft-thresholded by one halving: min(0, pred + 1).  A job moves

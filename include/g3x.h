@@ -100,6 +100,9 @@ const char *g3x_strerror(int code);
 #define G3X_KERNEL_LANE16  4  /* one job per lane, two cells per int16x2 instruction (jobs whose
                                  scores fit 16 bits) */
 #define G3X_KERNEL_LANE2   5  /* one job per lane, rows i and i+1 in flight together */
+#define G3X_KERNEL_BAND    6  /* one job per warp, the band's row buffer in registers over a window
+                                 of `tile` columns (256, 512 or 1024, 0 = 1024) that slides with
+                                 the band; jobs whose band 2w' + 2 exceeds it get TOO_LONG */
 
 typedef struct {
     int32_t schedule;     /* G3X_SCHED_* */
@@ -168,9 +171,12 @@ int g3x_ksw_extend2_batch_noalloc(int device, const g3x_score_t *score, const g3
 typedef struct {
     int32_t width;        /* widest query of the class (the last class: unbounded) */
     int32_t lanes;        /* 1 = lane-per-job kernel; 4, 8, 16, 32 = row-parallel groups */
-    int32_t tile;         /* row-parallel: cells per lane per tile (5, 9, 13); lane kernel: 0
-                             (int32, one job per lane), 2 (int16x2, two cells per instruction) or 4
-                             (int32, one job per lane with two of its rows in flight) */
+    int32_t tile;         /* row-parallel: cells per lane per tile (5, 9, 13); with 32 lanes, 256,
+                             512 or 1024 = the band kernel (G3X_KERNEL_BAND) with that window
+                             (not the last class: a job whose band exceeds the window goes to
+                             the last class); lane kernel: 0 (int32, one job per lane), 2 (int16x2,
+                             two cells per instruction) or 4 (int32, one job per lane with two of
+                             its rows in flight) */
     int32_t warp_batch;   /* 1: a warp takes its jobs together and waits for all of them */
     int32_t refill;       /* lane kernel: idle lanes that trigger a refill wave (1-32) */
 } g3x_tile_t;

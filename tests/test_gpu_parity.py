@@ -10,15 +10,17 @@ from tests.gpu_util import run_batch
 
 pytestmark = pytest.mark.gpu
 
-R, P, LN, L16, L2 = g.KERNEL_ROLLING, g.KERNEL_ROWPAR, g.KERNEL_LANE, g.KERNEL_LANE16, g.KERNEL_LANE2
+R, P, LN, L16, L2, B = (g.KERNEL_ROLLING, g.KERNEL_ROWPAR, g.KERNEL_LANE, g.KERNEL_LANE16, g.KERNEL_LANE2,
+                        g.KERNEL_BAND)
 # (schedule, kernel, lanes, tile)
 SCHEDULES = [(g.SCHED_PLAIN, R, 0, 0), (g.SCHED_SORTED, R, 8, 0), (g.SCHED_SORTED, R, 16, 0),
              (g.SCHED_SORTED, R, 32, 0), (g.SCHED_PLAIN, P, 0, 9)] + \
             [(g.SCHED_SORTED, P, l, t) for l in (4, 8, 16, 32) for t in (5, 9, 13)] + \
             [(g.SCHED_SORTED, LN, 1, rf) for rf in (1, 8, 32)] + \
             [(g.SCHED_SORTED, L16, 1, rf) for rf in (1, 8, 32)] + \
-            [(g.SCHED_SORTED, L2, 1, rf) for rf in (1, 8, 32)]
-NAMES = {R: "roll", P: "row", LN: "lane", L16: "lane16", L2: "lane2"}
+            [(g.SCHED_SORTED, L2, 1, rf) for rf in (1, 8, 32)] + \
+            [(g.SCHED_SORTED, B, 32, 256), (g.SCHED_SORTED, B, 32, 1024), (g.SCHED_PLAIN, B, 32, 512)]
+NAMES = {R: "roll", P: "row", LN: "lane", L16: "lane16", L2: "lane2", B: "band"}
 IDS = [f"{'plain' if s == 0 else 'pers'}-{NAMES[k]}-g{l}-c{t}" for s, k, l, t in SCHEDULES]
 
 
@@ -39,9 +41,35 @@ def lane_fits(jobs, score, kernel):
     return ok & ((hmax << k) < 32768) & small
 
 
-def check_status(jobs, score, kernel, status):
+def clamped_w(jobs, score):
+    """The band width after the clamp of ksw.cu:321-329: min(w, the insertion and deletion
+    limits (int)((qlen * max_score + end_bonus - o) / e + 1.), each at least 1)."""
+    q = jobs["qlen"].astype(np.int64)
+    max_sc = int(score["mat"][0].max())
+    eb = int(score["end_bonus"][0])
+    w = jobs["w"].astype(np.int64)
+    for o, e in ((int(score["o_ins"][0]), int(score["e_ins"][0])), (int(score["o_del"][0]), int(score["e_del"][0]))):
+        num = q * max_sc + eb - o
+        w = np.minimum(w, np.maximum(np.where(num >= 0, num // e + 1, 1), 1))
+    return w
+
+
+def band_fits(jobs, score, window):
+    """Jobs the band kernel takes: the band's 2w' + 2 entries fit the window and every H stays
+    below 2^21 (h0 + qlen * max_score)."""
+    max_sc = int(score["mat"][0].max())
+    hmax = np.maximum(jobs["h0"].astype(np.int64), 0) + jobs["qlen"].astype(np.int64) * max_sc
+    return (2 * clamped_w(jobs, score) + 2 <= window) & (hmax < (1 << 21))
+
+
+def check_status(jobs, score, kernel, status, tile=0):
     """Mask of the jobs whose outputs are compared: all of them, except the jobs a lane-per-job
-    kernel must reject (which must carry G3X_ERR_TOO_LONG)."""
+    kernel or the band kernel must reject (which must carry G3X_ERR_TOO_LONG)."""
+    if kernel == B:
+        fits = band_fits(jobs, score, tile or 1024)
+        assert (status[~fits] == g.G3X_ERR_TOO_LONG).all()
+        assert (status[fits] == 0).all(), np.unique(status[fits])
+        return fits
     if kernel in (LN, L16, L2):
         fits = lane_fits(jobs, score, kernel)
         assert (status[~fits] == g.G3X_ERR_TOO_LONG).all()
@@ -59,7 +87,7 @@ def test_gpu_matches_golden(name, sched, kernel, lanes, tile):
     if kernel in (LN, L16, L2) and jobs["qlen"].max() > 1000:
         pytest.skip("the lane-per-job kernels hold each lane's query in shared memory (short queries)")
     out, status, cells = run_batch(u8, jobs, score, sched, lanes, tile=tile, kernel=kernel)
-    keep = check_status(jobs, score, kernel, status)
+    keep = check_status(jobs, score, kernel, status, tile)
     bad = np.nonzero(((out != ext).any(1)) & keep)[0]
     assert bad.size == 0, f"{name}: jobs {bad[:5]} got {out[bad[:3]]} want {ext[bad[:3]]}"
 
@@ -74,7 +102,7 @@ def test_gpu_matches_oracle_fresh(kind, n, w, sched, kernel, lanes, tile):
     ref, rcells, rrows = nat.oracle_extend(wl.jobs, wl.u8, sc)
     out, status, cells, rows = run_batch(wl.u8, wl.jobs, sc, sched, lanes, tile=tile, kernel=kernel,
                                          with_rows=True)
-    keep = check_status(wl.jobs, sc, kernel, status)
+    keep = check_status(wl.jobs, sc, kernel, status, tile)
     bad = np.nonzero(((out != ref).any(1)) & keep)[0]
     assert bad.size == 0, f"jobs {bad[:5]}"
     assert (cells[keep] == rcells[keep]).all()
