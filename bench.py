@@ -956,7 +956,7 @@ def timed_steps(fn, k, w, stream, flush, nvtx=None):
 def kernel_name(t):
     """Kernel of a width class (width, lanes, tile, warp_batch, refill)."""
     if t[1] != 1:
-        return f"rowpar g{t[1]} c{t[2]}"
+        return f"band {t[2]}" if t[2] >= 64 else f"rowpar g{t[1]} c{t[2]}"
     if t[2] >= 64:
         return f"lane ring {t[2]}"
     return {2: "lane16", 4: "lane2"}.get(t[2], "lane")

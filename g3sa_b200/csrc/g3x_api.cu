@@ -623,7 +623,7 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
     // width (the unbounded class: 32-lane groups), each refilling per group or per warp.
     struct Cand { int lanes, tile, wb, refill; };
     Cand cands[64];
-    g3x::TileTable best = ctx->tiles;
+    g3x::TileTable best = ctx->tiles, best_nb = ctx->tiles;   // best_nb: the best without band classes
     for (int k = 0; k < ctx->tiles.n && rc == G3X_OK; ++k) {
         if (oc[2 * k + 1] == 0) continue;
         const int width = std::min(ctx->tiles.width[k], max_qlen);
@@ -650,7 +650,7 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
                 if (last ? l != 32 : (S < width || S > 2 * width + 40)) continue;
                 for (int wb = 0; wb < 2; ++wb) cands[nc++] = Cand{l, c, wb, 1};
             }
-        float best_ms = 1e30f;
+        float best_ms = 1e30f, best_nb_ms = 1e30f;
         for (int ci = 0; ci < nc && rc == G3X_OK; ++ci) {
             g3x::TileTable tt = ctx->tiles;
             tt.lanes[k] = cands[ci].lanes; tt.tile[k] = cands[ci].tile;
@@ -669,7 +669,37 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
                 best.lanes[k] = tt.lanes[k]; best.tile[k] = tt.tile[k];
                 best.warp_batch[k] = tt.warp_batch[k]; best.refill[k] = tt.refill[k];
             }
+            const bool band = tt.lanes[k] == 32 && tt.tile[k] >= 64;
+            if (rc == G3X_OK && !band && ms < best_nb_ms) {
+                best_nb_ms = ms;
+                best_nb.lanes[k] = tt.lanes[k]; best_nb.tile[k] = tt.tile[k];
+                best_nb.warp_batch[k] = tt.warp_batch[k]; best_nb.refill[k] = tt.refill[k];
+            }
         }
+    }
+    // Each class was timed alone; side by side, the band kernel's register-heavy warps and the
+    // lane kernels' shared-memory-heavy warps compete for the same SMs.  So a table with band
+    // classes is kept only if the whole batch runs faster with it than with those classes on
+    // their best other kernel.
+    bool has_band = false;
+    for (int k = 0; k < best.n; ++k) has_band |= best.lanes[k] == 32 && best.tile[k] >= 64;
+    if (rc == G3X_OK && has_band) {
+        auto whole = [&](const g3x::TileTable& tt, float* out_ms) -> int {
+            int r = G3X_OK;
+            for (int rep = 0; rep < 2 && r == G3X_OK; ++rep) {
+                cudaMemsetAsync(ctx->d_queue, 0, g3x::kMaxBuckets * sizeof(int32_t), st);
+                cudaEventRecord(e0, st);
+                r = g3x::launch_classes(ctx, base, sp, st, -1, &tt);
+                cudaEventRecord(e1, st);
+                if (cudaEventSynchronize(e1) != cudaSuccess) r = G3X_ERR_CUDA;
+                cudaEventElapsedTime(out_ms, e0, e1);
+            }
+            return r;
+        };
+        float ms_band = 0, ms_alt = 0;
+        rc = whole(best, &ms_band);
+        if (rc == G3X_OK) rc = whole(best_nb, &ms_alt);
+        if (rc == G3X_OK && ms_alt < ms_band) best = best_nb;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

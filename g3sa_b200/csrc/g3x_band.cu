@@ -195,22 +195,29 @@ __global__ void __launch_bounds__(128) band_kernel(LaunchDesc d, ScoreParams sp)
             const int32_t base = i - c.w;                 // column of window index 0
             const int32_t j0 = base + lane * R;           // this lane's first column
             const int32_t lo = beg - j0, hi = end - j0;   // this lane's cells: lo <= k < hi
-            // bit k: index k is a cell of the row (act), column beg (lom), column end (him)
-            const int32_t loc = lo < 0 ? 0 : (lo > R ? R : lo), hic = hi < 0 ? 0 : (hi > R ? R : hi);
-            const uint32_t act = (uint32_t)((((1ull << hic) - 1ull) & ~((1ull << loc) - 1ull)));
-            const uint32_t lom = lo >= 0 && lo < R ? 1u << lo : 0u;
-            const uint32_t him = hi >= 0 && hi < R ? 1u << hi : 0u;
-            const uint32_t upd = act | him;                // entries the row writes
-            // ---- pass 1: M and the lane-local F ----
+            // Every entry left of beg is {0, 0}: the first row's are (columns < 0), the trim moves
+            // beg only past entries found zero, and a zero entry left of beg stays zero (its M is at
+            // most 0, its E and F are 0).  So the columns left of beg need no mask: they add
+            // nothing to F and compute {0, 0} again.  Columns from end on keep their (stale)
+            // entries, except the end entry itself (ksw.cu:371).
+            // ---- pass 1: M and the F recurrence from 0 over each segment of kSeg columns (the
+            // segments' chains are independent) ----
+            constexpr int kSeg = R < 8 ? R : 8, kNs = R / kSeg;
             int32_t M[R];
-            int32_t f = 0, flast = 0;
+            int32_t so[kNs];                               // F leaving each segment, from 0 at its start
+            int32_t flast = 0;                             // F entering the last column, from 0 at its segment
+#pragma unroll
+            for (int q = 0; q < kNs; ++q) so[q] = 0;
 #pragma unroll
             for (int k = 0; k < R; ++k) {
                 const int32_t s = permute_score(pl.x, pl.y, S[k]);
-                M[k] = (act >> k) & 1u ? addmin_i32(Hb[k], s, Hb[k] << 8) : 0;
-                if (k == R - 1) flast = f;
-                f = addmax_i32(f, -e_ins, addmax_i32(M[k], -oe_ins, 0));
+                M[k] = addmin_i32(Hb[k], s, Hb[k] << 8);
+                if (k == R - 1) flast = so[k / kSeg];
+                so[k / kSeg] = addmax_i32(so[k / kSeg], -e_ins, addmax_i32(M[k], -oe_ins, 0));
             }
+            int32_t f = so[0];                             // F leaving the lane, from 0 at its start
+#pragma unroll
+            for (int q = 1; q < kNs; ++q) f = addmax_i32(f, -kSeg * e_ins, so[q]);
             // ---- F along the row: F entering each lane's first column ----
             int32_t x = f;
 #pragma unroll
@@ -220,37 +227,48 @@ __global__ void __launch_bounds__(128) band_kernel(LaunchDesc d, ScoreParams sp)
             }
             int32_t fin = __shfl_up_sync(0xFFFFFFFFu, x, 1);
             if (lane == 0) fin = 0;
+            int32_t sf[kNs];                               // F entering each segment
+            sf[0] = fin;
+#pragma unroll
+            for (int q = 1; q < kNs; ++q) sf[q] = addmax_i32(sf[q - 1], -kSeg * e_ins, so[q - 1]);
             // H at this lane's last column, for the next lane's first entry H(i, j-1)
-            const int32_t hl = max3_i32(M[R - 1], Eb[R - 1], addmax_i32(fin, -(R - 1) * e_ins, flast));
+            const int32_t hl = max3_i32(M[R - 1], Eb[R - 1], addmax_i32(sf[kNs - 1], -(kSeg - 1) * e_ins, flast));
             int32_t hleft = __shfl_up_sync(0xFFFFFFFFu, hl, 1);
+            if (lane == 0) hleft = 0;                      // left of the window: left of beg, so 0
             // ---- pass 2: H, the new entries (written one index down), row max, non-zero span ----
             // New entries: column beg (H(i, beg-1) = h1, E(i+1, beg)), columns beg+1 .. end-1
-            // (H(i, j-1), E(i+1, j)), column end (H(i, end-1), 0); the others keep their values.
+            // (H(i, j-1), E(i+1, j)), column end (H(i, end-1), 0); the later ones keep theirs.
             // For an empty row the end entry is never read again (the row ends the job).
-            int32_t f2 = 0, hend = 0;
-            int32_t lkey = -1;                             // lane's row max as H * 32 + k (ties: larger k)
-            uint32_t nzm = 0;
+            int32_t f2[kNs], hend = 0;
+            int32_t lk[kNs];                               // row max of each segment as H * 32 + k (ties: larger k)
+            uint32_t nz[kNs];                              // bit k: the new entry at k is non-zero
+#pragma unroll
+            for (int q = 0; q < kNs; ++q) { f2[q] = 0; lk[q] = -1; nz[q] = 0; }
             int32_t nh0 = 0, ne0 = 0;
             uint32_t s0 = 0;
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                const int32_t F = addmax_i32(fin, -k * e_ins, f2);
+                const int q = k / kSeg;
+                const int32_t F = addmax_i32(sf[q], -(k % kSeg) * e_ins, f2[q]);
                 const int32_t ti = addmax_i32(M[k], -oe_ins, 0);
-                f2 = addmax_i32(f2, -e_ins, ti);
+                f2[q] = addmax_i32(f2[q], -e_ins, ti);
                 const int32_t H = max3_i32(M[k], Eb[k], F);
                 const int32_t te = kSym ? ti : addmax_i32(M[k], -oe_del, 0);
                 const int32_t En = addmax_i32(Eb[k], -e_del, te);
-                const bool a = (act >> k) & 1u;
-                const int32_t nh = (lom >> k) & 1u ? h1 : ((upd >> k) & 1u ? hleft : Hb[k]);
-                const int32_t ne = a ? En : ((him >> k) & 1u ? 0 : Eb[k]);
-                if ((him >> k) & 1u) hend = hleft;
-                nzm |= (uint32_t)((nh | ne) != 0) << k;
-                lkey = a ? max(lkey, H * 32 + k) : lkey;
+                const bool in = k < hi, at_end = k == hi;
+                const int32_t nh = in ? (k == lo ? h1 : hleft) : (at_end ? hleft : Hb[k]);
+                const int32_t ne = in ? En : (at_end ? 0 : Eb[k]);
+                if (at_end) hend = hleft;
+                nz[q] = in ? (min((uint32_t)(nh | ne), 1u) << k) | nz[q] : nz[q];
+                lk[q] = in ? max(lk[q], H * 32 + k) : lk[q];
                 hleft = H;
                 if (k == 0) { nh0 = nh; ne0 = ne; s0 = S[0]; }
                 else { Hb[k - 1] = nh; Eb[k - 1] = ne; S[k - 1] = S[k]; }
             }
-            nzm &= act;
+            int32_t lkey = lk[0];
+            uint32_t nzm = nz[0];
+#pragma unroll
+            for (int q = 1; q < kNs; ++q) { lkey = max(lkey, lk[q]); nzm |= nz[q]; }
             const uint32_t key = lkey < 0 ? 0u
                                  : (((uint32_t)lkey >> 5) << 10 | (uint32_t)(lane * R + (lkey & 31))) + 1u;
             uint32_t fnz = nzm ? (uint32_t)(j0 + __ffs(nzm) - 1) + 1u : 0xFFFFFFFFu;
