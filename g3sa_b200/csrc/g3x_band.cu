@@ -335,14 +335,14 @@ static int launch_band_t(const LaunchDesc& d, const ScoreParams& sp, cudaStream_
     if (wb > max_smem) return G3X_ERR_TOO_LONG;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return G3X_ERR_CUDA;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    sms = sm_count();
     // warps per block: the choice among 1, 2 and 4 that keeps the most warps resident (registers
     // are allotted per block, so small blocks of this register-heavy kernel waste fewer)
     int best_wpb = 1, best_warps = 0, best_blocks = 0;
     for (int wpb = 1; wpb <= 4; wpb *= 2) {
         if ((size_t)wpb * wb > max_smem) break;
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, (size_t)wpb * wb);
+        per_sm = resident_blocks(kern, 32 * wpb, (size_t)wpb * wb);
         if (per_sm * wpb > best_warps) { best_warps = per_sm * wpb; best_wpb = wpb; best_blocks = per_sm; }
     }
     const size_t smem = (size_t)best_wpb * wb;

@@ -316,8 +316,8 @@ extern "C" int g3x_ksw_global2_batch(g3x_ctx* ctx, const g3x_score_t* score, con
     if (warp_smem > max_smem) return G3X_ERR_TOO_LONG;
     const int wpb = 2 * warp_smem <= max_smem ? 2 : 1;
     int sms = 0, per_sm = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, wpb * warp_smem);
+    sms = sm_count();
+    per_sm = resident_blocks(kern, 32 * wpb, wpb * warp_smem);
     int blocks = sms * std::max(per_sm, 1);
     // direction bytes: tmax rows x ncol columns x 32 lanes per resident warp, at most 8 GiB
     d.zwarp = (int64_t)d.tmax * d.ncol * 32;

@@ -1,5 +1,6 @@
 // g3x_internal.h -- declarations shared by the library's translation units.
 #pragma once
+#include <mutex>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/g3x.h"
@@ -122,22 +123,90 @@ constexpr int32_t kKernelBand = 6;      // one job per warp, the band's row buff
 
 int launch_extend(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t stream);
 
+// Launch facts that never change for a kernel on a device, cached for the process: the SM
+// count, the dynamic shared memory a block of a kernel may use (after its limit was raised once),
+// and the resident blocks per SM at a block size and dynamic shared memory.  Each CUDA query
+// costs microseconds of host time, and a chunked seed stream makes thousands of class launches
+// with a handful of configurations.
+struct LaunchCache {
+    struct Ent {
+        int kind;            // 0: dynamic shared memory limit, 1: resident blocks, 2: SMs
+        const void* fn;
+        int dev, threads;
+        size_t smem;
+        long long val;
+    };
+    std::mutex mu;
+    Ent e[1024];
+    int n = 0;
+    bool get(int kind, const void* fn, int dev, int threads, size_t smem, long long* val) {
+        std::lock_guard<std::mutex> g(mu);
+        for (int k = 0; k < n; ++k)
+            if (e[k].kind == kind && e[k].fn == fn && e[k].dev == dev && e[k].threads == threads &&
+                e[k].smem == smem) {
+                *val = e[k].val;
+                return true;
+            }
+        return false;
+    }
+    void put(int kind, const void* fn, int dev, int threads, size_t smem, long long val) {
+        std::lock_guard<std::mutex> g(mu);
+        if (n < 1024) e[n++] = Ent{kind, fn, dev, threads, smem, val};
+    }
+};
+inline LaunchCache& launch_cache() {
+    static LaunchCache c;
+    return c;
+}
+
+inline int sm_count() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    long long v;
+    if (launch_cache().get(2, nullptr, dev, 0, 0, &v)) return (int)v;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return 1;
+    launch_cache().put(2, nullptr, dev, 0, 0, sms);
+    return sms;
+}
+
 // Lets kernel `fn` launch with all the dynamic shared memory a block can have on this device
 // (the opt-in maximum less the kernel's static shared memory), which *limit receives.  Always
-// the same value: a kernel launched by several width classes (possibly captured in one CUDA
-// graph) must never see another launch lower its limit below its own size.
+// the same value, set once per device: a kernel launched by several width classes (possibly
+// captured in one CUDA graph) must never see another launch lower its limit below its own size.
 template <class F>
 inline cudaError_t allow_max_smem(F* fn, size_t* limit = nullptr) {
     int dev = 0, optin = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    long long v;
+    if (launch_cache().get(0, (const void*)fn, dev, 0, 0, &v)) {
+        if (limit) *limit = (size_t)v;
+        return cudaSuccess;
+    }
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes a;
     if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, fn);
     if (e != cudaSuccess) return e;
     const int dyn = optin - (int)a.sharedSizeBytes;
     if (limit) *limit = (size_t)dyn;
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (e == cudaSuccess) launch_cache().put(0, (const void*)fn, dev, 0, 0, dyn);
+    return e;
 }
+
+// Resident blocks per SM of `fn` with `threads` threads and `smem` bytes of dynamic shared
+// memory per block (0 when it does not fit).
+template <class F>
+inline int resident_blocks(F* fn, int threads, size_t smem) {
+    int dev = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    long long v;
+    if (launch_cache().get(1, (const void*)fn, dev, threads, smem, &v)) return (int)v;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) per_sm = 0;
+    launch_cache().put(1, (const void*)fn, dev, threads, smem, per_sm);
+    return per_sm;
+}
+
 // Launches a width-class kernel fn<<<grid, block, smem, st>>>(d, sp).  With d.pdl it goes out
 // as a programmatic dependent of the kernel before it on `st`: it may start as soon as every
 // block of that kernel has called pdl_trigger(), so the classes of one stream run side by side

@@ -149,8 +149,8 @@ static int launch_g(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t str
         if (blocks <= 0) {
             int dev = 0, sms = 0, per_sm = 0;
             cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, extend_kernel<G>, threads, smem);
+            sms = sm_count();
+            per_sm = resident_blocks(extend_kernel<G>, threads, smem);
             blocks = sms * (per_sm > 0 ? per_sm : 1);
         }
     } else {

@@ -479,7 +479,7 @@ static int launch_lane_t(const LaunchDesc& d, const ScoreParams& sp, cudaStream_
     if (wb > max_smem) return G3X_ERR_TOO_LONG;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return G3X_ERR_CUDA;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    sms = sm_count();
     // Warps per block: the choice among 1, 2 and 4 that keeps the most warps resident (shared
     // memory is allotted per block, so small blocks waste less of it).
     int best_wpb = 1, best_warps = 0, best_blocks = 0;
@@ -488,7 +488,7 @@ static int launch_lane_t(const LaunchDesc& d, const ScoreParams& sp, cudaStream_
         const size_t smem = (size_t)wpb * wb;
         if (smem > max_smem) break;
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane_kernel<kRing>, 32 * wpb, smem);
+        per_sm = resident_blocks(lane_kernel<kRing>, 32 * wpb, smem);
         if (per_sm * wpb >= best_warps) { best_warps = per_sm * wpb; best_wpb = wpb; best_blocks = per_sm; }
     }
     const size_t smem = (size_t)best_wpb * wb;

@@ -207,14 +207,14 @@ static int launch_lane16_t(const LaunchDesc& d, const ScoreParams& sp, cudaStrea
     if (wb > max_smem) return G3X_ERR_TOO_LONG;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return G3X_ERR_CUDA;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    sms = sm_count();
     int best_wpb = 1, best_warps = 0, best_blocks = 0;
     const int max_wpb = d.warps_per_block > 0 ? d.warps_per_block : 4;
     for (int wpb = 1; wpb <= max_wpb; wpb *= 2) {
         const size_t smem = (size_t)wpb * wb;
         if (smem > max_smem) break;
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane16_kernel<kSym>, 32 * wpb, smem);
+        per_sm = resident_blocks(lane16_kernel<kSym>, 32 * wpb, smem);
         if (per_sm * wpb >= best_warps) { best_warps = per_sm * wpb; best_wpb = wpb; best_blocks = per_sm; }
     }
     const size_t smem = (size_t)best_wpb * wb;

@@ -335,8 +335,8 @@ static int launch_rp(const LaunchDesc& d, const ScoreParams& sp, cudaStream_t st
         if (blocks <= 0) {
             int dev = 0, sms = 0, per_sm = 0;
             cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rowpar_kernel<G, C>, threads, smem);
+            sms = sm_count();
+            per_sm = resident_blocks(rowpar_kernel<G, C>, threads, smem);
             blocks = sms * (per_sm > 0 ? per_sm : 1);
         }
     } else {

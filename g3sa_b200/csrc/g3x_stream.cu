@@ -8,10 +8,10 @@
 // compute stream, buffer set, pinned staging, seed scratch and sort scratch, and chains its
 // width classes on its stream as programmatic dependent launches (side by side, without side
 // streams), so the latency-bound waves of one chunk (a wave's longest job runs alone at the
-// end) overlap the next chunks' waves.  The host work of a chunk (its range,
-// its staging copy) overlaps the device work of the chunks before it.  Results come back
-// through the lane's pinned staging.  All of it lives in the context and is grown on demand,
-// so repeated calls allocate nothing.
+// end) overlap the next chunks' waves.  The host work of a chunk (its range, its launches)
+// overlaps the device work of the chunks before it.  Host buffers that are pinned are copied
+// straight to and from; pageable ones go through the lane's pinned staging.  All of it lives in
+// the context and is grown on demand, so repeated calls allocate nothing.
 #include <cuda_runtime.h>
 #include <string.h>
 #include <algorithm>
@@ -110,6 +110,18 @@ int grow_stream(StreamScratch& ss, int64_t chunk, int64_t code_words, int64_t ma
     return G3X_OK;
 }
 
+// Whether host memory at p is pinned (page-locked or registered): then the copies go straight
+// between it and the device, asynchronously; pageable memory goes through the lane's pinned
+// staging, so that the copies still overlap the other lanes' work.
+bool pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();                            // older drivers report pageable memory so
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 // Range of plane bases chunk [first, first + count) reads; G3X_ERR_INVALID when a seed reaches
 // past the planes.
 int chunk_range(const g3x_seed_t* h_seeds, int64_t first, int64_t count, int64_t n_bases, ChunkRange& R) {
@@ -154,13 +166,16 @@ int extend_seeds_stream(StreamScratch& ss, const g3x_opt_t& opt, const ScorePara
         wr[l] = WaveRunner{runner->run, &cw[l]};
     }
     const int64_t total_code_words = (n_bases + 15) / 16, total_mask_words = (n_bases + 31) / 32;
+    const bool seeds_pinned = pinned(h_seeds), out_pinned = pinned(h_regs) && pinned(h_status);
     auto drain = [&](int l) -> int {
         StreamSet& s = ss.set[l];
         if (s.pending < 0) return G3X_OK;
         if (cudaEventSynchronize(s.done) != cudaSuccess) return G3X_ERR_CUDA;
         const ChunkRange& R = pend[(size_t)l];
-        memcpy(h_regs + R.first, s.h_regs, R.count * sizeof(g3x_reg_t));
-        memcpy(h_status + R.first, s.h_status, R.count * sizeof(int32_t));
+        if (!out_pinned) {
+            memcpy(h_regs + R.first, s.h_regs, R.count * sizeof(g3x_reg_t));
+            memcpy(h_status + R.first, s.h_status, R.count * sizeof(int32_t));
+        }
         s.pending = -1;
         return G3X_OK;
     };
@@ -178,9 +193,12 @@ int extend_seeds_stream(StreamScratch& ss, const g3x_opt_t& opt, const ScorePara
             if (rc || (rc = grow_stream(ss, chunk, cwn + cwn / 4, mwn + mwn / 4))) break;
         }
         if ((rc = drain(l))) break;                      // lane free: its last chunk is done
-        memcpy(s.h_seeds, h_seeds + R.first, R.count * sizeof(g3x_seed_t));
-        if (cudaMemcpyAsync(s.d_seeds, s.h_seeds, R.count * sizeof(g3x_seed_t), cudaMemcpyHostToDevice,
-                            ss.copy_st) ||
+        const g3x_seed_t* src = h_seeds + R.first;
+        if (!seeds_pinned) {
+            memcpy(s.h_seeds, src, R.count * sizeof(g3x_seed_t));
+            src = s.h_seeds;
+        }
+        if (cudaMemcpyAsync(s.d_seeds, src, R.count * sizeof(g3x_seed_t), cudaMemcpyHostToDevice, ss.copy_st) ||
             cudaMemcpyAsync(s.d_codes, h_codes + cw0w, cwn * sizeof(uint32_t), cudaMemcpyHostToDevice, ss.copy_st) ||
             cudaMemcpyAsync(s.d_nmask, h_nmask + mw0, mwn * sizeof(uint32_t), cudaMemcpyHostToDevice, ss.copy_st) ||
             cudaEventRecord(s.h2d, ss.copy_st) || cudaStreamWaitEvent(s.comp, s.h2d, 0)) {
@@ -193,8 +211,10 @@ int extend_seeds_stream(StreamScratch& ss, const g3x_opt_t& opt, const ScorePara
         if ((rc = extend_seeds(s.seeds, opt, sp, s.d_seeds, (int)R.count, s.d_codes, s.d_nmask, s.d_regs,
                                s.d_status, cp, s.comp, runner ? &wr[l] : nullptr)))
             break;
-        if (cudaMemcpyAsync(s.h_regs, s.d_regs, R.count * sizeof(g3x_reg_t), cudaMemcpyDeviceToHost, s.comp) ||
-            cudaMemcpyAsync(s.h_status, s.d_status, R.count * sizeof(int32_t), cudaMemcpyDeviceToHost, s.comp) ||
+        g3x_reg_t* dst_regs = out_pinned ? h_regs + R.first : s.h_regs;
+        int32_t* dst_status = out_pinned ? h_status + R.first : s.h_status;
+        if (cudaMemcpyAsync(dst_regs, s.d_regs, R.count * sizeof(g3x_reg_t), cudaMemcpyDeviceToHost, s.comp) ||
+            cudaMemcpyAsync(dst_status, s.d_status, R.count * sizeof(int32_t), cudaMemcpyDeviceToHost, s.comp) ||
             cudaEventRecord(s.done, s.comp)) {
             rc = G3X_ERR_CUDA;
             break;

@@ -449,9 +449,7 @@ int launch_class(const SwDesc& d0, const int32_t* range, int32_t* queue, int sms
     SwDesc d = d0;
     d.range = range;
     d.queue = queue;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sw_kernel<MAXSEG>, 32 * kWarps, 0) != cudaSuccess)
-        return G3X_ERR_CUDA;
+    const int per_sm = resident_blocks(sw_kernel<MAXSEG>, 32 * kWarps, 0);
     sw_kernel<MAXSEG><<<sms * std::max(per_sm, 1), 32 * kWarps, 0, st>>>(d);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }
@@ -523,7 +521,7 @@ extern "C" int g3x_ksw_align2_batch(g3x_ctx* ctx, const g3x_score_t* score, cons
     d.nedel = pack16(-sp.e_del); d.noedel = pack16(-sp.oe_del);
     d.neins = pack16(-sp.e_ins); d.noeins = pack16(-sp.oe_ins);
     int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    sms = sm_count();
     if ((rc = launch_class<32>(d, range, queue, sms, st))) return rc;
     if ((rc = launch_class<16>(d, range + 2, queue + 1, sms, st))) return rc;
     return launch_class<8>(d, range + 4, queue + 2, sms, st);

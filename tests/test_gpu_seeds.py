@@ -52,19 +52,22 @@ def test_seeds_fresh_vs_oracle(w):
         assert (regs[f] == ref[f]).all(), f
 
 
-@pytest.mark.parametrize("chunk", [4096, 65536])
-def test_seeds_stream_matches_device_form(chunk):
+@pytest.mark.parametrize("chunk,pin", [(4096, True), (65536, True), (4096, False)])
+def test_seeds_stream_matches_device_form(chunk, pin):
+    """Pinned host buffers are copied straight to and from the device, pageable ones through the
+    stream's pinned staging; both give the oracle's regions."""
     import torch
     wl = g.synth(2, 30000, seed=99, w=100, unrelated=0.2)
     codes, nmask = wl.planes()
     opt = g.default_opt(w=100)
     ds = g.device_seeds(wl.seeds)
     n = len(ds)
-    h_seeds = torch.from_numpy(ds.view(np.uint8).copy()).pin_memory()
-    h_codes = torch.from_numpy(codes.view(np.uint8).copy()).pin_memory()
-    h_nmask = torch.from_numpy(nmask.view(np.uint8).copy()).pin_memory()
-    h_regs = torch.zeros(n * g.REG_DT.itemsize, dtype=torch.uint8).pin_memory()
-    h_status = torch.full((n,), 99, dtype=torch.int32).pin_memory()
+    host = (lambda t: t.pin_memory()) if pin else (lambda t: t)   # noqa: E731
+    h_seeds = host(torch.from_numpy(ds.view(np.uint8).copy()))
+    h_codes = host(torch.from_numpy(codes.view(np.uint8).copy()))
+    h_nmask = host(torch.from_numpy(nmask.view(np.uint8).copy()))
+    h_regs = host(torch.zeros(n * g.REG_DT.itemsize, dtype=torch.uint8))
+    h_status = host(torch.full((n,), 99, dtype=torch.int32))
     mq = int(wl.seeds["l_query"].max())
     mt = int((wl.seeds["rmax1"] - wl.seeds["rmax0"]).max())
 
