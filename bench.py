@@ -1,7 +1,7 @@
 """Benchmark of the B200 ksw_extend2 batch path (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cfg2|cfg1|cfg4|cfg5|chains|global|seedsw] [--w W]
+                    [--workload cfg2|cfg1|cfg3|cfg4|cfg5|chains|global|seedsw] [--w W]
                     [--schedule auto|plain|sorted|learned]
 
 A step extends every job of one synthetic batch once: the uneven left+right extension
@@ -17,6 +17,10 @@ step), so scaling is weak and `value` is the sum over ranks / the slowest rank's
 --impl reference times the reference's own CPU ksw_extend2 (oracle/_ref, compiled from
 bwa/src/ksw.cu) on all host threads over the same workload, or the C restatement of it
 when oracle/_ref is absent.
+
+`cfg3` is config 3's own recipe: the cost model trained on 2M traces of config 1's generator,
+scheduling 1M held-out jobs of that generator (prediction error and warp idle fraction of
+each schedule in the line).
 
 `cfg5` is the seed-level band-retry stream (g3x_extend_seeds_stream, 2M seeds from host memory
 in 64k-job chunks), learned width classes against the plain kernel, its regions compared with the
@@ -56,13 +60,17 @@ WORKLOADS = {
              "reads, divergence U[0,5%], 20% unrelated targets, w={w}, a=1 b=4 o=6 e=1 zdrop=100"),
     "cfg1": (1, 100000, 100, 0.0,
              "100k right-extension jobs, qlen U[1,150], 1% subs / 0.1% indels, w={w} flank"),
+    "cfg3": (1, 1000000, 100, 0.0,
+             "learned cost-model scheduling as config 3 states it: the model trained on 2M traces of "
+             "config 1's generator, the schedule on 1M held-out jobs of that generator (right "
+             "extensions, qlen U[1,150], 1% subs / 0.1% indels, w={w} flank)"),
     "cfg4": (4, 200000, 100, 0.0,
              "200k long-segment jobs, qlen log-uniform [500,5000], divergence U[0.1%,1%], indels "
              "up to 20 bp, w={w}"),
 }
 # Trace units of the learned model's training batch per workload (the generator's units: seeds
 # for cfg2, jobs otherwise), about 2M jobs where that stays within host memory.
-TRAIN_UNITS = {"cfg2": 1_000_000, "cfg1": 2_000_000, "cfg4": 200_000}
+TRAIN_UNITS = {"cfg2": 1_000_000, "cfg1": 2_000_000, "cfg3": 2_000_000, "cfg4": 200_000}
 
 
 def workload(args):

@@ -267,8 +267,8 @@ static int run_scheduled(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParams
     int rc = alloc_sched(ctx->sched, base.n);
     if (rc) return rc;
     const float* pred = nullptr;
-    if (learned) {
-        if (!ctx->model.params || !ctx->model.trained) return G3X_ERR_NOT_TRAINED;
+    if (learned && (!ctx->model.params || !ctx->model.trained)) return G3X_ERR_NOT_TRAINED;
+    if (learned && ctx->model.active) {
         if ((rc = model_features(base.jobs, base.n, base.codes, base.nmask, base.n_bases, ctx->sched.feat, st)))
             return rc;
         if ((rc = model_predict(ctx->model.params, ctx->sched.feat, base.n, ctx->sched.pred, st))) return rc;
@@ -288,7 +288,7 @@ int run_class_wave(void* user, const LaunchDesc& d, const ScoreParams& sp, cudaS
     SchedScratch& sched = *res.sched;
     const float* pred = nullptr;
     int rc;
-    if (w->learned) {
+    if (w->learned && ctx->model.active) {
         if ((rc = model_features(d.jobs, d.n, d.codes, d.nmask, d.n_bases, sched.feat, st, d.order, d.count)))
             return rc;
         if ((rc = model_predict(ctx->model.params, sched.feat, d.n, sched.pred, st))) return rc;
@@ -605,7 +605,7 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     const float* pred = nullptr;
-    if (schedule == G3X_SCHED_LEARNED) {
+    if (schedule == G3X_SCHED_LEARNED && ctx->model.active) {
         rc = g3x::model_features(d_jobs, n, d_codes, d_nmask, n_bases, ctx->sched.feat, st);
         if (rc == G3X_OK) rc = g3x::model_predict(ctx->model.params, ctx->sched.feat, n, ctx->sched.pred, st);
         pred = ctx->sched.pred;
@@ -807,6 +807,12 @@ int g3x_mlp_predict(g3x_ctx* ctx, const float* d_feat, int32_t n, float* d_pred,
     if (!ctx->model.params) return G3X_ERR_NOT_TRAINED;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
     return g3x::model_predict(ctx->model.params, d_feat, n, d_pred, (cudaStream_t)stream);
+}
+
+int g3x_mlp_set_active(g3x_ctx* ctx, int32_t active) {
+    if (!ctx || (active != 0 && active != 1)) return G3X_ERR_INVALID;
+    ctx->model.active = active;
+    return G3X_OK;
 }
 
 int g3x_mlp_get_params(g3x_ctx* ctx, float* h_params) {

@@ -374,6 +374,7 @@ struct ModelState {
     int batch_cap = 0, perm_cap = 0;
     long long t = 0;       // Adam step
     int trained = 0;       // parameters set by training or by the caller
+    int active = 1;        // 0: the learned schedule uses the length order (no inference)
 };
 int model_alloc(ModelState& M, int batch);
 void model_free(ModelState& M);

@@ -33,7 +33,7 @@ def row_target(rows, tlen):
     return (np.log2(1.0 + rows.astype(np.float64)) - np.log2(1.0 + tlen.astype(np.float64))).astype(np.float32)
 
 
-def traces(ctx, n, seed, kind=1, w=100, unrelated=0.2, score=None):
+def traces(ctx, n, seed, kind=1, w=100, unrelated=0.2, score=None, with_jobs=False):
     """(features [m,5] device, targets [m] device, cells numpy) from the m jobs the generator
     `kind` makes for n units (jobs for kind 1, seeds for kind 2, segments for kind 4); the
     targets are row_target of the plain kernel's row counts."""
@@ -56,6 +56,8 @@ def traces(ctx, n, seed, kind=1, w=100, unrelated=0.2, score=None):
     torch.cuda.synchronize()
     if (status != 0).any():
         raise RuntimeError("trace run reported job errors")
+    if with_jobs:
+        return feat, target, cells.cpu().numpy(), wl.jobs
     return feat, target, cells.cpu().numpy()
 
 
@@ -64,13 +66,60 @@ def lr_schedule(lr, epochs):
     return [lr * 0.5 ** max(0, e - 1) for e in range(epochs)]
 
 
+# The learned schedule is kept only if, on the training traces, its order saves at least this
+# fraction of the warps' row work against the length order (warp_work); otherwise the length order
+# is already as good and the context falls back to it without running the inference.
+MIN_GAIN = 0.03
+
+
+def sort_keys(jobs, score, tiles, corr=None):
+    """The counting sort's key of each job (g3x_sched.cu cost_kernel): width class, then row bin
+    (log2(1 + tlen), plus min(0, corr + 1) when learned), then row-width bin."""
+    q = jobs["qlen"].astype(np.int64)
+    t = jobs["tlen"].astype(np.int64)
+    mat = np.asarray(score["mat"]).reshape(-1)
+    max_sc, eb = int(mat.max()), int(score["end_bonus"][0])
+    w = jobs["w"].astype(np.int64)
+    for o, e in ((int(score["o_ins"][0]), int(score["e_ins"][0])), (int(score["o_del"][0]), int(score["e_del"][0]))):
+        num = q * max_sc + eb - o
+        w = np.minimum(w, np.maximum(np.where(num >= 0, num // e + 1, 1), 1))
+    wide = np.minimum(q, 2 * w + 1)
+    widths = np.array([tw[0] for tw in tiles], np.int64)
+    cls = np.minimum(np.searchsorted(widths, q, side="left"), len(widths) - 1)
+    lr = np.log2(1.0 + t)
+    if corr is not None:
+        lr = lr + np.minimum(corr + 1.0, 0.0)
+    rb = np.clip(((16.0 - lr) * 4.0).astype(np.int64), 0, 63)
+    wb = 31 - np.minimum((wide + 7) >> 3, 31)
+    return cls * 2048 + rb * 32 + wb, cls, np.maximum((wide + 7) >> 3, 1)
+
+
+def warp_work(keys, cls, rows, blocks):
+    """Row work of warps that take 32 consecutive jobs of a width class in key order: per warp,
+    its longest job's rows times its widest job's row blocks (a row-synchronous warp's cost)."""
+    o = np.argsort(keys, kind="stable")
+    c, r, b = cls[o], rows[o].astype(np.int64), blocks[o].astype(np.int64)
+    total = 0
+    for k in np.unique(c):
+        sel = c == k
+        rk, bk = r[sel], b[sel]
+        pad = (-len(rk)) % 32
+        rk = np.concatenate([rk, np.zeros(pad, np.int64)]).reshape(-1, 32)
+        bk = np.concatenate([bk, np.zeros(pad, np.int64)]).reshape(-1, 32)
+        total += int((rk.max(1) * bk.max(1)).sum())
+    return total
+
+
 def train(ctx, n_train=2_000_000, seed_train=0xA11CE, epochs=5, batch=4096, lr=2e-3, init_seed=17,
           kind=1, w=100, unrelated=0.2):
     """Trains the context's model on the traces of n_train generator units, one g3x_mlp_train
-    call per epoch (the Adam state carries over) with the rate of lr_schedule; returns a
-    metrics dict."""
+    call per epoch (the Adam state carries over) with the rate of lr_schedule, and makes the
+    learned schedule consult it only if its order saves at least MIN_GAIN of the warps' row work
+    on those traces against the length order, with the context's width classes
+    (g3x_mlp_set_active); returns a metrics dict."""
     t0 = time.perf_counter()
-    feat, target, _ = traces(ctx, n_train, seed_train, kind=kind, w=w, unrelated=unrelated)
+    feat, target, _, jobs = traces(ctx, n_train, seed_train, kind=kind, w=w, unrelated=unrelated,
+                                   with_jobs=True)
     m = int(target.shape[0])
     t1 = time.perf_counter()
     ctx.mlp_init(init_seed)
@@ -78,9 +127,22 @@ def train(ctx, n_train=2_000_000, seed_train=0xA11CE, epochs=5, batch=4096, lr=2
     losses = [float(ctx.mlp_train(feat, target, m, 1, batch, r, seed=init_seed + e)[0])
               for e, r in enumerate(rates)]
     t2 = time.perf_counter()
+    import torch
+    pred = torch.zeros(m, dtype=torch.float32, device="cuda")
+    ctx.mlp_predict(feat, m, pred)
+    corr = pred.cpu().numpy().astype(np.float64)
+    tl = jobs["tlen"].astype(np.float64)
+    rows = np.rint(np.exp2(target.cpu().numpy().astype(np.float64) + np.log2(1.0 + tl)) - 1.0)
+    score, tiles = g.default_score(), ctx.get_tiles()
+    k_sorted, cls, blocks = sort_keys(jobs, score, tiles)
+    k_learned, _, _ = sort_keys(jobs, score, tiles, corr)
+    work_sorted, work_learned = warp_work(k_sorted, cls, rows, blocks), warp_work(k_learned, cls, rows, blocks)
+    gain = 1.0 - work_learned / max(work_sorted, 1)
+    ctx.mlp_set_active(gain >= MIN_GAIN)
     return {"traces": m, "trace_kind": kind, "trace_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3),
             "epochs": epochs, "batch": batch, "lr": [round(r, 6) for r in rates],
-            "loss_curve": [round(x, 5) for x in losses], "params": g.MLP_PARAMS}
+            "loss_curve": [round(x, 5) for x in losses], "params": g.MLP_PARAMS,
+            "warp_work_gain_on_traces": round(gain, 4), "active": bool(gain >= MIN_GAIN)}
 
 
 def prediction_error(ctx, jobs, d_jobs, n, d_codes, d_nmask, rows):

@@ -556,6 +556,11 @@ int g3x_mlp_gradient(g3x_ctx *ctx, const float *d_feat, const float *d_target, i
                      float *h_grad, float *h_loss);
 /* d_pred[k] = model output for job k. Asynchronous on `stream`. */
 int g3x_mlp_predict(g3x_ctx *ctx, const float *d_feat, int32_t n, float *d_pred, void *stream);
+/* Whether G3X_SCHED_LEARNED consults the model (1, the default) or falls back to the length order
+   without running the feature and network kernels (0): for workloads where the model predicts
+   no early ends, its order is the length order and the inference would only cost time.  The
+   trainer (g3sa_b200.learn) sets it from its traces. */
+int g3x_mlp_set_active(g3x_ctx *ctx, int32_t active);
 int g3x_mlp_get_params(g3x_ctx *ctx, float *h_params);
 int g3x_mlp_set_params(g3x_ctx *ctx, const float *h_params);
 
