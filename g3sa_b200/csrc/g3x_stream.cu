@@ -167,6 +167,22 @@ int extend_seeds_stream(StreamScratch& ss, const g3x_opt_t& opt, const ScorePara
     }
     const int64_t total_code_words = (n_bases + 15) / 16, total_mask_words = (n_bases + 31) / 32;
     const bool seeds_pinned = pinned(h_seeds), out_pinned = pinned(h_regs) && pinned(h_status);
+    // Each lane's seed pipeline for a full chunk (about 75 launches and copies) is captured as a
+    // CUDA graph at the lane's first full chunk of the call and replayed for the next ones: the
+    // host work per chunk, not the device, had bounded the stream.  A graph sees the lane's
+    // buffers at their capacity (the chunk's seeds lie inside its copied plane range by
+    // construction, so no read leaves the copied words), and the seeds are re-based on the copy
+    // stream, so nothing in it changes from chunk to chunk.  The last, partial chunk and any
+    // failed capture take the direct launches.
+    cudaGraphExec_t gx[kStreamLanes] = {};
+    bool graphs = true;
+    auto drop_graphs = [&]() {
+        for (int l = 0; l < kStreamLanes; ++l)
+            if (gx[l]) {
+                cudaGraphExecDestroy(gx[l]);
+                gx[l] = nullptr;
+            }
+    };
     auto drain = [&](int l) -> int {
         StreamSet& s = ss.set[l];
         if (s.pending < 0) return G3X_OK;
@@ -190,7 +206,10 @@ int extend_seeds_stream(StreamScratch& ss, const g3x_opt_t& opt, const ScorePara
         if (cwn > ss.code_words || mwn > ss.mask_words) {
             // a wider range than the sets hold: let every lane finish, then grow them
             for (int k = 0; k < kStreamLanes && rc == G3X_OK; ++k) rc = drain(k);
-            if (rc || (rc = grow_stream(ss, chunk, cwn + cwn / 4, mwn + mwn / 4))) break;
+            if (rc) break;
+            for (int k = 0; k < kStreamLanes; ++k) cudaStreamSynchronize(ss.set[k].comp);
+            drop_graphs();                               // their buffers are about to move
+            if ((rc = grow_stream(ss, chunk, cwn + cwn / 4, mwn + mwn / 4))) break;
         }
         if ((rc = drain(l))) break;                      // lane free: its last chunk is done
         const g3x_seed_t* src = h_seeds + R.first;
@@ -200,17 +219,50 @@ int extend_seeds_stream(StreamScratch& ss, const g3x_opt_t& opt, const ScorePara
         }
         if (cudaMemcpyAsync(s.d_seeds, src, R.count * sizeof(g3x_seed_t), cudaMemcpyHostToDevice, ss.copy_st) ||
             cudaMemcpyAsync(s.d_codes, h_codes + cw0w, cwn * sizeof(uint32_t), cudaMemcpyHostToDevice, ss.copy_st) ||
-            cudaMemcpyAsync(s.d_nmask, h_nmask + mw0, mwn * sizeof(uint32_t), cudaMemcpyHostToDevice, ss.copy_st) ||
-            cudaEventRecord(s.h2d, ss.copy_st) || cudaStreamWaitEvent(s.comp, s.h2d, 0)) {
+            cudaMemcpyAsync(s.d_nmask, h_nmask + mw0, mwn * sizeof(uint32_t), cudaMemcpyHostToDevice, ss.copy_st)) {
             rc = G3X_ERR_CUDA;
             break;
         }
-        rebase_kernel<<<(unsigned)((R.count + 255) / 256), 256, 0, s.comp>>>(s.d_seeds, (int)R.count, R.base);
-        LaunchDesc cp = proto;                 // the chunk's planes: its copied words, re-based
-        cp.n_bases = std::min<int64_t>(cwn * 16, mwn * 32);
-        if ((rc = extend_seeds(s.seeds, opt, sp, s.d_seeds, (int)R.count, s.d_codes, s.d_nmask, s.d_regs,
-                               s.d_status, cp, s.comp, runner ? &wr[l] : nullptr)))
+        rebase_kernel<<<(unsigned)((R.count + 255) / 256), 256, 0, ss.copy_st>>>(s.d_seeds, (int)R.count, R.base);
+        if (cudaEventRecord(s.h2d, ss.copy_st) || cudaStreamWaitEvent(s.comp, s.h2d, 0)) {
+            rc = G3X_ERR_CUDA;
             break;
+        }
+        const WaveRunner* run_l = runner ? &wr[l] : nullptr;
+        bool done = false;
+        if (graphs && R.count == chunk) {
+            if (!gx[l]) {
+                LaunchDesc gp = proto;         // the lane's planes at their capacity
+                gp.n_bases = std::min<int64_t>(ss.code_words * 16, ss.mask_words * 32);
+                cudaGraph_t gph = nullptr;
+                if (cudaStreamBeginCapture(s.comp, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                    const int rc2 = extend_seeds(s.seeds, opt, sp, s.d_seeds, (int)R.count, s.d_codes, s.d_nmask,
+                                                 s.d_regs, s.d_status, gp, s.comp, run_l);
+                    const cudaError_t e = cudaStreamEndCapture(s.comp, &gph);
+                    if (rc2 != G3X_OK || e != cudaSuccess || cudaGraphInstantiate(&gx[l], gph, 0) != cudaSuccess)
+                        gx[l] = nullptr;
+                    if (gph) cudaGraphDestroy(gph);
+                }
+                if (!gx[l]) {
+                    graphs = false;                  // capture refused: direct launches from here on
+                    cudaGetLastError();
+                }
+            }
+            if (gx[l]) {
+                if (cudaGraphLaunch(gx[l], s.comp) != cudaSuccess) {
+                    rc = G3X_ERR_CUDA;
+                    break;
+                }
+                done = true;
+            }
+        }
+        if (!done) {
+            LaunchDesc cp = proto;             // the chunk's planes: its copied words, re-based
+            cp.n_bases = std::min<int64_t>(cwn * 16, mwn * 32);
+            if ((rc = extend_seeds(s.seeds, opt, sp, s.d_seeds, (int)R.count, s.d_codes, s.d_nmask, s.d_regs,
+                                   s.d_status, cp, s.comp, run_l)))
+                break;
+        }
         g3x_reg_t* dst_regs = out_pinned ? h_regs + R.first : s.h_regs;
         int32_t* dst_status = out_pinned ? h_status + R.first : s.h_status;
         if (cudaMemcpyAsync(dst_regs, s.d_regs, R.count * sizeof(g3x_reg_t), cudaMemcpyDeviceToHost, s.comp) ||
@@ -228,6 +280,7 @@ int extend_seeds_stream(StreamScratch& ss, const g3x_opt_t& opt, const ScorePara
     }
     for (int l = 0; l < kStreamLanes; ++l) cudaStreamSynchronize(ss.set[l].comp);
     cudaStreamSynchronize(ss.copy_st);
+    drop_graphs();
     return rc;
 }
 
