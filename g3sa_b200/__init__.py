@@ -142,6 +142,7 @@ def lib():
         L.g3x_mlp_get_params.argtypes = [P, P]
         L.g3x_mlp_set_params.argtypes = [P, P]
         L.g3x_mlp_set_active.argtypes = [P, I32]
+        L.g3x_mlp_predict_jobs.argtypes = [P, P, I32, P, P, ctypes.c_int64, P, P]
         L.g3x_get_tiles.argtypes = [P, P, P]
         L.g3x_set_tiles.argtypes = [P, P, I32]
         L.g3x_autotune.argtypes = [P, P, P, I32, P, P, ctypes.c_int64, I32, I32, P, P]
@@ -316,6 +317,12 @@ class Context:
         _check(lib().g3x_features(self._h, _ptr(d_jobs), int(n), _ptr(d_codes), _ptr(d_nmask),
                                   plane_bases(d_codes, d_nmask, n_bases), _ptr(d_feat), _stream(stream)),
                "g3x_features")
+
+    def mlp_predict_jobs(self, d_jobs, n, d_codes, d_nmask, d_pred, stream=None, n_bases=None):
+        """g3x_mlp_predict_jobs: the learned schedule's own (bf16 tensor-core) prediction per job."""
+        _check(lib().g3x_mlp_predict_jobs(self._h, _ptr(d_jobs), int(n), _ptr(d_codes), _ptr(d_nmask),
+                                          plane_bases(d_codes, d_nmask, n_bases), _ptr(d_pred), _stream(stream)),
+               "g3x_mlp_predict_jobs")
 
     def mlp_set_active(self, active):
         """g3x_mlp_set_active: 0 makes the learned schedule use the length order, no inference."""

@@ -266,15 +266,12 @@ static int run_scheduled(g3x_ctx* ctx, const LaunchDesc& base, const ScoreParams
                          cudaStream_t st) {
     int rc = alloc_sched(ctx->sched, base.n);
     if (rc) return rc;
-    const float* pred = nullptr;
     if (learned && (!ctx->model.params || !ctx->model.trained)) return G3X_ERR_NOT_TRAINED;
-    if (learned && ctx->model.active) {
-        if ((rc = model_features(base.jobs, base.n, base.codes, base.nmask, base.n_bases, ctx->sched.feat, st)))
-            return rc;
-        if ((rc = model_predict(ctx->model.params, ctx->sched.feat, base.n, ctx->sched.pred, st))) return rc;
-        pred = ctx->sched.pred;
-    }
-    if ((rc = schedule_jobs(ctx->sched, base.jobs, base.n, sp, pred, ctx->tiles, st))) return rc;
+    rc = learned && ctx->model.active
+             ? schedule_jobs_learned(ctx->sched, base.jobs, base.n, base.codes, base.nmask, base.n_bases,
+                                     ctx->model.params, sp, ctx->tiles, st)
+             : schedule_jobs(ctx->sched, base.jobs, base.n, sp, nullptr, ctx->tiles, st);
+    if (rc) return rc;
     if (cudaMemsetAsync(ctx->d_queue, 0, kMaxBuckets * sizeof(int32_t), st) != cudaSuccess ||
         cudaMemsetAsync(ctx->d_stats, 0, 4 * sizeof(unsigned long long), st) != cudaSuccess)
         return G3X_ERR_CUDA;
@@ -286,15 +283,11 @@ int run_class_wave(void* user, const LaunchDesc& d, const ScoreParams& sp, cudaS
     g3x_ctx* ctx = w->ctx;
     const ClassRes res = w->res ? *w->res : ctx_res(ctx);
     SchedScratch& sched = *res.sched;
-    const float* pred = nullptr;
-    int rc;
-    if (w->learned && ctx->model.active) {
-        if ((rc = model_features(d.jobs, d.n, d.codes, d.nmask, d.n_bases, sched.feat, st, d.order, d.count)))
-            return rc;
-        if ((rc = model_predict(ctx->model.params, sched.feat, d.n, sched.pred, st))) return rc;
-        pred = sched.pred;
-    }
-    if ((rc = schedule_jobs(sched, d.jobs, d.n, sp, pred, ctx->tiles, st, d.order, d.count))) return rc;
+    int rc = w->learned && ctx->model.active
+                 ? schedule_jobs_learned(sched, d.jobs, d.n, d.codes, d.nmask, d.n_bases, ctx->model.params, sp,
+                                         ctx->tiles, st, d.order, d.count)
+                 : schedule_jobs(sched, d.jobs, d.n, sp, nullptr, ctx->tiles, st, d.order, d.count);
+    if (rc) return rc;
     if (cudaMemsetAsync(res.queue, 0, kMaxBuckets * sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
     LaunchDesc base = d;
     base.order = nullptr; base.count = nullptr; base.order_off = nullptr; base.queue = nullptr;
@@ -604,13 +597,11 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const float* pred = nullptr;
-    if (schedule == G3X_SCHED_LEARNED && ctx->model.active) {
-        rc = g3x::model_features(d_jobs, n, d_codes, d_nmask, n_bases, ctx->sched.feat, st);
-        if (rc == G3X_OK) rc = g3x::model_predict(ctx->model.params, ctx->sched.feat, n, ctx->sched.pred, st);
-        pred = ctx->sched.pred;
-    }
-    if (rc == G3X_OK) rc = g3x::schedule_jobs(ctx->sched, d_jobs, n, sp, pred, ctx->tiles, st);
+    if (rc == G3X_OK)
+        rc = schedule == G3X_SCHED_LEARNED && ctx->model.active
+                 ? g3x::schedule_jobs_learned(ctx->sched, d_jobs, n, d_codes, d_nmask, n_bases, ctx->model.params, sp,
+                                              ctx->tiles, st)
+                 : g3x::schedule_jobs(ctx->sched, d_jobs, n, sp, nullptr, ctx->tiles, st);
     // ring of the lane kernel's ring form: every band of the batch, 2w + 16 columns, rounded up
     int32_t wmax = 0, ring = 0;
     if (rc == G3X_OK) rc = g3x::batch_max_w(d_jobs, n, sp, ctx->d_queue + 32, &wmax, st);
@@ -807,6 +798,28 @@ int g3x_mlp_predict(g3x_ctx* ctx, const float* d_feat, int32_t n, float* d_pred,
     if (!ctx->model.params) return G3X_ERR_NOT_TRAINED;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
     return g3x::model_predict(ctx->model.params, d_feat, n, d_pred, (cudaStream_t)stream);
+}
+
+int g3x_mlp_predict_jobs(g3x_ctx* ctx, const g3x_job_t* d_jobs, int32_t n, const uint32_t* d_codes,
+                         const uint32_t* d_nmask, int64_t n_bases, float* d_pred, void* stream) {
+    if (!ctx || n < 0 || (n && (!d_jobs || !d_codes || !d_nmask || !d_pred))) return G3X_ERR_INVALID;
+    if (n_bases < 1 || n_bases > 0x100000000ll) return G3X_ERR_INVALID;
+    if (!ctx->model.params) return G3X_ERR_NOT_TRAINED;
+    if (n == 0) return G3X_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return G3X_ERR_CUDA;
+    int rc = g3x::alloc_sched(ctx->sched, n);
+    if (rc) return rc;
+    // the sort keys the kernel also forms land in the context's sort scratch and are not used
+    // here; they take BWA's default scoring
+    g3x::ScoreParams sp;
+    g3x_score_t sc;
+    memset(&sc, 0, sizeof(sc));
+    for (int a = 0; a < 5; ++a)
+        for (int b = 0; b < 5; ++b) sc.mat[a * 5 + b] = a == b ? 1 : -4;
+    sc.o_del = sc.o_ins = 6; sc.e_del = sc.e_ins = 1; sc.zdrop = 100; sc.end_bonus = 5; sc.m = 5;
+    if ((rc = g3x::score_params(&sc, &sp))) return rc;
+    return g3x::schedule_jobs_learned(ctx->sched, d_jobs, n, d_codes, d_nmask, n_bases, ctx->model.params, sp,
+                                      ctx->tiles, (cudaStream_t)stream, nullptr, nullptr, d_pred);
 }
 
 int g3x_mlp_set_active(g3x_ctx* ctx, int32_t active) {

@@ -110,6 +110,16 @@ struct SchedScratch {
 int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScoreParams& sp,
                   const float* pred, const TileTable& tt, cudaStream_t st,
                   const int32_t* subset = nullptr, const int32_t* subset_n = nullptr);
+// The same sort with the learned schedule's keys: the jobs' features, the network (params) and
+// the keys in one kernel (g3x_model.cu); pred_out (optional) receives each job's prediction.
+int schedule_jobs_learned(SchedScratch& s, const g3x_job_t* jobs, int n, const uint32_t* codes,
+                          const uint32_t* nmask, int64_t n_bases, const float* params, const ScoreParams& sp,
+                          const TileTable& tt, cudaStream_t st, const int32_t* subset = nullptr,
+                          const int32_t* subset_n = nullptr, float* pred_out = nullptr);
+int launch_learned_keys(const float* params, const g3x_job_t* jobs, int n, const uint32_t* codes,
+                        const uint32_t* nmask, int64_t n_bases, const ScoreParams& sp, const TileTable& tt,
+                        int32_t* bin, int32_t* hist, cudaStream_t st, const int32_t* subset,
+                        const int32_t* subset_n, float* pred_out);
 // Largest band width w (after the clamp of ksw.cu:321-329) over n jobs; blocks.
 int batch_max_w(const g3x_job_t* jobs, int n, const ScoreParams& sp, int32_t* d_tmp, int32_t* h_out,
                 cudaStream_t st);

@@ -13,6 +13,7 @@
 #include <math.h>
 #include "g3x_internal.h"
 #include "g3x_stage.cuh"
+#include "g3x_schedkey.cuh"
 
 namespace g3x {
 
@@ -28,19 +29,11 @@ static_assert(kParams == G3X_MLP_PARAMS, "parameter count");
 // over the first min(qlen, tlen) bases (from h0, +1 per identical base pair, -4 per other pair):
 // its best score / 64 and the bases at which that score is first reached / 128.  Where the
 // diagonal's score peaks tells how far the alignment runs before z-drop, and how high, how wide
-// its band grows.  One thread per job.
-__global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
-                                const uint32_t* __restrict__ codes,
-                                const uint32_t* __restrict__ nmask, int64_t n_bases, float* __restrict__ feat,
-                                const int32_t* __restrict__ subset, const int32_t* __restrict__ subset_n) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n || (subset_n && k >= *subset_n)) return;
-    if (subset) k = subset[k];              // features of job subset[k], stored at that job
-    const g3x_job_t jb = jobs[k];
+// its band grows.
+__device__ __forceinline__ void job_features(const g3x_job_t& jb, const uint32_t* __restrict__ codes,
+                                             const uint32_t* __restrict__ nmask, int64_t n_bases,
+                                             float (&f)[kF]) {
     const bool qrev = (jb.flags & G3X_JOB_QREV) != 0, trev = (jb.flags & G3X_JOB_TREV) != 0;
-    // The ungapped extension along the seed's diagonal: from h0, +1 per identical base pair and
-    // -4 per other pair (N on either side counts as different) over the first min(qlen, tlen)
-    // bases; its best score and the number of bases at which it is first reached.
     // (a job reaching past the planes reads nothing: its diagonal stays at h0)
     const int kk = !job_in_planes(jb, n_bases) ? 0 : (jb.qlen < jb.tlen ? jb.qlen : jb.tlen);
     int32_t sc = jb.h0, best = jb.h0, best_at = 0;
@@ -66,12 +59,26 @@ __global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
             }
         }
     }
-    float* f = feat + (size_t)k * kF;
     f[0] = jb.qlen * (1.0f / 128.0f);
     f[1] = jb.tlen * (1.0f / 256.0f);
     f[2] = jb.h0 * (1.0f / 64.0f);
     f[3] = best * (1.0f / 64.0f);
     f[4] = best_at * (1.0f / 128.0f);
+}
+
+// One thread per job.
+__global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
+                                const uint32_t* __restrict__ codes,
+                                const uint32_t* __restrict__ nmask, int64_t n_bases, float* __restrict__ feat,
+                                const int32_t* __restrict__ subset, const int32_t* __restrict__ subset_n) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n || (subset_n && k >= *subset_n)) return;
+    if (subset) k = subset[k];              // features of job subset[k], stored at that job
+    float f[kF];
+    job_features(jobs[k], codes, nmask, n_bases, f);
+    float* o = feat + (size_t)k * kF;
+#pragma unroll
+    for (int i = 0; i < kF; ++i) o[i] = f[i];
 }
 
 // ---- inference ---------------------------------------------------------------------------
@@ -302,6 +309,159 @@ int model_features(const g3x_job_t* jobs, int n, const uint32_t* codes, const ui
 int model_predict(const float* params, const float* feat, int n, float* out, cudaStream_t st) {
     if (n <= 0) return G3X_OK;
     predict_kernel<<<(n + 511) / 512, 256, 0, st>>>(params, feat, n, out);
+    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
+
+// ---- the learned schedule's keys: features, network and sort key in one kernel ----------
+
+namespace {
+
+// Two floats as a bf16 pair, rounded to nearest: x in the low half, y in the high half.
+__device__ __forceinline__ uint32_t bf16x2(float x, float y) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(y), "f"(x));
+    return r;
+}
+
+// D = A B + D on the tensor cores, m16n8k16, bf16 in, fp32 accumulate (PTX fragment layouts:
+// a thread g = lane / 4, t = lane % 4 holds A rows g and g + 8 at columns 2t, 2t + 1 (registers 0,
+// 1) and 2t + 8, 2t + 9 (registers 2, 3); B rows 2t, 2t + 1 and 2t + 8, 2t + 9 of column g; C rows
+// g and g + 8 at columns 2t, 2t + 1).
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+                 "{%8,%9}, {%0,%1,%2,%3};"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+constexpr int kW2Stride = kH + 8;   // bf16 per row of W2 in shared memory (conflict-free B loads)
+
+}  // namespace
+
+// The learned schedule's sort keys (g3x_schedkey.cuh) with the network's prediction: one warp
+// per 32 sort positions, each lane one job's features; the network runs on the tensor cores for
+// each half-warp's 16 jobs (layer 1: 5 features padded to 16 columns by 64 units; layer 2: 64 by
+// 64; both bf16 with fp32 sums, the biases and ReLUs in fp32), the 64 -> 1 layer as fp32 dot
+// products reduced over the four lanes that hold a job's row.  In bf16 the prediction differs
+// from g3x_mlp_predict's fp32 by a few hundredths of a log2 unit, a tenth of the row bin the key
+// rounds it to.  Replaces three kernels of the learned schedule (features, network, keys) and
+// their round trips through memory.  pred_out (optional) receives the predictions.
+__global__ void __launch_bounds__(128) learned_keys_kernel(const g3x_job_t* __restrict__ jobs, int n,
+                                                           const uint32_t* __restrict__ codes,
+                                                           const uint32_t* __restrict__ nmask, int64_t n_bases,
+                                                           const float* __restrict__ params, ScoreParams sp,
+                                                           TileTable tt, int32_t* __restrict__ bin,
+                                                           int32_t* __restrict__ hist,
+                                                           const int32_t* __restrict__ subset,
+                                                           const int32_t* __restrict__ subset_n,
+                                                           float* __restrict__ pred_out) {
+    __shared__ uint32_t w1b[8][32];                  // layer-1 B fragments (register 0) per n-tile, lane
+    __shared__ __align__(16) uint32_t w2s[kH * kW2Stride / 2];
+    __shared__ float b1s[kH], b2s[kH], w3s[kH], b3s;
+    for (int i = threadIdx.x; i < 8 * 32; i += blockDim.x) {
+        const int nn = i >> 5, l = i & 31, u = 8 * nn + (l >> 2), f0 = 2 * (l & 3);
+        const float x = f0 < kF ? params[oW1 + u * kF + f0] : 0.0f;
+        const float y = f0 + 1 < kF ? params[oW1 + u * kF + f0 + 1] : 0.0f;
+        w1b[nn][l] = bf16x2(x, y);
+    }
+    for (int i = threadIdx.x; i < kH * kH / 2; i += blockDim.x) {
+        const int u = i / (kH / 2), c = 2 * (i % (kH / 2));
+        w2s[(u * kW2Stride + c) / 2] = bf16x2(params[oW2 + u * kH + c], params[oW2 + u * kH + c + 1]);
+    }
+    for (int i = threadIdx.x; i < kH; i += blockDim.x) {
+        b1s[i] = params[ob1 + i];
+        b2s[i] = params[ob2 + i];
+        w3s[i] = params[oW3 + i];
+    }
+    if (threadIdx.x == 0) b3s = params[ob3];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int k0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31;   // the warp's first position
+    const int cnt = subset_n ? min(n, *subset_n) : n;
+    if (k0 >= cnt) return;                                         // the whole warp
+    const int k = k0 + lane;
+    const bool valid = k < cnt;
+    const int job = valid ? (subset ? subset[k] : k) : 0;
+    g3x_job_t jb = {};
+    float f[kF] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (valid) {
+        jb = jobs[job];
+        job_features(jb, codes, nmask, n_bases, f);
+    }
+    const uint32_t p0 = bf16x2(f[0], f[1]), p1 = bf16x2(f[2], f[3]), p2 = bf16x2(f[4], 0.0f);
+    float yv[2][2];                                   // [half-warp][row g, row g + 8]
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        const int ra = 16 * mt + g, rb = ra + 8;      // the lanes holding rows g and g + 8
+        const uint32_t qa0 = __shfl_sync(0xFFFFFFFFu, p0, ra), qa1 = __shfl_sync(0xFFFFFFFFu, p1, ra),
+                       qa2 = __shfl_sync(0xFFFFFFFFu, p2, ra);
+        const uint32_t qb0 = __shfl_sync(0xFFFFFFFFu, p0, rb), qb1 = __shfl_sync(0xFFFFFFFFu, p1, rb),
+                       qb2 = __shfl_sync(0xFFFFFFFFu, p2, rb);
+        const uint32_t a1[4] = {t == 0 ? qa0 : t == 1 ? qa1 : t == 2 ? qa2 : 0u,
+                                t == 0 ? qb0 : t == 1 ? qb1 : t == 2 ? qb2 : 0u, 0u, 0u};
+        float h1[8][4];
+#pragma unroll
+        for (int nn = 0; nn < 8; ++nn) {
+            const float bx = b1s[8 * nn + 2 * t], by = b1s[8 * nn + 2 * t + 1];
+            h1[nn][0] = bx; h1[nn][1] = by; h1[nn][2] = bx; h1[nn][3] = by;
+            mma_bf16(h1[nn], a1, w1b[nn][lane], 0u);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) h1[nn][e] = fmaxf(h1[nn][e], 0.0f);
+        }
+        float h2[8][4];
+#pragma unroll
+        for (int nn = 0; nn < 8; ++nn) {
+            const float bx = b2s[8 * nn + 2 * t], by = b2s[8 * nn + 2 * t + 1];
+            h2[nn][0] = bx; h2[nn][1] = by; h2[nn][2] = bx; h2[nn][3] = by;
+        }
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            // layer 1's C fragments of n-tiles 2kk, 2kk + 1 are layer 2's A fragment of k-step kk
+            const uint32_t a2[4] = {bf16x2(h1[2 * kk][0], h1[2 * kk][1]), bf16x2(h1[2 * kk][2], h1[2 * kk][3]),
+                                    bf16x2(h1[2 * kk + 1][0], h1[2 * kk + 1][1]),
+                                    bf16x2(h1[2 * kk + 1][2], h1[2 * kk + 1][3])};
+#pragma unroll
+            for (int nn = 0; nn < 8; ++nn) {
+                const uint32_t* row = w2s + (8 * nn + g) * (kW2Stride / 2);
+                mma_bf16(h2[nn], a2, row[8 * kk + t], row[8 * kk + t + 4]);
+            }
+        }
+        float ylo = 0.0f, yhi = 0.0f;
+#pragma unroll
+        for (int nn = 0; nn < 8; ++nn) {
+            const float wx = w3s[8 * nn + 2 * t], wy = w3s[8 * nn + 2 * t + 1];
+            ylo = fmaf(wx, fmaxf(h2[nn][0], 0.0f), ylo);
+            ylo = fmaf(wy, fmaxf(h2[nn][1], 0.0f), ylo);
+            yhi = fmaf(wx, fmaxf(h2[nn][2], 0.0f), yhi);
+            yhi = fmaf(wy, fmaxf(h2[nn][3], 0.0f), yhi);
+        }
+        ylo += __shfl_xor_sync(0xFFFFFFFFu, ylo, 1);
+        ylo += __shfl_xor_sync(0xFFFFFFFFu, ylo, 2);
+        yhi += __shfl_xor_sync(0xFFFFFFFFu, yhi, 1);
+        yhi += __shfl_xor_sync(0xFFFFFFFFu, yhi, 2);
+        yv[mt][0] = ylo + b3s;
+        yv[mt][1] = yhi + b3s;
+    }
+    // the lane's own job: row r = lane % 16 of half-warp lane / 16, held by lane 4 (r % 8)
+    const int r = lane & 15, src = (r & 7) << 2;
+    const float v00 = __shfl_sync(0xFFFFFFFFu, yv[0][0], src), v01 = __shfl_sync(0xFFFFFFFFu, yv[0][1], src);
+    const float v10 = __shfl_sync(0xFFFFFFFFu, yv[1][0], src), v11 = __shfl_sync(0xFFFFFFFFu, yv[1][1], src);
+    const float pr = lane < 16 ? (r < 8 ? v00 : v01) : (r < 8 ? v10 : v11);
+    if (valid) {
+        if (pred_out) pred_out[job] = pr;
+        const int bn = sched_key(jb, sp, tt, true, pr);
+        bin[k] = bn;
+        sched_count(hist, bn);
+    }
+}
+
+int launch_learned_keys(const float* params, const g3x_job_t* jobs, int n, const uint32_t* codes,
+                        const uint32_t* nmask, int64_t n_bases, const ScoreParams& sp, const TileTable& tt,
+                        int32_t* bin, int32_t* hist, cudaStream_t st, const int32_t* subset,
+                        const int32_t* subset_n, float* pred_out) {
+    if (n <= 0) return G3X_OK;
+    learned_keys_kernel<<<(n + 127) / 128, 128, 0, st>>>(jobs, n, codes, nmask, n_bases, params, sp, tt, bin, hist,
+                                                         subset, subset_n, pred_out);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }
 

@@ -20,15 +20,13 @@
 #include <math.h>
 #include "g3x_core.h"
 #include "g3x_internal.h"
+#include "g3x_schedkey.cuh"
 
 namespace g3x {
 
 namespace {
 
 constexpr int kLevels = kSchedLevels;  // key levels per bucket: 64 row-count x 32 width bins
-constexpr int kRowBins = 64, kWidthBins = 32;
-constexpr float kLearnedSlack = 1.0f;   // log2 rows the learned correction must exceed
-static_assert(kRowBins * kWidthBins == kLevels, "key layout");
 static_assert(kLevels % 1024 == 0 && kMaxBuckets * kLevels <= 16 * 1024, "scan: 1..16 bins per thread");
 
 // Job of sort position k: k itself, or subset[k] when sorting a subset of *subset_n jobs.
@@ -41,48 +39,9 @@ __global__ void cost_kernel(const g3x_job_t* __restrict__ jobs, int n, ScorePara
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n || (subset_n && k >= *subset_n)) return;
     const int job = job_at(k, subset);
-    const g3x_job_t jb = jobs[job];
-    const int w = clamp_w(jb.w, jb.qlen, sp.max_sc, sp.end_bonus, sp.o_del, sp.e_del, sp.o_ins, sp.e_ins);
-    const int wide = jb.qlen < 2 * w + 1 ? jb.qlen : 2 * w + 1;
-    // A class stages queries up to its width (the last class any query), and its tile covers
-    // its width, so the class follows qlen, which bounds the widest row.
-    int b = tt.n - 1;
-    for (int t = 0; t < tt.n; ++t)
-        if (tt.width[t] >= jb.qlen) { b = t; break; }
-    // A lane class holds H and E in 16-bit fields (int16x2 arithmetic when tile == 2): a job
-    // whose scores do not provably fit goes to the last class.
-    if (tt.lanes[b] == 1 && b != tt.n - 1) {
-        JobConst c;
-        c.qlen = jb.qlen; c.tlen = jb.tlen; c.h0 = jb.h0; c.w = w;
-        c.o_del = sp.o_del; c.e_del = sp.e_del; c.o_ins = sp.o_ins; c.e_ins = sp.e_ins;
-        c.oe_del = sp.oe_del; c.oe_ins = sp.oe_ins; c.zdrop = sp.zdrop;
-        bool fits = tt.tile[b] == 2 ? job_fits_int16(c, sp.max_sc) : job_fits_lane(c, sp.max_sc);
-        if (tt.tile[b] >= 64 && 2 * w + 16 > tt.tile[b]) fits = false;   // band wider than the ring
-        if (!fits) b = tt.n - 1;
-    } else if (tt.lanes[b] == 32 && tt.tile[b] >= 64 && b != tt.n - 1) {
-        // the band kernel: the band's 2w' + 2 entries fit its window, and every H stays below 2^21
-        const int64_t hmax = (int64_t)jb.qlen * sp.max_sc + (jb.h0 > 0 ? jb.h0 : 0);
-        if (2 * w + 2 > tt.tile[b] || hmax >= (1 << 21)) b = tt.n - 1;
-    }
-    // log2 of the row count, 0..16; four bins per doubling, more rows -> earlier bin
-    // The learned correction is soft-thresholded by one halving: min(0, pred + 1).  A job moves
-    // ahead of the length order only where the network predicts that it ends before half its
-    // rows (a z-drop on an unrelated target), and by how much further; its error on jobs that
-    // run to their end (a few tenths of a halving, now and then one) leaves them in length order,
-    // which is already near the true order for them.  Continuous, so jobs of equal predicted rows
-    // stay together.
-    float lr = log2f(1.0f + (float)jb.tlen);
-    if (pred) lr += fminf(pred[job] + kLearnedSlack, 0.0f);
-    int rb = (int)((16.0f - lr) * (kRowBins / 16.0f));
-    rb = rb < 0 ? 0 : (rb >= kRowBins ? kRowBins - 1 : rb);
-    // eight-column blocks of the widest row, wider -> earlier bin
-    int wb = (wide + 7) >> 3;
-    wb = kWidthBins - 1 - (wb < kWidthBins - 1 ? wb : kWidthBins - 1);
-    const int bn = b * kLevels + rb * kWidthBins + wb;
+    const int bn = sched_key(jobs[job], sp, tt, pred != nullptr, pred ? pred[job] : 0.0f);
     bin[k] = bn;
-    // one atomic per distinct bin of the warp (a batch has few populated bins)
-    const unsigned peers = __match_any_sync(__activemask(), bn);
-    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(hist + bn, __popc(peers));
+    sched_count(hist, bn);
 }
 
 // Exclusive scan of the nb bins in one block; also each bucket's (offset, count).  nb is a
@@ -183,6 +142,21 @@ int schedule_jobs(SchedScratch& s, const g3x_job_t* jobs, int n, const ScorePara
     cost_kernel<<<nb, tb, 0, st>>>(jobs, n, sp, pred, tt, s.bin, s.hist, subset, subset_n);
     scan_kernel<<<1, 1024, 0, st>>>(s.hist, nbins, s.cursor, s.bucket_oc, tt.n);
     scatter_kernel<<<nb, tb, 0, st>>>(s.bin, n, s.cursor, s.order, subset, subset_n);
+    return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
+}
+
+int schedule_jobs_learned(SchedScratch& s, const g3x_job_t* jobs, int n, const uint32_t* codes,
+                          const uint32_t* nmask, int64_t n_bases, const float* params, const ScoreParams& sp,
+                          const TileTable& tt, cudaStream_t st, const int32_t* subset, const int32_t* subset_n,
+                          float* pred_out) {
+    const int nbins = tt.n * kLevels;
+    if (cudaMemsetAsync(s.hist, 0, nbins * sizeof(int32_t), st) != cudaSuccess) return G3X_ERR_CUDA;
+    int rc = launch_learned_keys(params, jobs, n, codes, nmask, n_bases, sp, tt, s.bin, s.hist, st, subset, subset_n,
+                                 pred_out);
+    if (rc) return rc;
+    const int tb = 256, nb = (n + tb - 1) / tb;
+    scan_kernel<<<1, 1024, 0, st>>>(s.hist, nbins, s.cursor, s.bucket_oc, tt.n);
+    if (nb > 0) scatter_kernel<<<nb, tb, 0, st>>>(s.bin, n, s.cursor, s.order, subset, subset_n);
     return cudaPeekAtLastError() == cudaSuccess ? G3X_OK : G3X_ERR_CUDA;
 }
 

@@ -556,6 +556,11 @@ int g3x_mlp_gradient(g3x_ctx *ctx, const float *d_feat, const float *d_target, i
                      float *h_grad, float *h_loss);
 /* d_pred[k] = model output for job k. Asynchronous on `stream`. */
 int g3x_mlp_predict(g3x_ctx *ctx, const float *d_feat, int32_t n, float *d_pred, void *stream);
+/* d_pred[k] = the learned schedule's own prediction for job k: the features, the network in bf16
+   on the tensor cores (fp32 sums) and the sort key in one kernel, as G3X_SCHED_LEARNED computes it
+   (within a few hundredths of g3x_mlp_predict's fp32 value).  Asynchronous on `stream`. */
+int g3x_mlp_predict_jobs(g3x_ctx *ctx, const g3x_job_t *d_jobs, int32_t n, const uint32_t *d_codes,
+                         const uint32_t *d_nmask, int64_t n_bases, float *d_pred, void *stream);
 /* Whether G3X_SCHED_LEARNED consults the model (1, the default) or falls back to the length order
    without running the feature and network kernels (0): for workloads where the model predicts
    no early ends, its order is the length order and the inference would only cost time.  The

@@ -206,3 +206,25 @@ def test_learned_schedule_falls_back_to_length_order_without_early_ends():
     assert bs == bl and abs(i_s - il) <= 0.02 * max(i_s, il), stats
     m2 = learn.train(c, n_train=150000, seed_train=0x7EC, epochs=3, kind=2, w=100, unrelated=0.2)
     assert m2["active"] is True and m2["warp_work_gain_on_traces"] >= learn.MIN_GAIN, m2
+
+
+def test_scheduler_prediction_in_bf16_tracks_the_fp32_network():
+    """The learned schedule computes features, network and keys in one kernel with the network on
+    the tensor cores in bf16 (fp32 sums); its predictions stay within a few hundredths of a log2
+    unit of g3x_mlp_predict's fp32 forward pass (the schedule rounds them to row bins of 0.25)."""
+    import torch
+    from g3sa_b200 import learn
+    c = g.Context(0)
+    learn.train(c, n_train=60000, seed_train=0x7ED, epochs=2, kind=2, w=100, unrelated=0.2)
+    wl = g.synth(2, 20000, seed=0x4E1F, w=100, unrelated=0.2)
+    codes, nmask = wl.planes()
+    d_jobs, d_codes, d_nmask = to_dev(wl.jobs), to_dev(codes), to_dev(nmask)
+    feat = torch.zeros((wl.n, g.MLP_FEATURES), dtype=torch.float32, device="cuda")
+    ref = torch.zeros(wl.n, dtype=torch.float32, device="cuda")
+    fast = torch.full((wl.n,), 99.0, dtype=torch.float32, device="cuda")
+    c.features(d_jobs, wl.n, d_codes, d_nmask, feat)
+    c.mlp_predict(feat, wl.n, ref)
+    c.mlp_predict_jobs(d_jobs, wl.n, d_codes, d_nmask, fast)
+    torch.cuda.synchronize()
+    d = np.abs(fast.cpu().numpy() - ref.cpu().numpy())
+    assert np.median(d) < 0.02 and d.max() < 0.15, (np.median(d), d.max())
