@@ -66,7 +66,7 @@ WORKLOADS = {
              "extensions, qlen U[1,150], 1% subs / 0.1% indels, w={w} flank)"),
     "cfg4": (4, 200000, 100, 0.0,
              "200k long-segment jobs, qlen log-uniform [500,5000], divergence U[0.1%,1%], indels "
-             "up to 20 bp, w={w}"),
+             "up to 20 bp, w={w}, int32 scores (no int16 path)"),
 }
 # Trace units of the learned model's training batch per workload (the generator's units: seeds
 # for cfg2, jobs otherwise), about 2M jobs where that stays within host memory.
@@ -601,7 +601,9 @@ def run_cfg5_workload(args, ws, rank):
                          "sample": "whole rank-0 workload, one pass: the reference's band-retry lines, threads over seed slices",
                          "gpu_regions_identical": same_ref},
         "clocks": clk, "outputs_equal_plain_kernel": same_plain,
-        "gpu_launches": None,
+        # per chunk: the seed rebase, the five seed-level passes and four extension waves of
+        # (learned keys, scan, scatter, one launch per width class)
+        "gpu_launches": args.steps * -(-n // CFG5_CHUNK) * (1 + 5 + 4 * (3 + len(tiles))),
     }), flush=True)
 
 
@@ -1034,6 +1036,8 @@ def main():
     n = wl.n
     mq, mt = int(wl.jobs["qlen"].max()), int(wl.jobs["tlen"].max())
     ctx = g.Context(local)
+    if args.workload == "cfg4":
+        ctx.set_int16(False)    # long segments are scored in int32: no int16x2 class
     dev = torch.device("cuda", local)
     h_jobs = torch.from_numpy(wl.jobs.view(np.uint8).copy()).pin_memory()
     h_codes = torch.from_numpy(codes.view(np.uint8).copy()).pin_memory()
@@ -1274,7 +1278,9 @@ def main():
                              "kind": kind, "sample": f"whole rank-0 workload ({n} jobs), one pass",
                              "gpu_outputs_identical": bool(np.array_equal(cpu_out, plain_out))},
             "clocks": clk,
-            "gpu_launches": args.steps * (5 + sum(1 for _ in tiles)),
+            # per step: the schedule (learned keys or length keys, scan, scatter) and one
+            # persistent launch per width class
+            "gpu_launches": args.steps * (3 + len(tiles)),
         }
         print(json.dumps(line), flush=True)
     for gr in graphs.values():

@@ -150,6 +150,7 @@ def lib():
         L.g3x_last_stats.argtypes = [P, P]
         L.g3x_set_timing.argtypes = [P, I32]
         L.g3x_set_step_limit.argtypes = [P, ctypes.c_int64]
+        L.g3x_set_int16.argtypes = [P, I32]
         L.g3x_class_times.argtypes = [P, P, P, P]
         L.g3x_graph_capture.argtypes = [P, P, P, I32, P, P, P, P, P, ctypes.POINTER(P)]
         L.g3x_graph_launch.argtypes = [P, P]
@@ -383,6 +384,10 @@ class Context:
         s = np.zeros(3, np.uint64)
         _check(lib().g3x_last_stats(self._h, s.ctypes.data), "g3x_last_stats")
         return [int(v) for v in s]
+
+    def set_int16(self, enable):
+        """g3x_set_int16: False keeps the width classes (and the autotuner) to int32 kernels."""
+        _check(lib().g3x_set_int16(self._h, int(bool(enable))), "g3x_set_int16")
 
     def set_step_limit(self, limit):
         """g3x_set_step_limit: the plain kernel's per-job step bound (0: its own bound)."""

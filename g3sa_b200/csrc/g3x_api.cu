@@ -26,6 +26,7 @@ struct g3x_ctx {
     cudaEvent_t cls0[g3x::kMaxBuckets], cls1[g3x::kMaxBuckets];
     int cls_timed[g3x::kMaxBuckets];        // 1 when the last batch recorded class k
     int64_t step_limit;                     // g3x_set_step_limit (0: the kernels' own bound)
+    int no_int16;                           // g3x_set_int16(ctx, 0): width classes in int32 only
 };
 
 namespace g3x {
@@ -494,6 +495,7 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
         if ((!lane && t.lanes != 4 && t.lanes != 8 && t.lanes != 16 && t.lanes != 32) ||
             (!lane && !band && t.tile != 5 && t.tile != 9 && t.tile != 13) ||
             (lane && t.tile != 0 && t.tile != 2 && t.tile != 4 && (t.tile < 64 || t.tile % 16)) ||
+            (lane && t.tile == 2 && ctx->no_int16) ||
             t.width < 1 ||
             (k && t.width <= h[k - 1].width) || (t.warp_batch != 0 && t.warp_batch != 1) ||
             (lane && (t.refill < 1 || t.refill > 32)))
@@ -507,6 +509,15 @@ int g3x_set_tiles(g3x_ctx* ctx, const g3x_tile_t* h, int32_t n) {
         ctx->tiles.warp_batch[k] = h[k].warp_batch;
         ctx->tiles.refill[k] = h[k].refill < 1 ? 1 : h[k].refill;
     }
+    return G3X_OK;
+}
+
+int g3x_set_int16(g3x_ctx* ctx, int32_t enable) {
+    if (!ctx || (enable != 0 && enable != 1)) return G3X_ERR_INVALID;
+    ctx->no_int16 = !enable;
+    if (!enable)
+        for (int k = 0; k < ctx->tiles.n; ++k)
+            if (ctx->tiles.lanes[k] == 1 && ctx->tiles.tile[k] == 2) ctx->tiles.tile[k] = 0;
     return G3X_OK;
 }
 
@@ -622,7 +633,8 @@ int g3x_autotune_schedule(g3x_ctx* ctx, int32_t schedule, const g3x_score_t* sco
         int nc = 0;
         if (!last && g3x::lane_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen), max_tlen) <= 200 * 1024)
             for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 0, 0, rf};
-        if (!last && g3x::lane16_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen)) <= 200 * 1024)
+        if (!last && !ctx->no_int16 &&
+            g3x::lane16_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen)) <= 200 * 1024)
             for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 2, 0, rf};
         if (!last && g3x::lane2_smem_per_warp(g3x::class_qcap(ctx->tiles, k, max_qlen)) <= 200 * 1024)
             for (int rf : {1, 8, 32}) cands[nc++] = Cand{1, 4, 0, rf};

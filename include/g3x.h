@@ -187,6 +187,13 @@ typedef struct {
    batch. */
 int g3x_get_tiles(g3x_ctx *ctx, g3x_tile_t *h_tiles, int32_t *n);
 int g3x_set_tiles(g3x_ctx *ctx, const g3x_tile_t *h_tiles, int32_t n);
+/* Whether the context's width classes may use the int16x2 lane kernel (1, a new context's
+   setting) or compute every cell in int32 (0), for workloads that rule the 16-bit path out.
+   With 0 the context's int16x2 classes become int32 lane classes (tile 0, same refill),
+   g3x_autotune considers int32 kernels only, and g3x_set_tiles refuses tile 2 with
+   G3X_ERR_INVALID.  An explicit G3X_KERNEL_LANE16 batch is not affected.  Outputs are the same
+   either way. */
+int g3x_set_int16(g3x_ctx *ctx, int32_t enable);
 /* Fits the width classes to the given jobs (device buffers) and tunes them: the class widths
    become max_qlen x (0.138, 0.241, 0.379, 0.552, 0.724, 0.862, 1) (rounded up to 8 columns,
    duplicates dropped) plus

@@ -224,3 +224,35 @@ def test_gpu_ring_long_fresh():
     assert (status.cpu().numpy() == 0).all()
     np.testing.assert_array_equal(out.cpu().numpy(), ref)
     assert (cells.cpu().numpy() == rcells).all()
+
+
+def test_gpu_int32_only_classes():
+    """g3x_set_int16(ctx, 0): the context's int16x2 classes turn int32, set_tiles refuses tile 2,
+    the autotuner keeps to int32 kernels, and the outputs stay the oracle's (long segments at
+    w = 100 and short jobs, which the int16x2 kernel would otherwise take)."""
+    import torch
+    from tests.gpu_util import to_dev
+    ctx = g.Context(0)
+    assert any(t[1] == 1 and t[2] == 2 for t in ctx.get_tiles())
+    ctx.set_int16(False)
+    assert not any(t[1] == 1 and t[2] == 2 for t in ctx.get_tiles())
+    with pytest.raises(g.G3xError):
+        ctx.set_tiles([(128, 1, 2, 0, 8), (1 << 30, 32, 9, 0, 1)])
+    sc = g.default_score()
+    for kind, n, w in ((4, 300, 100), (2, 4000, 100)):
+        wl = g.synth(kind, n, seed=0x1632 + kind, w=w, unrelated=0.1)
+        ref, rcells, _ = nat.oracle_extend(wl.jobs, wl.u8, sc)
+        codes, nmask = wl.planes()
+        d_jobs, d_codes, d_nmask = to_dev(wl.jobs), to_dev(codes), to_dev(nmask)
+        mq, mt = int(wl.jobs["qlen"].max()), int(wl.jobs["tlen"].max())
+        tiles = ctx.autotune(sc, d_jobs, wl.n, d_codes, d_nmask, mq, mt)
+        assert not any(t[1] == 1 and t[2] == 2 for t in tiles), tiles
+        out = torch.full((wl.n, 6), -777, dtype=torch.int32, device="cuda")
+        status = torch.full((wl.n,), 99, dtype=torch.int32, device="cuda")
+        cells = torch.full((wl.n,), -1, dtype=torch.int32, device="cuda")
+        ctx.extend_batch(sc, d_jobs, wl.n, d_codes, d_nmask, out, status, mq, mt,
+                         schedule=g.SCHED_SORTED, d_cells=cells)
+        torch.cuda.synchronize()
+        assert (status.cpu().numpy() == 0).all()
+        np.testing.assert_array_equal(out.cpu().numpy(), ref)
+        assert (cells.cpu().numpy() == rcells).all()
