@@ -90,7 +90,9 @@ int run_job(const g3x_job_t& jb, const uint8_t* u8, const ScoreParams& sp, const
         // the warp's widest row in the kernel can have more blocks than this lane's: vary it
         const int kmax = nblk + (int)((i * 2654435761u + (uint32_t)jb.q_off) >> 30);
         uint32_t mF, mL;
-        l16::row_blocks<kSym>(P, 0, r, pc, ge, nblk, kmax, mF, mL);
+        // a one-block row elsewhere in the warp masks this lane's last block too: vary it
+        const bool any_single = nblk == 1 || ((i * 2246822519u + (uint32_t)jb.t_off) >> 31);
+        l16::row_blocks<kSym>(P, 0, r, pc, ge, nblk, kmax, any_single, mF, mL);
         l16::row_end(J, P, 0, r, sp, nonempty, mF, mL);
     }
     const Commit& K = J.K;

@@ -163,12 +163,13 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
         const bool nonempty = run && r.beg < r.end;
         const int nblk = run ? blocks_in_row(r) : 0;
         const int kmax = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nblk);
+        const bool any_single = __any_sync(0xFFFFFFFFu, nblk == 1);
         busy += nblk;
         idle += kmax - nblk;
 
         // ---- the row's blocks: masked first block, middle blocks two at a time, masked last block ----
         uint32_t mF, mL;
-        row_blocks<kSym>(P, lane, r, pc, ge, nblk, kmax, mF, mL);
+        row_blocks<kSym>(P, lane, r, pc, ge, nblk, kmax, any_single, mF, mL);
 
         // ---- row end (ksw.cu:371-391) ----
         G3X_PHASE(2);

@@ -85,6 +85,28 @@ G3X_HD int clz32(uint32_t x) {
     return x ? __builtin_clz(x) : 32;
 #endif
 }
+// Index of the highest set bit, -1 for 0 (PTX bfind.u32).
+G3X_HD int msb32(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    int r;
+    asm("bfind.u32 %0, %1;" : "=r"(r) : "r"(x));
+    return r;
+#else
+    return x ? 31 - __builtin_clz(x) : -1;
+#endif
+}
+// Bits pos .. pos + width - 1 set, for 0 <= pos < 32 and 0 < width <= 8 (PTX bmsk.clamp.b32;
+// other arguments give some mask that callers discard).
+G3X_HD uint32_t bits_at(int pos, int width) {
+#if defined(__CUDA_ARCH__)
+    uint32_t r;
+    asm("bmsk.clamp.b32 %0, %1, %2;" : "=r"(r) : "r"(pos), "r"(width));
+    return r;
+#else
+    if (width <= 0 || pos < 0 || pos >= 32) return 0u;
+    return (uint32_t)((((uint64_t)1 << (width < 32 ? width : 32)) - 1u) << pos);
+#endif
+}
 
 // Scores of columns p and p+4 of a block as int16x2: byte p of lo and byte p of hi, each
 // sign-extended to 16 bits.
@@ -203,12 +225,14 @@ G3X_HD void block_core(const uint32_t (&H2)[4], const uint32_t (&E2)[4], uint32_
     phase_b(a, r, pc, nh, h2);
 }
 
-// Row maximum of a block (of the given H words) into the running key.
+// Row maximum of a block (of the given H words) into the running key (max << 16) | kb: one key
+// per half of the block's pair maximum, the larger of the two and the running key kept (on
+// ties the later block, whose index is larger).
 G3X_HD void block_max(const uint32_t (&hm)[4], int32_t kb, RowState& r) {
     const uint32_t b2 = __vimax3_s16x2(__vimax3_s16x2(hm[0], hm[1], hm[2]), hm[3], hm[3]);
-    const uint32_t bx = __vimax3_s16x2(b2, prmt(b2, b2, 0x1032u), b2);   // max in both halves
-    const int32_t key = (int32_t)prmt((uint32_t)kb, bx, 0x7610u);        // (max << 16) | kb
-    r.key = r.key > key ? r.key : key;
+    const int32_t klo = (int32_t)prmt((uint32_t)kb, b2, 0x5410u);   // (low half << 16) | kb
+    const int32_t khi = (int32_t)prmt((uint32_t)kb, b2, 0x7610u);   // (high half << 16) | kb
+    r.key = __vimax3_s32(r.key, klo, khi);
 }
 
 // Bit t set when column jb+t of a block's words (H and E pairs in registers) is non-zero: every
@@ -291,21 +315,25 @@ G3X_HD uint32_t block_first(const Planes& P, int lane, int32_t jb, RowState& r, 
 // end keep their words, columns >= end stay out of the row maximum, r.h1 = H(i, end - 1).  When
 // column end is in the block its words become {h1, 0} here (ksw.cu:371): its H word is H(i, end-1)
 // as computed, its E word is cleared.  Returns the columns of the block up to column end whose
-// new H or E word is non-zero.
+// new H or E word is non-zero.  mask_beg: some lane of the warp runs a one-block row (the same
+// for every lane, so the branch is uniform); only then are words left of beg zeroed here.
 template <bool kSym>
-G3X_HD uint32_t block_last(const Planes& P, int lane, int32_t jb, bool first, RowState& r,
-                       const PairConst& pc, const uint4* ge) {
+G3X_HD uint32_t block_last(const Planes& P, int lane, int32_t jb, bool first, bool mask_beg, RowState& r,
+                           const PairConst& pc, const uint4* ge) {
     const int at = ((jb >> 3) << 5) + lane;
     const uint4 hq = P.H[at], eq = P.E[at];
-    const uint4 A = ge[first ? r.beg - jb : 0];
     const int hi = r.end - jb;                       // 1 .. 8
     const uint4 gv = ge[hi], gw = ge[hi + 1];
     const uint32_t Hq[4] = {hq.x, hq.y, hq.z, hq.w}, Eq[4] = {eq.x, eq.y, eq.z, eq.w};
-    const uint32_t Am[4] = {A.x, A.y, A.z, A.w}, V[4] = {~gv.x, ~gv.y, ~gv.z, ~gv.w};
+    const uint32_t V[4] = {~gv.x, ~gv.y, ~gv.z, ~gv.w};
     const uint32_t G[4] = {gw.x, gw.y, gw.z, gw.w};   // columns right of end
-    uint32_t H2[4], E2[4];
+    uint32_t H2[4] = {Hq[0], Hq[1], Hq[2], Hq[3]}, E2[4] = {Eq[0], Eq[1], Eq[2], Eq[3]};
+    if (mask_beg) {
+        const uint4 A = ge[first ? r.beg - jb : 0];
+        const uint32_t Am[4] = {A.x, A.y, A.z, A.w};
 #pragma unroll
-    for (int p = 0; p < 4; ++p) { H2[p] = Hq[p] & Am[p]; E2[p] = Eq[p] & Am[p]; }
+        for (int p = 0; p < 4; ++p) { H2[p] &= Am[p]; E2[p] &= Am[p]; }
+    }
     uint32_t nh[4], ne[4], h2[4], hm[4];
     block_core<kSym>(H2, E2, P.qn[(jb >> 3) * 32 + lane], r, pc, nh, ne, h2);
 #pragma unroll
@@ -336,24 +364,30 @@ G3X_HD uint32_t nonzero_cols(const Planes& P, int32_t b, int lane) {
     return (s & 0xFu) | ((s >> 12) & 0xF0u);
 }
 
-// The last column c in [lo, hi) of the block at mjb (lo, hi within mjb .. mjb + 8) with
-// H(i, c) == m, or -1.  H(i, c) sits in the H word of column c + 1: columns mjb .. mjb + 2 in
-// the low halves of words 1-3, mjb + 3 .. mjb + 6 in the high halves of words 0-3, mjb + 7 in
-// the low half of the next block's word 0.  Each half-word is reduced to 0 (equal) or 1.
-G3X_HD int32_t max_col(const Planes& P, int lane, int32_t mjb, int32_t lo, int32_t hi, int32_t m) {
-    const int at = ((mjb >> 3) << 5) + lane;
+// The column of the row maximum (ksw.cu:362-364, the last column reaching it): the last column c
+// in [beg, end) of the block in the key's low half with H(i, c) == m, the key's high half.
+// Every H of those columns is <= m and one of them equals it (the key's block reached m inside
+// the band), when m > 0; for m == 0 the result is meaningless and the caller discards it.
+// H(i, c) sits in the H word of column c + 1: columns mjb .. mjb + 2 in the low halves of words
+// 1-3, mjb + 3 .. mjb + 6 in the high halves of words 0-3, mjb + 7 in the low half of the next
+// block's word 0.  max(H - m, -1) makes each half-word 0 where H == m and all ones where
+// H < m (other values only outside [beg, end), masked off).
+G3X_HD int32_t max_col(const Planes& P, int lane, int32_t key, int32_t beg, int32_t end) {
+    const int32_t kb = key & 0xFFFF, mjb = kb << 3;
+    const int at = (kb << 5) + lane;
     const uint4 hq = P.H[at];
     const uint32_t nx = P.H32[(at + 32) << 2];
-    const uint32_t m2 = rep16(m), one = 0x00010001u;
-    const uint32_t z0 = __vimin3_u16x2(hq.x ^ m2, one, one), z1 = __vimin3_u16x2(hq.y ^ m2, one, one);
-    const uint32_t z2 = __vimin3_u16x2(hq.z ^ m2, one, one), z3 = __vimin3_u16x2(hq.w ^ m2, one, one);
-    const uint32_t zn = __vimin3_u16x2(nx ^ m2, one, one);
-    // bit t (low half: t = 0..3, high half: t = 4..7) = 1 where column mjb + t differs from m
-    const uint32_t s = z1 + 2u * z2 + 4u * z3 + 8u * prmt(z0, zn, 0x5432u);
-    const uint32_t ne = (s & 0xFu) | ((s >> 12) & 0xF0u);
-    const uint32_t range = (0xFFu >> (kLB - (hi - mjb))) & (0xFFu << (lo - mjb));
-    const uint32_t eq = ~ne & range;
-    return eq ? mjb + 31 - clz32(eq) : -1;
+    const int32_t nm = -(key >> 16);
+    const uint32_t nm2 = prmt((uint32_t)nm, (uint32_t)nm, 0x1010u), lt = 0xFFFFFFFFu;
+    const uint32_t d0 = __viaddmax_s16x2(hq.x, nm2, lt), d1 = __viaddmax_s16x2(hq.y, nm2, lt);
+    const uint32_t d2 = __viaddmax_s16x2(hq.z, nm2, lt), d3 = __viaddmax_s16x2(hq.w, nm2, lt);
+    const uint32_t dn = __viaddmax_s16x2(nx, nm2, lt);
+    // bit t (low half: t = 0..3, high half: bits 16-19 for t = 4..7) set where H < m
+    const uint32_t s = (d1 & 0x00010001u) | (d2 & 0x00020002u) | (d3 & 0x00040004u) |
+                       (prmt(d0, dn, 0x5432u) & 0x00080008u);
+    const int32_t lo = beg - mjb > 0 ? beg - mjb : 0, hi = end - mjb < kLB ? end - mjb : kLB;
+    const uint32_t eq = ~(s | (s >> 12)) & bits_at(lo, hi - lo);
+    return mjb + msb32(eq);
 }
 
 // Per-lane job state.
@@ -436,11 +470,8 @@ G3X_HD void row_end(LaneJob& J, const Planes& P, int lane, const RowState& r, co
     }
     RowDone rd;
     rd.m = r.key >> 16;
-    rd.mj = -1;
-    if (rd.m > 0) {
-        const int32_t mjb = (r.key & 0xFFFF) << 3;
-        rd.mj = max_col(P, lane, mjb, mjb > beg ? mjb : beg, mjb + kLB < end ? mjb + kLB : end, rd.m);
-    }
+    const int32_t mj = max_col(P, lane, r.key, beg, end);
+    rd.mj = rd.m > 0 ? mj : -1;
     rd.gval = (nonempty ? end : beg) == J.qlen ? r.h1 : -1;
     rd.ncells = nonempty ? end - beg : 0;
     commit_row_sel(J.K, job_const(J, sp), rd);
@@ -489,10 +520,11 @@ G3X_HD void row_end(LaneJob& J, const Planes& P, int lane, const RowState& r, co
 // blocks any lane of the warp has in this row, and every lane walks the same iterations, doing
 // only its own blocks: the first (masked), the middle ones two at a time (one alone when an odd
 // number of them is left for the warp), the last (masked).  Returns the first block's and the
-// last block's non-zero column masks for row_end in mF, mL.
+// last block's non-zero column masks for row_end in mF, mL.  any_single: some lane of the warp
+// has a one-block row (nblk == 1).
 template <bool kSym>
 G3X_HD void row_blocks(const Planes& P, int lane, RowState& r, const PairConst& pc, const uint4* ge,
-                       int nblk, int kmax, uint32_t& mF, uint32_t& mL) {
+                       int nblk, int kmax, bool any_single, uint32_t& mF, uint32_t& mL) {
     mF = mL = 0;
     const int32_t jb0 = r.beg & ~(kLB - 1);
     if (nblk > 1) mF = block_first<kSym>(P, lane, jb0, r, pc, ge);
@@ -500,7 +532,7 @@ G3X_HD void row_blocks(const Planes& P, int lane, RowState& r, const PairConst& 
     for (; k + 1 < kmax - 1; k += 2)
         if (k < nblk - 1) block_mid2<kSym>(P, lane, jb0 + k * kLB, k + 1 < nblk - 1, r, pc);
     if (k < kmax - 1 && k < nblk - 1) block_mid<kSym>(P, lane, jb0 + k * kLB, r, pc);
-    if (nblk > 0) mL = block_last<kSym>(P, lane, jb0 + (nblk - 1) * kLB, nblk == 1, r, pc, ge);
+    if (nblk > 0) mL = block_last<kSym>(P, lane, jb0 + (nblk - 1) * kLB, nblk == 1, any_single, r, pc, ge);
 }
 
 // Blocks of a row with a non-empty band [beg, end).
