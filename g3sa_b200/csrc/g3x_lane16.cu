@@ -81,7 +81,12 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
     LaneJob J;
     J.job = -1;
     bool exhausted = false;
+    // occupancy counters (diagnostics): 32-bit sums per row, folded into the 64-bit totals at
+    // every refill wave, every job end and every 16 rows of a running lane, so a lane's sums
+    // span at most 16 rows of its job, or the rows of the warp between its job's end and the next
+    // wave
     unsigned long long busy = 0, idle = 0, waves = 0;
+    uint32_t busy32 = 0, kmax32 = 0;
 #ifdef G3X_PHASE_CLOCKS
     unsigned long long ph_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long t0_ = clock64();
@@ -99,6 +104,7 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
             first = __shfl_sync(0xFFFFFFFFu, first, 0);
             if (first + want >= n) exhausted = true;
             ++waves;
+            busy += busy32; idle += kmax32 - busy32; busy32 = kmax32 = 0;
             if ((idle_mask >> lane) & 1u) {
                 const int slot = first + __popc(idle_mask & ((1u << lane) - 1u));
                 if (slot < n) {
@@ -148,11 +154,11 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
         const bool run = active && !J.K.stop;
 
         // ---- row begin (ksw.cu:335-345) ----
-        RowState r;
-        r.beg = 0; r.end = 0; r.h1 = 0; r.plo = 0; r.phi = 0; r.fr = 0; r.hlast = 0; r.key = 0;
+        RowState r;                             // set by row_begin; read only by running lanes
         if (run) {
             const int32_t i = J.K.next;
             if ((i & 15) == 0 && i > 0) {       // the prefetched chunk, then the next one's words
+                busy += busy32; idle += kmax32 - busy32; busy32 = kmax32 = 0;
                 decode16(J.t_off, J.tlen, i >> 4, J.trev, J.pv, J.pm, J.tx, J.tn);
                 const int ch = (i >> 4) + 1;
                 if ((ch << 4) < J.tlen) load16_raw(d.codes, d.nmask, J.t_off, J.tlen, ch, J.trev, J.pv, J.pm);
@@ -164,8 +170,8 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
         const int nblk = run ? blocks_in_row(r) : 0;
         const int kmax = __reduce_max_sync(0xFFFFFFFFu, (unsigned)nblk);
         const bool any_single = __any_sync(0xFFFFFFFFu, nblk == 1);
-        busy += nblk;
-        idle += kmax - nblk;
+        busy32 += nblk;
+        kmax32 += kmax;
 
         // ---- the row's blocks: masked first block, middle blocks two at a time, masked last block ----
         uint32_t mF, mL;
@@ -182,6 +188,7 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
             if (d.cells) d.cells[J.job] = (int32_t)K.cells;
             if (d.rows) d.rows[J.job] = K.next;
             J.job = -1;
+            busy += busy32; idle += kmax32 - busy32; busy32 = kmax32 = 0;
         }
         __syncwarp();
 #ifdef G3X_PHASE_CLOCKS
@@ -196,6 +203,7 @@ __global__ void __launch_bounds__(128) lane16_kernel(LaunchDesc d, ScoreParams s
         for (int q = 0; q < 7; ++q) atomicAdd(&g3x_phase_clocks[ci][q], ph_[q]);
     }
 #endif
+    busy += busy32; idle += kmax32 - busy32;
     if (d.stats) add_warp_stats(d.stats, busy, idle, waves, lane);
     pdl_chain_end();
 }

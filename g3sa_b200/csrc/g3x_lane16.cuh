@@ -235,38 +235,38 @@ G3X_HD void block_max(const uint32_t (&hm)[4], int32_t kb, RowState& r) {
     r.key = __vimax3_s32(r.key, klo, khi);
 }
 
-// Bit t set when column jb+t of a block's words (H and E pairs in registers) is non-zero: every
-// half-word is reduced to 0 or 1 by an unsigned min, then the four pairs are summed with weights
-// 1-8 (each half stays below 16), which leaves columns 0-3 in bits 0-3 and 4-7 in bits 16-19.
-G3X_HD uint32_t nonzero_mask(const uint32_t (&h)[4], const uint32_t (&e)[4]) {
+// Bit t set when column jb+t of a block's words (H and E pairs in registers) is non-zero, for the
+// columns in keep (a mask within bits 0-7): every half-word pair becomes min(H + E, 1) (H, E >= 0
+// below 2^15 in the band, so the sum does not wrap; columns outside keep may hold anything),
+// then the four pairs are summed with weights 1-8 (each half stays below 16), which leaves
+// columns 0-3 in bits 0-3 and 4-7 in bits 16-19, folded down to bits 4-7.
+G3X_HD uint32_t nonzero_mask(const uint32_t (&h)[4], const uint32_t (&e)[4], uint32_t keep) {
     const uint32_t one = 0x00010001u;
-    const uint32_t z0 = __vimin3_u16x2(h[0] | e[0], one, one), z1 = __vimin3_u16x2(h[1] | e[1], one, one);
-    const uint32_t z2 = __vimin3_u16x2(h[2] | e[2], one, one), z3 = __vimin3_u16x2(h[3] | e[3], one, one);
+    const uint32_t z0 = __viaddmin_u16x2(h[0], e[0], one), z1 = __viaddmin_u16x2(h[1], e[1], one);
+    const uint32_t z2 = __viaddmin_u16x2(h[2], e[2], one), z3 = __viaddmin_u16x2(h[3], e[3], one);
     const uint32_t s = z0 + 2u * z1 + 4u * z2 + 8u * z3;
-    return (s & 0xFu) | ((s >> 12) & 0xF0u);
+    return (s | (s >> 12)) & keep;
 }
 
 // A block strictly inside the row.
 template <bool kSym>
-G3X_HD void block_mid(const Planes& P, int lane, int32_t jb, RowState& r, const PairConst& pc) {
-    const int at = ((jb >> 3) << 5) + lane;
+G3X_HD void block_mid(const Planes& P, int at, int32_t kb, RowState& r, const PairConst& pc) {
     const uint4 hq = P.H[at], eq = P.E[at];
     const uint32_t H2[4] = {hq.x, hq.y, hq.z, hq.w}, E2[4] = {eq.x, eq.y, eq.z, eq.w};
     uint32_t nh[4], ne[4], h2[4];
-    block_core<kSym>(H2, E2, P.qn[(jb >> 3) * 32 + lane], r, pc, nh, ne, h2);
+    block_core<kSym>(H2, E2, P.qn[at], r, pc, nh, ne, h2);
     P.H[at] = make_uint4(nh[0], nh[1], nh[2], nh[3]);
     P.E[at] = make_uint4(ne[0], ne[1], ne[2], ne[3]);
-    block_max(h2, jb >> 3, r);
+    block_max(h2, kb, r);
 }
 
 // Two consecutive blocks strictly inside the row, the second only when `second` (else nothing of
 // it is stored and the row state stays as the first block leaves it).  The F-independent
 // phases of both blocks come first, so the two blocks' instructions interleave.
 template <bool kSym>
-G3X_HD void block_mid2(const Planes& P, int lane, int32_t jb, bool second, RowState& r, const PairConst& pc) {
-    const int at = ((jb >> 3) << 5) + lane;
+G3X_HD void block_mid2(const Planes& P, int at, int32_t kb, bool second, RowState& r, const PairConst& pc) {
     const uint4 hq0 = P.H[at], eq0 = P.E[at], hq1 = P.H[at + 32], eq1 = P.E[at + 32];
-    const uint32_t qw0 = P.qn[(jb >> 3) * 32 + lane], qw1 = P.qn[((jb >> 3) + 1) * 32 + lane];
+    const uint32_t qw0 = P.qn[at], qw1 = P.qn[at + 32];
     BlockA a0, a1;
     uint32_t ne0[4], ne1[4];
     {
@@ -283,32 +283,32 @@ G3X_HD void block_mid2(const Planes& P, int lane, int32_t jb, bool second, RowSt
     phase_b(a1, r1, pc, nh1, h21);
     P.E[at] = make_uint4(ne0[0], ne0[1], ne0[2], ne0[3]);
     P.H[at] = make_uint4(nh0[0], nh0[1], nh0[2], nh0[3]);
-    block_max(h20, jb >> 3, r);
+    block_max(h20, kb, r);
     if (second) {
         P.E[at + 32] = make_uint4(ne1[0], ne1[1], ne1[2], ne1[3]);
         P.H[at + 32] = make_uint4(nh1[0], nh1[1], nh1[2], nh1[3]);
         r.fr = r1.fr;
         r.hlast = r1.hlast;
-        block_max(h21, (jb >> 3) + 1, r);
+        block_max(h21, kb + 1, r);
     }
 }
 
 // The first block of a row with two or more blocks: the words left of beg are zeroed on load.
 // Returns the columns of the block at or right of beg whose new H or E word is non-zero.
 template <bool kSym>
-G3X_HD uint32_t block_first(const Planes& P, int lane, int32_t jb, RowState& r, const PairConst& pc,
+G3X_HD uint32_t block_first(const Planes& P, int at, int32_t kb, RowState& r, const PairConst& pc,
                             const uint4* ge) {
-    const int at = ((jb >> 3) << 5) + lane;
+    const int32_t jb = kb << 3;
     const uint4 hq = P.H[at], eq = P.E[at];
     const uint4 A = ge[r.beg - jb];
     const uint32_t H2[4] = {hq.x & A.x, hq.y & A.y, hq.z & A.z, hq.w & A.w};
     const uint32_t E2[4] = {eq.x & A.x, eq.y & A.y, eq.z & A.z, eq.w & A.w};
     uint32_t nh[4], ne[4], h2[4];
-    block_core<kSym>(H2, E2, P.qn[(jb >> 3) * 32 + lane], r, pc, nh, ne, h2);
+    block_core<kSym>(H2, E2, P.qn[at], r, pc, nh, ne, h2);
     P.H[at] = make_uint4(nh[0], nh[1], nh[2], nh[3]);
     P.E[at] = make_uint4(ne[0], ne[1], ne[2], ne[3]);
-    block_max(h2, jb >> 3, r);
-    return nonzero_mask(nh, ne) & (0xFFu << (r.beg - jb));
+    block_max(h2, kb, r);
+    return nonzero_mask(nh, ne, 0xFFu << (r.beg - jb));
 }
 
 // The last block of a row (first == true: also its first, the row's only block): columns right of
@@ -318,9 +318,9 @@ G3X_HD uint32_t block_first(const Planes& P, int lane, int32_t jb, RowState& r, 
 // new H or E word is non-zero.  mask_beg: some lane of the warp runs a one-block row (the same
 // for every lane, so the branch is uniform); only then are words left of beg zeroed here.
 template <bool kSym>
-G3X_HD uint32_t block_last(const Planes& P, int lane, int32_t jb, bool first, bool mask_beg, RowState& r,
+G3X_HD uint32_t block_last(const Planes& P, int at, int32_t kb, bool first, bool mask_beg, RowState& r,
                            const PairConst& pc, const uint4* ge) {
-    const int at = ((jb >> 3) << 5) + lane;
+    const int32_t jb = kb << 3;
     const uint4 hq = P.H[at], eq = P.E[at];
     const int hi = r.end - jb;                       // 1 .. 8
     const uint4 gv = ge[hi], gw = ge[hi + 1];
@@ -335,7 +335,7 @@ G3X_HD uint32_t block_last(const Planes& P, int lane, int32_t jb, bool first, bo
         for (int p = 0; p < 4; ++p) { H2[p] &= Am[p]; E2[p] &= Am[p]; }
     }
     uint32_t nh[4], ne[4], h2[4], hm[4];
-    block_core<kSym>(H2, E2, P.qn[(jb >> 3) * 32 + lane], r, pc, nh, ne, h2);
+    block_core<kSym>(H2, E2, P.qn[at], r, pc, nh, ne, h2);
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
         nh[p] = (nh[p] & ~G[p]) | (Hq[p] & G[p]);   // columns <= end: new; beyond: as they were
@@ -344,11 +344,15 @@ G3X_HD uint32_t block_last(const Planes& P, int lane, int32_t jb, bool first, bo
     }
     P.H[at] = make_uint4(nh[0], nh[1], nh[2], nh[3]);
     P.E[at] = make_uint4(ne[0], ne[1], ne[2], ne[3]);
-    block_max(hm, jb >> 3, r);
+    block_max(hm, kb, r);
+    // H(i, end - 1): column t = hi - 1, half t >> 2 of word t & 3, taken from the words (t & 2,
+    // (t & 2) + 1) by one permute of bytes off, off + 1 with off = 4 (t & 1) + 2 (t >> 2) (the
+    // nibbles of 0x62624040), zero-extended (the sign of H's high byte: H >= 0)
     const int t = hi - 1;
-    const uint32_t wl = (t & 2) ? ((t & 1) ? h2[3] : h2[2]) : ((t & 1) ? h2[1] : h2[0]);
-    r.h1 = (int32_t)((t & 4) ? (wl >> 16) : (wl & 0xFFFFu));
-    return nonzero_mask(nh, ne) & (0xFFu >> (7 - (hi < 8 ? hi : 7)));
+    const bool w2 = (t & 2) != 0;
+    const uint32_t off = (0x62624040u >> (t << 2)) & 0xFu;
+    r.h1 = (int32_t)prmt(w2 ? h2[2] : h2[0], w2 ? h2[3] : h2[1], off * 0x1111u + 0x9910u);
+    return nonzero_mask(nh, ne, 0xFFu >> (7 - (hi < 8 ? hi : 7)));
 }
 
 // Bit t set when column b+t (b a multiple of 8) has a non-zero H or E word: every half-word is
@@ -361,7 +365,7 @@ G3X_HD uint32_t nonzero_cols(const Planes& P, int32_t b, int lane) {
     const uint32_t z0 = __vimin3_u16x2(hq.x | eq.x, one, one), z1 = __vimin3_u16x2(hq.y | eq.y, one, one);
     const uint32_t z2 = __vimin3_u16x2(hq.z | eq.z, one, one), z3 = __vimin3_u16x2(hq.w | eq.w, one, one);
     const uint32_t s = z0 + 2u * z1 + 4u * z2 + 8u * z3;
-    return (s & 0xFu) | ((s >> 12) & 0xF0u);
+    return (s | (s >> 12)) & 0xFFu;
 }
 
 // The column of the row maximum (ksw.cu:362-364, the last column reaching it): the last column c
@@ -436,18 +440,20 @@ G3X_HD void row_begin(const LaneJob& J, const ScoreParams& sp, const uint2* pool
 // branches: to-end score, cell count, new maximum or z-drop, last row.
 G3X_HD void commit_row_sel(Commit& k, const JobConst& c, const RowDone& d) {
     const int32_t i = k.next;
-    const bool g = d.gval >= 0;
-    k.max_ie = (g && !(k.gscore > d.gval)) ? i : k.max_ie;                  // ksw.cu:372-375
-    k.gscore = (g && d.gval > k.gscore) ? d.gval : k.gscore;
+    // ksw.cu:372-375 for gval >= 0 (gval -1: no to-end score this row); gscore starts at -1 and
+    // only grows, so it is the running maximum of gval, and max_ie moves to i where gval >= 0
+    // reaches it
+    k.max_ie = d.gval >= (k.gscore > 0 ? k.gscore : 0) ? i : k.max_ie;
+    k.gscore = d.gval > k.gscore ? d.gval : k.gscore;
     k.cells += d.ncells;
     k.next = i + 1;
     const bool up = d.m > k.best;                                            // ksw.cu:377-379
     const int32_t di = i - k.best_i, dj = d.mj - k.best_j;                   // ksw.cu:380-386
     const int32_t drop = di > dj ? k.best - d.m - (di - dj) * c.e_del : k.best - d.m - (dj - di) * c.e_ins;
     const bool zstop = !up && c.zdrop > 0 && drop > c.zdrop;
-    const int32_t off = d.mj > i ? d.mj - i : i - d.mj;
-    k.max_off = up && off > k.max_off ? off : k.max_off;
-    k.best = up ? d.m : k.best;
+    const int32_t off = abs(d.mj - i);
+    k.max_off = up ? (off > k.max_off ? off : k.max_off) : k.max_off;
+    k.best = d.m > k.best ? d.m : k.best;
     k.best_i = up ? i : k.best_i;
     k.best_j = up ? d.mj : k.best_j;
     k.stop = d.m == 0 || zstop || k.next >= c.tlen;                         // ksw.cu:376, the row loop
@@ -526,13 +532,15 @@ template <bool kSym>
 G3X_HD void row_blocks(const Planes& P, int lane, RowState& r, const PairConst& pc, const uint4* ge,
                        int nblk, int kmax, bool any_single, uint32_t& mF, uint32_t& mL) {
     mF = mL = 0;
-    const int32_t jb0 = r.beg & ~(kLB - 1);
-    if (nblk > 1) mF = block_first<kSym>(P, lane, jb0, r, pc, ge);
-    int k = 1;
-    for (; k + 1 < kmax - 1; k += 2)
-        if (k < nblk - 1) block_mid2<kSym>(P, lane, jb0 + k * kLB, k + 1 < nblk - 1, r, pc);
-    if (k < kmax - 1 && k < nblk - 1) block_mid<kSym>(P, lane, jb0 + k * kLB, r, pc);
-    if (nblk > 0) mL = block_last<kSym>(P, lane, jb0 + (nblk - 1) * kLB, nblk == 1, any_single, r, pc, ge);
+    const int32_t kb0 = r.beg >> 3;                 // block index of the first block
+    const int at0 = (kb0 << 5) + lane;              // its uint4 index in the lane-interleaved planes
+    if (nblk > 1) mF = block_first<kSym>(P, at0, kb0, r, pc, ge);
+    int k = 1, at = at0 + 32;
+    for (; k + 1 < kmax - 1; k += 2, at += 64)
+        if (k < nblk - 1) block_mid2<kSym>(P, at, kb0 + k, k + 1 < nblk - 1, r, pc);
+    if (k < kmax - 1 && k < nblk - 1) block_mid<kSym>(P, at, kb0 + k, r, pc);
+    if (nblk > 0)
+        mL = block_last<kSym>(P, at0 + ((nblk - 1) << 5), kb0 + nblk - 1, nblk == 1, any_single, r, pc, ge);
 }
 
 // Blocks of a row with a non-empty band [beg, end).
