@@ -320,7 +320,9 @@ class Context:
                "g3x_features")
 
     def mlp_predict_jobs(self, d_jobs, n, d_codes, d_nmask, d_pred, stream=None, n_bases=None):
-        """g3x_mlp_predict_jobs: the learned schedule's own (bf16 tensor-core) prediction per job."""
+        """g3x_mlp_predict_jobs: the correction the learned schedule applies per job (its bf16
+        tensor-core prediction, or 0 where the near-diagonal check keeps an early call in the
+        length order)."""
         _check(lib().g3x_mlp_predict_jobs(self._h, _ptr(d_jobs), int(n), _ptr(d_codes), _ptr(d_nmask),
                                           plane_bases(d_codes, d_nmask, n_bases), _ptr(d_pred), _stream(stream)),
                "g3x_mlp_predict_jobs")

@@ -66,6 +66,58 @@ __device__ __forceinline__ void job_features(const g3x_job_t& jb, const uint32_t
     f[4] = best_at * (1.0f / 128.0f);
 }
 
+// Whether one of the 16 diagonals next to the seed's (offsets 1-8 either way) matches at least
+// kNearMatch of its first kNearLen base pairs (N on either side is no match).  The learned
+// schedule asks this of the jobs the network calls early-ending: such a job's seed is followed
+// by an indel and then by the same sequence, which its ungapped features (the seed's own
+// diagonal) cannot see, and it runs most of its rows; on config-2 jobs the check holds for about
+// 60% of the network's false early calls and for almost none of its right ones.
+constexpr int kNearDiag = 8, kNearLen = 32, kNearMatch = 18;
+
+// Bases 0 .. 47 of one sequence as 2-bit codes (lo: bases 0-31, hi: 32-47) and N bits.
+__device__ __forceinline__ void load48(const uint32_t* __restrict__ codes, const uint32_t* __restrict__ nmask,
+                                       uint32_t off, int len, bool rev, uint64_t& lo, uint32_t& hi,
+                                       uint64_t& nb) {
+    uint32_t x[3] = {0u, 0u, 0u}, n[3] = {0u, 0u, 0u};
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+        if ((ch << 4) < len) load16(codes, nmask, off, len, ch, rev, x[ch], n[ch]);
+    lo = (uint64_t)x[0] | ((uint64_t)x[1] << 32);
+    hi = x[2];
+    nb = (uint64_t)n[0] | ((uint64_t)n[1] << 16) | ((uint64_t)n[2] << 32);
+}
+
+// 32 bases from base a (0 <= a <= 8) of a sequence held as load48 leaves it.
+__device__ __forceinline__ uint64_t window32(uint64_t lo, uint32_t hi, int a) {
+    return a == 0 ? lo : (lo >> (2 * a)) | ((uint64_t)hi << (64 - 2 * a));
+}
+
+__device__ bool near_diagonal(const g3x_job_t& jb, const uint32_t* __restrict__ codes,
+                              const uint32_t* __restrict__ nmask, int64_t n_bases) {
+    if (!job_in_planes(jb, n_bases)) return false;
+    uint64_t qlo, tlo, qn, tn;
+    uint32_t qhi, thi;
+    load48(codes, nmask, jb.q_off, jb.qlen, (jb.flags & G3X_JOB_QREV) != 0, qlo, qhi, qn);
+    load48(codes, nmask, jb.t_off, jb.tlen, (jb.flags & G3X_JOB_TREV) != 0, tlo, thi, tn);
+#pragma unroll 1
+    for (int s = 0; s < 2 * kNearDiag; ++s) {
+        // offsets 1..8: query base k against target base k + d; -1..-8: query k + d, target k
+        const int d = 1 + (s >> 1), a = (s & 1) ? d : 0, b = (s & 1) ? 0 : d;
+        const int kk = min(kNearLen, min(jb.qlen - a, jb.tlen - b));
+        if (kk < kNearMatch) continue;
+        uint64_t x = window32(qlo, qhi, a) ^ window32(tlo, thi, b);
+        x = (x | (x >> 1)) & 0x5555555555555555ull;            // one bit per base: codes differ
+        x = (x | (x >> 1)) & 0x3333333333333333ull;
+        x = (x | (x >> 2)) & 0x0F0F0F0F0F0F0F0Full;
+        x = (x | (x >> 4)) & 0x00FF00FF00FF00FFull;
+        x = (x | (x >> 8)) & 0x0000FFFF0000FFFFull;
+        const uint32_t diff = (uint32_t)(x | (x >> 16)) | (uint32_t)(qn >> a) | (uint32_t)(tn >> b);
+        const uint32_t valid = kk >= 32 ? 0xFFFFFFFFu : (1u << kk) - 1u;
+        if (__popc(~diff & valid) >= kNearMatch) return true;
+    }
+    return false;
+}
+
 // One thread per job.
 __global__ void features_kernel(const g3x_job_t* __restrict__ jobs, int n,
                                 const uint32_t* __restrict__ codes,
@@ -345,7 +397,8 @@ constexpr int kW2Stride = kH + 8;   // bf16 per row of W2 in shared memory (conf
 // products reduced over the four lanes that hold a job's row.  In bf16 the prediction differs
 // from g3x_mlp_predict's fp32 by a few hundredths of a log2 unit, a tenth of the row bin the key
 // rounds it to.  Replaces three kernels of the learned schedule (features, network, keys) and
-// their round trips through memory.  pred_out (optional) receives the predictions.
+// their round trips through memory.  pred_out (optional) receives the corrections the keys use:
+// the predictions, or 0 where near_diagonal keeps an early call in the length order.
 __global__ void __launch_bounds__(128) learned_keys_kernel(const g3x_job_t* __restrict__ jobs, int n,
                                                            const uint32_t* __restrict__ codes,
                                                            const uint32_t* __restrict__ nmask, int64_t n_bases,
@@ -447,9 +500,12 @@ __global__ void __launch_bounds__(128) learned_keys_kernel(const g3x_job_t* __re
     const float v00 = __shfl_sync(0xFFFFFFFFu, yv[0][0], src), v01 = __shfl_sync(0xFFFFFFFFu, yv[0][1], src);
     const float v10 = __shfl_sync(0xFFFFFFFFu, yv[1][0], src), v11 = __shfl_sync(0xFFFFFFFFu, yv[1][1], src);
     const float pr = lane < 16 ? (r < 8 ? v00 : v01) : (r < 8 ? v10 : v11);
+    // a job the network calls early-ending stays in the length order when a diagonal next to the
+    // seed's continues the alignment (near_diagonal)
+    const float corr = valid && pr + kLearnedSlack < 0.0f && near_diagonal(jb, codes, nmask, n_bases) ? 0.0f : pr;
     if (valid) {
-        if (pred_out) pred_out[job] = pr;
-        const int bn = sched_key(jb, sp, tt, true, pr);
+        if (pred_out) pred_out[job] = corr;
+        const int bn = sched_key(jb, sp, tt, true, corr);
         bin[k] = bn;
         sched_count(hist, bn);
     }

@@ -57,7 +57,7 @@ def traces(ctx, n, seed, kind=1, w=100, unrelated=0.2, score=None, with_jobs=Fal
     if (status != 0).any():
         raise RuntimeError("trace run reported job errors")
     if with_jobs:
-        return feat, target, cells.cpu().numpy(), wl.jobs
+        return feat, target, cells.cpu().numpy(), wl.jobs, (d_jobs, d_codes, d_nmask)
     return feat, target, cells.cpu().numpy()
 
 
@@ -118,8 +118,8 @@ def train(ctx, n_train=2_000_000, seed_train=0xA11CE, epochs=5, batch=4096, lr=2
     on those traces against the length order, with the context's width classes
     (g3x_mlp_set_active); returns a metrics dict."""
     t0 = time.perf_counter()
-    feat, target, _, jobs = traces(ctx, n_train, seed_train, kind=kind, w=w, unrelated=unrelated,
-                                   with_jobs=True)
+    feat, target, _, jobs, (d_jobs, d_codes, d_nmask) = traces(ctx, n_train, seed_train, kind=kind, w=w,
+                                                               unrelated=unrelated, with_jobs=True)
     m = int(target.shape[0])
     t1 = time.perf_counter()
     ctx.mlp_init(init_seed)
@@ -128,8 +128,10 @@ def train(ctx, n_train=2_000_000, seed_train=0xA11CE, epochs=5, batch=4096, lr=2
               for e, r in enumerate(rates)]
     t2 = time.perf_counter()
     import torch
+    # the corrections the learned schedule itself would apply (its bf16 network and the
+    # near-diagonal check), so that the simulated order is the one it would run
     pred = torch.zeros(m, dtype=torch.float32, device="cuda")
-    ctx.mlp_predict(feat, m, pred)
+    ctx.mlp_predict_jobs(d_jobs, m, d_codes, d_nmask, pred)
     corr = pred.cpu().numpy().astype(np.float64)
     tl = jobs["tlen"].astype(np.float64)
     rows = np.rint(np.exp2(target.cpu().numpy().astype(np.float64) + np.log2(1.0 + tl)) - 1.0)

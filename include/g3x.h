@@ -563,9 +563,13 @@ int g3x_mlp_gradient(g3x_ctx *ctx, const float *d_feat, const float *d_target, i
                      float *h_grad, float *h_loss);
 /* d_pred[k] = model output for job k. Asynchronous on `stream`. */
 int g3x_mlp_predict(g3x_ctx *ctx, const float *d_feat, int32_t n, float *d_pred, void *stream);
-/* d_pred[k] = the learned schedule's own prediction for job k: the features, the network in bf16
-   on the tensor cores (fp32 sums) and the sort key in one kernel, as G3X_SCHED_LEARNED computes it
-   (within a few hundredths of g3x_mlp_predict's fp32 value).  Asynchronous on `stream`. */
+/* d_pred[k] = the correction the learned schedule applies to job k's row key: the features, the
+   network in bf16 on the tensor cores (fp32 sums) and the sort key in one kernel, as
+   G3X_SCHED_LEARNED computes it (within a few hundredths of g3x_mlp_predict's fp32 value), except
+   that a job the network calls early-ending (prediction below -1) gets 0 when one of the 16
+   diagonals next to the seed's (offsets 1-8 either way) matches at least 18 of its first 32 base
+   pairs: such a job continues past an indel and keeps its place in the length order.
+   Asynchronous on `stream`. */
 int g3x_mlp_predict_jobs(g3x_ctx *ctx, const g3x_job_t *d_jobs, int32_t n, const uint32_t *d_codes,
                          const uint32_t *d_nmask, int64_t n_bases, float *d_pred, void *stream);
 /* Whether G3X_SCHED_LEARNED consults the model (1, the default) or falls back to the length order
