@@ -30,9 +30,17 @@ static_assert(kParams == G3X_MLP_PARAMS, "parameter count");
 // its best score / 64 and the bases at which that score is first reached / 128.  Where the
 // diagonal's score peaks tells how far the alignment runs before z-drop, and how high, how wide
 // its band grows.
+// The first three 16-base chunks of a job's query and target as load16 leaves them (2-bit codes,
+// N bits), and which of them are loaded.
+struct Head48 {
+    uint32_t qx[3], qn[3], tx[3], tn[3];
+    int loaded;                          // chunks 0 .. loaded - 1 of both sequences
+};
+
+// head (optional) keeps the chunks the diagonal walk loads among the first three.
 __device__ __forceinline__ void job_features(const g3x_job_t& jb, const uint32_t* __restrict__ codes,
                                              const uint32_t* __restrict__ nmask, int64_t n_bases,
-                                             float (&f)[kF]) {
+                                             float (&f)[kF], Head48* head = nullptr) {
     const bool qrev = (jb.flags & G3X_JOB_QREV) != 0, trev = (jb.flags & G3X_JOB_TREV) != 0;
     // (a job reaching past the planes reads nothing: its diagonal stays at h0)
     const int kk = !job_in_planes(jb, n_bases) ? 0 : (jb.qlen < jb.tlen ? jb.qlen : jb.tlen);
@@ -41,6 +49,12 @@ __device__ __forceinline__ void job_features(const g3x_job_t& jb, const uint32_t
         uint32_t xq, nq, xt, nt;
         load16(codes, nmask, jb.q_off, jb.qlen, ch, qrev, xq, nq);
         load16(codes, nmask, jb.t_off, jb.tlen, ch, trev, xt, nt);
+        if (head && ch < 3) {                      // (constant indices: the chunks stay in registers)
+#pragma unroll
+            for (int c3 = 0; c3 < 3; ++c3)
+                if (c3 == ch) { head->qx[c3] = xq; head->qn[c3] = nq; head->tx[c3] = xt; head->tn[c3] = nt; }
+            head->loaded = ch + 1;
+        }
         const int nv = kk - (ch << 4) < 16 ? kk - (ch << 4) : 16;
         // bit t of m: base t of the chunk differs (2-bit codes differ, or N on either side)
         const uint32_t d2 = xq ^ xt;
@@ -74,14 +88,18 @@ __device__ __forceinline__ void job_features(const g3x_job_t& jb, const uint32_t
 // 60% of the network's false early calls and for almost none of its right ones.
 constexpr int kNearDiag = 8, kNearLen = 32, kNearMatch = 18;
 
-// Bases 0 .. 47 of one sequence as 2-bit codes (lo: bases 0-31, hi: 32-47) and N bits.
+// Bases 0 .. 47 of one sequence as 2-bit codes (lo: bases 0-31, hi: 32-47) and N bits, from the
+// chunks the feature walk loaded (the first `have`) and the planes for the rest.
 __device__ __forceinline__ void load48(const uint32_t* __restrict__ codes, const uint32_t* __restrict__ nmask,
-                                       uint32_t off, int len, bool rev, uint64_t& lo, uint32_t& hi,
+                                       uint32_t off, int len, bool rev, const uint32_t (&hx)[3],
+                                       const uint32_t (&hn)[3], int have, uint64_t& lo, uint32_t& hi,
                                        uint64_t& nb) {
     uint32_t x[3] = {0u, 0u, 0u}, n[3] = {0u, 0u, 0u};
 #pragma unroll
-    for (int ch = 0; ch < 3; ++ch)
-        if ((ch << 4) < len) load16(codes, nmask, off, len, ch, rev, x[ch], n[ch]);
+    for (int ch = 0; ch < 3; ++ch) {
+        if (ch < have) { x[ch] = hx[ch]; n[ch] = hn[ch]; }
+        else if ((ch << 4) < len) load16(codes, nmask, off, len, ch, rev, x[ch], n[ch]);
+    }
     lo = (uint64_t)x[0] | ((uint64_t)x[1] << 32);
     hi = x[2];
     nb = (uint64_t)n[0] | ((uint64_t)n[1] << 16) | ((uint64_t)n[2] << 32);
@@ -93,12 +111,14 @@ __device__ __forceinline__ uint64_t window32(uint64_t lo, uint32_t hi, int a) {
 }
 
 __device__ bool near_diagonal(const g3x_job_t& jb, const uint32_t* __restrict__ codes,
-                              const uint32_t* __restrict__ nmask, int64_t n_bases) {
+                              const uint32_t* __restrict__ nmask, int64_t n_bases, const Head48& head) {
     if (!job_in_planes(jb, n_bases)) return false;
     uint64_t qlo, tlo, qn, tn;
     uint32_t qhi, thi;
-    load48(codes, nmask, jb.q_off, jb.qlen, (jb.flags & G3X_JOB_QREV) != 0, qlo, qhi, qn);
-    load48(codes, nmask, jb.t_off, jb.tlen, (jb.flags & G3X_JOB_TREV) != 0, tlo, thi, tn);
+    load48(codes, nmask, jb.q_off, jb.qlen, (jb.flags & G3X_JOB_QREV) != 0, head.qx, head.qn, head.loaded,
+           qlo, qhi, qn);
+    load48(codes, nmask, jb.t_off, jb.tlen, (jb.flags & G3X_JOB_TREV) != 0, head.tx, head.tn, head.loaded,
+           tlo, thi, tn);
 #pragma unroll 1
     for (int s = 0; s < 2 * kNearDiag; ++s) {
         // offsets 1..8: query base k against target base k + d; -1..-8: query k + d, target k
@@ -437,9 +457,11 @@ __global__ void __launch_bounds__(128) learned_keys_kernel(const g3x_job_t* __re
     const int job = valid ? (subset ? subset[k] : k) : 0;
     g3x_job_t jb = {};
     float f[kF] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    Head48 head;
+    head.loaded = 0;
     if (valid) {
         jb = jobs[job];
-        job_features(jb, codes, nmask, n_bases, f);
+        job_features(jb, codes, nmask, n_bases, f, &head);
     }
     const uint32_t p0 = bf16x2(f[0], f[1]), p1 = bf16x2(f[2], f[3]), p2 = bf16x2(f[4], 0.0f);
     float yv[2][2];                                   // [half-warp][row g, row g + 8]
@@ -502,7 +524,7 @@ __global__ void __launch_bounds__(128) learned_keys_kernel(const g3x_job_t* __re
     const float pr = lane < 16 ? (r < 8 ? v00 : v01) : (r < 8 ? v10 : v11);
     // a job the network calls early-ending stays in the length order when a diagonal next to the
     // seed's continues the alignment (near_diagonal)
-    const float corr = valid && pr + kLearnedSlack < 0.0f && near_diagonal(jb, codes, nmask, n_bases) ? 0.0f : pr;
+    const float corr = valid && pr + kLearnedSlack < 0.0f && near_diagonal(jb, codes, nmask, n_bases, head) ? 0.0f : pr;
     if (valid) {
         if (pred_out) pred_out[job] = corr;
         const int bn = sched_key(jb, sp, tt, true, corr);
