@@ -431,7 +431,7 @@ CFG5_CHUNK = 32768       # seeds per chunk: 64k extension jobs, a left and a rig
 CFG5_DESC = ("band-retry stream: 2M seeds of the uneven left+right generator (100/150/250 bp reads, divergence "
              "U[0,5%], 20% unrelated targets) = 4M ksw_extend2 jobs before retries, each side run with w=100 "
              "and again with w=200 when the score changed and max_off >= 3w/4 (at most 2 tries), from pinned "
-             "host memory in 64k-job chunks (32k seeds), pinned copies with four chunks in flight (the config's "
+             "host memory in 64k-job chunks (32k seeds), pinned copies with seven chunks in flight (the config's "
              "double buffering, two sets deeper); a=1 b=4 o=6 e=1 zdrop=100")
 
 
@@ -578,7 +578,7 @@ def run_cfg5_workload(args, ws, rank):
         "config": cfg,
         "setup": {"chunk_seeds": CFG5_CHUNK, "chunks": chunks, "width_classes": tiles,
                   "note": "the workload lives in host memory: every step copies each chunk's seeds and plane "
-                          "words in and its regions out (pinned staging, four chunks in flight); value and e2e are the same "
+                          "words in and its regions out (pinned staging, seven chunks in flight); value and e2e are the same "
                           "measurement"},
         "seeds_per_s": round(tot_n / (t_learned * 1e-3), 1),
         "extensions_per_s": round(int(regs["learned"]["tries_left"].sum() + regs["learned"]["tries_right"].sum())

@@ -302,10 +302,11 @@ int run_class_wave(void* user, const LaunchDesc& d, const ScoreParams& sp, cudaS
 // compute stream with its own device buffer set, pinned staging, seed scratch and width-class
 // scratch, so one chunk's latency-bound waves overlap the next chunks' work.  A lane chains its
 // classes on its own stream as programmatic dependent launches (they still run side by side),
-// so the whole stream stays within a few CUDA streams: more streams than the device's hardware
-// work queues alias onto the same queues and serialise.  Kept in the context between calls and
-// grown on demand.
-constexpr int kStreamLanes = 4;
+// so the whole stream stays within eight CUDA streams (seven lanes and the copy stream), the
+// hardware work queues a context has by default: more streams than queues alias onto the same
+// queues and serialise.  Config 5 (2M seeds, 32k-seed chunks): 40.6 ms with four lanes, 33.8 with
+// six, 33.0 with seven.  Kept in the context between calls and grown on demand.
+constexpr int kStreamLanes = 7;
 struct StreamSet {
     g3x_seed_t* d_seeds = nullptr;
     uint32_t* d_codes = nullptr;

@@ -269,7 +269,7 @@ int g3x_extend_seeds(g3x_ctx *ctx, const g3x_opt_t *opt, const g3x_seed_t *d_see
                      int32_t *d_status, const g3x_batch_opts_t *opts, void *stream);
 
 /* The same over n host seeds in chunks of `chunk` seeds: each chunk's seeds and the plane
-   words they reference are copied to the GPU while the chunks before it are extended (four
+   words they reference are copied to the GPU while the chunks before it are extended (seven
    chunks in flight, each with its own device buffer set, pinned staging and compute stream,
    beside one copy stream), and the regions come back to h_regs/h_status.  Host planes should
    be pinned for the copies to overlap.  Blocks until all chunks are done.  A chunk with a
